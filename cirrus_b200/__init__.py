@@ -1,0 +1,314 @@
+"""cirrus_b200 -- B200-native GMG-PCG pressure solver for adaptive octree-tile grids.
+
+Python host layer over the C ABI of include/cirrus_b200.h.  It mirrors the reference's
+interface for the Poisson path (wang-mengdi/Cirrus):
+
+  reference                                   here
+  HADeviceGrid(h0, log2 hashes) + setTileHost  Topology(...).set_tile(...)
+  compressHost / syncHostAndDevice             Topology.compress()
+  SpawnGhostTiles / IterativeRefine            Topology.spawn_ghost_tiles() / iterative_refine()
+  CalcCellTypesFromLeafs                       Topology.calc_cell_types_from_leafs()
+  tile channels on the device                  DeviceGrid (HBM tile pool)
+  FullNegativeLaplacian, VCycle, Dot, ...      DeviceGrid methods
+  GMGSolver(one_over_alpha, prolong_coeff)     GMGSolver(...)
+    .solve(grid, verbose, max_iters, tol,       .solve(grid, verbose, max_iters, tol,
+           level_iters, coarsest_iters,                level_iters, coarsest_iters,
+           sync_stride, is_pure_neumann)               sync_stride, is_pure_neumann)
+           -> (iters, relative_residual)               -> (iters, relative_residual)
+
+All compute runs in the native library on the GPU; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable, Sequence
+
+import numpy as np
+
+from ._native import (CirrusError, LEVEL_TARGET_FN, SolveParams, SolveResult, check, lib)
+
+__all__ = [
+    "LEAF", "NONLEAF", "GHOST", "DIRICHLET", "INTERIOR", "NEUMANN",
+    "X_CHANNEL", "B_CHANNEL", "R_CHANNEL", "P_CHANNEL", "AP_CHANNEL", "Z_CHANNEL", "TMP_CHANNEL", "U_CHANNEL",
+    "FLUID_EULER_LOG2_HASH", "Topology", "DeviceGrid", "GMGSolver", "CirrusError", "lib",
+]
+
+LEAF, NONLEAF, GHOST = 1, 2, 4
+DIRICHLET, INTERIOR, NEUMANN = 1, 2, 4
+X_CHANNEL, B_CHANNEL, R_CHANNEL, P_CHANNEL, AP_CHANNEL, Z_CHANNEL, TMP_CHANNEL, U_CHANNEL = 0, 1, 1, 2, 3, 4, 5, 6
+PRECISION_FP32, PRECISION_MIXED_FP64 = 0, 1
+
+# per-level hash sizes of FluidEuler's grid (src/FluidEuler.h:416)
+FLUID_EULER_LOG2_HASH = (16, 16, 16, 16, 16, 16, 18, 16, 16, 16)
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class Topology:
+    """Octree of 8^3 tiles built on the host exactly as the reference builds it."""
+
+    def __init__(self, h0: float = 1.0 / 8, levels_log2_hash: Sequence[int] = FLUID_EULER_LOG2_HASH):
+        self.num_layers = len(levels_log2_hash)
+        self.h0 = float(h0)
+        arr = (C.c_uint32 * self.num_layers)(*levels_log2_hash)
+        h = C.c_void_p()
+        check(lib().cirrus_topology_create(self.num_layers, arr, self.h0, C.byref(h)), "cirrus_topology_create")
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().cirrus_topology_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_tile(self, level: int, coord: Sequence[int], tile_type: int = LEAF) -> None:
+        x, y, z = (int(c) for c in coord)
+        check(lib().cirrus_topology_set_tile(self._h, level, x, y, z, tile_type), "cirrus_topology_set_tile")
+
+    def compress(self) -> None:
+        check(lib().cirrus_topology_compress(self._h), "cirrus_topology_compress")
+
+    def spawn_ghost_tiles(self) -> None:
+        check(lib().cirrus_topology_spawn_ghost_tiles(self._h), "cirrus_topology_spawn_ghost_tiles")
+
+    def refine_leafs_one_step(self, level_target: Callable[[int, int, int, int], int]) -> list[int]:
+        fn = LEVEL_TARGET_FN(lambda _u, l, x, y, z: int(level_target(l, x, y, z)))
+        out = (C.c_int * self.num_layers)()
+        check(lib().cirrus_topology_refine_leafs_one_step(self._h, fn, None, out), "cirrus_topology_refine_leafs_one_step")
+        return list(out)
+
+    def iterative_refine(self, level_target: Callable[[int, int, int, int], int] | None = None,
+                         masks: Sequence[np.ndarray | None] | None = None) -> None:
+        """IterativeRefine with a level-target callback, or with dense per-level masks
+        (masks[l][x, y, z] != 0 -> a LEAF tile at level l is refined)."""
+        if masks is not None:
+            keep, ptrs, dims = _mask_args(masks, self.num_layers)
+            check(lib().cirrus_topology_iterative_refine_masks(self._h, ptrs, dims), "cirrus_topology_iterative_refine_masks")
+            del keep
+        else:
+            fn = LEVEL_TARGET_FN(lambda _u, l, x, y, z: int(level_target(l, x, y, z)))
+            check(lib().cirrus_topology_iterative_refine(self._h, fn, None), "cirrus_topology_iterative_refine")
+
+    @property
+    def num_tiles(self) -> int:
+        n = C.c_int()
+        check(lib().cirrus_topology_num_tiles(self._h, C.byref(n)), "cirrus_topology_num_tiles")
+        return n.value
+
+    @property
+    def max_level(self) -> int:
+        n = C.c_int()
+        check(lib().cirrus_topology_max_level(self._h, C.byref(n)), "cirrus_topology_max_level")
+        return n.value
+
+    def tiles(self) -> np.ndarray:
+        """(n, 5) int32: level, x, y, z, type in all-tiles order."""
+        out = np.empty((self.num_tiles, 5), dtype=np.int32)
+        check(lib().cirrus_topology_tiles(self._h, _ptr(out, C.c_int32)), "cirrus_topology_tiles")
+        return out
+
+    def hash_slots(self) -> np.ndarray:
+        out = np.empty(self.num_tiles, dtype=np.int32)
+        check(lib().cirrus_topology_hash_slots(self._h, _ptr(out, C.c_int32)), "cirrus_topology_hash_slots")
+        return out
+
+    def neighbor_tiles(self) -> np.ndarray:
+        """(n, 6) int32 (x-, y-, z-, x+, y+, z+) as CalculateNeighborTiles fills mNeighbors."""
+        out = np.empty((self.num_tiles, 6), dtype=np.int32)
+        check(lib().cirrus_topology_neighbor_tiles(self._h, _ptr(out, C.c_int32)), "cirrus_topology_neighbor_tiles")
+        return out
+
+    def set_cell_types(self, ctypes: np.ndarray) -> None:
+        a = np.ascontiguousarray(ctypes, dtype=np.uint8).reshape(self.num_tiles, 512)
+        check(lib().cirrus_topology_set_cell_types(self._h, _ptr(a, C.c_uint8)), "cirrus_topology_set_cell_types")
+
+    def cell_types(self) -> np.ndarray:
+        out = np.empty((self.num_tiles, 512), dtype=np.uint8)
+        check(lib().cirrus_topology_cell_types(self._h, _ptr(out, C.c_uint8)), "cirrus_topology_cell_types")
+        return out
+
+    def calc_cell_types_from_leafs(self) -> None:
+        check(lib().cirrus_topology_calc_cell_types_from_leafs(self._h), "cirrus_topology_calc_cell_types_from_leafs")
+
+
+def _mask_args(masks, num_layers):
+    keep = []
+    ptrs = (C.POINTER(C.c_uint8) * num_layers)()
+    dims = (C.c_int * (3 * num_layers))()
+    for l in range(num_layers):
+        m = masks[l] if l < len(masks) else None
+        if m is None:
+            ptrs[l] = C.POINTER(C.c_uint8)()
+            continue
+        a = np.ascontiguousarray(m, dtype=np.uint8)
+        keep.append(a)
+        ptrs[l] = _ptr(a, C.c_uint8)
+        dims[3 * l], dims[3 * l + 1], dims[3 * l + 2] = a.shape
+    return keep, ptrs, dims
+
+
+class DeviceGrid:
+    """The tile pool of a finalised topology resident on the current CUDA device."""
+
+    def __init__(self, topology: Topology):
+        h = C.c_void_p()
+        check(lib().cirrus_grid_create(topology.handle, C.byref(h)), "cirrus_grid_create")
+        self._h = h
+        n = C.c_int()
+        check(lib().cirrus_grid_num_tiles(h, C.byref(n)), "cirrus_grid_num_tiles")
+        self.num_tiles = n.value
+        self.tiles = topology.tiles()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().cirrus_grid_destroy(h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def dof(self) -> int:
+        d = C.c_int64()
+        check(lib().cirrus_grid_dof(self._h, C.byref(d)), "cirrus_grid_dof")
+        return d.value
+
+    @property
+    def device_bytes(self) -> int:
+        d = C.c_size_t()
+        check(lib().cirrus_grid_device_bytes(self._h, C.byref(d)), "cirrus_grid_device_bytes")
+        return d.value
+
+    def set_channel(self, channel: int, values: np.ndarray, stream: int = 0) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float32).reshape(self.num_tiles * 512)
+        check(lib().cirrus_grid_set_channel(self._h, channel, _ptr(a, C.c_float), C.c_void_p(stream)), "cirrus_grid_set_channel")
+
+    def get_channel(self, channel: int, stream: int = 0) -> np.ndarray:
+        out = np.empty((self.num_tiles, 512), dtype=np.float32)
+        check(lib().cirrus_grid_get_channel(self._h, channel, _ptr(out, C.c_float), C.c_void_p(stream)), "cirrus_grid_get_channel")
+        return out
+
+    def channel_ptr(self, channel: int) -> int:
+        p = C.c_void_p()
+        check(lib().cirrus_grid_channel_ptr(self._h, channel, C.byref(p)), "cirrus_grid_channel_ptr")
+        return p.value
+
+    # operators ------------------------------------------------------------------------
+    def full_negative_laplacian(self, x_channel: int, Ax_channel: int, stream: int = 0) -> None:
+        check(lib().cirrus_full_negative_laplacian(self._h, x_channel, Ax_channel, C.c_void_p(stream)),
+              "cirrus_full_negative_laplacian")
+
+    def gauss_seidel_sweep(self, level: int, x_channel: int, rhs_channel: int, color: int, stream: int = 0) -> None:
+        check(lib().cirrus_gauss_seidel_sweep(self._h, level, x_channel, rhs_channel, color, C.c_void_p(stream)),
+              "cirrus_gauss_seidel_sweep")
+
+    def residual_and_restrict(self, level: int, x_channel: int, rhs_channel: int, coarse_channel: int,
+                              one_over_alpha: float = 1.0, stream: int = 0) -> None:
+        check(lib().cirrus_residual_and_restrict(self._h, level, x_channel, rhs_channel, coarse_channel, one_over_alpha,
+                                                 C.c_void_p(stream)), "cirrus_residual_and_restrict")
+
+    def prolongate_and_update(self, fine_level: int, coarse_channel: int, fine_channel: int, prolong_coeff: float = 1.0,
+                              stream: int = 0) -> None:
+        check(lib().cirrus_prolongate_and_update(self._h, fine_level, coarse_channel, fine_channel, prolong_coeff,
+                                                 C.c_void_p(stream)), "cirrus_prolongate_and_update")
+
+    def vcycle(self, x_channel: int, f_channel: int, rhs_channel: int, level_iters: int = 1, coarsest_iters: int = 10,
+               stream: int = 0) -> None:
+        check(lib().cirrus_vcycle(self._h, x_channel, f_channel, rhs_channel, level_iters, coarsest_iters, C.c_void_p(stream)),
+              "cirrus_vcycle")
+
+    def dot(self, a_channel: int, b_channel: int, stream: int = 0) -> float:
+        r = C.c_double()
+        check(lib().cirrus_dot(self._h, a_channel, b_channel, C.byref(r), C.c_void_p(stream)), "cirrus_dot")
+        return r.value
+
+    def clear_neumann_neighbor_faces(self, u_channel: int = U_CHANNEL, stream: int = 0) -> None:
+        check(lib().cirrus_clear_neumann_neighbor_faces(self._h, u_channel, C.c_void_p(stream)),
+              "cirrus_clear_neumann_neighbor_faces")
+
+    def propagate_to_children(self, channel: int, stream: int = 0) -> None:
+        check(lib().cirrus_propagate_to_children(self._h, channel, C.c_void_p(stream)), "cirrus_propagate_to_children")
+
+    def velocity_volume_divergence_on_leafs(self, u_channel: int = U_CHANNEL, div_channel: int = B_CHANNEL,
+                                            stream: int = 0) -> None:
+        check(lib().cirrus_velocity_volume_divergence_on_leafs(self._h, u_channel, div_channel, C.c_void_p(stream)),
+              "cirrus_velocity_volume_divergence_on_leafs")
+
+    def projection_rhs(self, stream: int = 0) -> None:
+        """b = divergence of the face velocities in channels 6-8, as FluidEuler::project builds it
+        after the velocity boundary step (src/FluidEuler.h:583-586, src/FluidEuler.cu:43-60)."""
+        self.clear_neumann_neighbor_faces(U_CHANNEL, stream)
+        for a in range(3):
+            self.propagate_to_children(U_CHANNEL + a, stream)
+        self.velocity_volume_divergence_on_leafs(U_CHANNEL, B_CHANNEL, stream)
+
+    def true_residual(self, b: np.ndarray, stream: int = 0) -> float:
+        a = np.ascontiguousarray(b, dtype=np.float32).reshape(self.num_tiles * 512)
+        r = C.c_double()
+        check(lib().cirrus_true_residual(self._h, _ptr(a, C.c_float), C.byref(r), C.c_void_p(stream)), "cirrus_true_residual")
+        return r.value
+
+
+class GMGSolver:
+    """Geometric-multigrid-preconditioned CG (the reference's GMGSolver, src/GMGSolver.h:17-52)."""
+
+    def __init__(self, one_over_alpha: float = 1.0, prolong_coeff: float = 1.0, precision: int = PRECISION_FP32,
+                 inner_tolerance: float = 1e-3, max_outer_iters: int = 20, warm_start: bool = False):
+        self.one_over_alpha = one_over_alpha
+        self.prolong_coeff = prolong_coeff
+        self.precision = precision
+        self.inner_tolerance = inner_tolerance
+        self.max_outer_iters = max_outer_iters
+        self.warm_start = warm_start
+        self.last_result: SolveResult | None = None
+
+    def params(self, max_iters=1000, relative_tolerance=1e-6, level_iters=1, coarsest_iters=10, sync_stride=1,
+               is_pure_neumann=False) -> SolveParams:
+        p = SolveParams()
+        lib().cirrus_solve_params_default(C.byref(p))
+        p.max_iters = max_iters
+        p.relative_tolerance = relative_tolerance
+        p.level_iters = level_iters
+        p.coarsest_iters = coarsest_iters
+        p.sync_stride = sync_stride
+        p.is_pure_neumann = int(bool(is_pure_neumann))
+        p.one_over_alpha = self.one_over_alpha
+        p.prolong_coeff = self.prolong_coeff
+        p.precision = self.precision
+        p.warm_start = int(bool(self.warm_start))
+        p.inner_tolerance = self.inner_tolerance
+        p.max_outer_iters = self.max_outer_iters
+        return p
+
+    def solve(self, grid: DeviceGrid, verbose: bool = False, max_iters: int = 1000, relative_tolerance: float = 1e-6,
+              level_iters: int = 1, coarsest_iters: int = 10, sync_stride: int = 1, is_pure_neumann: bool = False,
+              stream: int = 0) -> tuple[int, float]:
+        """Solve -lap(x) = b (b in channel 1, x to channel 0); returns (iters, relative residual).
+        As in the reference, channel 1 ends holding the final residual."""
+        p = self.params(max_iters, relative_tolerance, level_iters, coarsest_iters, sync_stride, is_pure_neumann)
+        r = SolveResult()
+        check(lib().cirrus_gmg_solve(grid.handle, C.byref(p), C.c_void_p(stream), C.byref(r)), "cirrus_gmg_solve")
+        self.last_result = r
+        if verbose:
+            print(f"GMG-PCG: {r.iters} iters, relative residual {r.rel_residual:.3e}, status {r.status}")
+        return r.iters, r.rel_residual
+
+    def solve_host(self, grid: DeviceGrid, b: np.ndarray, x_out: np.ndarray, stream: int = 0, **kw) -> tuple[int, float]:
+        """End-to-end solve from host buffers (b in, x out; all-tiles order, 512 floats/tile)."""
+        p = self.params(**kw)
+        r = SolveResult()
+        check(lib().cirrus_gmg_solve_host(grid.handle, C.byref(p), _ptr(b, C.c_float), _ptr(x_out, C.c_float),
+                                          C.c_void_p(stream), C.byref(r)), "cirrus_gmg_solve_host")
+        self.last_result = r
+        return r.iters, r.rel_residual

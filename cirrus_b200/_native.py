@@ -1,0 +1,143 @@
+"""ctypes binding of libcirrus_b200.so (the C ABI of include/cirrus_b200.h).
+
+The library is loaded from cirrus_b200/_lib/; if it is missing it is built with nvcc (see
+cirrus_b200/build.py).  There is no fallback implementation: a failure to load or a missing
+CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+_LIB = None
+_LOCK = threading.Lock()
+
+
+class CirrusError(RuntimeError):
+    """A C-ABI call returned a status other than CIRRUS_OK."""
+
+    def __init__(self, status: int, func: str):
+        self.status = status
+        msg = lib().cirrus_status_string(status).decode() if _LIB is not None else str(status)
+        super().__init__(f"{func}: {msg} (status {status})")
+
+
+CIRRUS_OK = 0
+CIRRUS_ERR_NOT_CONVERGED = 5
+CIRRUS_ERR_NO_DEVICE = 8
+
+c_int_p = C.POINTER(C.c_int)
+c_i32_p = C.POINTER(C.c_int32)
+c_u8_p = C.POINTER(C.c_uint8)
+c_f32_p = C.POINTER(C.c_float)
+c_f64_p = C.POINTER(C.c_double)
+LEVEL_TARGET_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int)
+
+
+class SolveParams(C.Structure):
+    _fields_ = [
+        ("max_iters", C.c_int),
+        ("relative_tolerance", C.c_double),
+        ("level_iters", C.c_int),
+        ("coarsest_iters", C.c_int),
+        ("sync_stride", C.c_int),
+        ("is_pure_neumann", C.c_int),
+        ("one_over_alpha", C.c_float),
+        ("prolong_coeff", C.c_float),
+        ("precision", C.c_int),
+        ("warm_start", C.c_int),
+        ("inner_tolerance", C.c_double),
+        ("max_outer_iters", C.c_int),
+    ]
+
+
+class SolveResult(C.Structure):
+    _fields_ = [
+        ("iters", C.c_int),
+        ("outer_iters", C.c_int),
+        ("rel_residual", C.c_double),
+        ("true_rel_residual", C.c_double),
+        ("status", C.c_int),
+    ]
+
+
+# name -> (restype, argtypes); status-returning functions use c_int
+_PROTOS = {
+    "cirrus_status_string": (C.c_char_p, [C.c_int]),
+    "cirrus_version": (C.c_char_p, []),
+    "cirrus_topology_create": (C.c_int, [C.c_int, C.POINTER(C.c_uint32), C.c_double, C.POINTER(C.c_void_p)]),
+    "cirrus_topology_destroy": (None, [C.c_void_p]),
+    "cirrus_topology_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "cirrus_topology_compress": (C.c_int, [C.c_void_p]),
+    "cirrus_topology_spawn_ghost_tiles": (C.c_int, [C.c_void_p]),
+    "cirrus_topology_refine_leafs_one_step": (C.c_int, [C.c_void_p, LEVEL_TARGET_FN, C.c_void_p, c_int_p]),
+    "cirrus_topology_iterative_refine": (C.c_int, [C.c_void_p, LEVEL_TARGET_FN, C.c_void_p]),
+    "cirrus_topology_iterative_refine_masks": (C.c_int, [C.c_void_p, C.POINTER(c_u8_p), c_int_p]),
+    "cirrus_topology_num_tiles": (C.c_int, [C.c_void_p, c_int_p]),
+    "cirrus_topology_max_level": (C.c_int, [C.c_void_p, c_int_p]),
+    "cirrus_topology_tiles": (C.c_int, [C.c_void_p, c_i32_p]),
+    "cirrus_topology_hash_slots": (C.c_int, [C.c_void_p, c_i32_p]),
+    "cirrus_topology_set_cell_types": (C.c_int, [C.c_void_p, c_u8_p]),
+    "cirrus_topology_cell_types": (C.c_int, [C.c_void_p, c_u8_p]),
+    "cirrus_topology_calc_cell_types_from_leafs": (C.c_int, [C.c_void_p]),
+    "cirrus_topology_neighbor_tiles": (C.c_int, [C.c_void_p, c_i32_p]),
+    "cirrus_grid_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "cirrus_grid_destroy": (None, [C.c_void_p]),
+    "cirrus_grid_num_tiles": (C.c_int, [C.c_void_p, c_int_p]),
+    "cirrus_grid_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    "cirrus_grid_dof": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "cirrus_grid_set_channel": (C.c_int, [C.c_void_p, C.c_int, c_f32_p, C.c_void_p]),
+    "cirrus_grid_get_channel": (C.c_int, [C.c_void_p, C.c_int, c_f32_p, C.c_void_p]),
+    "cirrus_grid_channel_ptr": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "cirrus_full_negative_laplacian": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "cirrus_gauss_seidel_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "cirrus_residual_and_restrict": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
+    "cirrus_prolongate_and_update": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
+    "cirrus_vcycle": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "cirrus_dot": (C.c_int, [C.c_void_p, C.c_int, C.c_int, c_f64_p, C.c_void_p]),
+    "cirrus_clear_neumann_neighbor_faces": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "cirrus_propagate_to_children": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "cirrus_velocity_volume_divergence_on_leafs": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "cirrus_solve_params_default": (None, [C.POINTER(SolveParams)]),
+    "cirrus_gmg_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveResult)]),
+    "cirrus_gmg_solve_host": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p, C.POINTER(SolveResult)]),
+    "cirrus_true_residual": (C.c_int, [C.c_void_p, c_f32_p, c_f64_p, C.c_void_p]),
+}
+
+
+def library_path() -> Path:
+    from . import build as _build
+
+    return _build.LIB
+
+
+def lib():
+    """Load (building first if needed) and return the native library."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    with _LOCK:
+        if _LIB is not None:
+            return _LIB
+        from . import build as _build
+
+        path = _build.LIB
+        if not path.exists():
+            _build.build()
+        handle = C.CDLL(str(path))
+        for name, (res, args) in _PROTOS.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = handle
+        return _LIB
+
+
+def check(status: int, func: str) -> None:
+    if status != CIRRUS_OK:
+        raise CirrusError(status, func)
+
+
+def exported_symbols() -> list[str]:
+    return sorted(_PROTOS)

@@ -1,0 +1,386 @@
+// C ABI (include/cirrus_b200.h).  Every entry point validates its arguments, maps internal
+// failures to cirrus_status and never lets an exception cross the boundary.
+#include "../../include/cirrus_b200.h"
+#include "solver_internal.hpp"
+#include "topology.hpp"
+
+#include <cstring>
+#include <exception>
+#include <new>
+
+struct cirrus_topology {
+    cirrus::Topology* t;
+};
+struct cirrus_grid {
+    cirrus::DevGrid* g;
+};
+
+namespace {
+
+cirrus_status map_rc(int rc) {
+    switch (rc) {
+    case 0: return CIRRUS_OK;
+    case 1: return CIRRUS_ERR_INVALID_ARGUMENT;
+    case 2: return CIRRUS_ERR_CUDA;
+    case 3: return CIRRUS_ERR_OUT_OF_MEMORY;
+    case 4: return CIRRUS_ERR_TOPOLOGY;
+    case 5: return CIRRUS_ERR_NOT_CONVERGED;
+    case 6: return CIRRUS_ERR_NONFINITE;
+    case 7: return CIRRUS_ERR_BUDGET;
+    default: return CIRRUS_ERR_STATE;
+    }
+}
+
+inline bool channel_ok(int c) { return c >= 0 && c < cirrus::kNumChannels; }
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+template <class F>
+cirrus_status guard(F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return CIRRUS_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        return CIRRUS_ERR_STATE;
+    }
+}
+
+cirrus_status cuda_status() {
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return CIRRUS_OK;
+    return e == cudaErrorMemoryAllocation ? CIRRUS_ERR_OUT_OF_MEMORY : CIRRUS_ERR_CUDA;
+}
+
+void to_internal(const cirrus_solve_params* p, cirrus::SolveParams* q) {
+    q->max_iters = p->max_iters;
+    q->tol = p->relative_tolerance;
+    q->level_iters = p->level_iters;
+    q->coarsest_iters = p->coarsest_iters;
+    q->sync_stride = p->sync_stride;
+    q->pure_neumann = p->is_pure_neumann ? 1 : 0;
+    q->one_over_alpha = p->one_over_alpha;
+    q->prolong_coeff = p->prolong_coeff;
+    q->precision = p->precision;
+    q->warm_start = p->warm_start;
+    q->inner_tol = p->inner_tolerance;
+    q->max_outer = p->max_outer_iters;
+}
+
+bool params_ok(const cirrus_solve_params* p) {
+    return p && p->max_iters >= 0 && p->relative_tolerance >= 0 && p->level_iters >= 0 && p->coarsest_iters >= 0 &&
+           (p->precision == CIRRUS_PRECISION_FP32 || p->precision == CIRRUS_PRECISION_MIXED_FP64) && p->max_outer_iters >= 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cirrus_status_string(cirrus_status s) {
+    switch (s) {
+    case CIRRUS_OK: return "ok";
+    case CIRRUS_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case CIRRUS_ERR_CUDA: return "CUDA error";
+    case CIRRUS_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case CIRRUS_ERR_TOPOLOGY: return "topology error";
+    case CIRRUS_ERR_NOT_CONVERGED: return "not converged";
+    case CIRRUS_ERR_NONFINITE: return "non-finite residual";
+    case CIRRUS_ERR_BUDGET: return "HBM budget exceeded";
+    case CIRRUS_ERR_NO_DEVICE: return "no CUDA device";
+    case CIRRUS_ERR_STATE: return "invalid state";
+    }
+    return "unknown status";
+}
+
+const char* cirrus_version(void) { return "cirrus-b200 0.1.0 (sm_100a)"; }
+
+// ---------------------------------------------------------------- topology
+cirrus_status cirrus_topology_create(int num_layers, const uint32_t* log2_hash, double h0, cirrus_topology** out) {
+    if (!out || !log2_hash || num_layers < 1 || num_layers > 16 || !(h0 > 0)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    for (int l = 0; l < num_layers; l++)
+        if (log2_hash[l] < 1 || log2_hash[l] > 28) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        *out = new cirrus_topology{new cirrus::Topology(num_layers, log2_hash, h0)};
+        return CIRRUS_OK;
+    });
+}
+void cirrus_topology_destroy(cirrus_topology* topo) {
+    if (!topo) return;
+    delete topo->t;
+    delete topo;
+}
+cirrus_status cirrus_topology_set_tile(cirrus_topology* topo, int level, int x, int y, int z, int type) {
+    if (!topo || level < 0 || level >= topo->t->num_layers()) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (type != CIRRUS_LEAF && type != CIRRUS_NONLEAF && type != CIRRUS_GHOST) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return topo->t->set_tile(level, x, y, z, (uint8_t)type) ? CIRRUS_OK : CIRRUS_ERR_TOPOLOGY; });
+}
+cirrus_status cirrus_topology_compress(cirrus_topology* topo) {
+    if (!topo) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { topo->t->compress_and_sync(); return CIRRUS_OK; });
+}
+cirrus_status cirrus_topology_spawn_ghost_tiles(cirrus_topology* topo) {
+    if (!topo) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        topo->t->last_error.clear();
+        topo->t->spawn_ghost_tiles();
+        return topo->t->last_error.empty() ? CIRRUS_OK : CIRRUS_ERR_TOPOLOGY;
+    });
+}
+cirrus_status cirrus_topology_refine_leafs_one_step(cirrus_topology* topo, cirrus_level_target_fn fn, void* user,
+                                                    int* refined_per_level) {
+    if (!topo || !fn) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        topo->t->last_error.clear();
+        auto c = topo->t->refine_leafs_one_step([&](int l, int x, int y, int z) { return fn(user, l, x, y, z); });
+        if (refined_per_level)
+            for (size_t i = 0; i < c.size(); i++) refined_per_level[i] = c[i];
+        return topo->t->last_error.empty() ? CIRRUS_OK : CIRRUS_ERR_TOPOLOGY;
+    });
+}
+cirrus_status cirrus_topology_iterative_refine(cirrus_topology* topo, cirrus_level_target_fn fn, void* user) {
+    if (!topo || !fn) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        topo->t->last_error.clear();
+        topo->t->iterative_refine([&](int l, int x, int y, int z) { return fn(user, l, x, y, z); });
+        return topo->t->last_error.empty() ? CIRRUS_OK : CIRRUS_ERR_TOPOLOGY;
+    });
+}
+cirrus_status cirrus_topology_iterative_refine_masks(cirrus_topology* topo, const uint8_t* const* masks, const int* dims) {
+    if (!topo || !masks || !dims) return CIRRUS_ERR_INVALID_ARGUMENT;
+    const int nl = topo->t->num_layers();
+    return guard([&] {
+        topo->t->last_error.clear();
+        topo->t->iterative_refine([&](int l, int x, int y, int z) {
+            if (l < 0 || l >= nl || !masks[l]) return l;
+            const int* d = dims + 3 * l;
+            if (x < 0 || y < 0 || z < 0 || x >= d[0] || y >= d[1] || z >= d[2]) return l;
+            return masks[l][((size_t)x * d[1] + y) * d[2] + z] ? l + 1 : l;
+        });
+        return topo->t->last_error.empty() ? CIRRUS_OK : CIRRUS_ERR_TOPOLOGY;
+    });
+}
+cirrus_status cirrus_topology_num_tiles(const cirrus_topology* topo, int* num_tiles) {
+    if (!topo || !num_tiles) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *num_tiles = topo->t->num_tiles();
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_topology_max_level(const cirrus_topology* topo, int* max_level) {
+    if (!topo || !max_level) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *max_level = topo->t->max_level();
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_topology_tiles(const cirrus_topology* topo, int32_t* out5) {
+    if (!topo || !out5) return CIRRUS_ERR_INVALID_ARGUMENT;
+    topo->t->tiles(out5);
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_topology_hash_slots(const cirrus_topology* topo, int32_t* out) {
+    if (!topo || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    topo->t->hash_slots(out);
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_topology_set_cell_types(cirrus_topology* topo, const uint8_t* ctypes) {
+    if (!topo || !ctypes) return CIRRUS_ERR_INVALID_ARGUMENT;
+    topo->t->set_cell_types(ctypes);
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_topology_cell_types(const cirrus_topology* topo, uint8_t* ctypes) {
+    if (!topo || !ctypes) return CIRRUS_ERR_INVALID_ARGUMENT;
+    topo->t->cell_types(ctypes);
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_topology_calc_cell_types_from_leafs(cirrus_topology* topo) {
+    if (!topo) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { topo->t->calc_cell_types_from_leafs(); return CIRRUS_OK; });
+}
+cirrus_status cirrus_topology_neighbor_tiles(const cirrus_topology* topo, int32_t* out6) {
+    if (!topo || !out6) return CIRRUS_ERR_INVALID_ARGUMENT;
+    topo->t->neighbor_tiles(out6);
+    return CIRRUS_OK;
+}
+
+// ---------------------------------------------------------------- device grid
+cirrus_status cirrus_grid_create(const cirrus_topology* topo, cirrus_grid** out) {
+    if (!topo || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return CIRRUS_ERR_NO_DEVICE;
+    }
+    return guard([&] {
+        cirrus::DevGrid* g = nullptr;
+        std::string err;
+        int rc = cirrus::grid_create(*topo->t, &g, &err);
+        if (rc) return map_rc(rc);
+        *out = new cirrus_grid{g};
+        return CIRRUS_OK;
+    });
+}
+void cirrus_grid_destroy(cirrus_grid* grid) {
+    if (!grid) return;
+    cirrus::grid_destroy(grid->g);
+    delete grid;
+}
+cirrus_status cirrus_grid_num_tiles(const cirrus_grid* grid, int* num_tiles) {
+    if (!grid || !num_tiles) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *num_tiles = grid->g->n;
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_grid_device_bytes(const cirrus_grid* grid, size_t* bytes) {
+    if (!grid || !bytes) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *bytes = grid->g->bytes;
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_grid_dof(const cirrus_grid* grid, int64_t* dof) {
+    if (!grid || !dof) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *dof = grid->g->dof;
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_grid_set_channel(cirrus_grid* grid, int channel, const float* host, void* stream) {
+    if (!grid || !host || !channel_ok(channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    const size_t bytes = (size_t)grid->g->n * cirrus::kTileCells * sizeof(float);
+    if (cudaMemcpyAsync(grid->g->d_ch[channel], host, bytes, cudaMemcpyHostToDevice, S(stream)) != cudaSuccess) return cuda_status();
+    return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
+}
+cirrus_status cirrus_grid_get_channel(const cirrus_grid* grid, int channel, float* host, void* stream) {
+    if (!grid || !host || !channel_ok(channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    const size_t bytes = (size_t)grid->g->n * cirrus::kTileCells * sizeof(float);
+    if (cudaMemcpyAsync(host, grid->g->d_ch[channel], bytes, cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess) return cuda_status();
+    return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
+}
+cirrus_status cirrus_grid_channel_ptr(cirrus_grid* grid, int channel, float** device_ptr) {
+    if (!grid || !device_ptr || !channel_ok(channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *device_ptr = grid->g->d_ch[channel];
+    return CIRRUS_OK;
+}
+
+// ---------------------------------------------------------------- operators
+cirrus_status cirrus_full_negative_laplacian(cirrus_grid* grid, int x_channel, int Ax_channel, void* stream) {
+    if (!grid || !channel_ok(x_channel) || !channel_ok(Ax_channel) || x_channel == Ax_channel) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    cirrus::launch::full_laplacian<float>(g, g.d_ch[x_channel], g.d_ch[Ax_channel], nullptr, S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_gauss_seidel_sweep(cirrus_grid* grid, int level, int x_channel, int rhs_channel, int color, void* stream) {
+    if (!grid || !channel_ok(x_channel) || !channel_ok(rhs_channel) || (color != 0 && color != 1)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    if (level < 0 || level >= g.num_layers) return CIRRUS_ERR_INVALID_ARGUMENT;
+    cirrus::launch::gs_sweep(g, level, g.d_ch[x_channel], g.d_ch[rhs_channel], color, nullptr, S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_residual_and_restrict(cirrus_grid* grid, int level, int x_channel, int rhs_channel, int coarse_channel,
+                                           float one_over_alpha, void* stream) {
+    if (!grid || !channel_ok(x_channel) || !channel_ok(rhs_channel) || !channel_ok(coarse_channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    if (level < 1 || level >= g.num_layers) return CIRRUS_ERR_INVALID_ARGUMENT;
+    cirrus::launch::residual_restrict(g, level, g.d_ch[x_channel], g.d_ch[rhs_channel], g.d_ch[coarse_channel], one_over_alpha, nullptr,
+                                      S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_prolongate_and_update(cirrus_grid* grid, int fine_level, int coarse_channel, int fine_channel,
+                                           float prolong_coeff, void* stream) {
+    if (!grid || !channel_ok(coarse_channel) || !channel_ok(fine_channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    if (fine_level < 1 || fine_level >= g.num_layers) return CIRRUS_ERR_INVALID_ARGUMENT;
+    cirrus::launch::prolongate(g, fine_level, g.d_ch[coarse_channel], g.d_ch[fine_channel], prolong_coeff, nullptr, S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_vcycle(cirrus_grid* grid, int x_channel, int f_channel, int rhs_channel, int level_iters, int coarsest_iters,
+                            void* stream) {
+    if (!grid || !channel_ok(x_channel) || !channel_ok(f_channel) || !channel_ok(rhs_channel) || level_iters < 0 || coarsest_iters < 0)
+        return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    cirrus::vcycle(g, g.d_ch[x_channel], g.d_ch[f_channel], g.d_ch[rhs_channel], level_iters, coarsest_iters, 1.f, 1.f, nullptr,
+                   S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_dot(cirrus_grid* grid, int a_channel, int b_channel, double* result, void* stream) {
+    if (!grid || !result || !channel_ok(a_channel) || !channel_ok(b_channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    cirrus::SolveCtl ctl{};
+    cirrus::launch::leaf_reduce(cirrus::OP_DOT, g, g.d_ch[a_channel], g.d_ch[b_channel], nullptr, nullptr, g.d_scalars, ctl,
+                                cirrus::EPI_GAMMA, 0, S(stream));
+    cudaMemcpyAsync(g.h_scalars, g.d_scalars, sizeof(cirrus::Scalars), cudaMemcpyDeviceToHost, S(stream));
+    if (cudaStreamSynchronize(S(stream)) != cudaSuccess) return cuda_status();
+    *result = g.h_scalars->gamma;
+    return cuda_status();
+}
+
+cirrus_status cirrus_clear_neumann_neighbor_faces(cirrus_grid* grid, int u_channel, void* stream) {
+    if (!grid || u_channel < 0 || u_channel + 2 >= cirrus::kNumChannels) return CIRRUS_ERR_INVALID_ARGUMENT;
+    cirrus::launch::clear_neumann_faces(*grid->g, u_channel, S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_propagate_to_children(cirrus_grid* grid, int channel, void* stream) {
+    if (!grid || !channel_ok(channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    cirrus::launch::propagate_to_children(*grid->g, channel, S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_velocity_volume_divergence_on_leafs(cirrus_grid* grid, int u_channel, int div_channel, void* stream) {
+    if (!grid || u_channel < 0 || u_channel + 2 >= cirrus::kNumChannels || !channel_ok(div_channel) ||
+        (div_channel >= u_channel && div_channel <= u_channel + 2))
+        return CIRRUS_ERR_INVALID_ARGUMENT;
+    cirrus::launch::velocity_divergence(*grid->g, u_channel, div_channel, S(stream));
+    return cuda_status();
+}
+
+// ---------------------------------------------------------------- solve
+void cirrus_solve_params_default(cirrus_solve_params* p) {
+    if (!p) return;
+    p->max_iters = 1000;
+    p->relative_tolerance = 1e-6;
+    p->level_iters = 1;
+    p->coarsest_iters = 10;
+    p->sync_stride = 1;
+    p->is_pure_neumann = 0;
+    p->one_over_alpha = 1.f;
+    p->prolong_coeff = 1.f;
+    p->precision = CIRRUS_PRECISION_FP32;
+    p->warm_start = 0;
+    p->inner_tolerance = 1e-3;
+    p->max_outer_iters = 20;
+}
+
+cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream, cirrus_solve_result* result) {
+    if (!grid || !params_ok(params) || !result) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        cirrus::SolveParams p;
+        to_internal(params, &p);
+        cirrus::SolveResult r;
+        int rc = p.precision == CIRRUS_PRECISION_MIXED_FP64 ? cirrus::mixed_solve(*grid->g, p, S(stream), &r)
+                                                            : cirrus::pcg_solve(*grid->g, p, S(stream), &r);
+        if (rc) return map_rc(rc);
+        result->iters = r.iters;
+        result->outer_iters = r.outer;
+        result->rel_residual = r.rel;
+        result->true_rel_residual = r.true_rel;
+        result->status = (int)map_rc(r.status);
+        return CIRRUS_OK;
+    });
+}
+
+cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params* params, const float* b_host, float* x_host,
+                                    void* stream, cirrus_solve_result* result) {
+    if (!grid || !params_ok(params) || !b_host || !x_host || !result) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    const size_t bytes = (size_t)g.n * cirrus::kTileCells * sizeof(float);
+    if (cudaMemcpyAsync(g.d_ch[cirrus::kChB], b_host, bytes, cudaMemcpyHostToDevice, S(stream)) != cudaSuccess) return cuda_status();
+    cirrus_status st = cirrus_gmg_solve(grid, params, stream, result);
+    if (st != CIRRUS_OK) return st;
+    if (cudaMemcpyAsync(x_host, g.d_ch[cirrus::kChX], bytes, cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess) return cuda_status();
+    return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
+}
+
+cirrus_status cirrus_true_residual(cirrus_grid* grid, const float* b_host, double* rel, void* stream) {
+    if (!grid || !b_host || !rel) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    return guard([&] {
+        const size_t bytes = (size_t)g.n * cirrus::kTileCells * sizeof(float);
+        float* d_b = g.d_ch[cirrus::kChTmp];
+        // channel 5 (tmp) carries b for the evaluation
+        if (cudaMemcpyAsync(d_b, b_host, bytes, cudaMemcpyHostToDevice, S(stream)) != cudaSuccess) return cuda_status();
+        int rc = cirrus::true_residual(g, d_b, rel, S(stream));
+        return map_rc(rc);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,46 @@
+// Shared definitions of the device solver: constants, the per-tile metadata layout and the
+// kernel-side view of a grid.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace cirrus {
+
+constexpr int kTileCells = 512;
+constexpr int kNumChannels = 9;       // x, b/r, p, Ap, z, tmp, u, v, w (PoissonTile channel ids)
+constexpr int kChX = 0, kChB = 1, kChR = 1, kChP = 2, kChAp = 3, kChZ = 4, kChTmp = 5, kChU = 6;
+
+constexpr uint8_t LEAF_T = 1, NONLEAF_T = 2, GHOST_T = 4;
+constexpr uint8_t DIRICHLET_C = 1, INTERIOR_C = 2, NEUMANN_C = 4;
+
+// Per-tile metadata, 8 int32: [0..5] same-level neighbour in the reference's stencil face order
+// (x-, x+, y-, y+, z-, z+) or -1, [6] parent tile or -1, [7] packed = level | type << 8 |
+// octant << 16 (octant = child offset inside the parent, bit0 x, bit1 y, bit2 z).
+struct __align__(16) TileMeta {
+    int nb[6];
+    int parent;
+    int packed;
+};
+__host__ __device__ inline int meta_level(int packed) { return packed & 0xff; }
+__host__ __device__ inline int meta_type(int packed) { return (packed >> 8) & 0xff; }
+__host__ __device__ inline int meta_octant(int packed) { return (packed >> 16) & 0x7; }
+
+// Per-cell stencil mask byte: bit f (f in x-, x+, y-, y+, z-, z+) set when the face carries a
+// non-zero coefficient, bit 6 set for INTERIOR cells.  Two contexts exist: the full-tree
+// Laplacian (tile types as stored) and the multigrid level context (NONLEAF counts as LEAF at
+// its own level).  Per tile, fcls holds the coefficient class of the six cross-tile faces:
+// 2 bits per face, context lap in bits 0..11, mg in bits 12..23; class 1 = 1/h^2 (same level),
+// class 2 = (2/3)/h^2 (leaf-ghost T-junction).
+constexpr int kMaskInterior = 64;
+
+// Kernel-side view of the topology tables of a device grid (all arrays in all-tiles order).
+struct Topo {
+    const uint8_t* ctype;        // n*512 cell types
+    const uint8_t* mask_lap;     // n*512 stencil masks, full-tree Laplacian context
+    const uint8_t* mask_mg;      // n*512 stencil masks, multigrid level context
+    const TileMeta* meta;        // n
+    const uint32_t* fcls;        // n cross-face coefficient classes
+    float h0;                    // voxel size of level 0, stored in FP32 as the reference does
+};
+}  // namespace cirrus

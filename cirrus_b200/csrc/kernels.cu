@@ -1,0 +1,679 @@
+// Kernels of the GMG-PCG solve and their launchers.  Reference counterparts are cited per
+// kernel (paths inside the reference project).
+#include "kernels.cuh"
+#include "solver_internal.hpp"
+
+#include <cstdio>
+
+namespace cirrus {
+
+// ------------------------------------------------------------------ ghost value propagation
+// PropagateValuesToGhostTiles (src/PoissonGrid.cu:585-605): a GHOST cell takes its parent
+// cell's value when both are INTERIOR, 0 otherwise.
+template <class T>
+__global__ void __launch_bounds__(128) k_propagate_ghosts(Topo tp, const int* __restrict__ list, int n, T* X,
+                                                          const int* __restrict__ done) {
+    if (done && *done) return;
+    const int q = blockIdx.x;
+    if (q >= n) return;
+    const int tile = list[q];
+    const int t = threadIdx.x;
+    const TileMeta m = tp.meta[tile];
+    const TileIdx ix(t);
+    const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + (size_t)tile * kTileCells + t * 4);
+    V4<T> out = zero4<T>();
+    if (m.parent >= 0) {
+        const int oct = meta_octant(m.packed);
+        const int pi = (oct & 1) * 4 + (ix.i >> 1), pj = ((oct >> 1) & 1) * 4 + (ix.j >> 1);
+        const size_t pbase = (size_t)m.parent * kTileCells + pi * 64 + pj * 8 + ((oct >> 2) & 1) * 4 + (ix.k0 >> 1);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const size_t pid = pbase + (e >> 1);
+            const bool me = (ct4 >> (8 * e)) & INTERIOR_C;
+            const bool pin = tp.ctype[pid] & INTERIOR_C;
+            out.v[e] = (me && pin) ? X[pid] : T(0);
+        }
+    }
+    st4(X + (size_t)tile * kTileCells + t * 4, out);
+}
+
+// ------------------------------------------------------------------ Laplacian apply
+// NegativeLaplacianSameLevel128Kernel (src/GMGSolver.cu:145-194) on LEAF|GHOST tiles of all
+// levels with the tile types as stored (subtree level -1).
+template <class T, int TPB>
+__global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __restrict__ list, int n, const T* __restrict__ X,
+                                                         T* __restrict__ Y, const int* __restrict__ done) {
+    __shared__ TileShared<T> sh[TPB];
+    if (done && *done) return;
+    const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
+    const int q = blockIdx.x * TPB + g;
+    const bool active = q < n;
+    const int tile = active ? list[q] : 0;
+    TileMeta m;
+    if (active) {
+        m = tp.meta[tile];
+        stage_tile<T>(X, tile, m, t, sh[g]);
+    }
+    __syncthreads();
+    if (!active) return;
+    const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_lap + (size_t)tile * kTileCells + t * 4);
+    const LevelConst<T> L((T)tp.h0, meta_level(m.packed));
+    T out[4], dg[4];
+    neg_lap4<T, false>(sh[g].xs, sh[g].hx, t, mask4, tp.fcls[tile] & 0xfffu, L, out, dg);
+    V4<T> o;
+    o.v[0] = out[0]; o.v[1] = out[1]; o.v[2] = out[2]; o.v[3] = out[3];
+    st4(Y + (size_t)tile * kTileCells + t * 4, o);
+}
+
+// AccumulateToParents128Kernel on GHOST tiles, additive, coefficient 1, all cell types
+// (src/PoissonGrid.cu:664-710).  2x2x2 sums in the reference's (ii,jj,kk) order.
+template <class T>
+__global__ void __launch_bounds__(64) k_accumulate_ghosts(Topo tp, const int* __restrict__ list, int n, T* Y,
+                                                          const int* __restrict__ done) {
+    if (done && *done) return;
+    const int q = blockIdx.x;
+    if (q >= n) return;
+    const int tile = list[q];
+    const TileMeta m = tp.meta[tile];
+    if (m.parent < 0) return;
+    const int b = threadIdx.x;
+    const int fi = b / 16 * 2, fj = (b / 4) % 4 * 2, fk = b % 4 * 2;
+    const size_t base = (size_t)tile * kTileCells;
+    T sum = T(0);
+#pragma unroll
+    for (int ii = 0; ii < 2; ii++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int kk = 0; kk < 2; kk++) {
+                const size_t id = base + (fi + ii) * 64 + (fj + jj) * 8 + (fk + kk);
+                sum += (tp.ctype[id] & (INTERIOR_C | DIRICHLET_C | NEUMANN_C)) ? Y[id] : T(0);
+            }
+    const int oct = meta_octant(m.packed);
+    const size_t pid = (size_t)m.parent * kTileCells + ((oct & 1) * 4 + fi / 2) * 64 + (((oct >> 1) & 1) * 4 + fj / 2) * 8 +
+                       ((oct >> 2) & 1) * 4 + fk / 2;
+    Y[pid] = Y[pid] + sum;
+}
+
+// ------------------------------------------------------------------ Gauss-Seidel colour sweep
+// NegativeLaplacianAndGaussSeidelSameLevel128Kernel (src/GMGSolver.cu:216-269): on LEAF|NONLEAF
+// tiles of one level (NONLEAF counted as LEAF), cells of one colour (i+j+k)%2:
+// x += (b - A x) / D on INTERIOR cells.
+template <int TPB>
+__global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
+                                                        const float* __restrict__ R, int color, const int* __restrict__ done) {
+    __shared__ TileShared<float> sh[TPB];
+    if (done && *done) return;
+    const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
+    const int q = blockIdx.x * TPB + g;
+    const bool active = q < n;
+    const int tile = active ? list[q] : 0;
+    TileMeta m;
+    V4<float> own;
+    if (active) {
+        m = tp.meta[tile];
+        own = stage_tile<float>(X, tile, m, t, sh[g]);
+    }
+    __syncthreads();
+    if (!active) return;
+    const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
+    const V4<float> b = ld4(R + (size_t)tile * kTileCells + t * 4);
+    const LevelConst<float> L(tp.h0, meta_level(m.packed));
+    float ax[4], d[4];
+    neg_lap4<float, true>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
+    const TileIdx ix(t);
+    V4<float> o = own;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        if (((ix.i + ix.j + ix.k0 + e) & 1) != color) continue;
+        const bool interior = (mask4 >> (8 * e)) & kMaskInterior;
+        const float dx = interior ? (b.v[e] - ax[e]) / d[e] : 0.f;
+        o.v[e] = own.v[e] + dx;
+    }
+    st4(X + (size_t)tile * kTileCells + t * 4, o);
+}
+
+// A whole sequence of colour sweeps over a small level inside one CTA (used for the coarsest
+// level: GaussSeidelGMG(5, 0) + GaussSeidelGMG(5, 1), src/GMGSolver.cu:432-433).  Global-memory
+// writes of one sweep are made visible to the next sweep's halo loads by __syncthreads.
+__global__ void __launch_bounds__(1024) k_gs_sequence(Topo tp, const int* __restrict__ list, int n, float* X,
+                                                      const float* __restrict__ R, uint32_t colors, int nsweeps,
+                                                      const int* __restrict__ done) {
+    __shared__ TileShared<float> sh[8];
+    if (done && *done) return;
+    const int groups = blockDim.x >> 7;
+    const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
+    for (int s = 0; s < nsweeps; s++) {
+        const int color = (colors >> s) & 1;
+        for (int base = 0; base < n; base += groups) {
+            const int q = base + g;
+            const bool active = q < n;
+            const int tile = active ? list[q] : 0;
+            TileMeta m;
+            V4<float> own;
+            if (active) {
+                m = tp.meta[tile];
+                own = stage_tile<float>(X, tile, m, t, sh[g]);
+            }
+            __syncthreads();
+            if (active) {
+                const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
+                const V4<float> b = ld4(R + (size_t)tile * kTileCells + t * 4);
+                const LevelConst<float> L(tp.h0, meta_level(m.packed));
+                float ax[4], d[4];
+                neg_lap4<float, true>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
+                const TileIdx ix(t);
+                V4<float> o = own;
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    if (((ix.i + ix.j + ix.k0 + e) & 1) != color) continue;
+                    const bool interior = (mask4 >> (8 * e)) & kMaskInterior;
+                    const float dx = interior ? (b.v[e] - ax[e]) / d[e] : 0.f;
+                    o.v[e] = own.v[e] + dx;
+                }
+                st4(X + (size_t)tile * kTileCells + t * 4, o);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ------------------------------------------------------------------ residual + restriction
+// ResidualAndRestrict128Kernel (src/GMGSolver.cu:284-339): r = rhs - A x on every cell of the
+// level's tiles; 2x2x2 sums go to the parent cell: GHOST tiles add, others overwrite
+// (times one_over_alpha).
+template <int TPB>
+__global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int first, int n, const float* __restrict__ X,
+                                                                 const float* RHS, float* C, float one_over_alpha,
+                                                                 const int* __restrict__ done) {
+    __shared__ TileShared<float> sh[TPB];
+    if (done && *done) return;
+    const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
+    const int q = blockIdx.x * TPB + g;
+    const bool active = q < n;
+    const int tile = first + (active ? q : 0);
+    TileMeta m;
+    if (active) {
+        m = tp.meta[tile];
+        stage_tile<float>(X, tile, m, t, sh[g]);
+    }
+    __syncthreads();
+    float res[4];
+    if (active) {
+        const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
+        const V4<float> b = ld4(RHS + (size_t)tile * kTileCells + t * 4);
+        const LevelConst<float> L(tp.h0, meta_level(m.packed));
+        float ax[4], d[4];
+        neg_lap4<float, false>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
+#pragma unroll
+        for (int e = 0; e < 4; e++) res[e] = b.v[e] - ax[e];
+    }
+    __syncthreads();  // sh.xs is reused for the residual
+    if (active) {
+        V4<float> r4;
+        r4.v[0] = res[0]; r4.v[1] = res[1]; r4.v[2] = res[2]; r4.v[3] = res[3];
+        st4(sh[g].xs + t * 4, r4);
+    }
+    __syncthreads();
+    if (!active || t >= 64 || m.parent < 0) return;
+    const int fi = t / 16 * 2, fj = (t / 4) % 4 * 2, fk = t % 4 * 2;
+    float sum = 0.f;
+#pragma unroll
+    for (int ii = 0; ii < 2; ii++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int kk = 0; kk < 2; kk++) sum += sh[g].xs[(fi + ii) * 64 + (fj + jj) * 8 + (fk + kk)];
+    const int oct = meta_octant(m.packed);
+    const size_t pid = (size_t)m.parent * kTileCells + ((oct & 1) * 4 + fi / 2) * 64 + (((oct >> 1) & 1) * 4 + fj / 2) * 8 +
+                       ((oct >> 2) & 1) * 4 + fk / 2;
+    if (meta_type(m.packed) & GHOST_T) C[pid] += sum;
+    else C[pid] = sum * one_over_alpha;
+}
+
+// ------------------------------------------------------------------ prolongation + update
+// ProlongateAndUpdate128Kernel (src/GMGSolver.cu:345-376): injection of the parent value;
+// GHOST: x = cx, others: x += prolong_coeff * cx; INTERIOR cells only (0 elsewhere).
+__global__ void __launch_bounds__(128) k_prolongate(Topo tp, int first, int n, const float* __restrict__ CX, float* FX,
+                                                    float prolong_coeff, const int* __restrict__ done) {
+    if (done && *done) return;
+    const int q = blockIdx.x;
+    if (q >= n) return;
+    const int tile = first + q;
+    const int t = threadIdx.x;
+    const TileMeta m = tp.meta[tile];
+    const TileIdx ix(t);
+    const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + (size_t)tile * kTileCells + t * 4);
+    float c[2] = {0.f, 0.f};
+    if (m.parent >= 0) {
+        const int oct = meta_octant(m.packed);
+        const size_t pbase = (size_t)m.parent * kTileCells + ((oct & 1) * 4 + (ix.i >> 1)) * 64 +
+                             (((oct >> 1) & 1) * 4 + (ix.j >> 1)) * 8 + ((oct >> 2) & 1) * 4 + (ix.k0 >> 1);
+        c[0] = CX[pbase];
+        c[1] = CX[pbase + 1];
+    }
+    const bool ghost = meta_type(m.packed) & GHOST_T;
+    float* p = FX + (size_t)tile * kTileCells + t * 4;
+    V4<float> fx = ld4(p);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const bool interior = (ct4 >> (8 * e)) & INTERIOR_C;
+        const float cx = c[e >> 1];
+        fx.v[e] = interior ? (ghost ? cx : fmaf(prolong_coeff, cx, fx.v[e])) : 0.f;
+    }
+    st4(p, fx);
+}
+
+// V-cycle initialisation (src/GMGSolver.cu:386-403): x = 0 everywhere; rhs = f on LEAF and
+// NONLEAF tiles, 0 on GHOST tiles.
+__global__ void __launch_bounds__(256) k_vcycle_init(Topo tp, int n, float* X, float* RHS, const float* __restrict__ F,
+                                                     const int* __restrict__ done) {
+    if (done && *done) return;
+    const size_t nv = (size_t)n * (kTileCells / 4);
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+        const int tile = (int)(v >> 7);
+        const bool ghost = meta_type(tp.meta[tile].packed) & GHOST_T;
+        st4(X + v * 4, zero4<float>());
+        st4(RHS + v * 4, ghost ? zero4<float>() : ld4(F + v * 4));
+    }
+}
+
+// ------------------------------------------------------------------ reductions over LEAF tiles
+// Deterministic two-level sum: fixed grid-stride assignment, warp-shuffle trees, partials per
+// CTA, and the last CTA to finish (ticket counter) sums the partials in a fixed order and runs
+// the epilogue on the scalar state.  Per 4-cell vector the FP32 products are formed as the
+// reference's Dot128Kernel does (src/PoissonGrid.cu:177-181) and widened to FP64.
+__device__ __forceinline__ double dot4f(const V4<float>& a, const V4<float>& b) {
+    float s = fmaf(a.v[0], b.v[0], a.v[1] * b.v[1]);
+    s = fmaf(a.v[2], b.v[2], s);
+    s = fmaf(a.v[3], b.v[3], s);
+    return (double)s;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct Double2 { double a, b; };
+
+// Block-reduce (a, b), publish the partial, return true in thread 0 of the last CTA with the
+// grand total in `tot`.
+__device__ __forceinline__ bool reduce_and_elect(double a, double b, double* partials, unsigned int* counter, Double2& tot) {
+    __shared__ double wa[32], wb[32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) { wa[w] = a; wb[w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        a = lane < nw ? wa[lane] : 0.0;
+        b = lane < nw ? wb[lane] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+        if (lane == 0) {
+            partials[2 * blockIdx.x] = a;
+            partials[2 * blockIdx.x + 1] = b;
+            __threadfence();
+            const unsigned int ticket = atomicAdd(counter, 1u);
+            last = (ticket == gridDim.x - 1);
+        }
+    }
+    __syncthreads();
+    if (!last) return false;
+    if (w == 0) {
+        __threadfence();
+        double sa = 0.0, sb = 0.0;
+        for (int i = lane; i < (int)gridDim.x; i += 32) {
+            sa += __ldcg(partials + 2 * i);
+            sb += __ldcg(partials + 2 * i + 1);
+        }
+        sa = warp_sum(sa);
+        sb = warp_sum(sb);
+        if (lane == 0) {
+            tot.a = sa;
+            tot.b = sb;
+            *counter = 0u;
+        }
+    }
+    return threadIdx.x == 0;
+}
+
+__device__ __forceinline__ void set_cond(const SolveCtl& c, unsigned int v) {
+    if (c.use_cond) cudaGraphSetConditional(c.cond, v);
+}
+
+// Scalar epilogues of the PCG (src/GMGSolver.cu:540-653), executed by one thread.
+__device__ void epilogue(int which, const Double2& tot, Scalars* S, const SolveCtl& c) {
+    switch (which) {
+    case EPI_INIT: {  // rhs_norm2, zero-RHS early exit, threshold
+        S->rhs2 = tot.a;
+        S->iter = 0;
+        S->converged = 0;
+        if (c.sync_stride > 0) {
+            if (tot.a == 0.0) {
+                S->done = 1; S->converged = 1; S->iters = 0; S->rel = 0.0;
+                set_cond(c, 0u);
+                return;
+            }
+            double thr = c.tol * c.tol * tot.a;
+            S->thr2 = thr > 2.2250738585072014e-308 ? thr : 2.2250738585072014e-308;
+        }
+        if (c.max_iters <= 0) set_cond(c, 0u);
+        break;
+    }
+    case EPI_GAMMA: S->gamma = tot.a; break;
+    case EPI_ALPHA: S->fp = tot.a; S->alpha = S->gamma / tot.a; break;
+    case EPI_CHECK: {
+        const int i = S->iter;
+        S->iter = i + 1;
+        S->res2 = tot.a;
+        if (c.sync_stride > 0 && (i + 1) % c.sync_stride == 0) {
+            if (c.history && i < c.history_cap) c.history[i] = sqrt(tot.a / S->rhs2);
+            if (tot.a < S->thr2) {
+                S->done = 1; S->converged = 1; S->iters = i + 1; S->rel = sqrt(tot.a / S->rhs2);
+                set_cond(c, 0u);
+                return;
+            }
+            if (!(tot.a == tot.a) || isinf(tot.a)) {  // non-finite residual: stop, report
+                S->done = 1; S->nonfinite = 1; S->iters = i + 1; S->rel = tot.a;
+                set_cond(c, 0u);
+                return;
+            }
+        }
+        if (i + 1 >= c.max_iters) set_cond(c, 0u);
+        break;
+    }
+    case EPI_BETA: S->gamma_old = S->gamma; S->gamma = tot.a; S->beta = tot.a / S->gamma_old; break;
+    case EPI_MEAN: S->mean = tot.a / tot.b; break;
+    case EPI_FINAL:
+        if (!S->converged && !S->nonfinite) {
+            S->iters = S->iter;
+            S->res2 = tot.a;
+            S->rel = c.sync_stride > 0 ? sqrt(tot.a / S->rhs2) : -1.0;
+        }
+        break;
+    }
+}
+
+// Reduction kernel over the 4-cell vectors of LEAF tiles.  OP selects the fused elementwise
+// work done while reducing:
+//   OP_DOT       a.b                                  (Dot)
+//   OP_INIT      x = 0; r.r                           (Fill + Dot, src/GMGSolver.cu:537-542)
+//   OP_COPY_DOT  p = z; z.r                           (Copy + DotAsync, :564-568)
+//   OP_XR        x += a p, r -= a Ap (INTERIOR); r.r  (:587-612)
+//   OP_MEAN      (sum of 4 values, 2*#INTERIOR)       (MeanAsync, src/PoissonGrid.cu:231-325)
+template <int OP>
+__global__ void __launch_bounds__(256) k_leaf_reduce(Topo tp, const int* __restrict__ leaves, int nleaf, float* A, float* B,
+                                                     float* C, float* D, Scalars* S, SolveCtl ctl, int epi,
+                                                     double* partials, unsigned int* counter, int skip_if_done) {
+    if (skip_if_done && S->done) return;
+    double acc_a = 0.0, acc_b = 0.0;
+    const size_t nv = (size_t)nleaf * 128;
+    float alpha = 0.f;
+    if (OP == OP_XR) alpha = (float)S->alpha;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+        const int tile = leaves[v >> 7];
+        const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
+        if (OP == OP_DOT) {
+            acc_a += dot4f(ld4(A + off), ld4(B + off));
+        } else if (OP == OP_INIT) {  // A = x, B = r
+            st4(A + off, zero4<float>());
+            const V4<float> r = ld4(B + off);
+            acc_a += dot4f(r, r);
+        } else if (OP == OP_COPY_DOT) {  // A = z, B = r, C = p
+            const V4<float> z = ld4(A + off);
+            st4(C + off, z);
+            acc_a += dot4f(z, ld4(B + off));
+        } else if (OP == OP_XR) {  // A = x, B = p, C = r, D = Ap
+            const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+            V4<float> x = ld4(A + off), r = ld4(C + off);
+            const V4<float> p = ld4(B + off), ap = ld4(D + off);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                if ((ct4 >> (8 * e)) & INTERIOR_C) {
+                    x.v[e] = fmaf(alpha, p.v[e], x.v[e]);
+                    r.v[e] = fmaf(-alpha, ap.v[e], r.v[e]);
+                }
+            }
+            st4(A + off, x);
+            st4(C + off, r);
+            acc_a += dot4f(r, r);
+        } else if (OP == OP_MEAN) {  // A = channel
+            const V4<float> a = ld4(A + off);
+            acc_a += (double)(a.v[0] + a.v[1] + a.v[2] + a.v[3]);
+            const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+            acc_b += (double)((ct4 & INTERIOR_C) + ((ct4 >> 8) & INTERIOR_C) + ((ct4 >> 16) & INTERIOR_C) + ((ct4 >> 24) & INTERIOR_C));
+        }
+    }
+    Double2 tot{0.0, 0.0};
+    if (reduce_and_elect(acc_a, acc_b, partials, counter, tot)) epilogue(epi, tot, S, ctl);
+}
+
+// p = z + beta p on INTERIOR cells of LEAF tiles (src/GMGSolver.cu:642-653).
+__global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict__ leaves, int nleaf, float* P,
+                                                  const float* __restrict__ Z, const Scalars* S) {
+    if (S->done) return;
+    const float beta = (float)S->beta;
+    const size_t nv = (size_t)nleaf * 128;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+        const int tile = leaves[v >> 7];
+        const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
+        const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+        V4<float> p = ld4(P + off);
+        const V4<float> z = ld4(Z + off);
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            if ((ct4 >> (8 * e)) & INTERIOR_C) p.v[e] = fmaf(beta, p.v[e], z.v[e]);
+        st4(P + off, p);
+    }
+}
+
+// r -= mean on INTERIOR cells of LEAF tiles (ReCenterLeafVoxels, src/PoissonSolver.cu:356-368).
+__global__ void __launch_bounds__(256) k_recenter(Topo tp, const int* __restrict__ leaves, int nleaf, float* R,
+                                                  const Scalars* S, int skip_if_done) {
+    if (skip_if_done && S->done) return;
+    const double mean = S->mean;
+    const size_t nv = (size_t)nleaf * 128;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+        const int tile = leaves[v >> 7];
+        const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
+        const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+        V4<float> r = ld4(R + off);
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            if ((ct4 >> (8 * e)) & INTERIOR_C) r.v[e] = (float)((double)r.v[e] - mean);
+        st4(R + off, r);
+    }
+}
+
+// ------------------------------------------------------------------ FP64 defect correction
+// b - A x in FP64 for INTERIOR cells of LEAF tiles (0 elsewhere), with x held in FP64.  The
+// FP64 operator is the same FullNegativeLaplacian with FP64 coefficients.
+__global__ void __launch_bounds__(256) k_residual64(Topo tp, const int* __restrict__ leaves, int nleaf, const float* __restrict__ B,
+                                                    const double* __restrict__ AX, double* R64, float* R32) {
+    const size_t nv = (size_t)nleaf * 128;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+        const int tile = leaves[v >> 7];
+        const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
+        const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+        const V4<float> b = ld4(B + off);
+        const V4<double> ax = ld4(AX + off);
+        V4<double> r;
+        V4<float> r32;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            r.v[e] = ((ct4 >> (8 * e)) & INTERIOR_C) ? (double)b.v[e] - ax.v[e] : 0.0;
+            r32.v[e] = (float)r.v[e];
+        }
+        st4(R64 + off, r);
+        st4(R32 + off, r32);
+    }
+}
+
+// x64 += e (FP32 correction) on INTERIOR cells of LEAF tiles.
+__global__ void __launch_bounds__(256) k_accumulate_correction(Topo tp, const int* __restrict__ leaves, int nleaf, double* X64,
+                                                               float* E) {
+    const size_t nv = (size_t)nleaf * 128;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+        const int tile = leaves[v >> 7];
+        const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
+        const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+        V4<double> x = ld4(X64 + off);
+        const V4<float> e = ld4(E + off);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if ((ct4 >> (8 * q)) & INTERIOR_C) x.v[q] += (double)e.v[q];
+        st4(X64 + off, x);
+    }
+}
+
+// FP64 sum of squares of an FP64 leaf channel (norms of the defect-correction loop).
+__global__ void __launch_bounds__(256) k_norm64(const int* __restrict__ leaves, int nleaf, const double* __restrict__ A,
+                                                const float* __restrict__ B32, double* partials, unsigned int* counter,
+                                                double* out) {
+    double acc = 0.0;
+    const size_t nv = (size_t)nleaf * 128;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+        const int tile = leaves[v >> 7];
+        const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
+        if (A) {
+            const V4<double> a = ld4(A + off);
+            acc += a.v[0] * a.v[0] + a.v[1] * a.v[1] + a.v[2] * a.v[2] + a.v[3] * a.v[3];
+        } else {
+            const V4<float> a = ld4(B32 + off);
+            acc += (double)a.v[0] * a.v[0] + (double)a.v[1] * a.v[1] + (double)a.v[2] * a.v[2] + (double)a.v[3] * a.v[3];
+        }
+    }
+    Double2 tot{0.0, 0.0};
+    if (reduce_and_elect(acc, 0.0, partials, counter, tot)) *out = tot.a;
+}
+
+// float -> double and double -> float channel copies over all tiles
+__global__ void k_widen(const float* __restrict__ a, double* b, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = (double)a[i];
+}
+__global__ void k_narrow(const double* __restrict__ a, float* b, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+
+// ================================================================== launchers
+namespace launch {
+
+constexpr int kTPB = 2;  // tiles per CTA of the stencil kernels
+
+template <class T>
+void propagate_ghosts(const DevGrid& g, T* X, const int* done, cudaStream_t s) {
+    if (g.n_ghost == 0) return;
+    k_propagate_ghosts<T><<<g.n_ghost, 128, 0, s>>>(g.topo, g.d_ghost, g.n_ghost, X, done);
+}
+template <class T>
+void laplacian_tiles(const DevGrid& g, const T* X, T* Y, const int* done, cudaStream_t s) {
+    if (g.n_leafghost == 0) return;
+    k_laplacian<T, kTPB><<<(g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.d_leafghost, g.n_leafghost, X, Y, done);
+}
+template <class T>
+void accumulate_ghosts(const DevGrid& g, T* Y, const int* done, cudaStream_t s) {
+    if (g.n_ghost == 0) return;
+    k_accumulate_ghosts<T><<<g.n_ghost, 64, 0, s>>>(g.topo, g.d_ghost, g.n_ghost, Y, done);
+}
+template <class T>
+void full_laplacian(const DevGrid& g, T* X, T* Y, const int* done, cudaStream_t s) {
+    propagate_ghosts<T>(g, X, done, s);
+    laplacian_tiles<T>(g, X, Y, done, s);
+    accumulate_ghosts<T>(g, Y, done, s);
+}
+template void full_laplacian<float>(const DevGrid&, float*, float*, const int*, cudaStream_t);
+template void full_laplacian<double>(const DevGrid&, double*, double*, const int*, cudaStream_t);
+
+void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const int* done, cudaStream_t s) {
+    const int n = g.mg_count[level];
+    if (n == 0) return;
+    k_gs_sweep<kTPB><<<(n + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.d_mg + g.mg_offset[level], n, X, R, color, done);
+}
+
+void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t colors, int nsweeps, const int* done,
+                 cudaStream_t s) {
+    const int n = g.mg_count[level];
+    if (n == 0 || nsweeps == 0) return;
+    if (n <= 8) {
+        k_gs_sequence<<<1, 128 * n, 0, s>>>(g.topo, g.d_mg + g.mg_offset[level], n, X, R, colors, nsweeps, done);
+        return;
+    }
+    for (int k = 0; k < nsweeps; k++) gs_sweep(g, level, X, R, (colors >> k) & 1, done, s);
+}
+
+void residual_restrict(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha,
+                       const int* done, cudaStream_t s) {
+    const int n = g.level_count[level];
+    if (n == 0) return;
+    k_residual_restrict<kTPB><<<(n + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.level_first[level], n, X, RHS, C,
+                                                                            one_over_alpha, done);
+}
+
+void prolongate(const DevGrid& g, int level, const float* CX, float* FX, float prolong_coeff, const int* done,
+                cudaStream_t s) {
+    const int n = g.level_count[level];
+    if (n == 0) return;
+    k_prolongate<<<n, 128, 0, s>>>(g.topo, g.level_first[level], n, CX, FX, prolong_coeff, done);
+}
+
+void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const int* done, cudaStream_t s) {
+    const size_t nv = (size_t)g.n * 128;
+    int blocks = (int)std::min<size_t>((nv + 255) / 256, (size_t)g.sm_count * 8);
+    if (blocks < 1) blocks = 1;
+    k_vcycle_init<<<blocks, 256, 0, s>>>(g.topo, g.n, X, RHS, F, done);
+}
+
+int leaf_blocks(const DevGrid& g) { return g.red_blocks; }
+
+void leaf_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* D, Scalars* S, const SolveCtl& ctl,
+                 int epi, int skip_if_done, cudaStream_t s) {
+    const int blocks = leaf_blocks(g);
+    switch (op) {
+    case OP_DOT:
+        k_leaf_reduce<OP_DOT><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
+        break;
+    case OP_INIT:
+        k_leaf_reduce<OP_INIT><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
+        break;
+    case OP_COPY_DOT:
+        k_leaf_reduce<OP_COPY_DOT><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
+        break;
+    case OP_XR:
+        k_leaf_reduce<OP_XR><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
+        break;
+    case OP_MEAN:
+        k_leaf_reduce<OP_MEAN><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
+        break;
+    }
+}
+
+void update_p(const DevGrid& g, float* P, const float* Z, const Scalars* S, cudaStream_t s) {
+    k_update_p<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, P, Z, S);
+}
+
+void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cudaStream_t s) {
+    k_recenter<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, R, S, skip_if_done);
+}
+
+void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s) {
+    k_residual64<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, B, AX, R64, R32);
+}
+void accumulate_correction(const DevGrid& g, double* X64, float* E, cudaStream_t s) {
+    k_accumulate_correction<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, X64, E);
+}
+void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s) {
+    k_norm64<<<leaf_blocks(g), 256, 0, s>>>(g.d_leaf, g.n_leaf, A, B32, g.d_partials, g.d_counter, out);
+}
+void widen(const float* a, double* b, size_t n, cudaStream_t s) {
+    k_widen<<<(int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(a, b, n);
+}
+void narrow(const double* a, float* b, size_t n, cudaStream_t s) {
+    k_narrow<<<(int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(a, b, n);
+}
+
+}  // namespace launch
+}  // namespace cirrus

@@ -1,0 +1,196 @@
+/*
+ * cirrus_b200.h -- C ABI of the B200-native GMG-PCG Poisson solver for adaptive octree-tile
+ * grids (8^3-cell tiles).  Drop-in for the pressure-projection solve of wang-mengdi/Cirrus.
+ *
+ * Conventions
+ *   - Every function returns cirrus_status and never throws across the ABI.
+ *   - Plain pointers and sizes only; `stream` is a cudaStream_t passed as void* (NULL = the
+ *     legacy default stream).
+ *   - Host arrays are owned by the caller; device state is owned by the library until the
+ *     matching *_destroy call.
+ *   - Tiles are addressed in "all-tiles order": level-major, and inside a level in the order of
+ *     the level's open-addressing hash table, exactly as the reference's dAllTiles
+ *     (src/HAGrid.h:538-556).  Cell c of a tile is local (i,j,k) with c = i*64 + j*8 + k
+ *     (src/HAAccessor.h:32-34).
+ *   - Channel ids follow PoissonTile (src/PoissonTile.h:12-24): 0 x, 1 b (= r), 2 p, 3 Ap,
+ *     4 z, 5 tmp, 6 u, 7 v, 8 w.
+ *   - Calls on distinct grids are thread-safe; calls on one grid must be serialised.
+ */
+#ifndef CIRRUS_B200_H
+#define CIRRUS_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cirrus_status {
+    CIRRUS_OK = 0,
+    CIRRUS_ERR_INVALID_ARGUMENT = 1,
+    CIRRUS_ERR_CUDA = 2,
+    CIRRUS_ERR_OUT_OF_MEMORY = 3,
+    CIRRUS_ERR_TOPOLOGY = 4,        /* hash table full, bad level, inconsistent tree      */
+    CIRRUS_ERR_NOT_CONVERGED = 5,   /* iteration cap reached before the tolerance          */
+    CIRRUS_ERR_NONFINITE = 6,       /* NaN/Inf residual or CG scalar                       */
+    CIRRUS_ERR_BUDGET = 7,          /* admission refused: HBM budget exceeded              */
+    CIRRUS_ERR_NO_DEVICE = 8,
+    CIRRUS_ERR_STATE = 9            /* call out of order (e.g. grid not finalised)         */
+} cirrus_status;
+
+/* Tile types (src/HATileInfo.h:19) and cell types (src/PoissonTile.h:6). */
+enum { CIRRUS_LEAF = 1, CIRRUS_NONLEAF = 2, CIRRUS_GHOST = 4 };
+enum { CIRRUS_DIRICHLET = 1, CIRRUS_INTERIOR = 2, CIRRUS_NEUMANN = 4 };
+
+/* Returns a static, NUL-terminated description of a status code. */
+const char* cirrus_status_string(cirrus_status s);
+/* Library version string. */
+const char* cirrus_version(void);
+
+/* ------------------------------------------------------------------------------------------
+ * Host topology: the octree of tiles, built exactly as the reference builds it.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct cirrus_topology cirrus_topology;
+
+/* level_target callback: returns the target level of a LEAF tile (src/PoissonGrid.h:63). */
+typedef int (*cirrus_level_target_fn)(void* user, int level, int x, int y, int z);
+
+/* Replaces HADeviceGrid(h0, levels_log2_hash) (src/HAGrid.h:265-293). */
+cirrus_status cirrus_topology_create(int num_layers, const uint32_t* log2_hash, double h0, cirrus_topology** out);
+void cirrus_topology_destroy(cirrus_topology* topo);
+/* Replaces HADeviceGrid::setTileHost(level, b_ijk, Tile(), type) (src/HAGrid.h:387-407). */
+cirrus_status cirrus_topology_set_tile(cirrus_topology* topo, int level, int x, int y, int z, int type);
+/* Replaces compressHost() + syncHostAndDevice() (src/HAGrid.h:491-561). */
+cirrus_status cirrus_topology_compress(cirrus_topology* topo);
+/* Replaces SpawnGhostTiles(grid) (src/PoissonGrid.cu:30-60). */
+cirrus_status cirrus_topology_spawn_ghost_tiles(cirrus_topology* topo);
+/* Replaces RefineLeafsOneStep(grid, level_target) (src/PoissonGrid.h:35-162).
+ * refined_per_level (optional, num_layers ints) receives the refined-tile counts. */
+cirrus_status cirrus_topology_refine_leafs_one_step(cirrus_topology* topo, cirrus_level_target_fn fn, void* user,
+                                                    int* refined_per_level);
+/* Replaces IterativeRefine(grid, level_target) (src/PoissonGrid.h:316-326). */
+cirrus_status cirrus_topology_iterative_refine(cirrus_topology* topo, cirrus_level_target_fn fn, void* user);
+/* IterativeRefine with level_target(tile) = level + (mask[level][(x*dy+y)*dz+z] != 0); masks[l]
+ * may be NULL (never refine level l); dims holds 3 ints per layer. */
+cirrus_status cirrus_topology_iterative_refine_masks(cirrus_topology* topo, const uint8_t* const* masks, const int* dims);
+cirrus_status cirrus_topology_num_tiles(const cirrus_topology* topo, int* num_tiles);
+cirrus_status cirrus_topology_max_level(const cirrus_topology* topo, int* max_level);
+/* Tiles in all-tiles order, 5 int32 each: level, x, y, z, type (src/HAGrid.h:538-556). */
+cirrus_status cirrus_topology_tiles(const cirrus_topology* topo, int32_t* out5);
+/* Hash slot of each tile inside its level's table (src/HAAccessor.h:225-242). */
+cirrus_status cirrus_topology_hash_slots(const cirrus_topology* topo, int32_t* out);
+/* Cell types, num_tiles*512 bytes in all-tiles order.  set: only LEAF tiles' entries are used. */
+cirrus_status cirrus_topology_set_cell_types(cirrus_topology* topo, const uint8_t* ctypes);
+cirrus_status cirrus_topology_cell_types(const cirrus_topology* topo, uint8_t* ctypes);
+/* Replaces CalcCellTypesFromLeafs(grid) (src/PoissonSolver.cu:7-61). */
+cirrus_status cirrus_topology_calc_cell_types_from_leafs(cirrus_topology* topo);
+/* Replaces CalculateNeighborTiles(grid) (src/PoissonGrid.cu:121-134): 6 int32 per tile
+ * (x-, y-, z-, x+, y+, z+), the neighbour's all-tiles index or -1. */
+cirrus_status cirrus_topology_neighbor_tiles(const cirrus_topology* topo, int32_t* out6);
+
+/* ------------------------------------------------------------------------------------------
+ * Device grid: the tile pool resident in HBM (SoA channels, int32 topology tables).
+ * ---------------------------------------------------------------------------------------- */
+typedef struct cirrus_grid cirrus_grid;
+
+/* Uploads a finalised topology (cell types set) to the current CUDA device. */
+cirrus_status cirrus_grid_create(const cirrus_topology* topo, cirrus_grid** out);
+void cirrus_grid_destroy(cirrus_grid* grid);
+cirrus_status cirrus_grid_num_tiles(const cirrus_grid* grid, int* num_tiles);
+/* Device bytes held by the grid. */
+cirrus_status cirrus_grid_device_bytes(const cirrus_grid* grid, size_t* bytes);
+/* Number of DoF: INTERIOR cells of LEAF tiles. */
+cirrus_status cirrus_grid_dof(const cirrus_grid* grid, int64_t* dof);
+/* Channel transfer, num_tiles*512 floats in all-tiles order (host pointers; ordered on stream). */
+cirrus_status cirrus_grid_set_channel(cirrus_grid* grid, int channel, const float* host, void* stream);
+cirrus_status cirrus_grid_get_channel(const cirrus_grid* grid, int channel, float* host, void* stream);
+/* Device pointer of a channel (num_tiles*512 floats), for zero-copy integration. */
+cirrus_status cirrus_grid_channel_ptr(cirrus_grid* grid, int channel, float** device_ptr);
+
+/* ------------------------------------------------------------------------------------------
+ * Operators (the reference's public solver functions)
+ * ---------------------------------------------------------------------------------------- */
+/* FullNegativeLaplacian(grid, x_channel, Ax_channel) (src/GMGSolver.cu:203-213). */
+cirrus_status cirrus_full_negative_laplacian(cirrus_grid* grid, int x_channel, int Ax_channel, void* stream);
+/* One red-black colour sweep on LEAF|NONLEAF tiles of `level`
+ * (NegativeLaplacianAndGaussSeidelSameLevel128, src/GMGSolver.cu:216-274). */
+cirrus_status cirrus_gauss_seidel_sweep(cirrus_grid* grid, int level, int x_channel, int rhs_channel, int color, void* stream);
+/* ResidualAndRestrict (src/GMGSolver.cu:284-343) from `level` into level-1. */
+cirrus_status cirrus_residual_and_restrict(cirrus_grid* grid, int level, int x_channel, int rhs_channel,
+                                           int coarse_channel, float one_over_alpha, void* stream);
+/* ProlongateAndUpdate128 (src/GMGSolver.cu:345-380) into `fine_level`. */
+cirrus_status cirrus_prolongate_and_update(cirrus_grid* grid, int fine_level, int coarse_channel, int fine_channel,
+                                           float prolong_coeff, void* stream);
+/* GMGSolver::VCycle (src/GMGSolver.cu:383-447). */
+cirrus_status cirrus_vcycle(cirrus_grid* grid, int x_channel, int f_channel, int rhs_channel, int level_iters,
+                            int coarsest_iters, void* stream);
+/* Dot over LEAF tiles (src/PoissonGrid.cu:199-228); synchronises `stream`. */
+cirrus_status cirrus_dot(cirrus_grid* grid, int a_channel, int b_channel, double* result, void* stream);
+
+/* Right-hand side of the projection (the callers either side of the solve in FluidEuler::project).
+ * Velocities are the three lower-face components in channels u, u+1, u+2. */
+/* ClearAllNeumannNeighborFaces (src/FluidEuler.cu:43-60) on LEAF tiles. */
+cirrus_status cirrus_clear_neumann_neighbor_faces(cirrus_grid* grid, int u_channel, void* stream);
+/* PropagateToChildren(c, c, -1, GHOST, LAUNCH_SUBTREE, I|D|N) (src/PoissonGrid.cu:635-661). */
+cirrus_status cirrus_propagate_to_children(cirrus_grid* grid, int channel, void* stream);
+/* VelocityVolumeDivergenceOnLeafs (src/PoissonSolver.cu:66-142), including the accumulation of
+ * GHOST fluxes into their LEAF parents. */
+cirrus_status cirrus_velocity_volume_divergence_on_leafs(cirrus_grid* grid, int u_channel, int div_channel, void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * GMG-PCG solve (GMGSolver::solve, src/GMGSolver.cu:531-666)
+ * ---------------------------------------------------------------------------------------- */
+enum {
+    CIRRUS_PRECISION_FP32 = 0,          /* the reference's arithmetic: FP32 vectors, FP64 scalars */
+    CIRRUS_PRECISION_MIXED_FP64 = 1     /* FP32 V-cycle/matvec + FP64 defect correction           */
+};
+
+typedef struct cirrus_solve_params {
+    int max_iters;              /* 1000 at the reference call site (src/FluidEuler.h:598) */
+    double relative_tolerance;  /* 1e-6 */
+    int level_iters;            /* 1 */
+    int coarsest_iters;         /* 10 */
+    int sync_stride;            /* 1 */
+    int is_pure_neumann;        /* 0 / 1 */
+    float one_over_alpha;       /* 1 (GMGSolver constructor) */
+    float prolong_coeff;        /* 1 */
+    int precision;              /* CIRRUS_PRECISION_* */
+    int warm_start;             /* mixed mode: start from the x channel instead of 0 */
+    double inner_tolerance;     /* mixed mode: relative tolerance of each FP32 inner solve */
+    int max_outer_iters;        /* mixed mode: cap on defect-correction steps */
+} cirrus_solve_params;
+
+typedef struct cirrus_solve_result {
+    int iters;                  /* PCG iterations (summed over inner solves in mixed mode) */
+    int outer_iters;            /* defect-correction steps (0 in FP32 mode) */
+    double rel_residual;        /* ||r||/||b|| of the recursively updated residual (FP32 mode),
+                                   or of the FP64 true residual (mixed mode) */
+    double true_rel_residual;   /* ||b - A x||/||b|| evaluated in FP64 (or -1 if not computed) */
+    int status;                 /* cirrus_status of the solve */
+} cirrus_solve_result;
+
+/* Fills params with the reference call site's values (src/FluidEuler.h:591-598). */
+void cirrus_solve_params_default(cirrus_solve_params* params);
+
+/* Solves -lap(x) = b on the device-resident grid: b in channel 1 of LEAF tiles, x written to
+ * channel 0.  As in the reference, channel 1 is overwritten with the final residual and
+ * channels 2-4 are scratch.  The solve runs as one CUDA graph launch on `stream`; the call
+ * returns after the result scalars are on the host. */
+cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream,
+                               cirrus_solve_result* result);
+
+/* End-to-end variant for callers holding host arrays: copies b (num_tiles*512 floats, pinned or
+ * pageable) to the device, solves, and copies x back into x_host. */
+cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params* params, const float* b_host,
+                                    float* x_host, void* stream, cirrus_solve_result* result);
+
+/* FP64 true residual ||b - A x||/||b|| over INTERIOR cells of LEAF tiles, for a given b
+ * (host, num_tiles*512 floats) and the x held in channel 0. */
+cirrus_status cirrus_true_residual(cirrus_grid* grid, const float* b_host, double* rel, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CIRRUS_B200_H */

@@ -1,0 +1,946 @@
+// CPU oracle for the Cirrus GMG-PCG Poisson path.  TEST INFRASTRUCTURE ONLY.
+//
+// This file restates, on the CPU, the reference algorithm of wang-mengdi/Cirrus for the
+// pressure Poisson solve over the adaptive octree of 8^3-cell tiles.  It is the checker
+// against which the CUDA product path is compared; it is never linked into the product.
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.
+//
+// Two arithmetic modes share one template:
+//   * T = float  : mirrors the reference's FP32 arithmetic operation by operation
+//                  (fused multiply-adds where the reference's nvcc build contracts
+//                  a*b+c; FP64 CG scalars, FP32 vectors) -> parity checks;
+//   * T = double : the same algorithm in FP64 throughout -> the "FP64 oracle" that every
+//                  result's error is stated against.
+//
+// Parity pin: the topology, the FP32 kernels and the solve of this file are compared
+// against fixtures produced by the reference's own CUDA build (oracle/ref_harness.cu) run
+// on a B200; the fixtures and the script that made them live in tests/golden/.
+//
+// Reference citations (paths inside the reference project):
+//   hash + probing            src/HAAccessor.h:214-242
+//   setTileHost / compress    src/HAGrid.h:387-407, 491-561
+//   SpawnGhostTiles           src/PoissonGrid.cu:30-60
+//   RefineLeafsOneStep        src/PoissonGrid.h:35-162, IterativeRefine :316-326
+//   CalculateNeighborTiles    src/PoissonGrid.cu:121-134
+//   CalcCellTypesFromLeafs    src/PoissonSolver.cu:7-61
+//   NegativeLaplacianCoeff    src/GMGSolver.cu:12-40
+//   negativeLap / halo load   src/GMGSolver.cu:42-143
+//   FullNegativeLaplacian     src/GMGSolver.cu:203-213 (+ PoissonGrid.cu:585-605, 664-719)
+//   Gauss-Seidel sweep        src/GMGSolver.cu:216-282
+//   ResidualAndRestrict       src/GMGSolver.cu:284-343
+//   ProlongateAndUpdate       src/GMGSolver.cu:345-380
+//   VCycle                    src/GMGSolver.cu:383-447
+//   PCG solve                 src/GMGSolver.cu:531-666
+//   Dot / Mean / ReCenter     src/PoissonGrid.cu:165-325, src/PoissonSolver.cu:356-368
+//   Divergence (RHS)          src/PoissonSolver.cu:66-142, PoissonGrid.cu:635-661, 721-755
+//   face clearing             src/FluidEuler.cu:43-60, src/PoissonGrid.h:451-489
+
+#include <cstdint>
+#include <cstring>
+#include <cmath>
+#include <cfloat>
+#include <vector>
+#include <unordered_map>
+#include <algorithm>
+#include <chrono>
+#include <omp.h>
+
+namespace {
+
+enum : uint8_t { DIRICHLET = 1, INTERIOR = 2, NEUMANN = 4 };
+enum : uint8_t { LEAF = 1, NONLEAF = 2, GHOST = 4 };
+enum : int { REFINE_FLAG = 1 };
+
+constexpr int NCELL = 512;
+
+inline int loff(int i, int j, int k) { return (i << 6) + (j << 3) + k; }
+
+inline uint32_t hash3(int x, int y, int z, uint32_t log2) {
+    // src/HAAccessor.h:214-223
+    uint32_t r = 0;
+    r ^= (uint32_t)x * 1u;
+    r ^= (uint32_t)y * 2654435761u;
+    r ^= (uint32_t)z * 805459861u;
+    return r & ((1u << log2) - 1u);
+}
+
+// HATileInfo: a copy of (coord, tile memory id, level, type) kept in hash slots and arrays.
+struct Info {
+    int mem = -1;  // index into Grid::mem (tile memory); -1 = empty
+    int c[3] = {0, 0, 0};
+    int level = 0;
+    uint8_t type = 0;
+    bool empty() const { return mem < 0; }
+    uint8_t subtree_type(int sl) const { return (level == sl && type == NONLEAF) ? LEAF : type; }
+};
+
+// Tile memory: the fields the topology build and cell types need.
+struct TileMem {
+    int status = 0;
+    uint8_t ctype[NCELL];
+    TileMem() { std::memset(ctype, 0, sizeof(ctype)); }
+};
+
+struct Grid {
+    int num_layers = 0;
+    int max_level = -1;
+    std::vector<uint32_t> log2hash;
+    std::vector<TileMem> mem;
+    std::vector<std::vector<Info>> host_hash;  // hHashTables
+    std::vector<std::vector<Info>> dev_hash;   // dHashTables (copy at the last sync)
+    std::vector<std::vector<Info>> arrays;     // hTileArrays (compacted, hash-slot order)
+    std::vector<Info> all;                     // dAllTiles
+
+    static int probe(const std::vector<Info>& tab, uint32_t log2, int x, int y, int z) {
+        uint32_t mask = (1u << log2) - 1u;
+        uint32_t k0 = hash3(x, y, z, log2), k1 = k0;
+        do {
+            const Info& o = tab[k1];
+            if (o.empty() || (o.c[0] == x && o.c[1] == y && o.c[2] == z)) return (int)k1;
+            k1 = (k1 + 1) & mask;
+        } while (k1 != k0);
+        return -1;
+    }
+    Info host_info(int level, int x, int y, int z) const {
+        if (level < 0 || level >= num_layers) return Info();
+        int s = probe(host_hash[level], log2hash[level], x, y, z);
+        return s < 0 ? Info() : host_hash[level][s];
+    }
+    Info dev_info(int level, int x, int y, int z) const {
+        if (level < 0 || level >= num_layers) return Info();
+        int s = probe(dev_hash[level], log2hash[level], x, y, z);
+        return s < 0 ? Info() : dev_hash[level][s];
+    }
+    // src/HAGrid.h:387-407
+    bool set_tile_host(int level, int x, int y, int z, const TileMem& data, uint8_t type) {
+        auto& tab = host_hash[level];
+        int s = probe(tab, log2hash[level], x, y, z);
+        if (s < 0) return false;
+        Info& info = tab[s];
+        if (info.empty()) {
+            mem.push_back(TileMem());
+            info.mem = (int)mem.size() - 1;
+        }
+        mem[info.mem] = data;
+        info.c[0] = x; info.c[1] = y; info.c[2] = z; info.level = level; info.type = type;
+        return true;
+    }
+    void compress() {  // src/HAGrid.h:491-509
+        max_level = -1;
+        arrays.assign(num_layers, {});
+        for (int l = 0; l < num_layers; l++) {
+            for (const Info& o : host_hash[l]) if (!o.empty()) arrays[l].push_back(o);
+            if (!arrays[l].empty()) max_level = l;
+        }
+    }
+    void sync() {  // src/HAGrid.h:510-561
+        dev_hash = host_hash;
+        all.clear();
+        for (int l = 0; l < num_layers; l++) for (const Info& o : arrays[l]) all.push_back(o);
+    }
+};
+
+const int kNbOff[6][3] = {{-1,0,0},{1,0,0},{0,-1,0},{0,1,0},{0,0,-1},{0,0,1}};  // HAAccessor.h:161-168
+
+void spawn_ghosts(Grid& g) {  // src/PoissonGrid.cu:30-60
+    for (int level = g.max_level; level > 0; level--) {
+        const std::vector<Info> arr = g.arrays[level];
+        for (const Info& info : arr) {
+            if (!(info.type & (LEAF | NONLEAF))) continue;
+            for (int n = 0; n < 6; n++) {
+                int nx = info.c[0] + kNbOff[n][0], ny = info.c[1] + kNbOff[n][1], nz = info.c[2] + kNbOff[n][2];
+                if (!g.host_info(level, nx, ny, nz).empty()) continue;
+                Info p = g.host_info(level - 1, nx >> 1, ny >> 1, nz >> 1);
+                if (p.type & LEAF) g.set_tile_host(level, nx, ny, nz, TileMem(), GHOST);
+            }
+        }
+    }
+    g.compress();
+    g.sync();
+}
+
+// Dense per-level refinement masks: refine(l, x, y, z) == (level_target(tile) > l).
+struct Masks {
+    const uint8_t* const* m;
+    const int* dims;  // 3 ints per level
+    bool refine(int level, int x, int y, int z) const {
+        if (!m || !m[level]) return false;
+        const int* d = dims + 3 * level;
+        if (x < 0 || y < 0 || z < 0 || x >= d[0] || y >= d[1] || z >= d[2]) return false;
+        return m[level][((size_t)x * d[1] + y) * d[2] + z] != 0;
+    }
+};
+
+// childTile (src/PoissonTile.h:170-191): child cell types copy the parent's, status is copied.
+TileMem child_tile(const TileMem& parent, int ox, int oy, int oz) {
+    TileMem ch;
+    ch.status = parent.status;
+    for (int i = 0; i < 8; i++) for (int j = 0; j < 8; j++) for (int k = 0; k < 8; k++) {
+        int pi = (ox * 8 + i) >> 1, pj = (oy * 8 + j) >> 1, pk = (oz * 8 + k) >> 1;
+        ch.ctype[loff(i, j, k)] = parent.ctype[loff(pi, pj, pk)];
+    }
+    return ch;
+}
+
+// src/PoissonGrid.h:35-162.  Device reads see the hash tables of the last sync; host edits go
+// to the host tables; tile memory (status) is shared, as in the reference.
+std::vector<int> refine_step(Grid& g, const Masks& mk) {
+    std::vector<int> cnt(g.num_layers, 0);
+    const int dev_max = g.max_level;
+    for (int i = g.max_level; i >= 0; i--) {
+        const std::vector<Info> arr = g.arrays[i];  // dTileArrays[i] == hTileArrays[i] after sync
+        std::vector<int> flag(arr.size(), 0);
+        for (size_t j = 0; j < arr.size(); j++) {  // kernel on LEAF tiles of level i
+            const Info& info = arr[j];
+            if (!(info.type & LEAF)) continue;
+            bool to_refine = mk.refine(i, info.c[0], info.c[1], info.c[2]);
+            if (i < dev_max) {
+                for (int ci = 0; ci < 8; ci++) {
+                    int cx = info.c[0] * 2 + (ci & 1), cy = info.c[1] * 2 + ((ci >> 1) & 1), cz = info.c[2] * 2 + ((ci >> 2) & 1);
+                    Info ch = g.dev_info(i + 1, cx, cy, cz);
+                    if ((ch.type & GHOST) && (g.mem[ch.mem].status & REFINE_FLAG)) to_refine = true;
+                }
+            }
+            if (i + 1 >= g.num_layers) to_refine = false;
+            TileMem& tm = g.mem[info.mem];
+            tm.status = to_refine ? (tm.status | REFINE_FLAG) : (tm.status & ~REFINE_FLAG);
+            flag[j] = to_refine;
+        }
+        for (size_t j = 0; j < arr.size(); j++) {  // kernel on GHOST tiles of level i
+            const Info& info = arr[j];
+            if (!(info.type & GHOST)) continue;
+            bool rf = false;
+            for (int n = 0; n < 6; n++) {
+                Info nb = g.dev_info(i, info.c[0] + kNbOff[n][0], info.c[1] + kNbOff[n][1], info.c[2] + kNbOff[n][2]);
+                if ((nb.type & LEAF) && (g.mem[nb.mem].status & REFINE_FLAG)) rf = true;
+            }
+            TileMem& tm = g.mem[info.mem];
+            tm.status = rf ? (tm.status | REFINE_FLAG) : (tm.status & ~REFINE_FLAG);
+        }
+        for (size_t j = 0; j < arr.size(); j++) {  // host: create children
+            if (!flag[j]) continue;
+            cnt[i]++;
+            const Info& tmp = arr[j];
+            int s = Grid::probe(g.host_hash[i], g.log2hash[i], tmp.c[0], tmp.c[1], tmp.c[2]);
+            Info& hinfo = g.host_hash[i][s];
+            hinfo.type = NONLEAF;
+            TileMem parent = g.mem[hinfo.mem];
+            for (int ci = 0; ci < 8; ci++) {
+                int ox = ci & 1, oy = (ci >> 1) & 1, oz = (ci >> 2) & 1;
+                g.set_tile_host(i + 1, hinfo.c[0] * 2 + ox, hinfo.c[1] * 2 + oy, hinfo.c[2] * 2 + oz,
+                                child_tile(parent, ox, oy, oz), LEAF);
+            }
+        }
+    }
+    g.compress();
+    g.sync();
+    return cnt;
+}
+
+void iterative_refine(Grid& g, const Masks& mk) {  // src/PoissonGrid.h:316-326
+    while (true) {
+        auto c = refine_step(g, mk);
+        spawn_ghosts(g);
+        int tot = 0;
+        for (int v : c) tot += v;
+        if (tot == 0) break;
+    }
+}
+
+// ------------------------------------------------------------------- flat solver view
+inline uint64_t key(int level, int x, int y, int z) {
+    return ((uint64_t)(uint32_t)level << 60) ^ ((uint64_t)((uint32_t)x & 0xFFFFF) << 40) ^
+           ((uint64_t)((uint32_t)y & 0xFFFFF) << 20) ^ (uint64_t)((uint32_t)z & 0xFFFFF);
+}
+
+struct Flat {
+    int n = 0;
+    int num_layers = 0;
+    int max_level = -1;
+    double h0 = 0.125;
+    std::vector<int> level, cx, cy, cz;
+    std::vector<uint8_t> type;
+    std::vector<uint8_t> ctype;               // n*512
+    std::vector<std::vector<int>> by_level;  // tile indices per level (all-order)
+    std::unordered_map<uint64_t, int> lut;
+    std::vector<int> nbr;                     // n*6 (x-,y-,z-,x+,y+,z+), -1 empty
+    std::vector<int> parent;                  // tile at level-1 containing this tile, or -1
+
+    int find(int l, int x, int y, int z) const {
+        if (l < 0 || l >= num_layers) return -1;
+        auto it = lut.find(key(l, x, y, z));
+        return it == lut.end() ? -1 : it->second;
+    }
+    // findVoxel: global cell coordinate at level l -> (tile, local offset)
+    int find_voxel(int l, int gx, int gy, int gz, int& off) const {
+        int t = find(l, gx >> 3, gy >> 3, gz >> 3);
+        off = loff(gx & 7, gy & 7, gz & 7);
+        return t;
+    }
+    void build(const int* lv, const int* coords, const uint8_t* types, int ntiles, int nlayers) {
+        n = ntiles; num_layers = nlayers;
+        level.assign(lv, lv + n);
+        type.assign(types, types + n);
+        cx.resize(n); cy.resize(n); cz.resize(n);
+        by_level.assign(num_layers, {});
+        lut.clear();
+        max_level = -1;
+        for (int t = 0; t < n; t++) {
+            cx[t] = coords[3 * t]; cy[t] = coords[3 * t + 1]; cz[t] = coords[3 * t + 2];
+            by_level[level[t]].push_back(t);
+            lut[key(level[t], cx[t], cy[t], cz[t])] = t;
+            max_level = std::max(max_level, level[t]);
+        }
+        nbr.assign((size_t)n * 6, -1);
+        parent.assign(n, -1);
+        for (int t = 0; t < n; t++) {
+            for (int a = 0; a < 3; a++) {
+                int m[3] = {cx[t], cy[t], cz[t]}, p[3] = {cx[t], cy[t], cz[t]};
+                m[a]--; p[a]++;
+                nbr[(size_t)t * 6 + a] = find(level[t], m[0], m[1], m[2]);
+                nbr[(size_t)t * 6 + a + 3] = find(level[t], p[0], p[1], p[2]);
+            }
+            parent[t] = find(level[t] - 1, cx[t] >> 1, cy[t] >> 1, cz[t] >> 1);
+        }
+        ctype.assign((size_t)n * NCELL, 0);
+    }
+    uint8_t subtree_type(int t, int sl) const { return (level[t] == sl && type[t] == NONLEAF) ? LEAF : type[t]; }
+};
+
+// ------------------------------------------------------------------- arithmetic helpers
+template <class T> inline T fmaT(T a, T b, T c) { return std::fma(a, b, c); }
+
+template <class T>
+inline T voxel_size(int level) {  // HAAccessor.h:72-74, mH0 stored in T
+    return (T)0.125 / (T)(1 << level);
+}
+
+// src/GMGSolver.cu:12-40
+template <class T>
+inline T lap_coeff(T one_over_h, uint8_t tt0, uint8_t tt1, uint8_t ct0, uint8_t ct1) {
+    int both_leafs = int((tt0 & LEAF) && (tt1 & LEAF));
+    int one_leaf_one_ghost = int(((tt0 & LEAF) && (tt1 & GHOST)) || ((tt0 & GHOST) && (tt1 & LEAF)));
+    T odh = one_over_h * (T)both_leafs + (2 * one_over_h / 3) * (T)one_leaf_one_ghost;
+    int has_neumann = int((ct0 & NEUMANN) || (ct1 & NEUMANN));
+    return has_neumann ? (T)0 : odh * one_over_h;
+}
+
+// Stencil value access: value/ttype/ctype of the cell at local (i,j,k) of tile t, where one
+// coordinate may be -1 or 8 (face halo, src/GMGSolver.cu:90-143).
+template <class T>
+struct Halo {
+    const Flat& f;
+    const T* x;
+    int sl;  // subtree level
+    inline void get(int t, int i, int j, int k, T& xv, uint8_t& tt, uint8_t& ct) const {
+        int face = -1;
+        if (i < 0) face = 0; else if (i > 7) face = 3;
+        else if (j < 0) face = 1; else if (j > 7) face = 4;
+        else if (k < 0) face = 2; else if (k > 7) face = 5;
+        if (face < 0) {
+            int o = loff(i, j, k);
+            xv = x[(size_t)t * NCELL + o];
+            tt = f.subtree_type(t, sl);
+            ct = f.ctype[(size_t)t * NCELL + o];
+            return;
+        }
+        int nb = f.nbr[(size_t)t * 6 + face];
+        if (nb < 0) { xv = 0; tt = f.subtree_type(t, sl); ct = DIRICHLET; return; }
+        int o = loff(i & 7, j & 7, k & 7);
+        xv = x[(size_t)nb * NCELL + o];
+        tt = f.subtree_type(nb, sl);
+        ct = f.ctype[(size_t)nb * NCELL + o];
+    }
+};
+
+// GMGLaplacianTileData::negativeLap (src/GMGSolver.cu:56-76).  h^3 * sum_f c_f (x0 - x1).
+template <class T>
+inline T neg_lap(const Halo<T>& H, int t, int i, int j, int k, bool diag) {
+    T h = voxel_size<T>(H.f.level[t]);
+    T one_over_h = (T)1 / h;
+    T x0; uint8_t tt0, ct0;
+    H.get(t, i, j, k, x0, tt0, ct0);
+    T sum = 0;
+    for (int axis = 0; axis < 3; axis++) {
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+            int n[3] = {i, j, k};
+            n[axis] += sgn;
+            T x1; uint8_t tt1, ct1;
+            H.get(t, n[0], n[1], n[2], x1, tt1, ct1);
+            T c = lap_coeff<T>(one_over_h, tt0, tt1, ct0, ct1);
+            sum = diag ? sum + c : fmaT<T>(c, x0 - x1, sum);
+        }
+    }
+    return (ct0 & INTERIOR) ? sum * h * h * h : (T)0;
+}
+
+template <class T>
+struct Solver {
+    Flat& f;
+    std::vector<T> ch[6];  // 0 x, 1 b/r, 2 p, 3 Ap/rhs, 4 z, 5 scratch
+    T one_over_alpha = 1, prolong_coeff = 1;
+    explicit Solver(Flat& fl) : f(fl) { for (auto& c : ch) c.assign((size_t)f.n * NCELL, (T)0); }
+
+    T* C(int c) { return ch[c].data(); }
+
+    // PropagateValuesToGhostTiles (src/PoissonGrid.cu:585-605)
+    void propagate_ghosts(int c) {
+        T* v = C(c);
+#pragma omp parallel for schedule(static)
+        for (int t = 0; t < f.n; t++) {
+            if (!(f.type[t] & GHOST)) continue;
+            for (int o = 0; o < NCELL; o++) {
+                size_t id = (size_t)t * NCELL + o;
+                if (!(f.ctype[id] & INTERIOR)) { v[id] = 0; continue; }
+                int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                int gx = f.cx[t] * 8 + i, gy = f.cy[t] * 8 + j, gz = f.cz[t] * 8 + k;
+                int po;
+                int p = f.find_voxel(f.level[t] - 1, gx >> 1, gy >> 1, gz >> 1, po);
+                if (p < 0) { v[id] = 0; continue; }
+                size_t pid = (size_t)p * NCELL + po;
+                v[id] = (f.ctype[pid] & INTERIOR) ? v[pid] : (T)0;
+            }
+        }
+    }
+    // NegativeLaplacianSameLevel128 on LEAF|GHOST tiles of all levels (subtree -1)
+    void lap_tiles(int xc, int yc, bool diag) {
+        Halo<T> H{f, C(xc), -1};
+        T* y = C(yc);
+#pragma omp parallel for schedule(static)
+        for (int t = 0; t < f.n; t++) {
+            if (!(f.type[t] & (LEAF | GHOST))) continue;
+            for (int o = 0; o < NCELL; o++)
+                y[(size_t)t * NCELL + o] = neg_lap<T>(H, t, o >> 6, (o >> 3) & 7, o & 7, diag);
+        }
+    }
+    // AccumulateToParents128 on GHOST tiles, additive, cell types I|D|N (src/PoissonGrid.cu:664-719)
+    void accumulate_ghosts(int c) {
+        T* v = C(c);
+        for (int t = 0; t < f.n; t++) {  // sequential: parents of distinct ghosts are distinct cells
+            if (!(f.type[t] & GHOST)) continue;
+            for (int b = 0; b < 64; b++) {
+                int fi = b / 16 * 2, fj = (b / 4) % 4 * 2, fk = b % 4 * 2;
+                int gx = f.cx[t] * 8 + fi, gy = f.cy[t] * 8 + fj, gz = f.cz[t] * 8 + fk;
+                int po;
+                int p = f.find_voxel(f.level[t] - 1, gx >> 1, gy >> 1, gz >> 1, po);
+                if (p < 0) continue;
+                T sum = 0;
+                for (int ii = 0; ii < 2; ii++) for (int jj = 0; jj < 2; jj++) for (int kk = 0; kk < 2; kk++) {
+                    size_t id = (size_t)t * NCELL + loff(fi + ii, fj + jj, fk + kk);
+                    sum += (f.ctype[id] & (INTERIOR | DIRICHLET | NEUMANN)) ? v[id] : (T)0;
+                }
+                size_t pid = (size_t)p * NCELL + po;
+                v[pid] = fmaT<T>(sum, (T)1, v[pid]);
+            }
+        }
+    }
+    // FullNegativeLaplacian (src/GMGSolver.cu:203-213)
+    void full_lap(int xc, int yc) {
+        propagate_ghosts(xc);
+        lap_tiles(xc, yc, false);
+        accumulate_ghosts(yc);
+    }
+    // one red-black colour sweep on LEAF|NONLEAF tiles of 'level' (src/GMGSolver.cu:216-269)
+    void gs_sweep(int level, int xc, int rc, int color) {
+        Halo<T> H{f, C(xc), level};
+        T* x = C(xc);
+        const T* r = C(rc);
+        const auto& tl = f.by_level[level];
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < (int)tl.size(); q++) {
+            int t = tl[q];
+            if (!(f.subtree_type(t, level) & (LEAF | NONLEAF))) continue;
+            for (int o = 0; o < NCELL; o++) {
+                int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                if ((i + j + k) % 2 != color) continue;
+                size_t id = (size_t)t * NCELL + o;
+                uint8_t ct = f.ctype[id];
+                T b = r[id];
+                T Ax = neg_lap<T>(H, t, i, j, k, false);
+                T D = neg_lap<T>(H, t, i, j, k, true);
+                T dx = (ct & INTERIOR) ? (b - Ax) / D : (T)0;
+                x[id] = x[id] + dx;
+            }
+        }
+    }
+    void gauss_seidel(int iters, int order, int level, int xc, int rc) {  // GMGSolver.cu:277-282
+        for (int it = 0; it < iters; it++) {
+            gs_sweep(level, xc, rc, order);
+            gs_sweep(level, xc, rc, 1 - order);
+        }
+    }
+    // ResidualAndRestrict128Kernel (src/GMGSolver.cu:284-339)
+    void residual_restrict(int level, int xc, int rhsc, int coarsec) {
+        Halo<T> H{f, C(xc), level};
+        const T* rhs = C(rhsc);
+        T* crs = C(coarsec);
+        const auto& tl = f.by_level[level];
+        std::vector<T> res((size_t)tl.size() * NCELL);
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < (int)tl.size(); q++) {
+            int t = tl[q];
+            for (int o = 0; o < NCELL; o++)
+                res[(size_t)q * NCELL + o] = rhs[(size_t)t * NCELL + o] - neg_lap<T>(H, t, o >> 6, (o >> 3) & 7, o & 7, false);
+        }
+        for (int q = 0; q < (int)tl.size(); q++) {
+            int t = tl[q];
+            bool ghost = f.subtree_type(t, level) & GHOST;
+            for (int b = 0; b < 64; b++) {
+                int fi = b / 16 * 2, fj = (b / 4) % 4 * 2, fk = b % 4 * 2;
+                int gx = f.cx[t] * 8 + fi, gy = f.cy[t] * 8 + fj, gz = f.cz[t] * 8 + fk;
+                int po;
+                int p = f.find_voxel(level - 1, gx >> 1, gy >> 1, gz >> 1, po);
+                if (p < 0) continue;
+                T sum = 0;
+                for (int ii = 0; ii < 2; ii++) for (int jj = 0; jj < 2; jj++) for (int kk = 0; kk < 2; kk++)
+                    sum += res[(size_t)q * NCELL + loff(fi + ii, fj + jj, fk + kk)];
+                size_t pid = (size_t)p * NCELL + po;
+                if (ghost) crs[pid] += sum;
+                else crs[pid] = sum * one_over_alpha;
+            }
+        }
+    }
+    // ProlongateAndUpdate128Kernel (src/GMGSolver.cu:345-376)
+    void prolongate(int level, int cxc, int fxc) {
+        const auto& tl = f.by_level[level];
+        T* fx = C(fxc);
+        const T* cxv = C(cxc);
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < (int)tl.size(); q++) {
+            int t = tl[q];
+            uint8_t ft = f.subtree_type(t, level);
+            for (int o = 0; o < NCELL; o++) {
+                int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                int gx = f.cx[t] * 8 + i, gy = f.cy[t] * 8 + j, gz = f.cz[t] * 8 + k;
+                int po;
+                int p = f.find_voxel(level - 1, gx >> 1, gy >> 1, gz >> 1, po);
+                T c = (p < 0) ? (T)0 : cxv[(size_t)p * NCELL + po];
+                size_t id = (size_t)t * NCELL + o;
+                bool interior = f.ctype[id] & INTERIOR;
+                if (ft & GHOST) fx[id] = interior ? c : (T)0;
+                else fx[id] = interior ? fmaT<T>(prolong_coeff, c, fx[id]) : (T)0;
+            }
+        }
+    }
+    // GMGSolver::VCycle (src/GMGSolver.cu:383-447)
+    void vcycle(int xc, int fc, int rhsc, int level_iters, int coarsest_iters) {
+        T* x = C(xc); T* rhs = C(rhsc); const T* fv = C(fc);
+#pragma omp parallel for schedule(static)
+        for (int t = 0; t < f.n; t++) {
+            for (int o = 0; o < NCELL; o++) {
+                size_t id = (size_t)t * NCELL + o;
+                x[id] = 0;
+                rhs[id] = (f.type[t] & GHOST) ? (T)0 : fv[id];
+            }
+        }
+        for (int l = f.max_level; l > 0; l--) {
+            gauss_seidel(level_iters, 0, l, xc, rhsc);
+            residual_restrict(l, xc, rhsc, rhsc);
+        }
+        gauss_seidel(coarsest_iters / 2, 0, 0, xc, rhsc);
+        gauss_seidel(coarsest_iters / 2, 1, 0, xc, rhsc);
+        for (int l = 1; l <= f.max_level; l++) {
+            prolongate(l, xc, xc);
+            gauss_seidel(level_iters, 1, l, xc, rhsc);
+        }
+    }
+    // Dot over LEAF tiles: 4-cell FP32 partials widened to FP64 (src/PoissonGrid.cu:165-214)
+    double dot(int a, int b) {
+        const T* A = C(a); const T* B = C(b);
+        double total = 0;
+        for (int t = 0; t < f.n; t++) {
+            if (!(f.type[t] & LEAF)) continue;
+            for (int g = 0; g < 128; g++) {
+                const T* p = A + (size_t)t * NCELL + 4 * g;
+                const T* q = B + (size_t)t * NCELL + 4 * g;
+                T s = fmaT<T>(p[0], q[0], p[1] * q[1]);
+                s = fmaT<T>(p[2], q[2], s);
+                s = fmaT<T>(p[3], q[3], s);
+                total += (double)s;
+            }
+        }
+        return total;
+    }
+    // MeanAsync + ReCenterLeafVoxels (src/PoissonGrid.cu:231-325, src/PoissonSolver.cu:356-368)
+    void recenter(int c) {
+        T* v = C(c);
+        double sum = 0, count = 0;
+        for (int t = 0; t < f.n; t++) {
+            if (!(f.type[t] & LEAF)) continue;
+            for (int g = 0; g < 128; g++) {
+                const T* p = v + (size_t)t * NCELL + 4 * g;
+                sum += (double)(p[0] + p[1] + p[2] + p[3]);
+                for (int e = 0; e < 4; e++) count += (f.ctype[(size_t)t * NCELL + 4 * g + e] & INTERIOR) ? 2 : 0;
+            }
+        }
+        // InteriorCount128Kernel adds (type & INTERIOR), i.e. 2 per interior cell.
+        double mean = sum / count;
+        for (int t = 0; t < f.n; t++) {
+            if (!(f.type[t] & LEAF)) continue;
+            for (int o = 0; o < NCELL; o++) {
+                size_t id = (size_t)t * NCELL + o;
+                if (f.ctype[id] & INTERIOR) v[id] = (T)((double)v[id] - mean);
+            }
+        }
+    }
+    template <class F> void leaf_cells(F fn) {
+#pragma omp parallel for schedule(static)
+        for (int t = 0; t < f.n; t++) {
+            if (!(f.type[t] & LEAF)) continue;
+            for (int o = 0; o < NCELL; o++) fn((size_t)t * NCELL + o);
+        }
+    }
+    // GMGSolver::solve (src/GMGSolver.cu:531-666). Returns iterations; writes rel residual.
+    int solve(int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, bool pure_neumann,
+              double& rel, std::vector<double>* history) {
+        T* x = C(0); T* r = C(1); T* p = C(2); T* Ap = C(3); T* z = C(4);
+        leaf_cells([&](size_t id) { x[id] = 0; });
+        double rhs2 = 0, thr2 = 0;
+        if (sync_stride > 0) {
+            rhs2 = dot(1, 1);
+            if (rhs2 == 0.0) { rel = 0; return 0; }
+            thr2 = std::max(tol * tol * rhs2, DBL_MIN);
+        }
+        if (pure_neumann) recenter(1);
+        vcycle(4, 1, 3, level_iters, coarsest_iters);
+        leaf_cells([&](size_t id) { p[id] = z[id]; });
+        double gamma = dot(4, 1);
+        int i = 0;
+        for (i = 0; i < max_iters; i++) {
+            full_lap(2, 3);
+            double fp = dot(2, 3);
+            double alpha = gamma / fp;
+            T a = (T)alpha;
+            leaf_cells([&](size_t id) { if (f.ctype[id] & INTERIOR) x[id] = fmaT<T>(a, p[id], x[id]); });
+            leaf_cells([&](size_t id) { if (f.ctype[id] & INTERIOR) r[id] = fmaT<T>(-a, Ap[id], r[id]); });
+            if (sync_stride > 0 && (i + 1) % sync_stride == 0) {
+                double res2 = dot(1, 1);
+                if (history) history->push_back(std::sqrt(res2 / rhs2));
+                if (res2 < thr2) { rel = std::sqrt(res2 / rhs2); return i + 1; }
+            }
+            if (pure_neumann) recenter(1);
+            vcycle(4, 1, 3, level_iters, coarsest_iters);
+            double gamma_old = gamma;
+            gamma = dot(1, 4);
+            double beta = gamma / gamma_old;
+            T bb = (T)beta;
+            leaf_cells([&](size_t id) { if (f.ctype[id] & INTERIOR) p[id] = fmaT<T>(bb, p[id], z[id]); });
+        }
+        if (sync_stride > 0) { rel = std::sqrt(dot(1, 1) / rhs2); return i; }
+        rel = -1;
+        return i;
+    }
+};
+
+// ---------------------------------------------------------------- RHS construction
+// IterateFaceNeighborCellTypes (src/PoissonGrid.h:451-489) + ClearAllNeumannNeighborFaces
+// (src/FluidEuler.cu:43-60) on LEAF tiles; u,v,w are per-cell lower-face velocities.
+void clear_faces(const Flat& f, float* u[3]) {
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < f.n; t++) {
+        if (!(f.type[t] & LEAF)) continue;
+        for (int o = 0; o < NCELL; o++) {
+            int l[3] = {o >> 6, (o >> 3) & 7, o & 7};
+            int g[3] = {f.cx[t] * 8 + l[0], f.cy[t] * 8 + l[1], f.cz[t] * 8 + l[2]};
+            uint8_t t0 = f.ctype[(size_t)t * NCELL + o];
+            for (int axis = 0; axis < 3; axis++) {
+                bool to_set = false;
+                auto test = [&](uint8_t t1) {
+                    if ((t0 & NEUMANN) || (t1 & NEUMANN) || ((t0 & DIRICHLET) && (t1 & DIRICHLET))) to_set = true;
+                };
+                int ng[3] = {g[0], g[1], g[2]};
+                ng[axis]--;
+                int no;
+                int nt = f.find_voxel(f.level[t], ng[0], ng[1], ng[2], no);
+                if (nt >= 0) {
+                    if (!(f.type[nt] & LEAF)) {
+                        for (int oj = 0; oj < 2; oj++) for (int ok = 0; ok < 2; ok++) {
+                            int co[3];
+                            co[axis] = 1; co[(axis + 1) % 3] = oj; co[(axis + 2) % 3] = ok;
+                            int cg[3] = {ng[0] * 2 + co[0], ng[1] * 2 + co[1], ng[2] * 2 + co[2]};
+                            int cot;
+                            int ct = f.find_voxel(f.level[t] + 1, cg[0], cg[1], cg[2], cot);
+                            if (ct >= 0) test(f.ctype[(size_t)ct * NCELL + cot]);
+                        }
+                    } else {
+                        test(f.ctype[(size_t)nt * NCELL + no]);
+                    }
+                }
+                if (to_set) u[axis][(size_t)t * NCELL + o] = 0;
+            }
+        }
+    }
+}
+
+// PropagateToChildren(u, u, -1, GHOST, LAUNCH_SUBTREE, I|D|N) (src/PoissonGrid.cu:635-661)
+void propagate_u(const Flat& f, float* u) {
+    for (int l = 0; l < f.num_layers; l++) {
+        for (int t : f.by_level[l]) {
+            if (!(f.type[t] & GHOST)) continue;
+            for (int o = 0; o < NCELL; o++) {
+                size_t id = (size_t)t * NCELL + o;
+                if (!(f.ctype[id] & 7)) continue;
+                int gx = f.cx[t] * 8 + (o >> 6), gy = f.cy[t] * 8 + ((o >> 3) & 7), gz = f.cz[t] * 8 + (o & 7);
+                int po;
+                int p = f.find_voxel(l - 1, gx >> 1, gy >> 1, gz >> 1, po);
+                float val = 0;
+                if (p >= 0) {
+                    val = u[(size_t)p * NCELL + po];
+                    if (!(f.ctype[(size_t)p * NCELL + po] & 7)) val = 0;
+                }
+                u[id] = val;
+            }
+        }
+    }
+}
+
+// VelocityVolumeDivergenceOnLeafs (src/PoissonSolver.cu:66-142) + AccumulateToParents
+// (src/PoissonGrid.cu:721-755, LEAF, INTERIOR, coeff 1, additive).  FP32 as in the reference.
+void divergence(const Flat& f, float* const u[3], float* b) {
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < f.n; t++) {
+        if (!(f.type[t] & (LEAF | GHOST))) continue;
+        float h = voxel_size<float>(f.level[t]);
+        uint8_t tt = f.type[t];
+        for (int o = 0; o < NCELL; o++) {
+            size_t id = (size_t)t * NCELL + o;
+            uint8_t ct = f.ctype[id];
+            if (!(ct & INTERIOR)) { b[id] = 0; continue; }
+            int l[3] = {o >> 6, (o >> 3) & 7, o & 7};
+            int g[3] = {f.cx[t] * 8 + l[0], f.cy[t] * 8 + l[1], f.cz[t] * 8 + l[2]};
+            float sum = 0;
+            for (int axis = 0; axis < 3; axis++) {
+                for (int sgn = -1; sgn <= 1; sgn += 2) {
+                    int ng[3] = {g[0], g[1], g[2]};
+                    ng[axis] += sgn;
+                    int no;
+                    int nt = f.find_voxel(f.level[t], ng[0], ng[1], ng[2], no);
+                    float u0 = u[axis][id], u1;
+                    uint8_t ntt;
+                    if (nt < 0) { ntt = tt; u1 = 0; }
+                    else { ntt = f.type[nt]; u1 = u[axis][(size_t)nt * NCELL + no]; }
+                    bool ok = (tt == LEAF && ntt == LEAF) || (tt == LEAF && ntt == GHOST) || (tt == GHOST && ntt == LEAF);
+                    if (!ok) continue;
+                    float uu = (sgn == -1) ? -u0 : u1;
+                    sum = std::fma(uu * h, h, sum);
+                }
+            }
+            b[id] = sum;
+        }
+    }
+    for (int l = f.num_layers - 1; l >= 0; l--) {
+        for (int t : f.by_level[l]) {
+            if (!(f.type[t] & LEAF)) continue;
+            for (int o = 0; o < NCELL; o++) {
+                size_t id = (size_t)t * NCELL + o;
+                if (!(f.ctype[id] & INTERIOR)) continue;
+                int g[3] = {f.cx[t] * 8 + (o >> 6), f.cy[t] * 8 + ((o >> 3) & 7), f.cz[t] * 8 + (o & 7)};
+                float sum = 0;
+                for (int cid = 0; cid < 8; cid++) {
+                    int cg[3] = {g[0] * 2 + (cid & 1), g[1] * 2 + ((cid >> 1) & 1), g[2] * 2 + ((cid >> 2) & 1)};
+                    int co;
+                    int ct = f.find_voxel(l + 1, cg[0], cg[1], cg[2], co);
+                    if (ct >= 0 && (f.ctype[(size_t)ct * NCELL + co] & INTERIOR)) sum += b[(size_t)ct * NCELL + co];
+                }
+                b[id] = std::fma(sum, 1.0f, b[id]);
+            }
+        }
+    }
+}
+
+// CalcCellTypesFromLeafs (src/PoissonSolver.cu:7-61) on a flat view (types of LEAF tiles given)
+void calc_cell_types(Flat& f) {
+    for (int l = f.num_layers - 1; l >= 0; l--) {
+        for (int t : f.by_level[l]) {
+            if (!(f.type[t] & NONLEAF)) continue;
+            for (int o = 0; o < NCELL; o++) {
+                int g[3] = {f.cx[t] * 8 + (o >> 6), f.cy[t] * 8 + ((o >> 3) & 7), f.cz[t] * 8 + (o & 7)};
+                int dcnt = 0, icnt = 0;
+                for (int s = 0; s < 8; s++) {
+                    int cg[3] = {g[0] * 2 + (s & 1), g[1] * 2 + ((s >> 1) & 1), g[2] * 2 + ((s >> 2) & 1)};
+                    int co;
+                    int ct = f.find_voxel(l + 1, cg[0], cg[1], cg[2], co);
+                    if (ct < 0 || !(f.type[ct] & (LEAF | NONLEAF))) continue;
+                    uint8_t ty = f.ctype[(size_t)ct * NCELL + co];
+                    if (ty & DIRICHLET) dcnt++;
+                    else if (ty & INTERIOR) icnt++;
+                }
+                f.ctype[(size_t)t * NCELL + o] = dcnt > 0 ? DIRICHLET : (icnt > 0 ? INTERIOR : NEUMANN);
+            }
+        }
+    }
+    for (int t = 0; t < f.n; t++) {
+        if (!(f.type[t] & GHOST)) continue;
+        for (int o = 0; o < NCELL; o++) {
+            int g[3] = {f.cx[t] * 8 + (o >> 6), f.cy[t] * 8 + ((o >> 3) & 7), f.cz[t] * 8 + (o & 7)};
+            int po;
+            int p = f.find_voxel(f.level[t] - 1, g[0] >> 1, g[1] >> 1, g[2] >> 1, po);
+            f.ctype[(size_t)t * NCELL + o] = (p >= 0) ? f.ctype[(size_t)p * NCELL + po] : DIRICHLET;
+        }
+    }
+}
+
+}  // namespace
+
+// ===================================================================== C interface (ctypes)
+extern "C" {
+
+// --- topology restatement
+void* ocx_topo_create(int num_layers, const uint32_t* log2hash) {
+    Grid* g = new Grid();
+    g->num_layers = num_layers;
+    g->log2hash.assign(log2hash, log2hash + num_layers);
+    g->host_hash.resize(num_layers);
+    for (int l = 0; l < num_layers; l++) g->host_hash[l].assign(1u << log2hash[l], Info());
+    g->arrays.assign(num_layers, {});
+    g->dev_hash = g->host_hash;
+    return g;
+}
+void ocx_topo_destroy(void* h) { delete (Grid*)h; }
+int ocx_topo_set_tile(void* h, int level, int x, int y, int z, int type) {
+    return ((Grid*)h)->set_tile_host(level, x, y, z, TileMem(), (uint8_t)type) ? 0 : -1;
+}
+void ocx_topo_compress_sync(void* h) { ((Grid*)h)->compress(); ((Grid*)h)->sync(); }
+void ocx_topo_spawn_ghosts(void* h) { spawn_ghosts(*(Grid*)h); }
+int ocx_topo_refine_step(void* h, const uint8_t* const* masks, const int* dims, int* per_level) {
+    Masks mk{masks, dims};
+    auto c = refine_step(*(Grid*)h, mk);
+    int tot = 0;
+    for (size_t i = 0; i < c.size(); i++) { tot += c[i]; if (per_level) per_level[i] = c[i]; }
+    return tot;
+}
+void ocx_topo_iterative_refine(void* h, const uint8_t* const* masks, const int* dims) {
+    Masks mk{masks, dims};
+    iterative_refine(*(Grid*)h, mk);
+}
+int ocx_topo_num_tiles(void* h) { return (int)((Grid*)h)->all.size(); }
+// tiles in dAllTiles order: level, x, y, z, type per tile
+void ocx_topo_tiles(void* h, int* out) {
+    Grid* g = (Grid*)h;
+    for (size_t i = 0; i < g->all.size(); i++) {
+        const Info& o = g->all[i];
+        out[5 * i] = o.level; out[5 * i + 1] = o.c[0]; out[5 * i + 2] = o.c[1]; out[5 * i + 3] = o.c[2];
+        out[5 * i + 4] = o.type;
+    }
+}
+// hash-slot index of each tile in its level's table (for bit-exact layout checks)
+void ocx_topo_slots(void* h, int* out) {
+    Grid* g = (Grid*)h;
+    for (size_t i = 0; i < g->all.size(); i++) {
+        const Info& o = g->all[i];
+        out[i] = Grid::probe(g->host_hash[o.level], g->log2hash[o.level], o.c[0], o.c[1], o.c[2]);
+    }
+}
+
+// --- flat solver view
+struct OCX {
+    Flat f;
+    Solver<float>* s32 = nullptr;
+    Solver<double>* s64 = nullptr;
+};
+void* ocx_flat_create(const int* tiles5, int ntiles, int num_layers) {
+    OCX* o = new OCX();
+    std::vector<int> lv(ntiles), co(3 * ntiles);
+    std::vector<uint8_t> ty(ntiles);
+    for (int t = 0; t < ntiles; t++) {
+        lv[t] = tiles5[5 * t]; co[3 * t] = tiles5[5 * t + 1]; co[3 * t + 1] = tiles5[5 * t + 2];
+        co[3 * t + 2] = tiles5[5 * t + 3]; ty[t] = (uint8_t)tiles5[5 * t + 4];
+    }
+    o->f.build(lv.data(), co.data(), ty.data(), ntiles, num_layers);
+    return o;
+}
+void ocx_flat_destroy(void* h) {
+    OCX* o = (OCX*)h;
+    delete o->s32; delete o->s64; delete o;
+}
+void ocx_flat_set_ctypes(void* h, const uint8_t* ct) {
+    OCX* o = (OCX*)h;
+    std::memcpy(o->f.ctype.data(), ct, o->f.ctype.size());
+}
+void ocx_flat_get_ctypes(void* h, uint8_t* ct) {
+    OCX* o = (OCX*)h;
+    std::memcpy(ct, o->f.ctype.data(), o->f.ctype.size());
+}
+void ocx_flat_calc_cell_types(void* h) { calc_cell_types(((OCX*)h)->f); }
+void ocx_flat_neighbors(void* h, int* out) {
+    OCX* o = (OCX*)h;
+    std::memcpy(out, o->f.nbr.data(), o->f.nbr.size() * sizeof(int));
+}
+// RHS pipeline: clear faces, propagate to ghosts, divergence (+ accumulate to parents)
+void ocx_flat_rhs(void* h, float* u, float* v, float* w, float* b) {
+    OCX* o = (OCX*)h;
+    float* uu[3] = {u, v, w};
+    clear_faces(o->f, uu);
+    for (int a = 0; a < 3; a++) propagate_u(o->f, uu[a]);
+    divergence(o->f, uu, b);
+}
+
+static Solver<float>& S32(OCX* o) { if (!o->s32) o->s32 = new Solver<float>(o->f); return *o->s32; }
+static Solver<double>& S64(OCX* o) { if (!o->s64) o->s64 = new Solver<double>(o->f); return *o->s64; }
+
+// channel io; prec 0 = fp32 mirror, 1 = fp64
+void ocx_set_channel(void* h, int prec, int c, const double* data) {
+    OCX* o = (OCX*)h;
+    size_t n = (size_t)o->f.n * NCELL;
+    if (prec == 0) { auto& s = S32(o); for (size_t i = 0; i < n; i++) s.ch[c][i] = (float)data[i]; }
+    else { auto& s = S64(o); for (size_t i = 0; i < n; i++) s.ch[c][i] = data[i]; }
+}
+void ocx_get_channel(void* h, int prec, int c, double* data) {
+    OCX* o = (OCX*)h;
+    size_t n = (size_t)o->f.n * NCELL;
+    if (prec == 0) { auto& s = S32(o); for (size_t i = 0; i < n; i++) data[i] = s.ch[c][i]; }
+    else { auto& s = S64(o); for (size_t i = 0; i < n; i++) data[i] = s.ch[c][i]; }
+}
+void ocx_set_channel_f32(void* h, int c, const float* data) {
+    OCX* o = (OCX*)h;
+    auto& s = S32(o);
+    std::memcpy(s.ch[c].data(), data, s.ch[c].size() * sizeof(float));
+}
+void ocx_get_channel_f32(void* h, int c, float* data) {
+    OCX* o = (OCX*)h;
+    auto& s = S32(o);
+    std::memcpy(data, s.ch[c].data(), s.ch[c].size() * sizeof(float));
+}
+
+// individual operators (for kernel-level parity)
+void ocx_full_lap(void* h, int prec, int xc, int yc) {
+    OCX* o = (OCX*)h;
+    if (prec == 0) S32(o).full_lap(xc, yc); else S64(o).full_lap(xc, yc);
+}
+void ocx_gs_sweep(void* h, int prec, int level, int xc, int rc, int color) {
+    OCX* o = (OCX*)h;
+    if (prec == 0) S32(o).gs_sweep(level, xc, rc, color); else S64(o).gs_sweep(level, xc, rc, color);
+}
+void ocx_residual_restrict(void* h, int prec, int level, int xc, int rhsc, int coarsec) {
+    OCX* o = (OCX*)h;
+    if (prec == 0) S32(o).residual_restrict(level, xc, rhsc, coarsec);
+    else S64(o).residual_restrict(level, xc, rhsc, coarsec);
+}
+void ocx_prolongate(void* h, int prec, int level, int cxc, int fxc) {
+    OCX* o = (OCX*)h;
+    if (prec == 0) S32(o).prolongate(level, cxc, fxc); else S64(o).prolongate(level, cxc, fxc);
+}
+void ocx_vcycle(void* h, int prec, int xc, int fc, int rhsc, int level_iters, int coarsest_iters) {
+    OCX* o = (OCX*)h;
+    if (prec == 0) S32(o).vcycle(xc, fc, rhsc, level_iters, coarsest_iters);
+    else S64(o).vcycle(xc, fc, rhsc, level_iters, coarsest_iters);
+}
+double ocx_dot(void* h, int prec, int a, int b) {
+    OCX* o = (OCX*)h;
+    return prec == 0 ? S32(o).dot(a, b) : S64(o).dot(a, b);
+}
+// Full PCG solve; b in channel 1, x out in channel 0.  Returns iterations.
+int ocx_solve(void* h, int prec, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
+              int pure_neumann, double* rel, double* history, int hist_cap, int* hist_len) {
+    OCX* o = (OCX*)h;
+    std::vector<double> hist;
+    int it = prec == 0 ? S32(o).solve(max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0, *rel, &hist)
+                       : S64(o).solve(max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0, *rel, &hist);
+    if (hist_len) *hist_len = (int)hist.size();
+    if (history) for (int i = 0; i < (int)hist.size() && i < hist_cap; i++) history[i] = hist[i];
+    return it;
+}
+int ocx_num_threads() { return omp_get_max_threads(); }
+void ocx_set_threads(int n) { omp_set_num_threads(n); }
+
+}  // extern "C"

@@ -1,0 +1,236 @@
+// Harness around the reference's own CUDA implementation of the Poisson path.
+// TEST INFRASTRUCTURE ONLY: it is compiled together with the reference's unmodified sources
+// (src/GMGSolver.cu, src/PoissonSolver.cu, src/PoissonGrid.cu, src/HAGrid.cu,
+// common/Common.cpp) by oracle/build_ref.sh into oracle/_ref/libcirrus_ref.so, and is loaded
+// only by tests/, the fixture generator in tests/golden/ and bench.py's reference arm.
+//
+// It drives the reference through its public functions exactly as FluidEuler does
+// (src/FluidEuler.h:413-447 grid construction, :464 IterativeRefine, :581-612 project), with
+// a level-target lambda that reads dense per-level refinement masks.  The one piece restated
+// here is ClearAllNeumannNeighborFaces (src/FluidEuler.cu:43-60), because FluidEuler.cu needs
+// libraries absent from this image; it calls the reference's IterateFaceNeighborCellTypes.
+
+#include "GMGSolver.h"
+#include "PoissonSolver.h"
+
+#include <chrono>
+#include <cstddef>
+#include <map>
+#include <memory>
+
+// Non-static free functions of src/GMGSolver.cu that its header does not declare.
+void GaussSeidelGMG(int iters, int order, HADeviceGrid<Tile>& grid, int level, int x_channel, int rhs_channel);
+void ResidualAndRestrict(HADeviceGrid<Tile>& grid, int fine_x_channel, int fine_rhs_channel, int coarse_residual_channel,
+                         int level, uint8_t launch_tile_types, T one_over_alpha);
+void NegativeLaplacianAndGaussSeidelSameLevel128(HADeviceGrid<Tile>& grid, thrust::device_vector<HATileInfo<Tile>>& tiles,
+                                                 int launch_tile_num, int subtree_level, uint8_t launch_tile_types,
+                                                 int x_channel, int rhs_channel, int color);
+
+namespace {
+
+struct RefGrid {
+    std::unique_ptr<HADeviceGrid<Tile>> g;
+    std::unique_ptr<GMGSolver> solver;
+};
+
+__global__ void GatherChannelKernel(HATileInfo<Tile>* tiles, int c, float* out) {
+    const HATileInfo<Tile>& info = tiles[blockIdx.x];
+    for (int v = threadIdx.x; v < 512; v += blockDim.x) out[(size_t)blockIdx.x * 512 + v] = info.tile().mData[c][v];
+}
+__global__ void ScatterChannelKernel(HATileInfo<Tile>* tiles, int c, const float* in) {
+    const HATileInfo<Tile>& info = tiles[blockIdx.x];
+    for (int v = threadIdx.x; v < 512; v += blockDim.x) info.tile().mData[c][v] = in[(size_t)blockIdx.x * 512 + v];
+}
+__global__ void GatherTypesKernel(HATileInfo<Tile>* tiles, uint8_t* out) {
+    const HATileInfo<Tile>& info = tiles[blockIdx.x];
+    for (int v = threadIdx.x; v < 512; v += blockDim.x) out[(size_t)blockIdx.x * 512 + v] = info.tile().mCellType[v];
+}
+__global__ void ScatterTypesKernel(HATileInfo<Tile>* tiles, const uint8_t* in) {
+    const HATileInfo<Tile>& info = tiles[blockIdx.x];
+    for (int v = threadIdx.x; v < 512; v += blockDim.x) info.tile().mCellType[v] = in[(size_t)blockIdx.x * 512 + v];
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_device_ok() {
+    int n = 0;
+    return cudaGetDeviceCount(&n) == cudaSuccess && n > 0 ? 1 : 0;
+}
+
+void* ref_create(int num_layers, const uint32_t* log2hash, double h0) {
+    thrust::host_vector<uint32_t> l2(log2hash, log2hash + num_layers);
+    RefGrid* r = new RefGrid();
+    r->g = std::make_unique<HADeviceGrid<Tile>>((T)h0, l2);
+    return r;
+}
+void ref_destroy(void* h) {
+    RefGrid* r = (RefGrid*)h;
+    r->solver.reset();
+    r->g.reset();
+    delete r;
+}
+void ref_set_tile(void* h, int level, int x, int y, int z, int type) {
+    ((RefGrid*)h)->g->setTileHost(level, nanovdb::Coord(x, y, z), Tile(), (uint8_t)type);
+}
+// src/FluidEuler.h:445-447
+void ref_compress_sync_spawn(void* h) {
+    auto& grid = *((RefGrid*)h)->g;
+    grid.compressHost(false);
+    grid.syncHostAndDevice();
+    SpawnGhostTiles(grid, false);
+}
+// IterativeRefine with level_target(tile) = level + mask[level][tile], masks dense per level.
+void ref_iterative_refine(void* h, const uint8_t* const* masks, const int* dims, int num_levels) {
+    auto& grid = *((RefGrid*)h)->g;
+    std::vector<thrust::device_vector<uint8_t>> dm(num_levels);
+    thrust::host_vector<const uint8_t*> hp(num_levels, nullptr);
+    thrust::host_vector<int> hd(3 * num_levels, 0);
+    for (int l = 0; l < num_levels; l++) {
+        hd[3 * l] = dims[3 * l]; hd[3 * l + 1] = dims[3 * l + 1]; hd[3 * l + 2] = dims[3 * l + 2];
+        size_t n = (size_t)dims[3 * l] * dims[3 * l + 1] * dims[3 * l + 2];
+        if (masks[l] && n > 0) {
+            dm[l] = thrust::device_vector<uint8_t>(masks[l], masks[l] + n);
+            hp[l] = thrust::raw_pointer_cast(dm[l].data());
+        }
+    }
+    thrust::device_vector<const uint8_t*> dptr = hp;
+    thrust::device_vector<int> ddims = hd;
+    const uint8_t* const* mp = thrust::raw_pointer_cast(dptr.data());
+    const int* dp = thrust::raw_pointer_cast(ddims.data());
+    int nl = num_levels;
+    auto level_target = [mp, dp, nl] __device__(const HATileAccessor<Tile>& acc, HATileInfo<Tile>& info) -> int {
+        int l = info.mLevel;
+        if (l >= nl || mp[l] == nullptr) return l;
+        int x = info.mTileCoord[0], y = info.mTileCoord[1], z = info.mTileCoord[2];
+        if (x < 0 || y < 0 || z < 0 || x >= dp[3 * l] || y >= dp[3 * l + 1] || z >= dp[3 * l + 2]) return l;
+        return mp[l][((size_t)x * dp[3 * l + 1] + y) * dp[3 * l + 2] + z] ? l + 1 : l;
+    };
+    IterativeRefine(grid, level_target, false);
+    cudaDeviceSynchronize();
+}
+int ref_num_tiles(void* h) { return (int)((RefGrid*)h)->g->hAllTiles.size(); }
+int ref_max_level(void* h) { return ((RefGrid*)h)->g->mMaxLevel; }
+void ref_tiles(void* h, int* out) {
+    auto& grid = *((RefGrid*)h)->g;
+    for (size_t i = 0; i < grid.hAllTiles.size(); i++) {
+        const auto& o = grid.hAllTiles[i];
+        out[5 * i] = o.mLevel; out[5 * i + 1] = o.mTileCoord[0]; out[5 * i + 2] = o.mTileCoord[1];
+        out[5 * i + 3] = o.mTileCoord[2]; out[5 * i + 4] = o.mType;
+    }
+}
+void ref_slots(void* h, int* out) {
+    auto& grid = *((RefGrid*)h)->g;
+    auto acc = grid.hostAccessor();
+    for (size_t i = 0; i < grid.hAllTiles.size(); i++) {
+        const auto& o = grid.hAllTiles[i];
+        out[i] = (int)acc.tileIdx(o.mLevel, o.mTileCoord);
+    }
+}
+void ref_set_ctypes(void* h, const uint8_t* ct) {
+    auto& grid = *((RefGrid*)h)->g;
+    size_t n = grid.dAllTiles.size();
+    thrust::device_vector<uint8_t> d(ct, ct + n * 512);
+    ScatterTypesKernel<<<n, 128>>>(thrust::raw_pointer_cast(grid.dAllTiles.data()), thrust::raw_pointer_cast(d.data()));
+    cudaDeviceSynchronize();
+}
+void ref_get_ctypes(void* h, uint8_t* ct) {
+    auto& grid = *((RefGrid*)h)->g;
+    size_t n = grid.dAllTiles.size();
+    thrust::device_vector<uint8_t> d(n * 512);
+    GatherTypesKernel<<<n, 128>>>(thrust::raw_pointer_cast(grid.dAllTiles.data()), thrust::raw_pointer_cast(d.data()));
+    thrust::copy(d.begin(), d.end(), ct);
+}
+void ref_calc_cell_types(void* h) { CalcCellTypesFromLeafs(*((RefGrid*)h)->g); cudaDeviceSynchronize(); }
+void ref_calc_neighbors(void* h) { CalculateNeighborTiles(*((RefGrid*)h)->g); cudaDeviceSynchronize(); }
+// neighbour table read back from each tile's mNeighbors, as indices into the all-tiles order
+void ref_neighbors(void* h, int* out) {
+    auto& grid = *((RefGrid*)h)->g;
+    std::map<const Tile*, int> idx;
+    for (size_t i = 0; i < grid.hAllTiles.size(); i++) idx[grid.hAllTiles[i].mTilePtr] = (int)i;
+    for (size_t i = 0; i < grid.hAllTiles.size(); i++) {
+        HATileInfo<Tile> nb[6];
+        cudaMemcpy(nb, (const char*)grid.hAllTiles[i].mTilePtr + offsetof(Tile, mNeighbors), sizeof(nb), cudaMemcpyDeviceToHost);
+        for (int f = 0; f < 6; f++) {
+            auto it = idx.find(nb[f].mTilePtr);
+            out[6 * i + f] = (nb[f].mTilePtr == nullptr || it == idx.end()) ? -1 : it->second;
+        }
+    }
+}
+void ref_set_channel(void* h, int c, const float* data) {
+    auto& grid = *((RefGrid*)h)->g;
+    size_t n = grid.dAllTiles.size();
+    thrust::device_vector<float> d(data, data + n * 512);
+    ScatterChannelKernel<<<n, 128>>>(thrust::raw_pointer_cast(grid.dAllTiles.data()), c, thrust::raw_pointer_cast(d.data()));
+    cudaDeviceSynchronize();
+}
+void ref_get_channel(void* h, int c, float* data) {
+    auto& grid = *((RefGrid*)h)->g;
+    size_t n = grid.dAllTiles.size();
+    thrust::device_vector<float> d(n * 512);
+    GatherChannelKernel<<<n, 128>>>(thrust::raw_pointer_cast(grid.dAllTiles.data()), c, thrust::raw_pointer_cast(d.data()));
+    thrust::copy(d.begin(), d.end(), data);
+}
+// RHS exactly as FluidEuler::project builds it (src/FluidEuler.h:583-586), after the
+// velocity boundary step's face clearing (src/FluidEuler.cu:43-60).
+void ref_rhs(void* h) {
+    auto& grid = *((RefGrid*)h)->g;
+    grid.launchVoxelFunc(
+        [=] __device__(HATileAccessor<Tile>& acc, HATileInfo<Tile>& info, const Coord& l_ijk) {
+            for (int axis : {0, 1, 2}) {
+                bool to_set = false;
+                IterateFaceNeighborCellTypes(acc, info, l_ijk, axis, [&](const uint8_t type0, const uint8_t type1) {
+                    if ((type0 & NEUMANN) || (type1 & NEUMANN) || ((type0 & DIRICHLET) && (type1 & DIRICHLET))) to_set = true;
+                });
+                if (to_set) info.tile()(Tile::u_channel + axis, l_ijk) = 0;
+            }
+        },
+        -1, LEAF, LAUNCH_SUBTREE);
+    for (int axis : {0, 1, 2})
+        PropagateToChildren(grid, Tile::u_channel + axis, Tile::u_channel + axis, -1, GHOST, LAUNCH_SUBTREE, INTERIOR | DIRICHLET | NEUMANN);
+    VelocityVolumeDivergenceOnLeafs(grid, Tile::u_channel, Tile::b_channel);
+    cudaDeviceSynchronize();
+}
+void ref_full_lap(void* h, int xc, int yc) {
+    FullNegativeLaplacian(*((RefGrid*)h)->g, xc, yc, false);
+    cudaDeviceSynchronize();
+}
+void ref_gs_sweep(void* h, int level, int xc, int rc, int color) {
+    auto& grid = *((RefGrid*)h)->g;
+    NegativeLaplacianAndGaussSeidelSameLevel128(grid, grid.dTileArrays[level], grid.hNumTiles[level], level, LEAF | NONLEAF, xc, rc, color);
+    cudaDeviceSynchronize();
+}
+void ref_residual_restrict(void* h, int level, int xc, int rhsc, int coarsec) {
+    ResidualAndRestrict(*((RefGrid*)h)->g, xc, rhsc, coarsec, level, LEAF | NONLEAF | GHOST, (T)1);
+    cudaDeviceSynchronize();
+}
+void ref_prolongate(void* h, int level, int cxc, int fxc) {
+    ProlongateAndUpdate128(*((RefGrid*)h)->g, cxc, fxc, level, (T)1);
+    cudaDeviceSynchronize();
+}
+void ref_vcycle(void* h, int xc, int fc, int rhsc, int level_iters, int coarsest_iters) {
+    RefGrid* r = (RefGrid*)h;
+    if (!r->solver) r->solver = std::make_unique<GMGSolver>(1., 1.);
+    r->solver->VCycle(*r->g, xc, fc, rhsc, level_iters, coarsest_iters);
+    cudaDeviceSynchronize();
+}
+double ref_dot(void* h, int a, int b) { return Dot(*((RefGrid*)h)->g, a, b, LEAF); }
+// GMGSolver::solve as FluidEuler::project calls it; returns iterations, writes the relative
+// residual and the wall time of the call bracketed by device synchronisation (ms).
+int ref_solve(void* h, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann,
+              double* rel, double* ms) {
+    RefGrid* r = (RefGrid*)h;
+    if (!r->solver) r->solver = std::make_unique<GMGSolver>(1., 1.);
+    cudaDeviceSynchronize();
+    auto t0 = std::chrono::high_resolution_clock::now();
+    auto [iters, err] = r->solver->solve(*r->g, false, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0);
+    cudaDeviceSynchronize();
+    auto t1 = std::chrono::high_resolution_clock::now();
+    if (rel) *rel = err;
+    if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return iters;
+}
+int ref_last_error() { return (int)cudaGetLastError(); }
+
+}  // extern "C"

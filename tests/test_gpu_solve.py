@@ -1,0 +1,143 @@
+"""GMG-PCG solve on the GPU against the CPU oracle: same stopping rule, iteration count within
+one, pressure within 1e-5 relative L2 of the FP32 mirror; the error against the FP64 oracle is
+stated; mixed precision reaches 1e-8 relative FP64 residual."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from cirrus_b200 import DeviceGrid, GMGSolver, PRECISION_MIXED_FP64, workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL_X = 1e-5        # relative L2 of the pressure against the reference arithmetic
+NAMES = ["uniform32_small", "sphere64_small", "ring64_small"]
+
+
+def grid_with_rhs(b):
+    g = DeviceGrid(b.topology)
+    for a in range(3):
+        g.set_channel(6 + a, b.velocity[a])
+    g.projection_rhs()
+    return g
+
+
+def rel_l2(a, ref, mask):
+    a = a[mask].astype(np.float64)
+    r = ref[mask].astype(np.float64)
+    return float(np.linalg.norm(a - r) / max(np.linalg.norm(r), 1e-300))
+
+
+def oracle_solution(b, rhs, prec=O.CpuOracle.FP32, tol=1e-6, pure=False):
+    f = O.CpuOracle(b.tiles)
+    f.set_ctypes(b.ctypes)
+    if prec == O.CpuOracle.FP32:
+        f.set_channel_f32(1, rhs)
+        it, rel, _ = f.solve(prec, 1000, tol, pure_neumann=pure)
+        return it, rel, f.get_channel_f32(0)
+    f.set_channel(prec, 1, rhs.astype(np.float64))
+    it, rel, _ = f.solve(prec, 1000, tol, pure_neumann=pure)
+    return it, rel, f.get_channel(prec, 0)
+
+
+@pytest.mark.parametrize("name", NAMES + ["sphere64_neumann_small"])
+def test_solve_matches_oracle(name, built_cache):
+    b = built_cache(name)
+    g = grid_with_rhs(b)
+    rhs = g.get_channel(1)
+    pure = b.workload.pure_neumann
+    it, rel = GMGSolver().solve(g, False, 1000, 1e-6, 1, 10, 1, pure)
+    x = g.get_channel(0)
+    oit, orel, ox = oracle_solution(b, rhs, pure=pure)
+    leaf = (b.tiles[:, 4] & W.LEAF) != 0
+    assert rel < 1e-6 and orel < 1e-6
+    assert abs(it - oit) <= 1
+    assert rel_l2(x, ox, leaf) <= TOL_X
+
+
+@pytest.mark.parametrize("name", ["uniform128", "sphere256", "ring512"])
+def test_solve_full_size_against_fp64_oracle(name, built_cache):
+    b = built_cache(name)
+    g = grid_with_rhs(b)
+    rhs = g.get_channel(1)
+    it, rel = GMGSolver().solve(g)
+    x = g.get_channel(0)
+    assert rel < 1e-6 and 0 < it < 200
+    true_rel = g.true_residual(rhs)
+    assert true_rel < 5e-6
+    _, rel64, x64 = oracle_solution(b, rhs, O.CpuOracle.FP64, tol=1e-10)
+    err = rel_l2(x, x64, (b.tiles[:, 4] & W.LEAF) != 0)
+    print(f"{name}: iters {it} rel {rel:.3e} true {true_rel:.3e} err_vs_fp64 {err:.3e}")
+    assert err < 1e-4
+
+
+def test_graph_and_direct_launch_agree(built_cache):
+    b = built_cache("sphere64_small")
+    g = grid_with_rhs(b)
+    rhs = g.get_channel(1)
+    it1, rel1 = GMGSolver().solve(g)
+    x1 = g.get_channel(0)
+    g.set_channel(1, rhs)
+    os.environ["CIRRUS_NO_GRAPH"] = "1"
+    try:
+        it2, rel2 = GMGSolver().solve(g)
+    finally:
+        del os.environ["CIRRUS_NO_GRAPH"]
+    x2 = g.get_channel(0)
+    assert it1 == it2 and rel1 == rel2
+    assert np.array_equal(x1.view(np.uint32), x2.view(np.uint32))
+
+
+def test_repeat_solves_are_deterministic(built_cache):
+    b = built_cache("ring64_small")
+    g = grid_with_rhs(b)
+    rhs = g.get_channel(1)
+    res = []
+    for _ in range(3):
+        g.set_channel(1, rhs)
+        it, rel = GMGSolver().solve(g)
+        res.append((it, rel, g.get_channel(0).tobytes()))
+    assert res[0] == res[1] == res[2]
+
+
+def test_mixed_precision_reaches_1e8(built_cache):
+    b = built_cache("sphere64_small")
+    g = grid_with_rhs(b)
+    rhs = g.get_channel(1)
+    s = GMGSolver(precision=PRECISION_MIXED_FP64)
+    it, rel = s.solve(g, relative_tolerance=1e-8)
+    assert s.last_result.status == 0
+    assert rel < 1e-8
+    true_rel = g.true_residual(rhs)
+    assert true_rel < 2e-8
+    _, _, x64 = oracle_solution(b, rhs, O.CpuOracle.FP64, tol=1e-11)
+    err = rel_l2(g.get_channel(0), x64, (b.tiles[:, 4] & W.LEAF) != 0)
+    assert err < 1e-6, err
+
+
+def test_zero_rhs_and_iteration_cap(built_cache):
+    b = built_cache("uniform32_small")
+    g = DeviceGrid(b.topology)
+    g.set_channel(1, np.zeros((b.n, 512), np.float32))
+    s = GMGSolver()
+    assert s.solve(g) == (0, 0.0)
+    assert s.last_result.status == 0
+    g2 = grid_with_rhs(b)
+    it, rel = s.solve(g2, max_iters=2)
+    assert it == 2 and rel > 1e-6
+    assert s.last_result.status == 5  # CIRRUS_ERR_NOT_CONVERGED reported in the result
+
+
+def test_solve_host_end_to_end(built_cache):
+    b = built_cache("sphere64_small")
+    g = grid_with_rhs(b)
+    rhs = g.get_channel(1).copy()
+    x = np.zeros_like(rhs)
+    it, rel = GMGSolver().solve_host(g, rhs, x)
+    g2 = grid_with_rhs(b)
+    it2, rel2 = GMGSolver().solve(g2)
+    assert (it, rel) == (it2, rel2)
+    assert np.array_equal(x.view(np.uint32), g2.get_channel(0).view(np.uint32))

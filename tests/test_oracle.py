@@ -1,0 +1,108 @@
+"""The CPU oracle pinned against the reference's own outputs (golden fixtures produced by the
+reference CUDA build on a B200), plus its own consistency: FP32 mirror vs FP64 restatement."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_npz
+from cirrus_b200 import workloads as W
+from oracle import oracle as O
+
+SMALL = ["uniform32_small", "sphere64_small", "sphere64_neumann_small", "ring64_small"]
+
+
+def oracle_for(b):
+    f = O.CpuOracle(b.tiles)
+    f.set_ctypes(b.ctypes)
+    return f
+
+
+def leaf_mask(b):
+    return (b.tiles[:, 4] & W.LEAF) != 0
+
+
+def rel_l2(a, ref, mask):
+    a = a[mask].astype(np.float64)
+    r = ref[mask].astype(np.float64)
+    return float(np.linalg.norm(a - r) / max(np.linalg.norm(r), 1e-300))
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_rhs_matches_reference_bitwise(name, built_cache):
+    g = golden_npz(name)
+    b = built_cache(name)
+    rhs = oracle_for(b).rhs(b.velocity)
+    assert np.array_equal(rhs.view(np.uint32), g["b"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_laplacian_matches_reference(name, built_cache):
+    """FullNegativeLaplacian of b: bit-exact with the reference build."""
+    g = golden_npz(name)
+    b = built_cache(name)
+    f = oracle_for(b)
+    f.set_channel_f32(2, g["b"])
+    f.full_lap(O.CpuOracle.FP32, 2, 3)
+    ap = f.get_channel_f32(3)
+    lg = (b.tiles[:, 4] & (W.LEAF | W.GHOST)) != 0
+    assert np.array_equal(ap[lg].view(np.uint32), g["ap"][lg].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_vcycle_matches_reference(name, built_cache):
+    g = golden_npz(name)
+    b = built_cache(name)
+    f = oracle_for(b)
+    f.set_channel_f32(1, g["b"])
+    f.vcycle(O.CpuOracle.FP32, 4, 1, 3, 1, 10)
+    z = f.get_channel_f32(4)
+    m = leaf_mask(b)
+    assert rel_l2(z, g["z"], m) <= 1e-6
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_solve_matches_reference(name, built_cache):
+    g = golden_npz(name)
+    b = built_cache(name)
+    f = oracle_for(b)
+    f.set_channel_f32(1, g["b"])
+    it, rel, _ = f.solve(O.CpuOracle.FP32, 1000, 1e-6, 1, 10, 1, b.workload.pure_neumann)
+    assert abs(it - int(g["iters"])) <= 1
+    assert rel < 1e-6
+    x = f.get_channel_f32(0)
+    assert rel_l2(x, g["x"], leaf_mask(b)) <= 1e-5
+
+
+@pytest.mark.parametrize("name", ["uniform32_small", "sphere64_small", "ring64_small"])
+def test_fp32_mirror_against_fp64(name, built_cache):
+    """The FP32 mirror converges like the FP64 restatement; its pressure error is stated."""
+    b = built_cache(name)
+    f = oracle_for(b)
+    rhs = f.rhs(b.velocity)
+    f.set_channel_f32(1, rhs)
+    it32, rel32, hist = f.solve(O.CpuOracle.FP32, 1000, 1e-6)
+    x32 = f.get_channel_f32(0)
+    f.set_channel(O.CpuOracle.FP64, 1, rhs.astype(np.float64))
+    it64, rel64, _ = f.solve(O.CpuOracle.FP64, 1000, 1e-10)
+    x64 = f.get_channel(O.CpuOracle.FP64, 0)
+    assert rel32 < 1e-6 and rel64 < 1e-10
+    assert np.all(np.diff(hist) < 0.5 * hist[:-1] + 1e-12) or len(hist) < 3
+    err = rel_l2(x32, x64, leaf_mask(b))
+    assert err < 1e-4, err
+
+
+def test_zero_rhs_returns_immediately(built_cache):
+    b = built_cache("uniform32_small")
+    f = oracle_for(b)
+    f.set_channel_f32(1, np.zeros((b.n, 512), np.float32))
+    it, rel, _ = f.solve(O.CpuOracle.FP32)
+    assert it == 0 and rel == 0.0
+
+
+def test_pure_neumann_converges(built_cache):
+    b = built_cache("sphere64_neumann_small")
+    f = oracle_for(b)
+    f.set_channel_f32(1, f.rhs(b.velocity))
+    it, rel, _ = f.solve(O.CpuOracle.FP32, 1000, 1e-6, pure_neumann=True)
+    assert rel < 1e-6 and it < 200
