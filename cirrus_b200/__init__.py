@@ -199,6 +199,9 @@ class DeviceGrid:
         check(lib().cirrus_grid_get_channel(self._h, channel, _ptr(out, C.c_float), C.c_void_p(stream)), "cirrus_grid_get_channel")
         return out
 
+    def copy_channel(self, dst_channel: int, src_channel: int, stream: int = 0) -> None:
+        check(lib().cirrus_grid_copy_channel(self._h, dst_channel, src_channel, C.c_void_p(stream)), "cirrus_grid_copy_channel")
+
     def channel_ptr(self, channel: int) -> int:
         p = C.c_void_p()
         check(lib().cirrus_grid_channel_ptr(self._h, channel, C.byref(p)), "cirrus_grid_channel_ptr")
@@ -253,6 +256,13 @@ class DeviceGrid:
             self.propagate_to_children(U_CHANNEL + a, stream)
         self.velocity_volume_divergence_on_leafs(U_CHANNEL, B_CHANNEL, stream)
 
+    def solution_f64(self, stream: int = 0) -> np.ndarray:
+        """The last solution in FP64 (the FP64 iterate after a mixed-precision solve)."""
+        out = np.empty((self.num_tiles, 512), dtype=np.float64)
+        check(lib().cirrus_grid_get_solution_f64(self._h, _ptr(out, C.c_double), C.c_void_p(stream)),
+              "cirrus_grid_get_solution_f64")
+        return out
+
     def true_residual(self, b: np.ndarray, stream: int = 0) -> float:
         a = np.ascontiguousarray(b, dtype=np.float32).reshape(self.num_tiles * 512)
         r = C.c_double()
@@ -264,7 +274,7 @@ class GMGSolver:
     """Geometric-multigrid-preconditioned CG (the reference's GMGSolver, src/GMGSolver.h:17-52)."""
 
     def __init__(self, one_over_alpha: float = 1.0, prolong_coeff: float = 1.0, precision: int = PRECISION_FP32,
-                 inner_tolerance: float = 1e-3, max_outer_iters: int = 20, warm_start: bool = False):
+                 inner_tolerance: float = 1e-5, max_outer_iters: int = 20, warm_start: bool = False):
         self.one_over_alpha = one_over_alpha
         self.prolong_coeff = prolong_coeff
         self.precision = precision

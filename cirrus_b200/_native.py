@@ -59,6 +59,7 @@ class SolveResult(C.Structure):
         ("rel_residual", C.c_double),
         ("true_rel_residual", C.c_double),
         ("status", C.c_int),
+        ("kernel_launches", C.c_longlong),
     ]
 
 
@@ -90,6 +91,7 @@ _PROTOS = {
     "cirrus_grid_set_channel": (C.c_int, [C.c_void_p, C.c_int, c_f32_p, C.c_void_p]),
     "cirrus_grid_get_channel": (C.c_int, [C.c_void_p, C.c_int, c_f32_p, C.c_void_p]),
     "cirrus_grid_channel_ptr": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "cirrus_grid_copy_channel": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_full_negative_laplacian": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_gauss_seidel_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_residual_and_restrict": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
@@ -103,6 +105,7 @@ _PROTOS = {
     "cirrus_gmg_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveResult)]),
     "cirrus_gmg_solve_host": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p, C.POINTER(SolveResult)]),
     "cirrus_true_residual": (C.c_int, [C.c_void_p, c_f32_p, c_f64_p, C.c_void_p]),
+    "cirrus_grid_get_solution_f64": (C.c_int, [C.c_void_p, c_f64_p, C.c_void_p]),
 }
 
 

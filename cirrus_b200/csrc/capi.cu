@@ -247,6 +247,15 @@ cirrus_status cirrus_grid_get_channel(const cirrus_grid* grid, int channel, floa
     if (cudaMemcpyAsync(host, grid->g->d_ch[channel], bytes, cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess) return cuda_status();
     return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
 }
+cirrus_status cirrus_grid_copy_channel(cirrus_grid* grid, int dst_channel, int src_channel, void* stream) {
+    if (!grid || !channel_ok(dst_channel) || !channel_ok(src_channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (dst_channel == src_channel) return CIRRUS_OK;
+    const size_t bytes = (size_t)grid->g->n * cirrus::kTileCells * sizeof(float);
+    if (cudaMemcpyAsync(grid->g->d_ch[dst_channel], grid->g->d_ch[src_channel], bytes, cudaMemcpyDeviceToDevice, S(stream)) !=
+        cudaSuccess)
+        return cuda_status();
+    return CIRRUS_OK;
+}
 cirrus_status cirrus_grid_channel_ptr(cirrus_grid* grid, int channel, float** device_ptr) {
     if (!grid || !device_ptr || !channel_ok(channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
     *device_ptr = grid->g->d_ch[channel];
@@ -336,7 +345,7 @@ void cirrus_solve_params_default(cirrus_solve_params* p) {
     p->prolong_coeff = 1.f;
     p->precision = CIRRUS_PRECISION_FP32;
     p->warm_start = 0;
-    p->inner_tolerance = 1e-3;
+    p->inner_tolerance = 1e-5;
     p->max_outer_iters = 20;
 }
 
@@ -346,6 +355,7 @@ cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* par
         cirrus::SolveParams p;
         to_internal(params, &p);
         cirrus::SolveResult r;
+        if (p.precision != CIRRUS_PRECISION_MIXED_FP64) grid->g->x64_valid = false;
         int rc = p.precision == CIRRUS_PRECISION_MIXED_FP64 ? cirrus::mixed_solve(*grid->g, p, S(stream), &r)
                                                             : cirrus::pcg_solve(*grid->g, p, S(stream), &r);
         if (rc) return map_rc(rc);
@@ -354,6 +364,7 @@ cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* par
         result->rel_residual = r.rel;
         result->true_rel_residual = r.true_rel;
         result->status = (int)map_rc(r.status);
+        result->kernel_launches = r.launches;
         return CIRRUS_OK;
     });
 }
@@ -368,6 +379,11 @@ cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params
     if (st != CIRRUS_OK) return st;
     if (cudaMemcpyAsync(x_host, g.d_ch[cirrus::kChX], bytes, cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess) return cuda_status();
     return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
+}
+
+cirrus_status cirrus_grid_get_solution_f64(cirrus_grid* grid, double* host, void* stream) {
+    if (!grid || !host) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return map_rc(cirrus::solution_f64(*grid->g, host, S(stream))); });
 }
 
 cirrus_status cirrus_true_residual(cirrus_grid* grid, const float* b_host, double* rel, void* stream) {

@@ -212,7 +212,7 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
 
 void grid_destroy(DevGrid* g) {
     if (!g) return;
-    for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second.exec);
     cudaFree(g->d_chbuf);
     cudaFree(g->d_u8);
     cudaFree(g->d_meta);

@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __r
     const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_lap + (size_t)tile * kTileCells + t * 4);
     const LevelConst<T> L((T)tp.h0, meta_level(m.packed));
     T out[4], dg[4];
-    neg_lap4<T, false>(sh[g].xs, sh[g].hx, t, mask4, tp.fcls[tile] & 0xfffu, L, out, dg);
+    neg_lap4<T, false, false>(sh[g].xs, sh[g].hx, t, mask4, tp.fcls[tile] & 0xfffu, L, out, dg);
     V4<T> o;
     o.v[0] = out[0]; o.v[1] = out[1]; o.v[2] = out[2]; o.v[3] = out[3];
     st4(Y + (size_t)tile * kTileCells + t * 4, o);
@@ -567,16 +567,19 @@ constexpr int kTPB = 2;  // tiles per CTA of the stencil kernels
 template <class T>
 void propagate_ghosts(const DevGrid& g, T* X, const int* done, cudaStream_t s) {
     if (g.n_ghost == 0) return;
+    ++g.launch_count;
     k_propagate_ghosts<T><<<g.n_ghost, 128, 0, s>>>(g.topo, g.d_ghost, g.n_ghost, X, done);
 }
 template <class T>
 void laplacian_tiles(const DevGrid& g, const T* X, T* Y, const int* done, cudaStream_t s) {
     if (g.n_leafghost == 0) return;
+    ++g.launch_count;
     k_laplacian<T, kTPB><<<(g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.d_leafghost, g.n_leafghost, X, Y, done);
 }
 template <class T>
 void accumulate_ghosts(const DevGrid& g, T* Y, const int* done, cudaStream_t s) {
     if (g.n_ghost == 0) return;
+    ++g.launch_count;
     k_accumulate_ghosts<T><<<g.n_ghost, 64, 0, s>>>(g.topo, g.d_ghost, g.n_ghost, Y, done);
 }
 template <class T>
@@ -591,6 +594,7 @@ template void full_laplacian<double>(const DevGrid&, double*, double*, const int
 void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const int* done, cudaStream_t s) {
     const int n = g.mg_count[level];
     if (n == 0) return;
+    ++g.launch_count;
     k_gs_sweep<kTPB><<<(n + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.d_mg + g.mg_offset[level], n, X, R, color, done);
 }
 
@@ -599,6 +603,7 @@ void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t
     const int n = g.mg_count[level];
     if (n == 0 || nsweeps == 0) return;
     if (n <= 8) {
+        ++g.launch_count;
         k_gs_sequence<<<1, 128 * n, 0, s>>>(g.topo, g.d_mg + g.mg_offset[level], n, X, R, colors, nsweeps, done);
         return;
     }
@@ -609,6 +614,7 @@ void residual_restrict(const DevGrid& g, int level, const float* X, const float*
                        const int* done, cudaStream_t s) {
     const int n = g.level_count[level];
     if (n == 0) return;
+    ++g.launch_count;
     k_residual_restrict<kTPB><<<(n + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.level_first[level], n, X, RHS, C,
                                                                             one_over_alpha, done);
 }
@@ -617,6 +623,7 @@ void prolongate(const DevGrid& g, int level, const float* CX, float* FX, float p
                 cudaStream_t s) {
     const int n = g.level_count[level];
     if (n == 0) return;
+    ++g.launch_count;
     k_prolongate<<<n, 128, 0, s>>>(g.topo, g.level_first[level], n, CX, FX, prolong_coeff, done);
 }
 
@@ -624,6 +631,7 @@ void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const i
     const size_t nv = (size_t)g.n * 128;
     int blocks = (int)std::min<size_t>((nv + 255) / 256, (size_t)g.sm_count * 8);
     if (blocks < 1) blocks = 1;
+    ++g.launch_count;
     k_vcycle_init<<<blocks, 256, 0, s>>>(g.topo, g.n, X, RHS, F, done);
 }
 
@@ -634,44 +642,56 @@ void leaf_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* 
     const int blocks = leaf_blocks(g);
     switch (op) {
     case OP_DOT:
+        ++g.launch_count;
         k_leaf_reduce<OP_DOT><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
         break;
     case OP_INIT:
+        ++g.launch_count;
         k_leaf_reduce<OP_INIT><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
         break;
     case OP_COPY_DOT:
+        ++g.launch_count;
         k_leaf_reduce<OP_COPY_DOT><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
         break;
     case OP_XR:
+        ++g.launch_count;
         k_leaf_reduce<OP_XR><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
         break;
     case OP_MEAN:
+        ++g.launch_count;
         k_leaf_reduce<OP_MEAN><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
         break;
     }
 }
 
 void update_p(const DevGrid& g, float* P, const float* Z, const Scalars* S, cudaStream_t s) {
+    ++g.launch_count;
     k_update_p<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, P, Z, S);
 }
 
 void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cudaStream_t s) {
+    ++g.launch_count;
     k_recenter<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, R, S, skip_if_done);
 }
 
 void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s) {
+    ++g.launch_count;
     k_residual64<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, B, AX, R64, R32);
 }
 void accumulate_correction(const DevGrid& g, double* X64, float* E, cudaStream_t s) {
+    ++g.launch_count;
     k_accumulate_correction<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, X64, E);
 }
 void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s) {
+    ++g.launch_count;
     k_norm64<<<leaf_blocks(g), 256, 0, s>>>(g.d_leaf, g.n_leaf, A, B32, g.d_partials, g.d_counter, out);
 }
-void widen(const float* a, double* b, size_t n, cudaStream_t s) {
+void widen(const DevGrid& g, const float* a, double* b, size_t n, cudaStream_t s) {
+    ++g.launch_count;
     k_widen<<<(int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(a, b, n);
 }
-void narrow(const double* a, float* b, size_t n, cudaStream_t s) {
+void narrow(const DevGrid& g, const double* a, float* b, size_t n, cudaStream_t s) {
+    ++g.launch_count;
     k_narrow<<<(int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(a, b, n);
 }
 

@@ -8,16 +8,13 @@
 // Arithmetic mirrors the reference operation by operation so results agree bit for bit:
 //   coefficient  NegativeLaplacianCoeff          src/GMGSolver.cu:12-40
 //   stencil sum  GMGLaplacianTileData::negativeLap src/GMGSolver.cu:56-76 (face order x-,x+,
-//                y-,y+,z-,z+; a*b+c contracted to one fused multiply-add as nvcc does)
+//                y-,y+,z-,z+; fused multiply-add in the smoother and residual kernels,
+//                product-then-sum in the Laplacian apply, as the reference's build rounds them)
 #pragma once
 
 #include "common.cuh"
 
 namespace cirrus {
-
-#ifndef CIRRUS_LAP_FMA
-#define CIRRUS_LAP_FMA 1
-#endif
 
 template <class T> struct alignas(4 * sizeof(T)) V4 { T v[4]; };
 
@@ -25,12 +22,15 @@ template <class T> __device__ __forceinline__ V4<T> ld4(const T* p) { return *re
 template <class T> __device__ __forceinline__ void st4(T* p, const V4<T>& v) { *reinterpret_cast<V4<T>*>(p) = v; }
 template <class T> __device__ __forceinline__ V4<T> zero4() { V4<T> r; r.v[0] = r.v[1] = r.v[2] = r.v[3] = T(0); return r; }
 
-template <class T> __device__ __forceinline__ T fmadd(T a, T b, T c) {
-#if CIRRUS_LAP_FMA
-    return fma(a, b, c);
-#else
-    return a * b + c;
-#endif
+// sum + a*b.  FUSED: one rounding (fused multiply-add); otherwise the product is rounded, then
+// the sum, with intrinsics the compiler may not contract.  The reference's build fuses the
+// stencil sum in its Gauss-Seidel and residual kernels (negativeLap inlined with a literal
+// `diag`) but not in NegativeLaplacianSameLevel128Kernel, whose calc_diag is a runtime value.
+template <bool FUSED> __device__ __forceinline__ float fmadd(float a, float b, float c) {
+    return FUSED ? fmaf(a, b, c) : __fadd_rn(c, __fmul_rn(a, b));
+}
+template <bool FUSED> __device__ __forceinline__ double fmadd(double a, double b, double c) {
+    return FUSED ? fma(a, b, c) : __dadd_rn(c, __dmul_rn(a, b));
 }
 
 // Per-level constants of the stencil.  h = h0 / 2^level (src/HAAccessor.h:72-74); c1 = 1/h^2;
@@ -79,8 +79,9 @@ __device__ __forceinline__ void load_halo(const T* __restrict__ X, const TileMet
 
 // Negative Laplacian of the four cells of thread t, times h^3, for INTERIOR cells (0 elsewhere).
 // xs = tile values in shared memory (512), hx = halos, mask4 = the four mask bytes, cls = the
-// 12-bit cross-face class field of the context.  DIAG additionally returns the diagonal.
-template <class T, bool DIAG>
+// 12-bit cross-face class field of the context.  DIAG additionally returns the diagonal;
+// FUSED selects the rounding of the stencil sum (see fmadd).
+template <class T, bool DIAG, bool FUSED = true>
 __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32_t mask4, uint32_t cls,
                                          const LevelConst<T>& L, T out[4], T diag[4]) {
     const TileIdx ix(t);
@@ -111,12 +112,12 @@ __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32
         const T a4 = (m & 16u) ? (k == 0 ? czlo : L.c1) : T(0);
         const T a5 = (m & 32u) ? (k == 7 ? czhi : L.c1) : T(0);
         T s = T(0);
-        s = fmadd(a0, x0 - xm.v[e], s);
-        s = fmadd(a1, x0 - xp.v[e], s);
-        s = fmadd(a2, x0 - ym.v[e], s);
-        s = fmadd(a3, x0 - yp.v[e], s);
-        s = fmadd(a4, x0 - zl, s);
-        s = fmadd(a5, x0 - zr, s);
+        s = fmadd<FUSED>(a0, x0 - xm.v[e], s);
+        s = fmadd<FUSED>(a1, x0 - xp.v[e], s);
+        s = fmadd<FUSED>(a2, x0 - ym.v[e], s);
+        s = fmadd<FUSED>(a3, x0 - yp.v[e], s);
+        s = fmadd<FUSED>(a4, x0 - zl, s);
+        s = fmadd<FUSED>(a5, x0 - zr, s);
         const bool interior = m & kMaskInterior;
         out[e] = interior ? s * L.h * L.h * L.h : T(0);
         if (DIAG) {

@@ -169,19 +169,23 @@ namespace launch {
 
 void clear_neumann_faces(const DevGrid& g, int u_channel, cudaStream_t s) {
     if (g.n_leaf == 0) return;
+    ++g.launch_count;
     k_clear_faces<<<g.n_leaf, 128, 0, s>>>(g.topo, g.d_child, g.d_leaf, g.n_leaf, g.d_ch[u_channel], g.d_ch[u_channel + 1],
                                           g.d_ch[u_channel + 2]);
 }
 
 void propagate_to_children(const DevGrid& g, int channel, cudaStream_t s) {
     if (g.n_ghost == 0) return;
+    ++g.launch_count;
     k_propagate_children<<<g.n_ghost, 128, 0, s>>>(g.topo, g.d_ghost, g.n_ghost, g.d_ch[channel]);
 }
 
 void velocity_divergence(const DevGrid& g, int u_channel, int b_channel, cudaStream_t s) {
     if (g.n_leafghost == 0) return;
+    ++g.launch_count;
     k_divergence<<<g.n_leafghost, 128, 0, s>>>(g.topo, g.d_leafghost, g.n_leafghost, g.d_ch[u_channel], g.d_ch[u_channel + 1],
                                               g.d_ch[u_channel + 2], g.d_ch[b_channel]);
+    ++g.launch_count;
     k_accumulate_children<<<g.n_leaf, 128, 0, s>>>(g.topo, g.d_child, g.d_leaf, g.n_leaf, g.d_ch[b_channel]);
 }
 

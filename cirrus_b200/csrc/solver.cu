@@ -129,12 +129,13 @@ bool graphs_enabled() {
     } while (0)
 
 // Build the whole solve as one graph: prologue -> while(cond){ body } -> epilogue.
-cudaGraphExec_t build_graph(DevGrid& g, const SolveParams& p) {
+DevGrid::SolveGraph build_graph(DevGrid& g, const SolveParams& p) {
     bool ok = true;
+    DevGrid::SolveGraph out;
     cudaStream_t cs = nullptr, cs2 = nullptr;
     GK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     GK(cudaStreamCreateWithFlags(&cs2, cudaStreamNonBlocking));
-    if (!ok) return nullptr;
+    if (!ok) return out;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     GK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
@@ -145,7 +146,9 @@ cudaGraphExec_t build_graph(DevGrid& g, const SolveParams& p) {
     SolveCtl ctl = make_ctl(g, p);
     ctl.use_cond = 1;
     ctl.cond = handle;
+    long long c0 = g.launch_count;
     record_prologue(g, p, ctl, cs);
+    out.prologue = g.launch_count - c0;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
     GK(cudaStreamGetCaptureInfo(cs, &st, nullptr, &graph, &deps, &ndeps));
@@ -159,11 +162,15 @@ cudaGraphExec_t build_graph(DevGrid& g, const SolveParams& p) {
     if (ok) {
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         GK(cudaStreamBeginCaptureToGraph(cs2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        c0 = g.launch_count;
         record_body(g, p, ctl, cs2);
+        out.body = g.launch_count - c0;
         GK(cudaStreamEndCapture(cs2, &body));
         GK(cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies));
     }
+    c0 = g.launch_count;
     record_epilogue(g, ctl, cs);
+    out.epilogue = g.launch_count - c0;
     cudaGraph_t outg = nullptr;
     cudaError_t ee = cudaStreamEndCapture(cs, &outg);
     if (ee != cudaSuccess) {
@@ -177,9 +184,10 @@ cudaGraphExec_t build_graph(DevGrid& g, const SolveParams& p) {
     if (!ok) {
         cudaGetLastError();
         if (exec) cudaGraphExecDestroy(exec);
-        return nullptr;
+        return DevGrid::SolveGraph();
     }
-    return exec;
+    out.exec = exec;
+    return out;
 }
 
 void fill_result(const DevGrid& g, SolveResult* r) {
@@ -193,23 +201,25 @@ void fill_result(const DevGrid& g, SolveResult* r) {
 
 int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r) {
     GraphKey key{p.max_iters, p.level_iters, p.coarsest_iters, p.sync_stride, p.pure_neumann, p.tol, p.one_over_alpha, p.prolong_coeff};
-    cudaGraphExec_t exec = nullptr;
+    DevGrid::SolveGraph sg;
     if (graphs_enabled()) {
         auto it = g.graphs.find(key);
-        if (it != g.graphs.end()) exec = it->second;
+        if (it != g.graphs.end()) sg = it->second;
         else {
-            exec = build_graph(g, p);
-            if (exec) g.graphs[key] = exec;
+            sg = build_graph(g, p);
+            if (sg.exec) g.graphs[key] = sg;
         }
     }
-    if (exec) {
-        cudaError_t e = cudaGraphLaunch(exec, s);
+    long long direct = -1;
+    if (sg.exec) {
+        cudaError_t e = cudaGraphLaunch(sg.exec, s);
         if (e != cudaSuccess) {
             g.last_error = std::string("cudaGraphLaunch: ") + cudaGetErrorString(e);
             return 2;
         }
     } else {
         // Direct launches with a host-checked loop (the reference's sync_stride behaviour).
+        const long long c0 = g.launch_count;
         SolveCtl ctl = make_ctl(g, p);
         record_prologue(g, p, ctl, s);
         for (int i = 0; i < p.max_iters; i++) {
@@ -219,6 +229,7 @@ int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r) 
             record_body(g, p, ctl, s);
         }
         record_epilogue(g, ctl, s);
+        direct = g.launch_count - c0;
     }
     cudaMemcpyAsync(g.h_scalars, g.d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
@@ -227,6 +238,9 @@ int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r) 
         return 2;
     }
     fill_result(g, r);
+    // bodies executed = iterations entered (the counter is advanced once per body)
+    g.last_solve_launches = direct >= 0 ? direct : sg.prologue + (long long)g.h_scalars->iter * sg.body + sg.epilogue;
+    r->launches = g.last_solve_launches;
     if (p.sync_stride <= 0) r->status = 0;
     return 0;
 }
@@ -259,7 +273,7 @@ int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s) {
     const size_t cells = (size_t)g.n * kTileCells;
     launch::norm64(g, nullptr, d_b, g.d_norm, s);
     const double bb = read_norm(g, s);
-    launch::widen(g.d_ch[kChX], g.d_x64, cells, s);
+    if (!g.x64_valid) launch::widen(g, g.d_ch[kChX], g.d_x64, cells, s);
     launch::full_laplacian<double>(g, g.d_x64, g.d_ax64, nullptr, s);
     launch::residual64(g, d_b, g.d_ax64, g.d_r64, g.d_bsave, s);
     launch::norm64(g, g.d_r64, nullptr, g.d_norm, s);
@@ -274,8 +288,10 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
     int rc = ensure_fp64(g);
     if (rc) return rc;
     const size_t cells = (size_t)g.n * kTileCells;
+    const long long own0 = g.launch_count;
+    long long inner_recorded = 0, inner_executed = 0;
     cudaMemcpyAsync(g.d_bsave, g.d_ch[kChB], cells * sizeof(float), cudaMemcpyDeviceToDevice, s);
-    if (p.warm_start) launch::widen(g.d_ch[kChX], g.d_x64, cells, s);
+    if (p.warm_start) launch::widen(g, g.d_ch[kChX], g.d_x64, cells, s);
     else cudaMemsetAsync(g.d_x64, 0, cells * sizeof(double), s);
     launch::norm64(g, nullptr, g.d_bsave, g.d_norm, s);
     const double bb = read_norm(g, s);
@@ -286,6 +302,7 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
         r->rel = 0;
         r->true_rel = 0;
         r->status = 0;
+        r->launches = g.launch_count - own0;
         return cudaStreamSynchronize(s) == cudaSuccess ? 0 : 2;
     }
     double rel = 1.0;
@@ -298,22 +315,39 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
         if (!(rel == rel)) { r->status = 6; break; }
         if (rel < p.tol) { r->status = 0; break; }
         if (k == p.max_outer) break;
+        // each inner FP32 solve targets the defect that leaves the outer residual just under
+        // tol, but never tighter than inner_tol (where FP32 stalls) nor looser than 0.1
         SolveParams ip = p;
         ip.precision = 0;
         double tau = 0.5 * p.tol / rel;
-        tau = std::min(0.1, std::max(1e-5, tau));
+        tau = std::min(0.1, std::max(p.inner_tol, tau));
         ip.tol = tau;
         SolveResult ir;
+        const long long a = g.launch_count;
         int e = pcg_solve(g, ip, s, &ir);
         if (e) return e;
+        inner_recorded += g.launch_count - a;
+        inner_executed += ir.launches;
         r->iters += ir.iters;
         r->outer++;
         launch::accumulate_correction(g, g.d_x64, g.d_ch[kChX], s);
     }
-    launch::narrow(g.d_x64, g.d_ch[kChX], cells, s);
+    launch::narrow(g, g.d_x64, g.d_ch[kChX], cells, s);
+    g.x64_valid = true;
+    r->launches = (g.launch_count - own0 - inner_recorded) + inner_executed;
+    g.last_solve_launches = r->launches;
     // b channel ends as the last FP32 defect, mirroring "b channel will be modified"
     r->rel = rel;
     r->true_rel = rel;
+    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : 2;
+}
+
+int solution_f64(DevGrid& g, double* host, cudaStream_t s) {
+    int rc = ensure_fp64(g);
+    if (rc) return rc;
+    const size_t cells = (size_t)g.n * kTileCells;
+    if (!g.x64_valid) launch::widen(g, g.d_ch[kChX], g.d_x64, cells, s);
+    cudaMemcpyAsync(host, g.d_x64, cells * sizeof(double), cudaMemcpyDeviceToHost, s);
     return cudaStreamSynchronize(s) == cudaSuccess ? 0 : 2;
 }
 

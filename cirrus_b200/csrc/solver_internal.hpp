@@ -85,8 +85,15 @@ struct DevGrid {
     double* d_r64 = nullptr;
     double* d_norm = nullptr;
     float* d_bsave = nullptr;
+    bool x64_valid = false;      // the last solve was mixed precision: d_x64 holds its FP64 x
 
-    std::map<GraphKey, cudaGraphExec_t> graphs;
+    struct SolveGraph {
+        cudaGraphExec_t exec = nullptr;
+        long long prologue = 0, body = 0, epilogue = 0;  // kernel launches per section
+    };
+    std::map<GraphKey, SolveGraph> graphs;
+    mutable long long launch_count = 0;  // kernels launched (or recorded into graphs) so far
+    long long last_solve_launches = 0;   // kernels executed by the last solve
     std::string last_error;
 };
 
@@ -110,8 +117,8 @@ void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cu
 void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s);
 void accumulate_correction(const DevGrid& g, double* X64, float* E, cudaStream_t s);
 void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s);
-void widen(const float* a, double* b, size_t n, cudaStream_t s);
-void narrow(const double* a, float* b, size_t n, cudaStream_t s);
+void widen(const DevGrid& g, const float* a, double* b, size_t n, cudaStream_t s);
+void narrow(const DevGrid& g, const double* a, float* b, size_t n, cudaStream_t s);
 // right-hand side construction (rhs.cu)
 void clear_neumann_faces(const DevGrid& g, int u_channel, cudaStream_t s);
 void propagate_to_children(const DevGrid& g, int channel, cudaStream_t s);
@@ -134,13 +141,17 @@ struct SolveParams {
 struct SolveResult {
     int iters = 0, outer = 0, status = 0;
     double rel = 0, true_rel = -1;
+    long long launches = 0;  // kernels executed by the solve
 };
 
 // Plain FP32 GMG-PCG (GMGSolver::solve).  b in channel 1, x to channel 0.
 int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r);
 // Mixed precision: FP64 defect correction around FP32 PCG solves.
 int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r);
-// FP64 true relative residual of x (channel 0) against b (device FP32 leaf channel).
+// FP64 true relative residual of the last solution against b (device FP32 leaf channel): the
+// FP64 x of a mixed-precision solve, else channel 0 widened to FP64.
 int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s);
+// Copy the last solution to the host in FP64 (num_tiles*512 doubles).
+int solution_f64(DevGrid& g, double* host, cudaStream_t s);
 
 }  // namespace cirrus

@@ -105,6 +105,8 @@ cirrus_status cirrus_grid_dof(const cirrus_grid* grid, int64_t* dof);
 /* Channel transfer, num_tiles*512 floats in all-tiles order (host pointers; ordered on stream). */
 cirrus_status cirrus_grid_set_channel(cirrus_grid* grid, int channel, const float* host, void* stream);
 cirrus_status cirrus_grid_get_channel(const cirrus_grid* grid, int channel, float* host, void* stream);
+/* Device-to-device copy of a whole channel, ordered on `stream` (asynchronous). */
+cirrus_status cirrus_grid_copy_channel(cirrus_grid* grid, int dst_channel, int src_channel, void* stream);
 /* Device pointer of a channel (num_tiles*512 floats), for zero-copy integration. */
 cirrus_status cirrus_grid_channel_ptr(cirrus_grid* grid, int channel, float** device_ptr);
 
@@ -157,7 +159,8 @@ typedef struct cirrus_solve_params {
     float prolong_coeff;        /* 1 */
     int precision;              /* CIRRUS_PRECISION_* */
     int warm_start;             /* mixed mode: start from the x channel instead of 0 */
-    double inner_tolerance;     /* mixed mode: relative tolerance of each FP32 inner solve */
+    double inner_tolerance;     /* mixed mode: the tightest relative tolerance an FP32 inner solve
+                                   is asked for (each targets max(this, 0.5*tol/current residual)) */
     int max_outer_iters;        /* mixed mode: cap on defect-correction steps */
 } cirrus_solve_params;
 
@@ -168,6 +171,7 @@ typedef struct cirrus_solve_result {
                                    or of the FP64 true residual (mixed mode) */
     double true_rel_residual;   /* ||b - A x||/||b|| evaluated in FP64 (or -1 if not computed) */
     int status;                 /* cirrus_status of the solve */
+    long long kernel_launches;  /* CUDA kernels the solve executed on the device */
 } cirrus_solve_result;
 
 /* Fills params with the reference call site's values (src/FluidEuler.h:591-598). */
@@ -185,8 +189,13 @@ cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* par
 cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params* params, const float* b_host,
                                     float* x_host, void* stream, cirrus_solve_result* result);
 
-/* FP64 true residual ||b - A x||/||b|| over INTERIOR cells of LEAF tiles, for a given b
- * (host, num_tiles*512 floats) and the x held in channel 0. */
+/* The last solution in FP64 (num_tiles*512 doubles, all-tiles order): the FP64 iterate of a
+ * mixed-precision solve, else channel 0 widened.  Channel 0 always holds its FP32 rounding. */
+cirrus_status cirrus_grid_get_solution_f64(cirrus_grid* grid, double* host, void* stream);
+
+/* FP64 true residual ||b - A x||/||b|| over INTERIOR cells of LEAF tiles for a given b (host,
+ * num_tiles*512 floats) and the last solution (FP64 after a mixed-precision solve, else the
+ * FP32 channel 0). */
 cirrus_status cirrus_true_residual(cirrus_grid* grid, const float* b_host, double* rel, void* stream);
 
 #ifdef __cplusplus

@@ -354,8 +354,11 @@ struct Halo {
 };
 
 // GMGLaplacianTileData::negativeLap (src/GMGSolver.cu:56-76).  h^3 * sum_f c_f (x0 - x1).
+// `fused`: the reference's nvcc build contracts sum += c*(x0-x1) into one FMA where negativeLap
+// is inlined with a literal `diag` (Gauss-Seidel, residual/restriction kernels) but not in
+// NegativeLaplacianSameLevel128Kernel, whose calc_diag is a runtime argument (product then add).
 template <class T>
-inline T neg_lap(const Halo<T>& H, int t, int i, int j, int k, bool diag) {
+inline T neg_lap(const Halo<T>& H, int t, int i, int j, int k, bool diag, bool fused = true) {
     T h = voxel_size<T>(H.f.level[t]);
     T one_over_h = (T)1 / h;
     T x0; uint8_t tt0, ct0;
@@ -368,7 +371,9 @@ inline T neg_lap(const Halo<T>& H, int t, int i, int j, int k, bool diag) {
             T x1; uint8_t tt1, ct1;
             H.get(t, n[0], n[1], n[2], x1, tt1, ct1);
             T c = lap_coeff<T>(one_over_h, tt0, tt1, ct0, ct1);
-            sum = diag ? sum + c : fmaT<T>(c, x0 - x1, sum);
+            if (diag) sum = sum + c;
+            else if (fused) sum = fmaT<T>(c, x0 - x1, sum);
+            else { T prod = c * (x0 - x1); sum = sum + prod; }
         }
     }
     return (ct0 & INTERIOR) ? sum * h * h * h : (T)0;
@@ -410,7 +415,7 @@ struct Solver {
         for (int t = 0; t < f.n; t++) {
             if (!(f.type[t] & (LEAF | GHOST))) continue;
             for (int o = 0; o < NCELL; o++)
-                y[(size_t)t * NCELL + o] = neg_lap<T>(H, t, o >> 6, (o >> 3) & 7, o & 7, diag);
+                y[(size_t)t * NCELL + o] = neg_lap<T>(H, t, o >> 6, (o >> 3) & 7, o & 7, diag, false);
         }
     }
     // AccumulateToParents128 on GHOST tiles, additive, cell types I|D|N (src/PoissonGrid.cu:664-719)

@@ -52,13 +52,14 @@ def test_against_reference(name, built_cache, ref_ok):
     g.projection_rhs()
     rhs = g.get_channel(1)
     rrhs = ref.rhs(b.velocity)
-    assert np.array_equal(bits(rhs), bits(rrhs))
+    # the divergence writes LEAF and GHOST tiles; NONLEAF tiles keep whatever the channel held
+    lg = (b.tiles[:, 4] & (W.LEAF | W.GHOST)) != 0
+    assert np.array_equal(bits(rhs)[lg], bits(rrhs)[lg])
     # FullNegativeLaplacian
     g.set_channel(2, rhs)
     g.full_negative_laplacian(2, 3)
     ref.set_channel(2, rhs)
     ref.full_lap(2, 3)
-    lg = (b.tiles[:, 4] & (W.LEAF | W.GHOST)) != 0
     ap, rap = g.get_channel(3), ref.get_channel(3)
     assert np.array_equal(bits(ap)[lg], bits(rap)[lg])
     # V-cycle

@@ -71,7 +71,8 @@ def test_solve_full_size_against_fp64_oracle(name, built_cache):
     _, rel64, x64 = oracle_solution(b, rhs, O.CpuOracle.FP64, tol=1e-10)
     err = rel_l2(x, x64, (b.tiles[:, 4] & W.LEAF) != 0)
     print(f"{name}: iters {it} rel {rel:.3e} true {true_rel:.3e} err_vs_fp64 {err:.3e}")
-    assert err < 1e-4
+    # stated, not a parity bound: a 1e-6 relative residual leaves an O(cond * 1e-6) error
+    assert err < 1e-3
 
 
 def test_graph_and_direct_launch_agree(built_cache):
@@ -103,19 +104,29 @@ def test_repeat_solves_are_deterministic(built_cache):
     assert res[0] == res[1] == res[2]
 
 
-def test_mixed_precision_reaches_1e8(built_cache):
-    b = built_cache("sphere64_small")
+@pytest.mark.parametrize("name", ["sphere64_small", "ring512"])
+def test_mixed_precision_reaches_1e8_where_fp32_stalls(name, built_cache):
+    b = built_cache(name)
     g = grid_with_rhs(b)
     rhs = g.get_channel(1)
+    leaf = (b.tiles[:, 4] & W.LEAF) != 0
+    # plain FP32 PCG asked for 1e-10: its recursive residual drops, the true residual stalls
+    s32 = GMGSolver()
+    s32.solve(g, max_iters=300, relative_tolerance=1e-10)
+    stall = g.true_residual(rhs)
+    # FP32 V-cycle + FP64 defect correction
+    g.set_channel(1, rhs)
     s = GMGSolver(precision=PRECISION_MIXED_FP64)
     it, rel = s.solve(g, relative_tolerance=1e-8)
-    assert s.last_result.status == 0
-    assert rel < 1e-8
     true_rel = g.true_residual(rhs)
-    assert true_rel < 2e-8
-    _, _, x64 = oracle_solution(b, rhs, O.CpuOracle.FP64, tol=1e-11)
-    err = rel_l2(g.get_channel(0), x64, (b.tiles[:, 4] & W.LEAF) != 0)
-    assert err < 1e-6, err
+    x64 = g.solution_f64()
+    _, _, xo = oracle_solution(b, rhs, O.CpuOracle.FP64, tol=1e-12)
+    err = rel_l2(x64, xo, leaf)
+    print(f"{name}: fp32 true residual floor {stall:.2e}; mixed {it} iters/{s.last_result.outer_iters} outer, "
+          f"rel {rel:.2e} true {true_rel:.2e}, err vs FP64 oracle {err:.2e}")
+    assert s.last_result.status == 0 and rel < 1e-8 and true_rel < 1.5e-8
+    assert stall > 1e-8
+    assert err < 1e-5
 
 
 def test_zero_rhs_and_iteration_cap(built_cache):
