@@ -92,6 +92,10 @@ _PROTOS = {
     "cirrus_grid_get_channel": (C.c_int, [C.c_void_p, C.c_int, c_f32_p, C.c_void_p]),
     "cirrus_grid_channel_ptr": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "cirrus_grid_copy_channel": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "cirrus_topology_import_tiles": (C.c_int, [C.c_void_p, c_i32_p, C.c_int]),
+    "cirrus_grid_set_tile_pointers": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "cirrus_grid_gather_tiles": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_void_p]),
+    "cirrus_grid_scatter_tiles": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_void_p]),
     "cirrus_full_negative_laplacian": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_gauss_seidel_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_residual_and_restrict": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),

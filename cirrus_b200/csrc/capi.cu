@@ -113,6 +113,13 @@ cirrus_status cirrus_topology_set_tile(cirrus_topology* topo, int level, int x, 
     if (type != CIRRUS_LEAF && type != CIRRUS_NONLEAF && type != CIRRUS_GHOST) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] { return topo->t->set_tile(level, x, y, z, (uint8_t)type) ? CIRRUS_OK : CIRRUS_ERR_TOPOLOGY; });
 }
+cirrus_status cirrus_topology_import_tiles(cirrus_topology* topo, const int32_t* tiles5, int num_tiles) {
+    if (!topo || !tiles5 || num_tiles <= 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        topo->t->last_error.clear();
+        return topo->t->import_tiles(tiles5, num_tiles) ? CIRRUS_OK : CIRRUS_ERR_TOPOLOGY;
+    });
+}
 cirrus_status cirrus_topology_compress(cirrus_topology* topo) {
     if (!topo) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] { topo->t->compress_and_sync(); return CIRRUS_OK; });
@@ -255,6 +262,27 @@ cirrus_status cirrus_grid_copy_channel(cirrus_grid* grid, int dst_channel, int s
         cudaSuccess)
         return cuda_status();
     return CIRRUS_OK;
+}
+cirrus_status cirrus_grid_set_tile_pointers(cirrus_grid* grid, const void* const* tile_ptrs) {
+    if (!grid || !tile_ptrs) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    for (int i = 0; i < g.n; i++)
+        if (!tile_ptrs[i] || (reinterpret_cast<uintptr_t>(tile_ptrs[i]) & 15u)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (!g.d_tile_ptrs && cudaMalloc(&g.d_tile_ptrs, sizeof(void*) * g.n) != cudaSuccess) return cuda_status();
+    if (cudaMemcpy(g.d_tile_ptrs, tile_ptrs, sizeof(void*) * g.n, cudaMemcpyHostToDevice) != cudaSuccess) return cuda_status();
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_grid_gather_tiles(cirrus_grid* grid, int channel, size_t byte_offset, void* stream) {
+    if (!grid || !channel_ok(channel) || (byte_offset & 15u)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (!grid->g->d_tile_ptrs) return CIRRUS_ERR_STATE;
+    cirrus::launch::gather_tiles(*grid->g, channel, byte_offset, S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_grid_scatter_tiles(cirrus_grid* grid, int channel, size_t byte_offset, void* stream) {
+    if (!grid || !channel_ok(channel) || (byte_offset & 15u)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (!grid->g->d_tile_ptrs) return CIRRUS_ERR_STATE;
+    cirrus::launch::scatter_tiles(*grid->g, channel, byte_offset, S(stream));
+    return cuda_status();
 }
 cirrus_status cirrus_grid_channel_ptr(cirrus_grid* grid, int channel, float** device_ptr) {
     if (!grid || !device_ptr || !channel_ok(channel)) return CIRRUS_ERR_INVALID_ARGUMENT;

@@ -218,6 +218,7 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_meta);
     cudaFree(g->d_fcls);
     cudaFree(g->d_child);
+    cudaFree(g->d_tile_ptrs);
     cudaFree(g->d_lists);
     cudaFree(g->d_partials);
     cudaFree(g->d_counter);

@@ -63,6 +63,7 @@ struct DevGrid {
     TileMeta* d_meta = nullptr;
     uint32_t* d_fcls = nullptr;
     int* d_child = nullptr;      // n x 8 finer tiles per octant, -1 if absent
+    void** d_tile_ptrs = nullptr;  // optional external array-of-tiles storage (interop)
     int* d_lists = nullptr;
     const int* d_leaf = nullptr;
     const int* d_ghost = nullptr;
@@ -123,6 +124,9 @@ void narrow(const DevGrid& g, const double* a, float* b, size_t n, cudaStream_t 
 void clear_neumann_faces(const DevGrid& g, int u_channel, cudaStream_t s);
 void propagate_to_children(const DevGrid& g, int channel, cudaStream_t s);
 void velocity_divergence(const DevGrid& g, int u_channel, int b_channel, cudaStream_t s);
+// array-of-tiles interop (interop.cu)
+void gather_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream_t s);
+void scatter_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream_t s);
 }  // namespace launch
 
 // V-cycle with the reference's schedule (src/GMGSolver.cu:383-447).

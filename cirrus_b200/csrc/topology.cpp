@@ -48,6 +48,40 @@ bool Topology::set_tile(int level, int x, int y, int z, uint8_t type) {
     return put_host(level, x, y, z, Mem(), type);
 }
 
+bool Topology::import_tiles(const int32_t* t5, int n) {
+    for (int l = 0; l < num_layers_; l++) {
+        host_[l].slots.assign(host_[l].slots.size(), Slot());
+        arrays_[l].clear();
+    }
+    mem_.clear();
+    int prev = 0;
+    for (int i = 0; i < n; i++) {
+        const int level = t5[5 * i];
+        const uint8_t type = (uint8_t)t5[5 * i + 4];
+        if (level < prev || level >= num_layers_ || !(type == kLeaf || type == kNonLeaf || type == kGhost)) {
+            last_error = "import: tiles must be level-major with valid levels and types";
+            return false;
+        }
+        prev = level;
+        if (host_find(level, t5[5 * i + 1], t5[5 * i + 2], t5[5 * i + 3])) {
+            last_error = "import: duplicate tile";
+            return false;
+        }
+        if (!put_host(level, t5[5 * i + 1], t5[5 * i + 2], t5[5 * i + 3], Mem(), type)) return false;
+        const int64_t s = host_[level].probe(t5[5 * i + 1], t5[5 * i + 2], t5[5 * i + 3]);
+        arrays_[level].push_back(host_[level].slots[s]);
+    }
+    max_level_ = -1;
+    for (int l = 0; l < num_layers_; l++)
+        if (!arrays_[l].empty()) max_level_ = l;
+    dev_ = host_;
+    all_.clear();
+    for (int l = 0; l < num_layers_; l++) all_.insert(all_.end(), arrays_[l].begin(), arrays_[l].end());
+    mem_to_all_.assign(mem_.size(), -1);
+    for (size_t i = 0; i < all_.size(); i++) mem_to_all_[all_[i].mem] = (int32_t)i;
+    return true;
+}
+
 void Topology::compress_and_sync() {
     // src/HAGrid.h:491-509 then :510-561
     max_level_ = -1;

@@ -68,6 +68,9 @@ public:
     int max_level() const { return max_level_; }
 
     bool set_tile(int level, int x, int y, int z, uint8_t type);  // setTileHost with a blank tile
+    // Adopt an existing tile list in the given all-tiles order (level-major), e.g. the
+    // reference's hAllTiles: tables are filled for lookups, the order is kept as given.
+    bool import_tiles(const int32_t* tiles5, int n);
     void compress_and_sync();                                     // compressHost + syncHostAndDevice
     void spawn_ghost_tiles();                                     // SpawnGhostTiles
     std::vector<int> refine_leafs_one_step(const LevelTargetFn& target);

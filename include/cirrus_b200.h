@@ -61,6 +61,10 @@ cirrus_status cirrus_topology_create(int num_layers, const uint32_t* log2_hash, 
 void cirrus_topology_destroy(cirrus_topology* topo);
 /* Replaces HADeviceGrid::setTileHost(level, b_ijk, Tile(), type) (src/HAGrid.h:387-407). */
 cirrus_status cirrus_topology_set_tile(cirrus_topology* topo, int level, int x, int y, int z, int type);
+/* Adopts an existing tile list in the given all-tiles order (5 int32 per tile: level, x, y, z,
+ * type; level-major), e.g. a reference grid's hAllTiles (src/HAGrid.h:538-556): the order is
+ * kept as given so channel data can be exchanged tile for tile.  Replaces any previous content. */
+cirrus_status cirrus_topology_import_tiles(cirrus_topology* topo, const int32_t* tiles5, int num_tiles);
 /* Replaces compressHost() + syncHostAndDevice() (src/HAGrid.h:491-561). */
 cirrus_status cirrus_topology_compress(cirrus_topology* topo);
 /* Replaces SpawnGhostTiles(grid) (src/PoissonGrid.cu:30-60). */
@@ -105,6 +109,15 @@ cirrus_status cirrus_grid_dof(const cirrus_grid* grid, int64_t* dof);
 /* Channel transfer, num_tiles*512 floats in all-tiles order (host pointers; ordered on stream). */
 cirrus_status cirrus_grid_set_channel(cirrus_grid* grid, int channel, const float* host, void* stream);
 cirrus_status cirrus_grid_get_channel(const cirrus_grid* grid, int channel, float* host, void* stream);
+/* Array-of-tiles interop: register one device pointer per tile (all-tiles order; 16-byte
+ * aligned), e.g. the reference's HATileInfo::mTilePtr of every tile (src/HATileInfo.h:66-72).
+ * The table is copied to the device; the tiles stay owned by the caller. */
+cirrus_status cirrus_grid_set_tile_pointers(cirrus_grid* grid, const void* const* tile_ptrs);
+/* Copy 512 floats at tile_ptr + byte_offset of every registered tile into `channel`, or back
+ * (scatter), on the device.  For the reference's PoissonTile<float> channel c lies at
+ * c * 736 * 4 bytes (src/PoissonTile.h:39,51). */
+cirrus_status cirrus_grid_gather_tiles(cirrus_grid* grid, int channel, size_t byte_offset, void* stream);
+cirrus_status cirrus_grid_scatter_tiles(cirrus_grid* grid, int channel, size_t byte_offset, void* stream);
 /* Device-to-device copy of a whole channel, ordered on `stream` (asynchronous). */
 cirrus_status cirrus_grid_copy_channel(cirrus_grid* grid, int dst_channel, int src_channel, void* stream);
 /* Device pointer of a channel (num_tiles*512 floats), for zero-copy integration. */

@@ -32,8 +32,15 @@ for src in src/GMGSolver.cu src/PoissonSolver.cu src/PoissonGrid.cu src/HAGrid.c
 done
 "$NVCC" "${FLAGS[@]}" -x cu -dc -c "$REF/common/Common.cpp" -o "$OUT/obj/Common.cpp.o" &
 pids+=($!)
-"$NVCC" "${FLAGS[@]}" -dc -c "$HERE/ref_harness.cu" -o "$OUT/obj/ref_harness.cu.o" &
+"$NVCC" "${FLAGS[@]}" -I"$HERE/../include" -dc -c "$HERE/ref_harness.cu" -o "$OUT/obj/ref_harness.cu.o" &
 pids+=($!)
 for p in "${pids[@]}"; do wait "$p"; done
-"$NVCC" -shared -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC "$OUT"/obj/*.o -o "$OUT/libcirrus_ref.so"
+# the harness also exercises the product's header-only drop-in, so it links the product library
+PRODUCT_LIB="$HERE/../cirrus_b200/_lib"
+if [ ! -f "$PRODUCT_LIB/libcirrus_b200.so" ]; then
+  echo "build_ref: build the product library first (python cirrus_b200/build.py)" >&2
+  exit 3
+fi
+"$NVCC" -shared -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC "$OUT"/obj/*.o -o "$OUT/libcirrus_ref.so" \
+  -L"$PRODUCT_LIB" -lcirrus_b200 -Xlinker -rpath -Xlinker '$ORIGIN/../../cirrus_b200/_lib'
 echo "built $OUT/libcirrus_ref.so"

@@ -13,6 +13,9 @@
 #include "GMGSolver.h"
 #include "PoissonSolver.h"
 
+// the product's header-only drop-in, exercised against the reference grid it is meant for
+#include "cirrus_gmg_dropin.hpp"
+
 #include <chrono>
 #include <cstddef>
 #include <map>
@@ -31,6 +34,7 @@ namespace {
 struct RefGrid {
     std::unique_ptr<HADeviceGrid<Tile>> g;
     std::unique_ptr<GMGSolver> solver;
+    std::unique_ptr<cirrus_dropin::GMGSolver<HADeviceGrid<Tile>>> dropin;
 };
 
 __global__ void GatherChannelKernel(HATileInfo<Tile>* tiles, int c, float* out) {
@@ -67,6 +71,7 @@ void* ref_create(int num_layers, const uint32_t* log2hash, double h0) {
 }
 void ref_destroy(void* h) {
     RefGrid* r = (RefGrid*)h;
+    r->dropin.reset();
     r->solver.reset();
     r->g.reset();
     delete r;
@@ -225,6 +230,21 @@ int ref_solve(void* h, int max_iters, double tol, int level_iters, int coarsest_
     cudaDeviceSynchronize();
     auto t0 = std::chrono::high_resolution_clock::now();
     auto [iters, err] = r->solver->solve(*r->g, false, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0);
+    cudaDeviceSynchronize();
+    auto t1 = std::chrono::high_resolution_clock::now();
+    if (rel) *rel = err;
+    if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return iters;
+}
+// The same call through the product's drop-in (include/cirrus_gmg_dropin.hpp) on the same
+// reference grid: what FluidEuler::project would run after switching solver classes.
+int ref_solve_dropin(void* h, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann,
+                     double* rel, double* ms) {
+    RefGrid* r = (RefGrid*)h;
+    if (!r->dropin) r->dropin = std::make_unique<cirrus_dropin::GMGSolver<HADeviceGrid<Tile>>>(1.f, 1.f);
+    cudaDeviceSynchronize();
+    auto t0 = std::chrono::high_resolution_clock::now();
+    auto [iters, err] = r->dropin->solve(*r->g, false, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0);
     cudaDeviceSynchronize();
     auto t1 = std::chrono::high_resolution_clock::now();
     if (rel) *rel = err;

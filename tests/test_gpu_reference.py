@@ -81,3 +81,35 @@ def test_against_reference(name, built_cache, ref_ok):
     print(f"{name}: iters {it}/{rit} rel {rel:.3e}/{rrel:.3e} x_rel_l2 {err:.2e} vcycle_bitwise {vc_bitwise:.4f} ref_ms {ms:.2f}")
     assert abs(it - rit) <= 1
     assert err <= 1e-5
+
+
+@pytest.mark.parametrize("name", ["sphere64_small", "ring64_small", "ring512"])
+def test_dropin_in_reference_grid(name, built_cache, ref_ok):
+    """include/cirrus_gmg_dropin.hpp on the reference's own HADeviceGrid: what FluidEuler::project
+    runs after switching the solver class -- same iterations, same pressure and residual channels."""
+    import ctypes as C
+
+    b = built_cache(name)
+    w = b.workload
+    ref = O.RefHarness(w)
+    ref.calc_neighbors()
+    ref.set_ctypes(W.leaf_cell_types(w, b.tiles, b.nbr6))
+    ref.calc_cell_types()
+    ref.calc_neighbors()
+    rhs = ref.rhs(b.velocity)
+    it, rel, _ = ref.solve(1000, 1e-6, 1, 10, 1, w.pure_neumann)
+    x_ref, r_ref = ref.get_channel(0), ref.get_channel(1)
+    ref.set_channel(1, rhs)
+    ref.set_channel(0, np.zeros_like(rhs))
+    L = O.ref_lib()
+    L.ref_solve_dropin.restype = C.c_int
+    L.ref_solve_dropin.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    drel, dms = C.c_double(), C.c_double()
+    dit = L.ref_solve_dropin(ref.h, 1000, 1e-6, 1, 10, 1, int(w.pure_neumann), C.byref(drel), C.byref(dms))
+    x_d, r_d = ref.get_channel(0), ref.get_channel(1)
+    leaf = (b.tiles[:, 4] & W.LEAF) != 0
+    print(f"{name}: reference {it} iters {rel:.3e}; drop-in {dit} iters {drel.value:.3e} ({dms.value:.2f} ms incl. first bind)")
+    assert dit == it and drel.value == rel
+    assert np.array_equal(bits(x_d)[leaf], bits(x_ref)[leaf])
+    assert np.array_equal(bits(r_d)[leaf], bits(r_ref)[leaf])
