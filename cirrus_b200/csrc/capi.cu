@@ -326,8 +326,15 @@ cirrus_status cirrus_vcycle(cirrus_grid* grid, int x_channel, int f_channel, int
     if (!grid || !channel_ok(x_channel) || !channel_ok(f_channel) || !channel_ok(rhs_channel) || level_iters < 0 || coarsest_iters < 0)
         return CIRRUS_ERR_INVALID_ARGUMENT;
     auto& g = *grid->g;
-    cirrus::vcycle(g, g.d_ch[x_channel], g.d_ch[f_channel], g.d_ch[rhs_channel], level_iters, coarsest_iters, 1.f, 1.f, nullptr,
-                   S(stream));
+    if (cirrus::use_fused(g, level_iters, coarsest_iters) && x_channel != rhs_channel && f_channel != rhs_channel &&
+        x_channel != f_channel) {
+        // the fused schedule takes f already copied into the right-hand-side channel
+        cirrus::launch::vcycle_init(g, g.d_ch[x_channel], g.d_ch[rhs_channel], g.d_ch[f_channel], nullptr, S(stream));
+        cirrus::vcycle_fused(g, g.d_ch[x_channel], g.d_ch[rhs_channel], coarsest_iters, 1.f, 1.f, nullptr, S(stream));
+    } else {
+        cirrus::vcycle(g, g.d_ch[x_channel], g.d_ch[f_channel], g.d_ch[rhs_channel], level_iters, coarsest_iters, 1.f, 1.f,
+                       nullptr, S(stream));
+    }
     return cuda_status();
 }
 cirrus_status cirrus_dot(cirrus_grid* grid, int a_channel, int b_channel, double* result, void* stream) {

@@ -16,7 +16,8 @@ constexpr uint8_t DIRICHLET_C = 1, INTERIOR_C = 2, NEUMANN_C = 4;
 
 // Per-tile metadata, 8 int32: [0..5] same-level neighbour in the reference's stencil face order
 // (x-, x+, y-, y+, z-, z+) or -1, [6] parent tile or -1, [7] packed = level | type << 8 |
-// octant << 16 (octant = child offset inside the parent, bit0 x, bit1 y, bit2 z).
+// octant << 16 | (neighbour f is GHOST) << (24 + f)  (octant = child offset inside the parent,
+// bit0 x, bit1 y, bit2 z).
 struct __align__(16) TileMeta {
     int nb[6];
     int parent;
@@ -25,6 +26,7 @@ struct __align__(16) TileMeta {
 __host__ __device__ inline int meta_level(int packed) { return packed & 0xff; }
 __host__ __device__ inline int meta_type(int packed) { return (packed >> 8) & 0xff; }
 __host__ __device__ inline int meta_octant(int packed) { return (packed >> 16) & 0x7; }
+__host__ __device__ inline bool meta_nb_ghost(int packed, int f) { return (packed >> (24 + f)) & 1; }
 
 // Per-cell stencil mask byte: bit f (f in x-, x+, y-, y+, z-, z+) set when the face carries a
 // non-zero coefficient, bit 6 set for INTERIOR cells.  Two contexts exist: the full-tree
@@ -41,6 +43,9 @@ struct Topo {
     const uint8_t* mask_mg;      // n*512 stencil masks, multigrid level context
     const TileMeta* meta;        // n
     const uint32_t* fcls;        // n cross-face coefficient classes
+    const int* edge;             // n x 12 same-level edge neighbours (see Topology::edge_tiles)
+    const int* ghost_slot;       // n: index of a GHOST tile in the ghost list, else -1
+    const int* ghost_child;      // n x 8: ghost slot of the GHOST child in each octant, else -1
     float h0;                    // voxel size of level 0, stored in FP32 as the reference does
 };
 }  // namespace cirrus

@@ -45,12 +45,13 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
         if (err) *err = "empty topology";
         return 1;
     }
-    std::vector<int32_t> t5((size_t)n * 5), nb6((size_t)n * 6), par(n), ch8((size_t)n * 8);
+    std::vector<int32_t> t5((size_t)n * 5), nb6((size_t)n * 6), par(n), ch8((size_t)n * 8), e12((size_t)n * 12);
     std::vector<uint8_t> ct((size_t)n * kTileCells);
     topo.tiles(t5.data());
     topo.neighbor_tiles(nb6.data());
     topo.parent_tiles(par.data());
     topo.child_tiles(ch8.data());
+    topo.edge_tiles(e12.data());
     topo.cell_types(ct.data());
 
     std::vector<TileMeta> meta(n);
@@ -71,6 +72,8 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
         m.parent = par[t];
         const int oct = (t5[5 * t + 1] & 1) | ((t5[5 * t + 2] & 1) << 1) | ((t5[5 * t + 3] & 1) << 2);
         m.packed = level[t] | (type[t] << 8) | (oct << 16);
+        for (int f = 0; f < 6; f++)
+            if (m.nb[f] >= 0 && (type[m.nb[f]] & GHOST_T)) m.packed |= 1 << (24 + f);
         uint32_t cls_all = 0;
         for (int ctx = 0; ctx < 2; ctx++) {
             const int sl = ctx == 0 ? -1 : level[t];
@@ -174,6 +177,25 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
     CK(cudaMemcpy(g->d_fcls, fcls.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
     CK(cudaMalloc(&g->d_child, sizeof(int) * 8 * n));
     CK(cudaMemcpy(g->d_child, ch8.data(), sizeof(int) * 8 * n, cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g->d_edge, sizeof(int) * 12 * n));
+    CK(cudaMemcpy(g->d_edge, e12.data(), sizeof(int) * 12 * n, cudaMemcpyHostToDevice));
+    {
+        // ghost bookkeeping of the fused Laplacian: slot of each GHOST tile, the ghost slot of the
+        // GHOST child in each octant, and a 64-float partial-sum row per ghost
+        std::vector<int> gslot(n, -1), gchild((size_t)n * 8, -1);
+        for (size_t i = 0; i < ghost.size(); i++) gslot[ghost[i]] = (int)i;
+        for (int t = 0; t < n; t++)
+            for (int o = 0; o < 8; o++) {
+                const int c = ch8[(size_t)t * 8 + o];
+                if (c >= 0 && (type[c] & GHOST_T)) gchild[(size_t)t * 8 + o] = gslot[c];
+            }
+        CK(cudaMalloc(&g->d_ghost_tables, sizeof(int) * 9 * (size_t)n));
+        CK(cudaMemcpy(g->d_ghost_tables, gslot.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(g->d_ghost_tables + n, gchild.data(), sizeof(int) * 8 * (size_t)n, cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&g->d_gacc, sizeof(float) * 64 * std::max<size_t>(ghost.size(), 1)));
+        CK(cudaMalloc(&g->d_xpre, sizeof(float) * kTileCells * (size_t)n));
+        CK(cudaMemset(g->d_xpre, 0, sizeof(float) * kTileCells * (size_t)n));  // GHOST tiles stay 0
+    }
     const size_t nl = leaf.size() + ghost.size() + leafghost.size() + mg.size() + 1;
     CK(cudaMalloc(&g->d_lists, sizeof(int) * nl));
     std::vector<int> lists;
@@ -188,6 +210,26 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
     g->d_ghost = g->d_leaf + leaf.size();
     g->d_leafghost = g->d_ghost + ghost.size();
     g->d_mg = g->d_leafghost + leafghost.size();
+    {
+        std::vector<int> lt(4 * num_layers);
+        for (int l = 0; l < num_layers; l++) {
+            lt[l] = mg_off[l];
+            lt[num_layers + l] = mg_cnt[l];
+            lt[2 * num_layers + l] = lfirst[l];
+            lt[3 * num_layers + l] = lcnt[l];
+        }
+        CK(cudaMalloc(&g->d_level_tables, sizeof(int) * lt.size()));
+        CK(cudaMemcpy(g->d_level_tables, lt.data(), sizeof(int) * lt.size(), cudaMemcpyHostToDevice));
+        // levels handled by the shared-memory small-level kernel: the longest prefix of levels
+        // holding at most launch::kBottomTiles tiles in total
+        g->bottom_level = -1;
+        int cum = 0;
+        for (int l = 0; l <= g->max_level && cum + lcnt[l] <= launch::kBottomTiles; l++) {
+            cum += lcnt[l];
+            g->bottom_level = l;
+        }
+        launch::init_kernel_attributes();
+    }
     CK(cudaMalloc(&g->d_partials, sizeof(double) * 2 * std::max(g->red_blocks, 1)));
     CK(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CK(cudaMemset(g->d_counter, 0, sizeof(unsigned int) * 4));
@@ -203,6 +245,9 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
     g->topo.mask_mg = g->d_u8 + 2 * cells;
     g->topo.meta = g->d_meta;
     g->topo.fcls = g->d_fcls;
+    g->topo.edge = g->d_edge;
+    g->topo.ghost_slot = g->d_ghost_tables;
+    g->topo.ghost_child = g->d_ghost_tables + n;
     g->topo.h0 = g->h0;
     g->bytes = cells * kNumChannels * sizeof(float) + cells * 3 + sizeof(TileMeta) * n + sizeof(uint32_t) * n + sizeof(int) * nl +
                sizeof(int) * 8 * n;
@@ -218,6 +263,11 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_meta);
     cudaFree(g->d_fcls);
     cudaFree(g->d_child);
+    cudaFree(g->d_edge);
+    cudaFree(g->d_ghost_tables);
+    cudaFree(g->d_gacc);
+    cudaFree(g->d_xpre);
+    cudaFree(g->d_level_tables);
     cudaFree(g->d_tile_ptrs);
     cudaFree(g->d_lists);
     cudaFree(g->d_partials);

@@ -65,6 +65,104 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __r
     st4(Y + (size_t)tile * kTileCells + t * 4, o);
 }
 
+// Value a GHOST tile holds after PropagateValuesToGhostTiles (src/PoissonGrid.cu:585-605):
+// its parent cell's value when the ghost cell and the parent cell are INTERIOR, else 0.
+__device__ __forceinline__ float ghost_value(const Topo& tp, const float* __restrict__ X, int ghost_tile, const TileMeta& gm,
+                                             int off) {
+    if (!(tp.ctype[(size_t)ghost_tile * kTileCells + off] & INTERIOR_C) || gm.parent < 0) return 0.f;
+    const int oct = meta_octant(gm.packed);
+    const size_t pid = (size_t)gm.parent * kTileCells + ((oct & 1) * 4 + (off >> 7)) * 64 +
+                       (((oct >> 1) & 1) * 4 + ((off >> 4) & 3)) * 8 + ((oct >> 2) & 1) * 4 + ((off & 7) >> 1);
+    return (tp.ctype[pid] & INTERIOR_C) ? X[pid] : 0.f;
+}
+
+// FullNegativeLaplacian in one launch over LEAF|GHOST tiles: GHOST values (own or halo) are formed
+// from the parents on the fly instead of a propagation pass; LEAF tiles write A p; GHOST tiles
+// write their 2x2x2 child sums (AccumulateToParents128's order) to a per-ghost row, added to the
+// parent's A p by the p.Ap reduction that follows.
+template <int TPB>
+__global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ X,
+                                                               float* __restrict__ Y, float* __restrict__ GACC,
+                                                               const int* __restrict__ done) {
+    __shared__ TileShared<float> sh[TPB];
+    __shared__ float gsum[TPB][kTileCells];
+    if (done && *done) return;
+    const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
+    const int q = blockIdx.x * TPB + g;
+    const bool active = q < n;
+    const int tile = active ? list[q] : 0;
+    TileMeta m;
+    bool ghost = false;
+    if (active) {
+        m = tp.meta[tile];
+        ghost = meta_type(m.packed) & GHOST_T;
+        V4<float> own;
+        if (ghost) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) own.v[e] = ghost_value(tp, X, tile, m, t * 4 + e);
+        } else {
+            own = ld4(X + (size_t)tile * kTileCells + t * 4);
+        }
+        st4(sh[g].xs + t * 4, own);
+        // face halos: x and y faces as 16-byte vectors, z faces as scalars (see load_halo)
+        if (t < 64) {
+            const int face = t >> 4, qq = t & 15;
+            const int nb = m.nb[face];
+            int off;
+            if (face == 0) off = 448 + qq * 4;
+            else if (face == 1) off = qq * 4;
+            else if (face == 2) off = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
+            else off = (qq >> 1) * 64 + (qq & 1) * 4;
+            V4<float> v = zero4<float>();
+            if (nb >= 0) {
+                if (meta_nb_ghost(m.packed, face)) {
+                    const TileMeta nm = tp.meta[nb];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) v.v[e] = ghost_value(tp, X, nb, nm, off + e);
+                } else {
+                    v = ld4(X + (size_t)nb * kTileCells + off);
+                }
+            }
+            st4(sh[g].hx + face * 64 + qq * 4, v);
+        }
+        {
+            const int face = 4 + (t >> 6), c = t & 63;
+            const int nb = m.nb[face];
+            const int off = (c >> 3) * 64 + (c & 7) * 8 + (face == 4 ? 7 : 0);
+            float v = 0.f;
+            if (nb >= 0) v = meta_nb_ghost(m.packed, face) ? ghost_value(tp, X, nb, tp.meta[nb], off) : X[(size_t)nb * kTileCells + off];
+            sh[g].hx[face * 64 + c] = v;
+        }
+    }
+    __syncthreads();
+    if (active) {
+        const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_lap + (size_t)tile * kTileCells + t * 4);
+        const LevelConst<float> L(tp.h0, meta_level(m.packed));
+        float out[4], dg[4];
+        neg_lap4<float, false, false>(sh[g].xs, sh[g].hx, t, mask4, tp.fcls[tile] & 0xfffu, L, out, dg);
+        if (ghost) {
+            const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + (size_t)tile * kTileCells + t * 4);
+#pragma unroll
+            for (int e = 0; e < 4; e++) gsum[g][t * 4 + e] = ((ct4 >> (8 * e)) & (INTERIOR_C | DIRICHLET_C | NEUMANN_C)) ? out[e] : 0.f;
+        } else {
+            V4<float> o;
+            o.v[0] = out[0]; o.v[1] = out[1]; o.v[2] = out[2]; o.v[3] = out[3];
+            st4(Y + (size_t)tile * kTileCells + t * 4, o);
+        }
+    }
+    __syncthreads();
+    if (!active || !ghost || t >= 64) return;
+    const int fi = t / 16 * 2, fj = (t / 4) % 4 * 2, fk = t % 4 * 2;
+    float sum = 0.f;
+#pragma unroll
+    for (int ii = 0; ii < 2; ii++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int kk = 0; kk < 2; kk++) sum += gsum[g][(fi + ii) * 64 + (fj + jj) * 8 + (fk + kk)];
+    GACC[(size_t)tp.ghost_slot[tile] * 64 + t] = sum;
+}
+
 // AccumulateToParents128Kernel on GHOST tiles, additive, coefficient 1, all cell types
 // (src/PoissonGrid.cu:664-710).  2x2x2 sums in the reference's (ii,jj,kk) order.
 template <class T>
@@ -419,9 +517,10 @@ __global__ void __launch_bounds__(256) k_leaf_reduce(Topo tp, const int* __restr
         const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
         if (OP == OP_DOT) {
             acc_a += dot4f(ld4(A + off), ld4(B + off));
-        } else if (OP == OP_INIT) {  // A = x, B = r
+        } else if (OP == OP_INIT) {  // A = x, B = r, D = multigrid right-hand side (copy of r)
             st4(A + off, zero4<float>());
             const V4<float> r = ld4(B + off);
+            if (D) st4(D + off, r);
             acc_a += dot4f(r, r);
         } else if (OP == OP_COPY_DOT) {  // A = z, B = r, C = p
             const V4<float> z = ld4(A + off);
@@ -440,7 +539,21 @@ __global__ void __launch_bounds__(256) k_leaf_reduce(Topo tp, const int* __restr
             }
             st4(A + off, x);
             st4(C + off, r);
+            st4(D + off, r);  // Ap is consumed; the channel now carries r as the multigrid right-hand side
             acc_a += dot4f(r, r);
+        } else if (OP == OP_PAP) {  // A = p, B = Ap, C = ghost partial sums: Ap += ghost sums; p.Ap
+            const V4<float> p = ld4(A + off);
+            V4<float> ap = ld4(B + off);
+            const int qv = (int)(v & 127);
+            const int i = qv >> 4, j = (qv >> 1) & 7, k0 = (qv & 1) * 4;
+            const int gs = tp.ghost_child[(size_t)tile * 8 + ((i >> 2) | ((j >> 2) << 1) | ((k0 >> 2) << 2))];
+            if (gs >= 0) {
+                const float* row = C + (size_t)gs * 64 + (i & 3) * 16 + (j & 3) * 4 + (k0 & 3);
+#pragma unroll
+                for (int e = 0; e < 4; e++) ap.v[e] = ap.v[e] + row[e];
+                st4(B + off, ap);
+            }
+            acc_a += dot4f(p, ap);
         } else if (OP == OP_MEAN) {  // A = channel
             const V4<float> a = ld4(A + off);
             acc_a += (double)(a.v[0] + a.v[1] + a.v[2] + a.v[3]);
@@ -471,9 +584,10 @@ __global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict
     }
 }
 
-// r -= mean on INTERIOR cells of LEAF tiles (ReCenterLeafVoxels, src/PoissonSolver.cu:356-368).
+// r -= mean on INTERIOR cells of LEAF tiles (ReCenterLeafVoxels, src/PoissonSolver.cu:356-368);
+// RC (optional) receives a copy of the recentred r (the multigrid right-hand side).
 __global__ void __launch_bounds__(256) k_recenter(Topo tp, const int* __restrict__ leaves, int nleaf, float* R,
-                                                  const Scalars* S, int skip_if_done) {
+                                                  const Scalars* S, int skip_if_done, float* RC) {
     if (skip_if_done && S->done) return;
     const double mean = S->mean;
     const size_t nv = (size_t)nleaf * 128;
@@ -486,6 +600,7 @@ __global__ void __launch_bounds__(256) k_recenter(Topo tp, const int* __restrict
         for (int e = 0; e < 4; e++)
             if ((ct4 >> (8 * e)) & INTERIOR_C) r.v[e] = (float)((double)r.v[e] - mean);
         st4(R + off, r);
+        if (RC) st4(RC + off, r);
     }
 }
 
@@ -591,6 +706,13 @@ void full_laplacian(const DevGrid& g, T* X, T* Y, const int* done, cudaStream_t 
 template void full_laplacian<float>(const DevGrid&, float*, float*, const int*, cudaStream_t);
 template void full_laplacian<double>(const DevGrid&, double*, double*, const int*, cudaStream_t);
 
+void laplacian_fused(const DevGrid& g, const float* X, float* Y, const int* done, cudaStream_t s) {
+    if (g.n_leafghost == 0) return;
+    ++g.launch_count;
+    k_laplacian_fused<kTPB><<<(g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.d_leafghost, g.n_leafghost, X, Y,
+                                                                                      g.d_gacc, done);
+}
+
 void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const int* done, cudaStream_t s) {
     const int n = g.mg_count[level];
     if (n == 0) return;
@@ -661,6 +783,10 @@ void leaf_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* 
         ++g.launch_count;
         k_leaf_reduce<OP_MEAN><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
         break;
+    case OP_PAP:
+        ++g.launch_count;
+        k_leaf_reduce<OP_PAP><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
+        break;
     }
 }
 
@@ -669,9 +795,9 @@ void update_p(const DevGrid& g, float* P, const float* Z, const Scalars* S, cuda
     k_update_p<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, P, Z, S);
 }
 
-void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cudaStream_t s) {
+void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cudaStream_t s, float* RC) {
     ++g.launch_count;
-    k_recenter<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, R, S, skip_if_done);
+    k_recenter<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, R, S, skip_if_done, RC);
 }
 
 void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s) {

@@ -58,11 +58,38 @@ void vcycle(const DevGrid& g, float* X, const float* F, float* RHS, int level_it
     }
 }
 
+bool use_fused(const DevGrid& g, int level_iters, int coarsest_iters) {
+    const char* e = std::getenv("CIRRUS_VCYCLE");
+    if (e && std::strcmp(e, "generic") == 0) return false;
+    return level_iters == 1 && g.bottom_level >= 0 && launch::bottom_supported(coarsest_iters, std::min(g.bottom_level, g.max_level));
+}
+
+void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, float one_over_alpha, float prolong_coeff,
+                  const int* done, cudaStream_t s) {
+    const int lb = std::min(g.bottom_level, g.max_level);
+    for (int l = g.max_level; l > lb; l--) {
+        launch::presmooth(g, l, g.d_xpre, RHS, done, s);
+        launch::residual_restrict(g, l, g.d_xpre, RHS, RHS, one_over_alpha, done, s);
+    }
+    launch::bottom(g, lb, coarsest_iters, X, RHS, one_over_alpha, prolong_coeff, done, s);
+    for (int l = lb + 1; l <= g.max_level; l++) {
+        launch::prolong_sweep(g, l, X, g.d_xpre, RHS, prolong_coeff, done, s);
+        launch::gs_sweep(g, l, X, RHS, 0, done, s);
+    }
+}
+
 namespace {
 
 struct Ch {
     float *x, *r, *p, *ap, *z;
 };
+
+// z <- M^-1 r with the fused kernels when level_iters == 1 (RHS already holds r on LEAF tiles).
+void precondition(const DevGrid& g, const SolveParams& p, const int* done, cudaStream_t s) {
+    const Ch c{g.d_ch[kChX], g.d_ch[kChR], g.d_ch[kChP], g.d_ch[kChAp], g.d_ch[kChZ]};
+    if (use_fused(g, p.level_iters, p.coarsest_iters)) vcycle_fused(g, c.z, c.ap, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, done, s);
+    else vcycle(g, c.z, c.r, c.ap, p.level_iters, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, done, s);
+}
 Ch channels(const DevGrid& g) { return {g.d_ch[kChX], g.d_ch[kChR], g.d_ch[kChP], g.d_ch[kChAp], g.d_ch[kChZ]}; }
 
 // GMGSolver::solve, src/GMGSolver.cu:535-568
@@ -71,12 +98,15 @@ void record_prologue(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl
     Scalars* S = g.d_scalars;
     const int* done = &S->done;
     cudaMemsetAsync(S, 0, sizeof(Scalars), s);
-    launch::leaf_reduce(OP_INIT, g, c.x, c.r, nullptr, nullptr, S, ctl, EPI_INIT, 0, s);
+    // the fused V-cycle reads GHOST right-hand sides (channel Ap) as stored: 0; nothing in the
+    // fused iteration writes them
+    if (use_fused(g, p.level_iters, p.coarsest_iters)) launch::zero_ghost_tiles(g, c.ap, s);
+    launch::leaf_reduce(OP_INIT, g, c.x, c.r, nullptr, c.ap, S, ctl, EPI_INIT, 0, s);
     if (p.pure_neumann) {
         launch::leaf_reduce(OP_MEAN, g, c.r, nullptr, nullptr, nullptr, S, ctl, EPI_MEAN, 1, s);
-        launch::recenter(g, c.r, S, 1, s);
+        launch::recenter(g, c.r, S, 1, s, c.ap);
     }
-    vcycle(g, c.z, c.r, c.ap, p.level_iters, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, done, s);
+    precondition(g, p, done, s);
     launch::leaf_reduce(OP_COPY_DOT, g, c.z, c.r, c.p, nullptr, S, ctl, EPI_GAMMA, 1, s);
 }
 
@@ -85,14 +115,19 @@ void record_body(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl, cu
     const Ch c = channels(g);
     Scalars* S = g.d_scalars;
     const int* done = &S->done;
-    launch::full_laplacian<float>(g, c.p, c.ap, done, s);
-    launch::leaf_reduce(OP_DOT, g, c.p, c.ap, nullptr, nullptr, S, ctl, EPI_ALPHA, 1, s);
+    if (use_fused(g, p.level_iters, p.coarsest_iters)) {
+        launch::laplacian_fused(g, c.p, c.ap, done, s);
+        launch::leaf_reduce(OP_PAP, g, c.p, c.ap, g.d_gacc, nullptr, S, ctl, EPI_ALPHA, 1, s);
+    } else {
+        launch::full_laplacian<float>(g, c.p, c.ap, done, s);
+        launch::leaf_reduce(OP_DOT, g, c.p, c.ap, nullptr, nullptr, S, ctl, EPI_ALPHA, 1, s);
+    }
     launch::leaf_reduce(OP_XR, g, c.x, c.p, c.r, c.ap, S, ctl, EPI_CHECK, 1, s);
     if (p.pure_neumann) {
         launch::leaf_reduce(OP_MEAN, g, c.r, nullptr, nullptr, nullptr, S, ctl, EPI_MEAN, 1, s);
-        launch::recenter(g, c.r, S, 1, s);
+        launch::recenter(g, c.r, S, 1, s, c.ap);
     }
-    vcycle(g, c.z, c.r, c.ap, p.level_iters, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, done, s);
+    precondition(g, p, done, s);
     launch::leaf_reduce(OP_DOT, g, c.r, c.z, nullptr, nullptr, S, ctl, EPI_BETA, 1, s);
     launch::update_p(g, c.p, c.z, S, s);
 }
@@ -200,7 +235,8 @@ void fill_result(const DevGrid& g, SolveResult* r) {
 }  // namespace
 
 int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r) {
-    GraphKey key{p.max_iters, p.level_iters, p.coarsest_iters, p.sync_stride, p.pure_neumann, p.tol, p.one_over_alpha, p.prolong_coeff};
+    GraphKey key{p.max_iters, p.level_iters, p.coarsest_iters, p.sync_stride, p.pure_neumann, p.tol, p.one_over_alpha, p.prolong_coeff,
+                 use_fused(g, p.level_iters, p.coarsest_iters) ? 1 : 0};
     DevGrid::SolveGraph sg;
     if (graphs_enabled()) {
         auto it = g.graphs.find(key);

@@ -33,17 +33,18 @@ struct SolveCtl {
     cudaGraphConditionalHandle cond;
 };
 
-enum { OP_DOT = 0, OP_INIT = 1, OP_COPY_DOT = 2, OP_XR = 3, OP_MEAN = 4 };
+enum { OP_DOT = 0, OP_INIT = 1, OP_COPY_DOT = 2, OP_XR = 3, OP_MEAN = 4, OP_PAP = 5 };
 enum { EPI_NONE = -1, EPI_INIT = 0, EPI_GAMMA = 1, EPI_ALPHA = 2, EPI_CHECK = 3, EPI_BETA = 4, EPI_MEAN = 5, EPI_FINAL = 6 };
 
 struct GraphKey {
     int max_iters, level_iters, coarsest_iters, sync_stride, pure_neumann;
     double tol;
     float one_over_alpha, prolong_coeff;
+    int fused;
     bool operator<(const GraphKey& o) const {
-        return std::tie(max_iters, level_iters, coarsest_iters, sync_stride, pure_neumann, tol, one_over_alpha, prolong_coeff) <
+        return std::tie(max_iters, level_iters, coarsest_iters, sync_stride, pure_neumann, tol, one_over_alpha, prolong_coeff, fused) <
                std::tie(o.max_iters, o.level_iters, o.coarsest_iters, o.sync_stride, o.pure_neumann, o.tol, o.one_over_alpha,
-                        o.prolong_coeff);
+                        o.prolong_coeff, o.fused);
     }
 };
 
@@ -63,6 +64,10 @@ struct DevGrid {
     TileMeta* d_meta = nullptr;
     uint32_t* d_fcls = nullptr;
     int* d_child = nullptr;      // n x 8 finer tiles per octant, -1 if absent
+    int* d_edge = nullptr;       // n x 12 same-level edge neighbours, -1 if absent
+    int* d_ghost_tables = nullptr;  // ghost slot per tile (n) | ghost slot per child octant (n x 8)
+    float* d_gacc = nullptr;        // per GHOST tile: 64 partial sums of its A p (fused Laplacian)
+    float* d_xpre = nullptr;        // n x 512: pre-smoothed x of the fused V-cycle (read by the upstroke)
     void** d_tile_ptrs = nullptr;  // optional external array-of-tiles storage (interop)
     int* d_lists = nullptr;
     const int* d_leaf = nullptr;
@@ -71,6 +76,8 @@ struct DevGrid {
     const int* d_mg = nullptr;
     int n_leaf = 0, n_ghost = 0, n_leafghost = 0;
     std::vector<int> mg_offset, mg_count, level_first, level_count;
+    int* d_level_tables = nullptr;  // mg_offset | mg_count | level_first | level_count (num_layers each)
+    int bottom_level = -1;          // levels 0..bottom_level fit the shared-memory small-level kernel (-1: none)
     std::vector<uint8_t> h_tile_type;
 
     double* d_partials = nullptr;
@@ -104,6 +111,8 @@ void grid_destroy(DevGrid* g);
 
 namespace launch {
 template <class T> void full_laplacian(const DevGrid& g, T* X, T* Y, const int* done, cudaStream_t s);
+// FullNegativeLaplacian as one launch; the ghost-to-parent sums are completed by OP_PAP.
+void laplacian_fused(const DevGrid& g, const float* X, float* Y, const int* done, cudaStream_t s);
 void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const int* done, cudaStream_t s);
 void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t colors, int nsweeps, const int* done,
                  cudaStream_t s);
@@ -114,7 +123,7 @@ void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const i
 void leaf_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* D, Scalars* S, const SolveCtl& ctl, int epi,
                  int skip_if_done, cudaStream_t s);
 void update_p(const DevGrid& g, float* P, const float* Z, const Scalars* S, cudaStream_t s);
-void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cudaStream_t s);
+void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cudaStream_t s, float* RC = nullptr);
 void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s);
 void accumulate_correction(const DevGrid& g, double* X64, float* E, cudaStream_t s);
 void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s);
@@ -124,14 +133,31 @@ void narrow(const DevGrid& g, const double* a, float* b, size_t n, cudaStream_t 
 void clear_neumann_faces(const DevGrid& g, int u_channel, cudaStream_t s);
 void propagate_to_children(const DevGrid& g, int channel, cudaStream_t s);
 void velocity_divergence(const DevGrid& g, int u_channel, int b_channel, cudaStream_t s);
+// fused V-cycle (vcycle_fused.cu)
+void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const int* done, cudaStream_t s);
+void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const int* done,
+                   cudaStream_t s);
+void zero_ghost_tiles(const DevGrid& g, float* X, cudaStream_t s);
+bool bottom(const DevGrid& g, int lb, int coarsest_iters, float* Z, const float* RHS, float one_over_alpha, float prolong_coeff,
+            const int* done, cudaStream_t s);
+bool bottom_supported(int coarsest_iters, int lb);
+constexpr int kBottomTiles = 40;  // tiles the shared-memory small-level kernel holds
+void init_kernel_attributes();
 // array-of-tiles interop (interop.cu)
 void gather_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream_t s);
 void scatter_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream_t s);
 }  // namespace launch
 
-// V-cycle with the reference's schedule (src/GMGSolver.cu:383-447).
+// V-cycle with the reference's schedule (src/GMGSolver.cu:383-447), one launch per kernel of the
+// reference (any level_iters).
 void vcycle(const DevGrid& g, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters, float one_over_alpha,
             float prolong_coeff, const int* done, cudaStream_t s);
+// The same V-cycle with fused kernels (level_iters == 1).  Precondition: RHS holds f on LEAF
+// tiles (the PCG kernels that write r maintain this) and 0 on GHOST tiles; X needs no
+// initialisation.
+void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, float one_over_alpha, float prolong_coeff,
+                  const int* done, cudaStream_t s);
+bool use_fused(const DevGrid& g, int level_iters, int coarsest_iters);
 
 struct SolveParams {
     int max_iters = 1000;

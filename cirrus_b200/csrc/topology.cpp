@@ -248,6 +248,23 @@ void Topology::child_tiles(int32_t* out8) const {
     }
 }
 
+void Topology::edge_tiles(int32_t* out12) const {
+    static const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    size_t i = 0;
+    for (int l = 0; l < num_layers_; l++) {
+        for (const Slot& s : arrays_[l]) {
+            for (int e = 0; e < 12; e++) {
+                int c[3] = {s.x, s.y, s.z};
+                c[pairs[e >> 2][0]] += (e & 2) ? 1 : -1;
+                c[pairs[e >> 2][1]] += (e & 1) ? 1 : -1;
+                const Slot* t = dev_find(l, c[0], c[1], c[2]);
+                out12[12 * i + e] = t ? mem_to_all_[t->mem] : -1;
+            }
+            i++;
+        }
+    }
+}
+
 void Topology::set_cell_types(const uint8_t* ct) {
     for (size_t i = 0; i < all_.size(); i++) std::memcpy(mem_[all_[i].mem].ctype.data(), ct + i * kCells, kCells);
 }

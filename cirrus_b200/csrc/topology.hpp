@@ -89,6 +89,9 @@ public:
     void parent_tiles(int32_t* out) const;
     // the 8 tiles one level finer inside each tile (octant o = x | y<<1 | z<<2), or -1
     void child_tiles(int32_t* out8) const;
+    // the 12 same-level edge neighbours of each tile, or -1.  Edge e = 4*p + 2*(sa>0) + (sb>0)
+    // for axis pair p in {(x,y), (x,z), (y,z)} with offsets sa, sb in {-1,+1} on its two axes.
+    void edge_tiles(int32_t* out12) const;
 
     std::string last_error;
 

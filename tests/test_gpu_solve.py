@@ -152,3 +152,29 @@ def test_solve_host_end_to_end(built_cache):
     it2, rel2 = GMGSolver().solve(g2)
     assert (it, rel) == (it2, rel2)
     assert np.array_equal(x.view(np.uint32), g2.get_channel(0).view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["sphere64_small", "sphere64_neumann_small", "ring512", "uniform128"])
+def test_fused_vcycle_equals_generic(name, built_cache):
+    """The fused V-cycle schedule (one launch per level each way, small levels in one CTA) gives
+    bit-identical solves to the one-kernel-per-reference-kernel schedule."""
+    b = built_cache(name)
+    g = grid_with_rhs(b)
+    rhs = g.get_channel(1)
+    pure = b.workload.pure_neumann
+    s = GMGSolver()
+    it1, rel1 = s.solve(g, is_pure_neumann=pure)
+    n1 = s.last_result.kernel_launches
+    x1 = g.get_channel(0)
+    g.set_channel(1, rhs)
+    os.environ["CIRRUS_VCYCLE"] = "generic"
+    try:
+        it2, rel2 = s.solve(g, is_pure_neumann=pure)
+        n2 = s.last_result.kernel_launches
+    finally:
+        del os.environ["CIRRUS_VCYCLE"]
+    x2 = g.get_channel(0)
+    print(f"{name}: fused {it1} iters {n1} kernels; generic {it2} iters {n2} kernels")
+    assert (it1, rel1) == (it2, rel2)
+    assert np.array_equal(x1.view(np.uint32), x2.view(np.uint32))
+    assert n1 < n2
