@@ -102,6 +102,7 @@ _PROTOS = {
     "cirrus_prolongate_and_update": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "cirrus_vcycle": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_dot": (C.c_int, [C.c_void_p, C.c_int, C.c_int, c_f64_p, C.c_void_p]),
+    "cirrus_leaf_dot_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, c_f64_p, C.c_void_p]),
     "cirrus_clear_neumann_neighbor_faces": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "cirrus_propagate_to_children": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "cirrus_velocity_volume_divergence_on_leafs": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),

@@ -790,6 +790,13 @@ void leaf_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* 
     }
 }
 
+void leaf_dot_raw(const float* A, const float* B, const int* leaves, int nleaf, int blocks, double* partials,
+                  unsigned int* counter, Scalars* S, cudaStream_t s) {
+    const SolveCtl ctl{};
+    k_leaf_reduce<OP_DOT><<<blocks, 256, 0, s>>>(Topo{}, leaves, nleaf, const_cast<float*>(A), const_cast<float*>(B), nullptr,
+                                                 nullptr, S, ctl, EPI_GAMMA, partials, counter, 0);
+}
+
 void update_p(const DevGrid& g, float* P, const float* Z, const Scalars* S, cudaStream_t s) {
     ++g.launch_count;
     k_update_p<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, P, Z, S);

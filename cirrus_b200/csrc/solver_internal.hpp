@@ -122,6 +122,10 @@ void prolongate(const DevGrid& g, int level, const float* CX, float* FX, float p
 void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const int* done, cudaStream_t s);
 void leaf_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* D, Scalars* S, const SolveCtl& ctl, int epi,
                  int skip_if_done, cudaStream_t s);
+// OP_DOT over an explicit leaf list with caller-provided scratch (partials: 2 doubles per block;
+// counter 0 at launch); the sum goes to S->gamma.
+void leaf_dot_raw(const float* A, const float* B, const int* leaves, int nleaf, int blocks, double* partials,
+                  unsigned int* counter, Scalars* S, cudaStream_t s);
 void update_p(const DevGrid& g, float* P, const float* Z, const Scalars* S, cudaStream_t s);
 void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cudaStream_t s, float* RC = nullptr);
 void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s);

@@ -143,6 +143,29 @@ cirrus_status cirrus_vcycle(cirrus_grid* grid, int x_channel, int f_channel, int
 /* Dot over LEAF tiles (src/PoissonGrid.cu:199-228); synchronises `stream`. */
 cirrus_status cirrus_dot(cirrus_grid* grid, int a_channel, int b_channel, double* result, void* stream);
 
+/* Allocation-free LEAF dot product.  No counterpart in the reference: its Dot reduces through
+ * buffers allocated with the grid.  For callers that cannot call cudaMalloc at this point --
+ * cudaMalloc/cudaFree may synchronise the device, fail when the memory budget is spent, or be
+ * off-limits inside a caller's allocator or memory-pool callbacks -- and for callers that keep
+ * their tiles in their own memory and hold no cirrus_grid.  The result is bit-identical to
+ * cirrus_dot on a grid whose LEAF tiles are leaf_tiles (same kernel, same block count).
+ *   a, b        device pointers, 512 floats per tile (tile t at a + 512*t), 16-byte aligned
+ *   leaf_tiles  device array of n_leaf tile indices (the LEAF tiles in all-tiles order)
+ *   result      host pointer; the call synchronises `stream`
+ * All reduction scratch is one static device array of the library (about 17 KB per device):
+ * per-block partial sums for at most CIRRUS_NOALLOC_MAX_BLOCKS blocks, a result slot and a
+ * ticket counter that must be 0 when the kernel starts (the call zeroes it on `stream` first).
+ * The call needs min(ceil(n_leaf/2), 4 x SM count) blocks and returns
+ * CIRRUS_ERR_INVALID_ARGUMENT, doing nothing, when that exceeds CIRRUS_NOALLOC_MAX_BLOCKS
+ * (only on devices with more than 256 SMs).  The first call on each device looks up the
+ * scratch address (cudaGetSymbolAddress); make it before any stream capture on that device.
+ * Calls that can overlap on one device (several host threads, or streams not ordered with each
+ * other) share the scratch and race: serialise them.  Calls from one host thread never overlap,
+ * since each returns only after its stream is synchronised. */
+#define CIRRUS_NOALLOC_MAX_BLOCKS 1024
+cirrus_status cirrus_leaf_dot_noalloc(const float* a, const float* b, const int32_t* leaf_tiles, int n_leaf,
+                                      double* result, void* stream);
+
 /* Right-hand side of the projection (the callers either side of the solve in FluidEuler::project).
  * Velocities are the three lower-face components in channels u, u+1, u+2. */
 /* ClearAllNeumannNeighborFaces (src/FluidEuler.cu:43-60) on LEAF tiles. */
