@@ -156,14 +156,24 @@ def _mask_args(masks, num_layers):
 class DeviceGrid:
     """The tile pool of a finalised topology resident on the current CUDA device."""
 
-    def __init__(self, topology: Topology):
+    def __init__(self, topology: "Topology | Sequence[Topology]"):
+        """One instance (a Topology) or a batch of independent instances (a sequence of them) in
+        one tile pool; a batch is solved together by GMGSolver.solve_batch."""
         h = C.c_void_p()
-        check(lib().cirrus_grid_create(topology.handle, C.byref(h)), "cirrus_grid_create")
+        if isinstance(topology, Topology):
+            check(lib().cirrus_grid_create(topology.handle, C.byref(h)), "cirrus_grid_create")
+            topos = [topology]
+        else:
+            topos = list(topology)
+            arr = (C.c_void_p * len(topos))(*[t.handle.value for t in topos])
+            check(lib().cirrus_grid_create_batch(arr, len(topos), C.byref(h)), "cirrus_grid_create_batch")
         self._h = h
         n = C.c_int()
         check(lib().cirrus_grid_num_tiles(h, C.byref(n)), "cirrus_grid_num_tiles")
         self.num_tiles = n.value
-        self.tiles = topology.tiles()
+        self.num_instances = len(topos)
+        self.instance_tiles = [t.num_tiles for t in topos]
+        self.tiles = topos[0].tiles() if len(topos) == 1 else None
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -198,6 +208,22 @@ class DeviceGrid:
         out = np.empty((self.num_tiles, 512), dtype=np.float32)
         check(lib().cirrus_grid_get_channel(self._h, channel, _ptr(out, C.c_float), C.c_void_p(stream)), "cirrus_grid_get_channel")
         return out
+
+    def set_channel_instance(self, instance: int, channel: int, values: np.ndarray, stream: int = 0) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float32).reshape(self.instance_tiles[instance] * 512)
+        check(lib().cirrus_grid_set_channel_instance(self._h, instance, channel, _ptr(a, C.c_float), C.c_void_p(stream)),
+              "cirrus_grid_set_channel_instance")
+
+    def get_channel_instance(self, instance: int, channel: int, stream: int = 0) -> np.ndarray:
+        out = np.empty((self.instance_tiles[instance], 512), dtype=np.float32)
+        check(lib().cirrus_grid_get_channel_instance(self._h, instance, channel, _ptr(out, C.c_float), C.c_void_p(stream)),
+              "cirrus_grid_get_channel_instance")
+        return out
+
+    def instance_dof(self, instance: int) -> int:
+        d = C.c_int64()
+        check(lib().cirrus_grid_instance_info(self._h, instance, None, C.byref(d)), "cirrus_grid_instance_info")
+        return d.value
 
     def copy_channel(self, dst_channel: int, src_channel: int, stream: int = 0) -> None:
         check(lib().cirrus_grid_copy_channel(self._h, dst_channel, src_channel, C.c_void_p(stream)), "cirrus_grid_copy_channel")
@@ -263,11 +289,12 @@ class DeviceGrid:
               "cirrus_grid_get_solution_f64")
         return out
 
-    def true_residual(self, b: np.ndarray, stream: int = 0) -> float:
+    def true_residual(self, b: np.ndarray, stream: int = 0):
+        """FP64 ||b - A x|| / ||b|| of the last solution (a float; a list for a batch)."""
         a = np.ascontiguousarray(b, dtype=np.float32).reshape(self.num_tiles * 512)
-        r = C.c_double()
-        check(lib().cirrus_true_residual(self._h, _ptr(a, C.c_float), C.byref(r), C.c_void_p(stream)), "cirrus_true_residual")
-        return r.value
+        r = (C.c_double * self.num_instances)()
+        check(lib().cirrus_true_residual(self._h, _ptr(a, C.c_float), r, C.c_void_p(stream)), "cirrus_true_residual")
+        return r[0] if self.num_instances == 1 else list(r)
 
 
 class GMGSolver:
@@ -313,6 +340,20 @@ class GMGSolver:
         if verbose:
             print(f"GMG-PCG: {r.iters} iters, relative residual {r.rel_residual:.3e}, status {r.status}")
         return r.iters, r.rel_residual
+
+    def solve_batch(self, grid: DeviceGrid, active: Sequence[bool] | None = None, tolerances: Sequence[float] | None = None,
+                    stream: int = 0, **kw) -> list[tuple[int, float]]:
+        """Solve every (active) instance of a batched grid in one graph launch; per-instance
+        (iters, relative residual).  Each instance's bits do not depend on the rest of the batch."""
+        p = self.params(**kw)
+        k = grid.num_instances
+        res = (SolveResult * k)()
+        act = (C.c_int * k)(*[int(bool(a)) for a in active]) if active is not None else None
+        tol = (C.c_double * k)(*tolerances) if tolerances is not None else None
+        check(lib().cirrus_gmg_solve_batch(grid.handle, C.byref(p), act, tol, C.c_void_p(stream), res), "cirrus_gmg_solve_batch")
+        self.last_results = list(res)
+        self.last_result = res[0]
+        return [(r.iters, r.rel_residual) for r in res]
 
     def solve_host(self, grid: DeviceGrid, b: np.ndarray, x_out: np.ndarray, stream: int = 0, **kw) -> tuple[int, float]:
         """End-to-end solve from host buffers (b in, x out; all-tiles order, 512 floats/tile)."""

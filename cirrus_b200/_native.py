@@ -84,6 +84,11 @@ _PROTOS = {
     "cirrus_topology_calc_cell_types_from_leafs": (C.c_int, [C.c_void_p]),
     "cirrus_topology_neighbor_tiles": (C.c_int, [C.c_void_p, c_i32_p]),
     "cirrus_grid_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "cirrus_grid_create_batch": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
+    "cirrus_grid_num_instances": (C.c_int, [C.c_void_p, c_int_p]),
+    "cirrus_grid_instance_info": (C.c_int, [C.c_void_p, C.c_int, c_int_p, C.POINTER(C.c_int64)]),
+    "cirrus_grid_set_channel_instance": (C.c_int, [C.c_void_p, C.c_int, C.c_int, c_f32_p, C.c_void_p]),
+    "cirrus_grid_get_channel_instance": (C.c_int, [C.c_void_p, C.c_int, C.c_int, c_f32_p, C.c_void_p]),
     "cirrus_grid_destroy": (None, [C.c_void_p]),
     "cirrus_grid_num_tiles": (C.c_int, [C.c_void_p, c_int_p]),
     "cirrus_grid_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
@@ -108,6 +113,8 @@ _PROTOS = {
     "cirrus_velocity_volume_divergence_on_leafs": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_solve_params_default": (None, [C.POINTER(SolveParams)]),
     "cirrus_gmg_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveResult)]),
+    "cirrus_gmg_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_int_p, c_f64_p, C.c_void_p,
+                                         C.POINTER(SolveResult)]),
     "cirrus_gmg_solve_host": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p, C.POINTER(SolveResult)]),
     "cirrus_true_residual": (C.c_int, [C.c_void_p, c_f32_p, c_f64_p, C.c_void_p]),
     "cirrus_grid_get_solution_f64": (C.c_int, [C.c_void_p, c_f64_p, C.c_void_p]),

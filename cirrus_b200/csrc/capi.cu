@@ -7,6 +7,7 @@
 #include <cstring>
 #include <exception>
 #include <new>
+#include <vector>
 
 struct cirrus_topology {
     cirrus::Topology* t;
@@ -216,11 +217,58 @@ cirrus_status cirrus_grid_create(const cirrus_topology* topo, cirrus_grid** out)
     return guard([&] {
         cirrus::DevGrid* g = nullptr;
         std::string err;
-        int rc = cirrus::grid_create(*topo->t, &g, &err);
+        int rc = cirrus::grid_create({topo->t}, &g, &err);
         if (rc) return map_rc(rc);
         *out = new cirrus_grid{g};
         return CIRRUS_OK;
     });
+}
+cirrus_status cirrus_grid_create_batch(const cirrus_topology* const* topos, int count, cirrus_grid** out) {
+    if (!topos || count <= 0 || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < count; i++)
+        if (!topos[i]) return CIRRUS_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return CIRRUS_ERR_NO_DEVICE;
+    }
+    return guard([&] {
+        std::vector<const cirrus::Topology*> ts;
+        for (int i = 0; i < count; i++) ts.push_back(topos[i]->t);
+        cirrus::DevGrid* g = nullptr;
+        std::string err;
+        int rc = cirrus::grid_create(ts, &g, &err);
+        if (rc) return map_rc(rc);
+        *out = new cirrus_grid{g};
+        return CIRRUS_OK;
+    });
+}
+cirrus_status cirrus_grid_num_instances(const cirrus_grid* grid, int* count) {
+    if (!grid || !count) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *count = grid->g->num_inst;
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_grid_instance_info(const cirrus_grid* grid, int instance, int* num_tiles, int64_t* dof) {
+    if (!grid || instance < 0 || instance >= grid->g->num_inst) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (num_tiles) *num_tiles = grid->g->inst_tiles[instance];
+    if (dof) *dof = grid->g->inst_dof[instance];
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_grid_set_channel_instance(cirrus_grid* grid, int instance, int channel, const float* host, void* stream) {
+    if (!grid || !host || !channel_ok(channel) || instance < 0 || instance >= grid->g->num_inst) return CIRRUS_ERR_INVALID_ARGUMENT;
+    for (const cirrus::TileRun& r : grid->g->inst_runs[instance])
+        if (cudaMemcpyAsync(grid->g->d_ch[channel] + (size_t)r.global * cirrus::kTileCells, host + (size_t)r.local * cirrus::kTileCells,
+                            (size_t)r.count * cirrus::kTileCells * sizeof(float), cudaMemcpyHostToDevice, S(stream)) != cudaSuccess)
+            return cuda_status();
+    return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
+}
+cirrus_status cirrus_grid_get_channel_instance(const cirrus_grid* grid, int instance, int channel, float* host, void* stream) {
+    if (!grid || !host || !channel_ok(channel) || instance < 0 || instance >= grid->g->num_inst) return CIRRUS_ERR_INVALID_ARGUMENT;
+    for (const cirrus::TileRun& r : grid->g->inst_runs[instance])
+        if (cudaMemcpyAsync(host + (size_t)r.local * cirrus::kTileCells, grid->g->d_ch[channel] + (size_t)r.global * cirrus::kTileCells,
+                            (size_t)r.count * cirrus::kTileCells * sizeof(float), cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess)
+            return cuda_status();
+    return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
 }
 void cirrus_grid_destroy(cirrus_grid* grid) {
     if (!grid) return;
@@ -340,12 +388,10 @@ cirrus_status cirrus_vcycle(cirrus_grid* grid, int x_channel, int f_channel, int
 cirrus_status cirrus_dot(cirrus_grid* grid, int a_channel, int b_channel, double* result, void* stream) {
     if (!grid || !result || !channel_ok(a_channel) || !channel_ok(b_channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
     auto& g = *grid->g;
-    cirrus::SolveCtl ctl{};
-    cirrus::launch::leaf_reduce(cirrus::OP_DOT, g, g.d_ch[a_channel], g.d_ch[b_channel], nullptr, nullptr, g.d_scalars, ctl,
-                                cirrus::EPI_GAMMA, 0, S(stream));
-    cudaMemcpyAsync(g.h_scalars, g.d_scalars, sizeof(cirrus::Scalars), cudaMemcpyDeviceToHost, S(stream));
+    cirrus::launch::grid_dot(g, g.d_ch[a_channel], g.d_ch[b_channel], S(stream));
+    if (cudaMemcpyAsync(result, &g.d_dot->gamma, sizeof(double), cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess)
+        return cuda_status();
     if (cudaStreamSynchronize(S(stream)) != cudaSuccess) return cuda_status();
-    *result = g.h_scalars->gamma;
     return cuda_status();
 }
 
@@ -384,23 +430,45 @@ void cirrus_solve_params_default(cirrus_solve_params* p) {
     p->max_outer_iters = 20;
 }
 
-cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream, cirrus_solve_result* result) {
-    if (!grid || !params_ok(params) || !result) return CIRRUS_ERR_INVALID_ARGUMENT;
+cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_params* params, const int* active,
+                                     const double* tolerances, void* stream, cirrus_solve_result* results) {
+    if (!grid || !params_ok(params) || !results) return CIRRUS_ERR_INVALID_ARGUMENT;
+    const int K = grid->g->num_inst;
+    if (tolerances)
+        for (int i = 0; i < K; i++)
+            if (!(tolerances[i] >= 0)) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] {
         cirrus::SolveParams p;
         to_internal(params, &p);
-        cirrus::SolveResult r;
+        std::vector<cirrus::InstRequest> req(K);
+        for (int i = 0; i < K; i++) {
+            req[i].active = active ? (active[i] ? 1 : 0) : 1;
+            if (tolerances) req[i].tol = tolerances[i];
+        }
+        std::vector<cirrus::SolveResult> r(K);
         if (p.precision != CIRRUS_PRECISION_MIXED_FP64) grid->g->x64_valid = false;
-        int rc = p.precision == CIRRUS_PRECISION_MIXED_FP64 ? cirrus::mixed_solve(*grid->g, p, S(stream), &r)
-                                                            : cirrus::pcg_solve(*grid->g, p, S(stream), &r);
+        int rc = p.precision == CIRRUS_PRECISION_MIXED_FP64 ? cirrus::mixed_solve(*grid->g, p, S(stream), r.data(), req.data())
+                                                            : cirrus::pcg_solve(*grid->g, p, S(stream), r.data(), req.data());
         if (rc) return map_rc(rc);
-        result->iters = r.iters;
-        result->outer_iters = r.outer;
-        result->rel_residual = r.rel;
-        result->true_rel_residual = r.true_rel;
-        result->status = (int)map_rc(r.status);
-        result->kernel_launches = r.launches;
+        for (int i = 0; i < K; i++) {
+            results[i].iters = r[i].iters;
+            results[i].outer_iters = r[i].outer;
+            results[i].rel_residual = r[i].rel;
+            results[i].true_rel_residual = r[i].true_rel;
+            results[i].status = (int)map_rc(r[i].status);
+            results[i].kernel_launches = r[i].launches;
+        }
         return CIRRUS_OK;
+    });
+}
+
+cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream, cirrus_solve_result* result) {
+    if (!grid || !params_ok(params) || !result) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        std::vector<cirrus_solve_result> all(grid->g->num_inst);
+        cirrus_status st = cirrus_gmg_solve_batch(grid, params, nullptr, nullptr, stream, all.data());
+        if (st == CIRRUS_OK) *result = all[0];
+        return st;
     });
 }
 

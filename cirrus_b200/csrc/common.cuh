@@ -36,7 +36,25 @@ __host__ __device__ inline bool meta_nb_ghost(int packed, int f) { return (packe
 // class 2 = (2/3)/h^2 (leaf-ghost T-junction).
 constexpr int kMaskInterior = 64;
 
-// Kernel-side view of the topology tables of a device grid (all arrays in all-tiles order).
+// Scalar state of one PCG solve of one instance, resident in device memory (the reference keeps
+// gamma, beta, alpha, gamma_old, fp, mean, count as 7 device doubles, src/GMGSolver.h:22-30).
+struct Scalars {
+    double rhs2, thr2, gamma, gamma_old, beta, alpha, fp, res2, mean, rel;
+    int iter, iters, done, converged, nonfinite, pad;
+};
+
+// Per-instance parameters of one solve of a (batched) grid, written by the host before each solve.
+struct InstParams {
+    double tol;           // relative residual tolerance
+    int max_iters;
+    int active;           // 0: the instance takes no part in this solve (its channels stay untouched)
+    int pure_neumann;     // project r to zero mean each iteration (ReCenterLeafVoxels)
+    int pad;
+};
+
+// Kernel-side view of the topology tables of a device grid.  A grid holds one or more independent
+// instances (a batch); tiles are ordered level-major across the batch and, inside a level and
+// instance, in the instance's all-tiles order.
 struct Topo {
     const uint8_t* ctype;        // n*512 cell types
     const uint8_t* mask_lap;     // n*512 stencil masks, full-tree Laplacian context
@@ -46,6 +64,13 @@ struct Topo {
     const int* edge;             // n x 12 same-level edge neighbours (see Topology::edge_tiles)
     const int* ghost_slot;       // n: index of a GHOST tile in the ghost list, else -1
     const int* ghost_child;      // n x 8: ghost slot of the GHOST child in each octant, else -1
-    float h0;                    // voxel size of level 0, stored in FP32 as the reference does
+    const int* inst;             // n: instance of each tile
+    const float* inst_h0;        // per instance: voxel size of level 0, stored in FP32 as the reference does
 };
+
+__host__ __device__ inline float tile_h0(const Topo& tp, int tile) { return tp.inst_h0[tp.inst[tile]]; }
+// true when the tile's instance has finished (or takes no part in) the running solve
+__host__ __device__ inline bool tile_done(const Topo& tp, const Scalars* S, int tile) {
+    return S != nullptr && S[tp.inst[tile]].done != 0;
+}
 }  // namespace cirrus

@@ -1,11 +1,15 @@
-// Device grid construction: turns a finalised host topology into the HBM-resident tile pool.
+// Device grid construction: turns one or more finalised host topologies (the instances of a
+// batch) into one HBM-resident tile pool.
 //
-// Layout (all-tiles order, level-major as the reference's dAllTiles):
+// Layout (level-major across the batch: all instances' level-0 tiles, then level 1, ...; inside a
+// level, instance by instance in each instance's all-tiles order, so a single instance keeps the
+// reference's dAllTiles order):
 //   channels   9 x n x 512 FP32, one contiguous buffer (channel-major SoA)
 //   u8         ctype | mask_lap | mask_mg, 3 x n x 512 bytes
 //   meta       n x TileMeta (32 B): neighbours in stencil face order, parent, level/type/octant
 //   fcls       n x uint32 cross-face coefficient classes (Laplacian and multigrid contexts)
-//   lists      LEAF, GHOST, LEAF|GHOST tiles; LEAF|NONLEAF tiles per level
+//   inst       n x int32 instance of each tile
+//   lists      LEAF (instance by instance), GHOST, LEAF|GHOST tiles; LEAF|NONLEAF tiles per level
 // The per-cell stencil masks fold NegativeLaplacianCoeff's tile-type and Neumann tests
 // (src/GMGSolver.cu:26-39) into one byte so the kernels never load neighbour cell types.
 #include "solver_internal.hpp"
@@ -37,23 +41,86 @@ inline uint32_t coeff_class(uint8_t a, uint8_t b) {
         }                                                            \
     } while (0)
 
+template <class T> int upload(T** dst, const std::vector<T>& src) {
+    if (cudaMalloc(dst, sizeof(T) * std::max<size_t>(src.size(), 1)) != cudaSuccess) return 3;
+    if (!src.empty() && cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice) != cudaSuccess) return 2;
+    return 0;
+}
+
 }  // namespace
 
-int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
-    const int n = topo.num_tiles();
-    if (n <= 0) {
-        if (err) *err = "empty topology";
+int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::string* err) {
+    const int K = (int)topos.size();
+    if (K <= 0) {
+        if (err) *err = "no instances";
         return 1;
     }
+    // ------------------------------------------------------------------ merge the instances
+    int num_layers = 0;
+    std::vector<int> ni(K);
+    for (int i = 0; i < K; i++) {
+        ni[i] = topos[i]->num_tiles();
+        if (ni[i] <= 0) {
+            if (err) *err = "empty topology (instance " + std::to_string(i) + ")";
+            return 1;
+        }
+        num_layers = std::max(num_layers, topos[i]->num_layers());
+    }
+    // local tables, then the global order
+    std::vector<std::vector<int32_t>> lt5(K), lnb6(K), lpar(K), lch8(K), le12(K);
+    std::vector<std::vector<uint8_t>> lct(K);
+    for (int i = 0; i < K; i++) {
+        const Topology& tp = *topos[i];
+        const size_t m = (size_t)ni[i];
+        lt5[i].resize(m * 5); lnb6[i].resize(m * 6); lpar[i].resize(m); lch8[i].resize(m * 8); le12[i].resize(m * 12);
+        lct[i].resize(m * kTileCells);
+        tp.tiles(lt5[i].data());
+        tp.neighbor_tiles(lnb6[i].data());
+        tp.parent_tiles(lpar[i].data());
+        tp.child_tiles(lch8[i].data());
+        tp.edge_tiles(le12[i].data());
+        tp.cell_types(lct[i].data());
+    }
+    std::vector<std::vector<int>> l2g(K);
+    std::vector<std::vector<TileRun>> runs(K);
+    std::vector<int> g_inst, g_local;
+    for (int i = 0; i < K; i++) l2g[i].assign(ni[i], -1);
+    for (int l = 0; l < num_layers; l++)
+        for (int i = 0; i < K; i++) {
+            int first = -1, cnt = 0;
+            for (int t = 0; t < ni[i]; t++)
+                if (lt5[i][5 * t] == l) {
+                    if (first < 0) first = t;
+                    cnt++;
+                }
+            if (cnt == 0) continue;
+            runs[i].push_back({(int)g_inst.size(), first, cnt});
+            for (int t = first; t < first + cnt; t++) {
+                if (lt5[i][5 * t] != l) {
+                    if (err) *err = "instance tiles are not level-major";
+                    return 1;
+                }
+                l2g[i][t] = (int)g_inst.size();
+                g_inst.push_back(i);
+                g_local.push_back(t);
+            }
+        }
+    const int n = (int)g_inst.size();
     std::vector<int32_t> t5((size_t)n * 5), nb6((size_t)n * 6), par(n), ch8((size_t)n * 8), e12((size_t)n * 12);
     std::vector<uint8_t> ct((size_t)n * kTileCells);
-    topo.tiles(t5.data());
-    topo.neighbor_tiles(nb6.data());
-    topo.parent_tiles(par.data());
-    topo.child_tiles(ch8.data());
-    topo.edge_tiles(e12.data());
-    topo.cell_types(ct.data());
+    auto remap = [&](int i, int v) { return v >= 0 ? l2g[i][v] : -1; };
+    for (int t = 0; t < n; t++) {
+        const int i = g_inst[t], lt = g_local[t];
+        for (int a = 0; a < 5; a++) t5[5 * (size_t)t + a] = lt5[i][5 * (size_t)lt + a];
+        for (int a = 0; a < 6; a++) nb6[6 * (size_t)t + a] = remap(i, lnb6[i][6 * (size_t)lt + a]);
+        par[t] = remap(i, lpar[i][lt]);
+        for (int a = 0; a < 8; a++) ch8[8 * (size_t)t + a] = remap(i, lch8[i][8 * (size_t)lt + a]);
+        for (int a = 0; a < 12; a++) e12[12 * (size_t)t + a] = remap(i, le12[i][12 * (size_t)lt + a]);
+        std::memcpy(&ct[(size_t)t * kTileCells], &lct[i][(size_t)lt * kTileCells], kTileCells);
+    }
+    lt5.clear(); lnb6.clear(); lpar.clear(); lch8.clear(); le12.clear(); lct.clear();
 
+    // ------------------------------------------------------------------ per-tile metadata and masks
     std::vector<TileMeta> meta(n);
     std::vector<uint32_t> fcls(n);
     std::vector<uint8_t> mlap((size_t)n * kTileCells), mmg((size_t)n * kTileCells);
@@ -115,16 +182,20 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
         fcls[t] = cls_all;
     }
 
-    // lists
+    // ------------------------------------------------------------------ lists
     std::vector<int> leaf, ghost, leafghost, mg;
-    const int num_layers = topo.num_layers();
     std::vector<int> mg_off(num_layers, 0), mg_cnt(num_layers, 0), lfirst(num_layers, 0), lcnt(num_layers, 0);
-    int64_t dof = 0;
+    std::vector<int> inst_leaves(K, 0);
+    std::vector<int64_t> inst_dof(K, 0);
+    for (int i = 0; i < K; i++)  // LEAF tiles instance by instance (each instance's reductions see its own order)
+        for (const TileRun& r : runs[i])
+            for (int t = r.global; t < r.global + r.count; t++)
+                if (type[t] & LEAF_T) {
+                    leaf.push_back(t);
+                    inst_leaves[i]++;
+                    for (int o = 0; o < kTileCells; o++) inst_dof[i] += (ct[(size_t)t * kTileCells + o] & INTERIOR_C) ? 1 : 0;
+                }
     for (int t = 0; t < n; t++) {
-        if (type[t] & LEAF_T) {
-            leaf.push_back(t);
-            for (int o = 0; o < kTileCells; o++) dof += (ct[(size_t)t * kTileCells + o] & INTERIOR_C) ? 1 : 0;
-        }
         if (type[t] & GHOST_T) ghost.push_back(t);
         if (type[t] & (LEAF_T | GHOST_T)) leafghost.push_back(t);
     }
@@ -144,10 +215,18 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
     cudaGetDevice(&g->device);
     cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, g->device);
     g->n = n;
+    g->num_inst = K;
     g->num_layers = num_layers;
-    g->max_level = topo.max_level();
-    g->h0 = (float)topo.h0();
-    g->dof = dof;
+    for (int i = 0; i < K; i++) {
+        g->max_level = std::max(g->max_level, topos[i]->max_level());
+        g->inst_h0.push_back((float)topos[i]->h0());
+        g->inst_tiles.push_back(ni[i]);
+        g->inst_max_level.push_back(topos[i]->max_level());
+        g->dof += inst_dof[i];
+    }
+    g->inst_leaves = inst_leaves;
+    g->inst_dof = inst_dof;
+    g->inst_runs = runs;
     g->n_leaf = (int)leaf.size();
     g->n_ghost = (int)ghost.size();
     g->n_leafghost = (int)leafghost.size();
@@ -179,6 +258,8 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
     CK(cudaMemcpy(g->d_child, ch8.data(), sizeof(int) * 8 * n, cudaMemcpyHostToDevice));
     CK(cudaMalloc(&g->d_edge, sizeof(int) * 12 * n));
     CK(cudaMemcpy(g->d_edge, e12.data(), sizeof(int) * 12 * n, cudaMemcpyHostToDevice));
+    CK((cudaError_t)(upload(&g->d_inst, g_inst) ? cudaErrorMemoryAllocation : cudaSuccess));
+    CK((cudaError_t)(upload(&g->d_inst_h0, g->inst_h0) ? cudaErrorMemoryAllocation : cudaSuccess));
     {
         // ghost bookkeeping of the fused Laplacian: slot of each GHOST tile, the ghost slot of the
         // GHOST child in each octant, and a 64-float partial-sum row per ghost
@@ -210,35 +291,138 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
     g->d_ghost = g->d_leaf + leaf.size();
     g->d_leafghost = g->d_ghost + ghost.size();
     g->d_mg = g->d_leafghost + leafghost.size();
+
+    // ------------------------------------------------------------------ coarse-level boxes
+    // Levels handled by the shared-memory kernel, one CTA per instance: the longest prefix of
+    // levels (common to all instances, at most each instance's finest level) whose padded dense
+    // boxes (a level's tile bounding box in cells plus a one-cell halo) fit the kernel's
+    // shared-memory budget in every instance.  Absent tiles and the halo hold x = 0, the value the
+    // reference gives a missing neighbour.
     {
-        std::vector<int> lt(4 * num_layers);
-        for (int l = 0; l < num_layers; l++) {
-            lt[l] = mg_off[l];
-            lt[num_layers + l] = mg_cnt[l];
-            lt[2 * num_layers + l] = lfirst[l];
-            lt[3 * num_layers + l] = lcnt[l];
+        struct Box { int off, sy, sz, cells; int lo[3]; };
+        int lb = *std::min_element(g->inst_max_level.begin(), g->inst_max_level.end());
+        lb = std::min(lb, kBottomMaxLevels - 1);
+        std::vector<std::vector<Box>> boxes(K);
+        std::vector<std::vector<int>> ifirst(K, std::vector<int>(num_layers, 0)), icnt(K, std::vector<int>(num_layers, 0));
+        for (int i = 0; i < K; i++)
+            for (const TileRun& r : runs[i]) {
+                ifirst[i][level[r.global]] = r.global;
+                icnt[i][level[r.global]] = r.count;
+            }
+        for (int i = 0; i < K && lb >= 0; i++) {
+            long long acc = 0;
+            int tiles = 0, fit = -1;
+            for (int l = 0; l <= lb && icnt[i][l] > 0; l++) {
+                int lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+                for (int t = ifirst[i][l]; t < ifirst[i][l] + icnt[i][l]; t++)
+                    for (int a = 0; a < 3; a++) {
+                        lo[a] = std::min(lo[a], t5[5 * t + 1 + a]);
+                        hi[a] = std::max(hi[a], t5[5 * t + 1 + a]);
+                    }
+                const long long ex = 8LL * (hi[0] - lo[0] + 1) + 2, ey = 8LL * (hi[1] - lo[1] + 1) + 2, ez = 8LL * (hi[2] - lo[2] + 1) + 2;
+                if (ex > (1 << 15) || ey > (1 << 15) || ez > (1 << 15)) break;
+                const long long c = ex * ey * ez;
+                if (launch::bottom_smem_bytes(acc + c + 8, tiles + icnt[i][l]) > (size_t)launch::kBottomSmemBudget) break;
+                boxes[i].push_back({(int)acc, (int)(ey * ez), (int)ez, (int)c, {lo[0], lo[1], lo[2]}});
+                acc += c;
+                tiles += icnt[i][l];
+                fit = l;
+            }
+            lb = std::min(lb, fit);
         }
-        CK(cudaMalloc(&g->d_level_tables, sizeof(int) * lt.size()));
-        CK(cudaMemcpy(g->d_level_tables, lt.data(), sizeof(int) * lt.size(), cudaMemcpyHostToDevice));
-        // levels handled by the shared-memory small-level kernel: the longest prefix of levels
-        // holding at most launch::kBottomTiles tiles in total
-        g->bottom_level = -1;
-        int cum = 0;
-        for (int l = 0; l <= g->max_level && cum + lcnt[l] <= launch::kBottomTiles; l++) {
-            cum += lcnt[l];
-            g->bottom_level = l;
+        g->bottom_level = lb;
+        if (lb >= 0) {
+            std::vector<int4> rec;
+            std::vector<uint16_t> code;
+            std::vector<BottomInst> bi(K);
+            std::vector<int> base(n, -1);
+            for (int i = 0; i < K; i++) {
+                BottomInst& b = bi[i];
+                std::memset(&b, 0, sizeof(b));
+                b.rec_off = (int)rec.size();
+                b.code_off = (int)code.size();
+                // cells of levels 0..lb, padded to whole 16-byte vectors of codes
+                const long long cells_i = (long long)boxes[i][lb].off + boxes[i][lb].cells;
+                b.cells = (int)((cells_i + 7) & ~7LL);
+                code.resize(code.size() + b.cells, 0);
+                for (int l = 0; l <= lb; l++) {
+                    b.first[l] = (int)rec.size() - b.rec_off;
+                    b.cnt[l] = icnt[i][l];
+                    b.sy[l] = boxes[i][l].sy;
+                    b.sz[l] = boxes[i][l].sz;
+                    for (int t = ifirst[i][l]; t < ifirst[i][l] + icnt[i][l]; t++) {
+                        const Box& bx = boxes[i][l];
+                        base[t] = bx.off + (8 * (t5[5 * t + 1] - bx.lo[0]) + 1) * bx.sy + (8 * (t5[5 * t + 2] - bx.lo[1]) + 1) * bx.sz +
+                                  8 * (t5[5 * t + 3] - bx.lo[2]) + 1;
+                        int pbase = -1;
+                        if (par[t] >= 0) {
+                            const int lp = level[par[t]];
+                            const int oct = meta_octant(meta[t].packed);
+                            pbase = base[par[t]] + (oct & 1) * 4 * boxes[i][lp].sy + ((oct >> 1) & 1) * 4 * boxes[i][lp].sz +
+                                    ((oct >> 2) & 1) * 4;
+                        }
+                        rec.push_back(make_int4(base[t], pbase, type[t] | (level[t] << 8), t));
+                        const uint32_t mgcls = fcls[t] >> 12;
+                        for (int o = 0; o < kTileCells; o++) {
+                            const int ijk[3] = {o >> 6, (o >> 3) & 7, o & 7};
+                            uint16_t c = mmg[(size_t)t * kTileCells + o];
+                            for (int f = 0; f < 6; f++) {
+                                const bool edge = (f & 1) ? ijk[f >> 1] == 7 : ijk[f >> 1] == 0;
+                                if (edge && ((mgcls >> (2 * f)) & 3u) == 2u) c |= (uint16_t)(1u << (7 + f));
+                            }
+                            code[(size_t)b.code_off + base[t] + ijk[0] * bx.sy + ijk[1] * bx.sz + ijk[2]] = c;
+                        }
+                    }
+                }
+                b.nrec = (int)rec.size() - b.rec_off;
+                g->bottom_smem = std::max(g->bottom_smem, launch::bottom_smem_bytes(b.cells, b.nrec));
+            }
+            CK((cudaError_t)(upload(&g->d_bottom_tiles, rec) ? cudaErrorMemoryAllocation : cudaSuccess));
+            CK((cudaError_t)(upload(&g->d_bottom_code, code) ? cudaErrorMemoryAllocation : cudaSuccess));
+            CK((cudaError_t)(upload(&g->d_bottom_inst, bi) ? cudaErrorMemoryAllocation : cudaSuccess));
         }
         launch::init_kernel_attributes();
     }
-    CK(cudaMalloc(&g->d_partials, sizeof(double) * 2 * std::max(g->red_blocks, 1)));
+
+    // ------------------------------------------------------------------ per-instance reductions
+    {
+        std::vector<int4> chunks;
+        std::vector<int2> ich(K);
+        long long vbeg = 0;
+        for (int i = 0; i < K; i++) {
+            const long long nv = (long long)inst_leaves[i] * 128;
+            const int nch = (int)std::max(1LL, (nv + kChunkVecs - 1) / kChunkVecs);
+            ich[i] = make_int2((int)chunks.size(), nch);
+            for (int c = 0; c < nch; c++) {
+                const long long b = vbeg + (long long)c * kChunkVecs;
+                chunks.push_back(make_int4(i, (int)b, (int)std::min(vbeg + nv, b + kChunkVecs), 0));
+            }
+            vbeg += nv;
+        }
+        g->n_chunks = (int)chunks.size();
+        CK((cudaError_t)(upload(&g->d_chunks, chunks) ? cudaErrorMemoryAllocation : cudaSuccess));
+        CK((cudaError_t)(upload(&g->d_inst_chunks, ich) ? cudaErrorMemoryAllocation : cudaSuccess));
+    }
+    CK(cudaMalloc(&g->d_partials, sizeof(double) * 2 * std::max(g->red_blocks, g->n_chunks)));
     CK(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CK(cudaMemset(g->d_counter, 0, sizeof(unsigned int) * 4));
-    CK(cudaMalloc(&g->d_scalars, sizeof(Scalars)));
-    CK(cudaMemset(g->d_scalars, 0, sizeof(Scalars)));
-    CK(cudaMallocHost(&g->h_scalars, sizeof(Scalars)));
+    CK(cudaMalloc(&g->d_counters, sizeof(unsigned int) * K));
+    CK(cudaMemset(g->d_counters, 0, sizeof(unsigned int) * K));
+    CK(cudaMalloc(&g->d_scalars, sizeof(Scalars) * K));
+    CK(cudaMemset(g->d_scalars, 0, sizeof(Scalars) * K));
+    CK(cudaMallocHost(&g->h_scalars, sizeof(Scalars) * K));
+    std::memset(g->h_scalars, 0, sizeof(Scalars) * K);
+    CK(cudaMalloc(&g->d_dot, sizeof(Scalars)));
+    CK(cudaMemset(g->d_dot, 0, sizeof(Scalars)));
+    CK(cudaMalloc(&g->d_iparams, sizeof(InstParams) * K));
+    CK(cudaMemset(g->d_iparams, 0, sizeof(InstParams) * K));
+    CK(cudaMallocHost(&g->h_iparams, sizeof(InstParams) * K));
+    std::memset(g->h_iparams, 0, sizeof(InstParams) * K);
+    CK(cudaMalloc(&g->d_active, sizeof(int)));
+    CK(cudaMemset(g->d_active, 0, sizeof(int)));
     g->history_cap = 4096;
     CK(cudaMalloc(&g->d_history, sizeof(double) * g->history_cap));
-    CK(cudaMalloc(&g->d_norm, sizeof(double) * 4));
+    CK(cudaMalloc(&g->d_norm, sizeof(double) * (K + 4)));
 
     g->topo.ctype = g->d_u8;
     g->topo.mask_lap = g->d_u8 + cells;
@@ -248,9 +432,10 @@ int grid_create(const Topology& topo, DevGrid** out, std::string* err) {
     g->topo.edge = g->d_edge;
     g->topo.ghost_slot = g->d_ghost_tables;
     g->topo.ghost_child = g->d_ghost_tables + n;
-    g->topo.h0 = g->h0;
+    g->topo.inst = g->d_inst;
+    g->topo.inst_h0 = g->d_inst_h0;
     g->bytes = cells * kNumChannels * sizeof(float) + cells * 3 + sizeof(TileMeta) * n + sizeof(uint32_t) * n + sizeof(int) * nl +
-               sizeof(int) * 8 * n;
+               sizeof(int) * 22 * (size_t)n + cells * sizeof(float);
     *out = g;
     return 0;
 }
@@ -264,16 +449,27 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_fcls);
     cudaFree(g->d_child);
     cudaFree(g->d_edge);
+    cudaFree(g->d_inst);
+    cudaFree(g->d_inst_h0);
     cudaFree(g->d_ghost_tables);
     cudaFree(g->d_gacc);
     cudaFree(g->d_xpre);
-    cudaFree(g->d_level_tables);
+    cudaFree(g->d_bottom_tiles);
+    cudaFree(g->d_bottom_code);
+    cudaFree(g->d_bottom_inst);
     cudaFree(g->d_tile_ptrs);
     cudaFree(g->d_lists);
+    cudaFree(g->d_chunks);
+    cudaFree(g->d_inst_chunks);
     cudaFree(g->d_partials);
     cudaFree(g->d_counter);
+    cudaFree(g->d_counters);
     cudaFree(g->d_scalars);
     if (g->h_scalars) cudaFreeHost(g->h_scalars);
+    cudaFree(g->d_dot);
+    cudaFree(g->d_iparams);
+    if (g->h_iparams) cudaFreeHost(g->h_iparams);
+    cudaFree(g->d_active);
     cudaFree(g->d_history);
     cudaFree(g->d_x64);
     cudaFree(g->d_ax64);

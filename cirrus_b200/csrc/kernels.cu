@@ -4,6 +4,7 @@
 #include "solver_internal.hpp"
 
 #include <cstdio>
+#include <cstdlib>
 
 namespace cirrus {
 
@@ -12,11 +13,12 @@ namespace cirrus {
 // cell's value when both are INTERIOR, 0 otherwise.
 template <class T>
 __global__ void __launch_bounds__(128) k_propagate_ghosts(Topo tp, const int* __restrict__ list, int n, T* X,
-                                                          const int* __restrict__ done) {
-    if (done && *done) return;
+                                                          const Scalars* __restrict__ S) {
+    pdl_entry();
     const int q = blockIdx.x;
     if (q >= n) return;
     const int tile = list[q];
+    if (tile_done(tp, S, tile)) return;
     const int t = threadIdx.x;
     const TileMeta m = tp.meta[tile];
     const TileIdx ix(t);
@@ -42,13 +44,13 @@ __global__ void __launch_bounds__(128) k_propagate_ghosts(Topo tp, const int* __
 // levels with the tile types as stored (subtree level -1).
 template <class T, int TPB>
 __global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __restrict__ list, int n, const T* __restrict__ X,
-                                                         T* __restrict__ Y, const int* __restrict__ done) {
+                                                         T* __restrict__ Y, const Scalars* __restrict__ S) {
+    pdl_entry();
     __shared__ TileShared<T> sh[TPB];
-    if (done && *done) return;
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     const int q = blockIdx.x * TPB + g;
-    const bool active = q < n;
-    const int tile = active ? list[q] : 0;
+    const int tile = q < n ? list[q] : 0;
+    const bool active = q < n && !tile_done(tp, S, tile);
     TileMeta m;
     if (active) {
         m = tp.meta[tile];
@@ -57,7 +59,7 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __r
     __syncthreads();
     if (!active) return;
     const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_lap + (size_t)tile * kTileCells + t * 4);
-    const LevelConst<T> L((T)tp.h0, meta_level(m.packed));
+    const LevelConst<T> L((T)tile_h0(tp, tile), meta_level(m.packed));
     T out[4], dg[4];
     neg_lap4<T, false, false>(sh[g].xs, sh[g].hx, t, mask4, tp.fcls[tile] & 0xfffu, L, out, dg);
     V4<T> o;
@@ -83,14 +85,14 @@ __device__ __forceinline__ float ghost_value(const Topo& tp, const float* __rest
 template <int TPB>
 __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ X,
                                                                float* __restrict__ Y, float* __restrict__ GACC,
-                                                               const int* __restrict__ done) {
+                                                               const Scalars* __restrict__ S) {
+    pdl_entry();
     __shared__ TileShared<float> sh[TPB];
     __shared__ float gsum[TPB][kTileCells];
-    if (done && *done) return;
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     const int q = blockIdx.x * TPB + g;
-    const bool active = q < n;
-    const int tile = active ? list[q] : 0;
+    const int tile = q < n ? list[q] : 0;
+    const bool active = q < n && !tile_done(tp, S, tile);
     TileMeta m;
     bool ghost = false;
     if (active) {
@@ -137,7 +139,7 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const in
     __syncthreads();
     if (active) {
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_lap + (size_t)tile * kTileCells + t * 4);
-        const LevelConst<float> L(tp.h0, meta_level(m.packed));
+        const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
         float out[4], dg[4];
         neg_lap4<float, false, false>(sh[g].xs, sh[g].hx, t, mask4, tp.fcls[tile] & 0xfffu, L, out, dg);
         if (ghost) {
@@ -167,11 +169,12 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const in
 // (src/PoissonGrid.cu:664-710).  2x2x2 sums in the reference's (ii,jj,kk) order.
 template <class T>
 __global__ void __launch_bounds__(64) k_accumulate_ghosts(Topo tp, const int* __restrict__ list, int n, T* Y,
-                                                          const int* __restrict__ done) {
-    if (done && *done) return;
+                                                          const Scalars* __restrict__ S) {
+    pdl_entry();
     const int q = blockIdx.x;
     if (q >= n) return;
     const int tile = list[q];
+    if (tile_done(tp, S, tile)) return;
     const TileMeta m = tp.meta[tile];
     if (m.parent < 0) return;
     const int b = threadIdx.x;
@@ -199,13 +202,13 @@ __global__ void __launch_bounds__(64) k_accumulate_ghosts(Topo tp, const int* __
 // x += (b - A x) / D on INTERIOR cells.
 template <int TPB>
 __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
-                                                        const float* __restrict__ R, int color, const int* __restrict__ done) {
+                                                        const float* __restrict__ R, int color, const Scalars* __restrict__ S) {
+    pdl_entry();
     __shared__ TileShared<float> sh[TPB];
-    if (done && *done) return;
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     const int q = blockIdx.x * TPB + g;
-    const bool active = q < n;
-    const int tile = active ? list[q] : 0;
+    const int tile = q < n ? list[q] : 0;
+    const bool active = q < n && !tile_done(tp, S, tile);
     TileMeta m;
     V4<float> own;
     if (active) {
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __re
     if (!active) return;
     const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
     const V4<float> b = ld4(R + (size_t)tile * kTileCells + t * 4);
-    const LevelConst<float> L(tp.h0, meta_level(m.packed));
+    const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
     float ax[4], d[4];
     neg_lap4<float, true>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
     const TileIdx ix(t);
@@ -236,17 +239,17 @@ __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __re
 // writes of one sweep are made visible to the next sweep's halo loads by __syncthreads.
 __global__ void __launch_bounds__(1024) k_gs_sequence(Topo tp, const int* __restrict__ list, int n, float* X,
                                                       const float* __restrict__ R, uint32_t colors, int nsweeps,
-                                                      const int* __restrict__ done) {
+                                                      const Scalars* __restrict__ S) {
+    pdl_entry();
     __shared__ TileShared<float> sh[8];
-    if (done && *done) return;
     const int groups = blockDim.x >> 7;
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     for (int s = 0; s < nsweeps; s++) {
         const int color = (colors >> s) & 1;
         for (int base = 0; base < n; base += groups) {
             const int q = base + g;
-            const bool active = q < n;
-            const int tile = active ? list[q] : 0;
+            const int tile = q < n ? list[q] : 0;
+            const bool active = q < n && !tile_done(tp, S, tile);
             TileMeta m;
             V4<float> own;
             if (active) {
@@ -257,7 +260,7 @@ __global__ void __launch_bounds__(1024) k_gs_sequence(Topo tp, const int* __rest
             if (active) {
                 const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
                 const V4<float> b = ld4(R + (size_t)tile * kTileCells + t * 4);
-                const LevelConst<float> L(tp.h0, meta_level(m.packed));
+                const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
                 float ax[4], d[4];
                 neg_lap4<float, true>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
                 const TileIdx ix(t);
@@ -283,13 +286,13 @@ __global__ void __launch_bounds__(1024) k_gs_sequence(Topo tp, const int* __rest
 template <int TPB>
 __global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int first, int n, const float* __restrict__ X,
                                                                  const float* RHS, float* C, float one_over_alpha,
-                                                                 const int* __restrict__ done) {
+                                                                 const Scalars* __restrict__ S) {
+    pdl_entry();
     __shared__ TileShared<float> sh[TPB];
-    if (done && *done) return;
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     const int q = blockIdx.x * TPB + g;
-    const bool active = q < n;
-    const int tile = first + (active ? q : 0);
+    const int tile = first + (q < n ? q : 0);
+    const bool active = q < n && !tile_done(tp, S, tile);
     TileMeta m;
     if (active) {
         m = tp.meta[tile];
@@ -300,7 +303,7 @@ __global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int fi
     if (active) {
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
         const V4<float> b = ld4(RHS + (size_t)tile * kTileCells + t * 4);
-        const LevelConst<float> L(tp.h0, meta_level(m.packed));
+        const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
         float ax[4], d[4];
         neg_lap4<float, false>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
 #pragma unroll
@@ -333,11 +336,12 @@ __global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int fi
 // ProlongateAndUpdate128Kernel (src/GMGSolver.cu:345-376): injection of the parent value;
 // GHOST: x = cx, others: x += prolong_coeff * cx; INTERIOR cells only (0 elsewhere).
 __global__ void __launch_bounds__(128) k_prolongate(Topo tp, int first, int n, const float* __restrict__ CX, float* FX,
-                                                    float prolong_coeff, const int* __restrict__ done) {
-    if (done && *done) return;
+                                                    float prolong_coeff, const Scalars* __restrict__ S) {
+    pdl_entry();
     const int q = blockIdx.x;
     if (q >= n) return;
     const int tile = first + q;
+    if (tile_done(tp, S, tile)) return;
     const int t = threadIdx.x;
     const TileMeta m = tp.meta[tile];
     const TileIdx ix(t);
@@ -365,11 +369,12 @@ __global__ void __launch_bounds__(128) k_prolongate(Topo tp, int first, int n, c
 // V-cycle initialisation (src/GMGSolver.cu:386-403): x = 0 everywhere; rhs = f on LEAF and
 // NONLEAF tiles, 0 on GHOST tiles.
 __global__ void __launch_bounds__(256) k_vcycle_init(Topo tp, int n, float* X, float* RHS, const float* __restrict__ F,
-                                                     const int* __restrict__ done) {
-    if (done && *done) return;
+                                                     const Scalars* __restrict__ S) {
+    pdl_entry();
     const size_t nv = (size_t)n * (kTileCells / 4);
     for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
         const int tile = (int)(v >> 7);
+        if (tile_done(tp, S, tile)) continue;
         const bool ghost = meta_type(tp.meta[tile].packed) & GHOST_T;
         st4(X + v * 4, zero4<float>());
         st4(RHS + v * 4, ghost ? zero4<float>() : ld4(F + v * 4));
@@ -443,8 +448,14 @@ __device__ __forceinline__ void set_cond(const SolveCtl& c, unsigned int v) {
     if (c.use_cond) cudaGraphSetConditional(c.cond, v);
 }
 
-// Scalar epilogues of the PCG (src/GMGSolver.cu:540-653), executed by one thread.
-__device__ void epilogue(int which, const Double2& tot, Scalars* S, const SolveCtl& c) {
+// Instance `inst` stops iterating: the last instance to stop ends the graph's while loop.
+__device__ __forceinline__ void finish(Scalars* S, const SolveCtl& c) {
+    S->done = 1;
+    if (c.active && atomicSub(c.active, 1) == 1) set_cond(c, 0u);
+}
+
+// Scalar epilogues of the PCG (src/GMGSolver.cu:540-653) for one instance, executed by one thread.
+__device__ void epilogue(int which, const Double2& tot, Scalars* S, const InstParams& P, const SolveCtl& c, int inst) {
     switch (which) {
     case EPI_INIT: {  // rhs_norm2, zero-RHS early exit, threshold
         S->rhs2 = tot.a;
@@ -452,14 +463,14 @@ __device__ void epilogue(int which, const Double2& tot, Scalars* S, const SolveC
         S->converged = 0;
         if (c.sync_stride > 0) {
             if (tot.a == 0.0) {
-                S->done = 1; S->converged = 1; S->iters = 0; S->rel = 0.0;
-                set_cond(c, 0u);
+                S->converged = 1; S->iters = 0; S->rel = 0.0;
+                finish(S, c);
                 return;
             }
-            double thr = c.tol * c.tol * tot.a;
+            const double thr = P.tol * P.tol * tot.a;
             S->thr2 = thr > 2.2250738585072014e-308 ? thr : 2.2250738585072014e-308;
         }
-        if (c.max_iters <= 0) set_cond(c, 0u);
+        if (P.max_iters <= 0) finish(S, c);
         break;
     }
     case EPI_GAMMA: S->gamma = tot.a; break;
@@ -469,19 +480,19 @@ __device__ void epilogue(int which, const Double2& tot, Scalars* S, const SolveC
         S->iter = i + 1;
         S->res2 = tot.a;
         if (c.sync_stride > 0 && (i + 1) % c.sync_stride == 0) {
-            if (c.history && i < c.history_cap) c.history[i] = sqrt(tot.a / S->rhs2);
+            if (inst == 0 && c.history && i < c.history_cap) c.history[i] = sqrt(tot.a / S->rhs2);
             if (tot.a < S->thr2) {
-                S->done = 1; S->converged = 1; S->iters = i + 1; S->rel = sqrt(tot.a / S->rhs2);
-                set_cond(c, 0u);
+                S->converged = 1; S->iters = i + 1; S->rel = sqrt(tot.a / S->rhs2);
+                finish(S, c);
                 return;
             }
             if (!(tot.a == tot.a) || isinf(tot.a)) {  // non-finite residual: stop, report
-                S->done = 1; S->nonfinite = 1; S->iters = i + 1; S->rel = tot.a;
-                set_cond(c, 0u);
+                S->nonfinite = 1; S->iters = i + 1; S->rel = tot.a;
+                finish(S, c);
                 return;
             }
         }
-        if (i + 1 >= c.max_iters) set_cond(c, 0u);
+        if (i + 1 >= P.max_iters) finish(S, c);
         break;
     }
     case EPI_BETA: S->gamma_old = S->gamma; S->gamma = tot.a; S->beta = tot.a / S->gamma_old; break;
@@ -496,23 +507,94 @@ __device__ void epilogue(int which, const Double2& tot, Scalars* S, const SolveC
     }
 }
 
-// Reduction kernel over the 4-cell vectors of LEAF tiles.  OP selects the fused elementwise
-// work done while reducing:
-//   OP_DOT       a.b                                  (Dot)
-//   OP_INIT      x = 0; r.r                           (Fill + Dot, src/GMGSolver.cu:537-542)
-//   OP_COPY_DOT  p = z; z.r                           (Copy + DotAsync, :564-568)
-//   OP_XR        x += a p, r -= a Ap (INTERIOR); r.r  (:587-612)
-//   OP_MEAN      (sum of 4 values, 2*#INTERIOR)       (MeanAsync, src/PoissonGrid.cu:231-325)
-template <int OP>
-__global__ void __launch_bounds__(256) k_leaf_reduce(Topo tp, const int* __restrict__ leaves, int nleaf, float* A, float* B,
-                                                     float* C, float* D, Scalars* S, SolveCtl ctl, int epi,
-                                                     double* partials, unsigned int* counter, int skip_if_done) {
-    if (skip_if_done && S->done) return;
-    double acc_a = 0.0, acc_b = 0.0;
+// Whole-grid dot over the 4-cell vectors of LEAF tiles (Dot, src/PoissonGrid.cu:199-228):
+// grid-stride over the leaf list, per-vector FP32 products widened to FP64, the two-level
+// deterministic sum of reduce_and_elect; the sum goes to S->gamma.
+__global__ void __launch_bounds__(256) k_leaf_dot(const int* __restrict__ leaves, int nleaf, const float* __restrict__ A,
+                                                  const float* __restrict__ B, Scalars* S, double* partials,
+                                                  unsigned int* counter) {
+    pdl_entry();
+    double acc = 0.0;
     const size_t nv = (size_t)nleaf * 128;
-    float alpha = 0.f;
-    if (OP == OP_XR) alpha = (float)S->alpha;
     for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+        const size_t off = (size_t)leaves[v >> 7] * kTileCells + (v & 127) * 4;
+        acc += dot4f(ld4(A + off), ld4(B + off));
+    }
+    Double2 tot{0.0, 0.0};
+    if (reduce_and_elect(acc, 0.0, partials, counter, tot)) S->gamma = tot.a;
+}
+
+// Block-reduce (a, b) of one chunk, publish it as the chunk's partial, and in thread 0 of the
+// instance's last chunk CTA return true with the instance's total, the chunk partials added in
+// chunk order (fixed: the bits depend only on the instance's own data).
+__device__ __forceinline__ bool chunk_reduce_and_elect(double a, double b, double* partials, unsigned int* counter, int2 ich,
+                                                       Double2& tot) {
+    __shared__ double wa[32], wb[32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) { wa[w] = a; wb[w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        a = lane < nw ? wa[lane] : 0.0;
+        b = lane < nw ? wb[lane] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+        if (lane == 0) {
+            partials[2 * blockIdx.x] = a;
+            partials[2 * blockIdx.x + 1] = b;
+            __threadfence();
+            const unsigned int ticket = atomicAdd(counter, 1u);
+            last = (ticket == (unsigned int)ich.y - 1u);
+        }
+    }
+    __syncthreads();
+    if (!last) return false;
+    if (w == 0) {
+        __threadfence();
+        double sa = 0.0, sb = 0.0;
+        for (int i = lane; i < ich.y; i += 32) {
+            sa += __ldcg(partials + 2 * (ich.x + i));
+            sb += __ldcg(partials + 2 * (ich.x + i) + 1);
+        }
+        sa = warp_sum(sa);
+        sb = warp_sum(sb);
+        if (lane == 0) {
+            tot.a = sa;
+            tot.b = sb;
+            *counter = 0u;
+        }
+    }
+    return threadIdx.x == 0;
+}
+
+// Per-instance reduction over the 4-cell vectors of LEAF tiles, one CTA per chunk (the chunk table
+// cuts every instance's leaf vectors into pieces of kChunkVecs).  OP selects the fused
+// elementwise work done while reducing:
+//   OP_DOT       a.b                                  (Dot)
+//   OP_INIT      x = 0; D = r; r.r                    (Fill + Dot, src/GMGSolver.cu:537-542)
+//   OP_COPY_DOT  p = z; z.r                           (Copy + DotAsync, :564-568)
+//   OP_XR        x += a p, r -= a Ap (INTERIOR); D = r; r.r  (:587-612)
+//   OP_MEAN      (sum of 4 values, 2*#INTERIOR)       (MeanAsync, src/PoissonGrid.cu:231-325)
+//   OP_PAP       Ap += ghost partial sums (C); p.Ap    (the tail of the fused Laplacian + Dot)
+// skip: SKIP_DONE leaves out finished instances, SKIP_INACTIVE only those outside the solve;
+// OP_MEAN also leaves out instances that are not pure Neumann.
+template <int OP>
+__global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restrict__ leaves, const int4* __restrict__ chunks,
+                                                     const int2* __restrict__ inst_chunks, float* A, float* B, float* C, float* D,
+                                                     Scalars* S, const InstParams* __restrict__ ip, SolveCtl ctl, int epi,
+                                                     double* partials, unsigned int* counters, int skip) {
+    pdl_entry();
+    const int4 ch = chunks[blockIdx.x];
+    const int inst = ch.x;
+    Scalars* Si = S + inst;
+    const InstParams P = ip[inst];
+    if (!P.active || (skip == SKIP_DONE && Si->done) || (OP == OP_MEAN && !P.pure_neumann)) return;
+    double acc_a = 0.0, acc_b = 0.0;
+    float alpha = 0.f;
+    if (OP == OP_XR) alpha = (float)Si->alpha;
+    for (int v = ch.y + threadIdx.x; v < ch.z; v += blockDim.x) {
         const int tile = leaves[v >> 7];
         const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
         if (OP == OP_DOT) {
@@ -544,7 +626,7 @@ __global__ void __launch_bounds__(256) k_leaf_reduce(Topo tp, const int* __restr
         } else if (OP == OP_PAP) {  // A = p, B = Ap, C = ghost partial sums: Ap += ghost sums; p.Ap
             const V4<float> p = ld4(A + off);
             V4<float> ap = ld4(B + off);
-            const int qv = (int)(v & 127);
+            const int qv = v & 127;
             const int i = qv >> 4, j = (qv >> 1) & 7, k0 = (qv & 1) * 4;
             const int gs = tp.ghost_child[(size_t)tile * 8 + ((i >> 2) | ((j >> 2) << 1) | ((k0 >> 2) << 2))];
             if (gs >= 0) {
@@ -562,17 +644,42 @@ __global__ void __launch_bounds__(256) k_leaf_reduce(Topo tp, const int* __restr
         }
     }
     Double2 tot{0.0, 0.0};
-    if (reduce_and_elect(acc_a, acc_b, partials, counter, tot)) epilogue(epi, tot, S, ctl);
+    if (chunk_reduce_and_elect(acc_a, acc_b, partials, counters + inst, inst_chunks[inst], tot)) epilogue(epi, tot, Si, P, ctl, inst);
 }
 
-// p = z + beta p on INTERIOR cells of LEAF tiles (src/GMGSolver.cu:642-653).
+// Start of a solve: per-instance scalars zeroed, instances outside the solve marked done, the
+// count of iterating instances set (0 ends the graph's loop at once).
+__global__ void __launch_bounds__(256) k_begin(Scalars* S, const InstParams* __restrict__ ip, int ninst, SolveCtl ctl) {
+    pdl_entry();
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    int mine = 0;
+    for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
+        Scalars z;
+        memset(&z, 0, sizeof(z));
+        z.done = ip[i].active ? 0 : 1;
+        S[i] = z;
+        mine += ip[i].active ? 1 : 0;
+    }
+    atomicAdd(&cnt, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *ctl.active = cnt;
+        if (cnt == 0) set_cond(ctl, 0u);
+    }
+}
+
+// p = z + beta p on INTERIOR cells of LEAF tiles (src/GMGSolver.cu:642-653), per instance.
 __global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict__ leaves, int nleaf, float* P,
                                                   const float* __restrict__ Z, const Scalars* S) {
-    if (S->done) return;
-    const float beta = (float)S->beta;
+    pdl_entry();
     const size_t nv = (size_t)nleaf * 128;
     for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
         const int tile = leaves[v >> 7];
+        const Scalars& Si = S[tp.inst[tile]];
+        if (Si.done) continue;
+        const float beta = (float)Si.beta;
         const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
         const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
         V4<float> p = ld4(P + off);
@@ -584,15 +691,18 @@ __global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict
     }
 }
 
-// r -= mean on INTERIOR cells of LEAF tiles (ReCenterLeafVoxels, src/PoissonSolver.cu:356-368);
-// RC (optional) receives a copy of the recentred r (the multigrid right-hand side).
+// r -= mean on INTERIOR cells of LEAF tiles (ReCenterLeafVoxels, src/PoissonSolver.cu:356-368)
+// of the pure-Neumann instances still iterating; RC (optional) receives a copy of the recentred r
+// (the multigrid right-hand side).
 __global__ void __launch_bounds__(256) k_recenter(Topo tp, const int* __restrict__ leaves, int nleaf, float* R,
-                                                  const Scalars* S, int skip_if_done, float* RC) {
-    if (skip_if_done && S->done) return;
-    const double mean = S->mean;
+                                                  const Scalars* S, const InstParams* __restrict__ ip, float* RC) {
+    pdl_entry();
     const size_t nv = (size_t)nleaf * 128;
     for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
         const int tile = leaves[v >> 7];
+        const int inst = tp.inst[tile];
+        if (S[inst].done || !ip[inst].pure_neumann) continue;
+        const double mean = S[inst].mean;
         const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
         const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
         V4<float> r = ld4(R + off);
@@ -605,13 +715,16 @@ __global__ void __launch_bounds__(256) k_recenter(Topo tp, const int* __restrict
 }
 
 // ------------------------------------------------------------------ FP64 defect correction
-// b - A x in FP64 for INTERIOR cells of LEAF tiles (0 elsewhere), with x held in FP64.  The
-// FP64 operator is the same FullNegativeLaplacian with FP64 coefficients.
+// b - A x in FP64 for INTERIOR cells of LEAF tiles (0 elsewhere), with x held in FP64, for the
+// active instances.  The FP64 operator is the same FullNegativeLaplacian with FP64 coefficients.
 __global__ void __launch_bounds__(256) k_residual64(Topo tp, const int* __restrict__ leaves, int nleaf, const float* __restrict__ B,
-                                                    const double* __restrict__ AX, double* R64, float* R32) {
+                                                    const double* __restrict__ AX, double* R64, float* R32,
+                                                    const InstParams* __restrict__ ip) {
+    pdl_entry();
     const size_t nv = (size_t)nleaf * 128;
     for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
         const int tile = leaves[v >> 7];
+        if (!ip[tp.inst[tile]].active) continue;
         const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
         const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
         const V4<float> b = ld4(B + off);
@@ -628,12 +741,14 @@ __global__ void __launch_bounds__(256) k_residual64(Topo tp, const int* __restri
     }
 }
 
-// x64 += e (FP32 correction) on INTERIOR cells of LEAF tiles.
+// x64 += e (FP32 correction) on INTERIOR cells of LEAF tiles of the active instances.
 __global__ void __launch_bounds__(256) k_accumulate_correction(Topo tp, const int* __restrict__ leaves, int nleaf, double* X64,
-                                                               float* E) {
+                                                               float* E, const InstParams* __restrict__ ip) {
+    pdl_entry();
     const size_t nv = (size_t)nleaf * 128;
     for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
         const int tile = leaves[v >> 7];
+        if (!ip[tp.inst[tile]].active) continue;
         const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
         const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
         V4<double> x = ld4(X64 + off);
@@ -645,15 +760,17 @@ __global__ void __launch_bounds__(256) k_accumulate_correction(Topo tp, const in
     }
 }
 
-// FP64 sum of squares of an FP64 leaf channel (norms of the defect-correction loop).
-__global__ void __launch_bounds__(256) k_norm64(const int* __restrict__ leaves, int nleaf, const double* __restrict__ A,
-                                                const float* __restrict__ B32, double* partials, unsigned int* counter,
-                                                double* out) {
+// Per-instance FP64 sum of squares of a leaf channel (FP64 A, or FP32 B32 widened) into
+// out[instance], chunked like k_inst_reduce (every instance, active or not).
+__global__ void __launch_bounds__(256) k_inst_norm64(const int* __restrict__ leaves, const int4* __restrict__ chunks,
+                                                     const int2* __restrict__ inst_chunks, const double* __restrict__ A,
+                                                     const float* __restrict__ B32, double* partials, unsigned int* counters,
+                                                     double* out) {
+    pdl_entry();
+    const int4 ch = chunks[blockIdx.x];
     double acc = 0.0;
-    const size_t nv = (size_t)nleaf * 128;
-    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
-        const int tile = leaves[v >> 7];
-        const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
+    for (int v = ch.y + threadIdx.x; v < ch.z; v += blockDim.x) {
+        const size_t off = (size_t)leaves[v >> 7] * kTileCells + (v & 127) * 4;
         if (A) {
             const V4<double> a = ld4(A + off);
             acc += a.v[0] * a.v[0] + a.v[1] * a.v[1] + a.v[2] * a.v[2] + a.v[3] * a.v[3];
@@ -663,14 +780,16 @@ __global__ void __launch_bounds__(256) k_norm64(const int* __restrict__ leaves, 
         }
     }
     Double2 tot{0.0, 0.0};
-    if (reduce_and_elect(acc, 0.0, partials, counter, tot)) *out = tot.a;
+    if (chunk_reduce_and_elect(acc, 0.0, partials, counters + ch.x, inst_chunks[ch.x], tot)) out[ch.x] = tot.a;
 }
 
 // float -> double and double -> float channel copies over all tiles
 __global__ void k_widen(const float* __restrict__ a, double* b, size_t n) {
+    pdl_entry();
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = (double)a[i];
 }
 __global__ void k_narrow(const double* __restrict__ a, float* b, size_t n) {
+    pdl_entry();
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
 }
 
@@ -680,152 +799,157 @@ namespace launch {
 constexpr int kTPB = 2;  // tiles per CTA of the stencil kernels
 
 template <class T>
-void propagate_ghosts(const DevGrid& g, T* X, const int* done, cudaStream_t s) {
+void propagate_ghosts(const DevGrid& g, T* X, const Scalars* S, cudaStream_t s) {
     if (g.n_ghost == 0) return;
     ++g.launch_count;
-    k_propagate_ghosts<T><<<g.n_ghost, 128, 0, s>>>(g.topo, g.d_ghost, g.n_ghost, X, done);
+    launch_kernel(k_propagate_ghosts<T>, g.n_ghost, 128, 0, s, g.topo, g.d_ghost, g.n_ghost, X, S);
 }
 template <class T>
-void laplacian_tiles(const DevGrid& g, const T* X, T* Y, const int* done, cudaStream_t s) {
+void laplacian_tiles(const DevGrid& g, const T* X, T* Y, const Scalars* S, cudaStream_t s) {
     if (g.n_leafghost == 0) return;
     ++g.launch_count;
-    k_laplacian<T, kTPB><<<(g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.d_leafghost, g.n_leafghost, X, Y, done);
+    launch_kernel(k_laplacian<T, kTPB>, (g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.d_leafghost, g.n_leafghost,
+                  X, Y, S);
 }
 template <class T>
-void accumulate_ghosts(const DevGrid& g, T* Y, const int* done, cudaStream_t s) {
+void accumulate_ghosts(const DevGrid& g, T* Y, const Scalars* S, cudaStream_t s) {
     if (g.n_ghost == 0) return;
     ++g.launch_count;
-    k_accumulate_ghosts<T><<<g.n_ghost, 64, 0, s>>>(g.topo, g.d_ghost, g.n_ghost, Y, done);
+    launch_kernel(k_accumulate_ghosts<T>, g.n_ghost, 64, 0, s, g.topo, g.d_ghost, g.n_ghost, Y, S);
 }
 template <class T>
-void full_laplacian(const DevGrid& g, T* X, T* Y, const int* done, cudaStream_t s) {
-    propagate_ghosts<T>(g, X, done, s);
-    laplacian_tiles<T>(g, X, Y, done, s);
-    accumulate_ghosts<T>(g, Y, done, s);
+void full_laplacian(const DevGrid& g, T* X, T* Y, const Scalars* S, cudaStream_t s) {
+    propagate_ghosts<T>(g, X, S, s);
+    laplacian_tiles<T>(g, X, Y, S, s);
+    accumulate_ghosts<T>(g, Y, S, s);
 }
-template void full_laplacian<float>(const DevGrid&, float*, float*, const int*, cudaStream_t);
-template void full_laplacian<double>(const DevGrid&, double*, double*, const int*, cudaStream_t);
+template void full_laplacian<float>(const DevGrid&, float*, float*, const Scalars*, cudaStream_t);
+template void full_laplacian<double>(const DevGrid&, double*, double*, const Scalars*, cudaStream_t);
 
-void laplacian_fused(const DevGrid& g, const float* X, float* Y, const int* done, cudaStream_t s) {
+void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s) {
     if (g.n_leafghost == 0) return;
     ++g.launch_count;
-    k_laplacian_fused<kTPB><<<(g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.d_leafghost, g.n_leafghost, X, Y,
-                                                                                      g.d_gacc, done);
+    launch_kernel(k_laplacian_fused<kTPB>, (g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.d_leafghost,
+                  g.n_leafghost, X, Y, g.d_gacc, S);
 }
 
-void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const int* done, cudaStream_t s) {
+void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s) {
     const int n = g.mg_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    k_gs_sweep<kTPB><<<(n + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.d_mg + g.mg_offset[level], n, X, R, color, done);
+    launch_kernel(k_gs_sweep<kTPB>, (n + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.d_mg + g.mg_offset[level], n, X, R, color, S);
 }
 
-void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t colors, int nsweeps, const int* done,
+void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t colors, int nsweeps, const Scalars* S,
                  cudaStream_t s) {
     const int n = g.mg_count[level];
     if (n == 0 || nsweeps == 0) return;
     if (n <= 8) {
         ++g.launch_count;
-        k_gs_sequence<<<1, 128 * n, 0, s>>>(g.topo, g.d_mg + g.mg_offset[level], n, X, R, colors, nsweeps, done);
+        launch_kernel(k_gs_sequence, 1, 128 * n, 0, s, g.topo, g.d_mg + g.mg_offset[level], n, X, R, colors, nsweeps, S);
         return;
     }
-    for (int k = 0; k < nsweeps; k++) gs_sweep(g, level, X, R, (colors >> k) & 1, done, s);
+    for (int k = 0; k < nsweeps; k++) gs_sweep(g, level, X, R, (colors >> k) & 1, S, s);
 }
 
 void residual_restrict(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha,
-                       const int* done, cudaStream_t s) {
+                       const Scalars* S, cudaStream_t s) {
     const int n = g.level_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    k_residual_restrict<kTPB><<<(n + kTPB - 1) / kTPB, 128 * kTPB, 0, s>>>(g.topo, g.level_first[level], n, X, RHS, C,
-                                                                            one_over_alpha, done);
+    launch_kernel(k_residual_restrict<kTPB>, (n + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.level_first[level], n, X, RHS, C,
+                  one_over_alpha, S);
 }
 
-void prolongate(const DevGrid& g, int level, const float* CX, float* FX, float prolong_coeff, const int* done,
-                cudaStream_t s) {
+void prolongate(const DevGrid& g, int level, const float* CX, float* FX, float prolong_coeff, const Scalars* S, cudaStream_t s) {
     const int n = g.level_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    k_prolongate<<<n, 128, 0, s>>>(g.topo, g.level_first[level], n, CX, FX, prolong_coeff, done);
+    launch_kernel(k_prolongate, n, 128, 0, s, g.topo, g.level_first[level], n, CX, FX, prolong_coeff, S);
 }
 
-void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const int* done, cudaStream_t s) {
+void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const Scalars* S, cudaStream_t s) {
     const size_t nv = (size_t)g.n * 128;
     int blocks = (int)std::min<size_t>((nv + 255) / 256, (size_t)g.sm_count * 8);
     if (blocks < 1) blocks = 1;
     ++g.launch_count;
-    k_vcycle_init<<<blocks, 256, 0, s>>>(g.topo, g.n, X, RHS, F, done);
+    launch_kernel(k_vcycle_init, blocks, 256, 0, s, g.topo, g.n, X, RHS, F, S);
+}
+
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("CIRRUS_NO_PDL");
+        return !(e && e[0] == '1');
+    }();
+    return on;
 }
 
 int leaf_blocks(const DevGrid& g) { return g.red_blocks; }
 
-void leaf_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* D, Scalars* S, const SolveCtl& ctl,
-                 int epi, int skip_if_done, cudaStream_t s) {
-    const int blocks = leaf_blocks(g);
+void inst_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* D, const SolveCtl& ctl, int epi, int skip,
+                 cudaStream_t s) {
+    ++g.launch_count;
+#define CIRRUS_INST_REDUCE(OPV)                                                                                         \
+    launch_kernel(k_inst_reduce<OPV>, g.n_chunks, 256, 0, s, g.topo, g.d_leaf, g.d_chunks, g.d_inst_chunks, A, B, C, D, \
+                  g.d_scalars, g.d_iparams, ctl, epi, g.d_partials, g.d_counters, skip)
     switch (op) {
-    case OP_DOT:
-        ++g.launch_count;
-        k_leaf_reduce<OP_DOT><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
-        break;
-    case OP_INIT:
-        ++g.launch_count;
-        k_leaf_reduce<OP_INIT><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
-        break;
-    case OP_COPY_DOT:
-        ++g.launch_count;
-        k_leaf_reduce<OP_COPY_DOT><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
-        break;
-    case OP_XR:
-        ++g.launch_count;
-        k_leaf_reduce<OP_XR><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
-        break;
-    case OP_MEAN:
-        ++g.launch_count;
-        k_leaf_reduce<OP_MEAN><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
-        break;
-    case OP_PAP:
-        ++g.launch_count;
-        k_leaf_reduce<OP_PAP><<<blocks, 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, A, B, C, D, S, ctl, epi, g.d_partials, g.d_counter, skip_if_done);
-        break;
+    case OP_DOT: CIRRUS_INST_REDUCE(OP_DOT); break;
+    case OP_INIT: CIRRUS_INST_REDUCE(OP_INIT); break;
+    case OP_COPY_DOT: CIRRUS_INST_REDUCE(OP_COPY_DOT); break;
+    case OP_XR: CIRRUS_INST_REDUCE(OP_XR); break;
+    case OP_MEAN: CIRRUS_INST_REDUCE(OP_MEAN); break;
+    case OP_PAP: CIRRUS_INST_REDUCE(OP_PAP); break;
     }
+#undef CIRRUS_INST_REDUCE
+}
+
+void grid_dot(const DevGrid& g, const float* A, const float* B, cudaStream_t s) {
+    ++g.launch_count;
+    k_leaf_dot<<<leaf_blocks(g), 256, 0, s>>>(g.d_leaf, g.n_leaf, A, B, g.d_dot, g.d_partials, g.d_counter);
 }
 
 void leaf_dot_raw(const float* A, const float* B, const int* leaves, int nleaf, int blocks, double* partials,
                   unsigned int* counter, Scalars* S, cudaStream_t s) {
-    const SolveCtl ctl{};
-    k_leaf_reduce<OP_DOT><<<blocks, 256, 0, s>>>(Topo{}, leaves, nleaf, const_cast<float*>(A), const_cast<float*>(B), nullptr,
-                                                 nullptr, S, ctl, EPI_GAMMA, partials, counter, 0);
+    k_leaf_dot<<<blocks, 256, 0, s>>>(leaves, nleaf, A, B, S, partials, counter);
 }
 
-void update_p(const DevGrid& g, float* P, const float* Z, const Scalars* S, cudaStream_t s) {
+void begin_solve(const DevGrid& g, const SolveCtl& ctl, cudaStream_t s) {
     ++g.launch_count;
-    k_update_p<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, P, Z, S);
+    launch_kernel(k_begin, 1, 256, 0, s, g.d_scalars, g.d_iparams, g.num_inst, ctl);
 }
 
-void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cudaStream_t s, float* RC) {
+void update_p(const DevGrid& g, float* P, const float* Z, cudaStream_t s) {
     ++g.launch_count;
-    k_recenter<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, R, S, skip_if_done, RC);
+    launch_kernel(k_update_p, leaf_blocks(g), 256, 0, s, g.topo, g.d_leaf, g.n_leaf, P, Z, (const Scalars*)g.d_scalars);
+}
+
+void recenter(const DevGrid& g, float* R, float* RC, cudaStream_t s) {
+    ++g.launch_count;
+    launch_kernel(k_recenter, leaf_blocks(g), 256, 0, s, g.topo, g.d_leaf, g.n_leaf, R, (const Scalars*)g.d_scalars,
+                  (const InstParams*)g.d_iparams, RC);
 }
 
 void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s) {
     ++g.launch_count;
-    k_residual64<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, B, AX, R64, R32);
+    launch_kernel(k_residual64, leaf_blocks(g), 256, 0, s, g.topo, g.d_leaf, g.n_leaf, B, AX, R64, R32, (const InstParams*)g.d_iparams);
 }
 void accumulate_correction(const DevGrid& g, double* X64, float* E, cudaStream_t s) {
     ++g.launch_count;
-    k_accumulate_correction<<<leaf_blocks(g), 256, 0, s>>>(g.topo, g.d_leaf, g.n_leaf, X64, E);
+    launch_kernel(k_accumulate_correction, leaf_blocks(g), 256, 0, s, g.topo, g.d_leaf, g.n_leaf, X64, E,
+                  (const InstParams*)g.d_iparams);
 }
 void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s) {
     ++g.launch_count;
-    k_norm64<<<leaf_blocks(g), 256, 0, s>>>(g.d_leaf, g.n_leaf, A, B32, g.d_partials, g.d_counter, out);
+    launch_kernel(k_inst_norm64, g.n_chunks, 256, 0, s, (const int*)g.d_leaf, (const int4*)g.d_chunks, (const int2*)g.d_inst_chunks, A,
+                  B32, g.d_partials, g.d_counters, out);
 }
 void widen(const DevGrid& g, const float* a, double* b, size_t n, cudaStream_t s) {
     ++g.launch_count;
-    k_widen<<<(int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(a, b, n);
+    launch_kernel(k_widen, (int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s, a, b, n);
 }
 void narrow(const DevGrid& g, const double* a, float* b, size_t n, cudaStream_t s) {
     ++g.launch_count;
-    k_narrow<<<(int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(a, b, n);
+    launch_kernel(k_narrow, (int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s, a, b, n);
 }
 
 }  // namespace launch

@@ -16,6 +16,17 @@
 
 namespace cirrus {
 
+// Programmatic dependent launch.  Solve kernels are launched with programmatic stream
+// serialisation (launch_kernel), so a kernel's CTAs may be scheduled while its predecessor is
+// still running.  Every kernel first allows its own successor to be scheduled, then waits until
+// its predecessor grid has completed and that grid's memory operations are visible, before it
+// reads or writes anything; so results are those of plain stream order.  Without the launch
+// attribute both instructions return at once.
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 template <class T> struct alignas(4 * sizeof(T)) V4 { T v[4]; };
 
 template <class T> __device__ __forceinline__ V4<T> ld4(const T* p) { return *reinterpret_cast<const V4<T>*>(p); }

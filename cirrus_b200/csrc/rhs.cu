@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(128) k_divergence(Topo tp, const int* __restri
     const TileMeta m = tp.meta[tile];
     const int t = threadIdx.x;
     const uint8_t tt = (uint8_t)meta_type(m.packed);
-    const float h = tp.h0 / float(1 << meta_level(m.packed));
+    const float h = tile_h0(tp, tile) / float(1 << meta_level(m.packed));
     const float* U[3] = {U0, U1, U2};
     for (int e = 0; e < 4; e++) {
         const int o = t * 4 + e;

@@ -1,7 +1,10 @@
 // GMG-PCG driver: V-cycle schedule, the PCG loop captured as one CUDA graph with a device-side
 // while-conditional (no host round trip per iteration), and the FP64 defect-correction loop.
+// Every solve runs all active instances of a grid together: per-instance scalars and done flags,
+// one kernel per step for the whole batch; the loop ends when the last instance stops.
 #include "solver_internal.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -13,8 +16,8 @@ namespace cirrus {
 // GS(level_iters, order 0) + residual/restrict per level; coarsest GS(ci/2, 0) + GS(ci/2, 1);
 // upstroke prolongate + GS(level_iters, order 1).
 void vcycle(const DevGrid& g, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters, float one_over_alpha,
-            float prolong_coeff, const int* done, cudaStream_t s) {
-    launch::vcycle_init(g, X, RHS, F, done, s);
+            float prolong_coeff, const Scalars* S, cudaStream_t s) {
+    launch::vcycle_init(g, X, RHS, F, S, s);
     auto smooth = [&](int level, int iters, int order) {
         // GaussSeidelGMG: colours (order, 1-order) per iteration
         uint32_t colors = 0;
@@ -22,7 +25,7 @@ void vcycle(const DevGrid& g, float* X, const float* F, float* RHS, int level_it
         for (int it = 0; it < iters; it++) {
             for (int c : {order, 1 - order}) {
                 if (ns == 32) {
-                    launch::gs_sequence(g, level, X, RHS, colors, ns, done, s);
+                    launch::gs_sequence(g, level, X, RHS, colors, ns, S, s);
                     colors = 0;
                     ns = 0;
                 }
@@ -30,18 +33,18 @@ void vcycle(const DevGrid& g, float* X, const float* F, float* RHS, int level_it
                 ns++;
             }
         }
-        if (ns) launch::gs_sequence(g, level, X, RHS, colors, ns, done, s);
+        if (ns) launch::gs_sequence(g, level, X, RHS, colors, ns, S, s);
     };
     for (int l = g.max_level; l > 0; l--) {
         smooth(l, level_iters, 0);
-        launch::residual_restrict(g, l, X, RHS, RHS, one_over_alpha, done, s);
+        launch::residual_restrict(g, l, X, RHS, RHS, one_over_alpha, S, s);
     }
     {
         uint32_t colors = 0;
         int ns = 0;
         auto push = [&](int c) {
             if (ns == 32) {
-                launch::gs_sequence(g, 0, X, RHS, colors, ns, done, s);
+                launch::gs_sequence(g, 0, X, RHS, colors, ns, S, s);
                 colors = 0;
                 ns = 0;
             }
@@ -50,10 +53,10 @@ void vcycle(const DevGrid& g, float* X, const float* F, float* RHS, int level_it
         };
         for (int it = 0; it < coarsest_iters / 2; it++) { push(0); push(1); }
         for (int it = 0; it < coarsest_iters / 2; it++) { push(1); push(0); }
-        if (ns) launch::gs_sequence(g, 0, X, RHS, colors, ns, done, s);
+        if (ns) launch::gs_sequence(g, 0, X, RHS, colors, ns, S, s);
     }
     for (int l = 1; l <= g.max_level; l++) {
-        launch::prolongate(g, l, X, X, prolong_coeff, done, s);
+        launch::prolongate(g, l, X, X, prolong_coeff, S, s);
         smooth(l, level_iters, 1);
     }
 }
@@ -61,20 +64,20 @@ void vcycle(const DevGrid& g, float* X, const float* F, float* RHS, int level_it
 bool use_fused(const DevGrid& g, int level_iters, int coarsest_iters) {
     const char* e = std::getenv("CIRRUS_VCYCLE");
     if (e && std::strcmp(e, "generic") == 0) return false;
-    return level_iters == 1 && g.bottom_level >= 0 && launch::bottom_supported(coarsest_iters, std::min(g.bottom_level, g.max_level));
+    return level_iters == 1 && g.bottom_level >= 0 && launch::bottom_supported(coarsest_iters, g.bottom_level);
 }
 
 void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, float one_over_alpha, float prolong_coeff,
-                  const int* done, cudaStream_t s) {
-    const int lb = std::min(g.bottom_level, g.max_level);
+                  const Scalars* S, cudaStream_t s) {
+    const int lb = g.bottom_level;
     for (int l = g.max_level; l > lb; l--) {
-        launch::presmooth(g, l, g.d_xpre, RHS, done, s);
-        launch::residual_restrict(g, l, g.d_xpre, RHS, RHS, one_over_alpha, done, s);
+        launch::presmooth(g, l, g.d_xpre, RHS, S, s);
+        launch::residual_restrict(g, l, g.d_xpre, RHS, RHS, one_over_alpha, S, s);
     }
-    launch::bottom(g, lb, coarsest_iters, X, RHS, one_over_alpha, prolong_coeff, done, s);
+    launch::bottom(g, lb, coarsest_iters, X, RHS, one_over_alpha, prolong_coeff, S, s);
     for (int l = lb + 1; l <= g.max_level; l++) {
-        launch::prolong_sweep(g, l, X, g.d_xpre, RHS, prolong_coeff, done, s);
-        launch::gs_sweep(g, l, X, RHS, 0, done, s);
+        launch::prolong_sweep(g, l, X, g.d_xpre, RHS, prolong_coeff, S, s);
+        launch::gs_sweep(g, l, X, RHS, 0, S, s);
     }
 }
 
@@ -83,69 +86,65 @@ namespace {
 struct Ch {
     float *x, *r, *p, *ap, *z;
 };
+Ch channels(const DevGrid& g) { return {g.d_ch[kChX], g.d_ch[kChR], g.d_ch[kChP], g.d_ch[kChAp], g.d_ch[kChZ]}; }
 
 // z <- M^-1 r with the fused kernels when level_iters == 1 (RHS already holds r on LEAF tiles).
-void precondition(const DevGrid& g, const SolveParams& p, const int* done, cudaStream_t s) {
-    const Ch c{g.d_ch[kChX], g.d_ch[kChR], g.d_ch[kChP], g.d_ch[kChAp], g.d_ch[kChZ]};
-    if (use_fused(g, p.level_iters, p.coarsest_iters)) vcycle_fused(g, c.z, c.ap, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, done, s);
-    else vcycle(g, c.z, c.r, c.ap, p.level_iters, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, done, s);
+void precondition(const DevGrid& g, const SolveParams& p, cudaStream_t s) {
+    const Ch c = channels(g);
+    const Scalars* S = g.d_scalars;
+    if (use_fused(g, p.level_iters, p.coarsest_iters)) vcycle_fused(g, c.z, c.ap, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, S, s);
+    else vcycle(g, c.z, c.r, c.ap, p.level_iters, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, S, s);
 }
-Ch channels(const DevGrid& g) { return {g.d_ch[kChX], g.d_ch[kChR], g.d_ch[kChP], g.d_ch[kChAp], g.d_ch[kChZ]}; }
 
 // GMGSolver::solve, src/GMGSolver.cu:535-568
 void record_prologue(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl, cudaStream_t s) {
     const Ch c = channels(g);
-    Scalars* S = g.d_scalars;
-    const int* done = &S->done;
-    cudaMemsetAsync(S, 0, sizeof(Scalars), s);
+    launch::begin_solve(g, ctl, s);
     // the fused V-cycle reads GHOST right-hand sides (channel Ap) as stored: 0; nothing in the
     // fused iteration writes them
     if (use_fused(g, p.level_iters, p.coarsest_iters)) launch::zero_ghost_tiles(g, c.ap, s);
-    launch::leaf_reduce(OP_INIT, g, c.x, c.r, nullptr, c.ap, S, ctl, EPI_INIT, 0, s);
+    launch::inst_reduce(OP_INIT, g, c.x, c.r, nullptr, c.ap, ctl, EPI_INIT, SKIP_INACTIVE, s);
     if (p.pure_neumann) {
-        launch::leaf_reduce(OP_MEAN, g, c.r, nullptr, nullptr, nullptr, S, ctl, EPI_MEAN, 1, s);
-        launch::recenter(g, c.r, S, 1, s, c.ap);
+        launch::inst_reduce(OP_MEAN, g, c.r, nullptr, nullptr, nullptr, ctl, EPI_MEAN, SKIP_DONE, s);
+        launch::recenter(g, c.r, c.ap, s);
     }
-    precondition(g, p, done, s);
-    launch::leaf_reduce(OP_COPY_DOT, g, c.z, c.r, c.p, nullptr, S, ctl, EPI_GAMMA, 1, s);
+    precondition(g, p, s);
+    launch::inst_reduce(OP_COPY_DOT, g, c.z, c.r, c.p, nullptr, ctl, EPI_GAMMA, SKIP_DONE, s);
 }
 
 // One PCG iteration, src/GMGSolver.cu:573-653
 void record_body(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl, cudaStream_t s) {
     const Ch c = channels(g);
-    Scalars* S = g.d_scalars;
-    const int* done = &S->done;
     if (use_fused(g, p.level_iters, p.coarsest_iters)) {
-        launch::laplacian_fused(g, c.p, c.ap, done, s);
-        launch::leaf_reduce(OP_PAP, g, c.p, c.ap, g.d_gacc, nullptr, S, ctl, EPI_ALPHA, 1, s);
+        launch::laplacian_fused(g, c.p, c.ap, g.d_scalars, s);
+        launch::inst_reduce(OP_PAP, g, c.p, c.ap, g.d_gacc, nullptr, ctl, EPI_ALPHA, SKIP_DONE, s);
     } else {
-        launch::full_laplacian<float>(g, c.p, c.ap, done, s);
-        launch::leaf_reduce(OP_DOT, g, c.p, c.ap, nullptr, nullptr, S, ctl, EPI_ALPHA, 1, s);
+        launch::full_laplacian<float>(g, c.p, c.ap, g.d_scalars, s);
+        launch::inst_reduce(OP_DOT, g, c.p, c.ap, nullptr, nullptr, ctl, EPI_ALPHA, SKIP_DONE, s);
     }
-    launch::leaf_reduce(OP_XR, g, c.x, c.p, c.r, c.ap, S, ctl, EPI_CHECK, 1, s);
+    launch::inst_reduce(OP_XR, g, c.x, c.p, c.r, c.ap, ctl, EPI_CHECK, SKIP_DONE, s);
     if (p.pure_neumann) {
-        launch::leaf_reduce(OP_MEAN, g, c.r, nullptr, nullptr, nullptr, S, ctl, EPI_MEAN, 1, s);
-        launch::recenter(g, c.r, S, 1, s, c.ap);
+        launch::inst_reduce(OP_MEAN, g, c.r, nullptr, nullptr, nullptr, ctl, EPI_MEAN, SKIP_DONE, s);
+        launch::recenter(g, c.r, c.ap, s);
     }
-    precondition(g, p, done, s);
-    launch::leaf_reduce(OP_DOT, g, c.r, c.z, nullptr, nullptr, S, ctl, EPI_BETA, 1, s);
-    launch::update_p(g, c.p, c.z, S, s);
+    precondition(g, p, s);
+    launch::inst_reduce(OP_DOT, g, c.r, c.z, nullptr, nullptr, ctl, EPI_BETA, SKIP_DONE, s);
+    launch::update_p(g, c.p, c.z, s);
 }
 
 void record_epilogue(const DevGrid& g, const SolveCtl& ctl, cudaStream_t s) {
     const Ch c = channels(g);
-    launch::leaf_reduce(OP_DOT, g, c.r, c.r, nullptr, nullptr, g.d_scalars, ctl, EPI_FINAL, 0, s);
+    launch::inst_reduce(OP_DOT, g, c.r, c.r, nullptr, nullptr, ctl, EPI_FINAL, SKIP_INACTIVE, s);
 }
 
 SolveCtl make_ctl(const DevGrid& g, const SolveParams& p) {
     SolveCtl c{};
     c.sync_stride = p.sync_stride;
-    c.max_iters = p.max_iters;
-    c.tol = p.tol;
     c.history = g.d_history;
     c.history_cap = g.history_cap;
     c.use_cond = 0;
     c.cond = 0;
+    c.active = g.d_active;
     return c;
 }
 
@@ -225,17 +224,32 @@ DevGrid::SolveGraph build_graph(DevGrid& g, const SolveParams& p) {
     return out;
 }
 
-void fill_result(const DevGrid& g, SolveResult* r) {
-    const Scalars& S = *g.h_scalars;
-    r->iters = S.iters;
-    r->rel = S.rel;
-    r->status = S.nonfinite ? 6 : (S.converged ? 0 : 5);
+// Per-instance parameters of a solve into the pinned mirror and onto the device (ordered on s).
+void upload_params(DevGrid& g, const SolveParams& p, const InstRequest* req, cudaStream_t s) {
+    for (int i = 0; i < g.num_inst; i++) {
+        InstParams& q = g.h_iparams[i];
+        q.tol = (req && req[i].tol >= 0) ? req[i].tol : p.tol;
+        q.max_iters = p.max_iters;
+        q.active = req ? (req[i].active ? 1 : 0) : 1;
+        q.pure_neumann = (req && req[i].pure_neumann >= 0) ? req[i].pure_neumann : p.pure_neumann;
+        q.pad = 0;
+    }
+    cudaMemcpyAsync(g.d_iparams, g.h_iparams, sizeof(InstParams) * g.num_inst, cudaMemcpyHostToDevice, s);
+}
+
+bool any_pure_neumann(const DevGrid& g) {
+    for (int i = 0; i < g.num_inst; i++)
+        if (g.h_iparams[i].active && g.h_iparams[i].pure_neumann) return true;
+    return false;
 }
 
 }  // namespace
 
-int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r) {
-    GraphKey key{p.max_iters, p.level_iters, p.coarsest_iters, p.sync_stride, p.pure_neumann, p.tol, p.one_over_alpha, p.prolong_coeff,
+int pcg_solve(DevGrid& g, const SolveParams& p0, cudaStream_t s, SolveResult* r, const InstRequest* req) {
+    upload_params(g, p0, req, s);
+    SolveParams p = p0;
+    p.pure_neumann = any_pure_neumann(g) ? 1 : 0;
+    GraphKey key{0, p.level_iters, p.coarsest_iters, p.sync_stride, p.pure_neumann, p.one_over_alpha, p.prolong_coeff,
                  use_fused(g, p.level_iters, p.coarsest_iters) ? 1 : 0};
     DevGrid::SolveGraph sg;
     if (graphs_enabled()) {
@@ -259,25 +273,39 @@ int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r) 
         SolveCtl ctl = make_ctl(g, p);
         record_prologue(g, p, ctl, s);
         for (int i = 0; i < p.max_iters; i++) {
-            cudaMemcpyAsync(g.h_scalars, g.d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(g.h_scalars, g.d_scalars, sizeof(Scalars) * g.num_inst, cudaMemcpyDeviceToHost, s);
             cudaStreamSynchronize(s);
-            if (g.h_scalars->done) break;
+            bool all_done = true;
+            for (int k = 0; k < g.num_inst; k++) all_done = all_done && g.h_scalars[k].done;
+            if (all_done) break;
             record_body(g, p, ctl, s);
         }
         record_epilogue(g, ctl, s);
         direct = g.launch_count - c0;
     }
-    cudaMemcpyAsync(g.h_scalars, g.d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(g.h_scalars, g.d_scalars, sizeof(Scalars) * g.num_inst, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         g.last_error = std::string("solve: ") + cudaGetErrorString(e);
         return 2;
     }
-    fill_result(g, r);
-    // bodies executed = iterations entered (the counter is advanced once per body)
-    g.last_solve_launches = direct >= 0 ? direct : sg.prologue + (long long)g.h_scalars->iter * sg.body + sg.epilogue;
-    r->launches = g.last_solve_launches;
-    if (p.sync_stride <= 0) r->status = 0;
+    // bodies executed = the largest iteration count of the instances (each body advances every
+    // iterating instance's counter once)
+    int loops = 0;
+    for (int k = 0; k < g.num_inst; k++)
+        if (g.h_iparams[k].active) loops = std::max(loops, g.h_scalars[k].iter);
+    g.last_solve_launches = direct >= 0 ? direct : sg.prologue + (long long)loops * sg.body + sg.epilogue;
+    for (int k = 0; k < g.num_inst; k++) {
+        const Scalars& S = g.h_scalars[k];
+        SolveResult& o = r[k];
+        o = SolveResult();
+        o.iters = S.iters;
+        o.rel = S.rel;
+        o.status = S.nonfinite ? 6 : (S.converged ? 0 : 5);
+        if (p.sync_stride <= 0) o.status = 0;
+        if (!g.h_iparams[k].active) o.status = 0;
+        o.launches = g.last_solve_launches;
+    }
     return 0;
 }
 
@@ -295,11 +323,16 @@ int ensure_fp64(DevGrid& g) {
     return 0;
 }
 
-double read_norm(DevGrid& g, cudaStream_t s) {
-    double v = 0;
-    cudaMemcpyAsync(&v, g.d_norm, sizeof(double), cudaMemcpyDeviceToHost, s);
+// Per-instance norms computed on the device into host doubles.
+void read_norms(DevGrid& g, std::vector<double>& out, cudaStream_t s) {
+    out.assign(g.num_inst, 0.0);
+    cudaMemcpyAsync(out.data(), g.d_norm, sizeof(double) * g.num_inst, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
-    return v;
+}
+
+void set_active(DevGrid& g, const std::vector<uint8_t>& active, cudaStream_t s) {
+    for (int i = 0; i < g.num_inst; i++) g.h_iparams[i].active = active[i];
+    cudaMemcpyAsync(g.d_iparams, g.h_iparams, sizeof(InstParams) * g.num_inst, cudaMemcpyHostToDevice, s);
 }
 }  // namespace
 
@@ -307,74 +340,104 @@ int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s) {
     int rc = ensure_fp64(g);
     if (rc) return rc;
     const size_t cells = (size_t)g.n * kTileCells;
+    set_active(g, std::vector<uint8_t>(g.num_inst, 1), s);
+    std::vector<double> bb, rr;
     launch::norm64(g, nullptr, d_b, g.d_norm, s);
-    const double bb = read_norm(g, s);
+    read_norms(g, bb, s);
     if (!g.x64_valid) launch::widen(g, g.d_ch[kChX], g.d_x64, cells, s);
     launch::full_laplacian<double>(g, g.d_x64, g.d_ax64, nullptr, s);
     launch::residual64(g, d_b, g.d_ax64, g.d_r64, g.d_bsave, s);
     launch::norm64(g, g.d_r64, nullptr, g.d_norm, s);
-    const double rr = read_norm(g, s);
-    *rel = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+    read_norms(g, rr, s);
+    for (int i = 0; i < g.num_inst; i++) rel[i] = bb[i] > 0 ? std::sqrt(rr[i] / bb[i]) : 0.0;
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
-// FP64 defect correction: x64 accumulates FP32 PCG corrections e solving A e = r, with
-// r = b - A x64 formed in FP64 on the device; stops when ||r||/||b|| < tol (FP64 true residual).
-int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r) {
+// FP64 defect correction of every active instance: x64 accumulates FP32 PCG corrections e
+// solving A e = r, with r = b - A x64 formed in FP64 on the device; an instance stops when its
+// ||r||/||b|| < tol (FP64 true residual).  All instances still correcting share each inner solve.
+int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r, const InstRequest* req) {
     int rc = ensure_fp64(g);
     if (rc) return rc;
+    const int K = g.num_inst;
     const size_t cells = (size_t)g.n * kTileCells;
     const long long own0 = g.launch_count;
     long long inner_recorded = 0, inner_executed = 0;
+    std::vector<uint8_t> want(K), active(K);
+    std::vector<double> tol(K);
+    for (int i = 0; i < K; i++) {
+        want[i] = req ? (req[i].active ? 1 : 0) : 1;
+        tol[i] = (req && req[i].tol >= 0) ? req[i].tol : p.tol;
+        r[i] = SolveResult();
+        r[i].status = want[i] ? 5 : 0;
+    }
     cudaMemcpyAsync(g.d_bsave, g.d_ch[kChB], cells * sizeof(float), cudaMemcpyDeviceToDevice, s);
     if (p.warm_start) launch::widen(g, g.d_ch[kChX], g.d_x64, cells, s);
     else cudaMemsetAsync(g.d_x64, 0, cells * sizeof(double), s);
+    std::vector<double> bb, rr;
     launch::norm64(g, nullptr, g.d_bsave, g.d_norm, s);
-    const double bb = read_norm(g, s);
-    r->iters = 0;
-    r->outer = 0;
-    if (bb == 0.0) {
-        cudaMemsetAsync(g.d_ch[kChX], 0, cells * sizeof(float), s);
-        r->rel = 0;
-        r->true_rel = 0;
-        r->status = 0;
-        r->launches = g.launch_count - own0;
-        return cudaStreamSynchronize(s) == cudaSuccess ? 0 : 2;
+    read_norms(g, bb, s);
+    for (int i = 0; i < K; i++) {
+        active[i] = want[i] && bb[i] != 0.0;
+        if (want[i] && bb[i] == 0.0) {  // zero right-hand side: x = 0
+            r[i].status = 0;
+            r[i].rel = 0;
+            r[i].true_rel = 0;
+        }
     }
-    double rel = 1.0;
-    r->status = 5;
+    std::vector<double> rel(K, 1.0);
     for (int k = 0; k <= p.max_outer; k++) {
+        set_active(g, active, s);
         launch::full_laplacian<double>(g, g.d_x64, g.d_ax64, nullptr, s);
         launch::residual64(g, g.d_bsave, g.d_ax64, g.d_r64, g.d_ch[kChB], s);
         launch::norm64(g, g.d_r64, nullptr, g.d_norm, s);
-        rel = std::sqrt(read_norm(g, s) / bb);
-        if (!(rel == rel)) { r->status = 6; break; }
-        if (rel < p.tol) { r->status = 0; break; }
-        if (k == p.max_outer) break;
-        // each inner FP32 solve targets the defect that leaves the outer residual just under
-        // tol, but never tighter than inner_tol (where FP32 stalls) nor looser than 0.1
+        read_norms(g, rr, s);
+        bool any = false;
+        std::vector<InstRequest> inner(K);
+        for (int i = 0; i < K; i++) {
+            inner[i].active = 0;
+            if (!active[i]) continue;
+            rel[i] = std::sqrt(rr[i] / bb[i]);
+            if (!(rel[i] == rel[i])) { r[i].status = 6; active[i] = 0; continue; }
+            if (rel[i] < tol[i]) { r[i].status = 0; active[i] = 0; continue; }
+            if (k == p.max_outer) { active[i] = 0; continue; }
+            // each inner FP32 solve targets the defect that leaves the outer residual just under
+            // tol, but never tighter than inner_tol (where FP32 stalls) nor looser than 0.1
+            double tau = 0.5 * tol[i] / rel[i];
+            tau = std::min(0.1, std::max(p.inner_tol, tau));
+            inner[i].active = 1;
+            inner[i].tol = tau;
+            any = true;
+        }
+        if (!any) break;
         SolveParams ip = p;
         ip.precision = 0;
-        double tau = 0.5 * p.tol / rel;
-        tau = std::min(0.1, std::max(p.inner_tol, tau));
-        ip.tol = tau;
-        SolveResult ir;
+        std::vector<SolveResult> ir(K);
         const long long a = g.launch_count;
-        int e = pcg_solve(g, ip, s, &ir);
+        int e = pcg_solve(g, ip, s, ir.data(), inner.data());
         if (e) return e;
         inner_recorded += g.launch_count - a;
-        inner_executed += ir.launches;
-        r->iters += ir.iters;
-        r->outer++;
+        inner_executed += ir[0].launches;
+        for (int i = 0; i < K; i++)
+            if (inner[i].active) {
+                r[i].iters += ir[i].iters;
+                r[i].outer++;
+            }
+        // the inner solve left the active flags of this step on the device
         launch::accumulate_correction(g, g.d_x64, g.d_ch[kChX], s);
     }
     launch::narrow(g, g.d_x64, g.d_ch[kChX], cells, s);
     g.x64_valid = true;
-    r->launches = (g.launch_count - own0 - inner_recorded) + inner_executed;
-    g.last_solve_launches = r->launches;
+    const long long launches = (g.launch_count - own0 - inner_recorded) + inner_executed;
+    g.last_solve_launches = launches;
+    for (int i = 0; i < K; i++) {
+        if (want[i] && bb[i] != 0.0) {
+            r[i].rel = rel[i];
+            r[i].true_rel = rel[i];
+        }
+        r[i].launches = launches;
+    }
     // b channel ends as the last FP32 defect, mirroring "b channel will be modified"
-    r->rel = rel;
-    r->true_rel = rel;
     return cudaStreamSynchronize(s) == cudaSuccess ? 0 : 2;
 }
 

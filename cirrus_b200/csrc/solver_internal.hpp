@@ -5,6 +5,7 @@
 #include "common.cuh"
 
 #include <cuda_runtime.h>
+#include <array>
 #include <cstdint>
 #include <map>
 #include <string>
@@ -15,48 +16,65 @@ namespace cirrus {
 
 class Topology;
 
-// Scalar state of one PCG solve, resident in device memory (the reference keeps gamma, beta,
-// alpha, gamma_old, fp, mean, count as 7 device doubles, src/GMGSolver.h:22-30).
-struct Scalars {
-    double rhs2, thr2, gamma, gamma_old, beta, alpha, fp, res2, mean, rel;
-    int iter, iters, done, converged, nonfinite, pad;
-};
-
-// Per-solve constants passed by value to the reduction kernels.
+// Per-solve constants passed by value to the reduction kernels (tolerances and iteration caps are
+// per instance, in InstParams).
 struct SolveCtl {
     int sync_stride;
-    int max_iters;
-    double tol;
-    double* history;       // optional per-iteration relative residuals (device)
+    double* history;       // optional per-iteration relative residuals of instance 0 (device)
     int history_cap;
     int use_cond;          // 1 when running inside a graph with a while-conditional node
     cudaGraphConditionalHandle cond;
+    int* active;           // instances still iterating; the last to stop ends the graph's loop
+};
+
+constexpr int kBottomMaxLevels = 16;
+// Coarse-level boxes of one instance for the shared-memory coarse-level kernel: its tile records
+// (rec_off.., level-major), its stencil codes (code_off.., cells, a multiple of 8), and per level
+// the record range and the box strides.
+struct BottomInst {
+    int rec_off, nrec, code_off, cells;
+    int first[kBottomMaxLevels], cnt[kBottomMaxLevels], sy[kBottomMaxLevels], sz[kBottomMaxLevels];
 };
 
 enum { OP_DOT = 0, OP_INIT = 1, OP_COPY_DOT = 2, OP_XR = 3, OP_MEAN = 4, OP_PAP = 5 };
+enum { SKIP_INACTIVE = 0, SKIP_DONE = 1 };  // which instances a reduction leaves out
+constexpr int kChunkVecs = 1024;            // 4-cell vectors per reduction chunk (one CTA)
 enum { EPI_NONE = -1, EPI_INIT = 0, EPI_GAMMA = 1, EPI_ALPHA = 2, EPI_CHECK = 3, EPI_BETA = 4, EPI_MEAN = 5, EPI_FINAL = 6 };
 
 struct GraphKey {
     int max_iters, level_iters, coarsest_iters, sync_stride, pure_neumann;
-    double tol;
     float one_over_alpha, prolong_coeff;
     int fused;
     bool operator<(const GraphKey& o) const {
-        return std::tie(max_iters, level_iters, coarsest_iters, sync_stride, pure_neumann, tol, one_over_alpha, prolong_coeff, fused) <
-               std::tie(o.max_iters, o.level_iters, o.coarsest_iters, o.sync_stride, o.pure_neumann, o.tol, o.one_over_alpha,
+        return std::tie(max_iters, level_iters, coarsest_iters, sync_stride, pure_neumann, one_over_alpha, prolong_coeff, fused) <
+               std::tie(o.max_iters, o.level_iters, o.coarsest_iters, o.sync_stride, o.pure_neumann, o.one_over_alpha,
                         o.prolong_coeff, o.fused);
     }
+};
+
+// A contiguous run of one instance's tiles inside the merged pool: tiles local..local+count of
+// the instance's all-tiles order are global..global+count (one run per level).
+struct TileRun {
+    int global, local, count;
 };
 
 struct DevGrid {
     int device = 0;
     int n = 0, num_layers = 0, max_level = -1;
+    int num_inst = 1;
     int sm_count = 148;
-    int red_blocks = 1;          // CTAs of the leaf reductions (fixed per grid: deterministic sums)
+    int red_blocks = 1;          // CTAs of the whole-grid leaf dot (cirrus_dot)
     int64_t dof = 0;
     size_t bytes = 0;
     Topo topo{};
-    float h0 = 0.125f;
+
+    // instances
+    std::vector<float> inst_h0;
+    std::vector<int> inst_tiles, inst_leaves, inst_max_level;
+    std::vector<int64_t> inst_dof;
+    std::vector<std::vector<TileRun>> inst_runs;
+    int* d_inst = nullptr;          // n: instance of each tile
+    float* d_inst_h0 = nullptr;
 
     float* d_chbuf = nullptr;
     float* d_ch[kNumChannels] = {};
@@ -70,20 +88,35 @@ struct DevGrid {
     float* d_xpre = nullptr;        // n x 512: pre-smoothed x of the fused V-cycle (read by the upstroke)
     void** d_tile_ptrs = nullptr;  // optional external array-of-tiles storage (interop)
     int* d_lists = nullptr;
-    const int* d_leaf = nullptr;
+    const int* d_leaf = nullptr;   // LEAF tiles, instance by instance, each in its all-tiles order
     const int* d_ghost = nullptr;
     const int* d_leafghost = nullptr;
     const int* d_mg = nullptr;
     int n_leaf = 0, n_ghost = 0, n_leafghost = 0;
     std::vector<int> mg_offset, mg_count, level_first, level_count;
-    int* d_level_tables = nullptr;  // mg_offset | mg_count | level_first | level_count (num_layers each)
-    int bottom_level = -1;          // levels 0..bottom_level fit the shared-memory small-level kernel (-1: none)
     std::vector<uint8_t> h_tile_type;
 
-    double* d_partials = nullptr;
-    unsigned int* d_counter = nullptr;
-    Scalars* d_scalars = nullptr;
-    Scalars* h_scalars = nullptr;  // pinned
+    // coarse levels 0..bottom_level of every instance in the shared-memory kernel (-1: none)
+    int bottom_level = -1;
+    size_t bottom_smem = 0;
+    int4* d_bottom_tiles = nullptr;     // per record: box base, parent-cell base, type | level << 8, tile
+    uint16_t* d_bottom_code = nullptr;  // per box cell: stencil mask byte | cross-level (c2) face flags << 7
+    BottomInst* d_bottom_inst = nullptr;
+
+    // per-instance reductions: chunk table (instance, first vector, end vector) and per instance
+    // (first chunk, chunk count)
+    int n_chunks = 0;
+    int4* d_chunks = nullptr;
+    int2* d_inst_chunks = nullptr;
+    unsigned int* d_counters = nullptr;  // ticket counter per instance
+    double* d_partials = nullptr;        // 2 doubles per chunk (and per cirrus_dot block)
+    unsigned int* d_counter = nullptr;   // ticket counter of the whole-grid reductions
+    Scalars* d_scalars = nullptr;        // per instance
+    Scalars* h_scalars = nullptr;        // pinned mirror
+    Scalars* d_dot = nullptr;            // result slot of the whole-grid reductions
+    InstParams* d_iparams = nullptr;
+    InstParams* h_iparams = nullptr;     // pinned
+    int* d_active = nullptr;             // instances still iterating in the running solve
     double* d_history = nullptr;
     int history_cap = 0;
 
@@ -91,7 +124,7 @@ struct DevGrid {
     double* d_x64 = nullptr;
     double* d_ax64 = nullptr;
     double* d_r64 = nullptr;
-    double* d_norm = nullptr;
+    double* d_norm = nullptr;      // per instance
     float* d_bsave = nullptr;
     bool x64_valid = false;      // the last solve was mixed precision: d_x64 holds its FP64 x
 
@@ -105,31 +138,59 @@ struct DevGrid {
     std::string last_error;
 };
 
-// Builds the device grid from a finalised topology (cell types set, CalcCellTypesFromLeafs done).
-int grid_create(const Topology& topo, DevGrid** out, std::string* err);
+// Builds the device grid of one or more instances from finalised topologies (cell types set,
+// CalcCellTypesFromLeafs done).
+int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::string* err);
 void grid_destroy(DevGrid* g);
 
 namespace launch {
-template <class T> void full_laplacian(const DevGrid& g, T* X, T* Y, const int* done, cudaStream_t s);
+// Programmatic dependent launch of the solve kernels (on unless CIRRUS_NO_PDL=1).
+bool pdl_enabled();
+// Launches kernel k on stream s with programmatic stream serialisation: the kernel may be
+// scheduled while its predecessor finishes; the kernel itself waits for the predecessor's
+// completion (pdl_entry) before touching memory.
+template <class... KArgs, class... Args>
+inline void launch_kernel(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+// S (nullable): per-instance scalars; tiles of finished instances are skipped.
+template <class T> void full_laplacian(const DevGrid& g, T* X, T* Y, const Scalars* S, cudaStream_t s);
 // FullNegativeLaplacian as one launch; the ghost-to-parent sums are completed by OP_PAP.
-void laplacian_fused(const DevGrid& g, const float* X, float* Y, const int* done, cudaStream_t s);
-void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const int* done, cudaStream_t s);
-void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t colors, int nsweeps, const int* done,
+void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s);
+void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s);
+void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t colors, int nsweeps, const Scalars* S,
                  cudaStream_t s);
 void residual_restrict(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha,
-                       const int* done, cudaStream_t s);
-void prolongate(const DevGrid& g, int level, const float* CX, float* FX, float prolong_coeff, const int* done, cudaStream_t s);
-void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const int* done, cudaStream_t s);
-void leaf_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* D, Scalars* S, const SolveCtl& ctl, int epi,
-                 int skip_if_done, cudaStream_t s);
+                       const Scalars* S, cudaStream_t s);
+void prolongate(const DevGrid& g, int level, const float* CX, float* FX, float prolong_coeff, const Scalars* S, cudaStream_t s);
+void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const Scalars* S, cudaStream_t s);
+// Per-instance reduction over LEAF vectors with the fused elementwise work of `op`; the
+// instance's epilogue `epi` runs on its scalars.
+void inst_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* D, const SolveCtl& ctl, int epi, int skip,
+                 cudaStream_t s);
+// Whole-grid dot over all LEAF tiles into g.d_dot->gamma (cirrus_dot).
+void grid_dot(const DevGrid& g, const float* A, const float* B, cudaStream_t s);
 // OP_DOT over an explicit leaf list with caller-provided scratch (partials: 2 doubles per block;
 // counter 0 at launch); the sum goes to S->gamma.
 void leaf_dot_raw(const float* A, const float* B, const int* leaves, int nleaf, int blocks, double* partials,
                   unsigned int* counter, Scalars* S, cudaStream_t s);
-void update_p(const DevGrid& g, float* P, const float* Z, const Scalars* S, cudaStream_t s);
-void recenter(const DevGrid& g, float* R, const Scalars* S, int skip_if_done, cudaStream_t s, float* RC = nullptr);
+// Sets up the per-instance scalars of a solve from g.d_iparams.
+void begin_solve(const DevGrid& g, const SolveCtl& ctl, cudaStream_t s);
+void update_p(const DevGrid& g, float* P, const float* Z, cudaStream_t s);
+void recenter(const DevGrid& g, float* R, float* RC, cudaStream_t s);
 void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s);
 void accumulate_correction(const DevGrid& g, double* X64, float* E, cudaStream_t s);
+// per-instance FP64 sums of squares into out[instance] (A, or B32 widened)
 void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s);
 void widen(const DevGrid& g, const float* a, double* b, size_t n, cudaStream_t s);
 void narrow(const DevGrid& g, const double* a, float* b, size_t n, cudaStream_t s);
@@ -138,14 +199,15 @@ void clear_neumann_faces(const DevGrid& g, int u_channel, cudaStream_t s);
 void propagate_to_children(const DevGrid& g, int channel, cudaStream_t s);
 void velocity_divergence(const DevGrid& g, int u_channel, int b_channel, cudaStream_t s);
 // fused V-cycle (vcycle_fused.cu)
-void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const int* done, cudaStream_t s);
-void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const int* done,
+void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s);
+void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
                    cudaStream_t s);
 void zero_ghost_tiles(const DevGrid& g, float* X, cudaStream_t s);
 bool bottom(const DevGrid& g, int lb, int coarsest_iters, float* Z, const float* RHS, float one_over_alpha, float prolong_coeff,
-            const int* done, cudaStream_t s);
+            const Scalars* S, cudaStream_t s);
 bool bottom_supported(int coarsest_iters, int lb);
-constexpr int kBottomTiles = 40;  // tiles the shared-memory small-level kernel holds
+constexpr int kBottomSmemBudget = 224 * 1024;  // dynamic shared memory of the coarse-level kernel
+size_t bottom_smem_bytes(long long cells, int tiles);
 void init_kernel_attributes();
 // array-of-tiles interop (interop.cu)
 void gather_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream_t s);
@@ -155,12 +217,12 @@ void scatter_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream
 // V-cycle with the reference's schedule (src/GMGSolver.cu:383-447), one launch per kernel of the
 // reference (any level_iters).
 void vcycle(const DevGrid& g, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters, float one_over_alpha,
-            float prolong_coeff, const int* done, cudaStream_t s);
+            float prolong_coeff, const Scalars* S, cudaStream_t s);
 // The same V-cycle with fused kernels (level_iters == 1).  Precondition: RHS holds f on LEAF
 // tiles (the PCG kernels that write r maintain this) and 0 on GHOST tiles; X needs no
 // initialisation.
 void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, float one_over_alpha, float prolong_coeff,
-                  const int* done, cudaStream_t s);
+                  const Scalars* S, cudaStream_t s);
 bool use_fused(const DevGrid& g, int level_iters, int coarsest_iters);
 
 struct SolveParams {
@@ -175,17 +237,24 @@ struct SolveParams {
 struct SolveResult {
     int iters = 0, outer = 0, status = 0;
     double rel = 0, true_rel = -1;
-    long long launches = 0;  // kernels executed by the solve
+    long long launches = 0;  // kernels executed by the solve (the whole batch's)
+};
+// Per-instance part of a batched solve request (defaults: the shared SolveParams).
+struct InstRequest {
+    int active = 1;
+    double tol = -1;          // < 0: SolveParams::tol
+    int pure_neumann = -1;    // < 0: SolveParams::pure_neumann
 };
 
-// Plain FP32 GMG-PCG (GMGSolver::solve).  b in channel 1, x to channel 0.
-int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r);
+// Plain FP32 GMG-PCG (GMGSolver::solve) of every active instance: b in channel 1, x to channel 0.
+// r: one result per instance; req: one request per instance or null (all active).
+int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r, const InstRequest* req = nullptr);
 // Mixed precision: FP64 defect correction around FP32 PCG solves.
-int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r);
-// FP64 true relative residual of the last solution against b (device FP32 leaf channel): the
-// FP64 x of a mixed-precision solve, else channel 0 widened to FP64.
+int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r, const InstRequest* req = nullptr);
+// FP64 true relative residual of the last solution of each instance against b (device FP32
+// channel): the FP64 x of a mixed-precision solve, else channel 0 widened to FP64.
 int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s);
-// Copy the last solution to the host in FP64 (num_tiles*512 doubles).
+// Copy the last solution to the host in FP64 (num_tiles*512 doubles, pool order).
 int solution_f64(DevGrid& g, double* host, cudaStream_t s);
 
 }  // namespace cirrus

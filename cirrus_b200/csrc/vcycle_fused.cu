@@ -7,8 +7,9 @@
 //                                    of the first cell layer of each face neighbour, recomputed
 //                                    in place;
 //                   k_residual_restrict (GHOST x and right-hand sides are 0)
-//   levels 0..lb:   k_bottom         the whole V-cycle of the small coarse levels in one CTA with
-//                                    x, right-hand side, masks and metadata in shared memory
+//   levels 0..lb:   k_bottom         the whole V-cycle of the small coarse levels in one CTA, each
+//                                    level a dense box of x, right-hand side and stencil codes in
+//                                    shared memory
 //   up, level l:    k_prolong_sweep  ProlongateAndUpdate128 applied while staging the tile and
 //                                    its face halos, then the first colour (1) of
 //                                    GaussSeidelGMG(1, 1);
@@ -73,21 +74,21 @@ __device__ __forceinline__ float first_colour(const Topo& tp, const float* __res
 // result goes to XP.  GHOST neighbours hold x = 0 on the way down (they are not smoothed).
 template <int TPB>
 __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __restrict__ list, int n, float* XP,
-                                                         const float* __restrict__ RHS, const int* __restrict__ done) {
+                                                         const float* __restrict__ RHS, const Scalars* __restrict__ S) {
+    pdl_entry();
     __shared__ TileShared<float> sh[TPB];
-    if (done && *done) return;
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     const int q = blockIdx.x * TPB + g;
-    const bool active = q < n;
-    const int tile = active ? list[q] : 0;
+    const int tile = q < n ? list[q] : 0;
+    const bool active = q < n && !tile_done(tp, S, tile);
     const TileIdx ix(t);
     TileMeta m;
     V4<float> b;
     uint32_t mask4 = 0, cls = 0;
-    LevelConst<float> L(tp.h0, 0);
+    LevelConst<float> L(1.f, 0);
     if (active) {
         m = tp.meta[tile];
-        L = LevelConst<float>(tp.h0, meta_level(m.packed));
+        L = LevelConst<float>(tile_h0(tp, tile), meta_level(m.packed));
         b = ld4(RHS + (size_t)tile * kTileCells + t * 4);
         mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
         cls = (tp.fcls[tile] >> 12) & 0xfffu;
@@ -160,13 +161,13 @@ __device__ __forceinline__ float prolongated(const Topo& tp, const float* __rest
 template <int TPB>
 __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first, int n, float* Z, const float* __restrict__ XP,
                                                              const float* __restrict__ RHS, float prolong_coeff,
-                                                             const int* __restrict__ done) {
+                                                             const Scalars* __restrict__ S) {
+    pdl_entry();
     __shared__ TileShared<float> sh[TPB];
-    if (done && *done) return;
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     const int q = blockIdx.x * TPB + g;
-    const bool active = q < n;
-    const int tile = first + (active ? q : 0);
+    const int tile = first + (q < n ? q : 0);
+    const bool active = q < n && !tile_done(tp, S, tile);
     TileMeta m;
     bool ghost = false;
     if (active) {
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first,
     if (!ghost) {
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
         const V4<float> b = ld4(RHS + (size_t)tile * kTileCells + t * 4);
-        const LevelConst<float> L(tp.h0, meta_level(m.packed));
+        const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
         float ax[4], d[4];
         neg_lap4<float, true>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
         const TileIdx ix(t);
@@ -224,58 +225,36 @@ __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first,
 
 // Right-hand sides of GHOST tiles to 0 (the V-cycle's initialisation of them, src/GMGSolver.cu:393-396).
 __global__ void __launch_bounds__(128) k_zero_tiles(const int* __restrict__ list, int n, float* X) {
+    pdl_entry();
     const int q = blockIdx.x;
     if (q < n) st4(X + (size_t)list[q] * kTileCells + threadIdx.x * 4, zero4<float>());
 }
 
-// ---------------------------------------------------------------------------- small levels
-// Levels 0..lb (the first nb tiles of the all-tiles order) in one CTA: x, right-hand side, masks,
-// metadata and the mg list in shared memory; a phase program of colour sweeps, residual +
-// restrictions and prolongations (the reference's schedule) separated by __syncthreads.
+// ---------------------------------------------------------------------------- coarse levels
+// Levels 0..lb of each instance in one CTA per instance.  Each level lives in
+// shared memory as a dense box over its tiles' bounding box plus a one-cell halo, so a stencil
+// reads x at q +- 1 (z), q +- sz (y), q +- sy (x); cells of absent tiles and of the halo hold 0,
+// the value the reference gives a missing neighbour.  A per-cell 16-bit code carries the stencil
+// mask (bits 0-5 faces x-,x+,y-,y+,z-,z+, bit 6 INTERIOR) and, on tile faces, the cross-level
+// coefficient flag (bits 7-12: (2/3)/h^2 instead of 1/h^2).  A phase program of colour sweeps,
+// residual + restrictions and prolongations (the reference's schedule) runs with __syncthreads
+// between phases.
 constexpr int kBottomMaxPhases = 256;
-constexpr int kBottomMaxLevels = 16;
 struct BottomProgram {
     int nphase;
     uint8_t op[kBottomMaxPhases];  // 1 sweep, 2 residual+restrict, 3 prolongate
     uint8_t level[kBottomMaxPhases];
     uint8_t color[kBottomMaxPhases];
 };
-struct BottomLevels {
-    int mg_off[kBottomMaxLevels], mg_cnt[kBottomMaxLevels], first[kBottomMaxLevels], cnt[kBottomMaxLevels];
-};
-
-struct BottomView {
-    const float* X;
-    const uint8_t* MK;
-    const TileMeta* M;
-    const uint32_t* CL;
-};
-
-// negativeLap (times h^3, INTERIOR cells) of cell (i, j, k) of shared tile `tile`, and its
-// diagonal: the operation order of neg_lap4.
+// negativeLap (times h^3, INTERIOR cells) of box cell q, and its diagonal: the operation order of
+// neg_lap4 (coefficients a_f, fused multiply-adds in face order, diagonal summed in face order).
 template <bool DIAG>
-__device__ __forceinline__ float smem_neglap(const BottomView& v, int tile, int i, int j, int k, const LevelConst<float>& L,
-                                             float* diag) {
-    const float* xs = v.X + tile * kTileCells;
-    const TileMeta& m = v.M[tile];
-    auto nbv = [&](int f, int off) -> float { return m.nb[f] >= 0 ? v.X[m.nb[f] * kTileCells + off] : 0.f; };
-    const int c = (i << 6) | (j << 3) | k;
-    const uint32_t mm = v.MK[tile * kTileCells + c];
-    const uint32_t cls = v.CL[tile];
-    auto cross = [&](int f) -> float { return ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1; };
-    const float x0 = xs[c];
-    const float xm = i > 0 ? xs[c - 64] : nbv(0, 448 + (c & 63));
-    const float xp = i < 7 ? xs[c + 64] : nbv(1, c & 63);
-    const float ym = j > 0 ? xs[c - 8] : nbv(2, (i << 6) | 56 | k);
-    const float yp = j < 7 ? xs[c + 8] : nbv(3, (i << 6) | k);
-    const float zm = k > 0 ? xs[c - 1] : nbv(4, c | 7);
-    const float zp = k < 7 ? xs[c + 1] : nbv(5, c & ~7);
-    const float a0 = (mm & 1u) ? (i == 0 ? cross(0) : L.c1) : 0.f;
-    const float a1 = (mm & 2u) ? (i == 7 ? cross(1) : L.c1) : 0.f;
-    const float a2 = (mm & 4u) ? (j == 0 ? cross(2) : L.c1) : 0.f;
-    const float a3 = (mm & 8u) ? (j == 7 ? cross(3) : L.c1) : 0.f;
-    const float a4 = (mm & 16u) ? (k == 0 ? cross(4) : L.c1) : 0.f;
-    const float a5 = (mm & 32u) ? (k == 7 ? cross(5) : L.c1) : 0.f;
+__device__ __forceinline__ float box_neglap(const float* X, int q, uint32_t code, int sy, int sz, const LevelConst<float>& L,
+                                            float* diag) {
+    const float x0 = X[q];
+    const float xm = X[q - sy], xp = X[q + sy], ym = X[q - sz], yp = X[q + sz], zm = X[q - 1], zp = X[q + 1];
+    auto coef = [&](int f) -> float { return ((code >> f) & 1u) ? (((code >> (7 + f)) & 1u) ? L.c2 : L.c1) : 0.f; };
+    const float a0 = coef(0), a1 = coef(1), a2 = coef(2), a3 = coef(3), a4 = coef(4), a5 = coef(5);
     float s = 0.f;
     s = fmaf(a0, x0 - xm, s);
     s = fmaf(a1, x0 - xp, s);
@@ -283,7 +262,7 @@ __device__ __forceinline__ float smem_neglap(const BottomView& v, int tile, int 
     s = fmaf(a3, x0 - yp, s);
     s = fmaf(a4, x0 - zm, s);
     s = fmaf(a5, x0 - zp, s);
-    const bool interior = mm & kMaskInterior;
+    const bool interior = code & kMaskInterior;
     if (DIAG) {
         float d = 0.f;
         d = d + a0; d = d + a1; d = d + a2; d = d + a3; d = d + a4; d = d + a5;
@@ -292,58 +271,78 @@ __device__ __forceinline__ float smem_neglap(const BottomView& v, int tile, int 
     return interior ? s * L.h * L.h * L.h : 0.f;
 }
 
-size_t bottom_smem_bytes(int nb) {
-    return (size_t)nb * (2 * kTileCells * sizeof(float) + kTileCells + sizeof(TileMeta) + sizeof(uint32_t) + sizeof(int)) + 64;
+namespace launch {
+size_t bottom_smem_bytes(long long cells, int tiles) {
+    return (size_t)tiles * sizeof(int4) + (size_t)cells * (2 * sizeof(float) + sizeof(uint16_t)) + 16;
 }
+}  // namespace launch
 
-__global__ void __launch_bounds__(1024) k_bottom(Topo tp, int nb, int nmg, const int* __restrict__ mg, float* Z,
-                                                 const float* __restrict__ RHS, float one_over_alpha, float prolong_coeff,
-                                                 BottomProgram prog, BottomLevels lv, const int* __restrict__ done) {
+__global__ void __launch_bounds__(1024) k_bottom(Topo tp, const BottomInst* __restrict__ insts, const int4* __restrict__ tiles,
+                                                 const uint16_t* __restrict__ codes, float* Z, const float* __restrict__ RHS,
+                                                 float one_over_alpha, float prolong_coeff, BottomProgram prog,
+                                                 const Scalars* __restrict__ S) {
+    pdl_entry();
     extern __shared__ __align__(16) unsigned char bsm[];
-    float* X = reinterpret_cast<float*>(bsm);
-    float* B = X + nb * kTileCells;
-    TileMeta* M = reinterpret_cast<TileMeta*>(B + nb * kTileCells);
-    uint8_t* MK = reinterpret_cast<uint8_t*>(M + nb);
-    uint32_t* CL = reinterpret_cast<uint32_t*>(MK + nb * kTileCells);
-    int* MG = reinterpret_cast<int*>(CL + nb);
-    if (done && *done) return;
-    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
-        M[t] = tp.meta[t];
-        CL[t] = (tp.fcls[t] >> 12) & 0xfffu;
+    __shared__ BottomInst bi;
+    const int inst = blockIdx.x;
+    if (S && S[inst].done) return;
+    if (threadIdx.x == 0) bi = insts[inst];
+    __syncthreads();
+    const int nb = bi.nrec, cells = bi.cells;
+    int4* T = reinterpret_cast<int4*>(bsm);  // base, parent-cell base, type | level << 8, tile
+    float* X = reinterpret_cast<float*>(T + nb);
+    float* B = X + cells;
+    uint16_t* CODE = reinterpret_cast<uint16_t*>(B + cells);
+    const float h0 = tp.inst_h0[inst];
+    // cells is a multiple of 8: every region is 16-byte aligned and copied in 16-byte vectors
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) T[t] = tiles[bi.rec_off + t];
+    for (int v = threadIdx.x; v < cells / 4; v += blockDim.x) {
+        st4(X + 4 * v, zero4<float>());
+        st4(B + 4 * v, zero4<float>());
     }
-    for (int i = threadIdx.x; i < nmg; i += blockDim.x) MG[i] = mg[i];
-    for (int u = threadIdx.x; u < nb * 128; u += blockDim.x) {
-        const bool ghost = meta_type(tp.meta[u >> 7].packed) & GHOST_T;
-        st4(X + u * 4, zero4<float>());
-        st4(B + u * 4, ghost ? zero4<float>() : ld4(RHS + (size_t)u * 4));
-        *reinterpret_cast<uint32_t*>(MK + u * 4) = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)u * 4);
+    for (int v = threadIdx.x; v < cells / 8; v += blockDim.x)
+        reinterpret_cast<uint4*>(CODE)[v] = reinterpret_cast<const uint4*>(codes + bi.code_off)[v];
+    __syncthreads();
+    // right-hand sides of the non-GHOST tiles (GHOST right-hand sides are 0); a tile row of 8
+    // cells is contiguous in its box
+    for (int v = threadIdx.x; v < nb * 128; v += blockDim.x) {
+        const int4 r = T[v >> 7];
+        if (r.z & GHOST_T) continue;
+        const int lvl = r.z >> 8;
+        const int c = (v & 127) * 4;
+        const V4<float> b = ld4(RHS + (size_t)r.w * kTileCells + c);
+        float* dst = B + r.x + (c >> 6) * bi.sy[lvl] + ((c >> 3) & 7) * bi.sz[lvl] + (c & 7);
+        dst[0] = b.v[0]; dst[1] = b.v[1]; dst[2] = b.v[2]; dst[3] = b.v[3];
     }
     __syncthreads();
-    const BottomView v{X, MK, M, CL};
     for (int ph = 0; ph < prog.nphase; ph++) {
         const int op = prog.op[ph], level = prog.level[ph];
-        const LevelConst<float> L(tp.h0, level);
+        const LevelConst<float> L(h0, level);
+        const int sy = bi.sy[level], sz = bi.sz[level], first = bi.first[level];
         if (op == 1) {
-            // one colour of GaussSeidelGMG on the level's mg tiles; items are the 256 cells of the
-            // colour, whose neighbours all have the other colour
+            // one colour of GaussSeidelGMG on the level's LEAF|NONLEAF tiles; items are the 256 cells
+            // of the colour (a warp covers one (tile, i) plane), whose neighbours all have the other colour
             const int color = prog.color[ph];
-            const int n = lv.mg_cnt[level] * 256, base = lv.mg_off[level];
+            const int n = bi.cnt[level] * 256;
             for (int it = threadIdx.x; it < n; it += blockDim.x) {
-                const int tile = MG[base + (it >> 8)], u = it & 255;
+                const int4 r = T[first + (it >> 8)];
+                if (r.z & GHOST_T) continue;
+                const int u = it & 255;
                 const int i = u >> 5, j = (u >> 2) & 7, k = ((u & 3) << 1) | ((i + j + color) & 1);
+                const int q = r.x + i * sy + j * sz + k;
+                const uint32_t code = CODE[q];
                 float d;
-                const float ax = smem_neglap<true>(v, tile, i, j, k, L, &d);
-                const int c = tile * kTileCells + ((i << 6) | (j << 3) | k);
-                const bool interior = MK[c] & kMaskInterior;
-                X[c] = X[c] + (interior ? (B[c] - ax) / d : 0.f);
+                const float ax = box_neglap<true>(X, q, code, sy, sz, L, &d);
+                X[q] = X[q] + ((code & kMaskInterior) ? (B[q] - ax) / d : 0.f);
             }
         } else if (op == 2) {
-            // residual and restriction; items are the 64 2x2x2 blocks of the level's tiles
-            const int n = lv.cnt[level] * 64, first = lv.first[level];
+            // residual and restriction into level - 1; items are the 64 2x2x2 blocks of each tile
+            const int syp = bi.sy[level - 1], szp = bi.sz[level - 1];
+            const int n = bi.cnt[level] * 64;
             for (int it = threadIdx.x; it < n; it += blockDim.x) {
-                const int tile = first + (it >> 6), blk = it & 63;
-                const TileMeta& m = M[tile];
-                if (m.parent < 0) continue;
+                const int4 r = T[first + (it >> 6)];
+                if (r.y < 0) continue;
+                const int blk = it & 63;
                 const int fi = blk / 16 * 2, fj = (blk / 4) % 4 * 2, fk = blk % 4 * 2;
                 float sum = 0.f;
 #pragma unroll
@@ -352,67 +351,71 @@ __global__ void __launch_bounds__(1024) k_bottom(Topo tp, int nb, int nmg, const
                     for (int jj = 0; jj < 2; jj++)
 #pragma unroll
                         for (int kk = 0; kk < 2; kk++) {
-                            const int i = fi + ii, j = fj + jj, k = fk + kk;
-                            const float ax = smem_neglap<false>(v, tile, i, j, k, L, nullptr);
-                            sum += B[tile * kTileCells + ((i << 6) | (j << 3) | k)] - ax;
+                            const int q = r.x + (fi + ii) * sy + (fj + jj) * sz + fk + kk;
+                            const float ax = box_neglap<false>(X, q, CODE[q], sy, sz, L, nullptr);
+                            sum += B[q] - ax;
                         }
-                const int oct = meta_octant(m.packed);
-                const int pid = m.parent * kTileCells + ((oct & 1) * 4 + fi / 2) * 64 + (((oct >> 1) & 1) * 4 + fj / 2) * 8 +
-                                ((oct >> 2) & 1) * 4 + fk / 2;
                 // parents are one level coarser: no cell written here is read in this phase, and
                 // each parent cell has exactly one child block
-                if (meta_type(m.packed) & GHOST_T) B[pid] += sum;
-                else B[pid] = sum * one_over_alpha;
+                const int p = r.y + (fi / 2) * syp + (fj / 2) * szp + fk / 2;
+                if (r.z & GHOST_T) B[p] += sum;
+                else B[p] = sum * one_over_alpha;
             }
         } else {
-            // prolongation and update of the level's tiles (parents one level coarser)
-            const int n = lv.cnt[level] * kTileCells, first = lv.first[level];
+            // prolongation and update of the level's tiles from level - 1
+            const int syp = bi.sy[level - 1], szp = bi.sz[level - 1];
+            const int n = bi.cnt[level] * kTileCells;
             for (int it = threadIdx.x; it < n; it += blockDim.x) {
-                const int tile = first + (it >> 9), c = it & (kTileCells - 1);
-                const TileMeta& m = M[tile];
-                float cx = 0.f;
-                if (m.parent >= 0) {
-                    const int oct = meta_octant(m.packed);
-                    cx = X[m.parent * kTileCells + ((oct & 1) * 4 + (c >> 7)) * 64 + (((oct >> 1) & 1) * 4 + ((c >> 4) & 3)) * 8 +
-                           ((oct >> 2) & 1) * 4 + ((c & 7) >> 1)];
-                }
-                float& x = X[tile * kTileCells + c];
-                x = (MK[tile * kTileCells + c] & kMaskInterior) ? ((meta_type(m.packed) & GHOST_T) ? cx : fmaf(prolong_coeff, cx, x)) : 0.f;
+                const int4 r = T[first + (it >> 9)];
+                const int c = it & (kTileCells - 1);
+                const int i = c >> 6, j = (c >> 3) & 7, k = c & 7;
+                const int q = r.x + i * sy + j * sz + k;
+                const float cx = r.y >= 0 ? X[r.y + (i >> 1) * syp + (j >> 1) * szp + (k >> 1)] : 0.f;
+                X[q] = (CODE[q] & kMaskInterior) ? ((r.z & GHOST_T) ? cx : fmaf(prolong_coeff, cx, X[q])) : 0.f;
             }
         }
         __syncthreads();
     }
-    for (int u = threadIdx.x; u < nb * 128; u += blockDim.x) st4(Z + (size_t)u * 4, ld4(X + u * 4));
+    for (int v = threadIdx.x; v < nb * 128; v += blockDim.x) {
+        const int4 r = T[v >> 7];
+        const int lvl = r.z >> 8;
+        const int c = (v & 127) * 4;
+        const float* src = X + r.x + (c >> 6) * bi.sy[lvl] + ((c >> 3) & 7) * bi.sz[lvl] + (c & 7);
+        V4<float> o;
+        o.v[0] = src[0]; o.v[1] = src[1]; o.v[2] = src[2]; o.v[3] = src[3];
+        st4(Z + (size_t)r.w * kTileCells + c, o);
+    }
 }
 
 namespace launch {
 
 constexpr int kTPB2 = 2;
 
-void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const int* done, cudaStream_t s) {
+void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s) {
     const int n = g.mg_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    k_presmooth<kTPB2><<<(n + kTPB2 - 1) / kTPB2, 128 * kTPB2, 0, s>>>(g.topo, g.d_mg + g.mg_offset[level], n, XP, RHS, done);
+    launch_kernel(k_presmooth<kTPB2>, (n + kTPB2 - 1) / kTPB2, 128 * kTPB2, 0, s, g.topo, g.d_mg + g.mg_offset[level], n, XP, RHS, S);
 }
 
-void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const int* done,
+void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
                    cudaStream_t s) {
     const int n = g.level_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    k_prolong_sweep<kTPB2><<<(n + kTPB2 - 1) / kTPB2, 128 * kTPB2, 0, s>>>(g.topo, g.level_first[level], n, Z, XP, RHS,
-                                                                           prolong_coeff, done);
+    launch_kernel(k_prolong_sweep<kTPB2>, (n + kTPB2 - 1) / kTPB2, 128 * kTPB2, 0, s, g.topo, g.level_first[level], n, Z, XP, RHS,
+                  prolong_coeff, S);
 }
 
 void zero_ghost_tiles(const DevGrid& g, float* X, cudaStream_t s) {
     if (g.n_ghost == 0) return;
     ++g.launch_count;
-    k_zero_tiles<<<g.n_ghost, 128, 0, s>>>(g.d_ghost, g.n_ghost, X);
+    launch_kernel(k_zero_tiles, g.n_ghost, 128, 0, s, g.d_ghost, g.n_ghost, X);
 }
 
 bool bottom(const DevGrid& g, int lb, int coarsest_iters, float* Z, const float* RHS, float one_over_alpha, float prolong_coeff,
-            const int* done, cudaStream_t s) {
+            const Scalars* S, cudaStream_t s) {
+    if (lb < 0 || lb != g.bottom_level) return false;
     BottomProgram p{};
     auto push = [&](int op, int level, int color) {
         if (p.nphase >= kBottomMaxPhases) return false;
@@ -422,33 +425,24 @@ bool bottom(const DevGrid& g, int lb, int coarsest_iters, float* Z, const float*
         p.nphase++;
         return true;
     };
-    bool ok = lb < kBottomMaxLevels;
+    bool ok = true;
     for (int l = lb; ok && l > 0; l--) ok = push(1, l, 0) && push(1, l, 1) && push(2, l, 0);
     for (int it = 0; ok && it < coarsest_iters / 2; it++) ok = push(1, 0, 0) && push(1, 0, 1);
     for (int it = 0; ok && it < coarsest_iters / 2; it++) ok = push(1, 0, 1) && push(1, 0, 0);
     for (int l = 1; ok && l <= lb; l++) ok = push(3, l, 0) && push(1, l, 1) && push(1, l, 0);
     if (!ok) return false;
-    BottomLevels lv{};
-    for (int l = 0; l <= lb; l++) {
-        lv.mg_off[l] = g.mg_offset[l];
-        lv.mg_cnt[l] = g.mg_count[l];
-        lv.first[l] = g.level_first[l];
-        lv.cnt[l] = g.level_count[l];
-    }
-    const int nb = g.level_first[lb] + g.level_count[lb];
-    const int nmg = g.mg_offset[lb] + g.mg_count[lb];
-    if (nb > kBottomTiles) return false;
     ++g.launch_count;
-    k_bottom<<<1, 1024, bottom_smem_bytes(nb), s>>>(g.topo, nb, nmg, g.d_mg, Z, RHS, one_over_alpha, prolong_coeff, p, lv, done);
+    launch_kernel(k_bottom, g.num_inst, 1024, g.bottom_smem, s, g.topo, (const BottomInst*)g.d_bottom_inst,
+                  (const int4*)g.d_bottom_tiles, (const uint16_t*)g.d_bottom_code, Z, RHS, one_over_alpha, prolong_coeff, p, S);
     return true;
 }
 
 bool bottom_supported(int coarsest_iters, int lb) {
-    return lb < kBottomMaxLevels && 2 * coarsest_iters + 6 * lb <= kBottomMaxPhases;
+    return lb >= 0 && lb < kBottomMaxLevels && 2 * coarsest_iters + 6 * lb <= kBottomMaxPhases;
 }
 
 void init_kernel_attributes() {
-    cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bottom_smem_bytes(kBottomTiles));
+    cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBudget);
 }
 
 }  // namespace launch

@@ -100,6 +100,17 @@ typedef struct cirrus_grid cirrus_grid;
 
 /* Uploads a finalised topology (cell types set) to the current CUDA device. */
 cirrus_status cirrus_grid_create(const cirrus_topology* topo, cirrus_grid** out);
+/* Batched grid: `count` independent instances (finalised topologies, any sizes, depths and h0)
+ * in one tile pool, solved together by cirrus_gmg_solve_batch.  No counterpart in the reference
+ * (one HADeviceGrid per solve).  Pool order is level-major across the instances; inside a level,
+ * instance by instance in each one's all-tiles order (a batch of one is the plain grid). */
+cirrus_status cirrus_grid_create_batch(const cirrus_topology* const* topos, int count, cirrus_grid** out);
+cirrus_status cirrus_grid_num_instances(const cirrus_grid* grid, int* count);
+/* Tiles and DoF (INTERIOR cells of LEAF tiles) of one instance; either output may be NULL. */
+cirrus_status cirrus_grid_instance_info(const cirrus_grid* grid, int instance, int* num_tiles, int64_t* dof);
+/* Channel transfer of one instance: its num_tiles*512 floats in its own all-tiles order. */
+cirrus_status cirrus_grid_set_channel_instance(cirrus_grid* grid, int instance, int channel, const float* host, void* stream);
+cirrus_status cirrus_grid_get_channel_instance(const cirrus_grid* grid, int instance, int channel, float* host, void* stream);
 void cirrus_grid_destroy(cirrus_grid* grid);
 cirrus_status cirrus_grid_num_tiles(const cirrus_grid* grid, int* num_tiles);
 /* Device bytes held by the grid. */
@@ -220,6 +231,16 @@ void cirrus_solve_params_default(cirrus_solve_params* params);
 cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream,
                                cirrus_solve_result* result);
 
+/* Solves every instance of a (batched) grid in one graph launch: one kernel per step for the whole
+ * batch, per-instance CG scalars and stopping, the loop running until the last instance stops.
+ * active (NULL = all): instances with 0 take no part and keep their channels; tolerances (NULL =
+ * params->relative_tolerance): per-instance relative tolerance.  results: one per instance.  An
+ * instance's result is bit-identical whatever else is in the batch (per-instance reductions
+ * in a fixed order).  cirrus_gmg_solve on a batched grid solves all instances and reports
+ * instance 0. */
+cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_params* params, const int* active,
+                                     const double* tolerances, void* stream, cirrus_solve_result* results);
+
 /* End-to-end variant for callers holding host arrays: copies b (num_tiles*512 floats, pinned or
  * pageable) to the device, solves, and copies x back into x_host. */
 cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params* params, const float* b_host,
@@ -231,7 +252,7 @@ cirrus_status cirrus_grid_get_solution_f64(cirrus_grid* grid, double* host, void
 
 /* FP64 true residual ||b - A x||/||b|| over INTERIOR cells of LEAF tiles for a given b (host,
  * num_tiles*512 floats) and the last solution (FP64 after a mixed-precision solve, else the
- * FP32 channel 0). */
+ * FP32 channel 0); one value per instance (rel holds num_instances doubles). */
 cirrus_status cirrus_true_residual(cirrus_grid* grid, const float* b_host, double* rel, void* stream);
 
 #ifdef __cplusplus
