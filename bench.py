@@ -1,23 +1,27 @@
-"""Benchmark of the GMG-PCG Poisson solve (one step = one full solve to 1e-6 relative residual).
+"""Benchmark of the GMG-PCG Poisson solve.  One step = one batched solve: K independent
+instances of the workload, each to 1e-6 relative residual, in one graph launch.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+    python bench.py [--gpus N] [--steps S] [--warmup W] [--batch K] [--impl ours|reference]
+                    [--workload NAME]
 
 Default workload: ring512 -- the adaptive 5-level octree with 512x512x1024 effective resolution
 (domain 1x1x2, leaves at levels 2-6 refined around a synthetic vortex ring, box obstacle),
-seeded synthetic velocity -> divergence right-hand side.  Prints one JSON line on rank 0.
+seeded synthetic velocity -> divergence right-hand side; instance i of rank r uses velocity seed
+r*K + i.  Prints one JSON line on rank 0.
 
-  value     solves/s with inputs resident in HBM (device-timed, CUDA events, L2 flushed
-            between steps by writing a 256 MiB buffer)
-  e2e       solves/s through cirrus_gmg_solve_host with pinned host buffers: H2D of b,
-            solve, D2H of x inside the timed region
-  roofline  the dominant kernel (Gauss-Seidel colour sweep on the finest level), algorithmic
+  value     solves/s of the batched solver with inputs resident in HBM (device-timed, CUDA events,
+            L2 flushed between steps by writing a 256 MiB buffer)
+  e2e       the same through cirrus_gmg_solve_host with pinned host buffers: H2D of the batch's
+            b, solve, D2H of x inside the timed region
+  latency_ms  one instance solved alone (batch of one): p50/p99 over the steps
+  roofline  the dominant kernel (the fused Laplacian, ~a quarter of an iteration): algorithmic
             bytes / CUDA-event duration against the measured HBM copy bandwidth
-  cpu_baseline  the CPU oracle (FP32 mirror of the reference arithmetic, OpenMP) on a bounded
-            sample of PCG iterations of the same workload, extrapolated to solves/s
+  cpu_baseline  the CPU oracle (FP32 mirror of the reference arithmetic, OpenMP) on full solves
+            of one instance, about 10 s of work
 
-Multi-GPU (torchrun): replicas only -- every rank solves its own instance (seed = rank); no
-collective on the data path; value = all ranks' solves / max-over-ranks time.
---impl reference runs the reference's own CUDA build (oracle/_ref) on the same workload.
+Multi-GPU (torchrun): replicas only -- every rank solves its own batch; no collective on the
+data path; value = all ranks' solves / max-over-ranks time.
+--impl reference runs the reference's own CUDA build (oracle/_ref), one solve at a time.
 """
 from __future__ import annotations
 
@@ -35,14 +39,21 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-GS_BYTES_PER_CELL = 9.0  # read x 4 + rhs 2 (one colour) + mask 1 + write x 2 (algorithmic)
+# algorithmic bytes of one fused-Laplacian launch: per LEAF tile read x + mask, write A x; per GHOST
+# tile read cell types + mask + the parent's eighth of x, write its 64-float partial-sum row
+LAP_BYTES_LEAF = 2048 + 512 + 2048
+LAP_BYTES_GHOST = 512 + 512 + 256 + 256
+# DRAM bytes (read + write) of one fused-Laplacian launch from an ncu capture (profiles/), per
+# (workload, batch); None where no capture of that configuration exists
+LAP_TRAFFIC_PER_LAUNCH = {("ring512", 16): None}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ring512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -50,52 +61,55 @@ def parse():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """NVML sampling (read-only) of the SM clock and clock-event reasons every 10 ms during the
+    timed region, in a background thread."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"cirrus_clocks_{os.getpid()}.csv"
+    def __init__(self, device: int):
+        self.device = device
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.thread = None
+        self.err = None
 
     def start(self):
+        import threading
+
         try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # NVML missing or device not found: report instead of failing the bench
+            self.err = f"nvml unavailable: {type(e).__name__}"
+            return
+        self.stop_flag = False
+
+        def run():
+            while not self.stop_flag:
+                try:
+                    self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    for n, bit in self.REASONS.items():
+                        if r & bit:
+                            self.reasons.add(n)
+                except Exception:
+                    pass
+                time.sleep(0.01)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.f.close()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
-            p = [x.strip() for x in line.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                smax = float(p[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, p[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        self.path.unlink(missing_ok=True)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
-                "reasons": sorted(reasons)}
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "samples": 0, "reasons": [self.err or "not sampled"]}
+        self.stop_flag = True
+        self.thread.join()
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "samples": len(self.samples), "reasons": sorted(self.reasons)}
 
 
 def measured_peaks() -> dict:
@@ -134,13 +148,17 @@ def barrier_max(pg, value: float) -> float:
     return float(t.item())
 
 
-def build_instance(name: str, seed: int):
+def build_batch(name: str, seeds: list[int]):
+    """K instances of one workload topology with their own seeded velocities; projection
+    right-hand side in channel 1 and a copy in channel 5."""
     from cirrus_b200 import DeviceGrid, workloads as W
 
-    b = W.build(W.make(name, seed))
-    g = DeviceGrid(b.topology)
-    for a in range(3):
-        g.set_channel(6 + a, b.velocity[a])
+    b = W.build(W.make(name, seeds[0]))
+    g = DeviceGrid([b.topology] * len(seeds))
+    for i, sd in enumerate(seeds):
+        vel = b.velocity if sd == seeds[0] else W.face_velocity(b.tiles, sd)
+        for a in range(3):
+            g.set_channel_instance(i, 6 + a, vel[a])
     g.projection_rhs()
     return b, g
 
@@ -166,9 +184,10 @@ def cpu_baseline(b, rhs, budget_s: float = 10.0, max_solves: int = 5) -> dict:
 def run_ours(args, world, rank, local, pg):
     import torch
 
-    from cirrus_b200 import GMGSolver, B_CHANNEL, TMP_CHANNEL
+    from cirrus_b200 import B_CHANNEL, KERNEL_LAPLACIAN, TMP_CHANNEL, GMGSolver
 
-    b, g = build_instance(args.workload, seed=rank)
+    K = args.batch
+    b, g = build_batch(args.workload, [rank * K + i for i in range(K)])
     rhs = g.get_channel(B_CHANNEL)
     g.copy_channel(TMP_CHANNEL, B_CHANNEL)  # keep b resident for restoring between steps
     stream = torch.cuda.current_stream()
@@ -177,23 +196,24 @@ def run_ours(args, world, rank, local, pg):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     iters_seen, launches = [], []
 
-    def one(timed: bool):
+    def one():
         g.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        it, rel = solver.solve(g, stream=sh)
+        res = solver.solve_batch(g, stream=sh)
         e1.record(stream)
         torch.cuda.synchronize()
-        iters_seen.append(it)
+        iters_seen.extend(r[0] for r in res)
         launches.append(solver.last_result.kernel_launches)
-        if rel >= 1e-6:
-            raise RuntimeError(f"solve did not converge: rel {rel}")
+        worst = max(r[1] for r in res)
+        if worst >= 1e-6:
+            raise RuntimeError(f"solve did not converge: rel {worst}")
         return e0.elapsed_time(e1)
 
     for _ in range(args.warmup):
-        one(False)
+        one()
     iters_seen.clear()
     launches.clear()
     clocks = None
@@ -203,13 +223,13 @@ def run_ours(args, world, rank, local, pg):
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
-    times = [one(True) for _ in range(args.steps)]
+    times = [one() for _ in range(args.steps)]
     torch.cuda.synchronize()
     if rank == 0:
         clocks = clk.stop()
     total_ms = barrier_max(pg, sum(times))
 
-    # end to end: host buffers through the public C ABI (H2D b, solve, D2H x)
+    # end to end: host buffers through the public C ABI (H2D of the batch's b, solve, D2H of x)
     b_host = torch.from_numpy(rhs.reshape(-1)).pin_memory()
     x_host = torch.empty_like(b_host).pin_memory()
     b_np, x_np = b_host.numpy(), x_host.numpy()
@@ -227,27 +247,45 @@ def run_ours(args, world, rank, local, pg):
         e2e_times.append((time.perf_counter() - t0) * 1e3)
     e2e_total = barrier_max(pg, sum(e2e_times))
 
-    # roofline of the dominant kernel: GS colour sweep on the finest level, same data, on `stream`
-    maxl = int(b.tiles[:, 0].max())
-    mg_cells = int(((b.tiles[:, 0] == maxl) & ((b.tiles[:, 4] & 3) != 0)).sum()) * 512
-    g.copy_channel(3, B_CHANNEL, sh)
-    reps = 200
-    for _ in range(10):
-        g.gauss_seidel_sweep(maxl, 4, 3, 0, stream=sh)
+    # roofline of the dominant kernel (fused Laplacian over the batch's LEAF|GHOST tiles), timed
+    # with CUDA events on the stream it is launched on
+    g.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
+    g.copy_channel(2, B_CHANNEL, sh)
+    reps = 50
+    g.bench_launch(KERNEL_LAPLACIAN, 0, 5, stream=sh)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for i in range(reps):
-        g.gauss_seidel_sweep(maxl, 4, 3, i & 1, stream=sh)
+    g.bench_launch(KERNEL_LAPLACIAN, 0, reps, stream=sh)
     e1.record(stream)
     torch.cuda.synchronize()
-    gs_ms = e0.elapsed_time(e1) / reps
+    lap_ms = e0.elapsed_time(e1) / reps
+    n_leaf = int(((b.tiles[:, 4] & 1) != 0).sum()) * K
+    n_ghost = int(((b.tiles[:, 4] & 4) != 0).sum()) * K
+    lap_bytes = n_leaf * LAP_BYTES_LEAF + n_ghost * LAP_BYTES_GHOST
     peaks = measured_peaks()
-    achieved = mg_cells * GS_BYTES_PER_CELL / (gs_ms * 1e-3) / 1e9
+    achieved = lap_bytes / (lap_ms * 1e-3) / 1e9
 
-    n = args.steps * world
+    # one instance alone (batch of one): latency
+    b1, g1 = build_batch(args.workload, [rank * K])
+    g1.copy_channel(TMP_CHANNEL, B_CHANNEL)
+    lat = []
+    for i in range(args.warmup + args.steps):
+        g1.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.solve(g1, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            lat.append(e0.elapsed_time(e1))
+
+    n = args.steps * world * K
     value = n / (total_ms * 1e-3)
-    dof = g.dof
+    dof = g.dof // K
+    maxl = int(b.tiles[:, 0].max())
     out = {
         "metric": "Poisson solves/s to 1e-6 relative residual (GMG-PCG, reference arithmetic)",
         "value": round(value, 3),
@@ -261,31 +299,37 @@ def run_ours(args, world, rank, local, pg):
         "vs_baseline": None,
         "dtype": "f32 (fp64 CG scalars)",
         "data": "synthetic (seeded face velocities, divergence right-hand side)",
-        "config": {"workload": args.workload, "tiles": int(b.tiles.shape[0]), "dof": int(dof),
+        "config": {"workload": f"{args.workload} x{K} batch", "instances_per_step": K, "tiles_per_instance": int(b.tiles.shape[0]),
+                   "dof_per_instance": int(dof),
                    "effective_resolution": "512x512x1024" if args.workload == "ring512" else args.workload,
                    "levels": f"leaves {int(b.tiles[(b.tiles[:, 4] & 1) != 0, 0].min())}-{maxl}",
-                   "tolerance": 1e-6, "stopping_rule": "recursive ||r||/||b|| < tol, checked every iteration",
+                   "tolerance": 1e-6, "stopping_rule": "recursive ||r||/||b|| < tol per instance, checked every iteration",
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
         "mdof_per_s": round(dof * value / 1e6, 2),
         "iters_per_solve": int(statistics.median(iters_seen)),
-        "latency_ms": {"p50": round(float(np.percentile(times, 50)), 4), "p99": round(float(np.percentile(times, 99)), 4)},
+        "latency_ms": {"single_p50": round(float(np.percentile(lat, 50)), 4), "single_p99": round(float(np.percentile(lat, 99)), 4),
+                       "batch_p50": round(float(np.percentile(times, 50)), 4), "batch_p99": round(float(np.percentile(times, 99)), 4)},
+        "single_solves_per_s": round(1e3 / float(np.mean(lat)), 3),
         "gpu_launches": int(sum(launches)),
         "e2e": {"value": round(n / (e2e_total * 1e-3), 3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(rhs.nbytes), "d2h_bytes_per_step": int(rhs.nbytes)},
-        "roofline": {"kernel": "k_gs_sweep (finest level, one colour)", "bound": "hbm",
+        "roofline": {"kernel": f"k_laplacian_fused ({K} instances, {n_leaf} LEAF + {n_ghost} GHOST tiles)", "bound": "hbm",
                      "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peaks["source"],
-                     "algorithmic_bytes_per_launch": int(mg_cells * GS_BYTES_PER_CELL),
-                     "launch_us": round(gs_ms * 1e3, 3), "traffic": None},
+                     "algorithmic_bytes_per_launch": int(lap_bytes), "launch_us": round(lap_ms * 1e3, 3),
+                     "traffic": LAP_TRAFFIC_PER_LAUNCH.get((args.workload, K))},
         "clocks": clocks,
     }
+    g1.close()
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        cb = cpu_baseline(b, rhs)
+        rhs1 = rhs[: b.tiles.shape[0]] if K == 1 else g.get_channel_instance(0, TMP_CHANNEL)
+        cb = cpu_baseline(b, rhs1)
         out["cpu_baseline"] = {"value": round(cb["solves"] / cb["seconds"], 4), "unit": "solves/s", "cores": cb["threads"],
                                "kind": "port",
-                               "sample": f"{cb['solves']} full solves of {args.workload} to 1e-6 ({cb['iters']} PCG "
-                                         f"iterations each) by the CPU oracle (FP32 mirror of the reference "
+                               "sample": f"{cb['solves']} full solves of one {args.workload} instance to 1e-6 ({cb['iters']} "
+                                         f"PCG iterations each) by the CPU oracle (FP32 mirror of the reference "
                                          f"arithmetic, OpenMP), {cb['seconds']:.1f} s wall"}
+    g.close()
     return out
 
 

@@ -34,6 +34,8 @@ __all__ = [
 ]
 
 LEAF, NONLEAF, GHOST = 1, 2, 4
+# kernels of cirrus_bench_launch
+KERNEL_LAPLACIAN, KERNEL_GS_SWEEP, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP, KERNEL_RESIDUAL_RESTRICT, KERNEL_COARSE, KERNEL_DOT = range(7)
 DIRICHLET, INTERIOR, NEUMANN = 1, 2, 4
 X_CHANNEL, B_CHANNEL, R_CHANNEL, P_CHANNEL, AP_CHANNEL, Z_CHANNEL, TMP_CHANNEL, U_CHANNEL = 0, 1, 1, 2, 3, 4, 5, 6
 PRECISION_FP32, PRECISION_MIXED_FP64 = 0, 1
@@ -219,6 +221,11 @@ class DeviceGrid:
         check(lib().cirrus_grid_get_channel_instance(self._h, instance, channel, _ptr(out, C.c_float), C.c_void_p(stream)),
               "cirrus_grid_get_channel_instance")
         return out
+
+    def bench_launch(self, kernel: int, level: int = 0, reps: int = 1, stream: int = 0) -> None:
+        """Launch one solve kernel `reps` times on `stream` (for timing with the caller's events);
+        overwrites channels 2-5."""
+        check(lib().cirrus_bench_launch(self._h, kernel, level, reps, C.c_void_p(stream)), "cirrus_bench_launch")
 
     def instance_dof(self, instance: int) -> int:
         d = C.c_int64()

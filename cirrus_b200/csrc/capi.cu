@@ -484,6 +484,32 @@ cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params
     return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
 }
 
+cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int reps, void* stream) {
+    if (!grid || reps < 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    const bool per_level = kernel >= CIRRUS_KERNEL_GS_SWEEP && kernel <= CIRRUS_KERNEL_RESIDUAL_RESTRICT;
+    if (per_level && (level < 0 || level > g.max_level)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (kernel == CIRRUS_KERNEL_RESIDUAL_RESTRICT && level < 1) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if ((kernel == CIRRUS_KERNEL_PRESMOOTH || kernel == CIRRUS_KERNEL_PROLONG_SWEEP || kernel == CIRRUS_KERNEL_COARSE) &&
+        g.bottom_level < 0)
+        return CIRRUS_ERR_STATE;
+    float *p = g.d_ch[2], *ap = g.d_ch[3], *z = g.d_ch[4], *tmp = g.d_ch[5];
+    cudaStream_t s = S(stream);
+    for (int i = 0; i < reps; i++) {
+        switch (kernel) {
+        case CIRRUS_KERNEL_LAPLACIAN: cirrus::launch::laplacian_fused(g, p, tmp, nullptr, s); break;
+        case CIRRUS_KERNEL_GS_SWEEP: cirrus::launch::gs_sweep(g, level, z, ap, i & 1, nullptr, s); break;
+        case CIRRUS_KERNEL_PRESMOOTH: cirrus::launch::presmooth(g, level, g.d_xpre, ap, nullptr, s); break;
+        case CIRRUS_KERNEL_PROLONG_SWEEP: cirrus::launch::prolong_sweep(g, level, z, g.d_xpre, ap, 1.f, nullptr, s); break;
+        case CIRRUS_KERNEL_RESIDUAL_RESTRICT: cirrus::launch::residual_restrict(g, level, g.d_xpre, ap, tmp, 1.f, nullptr, s); break;
+        case CIRRUS_KERNEL_COARSE: cirrus::launch::bottom(g, g.bottom_level, 10, z, ap, 1.f, 1.f, nullptr, s); break;
+        case CIRRUS_KERNEL_DOT: cirrus::launch::grid_dot(g, p, z, s); break;
+        default: return CIRRUS_ERR_INVALID_ARGUMENT;
+        }
+    }
+    return cuda_status();
+}
+
 cirrus_status cirrus_grid_get_solution_f64(cirrus_grid* grid, double* host, void* stream) {
     if (!grid || !host) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] { return map_rc(cirrus::solution_f64(*grid->g, host, S(stream))); });

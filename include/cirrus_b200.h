@@ -250,6 +250,21 @@ cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params
  * mixed-precision solve, else channel 0 widened.  Channel 0 always holds its FP32 rounding. */
 cirrus_status cirrus_grid_get_solution_f64(cirrus_grid* grid, double* host, void* stream);
 
+/* Measurement hook: launches one kernel of the solve `reps` times back to back on `stream` (no
+ * synchronisation), so a caller can time it with its own CUDA events on that stream.  Uses
+ * channels 2-5 (the solve's scratch) and overwrites them.  level: the level of the per-level
+ * kernels (ignored by the others).  No counterpart in the reference. */
+enum {
+    CIRRUS_KERNEL_LAPLACIAN = 0,        /* fused FullNegativeLaplacian over LEAF|GHOST tiles        */
+    CIRRUS_KERNEL_GS_SWEEP = 1,         /* one red-black colour sweep of a level                    */
+    CIRRUS_KERNEL_PRESMOOTH = 2,        /* two-colour pre-smoothing from x = 0 of a level           */
+    CIRRUS_KERNEL_PROLONG_SWEEP = 3,    /* prolongation + first post-smoothing colour of a level    */
+    CIRRUS_KERNEL_RESIDUAL_RESTRICT = 4,/* residual and restriction of a level                      */
+    CIRRUS_KERNEL_COARSE = 5,           /* the shared-memory coarse-level V-cycle                   */
+    CIRRUS_KERNEL_DOT = 6               /* whole-grid LEAF dot product                              */
+};
+cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int reps, void* stream);
+
 /* FP64 true residual ||b - A x||/||b|| over INTERIOR cells of LEAF tiles for a given b (host,
  * num_tiles*512 floats) and the last solution (FP64 after a mixed-precision solve, else the
  * FP32 channel 0); one value per instance (rel holds num_instances doubles). */
