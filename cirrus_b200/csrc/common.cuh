@@ -34,7 +34,11 @@ __host__ __device__ inline bool meta_nb_ghost(int packed, int f) { return (packe
 // its own level).  Per tile, fcls holds the coefficient class of the six cross-tile faces:
 // 2 bits per face, context lap in bits 0..11, mg in bits 12..23; class 1 = 1/h^2 (same level),
 // class 2 = (2/3)/h^2 (leaf-ghost T-junction).
+// Bit 7 is set when at least one face of the cell carries the (2/3)/h^2 coefficient, so a byte of
+// exactly kMaskFull marks an INTERIOR cell with six 1/h^2 faces (the kernels' uniform fast path).
 constexpr int kMaskInterior = 64;
+constexpr int kMaskC2 = 128;
+constexpr int kMaskFull = 0x7F;
 
 // Scalar state of one PCG solve of one instance, resident in device memory (the reference keeps
 // gamma, beta, alpha, gamma_old, fp, mean, count as 7 device doubles, src/GMGSolver.h:22-30).
@@ -64,6 +68,7 @@ struct Topo {
     const int* edge;             // n x 12 same-level edge neighbours (see Topology::edge_tiles)
     const int* ghost_slot;       // n: index of a GHOST tile in the ghost list, else -1
     const int* ghost_child;      // n x 8: ghost slot of the GHOST child in each octant, else -1
+    const int* ghost_list;       // GHOST tile of each ghost slot
     const int* inst;             // n: instance of each tile
     const float* inst_h0;        // per instance: voxel size of level 0, stored in FP32 as the reference does
 };

@@ -174,7 +174,10 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
                         ct1 = nb < 0 ? DIRICHLET_C : ct[(size_t)nb * kTileCells + ((nn[0] << 6) | (nn[1] << 3) | nn[2])];
                     }
                     const bool neumann = (ct0 & NEUMANN_C) || (ct1 & NEUMANN_C);
-                    if (cls != 0 && !neumann) bits |= (uint8_t)(1u << f);
+                    if (cls != 0 && !neumann) {
+                        bits |= (uint8_t)(1u << f);
+                        if (cls == 2u) bits |= kMaskC2;  // a face with the (2/3)/h^2 coefficient
+                    }
                 }
                 mask[o] = bits;
             }
@@ -365,7 +368,7 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
                         const uint32_t mgcls = fcls[t] >> 12;
                         for (int o = 0; o < kTileCells; o++) {
                             const int ijk[3] = {o >> 6, (o >> 3) & 7, o & 7};
-                            uint16_t c = mmg[(size_t)t * kTileCells + o];
+                            uint16_t c = mmg[(size_t)t * kTileCells + o] & (kMaskFull);
                             for (int f = 0; f < 6; f++) {
                                 const bool edge = (f & 1) ? ijk[f >> 1] == 7 : ijk[f >> 1] == 0;
                                 if (edge && ((mgcls >> (2 * f)) & 3u) == 2u) c |= (uint16_t)(1u << (7 + f));
@@ -382,6 +385,8 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
             CK((cudaError_t)(upload(&g->d_bottom_inst, bi) ? cudaErrorMemoryAllocation : cudaSuccess));
         }
         launch::init_kernel_attributes();
+        launch::init_stencil_attributes();
+        g->shapes.assign((size_t)KS_COUNT * num_layers, 1);
     }
 
     // ------------------------------------------------------------------ per-instance reductions
@@ -432,6 +437,7 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
     g->topo.edge = g->d_edge;
     g->topo.ghost_slot = g->d_ghost_tables;
     g->topo.ghost_child = g->d_ghost_tables + n;
+    g->topo.ghost_list = g->d_ghost;
     g->topo.inst = g->d_inst;
     g->topo.inst_h0 = g->d_inst_h0;
     g->bytes = cells * kNumChannels * sizeof(float) + cells * 3 + sizeof(TileMeta) * n + sizeof(uint32_t) * n + sizeof(int) * nl +

@@ -67,102 +67,70 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __r
     st4(Y + (size_t)tile * kTileCells + t * 4, o);
 }
 
-// Value a GHOST tile holds after PropagateValuesToGhostTiles (src/PoissonGrid.cu:585-605):
-// its parent cell's value when the ghost cell and the parent cell are INTERIOR, else 0.
-__device__ __forceinline__ float ghost_value(const Topo& tp, const float* __restrict__ X, int ghost_tile, const TileMeta& gm,
-                                             int off) {
-    if (!(tp.ctype[(size_t)ghost_tile * kTileCells + off] & INTERIOR_C) || gm.parent < 0) return 0.f;
-    const int oct = meta_octant(gm.packed);
-    const size_t pid = (size_t)gm.parent * kTileCells + ((oct & 1) * 4 + (off >> 7)) * 64 +
-                       (((oct >> 1) & 1) * 4 + ((off >> 4) & 3)) * 8 + ((oct >> 2) & 1) * 4 + ((off & 7) >> 1);
-    return (tp.ctype[pid] & INTERIOR_C) ? X[pid] : 0.f;
-}
-
-// FullNegativeLaplacian in one launch over LEAF|GHOST tiles: GHOST values (own or halo) are formed
-// from the parents on the fly instead of a propagation pass; LEAF tiles write A p; GHOST tiles
-// write their 2x2x2 child sums (AccumulateToParents128's order) to a per-ghost row, added to the
-// parent's A p by the p.Ap reduction that follows.
-template <int TPB>
+// FullNegativeLaplacian in one launch over LEAF|GHOST tiles.  p on GHOST tiles is kept valid by
+// the kernels that write p (push_to_ghost_child), so no propagation pass runs; LEAF tiles write
+// A p; GHOST tiles write the 2x2x2 child sums of their A p (AccumulateToParents128's order) to a
+// per-ghost row, added to the parent's A p by the p.Ap reduction that follows.  Tiles are staged
+// with asynchronous copies, NT per 128-thread group.
+template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ X,
                                                                float* __restrict__ Y, float* __restrict__ GACC,
                                                                const Scalars* __restrict__ S) {
     pdl_entry();
-    __shared__ TileShared<float> sh[TPB];
-    __shared__ float gsum[TPB][kTileCells];
+    extern __shared__ __align__(16) unsigned char lap_smem[];
+    TileStage* st = reinterpret_cast<TileStage*>(lap_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-    const int q = blockIdx.x * TPB + g;
-    const int tile = q < n ? list[q] : 0;
-    const bool active = q < n && !tile_done(tp, S, tile);
-    TileMeta m;
-    bool ghost = false;
-    if (active) {
-        m = tp.meta[tile];
-        ghost = meta_type(m.packed) & GHOST_T;
-        V4<float> own;
-        if (ghost) {
+    int tile[NT];
+    bool act[NT];
 #pragma unroll
-            for (int e = 0; e < 4; e++) own.v[e] = ghost_value(tp, X, tile, m, t * 4 + e);
-        } else {
-            own = ld4(X + (size_t)tile * kTileCells + t * 4);
-        }
-        st4(sh[g].xs + t * 4, own);
-        // face halos: x and y faces as 16-byte vectors, z faces as scalars (see load_halo)
-        if (t < 64) {
-            const int face = t >> 4, qq = t & 15;
-            const int nb = m.nb[face];
-            int off;
-            if (face == 0) off = 448 + qq * 4;
-            else if (face == 1) off = qq * 4;
-            else if (face == 2) off = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
-            else off = (qq >> 1) * 64 + (qq & 1) * 4;
-            V4<float> v = zero4<float>();
-            if (nb >= 0) {
-                if (meta_nb_ghost(m.packed, face)) {
-                    const TileMeta nm = tp.meta[nb];
-#pragma unroll
-                    for (int e = 0; e < 4; e++) v.v[e] = ghost_value(tp, X, nb, nm, off + e);
-                } else {
-                    v = ld4(X + (size_t)nb * kTileCells + off);
-                }
-            }
-            st4(sh[g].hx + face * 64 + qq * 4, v);
-        }
-        {
-            const int face = 4 + (t >> 6), c = t & 63;
-            const int nb = m.nb[face];
-            const int off = (c >> 3) * 64 + (c & 7) * 8 + (face == 4 ? 7 : 0);
-            float v = 0.f;
-            if (nb >= 0) v = meta_nb_ghost(m.packed, face) ? ghost_value(tp, X, nb, tp.meta[nb], off) : X[(size_t)nb * kTileCells + off];
-            sh[g].hx[face * 64 + c] = v;
-        }
+    for (int u = 0; u < NT; u++) {
+        const int q = (blockIdx.x * NT + u) * TPB + g;
+        tile[u] = q < n ? list[q] : 0;
+        act[u] = q < n && !tile_done(tp, S, tile[u]);
     }
-    __syncthreads();
-    if (active) {
-        const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_lap + (size_t)tile * kTileCells + t * 4);
-        const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
-        float out[4], dg[4];
-        neg_lap4<float, false, false>(sh[g].xs, sh[g].hx, t, mask4, tp.fcls[tile] & 0xfffu, L, out, dg);
-        if (ghost) {
-            const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + (size_t)tile * kTileCells + t * 4);
 #pragma unroll
-            for (int e = 0; e < 4; e++) gsum[g][t * 4 + e] = ((ct4 >> (8 * e)) & (INTERIOR_C | DIRICHLET_C | NEUMANN_C)) ? out[e] : 0.f;
+    for (int u = 0; u < NT; u++)
+        if (act[u]) stage_async(X, nullptr, tp.mask_lap, tile[u], halo_nb(tp.meta, tile[u], t), t, st[u * TPB + g]);
+    cp_async_wait_all();
+    __syncthreads();
+    bool ghost[NT];
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        ghost[u] = false;
+        if (!act[u]) continue;
+        TileStage& ts = st[u * TPB + g];
+        const int packed = tp.meta[tile[u]].packed;
+        ghost[u] = meta_type(packed) & GHOST_T;
+        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(packed));
+        float out[4], dg[4];
+        neg_lap4<float, false, false>(ts.xs, ts.hx, t, *reinterpret_cast<const uint32_t*>(ts.mask + t * 4), tp.fcls[tile[u]] & 0xfffu,
+                                      L, out, dg);
+        if (ghost[u]) {
+            const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + (size_t)tile[u] * kTileCells + t * 4);
+#pragma unroll
+            for (int e = 0; e < 4; e++) ts.b[t * 4 + e] = ((ct4 >> (8 * e)) & (INTERIOR_C | DIRICHLET_C | NEUMANN_C)) ? out[e] : 0.f;
         } else {
             V4<float> o;
             o.v[0] = out[0]; o.v[1] = out[1]; o.v[2] = out[2]; o.v[3] = out[3];
-            st4(Y + (size_t)tile * kTileCells + t * 4, o);
+            st4(Y + (size_t)tile[u] * kTileCells + t * 4, o);
         }
     }
     __syncthreads();
-    if (!active || !ghost || t >= 64) return;
+    if (t >= 64) return;
     const int fi = t / 16 * 2, fj = (t / 4) % 4 * 2, fk = t % 4 * 2;
-    float sum = 0.f;
 #pragma unroll
-    for (int ii = 0; ii < 2; ii++)
+    for (int u = 0; u < NT; u++) {
+        if (!act[u] || !ghost[u]) continue;
+        const float* gsum = st[u * TPB + g].b;
+        float sum = 0.f;
 #pragma unroll
-        for (int jj = 0; jj < 2; jj++)
+        for (int ii = 0; ii < 2; ii++)
 #pragma unroll
-            for (int kk = 0; kk < 2; kk++) sum += gsum[g][(fi + ii) * 64 + (fj + jj) * 8 + (fk + kk)];
-    GACC[(size_t)tp.ghost_slot[tile] * 64 + t] = sum;
+            for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+                for (int kk = 0; kk < 2; kk++) sum += gsum[(fi + ii) * 64 + (fj + jj) * 8 + (fk + kk)];
+        GACC[(size_t)tp.ghost_slot[tile[u]] * 64 + t] = sum;
+    }
 }
 
 // AccumulateToParents128Kernel on GHOST tiles, additive, coefficient 1, all cell types
@@ -200,38 +168,37 @@ __global__ void __launch_bounds__(64) k_accumulate_ghosts(Topo tp, const int* __
 // NegativeLaplacianAndGaussSeidelSameLevel128Kernel (src/GMGSolver.cu:216-269): on LEAF|NONLEAF
 // tiles of one level (NONLEAF counted as LEAF), cells of one colour (i+j+k)%2:
 // x += (b - A x) / D on INTERIOR cells.
-template <int TPB>
+// The tiles of a CTA are NT groups of TPB consecutive list entries, one 128-thread group per
+// tile, all staged with asynchronous copies before any is computed (NT tiles per group in flight).
+template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
                                                         const float* __restrict__ R, int color, const Scalars* __restrict__ S) {
     pdl_entry();
-    __shared__ TileShared<float> sh[TPB];
+    extern __shared__ __align__(16) unsigned char gs_smem[];
+    TileStage* st = reinterpret_cast<TileStage*>(gs_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-    const int q = blockIdx.x * TPB + g;
-    const int tile = q < n ? list[q] : 0;
-    const bool active = q < n && !tile_done(tp, S, tile);
-    TileMeta m;
-    V4<float> own;
-    if (active) {
-        m = tp.meta[tile];
-        own = stage_tile<float>(X, tile, m, t, sh[g]);
-    }
-    __syncthreads();
-    if (!active) return;
-    const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
-    const V4<float> b = ld4(R + (size_t)tile * kTileCells + t * 4);
-    const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
-    float ax[4], d[4];
-    neg_lap4<float, true>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
-    const TileIdx ix(t);
-    V4<float> o = own;
+    int tile[NT];
+    bool act[NT];
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-        if (((ix.i + ix.j + ix.k0 + e) & 1) != color) continue;
-        const bool interior = (mask4 >> (8 * e)) & kMaskInterior;
-        const float dx = interior ? (b.v[e] - ax[e]) / d[e] : 0.f;
-        o.v[e] = own.v[e] + dx;
+    for (int u = 0; u < NT; u++) {
+        const int q = (blockIdx.x * NT + u) * TPB + g;
+        tile[u] = q < n ? list[q] : 0;
+        act[u] = q < n && !tile_done(tp, S, tile[u]);
     }
-    st4(X + (size_t)tile * kTileCells + t * 4, o);
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (act[u]) stage_async(X, R, tp.mask_mg, tile[u], halo_nb(tp.meta, tile[u], t), t, st[u * TPB + g]);
+    cp_async_wait_all();
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        if (!act[u]) continue;
+        const TileStage& ts = st[u * TPB + g];
+        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(tp.meta[tile[u]].packed));
+        const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ts.mask + t * 4);
+        st4(X + (size_t)tile[u] * kTileCells + t * 4,
+            colour_update(ts.xs, ts.hx, t, mask4, (tp.fcls[tile[u]] >> 12) & 0xfffu, L, ld4(ts.b + t * 4), color));
+    }
 }
 
 // A whole sequence of colour sweeps over a small level inside one CTA (used for the coarsest
@@ -251,28 +218,17 @@ __global__ void __launch_bounds__(1024) k_gs_sequence(Topo tp, const int* __rest
             const int tile = q < n ? list[q] : 0;
             const bool active = q < n && !tile_done(tp, S, tile);
             TileMeta m;
-            V4<float> own;
             if (active) {
                 m = tp.meta[tile];
-                own = stage_tile<float>(X, tile, m, t, sh[g]);
+                stage_tile<float>(X, tile, m, t, sh[g]);
             }
             __syncthreads();
             if (active) {
                 const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
                 const V4<float> b = ld4(R + (size_t)tile * kTileCells + t * 4);
                 const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
-                float ax[4], d[4];
-                neg_lap4<float, true>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
-                const TileIdx ix(t);
-                V4<float> o = own;
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    if (((ix.i + ix.j + ix.k0 + e) & 1) != color) continue;
-                    const bool interior = (mask4 >> (8 * e)) & kMaskInterior;
-                    const float dx = interior ? (b.v[e] - ax[e]) / d[e] : 0.f;
-                    o.v[e] = own.v[e] + dx;
-                }
-                st4(X + (size_t)tile * kTileCells + t * 4, o);
+                st4(X + (size_t)tile * kTileCells + t * 4,
+                    colour_update(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, b, color));
             }
             __syncthreads();
         }
@@ -283,53 +239,63 @@ __global__ void __launch_bounds__(1024) k_gs_sequence(Topo tp, const int* __rest
 // ResidualAndRestrict128Kernel (src/GMGSolver.cu:284-339): r = rhs - A x on every cell of the
 // level's tiles; 2x2x2 sums go to the parent cell: GHOST tiles add, others overwrite
 // (times one_over_alpha).
-template <int TPB>
+template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int first, int n, const float* __restrict__ X,
                                                                  const float* RHS, float* C, float one_over_alpha,
                                                                  const Scalars* __restrict__ S) {
     pdl_entry();
-    __shared__ TileShared<float> sh[TPB];
+    extern __shared__ __align__(16) unsigned char rr_smem[];
+    TileStage* st = reinterpret_cast<TileStage*>(rr_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-    const int q = blockIdx.x * TPB + g;
-    const int tile = first + (q < n ? q : 0);
-    const bool active = q < n && !tile_done(tp, S, tile);
-    TileMeta m;
-    if (active) {
-        m = tp.meta[tile];
-        stage_tile<float>(X, tile, m, t, sh[g]);
+    int tile[NT];
+    bool act[NT];
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        const int q = (blockIdx.x * NT + u) * TPB + g;
+        tile[u] = first + (q < n ? q : 0);
+        act[u] = q < n && !tile_done(tp, S, tile[u]);
     }
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (act[u]) stage_async(X, RHS, tp.mask_mg, tile[u], halo_nb(tp.meta, tile[u], t), t, st[u * TPB + g]);
+    cp_async_wait_all();
     __syncthreads();
-    float res[4];
-    if (active) {
-        const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
-        const V4<float> b = ld4(RHS + (size_t)tile * kTileCells + t * 4);
-        const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        if (!act[u]) continue;
+        TileStage& ts = st[u * TPB + g];
+        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(tp.meta[tile[u]].packed));
         float ax[4], d[4];
-        neg_lap4<float, false>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
+        neg_lap4<float, false>(ts.xs, ts.hx, t, *reinterpret_cast<const uint32_t*>(ts.mask + t * 4),
+                               (tp.fcls[tile[u]] >> 12) & 0xfffu, L, ax, d);
+        const V4<float> b = ld4(ts.b + t * 4);
+        V4<float> r;
 #pragma unroll
-        for (int e = 0; e < 4; e++) res[e] = b.v[e] - ax[e];
-    }
-    __syncthreads();  // sh.xs is reused for the residual
-    if (active) {
-        V4<float> r4;
-        r4.v[0] = res[0]; r4.v[1] = res[1]; r4.v[2] = res[2]; r4.v[3] = res[3];
-        st4(sh[g].xs + t * 4, r4);
+        for (int e = 0; e < 4; e++) r.v[e] = b.v[e] - ax[e];
+        st4(ts.b + t * 4, r);  // the residual replaces the thread's own right-hand side values
     }
     __syncthreads();
-    if (!active || t >= 64 || m.parent < 0) return;
+    if (t >= 64) return;
     const int fi = t / 16 * 2, fj = (t / 4) % 4 * 2, fk = t % 4 * 2;
-    float sum = 0.f;
 #pragma unroll
-    for (int ii = 0; ii < 2; ii++)
+    for (int u = 0; u < NT; u++) {
+        if (!act[u]) continue;
+        const TileMeta m = tp.meta[tile[u]];
+        if (m.parent < 0) continue;
+        const float* res = st[u * TPB + g].b;
+        float sum = 0.f;
 #pragma unroll
-        for (int jj = 0; jj < 2; jj++)
+        for (int ii = 0; ii < 2; ii++)
 #pragma unroll
-            for (int kk = 0; kk < 2; kk++) sum += sh[g].xs[(fi + ii) * 64 + (fj + jj) * 8 + (fk + kk)];
-    const int oct = meta_octant(m.packed);
-    const size_t pid = (size_t)m.parent * kTileCells + ((oct & 1) * 4 + fi / 2) * 64 + (((oct >> 1) & 1) * 4 + fj / 2) * 8 +
-                       ((oct >> 2) & 1) * 4 + fk / 2;
-    if (meta_type(m.packed) & GHOST_T) C[pid] += sum;
-    else C[pid] = sum * one_over_alpha;
+            for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+                for (int kk = 0; kk < 2; kk++) sum += res[(fi + ii) * 64 + (fj + jj) * 8 + (fk + kk)];
+        const int oct = meta_octant(m.packed);
+        const size_t pid = (size_t)m.parent * kTileCells + ((oct & 1) * 4 + fi / 2) * 64 + (((oct >> 1) & 1) * 4 + fj / 2) * 8 +
+                           ((oct >> 2) & 1) * 4 + fk / 2;
+        if (meta_type(m.packed) & GHOST_T) C[pid] += sum;
+        else C[pid] = sum * one_over_alpha;
+    }
 }
 
 // ------------------------------------------------------------------ prolongation + update
@@ -569,6 +535,36 @@ __device__ __forceinline__ bool chunk_reduce_and_elect(double a, double b, doubl
     return threadIdx.x == 0;
 }
 
+// PropagateValuesToGhostTiles (src/PoissonGrid.cu:585-605) for the GHOST child, if any, of the
+// octant holding the four cells (i, j, k0..k0+3) of vector qv of LEAF tile `tile`: the 2x2x2
+// children of each cell take its new value p where child and parent cell are INTERIOR, 0
+// elsewhere.  Every GHOST tile is the child of a LEAF tile, so the kernels that write p on LEAF
+// tiles keep p valid on all GHOST tiles and the Laplacian reads it there directly.
+__device__ __forceinline__ void push_to_ghost_child(const Topo& tp, float* P, int tile, int qv, const V4<float>& p, uint32_t ct4) {
+    const int i = qv >> 4, j = (qv >> 1) & 7, k0 = (qv & 1) * 4;
+    const int gs = tp.ghost_child[(size_t)tile * 8 + ((i >> 2) | ((j >> 2) << 1) | ((k0 >> 2) << 2))];
+    if (gs < 0) return;
+    const int gt = tp.ghost_list[gs];
+    float pv[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) pv[e] = ((ct4 >> (8 * e)) & INTERIOR_C) ? p.v[e] : 0.f;
+#pragma unroll
+    for (int di = 0; di < 2; di++)
+#pragma unroll
+        for (int dj = 0; dj < 2; dj++) {
+            const size_t row = (size_t)gt * kTileCells + (2 * (i & 3) + di) * 64 + (2 * (j & 3) + dj) * 8;
+            const uint2 cc = *reinterpret_cast<const uint2*>(tp.ctype + row);
+            V4<float> lo, hi;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                lo.v[k] = ((cc.x >> (8 * k)) & INTERIOR_C) ? pv[k >> 1] : 0.f;
+                hi.v[k] = ((cc.y >> (8 * k)) & INTERIOR_C) ? pv[2 + (k >> 1)] : 0.f;
+            }
+            st4(P + row, lo);
+            st4(P + row + 4, hi);
+        }
+}
+
 // Per-instance reduction over the 4-cell vectors of LEAF tiles, one CTA per chunk (the chunk table
 // cuts every instance's leaf vectors into pieces of kChunkVecs).  OP selects the fused
 // elementwise work done while reducing:
@@ -604,9 +600,10 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
             const V4<float> r = ld4(B + off);
             if (D) st4(D + off, r);
             acc_a += dot4f(r, r);
-        } else if (OP == OP_COPY_DOT) {  // A = z, B = r, C = p
+        } else if (OP == OP_COPY_DOT) {  // A = z, B = r, C = p (also on the GHOST children)
             const V4<float> z = ld4(A + off);
             st4(C + off, z);
+            push_to_ghost_child(tp, C, tile, v & 127, z, *reinterpret_cast<const uint32_t*>(tp.ctype + off));
             acc_a += dot4f(z, ld4(B + off));
         } else if (OP == OP_XR) {  // A = x, B = p, C = r, D = Ap
             const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
@@ -670,7 +667,8 @@ __global__ void __launch_bounds__(256) k_begin(Scalars* S, const InstParams* __r
     }
 }
 
-// p = z + beta p on INTERIOR cells of LEAF tiles (src/GMGSolver.cu:642-653), per instance.
+// p = z + beta p on INTERIOR cells of LEAF tiles (src/GMGSolver.cu:642-653), per instance; the
+// GHOST children receive the new p (push_to_ghost_child).
 __global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict__ leaves, int nleaf, float* P,
                                                   const float* __restrict__ Z, const Scalars* S) {
     pdl_entry();
@@ -688,6 +686,7 @@ __global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict
         for (int e = 0; e < 4; e++)
             if ((ct4 >> (8 * e)) & INTERIOR_C) p.v[e] = fmaf(beta, p.v[e], z.v[e]);
         st4(P + off, p);
+        push_to_ghost_child(tp, P, tile, (int)(v & 127), p, ct4);
     }
 }
 
@@ -826,18 +825,44 @@ void full_laplacian(const DevGrid& g, T* X, T* Y, const Scalars* S, cudaStream_t
 template void full_laplacian<float>(const DevGrid&, float*, float*, const Scalars*, cudaStream_t);
 template void full_laplacian<double>(const DevGrid&, double*, double*, const Scalars*, cudaStream_t);
 
+template <int TPB, int NT>
+void laplacian_shape(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s) {
+    const int per = TPB * NT;
+    launch_kernel(k_laplacian_fused<TPB, NT>, (g.n_leafghost + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
+                  g.d_leafghost, g.n_leafghost, X, Y, g.d_gacc, S);
+}
+
 void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s) {
     if (g.n_leafghost == 0) return;
     ++g.launch_count;
-    launch_kernel(k_laplacian_fused<kTPB>, (g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.d_leafghost,
-                  g.n_leafghost, X, Y, g.d_gacc, S);
+    switch (g.shape(KS_LAPLACIAN, 0)) {
+    case 0: laplacian_shape<2, 1>(g, X, Y, S, s); break;
+    case 1: laplacian_shape<2, 2>(g, X, Y, S, s); break;
+    case 2: laplacian_shape<1, 4>(g, X, Y, S, s); break;
+    default: laplacian_shape<2, 4>(g, X, Y, S, s); break;
+    }
+}
+
+// Launch shapes of the staged kernels: TPB tiles per CTA side by side, NT tiles per 128-thread
+// group in flight.
+template <int TPB, int NT>
+void gs_sweep_shape(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s) {
+    const int n = g.mg_count[level];
+    const int per = TPB * NT;
+    launch_kernel(k_gs_sweep<TPB, NT>, (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
+                  g.d_mg + g.mg_offset[level], n, X, R, color, S);
 }
 
 void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s) {
     const int n = g.mg_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    launch_kernel(k_gs_sweep<kTPB>, (n + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.d_mg + g.mg_offset[level], n, X, R, color, S);
+    switch (g.shape(KS_GS_SWEEP, level)) {
+    case 0: gs_sweep_shape<2, 1>(g, level, X, R, color, S, s); break;
+    case 1: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s); break;
+    case 2: gs_sweep_shape<1, 4>(g, level, X, R, color, S, s); break;
+    default: gs_sweep_shape<2, 4>(g, level, X, R, color, S, s); break;
+    }
 }
 
 void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t colors, int nsweeps, const Scalars* S,
@@ -852,13 +877,26 @@ void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t
     for (int k = 0; k < nsweeps; k++) gs_sweep(g, level, X, R, (colors >> k) & 1, S, s);
 }
 
+template <int TPB, int NT>
+void residual_shape(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha, const Scalars* S,
+                    cudaStream_t s) {
+    const int n = g.level_count[level];
+    const int per = TPB * NT;
+    launch_kernel(k_residual_restrict<TPB, NT>, (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
+                  g.level_first[level], n, X, RHS, C, one_over_alpha, S);
+}
+
 void residual_restrict(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha,
                        const Scalars* S, cudaStream_t s) {
     const int n = g.level_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    launch_kernel(k_residual_restrict<kTPB>, (n + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.level_first[level], n, X, RHS, C,
-                  one_over_alpha, S);
+    switch (g.shape(KS_RESIDUAL, level)) {
+    case 0: residual_shape<2, 1>(g, level, X, RHS, C, one_over_alpha, S, s); break;
+    case 1: residual_shape<2, 2>(g, level, X, RHS, C, one_over_alpha, S, s); break;
+    case 2: residual_shape<1, 4>(g, level, X, RHS, C, one_over_alpha, S, s); break;
+    default: residual_shape<2, 4>(g, level, X, RHS, C, one_over_alpha, S, s); break;
+    }
 }
 
 void prolongate(const DevGrid& g, int level, const float* CX, float* FX, float prolong_coeff, const Scalars* S, cudaStream_t s) {
@@ -874,6 +912,15 @@ void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const S
     if (blocks < 1) blocks = 1;
     ++g.launch_count;
     launch_kernel(k_vcycle_init, blocks, 256, 0, s, g.topo, g.n, X, RHS, F, S);
+}
+
+void init_stencil_attributes() {
+    static bool done = false;
+    if (done) return;
+    done = true;
+    cudaFuncSetAttribute(k_gs_sweep<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
+    cudaFuncSetAttribute(k_laplacian_fused<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
+    cudaFuncSetAttribute(k_residual_restrict<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
 }
 
 bool pdl_enabled() {

@@ -46,15 +46,24 @@ template <bool FUSED> __device__ __forceinline__ double fmadd(double a, double b
 
 // Per-level constants of the stencil.  h = h0 / 2^level (src/HAAccessor.h:72-74); c1 = 1/h^2;
 // c2 = (2*(1/h)/3)*(1/h) exactly as the reference rounds it.
+// dfast: the diagonal of a cell with six 1/h^2 faces, summed and scaled as neg_lap4 does.
 template <class T> struct LevelConst {
-    T h, c1, c2;
+    T h, c1, c2, dfast;
     __device__ __forceinline__ LevelConst(T h0, int level) {
         h = h0 / T(1 << level);
         const T ooh = T(1) / h;
         c1 = ooh * ooh;                  // (ooh*1 + x*0) * ooh
         c2 = (T(2) * ooh / T(3)) * ooh;  // (ooh*0 + (2*ooh/3)*1) * ooh
+        T d = T(0);
+        d = d + c1; d = d + c1; d = d + c1; d = d + c1; d = d + c1; d = d + c1;
+        dfast = d * h * h * h;
     }
 };
+
+// s * h * h * h rounded after each product, as three separate multiplies (intrinsics, so the
+// compiler never fuses the last product into a following addition).
+__device__ __forceinline__ float mul_h3(float s, float h) { return __fmul_rn(__fmul_rn(__fmul_rn(s, h), h), h); }
+__device__ __forceinline__ double mul_h3(double s, double h) { return __dmul_rn(__dmul_rn(__dmul_rn(s, h), h), h); }
 
 struct TileIdx {
     int i, j, k0;
@@ -103,6 +112,26 @@ __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32
     const V4<T> yp = ix.j < 7 ? ld4(xs + (t + 2) * 4) : ld4(hx + 3 * 64 + ix.i * 8 + ix.k0);
     const T zlo = ix.k0 > 0 ? xs[t * 4 - 1] : hx[4 * 64 + ix.i * 8 + ix.j];
     const T zhi = ix.k0 < 4 ? xs[t * 4 + 4] : hx[5 * 64 + ix.i * 8 + ix.j];
+    if (mask4 == 0x7F7F7F7Fu) {
+        // the four cells are INTERIOR with six 1/h^2 faces: every coefficient is c1 (the same
+        // operations as the general path below with a_f = c1)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const T x0 = xc.v[e];
+            const T zl = e > 0 ? xc.v[e - 1] : zlo;
+            const T zr = e < 3 ? xc.v[e + 1] : zhi;
+            T s = T(0);
+            s = fmadd<FUSED>(L.c1, x0 - xm.v[e], s);
+            s = fmadd<FUSED>(L.c1, x0 - xp.v[e], s);
+            s = fmadd<FUSED>(L.c1, x0 - ym.v[e], s);
+            s = fmadd<FUSED>(L.c1, x0 - yp.v[e], s);
+            s = fmadd<FUSED>(L.c1, x0 - zl, s);
+            s = fmadd<FUSED>(L.c1, x0 - zr, s);
+            out[e] = mul_h3(s, L.h);
+            if (DIAG) diag[e] = L.dfast;
+        }
+        return;
+    }
     auto cross = [&](int f) -> T { return ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1; };
     const T cxm = ix.i == 0 ? cross(0) : L.c1;
     const T cxp = ix.i == 7 ? cross(1) : L.c1;
@@ -136,6 +165,127 @@ __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32
             d = d + a0; d = d + a1; d = d + a2; d = d + a3; d = d + a4; d = d + a5;
             diag[e] = interior ? d * L.h * L.h * L.h : T(0);
         }
+    }
+}
+
+// One Gauss-Seidel update x0 + (b - A x)/D of a single cell with mask byte m at local (i, j, k),
+// given its six neighbour values in face order: the operations of neg_lap4 + the sweep update.
+__device__ __forceinline__ float gs_cell(float x0, float xm, float xp, float ym, float yp, float zl, float zr, float b, uint32_t m,
+                                         int i, int j, int k, uint32_t cls, const LevelConst<float>& L) {
+    if (m == (uint32_t)kMaskFull) {
+        float s = 0.f;
+        s = fmaf(L.c1, x0 - xm, s);
+        s = fmaf(L.c1, x0 - xp, s);
+        s = fmaf(L.c1, x0 - ym, s);
+        s = fmaf(L.c1, x0 - yp, s);
+        s = fmaf(L.c1, x0 - zl, s);
+        s = fmaf(L.c1, x0 - zr, s);
+        return x0 + (b - mul_h3(s, L.h)) / L.dfast;
+    }
+    auto cross = [&](int f) -> float { return ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1; };
+    const float a0 = (m & 1u) ? (i == 0 ? cross(0) : L.c1) : 0.f;
+    const float a1 = (m & 2u) ? (i == 7 ? cross(1) : L.c1) : 0.f;
+    const float a2 = (m & 4u) ? (j == 0 ? cross(2) : L.c1) : 0.f;
+    const float a3 = (m & 8u) ? (j == 7 ? cross(3) : L.c1) : 0.f;
+    const float a4 = (m & 16u) ? (k == 0 ? cross(4) : L.c1) : 0.f;
+    const float a5 = (m & 32u) ? (k == 7 ? cross(5) : L.c1) : 0.f;
+    float s = 0.f;
+    s = fmaf(a0, x0 - xm, s);
+    s = fmaf(a1, x0 - xp, s);
+    s = fmaf(a2, x0 - ym, s);
+    s = fmaf(a3, x0 - yp, s);
+    s = fmaf(a4, x0 - zl, s);
+    s = fmaf(a5, x0 - zr, s);
+    const bool interior = m & kMaskInterior;
+    const float ax = interior ? s * L.h * L.h * L.h : 0.f;
+    float d = 0.f;
+    d = d + a0; d = d + a1; d = d + a2; d = d + a3; d = d + a4; d = d + a5;
+    const float dd = interior ? d * L.h * L.h * L.h : 0.f;
+    return x0 + (interior ? (b - ax) / dd : 0.f);
+}
+
+// One colour of a red-black sweep on thread t's four cells: the two cells of colour `color`
+// (k0 is even, so they are e = p and p + 2 with p = (color + i + j) & 1) get the update, the
+// other two keep their values.  xs/hx: the tile and its halos in shared memory.
+__device__ __forceinline__ V4<float> colour_update(const float* xs, const float* hx, int t, uint32_t mask4, uint32_t cls,
+                                                   const LevelConst<float>& L, const V4<float>& b, int color) {
+    const TileIdx ix(t);
+    const V4<float> xc = ld4(xs + t * 4);
+    const V4<float> xm = ix.i > 0 ? ld4(xs + (t - 16) * 4) : ld4(hx + 0 * 64 + ix.j * 8 + ix.k0);
+    const V4<float> xp = ix.i < 7 ? ld4(xs + (t + 16) * 4) : ld4(hx + 1 * 64 + ix.j * 8 + ix.k0);
+    const V4<float> ym = ix.j > 0 ? ld4(xs + (t - 2) * 4) : ld4(hx + 2 * 64 + ix.i * 8 + ix.k0);
+    const V4<float> yp = ix.j < 7 ? ld4(xs + (t + 2) * 4) : ld4(hx + 3 * 64 + ix.i * 8 + ix.k0);
+    const float zlo = ix.k0 > 0 ? xs[t * 4 - 1] : hx[4 * 64 + ix.i * 8 + ix.j];
+    const float zhi = ix.k0 < 4 ? xs[t * 4 + 4] : hx[5 * 64 + ix.i * 8 + ix.j];
+    const bool p = (color + ix.i + ix.j) & 1;
+    const uint32_t mA = (mask4 >> (p ? 8 : 0)) & 0xffu, mB = (mask4 >> (p ? 24 : 16)) & 0xffu;
+    const float A = gs_cell(p ? xc.v[1] : xc.v[0], p ? xm.v[1] : xm.v[0], p ? xp.v[1] : xp.v[0], p ? ym.v[1] : ym.v[0],
+                            p ? yp.v[1] : yp.v[0], p ? xc.v[0] : zlo, p ? xc.v[2] : xc.v[1], p ? b.v[1] : b.v[0], mA, ix.i, ix.j,
+                            ix.k0 + (p ? 1 : 0), cls, L);
+    const float B = gs_cell(p ? xc.v[3] : xc.v[2], p ? xm.v[3] : xm.v[2], p ? xp.v[3] : xp.v[2], p ? ym.v[3] : ym.v[2],
+                            p ? yp.v[3] : yp.v[2], p ? xc.v[2] : xc.v[1], p ? zhi : xc.v[3], p ? b.v[3] : b.v[2], mB, ix.i, ix.j,
+                            ix.k0 + (p ? 3 : 2), cls, L);
+    V4<float> o = xc;
+    if (p) { o.v[1] = A; o.v[3] = B; } else { o.v[0] = A; o.v[2] = B; }
+    return o;
+}
+
+// Asynchronous global -> shared copies (cp.async): the data goes straight to shared memory
+// without passing through registers, so a CTA can keep several tiles' loads in flight at once.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Staging area of one tile: its values, face halos, a second channel (right-hand side) and the
+// stencil mask bytes.
+struct __align__(16) TileStage {
+    float xs[kTileCells];
+    float hx[6 * 64];
+    float b[kTileCells];
+    uint8_t mask[kTileCells];
+};
+
+// Neighbour tiles whose halo cells thread t copies: face t>>4 (threads 0..63, 16-byte pieces of
+// an x or y face) and z face 4 + (t>>6) (one scalar).
+struct HaloNb {
+    int f, z;
+};
+__device__ __forceinline__ HaloNb halo_nb(const TileMeta* __restrict__ meta, int tile, int t) {
+    HaloNb h;
+    h.f = t < 64 ? meta[tile].nb[t >> 4] : -1;
+    h.z = meta[tile].nb[4 + (t >> 6)];
+    return h;
+}
+
+// Issue the copies of `tile` into st: channel X's values and face halos (0 for absent
+// neighbours), channel B (if given) and the mask bytes (if given).  Completed by
+// cp_async_wait_all + __syncthreads.
+__device__ __forceinline__ void stage_async(const float* __restrict__ X, const float* __restrict__ B, const uint8_t* __restrict__ mask,
+                                            int tile, HaloNb nb, int t, TileStage& st) {
+    const size_t base = (size_t)tile * kTileCells;
+    cp_async16(st.xs + t * 4, X + base + t * 4);
+    if (B) cp_async16(st.b + t * 4, B + base + t * 4);
+    if (mask && t < 32) cp_async16(st.mask + t * 16, mask + base + t * 16);
+    if (t < 64) {
+        const int face = t >> 4, q = t & 15;
+        int off;
+        if (face == 0) off = 448 + q * 4;
+        else if (face == 1) off = q * 4;
+        else if (face == 2) off = (q >> 1) * 64 + 56 + (q & 1) * 4;
+        else off = (q >> 1) * 64 + (q & 1) * 4;
+        if (nb.f >= 0) cp_async16(st.hx + face * 64 + q * 4, X + (size_t)nb.f * kTileCells + off);
+        else st4(st.hx + face * 64 + q * 4, zero4<float>());
+    }
+    {
+        const int face = 4 + (t >> 6), c = t & 63;
+        if (nb.z >= 0) cp_async4(st.hx + face * 64 + c, X + (size_t)nb.z * kTileCells + (c >> 3) * 64 + (c & 7) * 8 + (face == 4 ? 7 : 0));
+        else st.hx[face * 64 + c] = 0.f;
     }
 }
 

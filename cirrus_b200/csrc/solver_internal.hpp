@@ -52,6 +52,12 @@ struct GraphKey {
     }
 };
 
+// Kernels with selectable launch shapes (tiles per CTA x tiles in flight per thread group); the
+// choice per kernel and level is made by the autotuner (autotune.cu) and is bit-neutral: every
+// shape computes each tile with the same operations.
+enum { KS_GS_SWEEP = 0, KS_PRESMOOTH = 1, KS_PROLONG = 2, KS_RESIDUAL = 3, KS_LAPLACIAN = 4, KS_COUNT = 5 };
+constexpr int kNumShapes = 4;
+
 // A contiguous run of one instance's tiles inside the merged pool: tiles local..local+count of
 // the instance's all-tiles order are global..global+count (one run per level).
 struct TileRun {
@@ -95,6 +101,8 @@ struct DevGrid {
     int n_leaf = 0, n_ghost = 0, n_leafghost = 0;
     std::vector<int> mg_offset, mg_count, level_first, level_count;
     std::vector<uint8_t> h_tile_type;
+    std::vector<uint8_t> shapes;  // KS_COUNT x num_layers launch-shape choices
+    int shape(int kind, int level) const { return shapes.empty() ? 1 : shapes[(size_t)kind * num_layers + level]; }
 
     // coarse levels 0..bottom_level of every instance in the shared-memory kernel (-1: none)
     int bottom_level = -1;
@@ -209,6 +217,7 @@ bool bottom_supported(int coarsest_iters, int lb);
 constexpr int kBottomSmemBudget = 224 * 1024;  // dynamic shared memory of the coarse-level kernel
 size_t bottom_smem_bytes(long long cells, int tiles);
 void init_kernel_attributes();
+void init_stencil_attributes();
 // array-of-tiles interop (interop.cu)
 void gather_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream_t s);
 void scatter_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream_t s);

@@ -29,6 +29,7 @@ namespace {
 // Diagonal h^3 * sum_f c_f of cell (i, j, k) with stencil mask mm in a tile whose multigrid
 // cross-face classes are `cls`: the summation order of neg_lap4's diagonal.
 __device__ __forceinline__ float cell_diag(int i, int j, int k, uint32_t mm, uint32_t cls, const LevelConst<float>& L) {
+    if (mm == (uint32_t)kMaskFull) return L.dfast;
     auto cross = [&](int f) -> float { return ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1; };
     const float a0 = (mm & 1u) ? (i == 0 ? cross(0) : L.c1) : 0.f;
     const float a1 = (mm & 2u) ? (i == 7 ? cross(1) : L.c1) : 0.f;
@@ -104,17 +105,28 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
             x1.v[e] = v;
         }
         st4(sh[g].xs + t * 4, x1);
-        // first colour of the face neighbours' first cell layer
+        // first colour of the face neighbours' first cell layer; x and y faces as runs of four
+        // cells along k (one 16-byte right-hand-side load and one 4-byte mask load)
         if (t < 64) {
             const int face = t >> 4, qq = t & 15;
             const int nb = m.nb[face];
-            const bool live = nb >= 0 && !meta_nb_ghost(m.packed, face);
-            V4<float> v;
+            V4<float> v = zero4<float>();
+            if (nb >= 0 && !meta_nb_ghost(m.packed, face)) {
+                int off;
+                if (face == 0) off = 448 + qq * 4;
+                else if (face == 1) off = qq * 4;
+                else if (face == 2) off = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
+                else off = (qq >> 1) * 64 + (qq & 1) * 4;
+                const V4<float> nbb = ld4(RHS + (size_t)nb * kTileCells + off);
+                const uint32_t nm4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)nb * kTileCells + off);
+                const uint32_t ncls = (tp.fcls[nb] >> 12) & 0xfffu;
+                const int ni = off >> 6, nj = (off >> 3) & 7, nk0 = off & 7;
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
-                int i, j, k;
-                halo_cell_ijk(face, qq * 4 + e, i, j, k);
-                v.v[e] = live ? first_colour(tp, RHS, nb, i, j, k, L) : 0.f;
+                for (int e = 0; e < 4; e++) {
+                    const uint32_t mm = (nm4 >> (8 * e)) & 0xffu;
+                    if (((ni + nj + nk0 + e) & 1) == 0 && (mm & kMaskInterior))
+                        v.v[e] = 0.f + (nbb.v[e] - 0.f) / cell_diag(ni, nj, nk0 + e, mm, ncls, L);
+                }
             }
             st4(sh[g].hx + face * 64 + qq * 4, v);
         }
@@ -129,16 +141,7 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
     __syncthreads();
     if (!active) return;
     // second colour (1), from the first-colour values
-    float ax[4], d[4];
-    neg_lap4<float, true>(sh[g].xs, sh[g].hx, t, mask4, cls, L, ax, d);
-    V4<float> o = ld4(sh[g].xs + t * 4);
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-        if (((ix.i + ix.j + ix.k0 + e) & 1) != 1) continue;
-        const bool interior = (mask4 >> (8 * e)) & kMaskInterior;
-        o.v[e] = o.v[e] + (interior ? (b.v[e] - ax[e]) / d[e] : 0.f);
-    }
-    st4(XP + (size_t)tile * kTileCells + t * 4, o);
+    st4(XP + (size_t)tile * kTileCells + t * 4, colour_update(sh[g].xs, sh[g].hx, t, mask4, cls, L, b, 1));
 }
 
 // ---------------------------------------------------------------------------- up: prolongation + first colour
@@ -154,6 +157,32 @@ __device__ __forceinline__ float prolongated(const Topo& tp, const float* __rest
                ((oct >> 2) & 1) * 4 + ((off & 7) >> 1)];
     }
     return (meta_type(tm.packed) & GHOST_T) ? cx : fmaf(prolong_coeff, cx, XP[(size_t)tile * kTileCells + off]);
+}
+
+// prolongated() for the four cells off4..off4+3 (off4 a multiple of 4: one run along k, whose
+// parent values are two consecutive cells).
+__device__ __forceinline__ V4<float> prolongated4(const Topo& tp, const float* __restrict__ Z, const float* __restrict__ XP, int tile,
+                                                  const TileMeta& tm, int off4, float prolong_coeff) {
+    const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + off4);
+    const bool ghost = meta_type(tm.packed) & GHOST_T;
+    float cx0 = 0.f, cx1 = 0.f;
+    if (tm.parent >= 0) {
+        const int oct = meta_octant(tm.packed);
+        const float2 c = *reinterpret_cast<const float2*>(
+            Z + (size_t)tm.parent * kTileCells + ((oct & 1) * 4 + (off4 >> 7)) * 64 + (((oct >> 1) & 1) * 4 + ((off4 >> 4) & 3)) * 8 +
+            ((oct >> 2) & 1) * 4 + ((off4 & 7) >> 1));
+        cx0 = c.x;
+        cx1 = c.y;
+    }
+    V4<float> xp = zero4<float>();
+    if (!ghost) xp = ld4(XP + (size_t)tile * kTileCells + off4);
+    V4<float> o;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const float cx = e < 2 ? cx0 : cx1;
+        o.v[e] = ((mask4 >> (8 * e)) & kMaskInterior) ? (ghost ? cx : fmaf(prolong_coeff, cx, xp.v[e])) : 0.f;
+    }
+    return o;
 }
 
 // Prolongation into every tile of one level; on mg tiles also the first colour (1) of
@@ -173,10 +202,7 @@ __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first,
     if (active) {
         m = tp.meta[tile];
         ghost = meta_type(m.packed) & GHOST_T;
-        V4<float> own;
-#pragma unroll
-        for (int e = 0; e < 4; e++) own.v[e] = prolongated(tp, Z, XP, tile, m, t * 4 + e, prolong_coeff);
-        st4(sh[g].xs + t * 4, own);
+        st4(sh[g].xs + t * 4, prolongated4(tp, Z, XP, tile, m, t * 4, prolong_coeff));
         if (!ghost) {
             if (t < 64) {
                 const int face = t >> 4, qq = t & 15;
@@ -186,13 +212,7 @@ __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first,
                 else if (face == 1) off = qq * 4;
                 else if (face == 2) off = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
                 else off = (qq >> 1) * 64 + (qq & 1) * 4;
-                V4<float> v = zero4<float>();
-                if (nb >= 0) {
-                    const TileMeta nm = tp.meta[nb];
-#pragma unroll
-                    for (int e = 0; e < 4; e++) v.v[e] = prolongated(tp, Z, XP, nb, nm, off + e, prolong_coeff);
-                }
-                st4(sh[g].hx + face * 64 + qq * 4, v);
+                st4(sh[g].hx + face * 64 + qq * 4, nb >= 0 ? prolongated4(tp, Z, XP, nb, tp.meta[nb], off, prolong_coeff) : zero4<float>());
             }
             {
                 const int face = 4 + (t >> 6), c = t & 63;
@@ -210,15 +230,7 @@ __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first,
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
         const V4<float> b = ld4(RHS + (size_t)tile * kTileCells + t * 4);
         const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
-        float ax[4], d[4];
-        neg_lap4<float, true>(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, ax, d);
-        const TileIdx ix(t);
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            if (((ix.i + ix.j + ix.k0 + e) & 1) != 1) continue;
-            const bool interior = (mask4 >> (8 * e)) & kMaskInterior;
-            o.v[e] = o.v[e] + (interior ? (b.v[e] - ax[e]) / d[e] : 0.f);
-        }
+        o = colour_update(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, b, 1);
     }
     st4(Z + (size_t)tile * kTileCells + t * 4, o);
 }
@@ -253,6 +265,17 @@ __device__ __forceinline__ float box_neglap(const float* X, int q, uint32_t code
                                             float* diag) {
     const float x0 = X[q];
     const float xm = X[q - sy], xp = X[q + sy], ym = X[q - sz], yp = X[q + sz], zm = X[q - 1], zp = X[q + 1];
+    if ((code & 0x1FFFu) == (uint32_t)kMaskFull) {  // INTERIOR, six 1/h^2 faces
+        float s = 0.f;
+        s = fmaf(L.c1, x0 - xm, s);
+        s = fmaf(L.c1, x0 - xp, s);
+        s = fmaf(L.c1, x0 - ym, s);
+        s = fmaf(L.c1, x0 - yp, s);
+        s = fmaf(L.c1, x0 - zm, s);
+        s = fmaf(L.c1, x0 - zp, s);
+        if (DIAG) *diag = L.dfast;
+        return mul_h3(s, L.h);
+    }
     auto coef = [&](int f) -> float { return ((code >> f) & 1u) ? (((code >> (7 + f)) & 1u) ? L.c2 : L.c1) : 0.f; };
     const float a0 = coef(0), a1 = coef(1), a2 = coef(2), a3 = coef(3), a4 = coef(4), a5 = coef(5);
     float s = 0.f;
