@@ -222,6 +222,11 @@ class DeviceGrid:
               "cirrus_grid_get_channel_instance")
         return out
 
+    def autotune(self, reps: int = 20, stream: int = 0) -> None:
+        """Pick the fastest launch shape of each staged stencil kernel per level on this grid
+        (results are unchanged by the choice); overwrites channels 2-5."""
+        check(lib().cirrus_grid_autotune(self._h, reps, C.c_void_p(stream)), "cirrus_grid_autotune")
+
     def bench_launch(self, kernel: int, level: int = 0, reps: int = 1, stream: int = 0) -> None:
         """Launch one solve kernel `reps` times on `stream` (for timing with the caller's events);
         overwrites channels 2-5."""

@@ -116,6 +116,7 @@ _PROTOS = {
     "cirrus_gmg_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_int_p, c_f64_p, C.c_void_p,
                                          C.POINTER(SolveResult)]),
     "cirrus_gmg_solve_host": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p, C.POINTER(SolveResult)]),
+    "cirrus_grid_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "cirrus_bench_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_true_residual": (C.c_int, [C.c_void_p, c_f32_p, c_f64_p, C.c_void_p]),
     "cirrus_grid_get_solution_f64": (C.c_int, [C.c_void_p, c_f64_p, C.c_void_p]),

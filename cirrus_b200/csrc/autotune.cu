@@ -1,0 +1,84 @@
+// Autotuner of the launch shapes: for every kernel with selectable shapes and every level it runs
+// on, each shape is timed on the grid itself (back-to-back launches captured in a CUDA graph,
+// CUDA events around one graph launch) and the fastest is kept.  The shapes compute every tile
+// with the same operations, so the choice changes timing only, never results.
+#include "solver_internal.hpp"
+
+#include <cstdio>
+
+namespace cirrus {
+
+namespace {
+
+template <class F>
+float time_graph(F launch, int reps, cudaStream_t s) {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    float ms = -1.f;
+    launch();  // first run outside the graph (lazy loading of the kernel)
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return -1.f;
+    for (int i = 0; i < reps; i++) launch();
+    if (cudaStreamEndCapture(s, &graph) != cudaSuccess || !graph) return -1.f;
+    if (cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaGraphLaunch(exec, s);  // warm
+        cudaEventRecord(a, s);
+        cudaGraphLaunch(exec, s);
+        cudaEventRecord(b, s);
+        if (cudaEventSynchronize(b) == cudaSuccess) cudaEventElapsedTime(&ms, a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaGraphExecDestroy(exec);
+    }
+    cudaGraphDestroy(graph);
+    return ms;
+}
+
+}  // namespace
+
+int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
+    if (reps < 1) reps = 1;
+    // timing runs on a private stream (the caller's may be the legacy default stream, which
+    // cannot be captured), after the caller's pending work
+    if (cudaStreamSynchronize(user) != cudaSuccess) return 2;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return 2;
+    float *p = g.d_ch[kChP], *ap = g.d_ch[kChAp], *z = g.d_ch[kChZ], *tmp = g.d_ch[kChTmp];
+    const long long count0 = g.launch_count;
+    const int lo = g.bottom_level >= 0 ? g.bottom_level + 1 : 0;
+    auto pick = [&](int kind, int level, auto&& launch) {
+        float best = 0.f;
+        int best_shape = g.shape(kind, level);
+        for (int sh = 0; sh < kNumShapes; sh++) {
+            g.shapes[(size_t)kind * g.num_layers + level] = (uint8_t)sh;
+            const float ms = time_graph(launch, reps, s);
+            if (ms > 0.f && (best == 0.f || ms < best)) {
+                best = ms;
+                best_shape = sh;
+            }
+        }
+        g.shapes[(size_t)kind * g.num_layers + level] = (uint8_t)best_shape;
+        if (report) {
+            char line[128];
+            std::snprintf(line, sizeof line, "kind %d level %d shape %d %.2f us\n", kind, level, best_shape, 1e3f * best / reps);
+            *report += line;
+        }
+    };
+    for (int l = lo; l <= g.max_level; l++) {
+        if (g.mg_count[l] > 0) pick(KS_GS_SWEEP, l, [&] { launch::gs_sweep(g, l, z, ap, 0, nullptr, s); });
+        if (l >= 1 && g.level_count[l] > 0)
+            pick(KS_RESIDUAL, l, [&] { launch::residual_restrict(g, l, g.d_xpre, ap, tmp, 1.f, nullptr, s); });
+    }
+    if (g.n_leafghost > 0) pick(KS_LAPLACIAN, 0, [&] { launch::laplacian_fused(g, p, tmp, nullptr, s); });
+    g.launch_count = count0;
+    // solve graphs captured with the previous shapes are rebuilt on the next solve
+    for (auto& kv : g.graphs) cudaGraphExecDestroy(kv.second.exec);
+    g.graphs.clear();
+    const bool ok = cudaStreamSynchronize(s) == cudaSuccess;
+    cudaStreamDestroy(s);
+    return ok ? 0 : 2;
+}
+
+}  // namespace cirrus

@@ -484,6 +484,11 @@ cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params
     return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
 }
 
+cirrus_status cirrus_grid_autotune(cirrus_grid* grid, int reps, void* stream) {
+    if (!grid) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return map_rc(cirrus::autotune(*grid->g, S(stream), reps > 0 ? reps : 20, nullptr)); });
+}
+
 cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int reps, void* stream) {
     if (!grid || reps < 0) return CIRRUS_ERR_INVALID_ARGUMENT;
     auto& g = *grid->g;

@@ -263,6 +263,10 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
 // FP64 true relative residual of the last solution of each instance against b (device FP32
 // channel): the FP64 x of a mixed-precision solve, else channel 0 widened to FP64.
 int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s);
+// Times every launch shape of the shape-selectable kernels on this grid and keeps the fastest per
+// kernel and level (autotune.cu); overwrites the scratch channels 2-5.  report (optional) gets one
+// line per choice.
+int autotune(DevGrid& g, cudaStream_t s, int reps, std::string* report);
 // Copy the last solution to the host in FP64 (num_tiles*512 doubles, pool order).
 int solution_f64(DevGrid& g, double* host, cudaStream_t s);
 

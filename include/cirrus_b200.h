@@ -250,6 +250,13 @@ cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params
  * mixed-precision solve, else channel 0 widened.  Channel 0 always holds its FP32 rounding. */
 cirrus_status cirrus_grid_get_solution_f64(cirrus_grid* grid, double* host, void* stream);
 
+/* Autotuner (no counterpart in the reference): times every launch shape (tiles per CTA, tiles in
+ * flight per thread group) of the staged stencil kernels on this grid -- per kernel and level --
+ * and keeps the fastest for the following solves.  Shapes never change results.  Overwrites
+ * channels 2-5 (the solve's scratch); synchronises `stream`; takes about reps x (number of
+ * kernels x levels x shapes) launches.  reps <= 0 picks 20. */
+cirrus_status cirrus_grid_autotune(cirrus_grid* grid, int reps, void* stream);
+
 /* Measurement hook: launches one kernel of the solve `reps` times back to back on `stream` (no
  * synchronisation), so a caller can time it with its own CUDA events on that stream.  Uses
  * channels 2-5 (the solve's scratch) and overwrites them.  level: the level of the per-level
