@@ -140,13 +140,20 @@ def dist_setup(args):
 
 
 def barrier_max(pg, value: float) -> float:
+    """The max of a per-rank value over the ranks (the only collective of the replica path)."""
     if pg is None:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def batch_seeds(rank: int, batch: int) -> list[int]:
+    """Velocity seeds of rank `rank`'s instances: disjoint across ranks (replicas, weak scaling)."""
+    return [rank * batch + i for i in range(batch)]
 
 
 def build_batch(name: str, seeds: list[int]):
@@ -188,7 +195,7 @@ def run_ours(args, world, rank, local, pg):
     from cirrus_b200 import B_CHANNEL, KERNEL_LAPLACIAN, TMP_CHANNEL, GMGSolver
 
     K = args.batch
-    b, g = build_batch(args.workload, [rank * K + i for i in range(K)])
+    b, g = build_batch(args.workload, batch_seeds(rank, K))
     g.autotune()  # launch shapes per kernel and level for this grid (results unchanged)
     rhs = g.get_channel(B_CHANNEL)
     g.copy_channel(TMP_CHANNEL, B_CHANNEL)  # keep b resident for restoring between steps
