@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ring512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
     return ap.parse_args()
 
 
@@ -169,6 +170,93 @@ def build_batch(name: str, seeds: list[int]):
             g.set_channel_instance(i, 6 + a, vel[a])
     g.projection_rhs()
     return b, g
+
+
+SERVE_WORKLOADS = ["ring512", "sphere256", "uniform128", "ring64_small", "sphere64_small", "uniform32_small"]
+
+
+def run_serving(rank: int, built: dict, n_requests: int = 96, rates=(100.0, 400.0), slots: int = 8) -> dict:
+    """Serving loop under Poisson arrivals: sessions of six sizes (32^3 ... 512x512x1024 effective),
+    each request the next right-hand side of its session (a 1e-3 relative change, as from the next
+    time step), warm-started from the session's previous pressure, mixed precision to 1e-6.
+    Reported per arrival rate: throughput and p50/p99 latency (arrival to completion), against
+    the same arrival stream served one at a time by plain FP32 cold solves (service times
+    measured, queueing computed from them)."""
+    import torch
+
+    from cirrus_b200 import B_CHANNEL, DeviceGrid, GMGSolver, Server, workloads as W
+
+    base = {}
+    for name in SERVE_WORKLOADS:
+        b = built.get(name) or W.build(W.make(name, rank))
+        built[name] = b
+        g = DeviceGrid(b.topology)
+        for a in range(3):
+            g.set_channel(6 + a, b.velocity[a])
+        g.projection_rhs()
+        base[name] = (b, g.get_channel(B_CHANNEL))
+        g.close()
+    rng = np.random.default_rng(1000 + rank)
+    out = {"sessions": {n: int(base[n][0].tiles.shape[0]) for n in SERVE_WORKLOADS}, "slots": slots, "requests": n_requests,
+           "precision": "mixed (FP32 V-cycle, FP64 defect correction), warm start", "tolerance": 1e-6, "rates": []}
+    for rate in rates:
+        picks = rng.integers(0, len(SERVE_WORKLOADS), n_requests)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+        bs = [(base[SERVE_WORKLOADS[k]][1] * (1 + np.float32(1e-3) * rng.standard_normal(base[SERVE_WORKLOADS[k]][1].shape)
+                                              .astype(np.float32))).astype(np.float32) for k in picks]
+        srv = Server(40 << 30, slots)
+        sids = {n: srv.add_session(base[n][0].topology) for n in SERVE_WORKLOADS}
+        warm = [np.zeros_like(base[n][1]) for n in SERVE_WORKLOADS]
+        for n, x in zip(SERVE_WORKLOADS, warm):  # each session has solved once before the stream starts
+            srv.submit(sids[n], base[n][1], x)
+        got = 0
+        while got < len(SERVE_WORKLOADS):
+            got += len(srv.poll(wait_ms=1000))
+        xs = [np.zeros_like(x) for x in bs]
+        t0 = time.perf_counter()
+        sub, done = {}, {}
+        for i in range(n_requests):
+            while time.perf_counter() - t0 < arrivals[i]:
+                for c in srv.poll(wait_ms=0):
+                    done[c["ticket"]] = c
+                time.sleep(0.0002)
+            sub[srv.submit(sids[SERVE_WORKLOADS[picks[i]]], bs[i], xs[i])] = i
+        while len(done) < n_requests:
+            for c in srv.poll(wait_ms=1000):
+                done[c["ticket"]] = c
+        span = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        lat = np.array([done[t]["latency_ms"] for t in sub])
+        ok = all(done[t]["status"] == 0 and done[t]["rel_residual"] < 1e-6 for t in sub)
+        # the same stream one at a time: plain FP32 solves from x = 0 (service times on the GPU)
+        grids = {n: DeviceGrid(base[n][0].topology) for n in SERVE_WORKLOADS}
+        solver = GMGSolver()
+        stream = torch.cuda.current_stream()
+        svc = []
+        for i in range(n_requests):
+            g = grids[SERVE_WORKLOADS[picks[i]]]
+            g.set_channel(B_CHANNEL, bs[i])
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.solve(g, stream=stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            svc.append(e0.elapsed_time(e1))
+        for g in grids.values():
+            g.close()
+        finish, lat1 = 0.0, []
+        for i in range(n_requests):
+            finish = max(finish, arrivals[i] * 1e3) + svc[i]
+            lat1.append(finish - arrivals[i] * 1e3)
+        out["rates"].append({
+            "arrival_rate_rps": rate, "throughput_rps": round(n_requests / span, 2),
+            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+            "all_converged": ok, "peak_resident_gb": round(st["peak_bytes"] / 2**30, 3),
+            "one_at_a_time_fp32": {"throughput_rps": round(n_requests / (finish / 1e3), 2),
+                                   "p50_ms": round(float(np.percentile(lat1, 50)), 3),
+                                   "p99_ms": round(float(np.percentile(lat1, 99)), 3)}})
+    return out
 
 
 def cpu_baseline(b, rhs, budget_s: float = 10.0, max_solves: int = 5) -> dict:
@@ -342,6 +430,8 @@ def run_ours(args, world, rank, local, pg):
                                          f"PCG iterations each) by the CPU oracle (FP32 mirror of the reference "
                                          f"arithmetic, OpenMP), {cb['seconds']:.1f} s wall"}
     g.close()
+    if rank == 0 and not args.no_serve and args.workload == "ring512":
+        out["serving"] = run_serving(rank, {"ring512": b})
     return out
 
 

@@ -25,7 +25,7 @@ from typing import Callable, Sequence
 
 import numpy as np
 
-from ._native import (CirrusError, LEVEL_TARGET_FN, SolveParams, SolveResult, check, lib)
+from ._native import (CirrusError, Completion, LEVEL_TARGET_FN, SolveParams, SolveResult, check, lib)
 
 __all__ = [
     "LEAF", "NONLEAF", "GHOST", "DIRICHLET", "INTERIOR", "NEUMANN",
@@ -375,3 +375,69 @@ class GMGSolver:
                                           C.c_void_p(stream), C.byref(r)), "cirrus_gmg_solve_host")
         self.last_result = r
         return r.iters, r.rel_residual
+
+
+class Server:
+    """Serving loop: sessions (independent problems) with device-resident tile pools and warm-start
+    pressure; solves submitted as they arrive run concurrently on `slots` slots, admitted against
+    an HBM budget (idle sessions evicted least recently used first)."""
+
+    def __init__(self, hbm_budget_bytes: int, slots: int = 4):
+        h = C.c_void_p()
+        check(lib().cirrus_server_create(int(hbm_budget_bytes), int(slots), C.byref(h)), "cirrus_server_create")
+        self._h = h
+        self._topos = {}
+        self._live = {}  # ticket -> (b, x) kept alive until the completion is polled
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().cirrus_server_destroy(h)
+            self._h = None
+        self._live.clear()
+
+    def __del__(self):
+        self.close()
+
+    def add_session(self, topology: Topology) -> int:
+        sid = C.c_int()
+        check(lib().cirrus_server_add_session(self._h, topology.handle, C.byref(sid)), "cirrus_server_add_session")
+        self._topos[sid.value] = topology
+        return sid.value
+
+    def close_session(self, session: int) -> None:
+        check(lib().cirrus_server_close_session(self._h, session), "cirrus_server_close_session")
+        self._topos.pop(session, None)
+
+    def submit(self, session: int, b: np.ndarray, x_out: np.ndarray, relative_tolerance: float = 1e-6,
+               max_iters: int = 1000, inner_tolerance: float = 1e-5) -> int:
+        p = SolveParams()
+        lib().cirrus_solve_params_default(C.byref(p))
+        p.relative_tolerance = relative_tolerance
+        p.max_iters = max_iters
+        p.inner_tolerance = inner_tolerance
+        p.precision = PRECISION_MIXED_FP64
+        b = np.ascontiguousarray(b, dtype=np.float32)
+        assert x_out.dtype == np.float32 and x_out.flags["C_CONTIGUOUS"]
+        t = C.c_uint64()
+        check(lib().cirrus_server_submit(self._h, session, C.byref(p), _ptr(b, C.c_float), _ptr(x_out, C.c_float), C.byref(t)),
+              "cirrus_server_submit")
+        self._live[t.value] = (b, x_out)
+        return t.value
+
+    def poll(self, max_items: int = 64, wait_ms: int = 0) -> list[dict]:
+        out = (Completion * max_items)()
+        n = C.c_int()
+        check(lib().cirrus_server_poll(self._h, out, max_items, C.byref(n), wait_ms), "cirrus_server_poll")
+        res = []
+        for c in out[: n.value]:
+            self._live.pop(c.ticket, None)
+            res.append({f: getattr(c, f) for f, _ in Completion._fields_})
+        return res
+
+    def stats(self) -> dict:
+        r, pk, e = C.c_size_t(), C.c_size_t(), C.c_longlong()
+        rs, pd = C.c_int(), C.c_int()
+        check(lib().cirrus_server_stats(self._h, C.byref(r), C.byref(pk), C.byref(rs), C.byref(pd), C.byref(e)), "cirrus_server_stats")
+        return {"resident_bytes": r.value, "peak_bytes": pk.value, "resident_sessions": rs.value, "pending": pd.value,
+                "evictions": e.value}

@@ -63,6 +63,21 @@ class SolveResult(C.Structure):
     ]
 
 
+class Completion(C.Structure):
+    _fields_ = [
+        ("ticket", C.c_uint64),
+        ("session", C.c_int),
+        ("slot", C.c_int),
+        ("status", C.c_int),
+        ("iters", C.c_int),
+        ("outer_iters", C.c_int),
+        ("warm", C.c_int),
+        ("rel_residual", C.c_double),
+        ("latency_ms", C.c_double),
+        ("device_ms", C.c_double),
+    ]
+
+
 # name -> (restype, argtypes); status-returning functions use c_int
 _PROTOS = {
     "cirrus_status_string": (C.c_char_p, [C.c_int]),
@@ -116,6 +131,14 @@ _PROTOS = {
     "cirrus_gmg_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_int_p, c_f64_p, C.c_void_p,
                                          C.POINTER(SolveResult)]),
     "cirrus_gmg_solve_host": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p, C.POINTER(SolveResult)]),
+    "cirrus_server_create": (C.c_int, [C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),
+    "cirrus_server_destroy": (None, [C.c_void_p]),
+    "cirrus_server_add_session": (C.c_int, [C.c_void_p, C.c_void_p, c_int_p]),
+    "cirrus_server_close_session": (C.c_int, [C.c_void_p, C.c_int]),
+    "cirrus_server_submit": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.POINTER(C.c_uint64)]),
+    "cirrus_server_poll": (C.c_int, [C.c_void_p, C.POINTER(Completion), C.c_int, c_int_p, C.c_int]),
+    "cirrus_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), c_int_p, c_int_p,
+                                      C.POINTER(C.c_longlong)]),
     "cirrus_grid_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "cirrus_bench_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_true_residual": (C.c_int, [C.c_void_p, c_f32_p, c_f64_p, C.c_void_p]),

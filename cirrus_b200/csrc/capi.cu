@@ -1,6 +1,7 @@
 // C ABI (include/cirrus_b200.h).  Every entry point validates its arguments, maps internal
 // failures to cirrus_status and never lets an exception cross the boundary.
 #include "../../include/cirrus_b200.h"
+#include "serve.hpp"
 #include "solver_internal.hpp"
 #include "topology.hpp"
 
@@ -14,6 +15,9 @@ struct cirrus_topology {
 };
 struct cirrus_grid {
     cirrus::DevGrid* g;
+};
+struct cirrus_server {
+    cirrus::Server* s;
 };
 
 namespace {
@@ -531,6 +535,74 @@ cirrus_status cirrus_true_residual(cirrus_grid* grid, const float* b_host, doubl
         int rc = cirrus::true_residual(g, d_b, rel, S(stream));
         return map_rc(rc);
     });
+}
+
+// ---------------------------------------------------------------- serving loop
+cirrus_status cirrus_server_create(size_t hbm_budget_bytes, int slots, cirrus_server** out) {
+    if (!out || slots < 1 || slots > 64 || hbm_budget_bytes == 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return CIRRUS_ERR_NO_DEVICE;
+    }
+    return guard([&] {
+        *out = new cirrus_server{new cirrus::Server(hbm_budget_bytes, slots)};
+        return CIRRUS_OK;
+    });
+}
+void cirrus_server_destroy(cirrus_server* server) {
+    if (!server) return;
+    delete server->s;
+    delete server;
+}
+cirrus_status cirrus_server_add_session(cirrus_server* server, const cirrus_topology* topo, int* session) {
+    if (!server || !topo || !session || topo->t->num_tiles() <= 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        *session = server->s->add_session(topo->t);
+        return CIRRUS_OK;
+    });
+}
+cirrus_status cirrus_server_close_session(cirrus_server* server, int session) {
+    if (!server) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return server->s->close_session(session) ? CIRRUS_ERR_INVALID_ARGUMENT : CIRRUS_OK; });
+}
+cirrus_status cirrus_server_submit(cirrus_server* server, int session, const cirrus_solve_params* params, const float* b_host,
+                                   float* x_host, uint64_t* ticket) {
+    if (!server || !params_ok(params) || !b_host || !ticket) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        cirrus::SolveParams p;
+        to_internal(params, &p);
+        return server->s->submit(session, p, b_host, x_host, ticket) ? CIRRUS_ERR_INVALID_ARGUMENT : CIRRUS_OK;
+    });
+}
+cirrus_status cirrus_server_poll(cirrus_server* server, cirrus_completion* out, int max, int* count, int wait_ms) {
+    if (!server || !out || max < 1 || !count) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        std::vector<cirrus::Server::Completion> v;
+        server->s->poll(v, max, wait_ms);
+        for (size_t i = 0; i < v.size(); i++) {
+            cirrus_completion& c = out[i];
+            c.ticket = v[i].ticket;
+            c.session = v[i].session;
+            c.slot = v[i].slot;
+            c.status = (int)map_rc(v[i].status);
+            c.iters = v[i].iters;
+            c.outer_iters = v[i].outer;
+            c.warm = v[i].warm;
+            c.rel_residual = v[i].rel;
+            c.latency_ms = v[i].latency_ms;
+            c.device_ms = v[i].device_ms;
+        }
+        *count = (int)v.size();
+        return CIRRUS_OK;
+    });
+}
+cirrus_status cirrus_server_stats(cirrus_server* server, size_t* resident_bytes, size_t* peak_bytes, int* resident_sessions,
+                                  int* pending, long long* evictions) {
+    if (!server) return CIRRUS_ERR_INVALID_ARGUMENT;
+    server->s->stats(resident_bytes, peak_bytes, resident_sessions, pending);
+    if (evictions) *evictions = server->s->evictions();
+    return CIRRUS_OK;
 }
 
 }  // extern "C"

@@ -5,6 +5,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
 
 namespace cirrus {
 
@@ -915,12 +916,12 @@ void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const S
 }
 
 void init_stencil_attributes() {
-    static bool done = false;
-    if (done) return;
-    done = true;
+    static std::once_flag once;
+    std::call_once(once, [] {
     cudaFuncSetAttribute(k_gs_sweep<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
     cudaFuncSetAttribute(k_laplacian_fused<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
     cudaFuncSetAttribute(k_residual_restrict<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
+    });
 }
 
 bool pdl_enabled() {

@@ -277,6 +277,51 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
  * FP32 channel 0); one value per instance (rel holds num_instances doubles). */
 cirrus_status cirrus_true_residual(cirrus_grid* grid, const float* b_host, double* rel, void* stream);
 
+/* ------------------------------------------------------------------------------------------
+ * Serving loop (no counterpart in the reference): independent problems ("sessions") whose
+ * solves arrive over time run concurrently on `slots` worker slots (one host thread and one
+ * CUDA stream each, so their kernels overlap on the GPU), admitted against an HBM budget.  A
+ * session's tile pool and last pressure stay on the device between its solves, and every solve
+ * after its first starts from that pressure (mixed precision: FP64 defect correction from the
+ * warm start to params->relative_tolerance).  Idle sessions are evicted least recently used
+ * first when a new one needs the memory; their pressure is kept on the host for the next warm
+ * start.  A session's solves run one at a time, in submission order.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct cirrus_server cirrus_server;
+
+typedef struct cirrus_completion {
+    uint64_t ticket;
+    int session;
+    int slot;
+    int status;               /* cirrus_status of the solve (CIRRUS_ERR_BUDGET: larger than the budget) */
+    int iters;                /* FP32 PCG iterations summed over the defect-correction steps */
+    int outer_iters;
+    int warm;                 /* 1 if the solve started from the session's previous pressure */
+    double rel_residual;      /* FP64 true relative residual */
+    double latency_ms;        /* submission to completion (host clock) */
+    double device_ms;         /* the solve on its stream, b upload to x download (CUDA events) */
+} cirrus_completion;
+
+/* hbm_budget_bytes: device memory the sessions' state may occupy; slots: concurrent solves. */
+cirrus_status cirrus_server_create(size_t hbm_budget_bytes, int slots, cirrus_server** out);
+/* Finishes running solves, drops queued ones, frees every session's device state. */
+void cirrus_server_destroy(cirrus_server* server);
+/* Registers a problem (a finalised topology, which must outlive the session); no device memory
+ * is taken until its first solve is admitted. */
+cirrus_status cirrus_server_add_session(cirrus_server* server, const cirrus_topology* topo, int* session);
+/* Waits for the session's queued and running solves, then frees its device state. */
+cirrus_status cirrus_server_close_session(cirrus_server* server, int session);
+/* Queues a solve of the session: b_host (the session's num_tiles*512 floats, all-tiles order)
+ * is read and x_host written when the solve runs; both must stay valid until its completion is
+ * polled. */
+cirrus_status cirrus_server_submit(cirrus_server* server, int session, const cirrus_solve_params* params, const float* b_host,
+                                   float* x_host, uint64_t* ticket);
+/* Up to max completions (oldest first); waits up to wait_ms for the first if none is ready. */
+cirrus_status cirrus_server_poll(cirrus_server* server, cirrus_completion* out, int max, int* count, int wait_ms);
+/* Resident bytes now and at peak, resident sessions, queued solves, evictions so far (any may be NULL). */
+cirrus_status cirrus_server_stats(cirrus_server* server, size_t* resident_bytes, size_t* peak_bytes, int* resident_sessions,
+                                  int* pending, long long* evictions);
+
 #ifdef __cplusplus
 }
 #endif
