@@ -286,6 +286,11 @@ class DeviceGrid:
         check(lib().cirrus_velocity_volume_divergence_on_leafs(self._h, u_channel, div_channel, C.c_void_p(stream)),
               "cirrus_velocity_volume_divergence_on_leafs")
 
+    def add_gradient_to_face_centers(self, p_channel: int = X_CHANNEL, u_channel: int = U_CHANNEL, stream: int = 0) -> None:
+        """AddGradientToFaceCenters: the velocity update from the solved pressure."""
+        check(lib().cirrus_add_gradient_to_face_centers(self._h, p_channel, u_channel, C.c_void_p(stream)),
+              "cirrus_add_gradient_to_face_centers")
+
     def projection_rhs(self, stream: int = 0) -> None:
         """b = divergence of the face velocities in channels 6-8, as FluidEuler::project builds it
         after the velocity boundary step (src/FluidEuler.h:583-586, src/FluidEuler.cu:43-60)."""

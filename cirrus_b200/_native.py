@@ -126,6 +126,7 @@ _PROTOS = {
     "cirrus_clear_neumann_neighbor_faces": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "cirrus_propagate_to_children": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "cirrus_velocity_volume_divergence_on_leafs": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "cirrus_add_gradient_to_face_centers": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_solve_params_default": (None, [C.POINTER(SolveParams)]),
     "cirrus_gmg_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveResult)]),
     "cirrus_gmg_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_int_p, c_f64_p, C.c_void_p,

@@ -68,6 +68,8 @@ int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
     };
     for (int l = lo; l <= g.max_level; l++) {
         if (g.mg_count[l] > 0) pick(KS_GS_SWEEP, l, [&] { launch::gs_sweep(g, l, z, ap, 0, nullptr, s); });
+        if (g.mg_count[l] > 0 && g.bottom_level >= 0)
+            pick(KS_PRESMOOTH, l, [&] { launch::presmooth(g, l, g.d_xpre, ap, nullptr, s); });
         if (l >= 1 && g.level_count[l] > 0)
             pick(KS_RESIDUAL, l, [&] { launch::residual_restrict(g, l, g.d_xpre, ap, tmp, 1.f, nullptr, s); });
     }

@@ -417,6 +417,14 @@ cirrus_status cirrus_velocity_volume_divergence_on_leafs(cirrus_grid* grid, int 
     return cuda_status();
 }
 
+cirrus_status cirrus_add_gradient_to_face_centers(cirrus_grid* grid, int p_channel, int u_channel, void* stream) {
+    if (!grid || !channel_ok(p_channel) || u_channel < 0 || u_channel + 2 >= cirrus::kNumChannels ||
+        (p_channel >= u_channel && p_channel <= u_channel + 2))
+        return CIRRUS_ERR_INVALID_ARGUMENT;
+    cirrus::launch::add_gradient(*grid->g, p_channel, u_channel, S(stream));
+    return cuda_status();
+}
+
 // ---------------------------------------------------------------- solve
 void cirrus_solve_params_default(cirrus_solve_params* p) {
     if (!p) return;

@@ -823,6 +823,7 @@ void full_laplacian(const DevGrid& g, T* X, T* Y, const Scalars* S, cudaStream_t
     laplacian_tiles<T>(g, X, Y, S, s);
     accumulate_ghosts<T>(g, Y, S, s);
 }
+template void propagate_ghosts<float>(const DevGrid&, float*, const Scalars*, cudaStream_t);
 template void full_laplacian<float>(const DevGrid&, float*, float*, const Scalars*, cudaStream_t);
 template void full_laplacian<double>(const DevGrid&, double*, double*, const Scalars*, cudaStream_t);
 

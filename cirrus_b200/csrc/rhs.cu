@@ -137,10 +137,10 @@ __global__ void __launch_bounds__(128) k_divergence(Topo tp, const int* __restri
 }
 
 // AccumulateToParents(b, b, -1, LEAF, LAUNCH_SUBTREE, INTERIOR, 1, additive)
-// (src/PoissonGrid.cu:721-755): INTERIOR cells of LEAF tiles add their INTERIOR children's values
-// (children in childCoord order, x fastest).
+// (src/PoissonGrid.cu:721-755): cells of LEAF tiles whose type is in cell_types add coeff times
+// the sum of their children's values over children of those types (childCoord order, x fastest).
 __global__ void __launch_bounds__(128) k_accumulate_children(Topo tp, const int* __restrict__ child, const int* __restrict__ list,
-                                                             int n, float* B) {
+                                                             int n, float* B, uint8_t cell_types, float coeff) {
     const int q = blockIdx.x;
     if (q >= n) return;
     const int tile = list[q];
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(128) k_accumulate_children(Topo tp, const int*
     const TileIdx ix(t);
     for (int e = 0; e < 4; e++) {
         const size_t id = (size_t)tile * kTileCells + t * 4 + e;
-        if (!(tp.ctype[id] & INTERIOR_C)) continue;
+        if (!(tp.ctype[id] & cell_types)) continue;
         const int l[3] = {ix.i, ix.j, ix.k0 + e};
         const int oct = (l[0] >> 2) | ((l[1] >> 2) << 1) | ((l[2] >> 2) << 2);
         const int ct = child[(size_t)tile * 8 + oct];
@@ -157,9 +157,68 @@ __global__ void __launch_bounds__(128) k_accumulate_children(Topo tp, const int*
         for (int cid = 0; cid < 8; cid++) {
             const int c0 = (l[0] * 2 + (cid & 1)) & 7, c1 = (l[1] * 2 + ((cid >> 1) & 1)) & 7, c2 = (l[2] * 2 + ((cid >> 2) & 1)) & 7;
             const size_t cidx = (size_t)ct * kTileCells + (c0 << 6 | c1 << 3 | c2);
-            if (tp.ctype[cidx] & INTERIOR_C) sum += B[cidx];
+            if (tp.ctype[cidx] & cell_types) sum += B[cidx];
         }
-        B[id] = fmaf(sum, 1.0f, B[id]);
+        B[id] = fmaf(sum, coeff, B[id]);
+    }
+}
+
+// The face terms of AddGradientToFaceCenters (src/PoissonSolver.cu:144-200) on LEAF|GHOST tiles:
+// on each lower face (x-, y-, z-) u += (p1 - p0) / dh with dh = h between LEAF cells and 1.5 h
+// across a LEAF-GHOST face (no term otherwise, nor across a NEUMANN cell); p1, p0 the INTERIOR
+// values (0 elsewhere); an absent neighbour counts as the cell's own tile and cell type with
+// p0 = 0.  GHOST tiles start from u = 0.
+__global__ void __launch_bounds__(128) k_gradient(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ P, float* U0,
+                                                  float* U1, float* U2) {
+    const int q = blockIdx.x;
+    if (q >= n) return;
+    const int tile = list[q];
+    const TileMeta m = tp.meta[tile];
+    const int t = threadIdx.x;
+    const uint8_t tt = (uint8_t)meta_type(m.packed);
+    const float h = tile_h0(tp, tile) / float(1 << meta_level(m.packed));
+    const float h15 = (float)(1.5 * (double)h);
+    float* U[3] = {U0, U1, U2};
+    for (int e = 0; e < 4; e++) {
+        const int o = t * 4 + e;
+        const size_t id = (size_t)tile * kTileCells + o;
+        const uint8_t ct = tp.ctype[id];
+        const float p1 = (ct & INTERIOR_C) ? P[id] : 0.f;
+        const int l[3] = {o >> 6, (o >> 3) & 7, o & 7};
+        for (int a = 0; a < 3; a++) {
+            float u = tt == GHOST_T ? 0.f : U[a][id];
+            int nl[3] = {l[0], l[1], l[2]};
+            nl[a] -= 1;
+            uint8_t ntt, nct;
+            float p0;
+            if (nl[a] >= 0) {
+                const size_t nid = (size_t)tile * kTileCells + (nl[0] << 6 | nl[1] << 3 | nl[2]);
+                ntt = tt;
+                nct = tp.ctype[nid];
+                p0 = (nct & INTERIOR_C) ? P[nid] : 0.f;
+            } else {
+                const int nb = m.nb[2 * a];
+                nl[a] = 7;
+                if (nb < 0) {
+                    ntt = tt;
+                    nct = ct;
+                    p0 = 0.f;
+                } else {
+                    const size_t nid = (size_t)nb * kTileCells + (nl[0] << 6 | nl[1] << 3 | nl[2]);
+                    ntt = (uint8_t)meta_type(tp.meta[nb].packed);
+                    nct = tp.ctype[nid];
+                    p0 = (nct & INTERIOR_C) ? P[nid] : 0.f;
+                }
+            }
+            float dh;
+            bool term = true;
+            if ((tt & LEAF_T) && (ntt & LEAF_T)) dh = h;
+            else if (((tt & LEAF_T) && (ntt & GHOST_T)) || ((tt & GHOST_T) && (ntt & LEAF_T))) dh = h15;
+            else term = false;
+            if ((ct & NEUMANN_C) || (nct & NEUMANN_C)) term = false;
+            if (term) u = u + (p1 - p0) / dh;
+            if (term || tt == GHOST_T) U[a][id] = u;
+        }
     }
 }
 
@@ -186,7 +245,23 @@ void velocity_divergence(const DevGrid& g, int u_channel, int b_channel, cudaStr
     k_divergence<<<g.n_leafghost, 128, 0, s>>>(g.topo, g.d_leafghost, g.n_leafghost, g.d_ch[u_channel], g.d_ch[u_channel + 1],
                                               g.d_ch[u_channel + 2], g.d_ch[b_channel]);
     ++g.launch_count;
-    k_accumulate_children<<<g.n_leaf, 128, 0, s>>>(g.topo, g.d_child, g.d_leaf, g.n_leaf, g.d_ch[b_channel]);
+    k_accumulate_children<<<g.n_leaf, 128, 0, s>>>(g.topo, g.d_child, g.d_leaf, g.n_leaf, g.d_ch[b_channel], (uint8_t)INTERIOR_C,
+                                                   1.0f);
+}
+
+void add_gradient(const DevGrid& g, int p_channel, int u_channel, cudaStream_t s) {
+    propagate_ghosts<float>(g, g.d_ch[p_channel], nullptr, s);
+    if (g.n_leafghost > 0) {
+        ++g.launch_count;
+        k_gradient<<<g.n_leafghost, 128, 0, s>>>(g.topo, g.d_leafghost, g.n_leafghost, g.d_ch[p_channel], g.d_ch[u_channel],
+                                                 g.d_ch[u_channel + 1], g.d_ch[u_channel + 2]);
+    }
+    if (g.n_leaf == 0) return;
+    for (int a = 0; a < 3; a++) {
+        ++g.launch_count;
+        k_accumulate_children<<<g.n_leaf, 128, 0, s>>>(g.topo, g.d_child, g.d_leaf, g.n_leaf, g.d_ch[u_channel + a],
+                                                       (uint8_t)(INTERIOR_C | DIRICHLET_C), 0.25f);
+    }
 }
 
 }  // namespace launch

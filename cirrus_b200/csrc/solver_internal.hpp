@@ -206,6 +206,11 @@ void narrow(const DevGrid& g, const double* a, float* b, size_t n, cudaStream_t 
 void clear_neumann_faces(const DevGrid& g, int u_channel, cudaStream_t s);
 void propagate_to_children(const DevGrid& g, int channel, cudaStream_t s);
 void velocity_divergence(const DevGrid& g, int u_channel, int b_channel, cudaStream_t s);
+// AddGradientToFaceCenters (src/PoissonSolver.cu:144-206): p propagated to GHOST cells, face
+// gradient terms, GHOST children accumulated into LEAF parents (1/4, INTERIOR|DIRICHLET).
+void add_gradient(const DevGrid& g, int p_channel, int u_channel, cudaStream_t s);
+// PropagateValuesToGhostTiles (src/PoissonGrid.cu:585-605) of channel X.
+template <class T> void propagate_ghosts(const DevGrid& g, T* X, const Scalars* S, cudaStream_t s);
 // fused V-cycle (vcycle_fused.cu)
 void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s);
 void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,

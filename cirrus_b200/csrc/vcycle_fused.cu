@@ -56,70 +56,109 @@ __device__ __forceinline__ void halo_cell_ijk(int face, int h, int& i, int& j, i
     }
 }
 
-// First-colour (0) value of cell (i, j, k) of mg tile `tile` after one sweep from x = 0:
-// 0 + (b - 0) / D on INTERIOR cells of colour 0, else 0.
-__device__ __forceinline__ float first_colour(const Topo& tp, const float* __restrict__ RHS, int tile, int i, int j, int k,
-                                              const LevelConst<float>& L) {
-    if (((i + j + k) & 1) != 0) return 0.f;
-    const int off = (i << 6) | (j << 3) | k;
-    const uint32_t mm = tp.mask_mg[(size_t)tile * kTileCells + off];
-    if (!(mm & kMaskInterior)) return 0.f;
-    const float D = cell_diag(i, j, k, mm, (tp.fcls[tile] >> 12) & 0xfffu, L);
-    return 0.f + (RHS[(size_t)tile * kTileCells + off] - 0.f) / D;
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------- down: pre-smoother
+// Staging area of the pre-smoother: first-colour values of the tile (xs) and of the face
+// neighbours' first layer (hx) are computed in place from the staged right-hand sides (b, hx)
+// and masks (mask, hmask).
+struct __align__(16) PreStage {
+    float xs[kTileCells];
+    float hx[6 * 64];
+    float b[kTileCells];
+    uint8_t mask[kTileCells];
+    uint8_t hmask[6 * 64];
+};
+
 // GaussSeidelGMG(1, 0) on the mg tiles (LEAF|NONLEAF) of one level, x starting from 0; the
 // result goes to XP.  GHOST neighbours hold x = 0 on the way down (they are not smoothed).
-template <int TPB>
+// NT tiles per 128-thread group are staged with asynchronous copies before any is computed.
+template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __restrict__ list, int n, float* XP,
                                                          const float* __restrict__ RHS, const Scalars* __restrict__ S) {
     pdl_entry();
-    __shared__ TileShared<float> sh[TPB];
+    extern __shared__ __align__(16) unsigned char pre_smem[];
+    PreStage* st = reinterpret_cast<PreStage*>(pre_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-    const int q = blockIdx.x * TPB + g;
-    const int tile = q < n ? list[q] : 0;
-    const bool active = q < n && !tile_done(tp, S, tile);
     const TileIdx ix(t);
-    TileMeta m;
-    V4<float> b;
-    uint32_t mask4 = 0, cls = 0;
-    LevelConst<float> L(1.f, 0);
-    if (active) {
-        m = tp.meta[tile];
-        L = LevelConst<float>(tile_h0(tp, tile), meta_level(m.packed));
-        b = ld4(RHS + (size_t)tile * kTileCells + t * 4);
-        mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
-        cls = (tp.fcls[tile] >> 12) & 0xfffu;
-        // first colour of the own cells
+    int tile[NT];
+    bool act[NT];
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        const int q = (blockIdx.x * NT + u) * TPB + g;
+        tile[u] = q < n ? list[q] : 0;
+        act[u] = q < n && !tile_done(tp, S, tile[u]);
+    }
+    // neighbour of this thread's x/y-face piece (t < 64) and z-face cell; GHOST neighbours count
+    // as absent (their x is 0 on the way down)
+    int nbf[NT], nbz[NT];
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        nbf[u] = nbz[u] = -1;
+        if (!act[u]) continue;
+        PreStage& ps = st[u * TPB + g];
+        const TileMeta m = tp.meta[tile[u]];
+        const size_t base = (size_t)tile[u] * kTileCells;
+        cp_async16(ps.b + t * 4, RHS + base + t * 4);
+        if (t < 32) cp_async16(ps.mask + t * 16, tp.mask_mg + base + t * 16);
+        if (t < 64) {
+            const int face = t >> 4, qq = t & 15;
+            int off;
+            if (face == 0) off = 448 + qq * 4;
+            else if (face == 1) off = qq * 4;
+            else if (face == 2) off = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
+            else off = (qq >> 1) * 64 + (qq & 1) * 4;
+            const int nb = m.nb[face];
+            if (nb >= 0 && !meta_nb_ghost(m.packed, face)) {
+                nbf[u] = nb;
+                cp_async16(ps.hx + face * 64 + qq * 4, RHS + (size_t)nb * kTileCells + off);
+                cp_async4(ps.hmask + face * 64 + qq * 4, tp.mask_mg + (size_t)nb * kTileCells + off);
+            }
+        }
+        {
+            const int face = 4 + (t >> 6), c = t & 63;
+            const int nb = m.nb[face];
+            if (nb >= 0 && !meta_nb_ghost(m.packed, face)) {
+                nbz[u] = nb;
+                const int off = (c >> 3) * 64 + (c & 7) * 8 + (face == 4 ? 7 : 0);
+                cp_async4(ps.hx + face * 64 + c, RHS + (size_t)nb * kTileCells + off);
+                ps.hmask[face * 64 + c] = tp.mask_mg[(size_t)nb * kTileCells + off];
+            }
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // first colour (0) of the own cells and of the live neighbours' first layer, in place
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        if (!act[u]) continue;
+        PreStage& ps = st[u * TPB + g];
+        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(tp.meta[tile[u]].packed));
+        const uint32_t cls = (tp.fcls[tile[u]] >> 12) & 0xfffu;
+        const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ps.mask + t * 4);
+        const V4<float> b = ld4(ps.b + t * 4);
         V4<float> x1;
 #pragma unroll
         for (int e = 0; e < 4; e++) {
             const int k = ix.k0 + e;
             const uint32_t mm = (mask4 >> (8 * e)) & 0xffu;
             float v = 0.f;
-            if (((ix.i + ix.j + k) & 1) == 0 && (mm & kMaskInterior))
-                v = 0.f + (b.v[e] - 0.f) / cell_diag(ix.i, ix.j, k, mm, cls, L);
+            if (((ix.i + ix.j + k) & 1) == 0 && (mm & kMaskInterior)) v = 0.f + (b.v[e] - 0.f) / cell_diag(ix.i, ix.j, k, mm, cls, L);
             x1.v[e] = v;
         }
-        st4(sh[g].xs + t * 4, x1);
-        // first colour of the face neighbours' first cell layer; x and y faces as runs of four
-        // cells along k (one 16-byte right-hand-side load and one 4-byte mask load)
+        st4(ps.xs + t * 4, x1);
         if (t < 64) {
             const int face = t >> 4, qq = t & 15;
-            const int nb = m.nb[face];
             V4<float> v = zero4<float>();
-            if (nb >= 0 && !meta_nb_ghost(m.packed, face)) {
+            if (nbf[u] >= 0) {
+                const V4<float> nbb = ld4(ps.hx + face * 64 + qq * 4);
+                const uint32_t nm4 = *reinterpret_cast<const uint32_t*>(ps.hmask + face * 64 + qq * 4);
+                const uint32_t ncls = (tp.fcls[nbf[u]] >> 12) & 0xfffu;
                 int off;
                 if (face == 0) off = 448 + qq * 4;
                 else if (face == 1) off = qq * 4;
                 else if (face == 2) off = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
                 else off = (qq >> 1) * 64 + (qq & 1) * 4;
-                const V4<float> nbb = ld4(RHS + (size_t)nb * kTileCells + off);
-                const uint32_t nm4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)nb * kTileCells + off);
-                const uint32_t ncls = (tp.fcls[nb] >> 12) & 0xfffu;
                 const int ni = off >> 6, nj = (off >> 3) & 7, nk0 = off & 7;
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
@@ -128,20 +167,32 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
                         v.v[e] = 0.f + (nbb.v[e] - 0.f) / cell_diag(ni, nj, nk0 + e, mm, ncls, L);
                 }
             }
-            st4(sh[g].hx + face * 64 + qq * 4, v);
+            st4(ps.hx + face * 64 + qq * 4, v);
         }
         {
             const int face = 4 + (t >> 6), c = t & 63;
-            const int nb = m.nb[face];
-            int i, j, k;
-            halo_cell_ijk(face, c, i, j, k);
-            sh[g].hx[face * 64 + c] = (nb >= 0 && !meta_nb_ghost(m.packed, face)) ? first_colour(tp, RHS, nb, i, j, k, L) : 0.f;
+            float v = 0.f;
+            if (nbz[u] >= 0) {
+                int i, j, k;
+                halo_cell_ijk(face, c, i, j, k);
+                const uint32_t mm = ps.hmask[face * 64 + c];
+                if (((i + j + k) & 1) == 0 && (mm & kMaskInterior))
+                    v = 0.f + (ps.hx[face * 64 + c] - 0.f) / cell_diag(i, j, k, mm, (tp.fcls[nbz[u]] >> 12) & 0xfffu, L);
+            }
+            ps.hx[face * 64 + c] = v;
         }
     }
     __syncthreads();
-    if (!active) return;
     // second colour (1), from the first-colour values
-    st4(XP + (size_t)tile * kTileCells + t * 4, colour_update(sh[g].xs, sh[g].hx, t, mask4, cls, L, b, 1));
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        if (!act[u]) continue;
+        PreStage& ps = st[u * TPB + g];
+        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(tp.meta[tile[u]].packed));
+        st4(XP + (size_t)tile[u] * kTileCells + t * 4,
+            colour_update(ps.xs, ps.hx, t, *reinterpret_cast<const uint32_t*>(ps.mask + t * 4), (tp.fcls[tile[u]] >> 12) & 0xfffu, L,
+                          ld4(ps.b + t * 4), 1));
+    }
 }
 
 // ---------------------------------------------------------------------------- up: prolongation + first colour
@@ -414,11 +465,24 @@ namespace launch {
 
 constexpr int kTPB2 = 2;
 
+template <int TPB, int NT>
+void presmooth_shape(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s) {
+    const int n = g.mg_count[level];
+    const int per = TPB * NT;
+    launch_kernel(k_presmooth<TPB, NT>, (n + per - 1) / per, 128 * TPB, sizeof(PreStage) * per, s, g.topo, g.d_mg + g.mg_offset[level], n,
+                  XP, RHS, S);
+}
+
 void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s) {
     const int n = g.mg_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    launch_kernel(k_presmooth<kTPB2>, (n + kTPB2 - 1) / kTPB2, 128 * kTPB2, 0, s, g.topo, g.d_mg + g.mg_offset[level], n, XP, RHS, S);
+    switch (g.shape(KS_PRESMOOTH, level)) {
+    case 0: presmooth_shape<2, 1>(g, level, XP, RHS, S, s); break;
+    case 1: presmooth_shape<2, 2>(g, level, XP, RHS, S, s); break;
+    case 2: presmooth_shape<1, 4>(g, level, XP, RHS, S, s); break;
+    default: presmooth_shape<2, 4>(g, level, XP, RHS, S, s); break;
+    }
 }
 
 void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
@@ -466,6 +530,7 @@ bool bottom_supported(int coarsest_iters, int lb) {
 
 void init_kernel_attributes() {
     cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBudget);
+    cudaFuncSetAttribute(k_presmooth<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PreStage) * 8);
 }
 
 }  // namespace launch

@@ -186,6 +186,11 @@ cirrus_status cirrus_propagate_to_children(cirrus_grid* grid, int channel, void*
 /* VelocityVolumeDivergenceOnLeafs (src/PoissonSolver.cu:66-142), including the accumulation of
  * GHOST fluxes into their LEAF parents. */
 cirrus_status cirrus_velocity_volume_divergence_on_leafs(cirrus_grid* grid, int u_channel, int div_channel, void* stream);
+/* AddGradientToFaceCenters(grid, p_channel, u_channel) (src/PoissonSolver.cu:144-206), the step
+ * after the solve in FluidEuler::project (src/FluidEuler.h:607): p is propagated to GHOST cells,
+ * the lower-face velocities of LEAF and GHOST tiles get (p1 - p0)/dh, and GHOST children are
+ * accumulated into their LEAF parents. */
+cirrus_status cirrus_add_gradient_to_face_centers(cirrus_grid* grid, int p_channel, int u_channel, void* stream);
 
 /* ------------------------------------------------------------------------------------------
  * GMG-PCG solve (GMGSolver::solve, src/GMGSolver.cu:531-666)

@@ -753,6 +753,83 @@ void divergence(const Flat& f, float* const u[3], float* b) {
     }
 }
 
+// AddGradientToFaceCenters (src/PoissonSolver.cu:144-206) on a flat view, FP32 as the reference:
+// PropagateValues(p, p, -1, GHOST) (src/PoissonGrid.cu:611-632, coarse first); on LEAF|GHOST
+// tiles each lower face gets u += (p1 - p0) / dh (dh = h LEAF-LEAF, (float)(1.5 h) LEAF-GHOST,
+// nothing else or across a NEUMANN cell; an absent neighbour counts as the cell itself with
+// p0 = 0; GHOST tiles start from u = 0); then per axis AccumulateToParents(u, u, -1, LEAF,
+// INTERIOR|DIRICHLET, 1/4, additive) (src/PoissonGrid.cu:721-755, fine first).
+void gradient(const Flat& f, float* p, float* u[3]) {
+    for (int l = 0; l < f.num_layers; l++) {
+        for (int t : f.by_level[l]) {
+            if (!(f.type[t] & GHOST)) continue;
+            for (int o = 0; o < NCELL; o++) {
+                size_t id = (size_t)t * NCELL + o;
+                if (!(f.ctype[id] & INTERIOR)) { p[id] = 0; continue; }
+                int gx = f.cx[t] * 8 + (o >> 6), gy = f.cy[t] * 8 + ((o >> 3) & 7), gz = f.cz[t] * 8 + (o & 7);
+                int po;
+                int pt = f.find_voxel(l - 1, gx >> 1, gy >> 1, gz >> 1, po);
+                p[id] = (pt >= 0 && (f.ctype[(size_t)pt * NCELL + po] & INTERIOR)) ? p[(size_t)pt * NCELL + po] : 0.f;
+            }
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < f.n; t++) {
+        if (!(f.type[t] & (LEAF | GHOST))) continue;
+        const float h = voxel_size<float>(f.level[t]);
+        const float h15 = (float)(1.5 * (double)h);
+        const uint8_t tt = f.type[t];
+        for (int o = 0; o < NCELL; o++) {
+            size_t id = (size_t)t * NCELL + o;
+            uint8_t ct = f.ctype[id];
+            float p1 = (ct & INTERIOR) ? p[id] : 0.f;
+            int g[3] = {f.cx[t] * 8 + (o >> 6), f.cy[t] * 8 + ((o >> 3) & 7), f.cz[t] * 8 + (o & 7)};
+            if (tt == GHOST)
+                for (int a = 0; a < 3; a++) u[a][id] = 0.f;
+            for (int a = 0; a < 3; a++) {
+                int ng[3] = {g[0], g[1], g[2]};
+                ng[a]--;
+                int no;
+                int nt = f.find_voxel(f.level[t], ng[0], ng[1], ng[2], no);
+                uint8_t ntt, nct;
+                float p0;
+                if (nt < 0) { ntt = tt; nct = ct; p0 = 0.f; }
+                else {
+                    ntt = f.type[nt];
+                    nct = f.ctype[(size_t)nt * NCELL + no];
+                    p0 = (nct & INTERIOR) ? p[(size_t)nt * NCELL + no] : 0.f;
+                }
+                float dh;
+                if ((tt & LEAF) && (ntt & LEAF)) dh = h;
+                else if (((tt & LEAF) && (ntt & GHOST)) || ((tt & GHOST) && (ntt & LEAF))) dh = h15;
+                else continue;
+                if ((ct & NEUMANN) || (nct & NEUMANN)) continue;
+                u[a][id] = u[a][id] + (p1 - p0) / dh;
+            }
+        }
+    }
+    for (int a = 0; a < 3; a++) {
+        for (int l = f.num_layers - 1; l >= 0; l--) {
+            for (int t : f.by_level[l]) {
+                if (!(f.type[t] & LEAF)) continue;
+                for (int o = 0; o < NCELL; o++) {
+                    size_t id = (size_t)t * NCELL + o;
+                    if (!(f.ctype[id] & (INTERIOR | DIRICHLET))) continue;
+                    int g[3] = {f.cx[t] * 8 + (o >> 6), f.cy[t] * 8 + ((o >> 3) & 7), f.cz[t] * 8 + (o & 7)};
+                    float sum = 0;
+                    for (int cid = 0; cid < 8; cid++) {
+                        int cg[3] = {g[0] * 2 + (cid & 1), g[1] * 2 + ((cid >> 1) & 1), g[2] * 2 + ((cid >> 2) & 1)};
+                        int co;
+                        int c = f.find_voxel(l + 1, cg[0], cg[1], cg[2], co);
+                        if (c >= 0 && (f.ctype[(size_t)c * NCELL + co] & (INTERIOR | DIRICHLET))) sum += u[a][(size_t)c * NCELL + co];
+                    }
+                    u[a][id] = std::fma(sum, 0.25f, u[a][id]);
+                }
+            }
+        }
+    }
+}
+
 // CalcCellTypesFromLeafs (src/PoissonSolver.cu:7-61) on a flat view (types of LEAF tiles given)
 void calc_cell_types(Flat& f) {
     for (int l = f.num_layers - 1; l >= 0; l--) {
@@ -878,6 +955,13 @@ void ocx_flat_rhs(void* h, float* u, float* v, float* w, float* b) {
     clear_faces(o->f, uu);
     for (int a = 0; a < 3; a++) propagate_u(o->f, uu[a]);
     divergence(o->f, uu, b);
+}
+
+// AddGradientToFaceCenters on host arrays (p and u, v, w updated in place)
+void ocx_flat_gradient(void* h, float* p, float* u, float* v, float* w) {
+    OCX* o = (OCX*)h;
+    float* uu[3] = {u, v, w};
+    gradient(o->f, p, uu);
 }
 
 static Solver<float>& S32(OCX* o) { if (!o->s32) o->s32 = new Solver<float>(o->f); return *o->s32; }

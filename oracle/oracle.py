@@ -94,6 +94,7 @@ def oracle_lib():
             "ocx_flat_calc_cell_types": (None, [P]),
             "ocx_flat_neighbors": (None, [P, i32p]),
             "ocx_flat_rhs": (None, [P, f32p, f32p, f32p, f32p]),
+            "ocx_flat_gradient": (None, [P, f32p, f32p, f32p, f32p]),
             "ocx_set_channel": (None, [P, C.c_int, C.c_int, f64p]),
             "ocx_get_channel": (None, [P, C.c_int, C.c_int, f64p]),
             "ocx_set_channel_f32": (None, [P, C.c_int, f32p]),
@@ -206,6 +207,13 @@ class CpuOracle:
         oracle_lib().ocx_flat_rhs(self.h, _p(u[0], C.c_float), _p(u[1], C.c_float), _p(u[2], C.c_float), _p(b, C.c_float))
         return b
 
+    def add_gradient(self, p: np.ndarray, velocity: np.ndarray):
+        """AddGradientToFaceCenters on copies: returns (p with GHOST cells propagated, u, v, w)."""
+        pp = np.ascontiguousarray(p, dtype=np.float32).copy()
+        u = [np.ascontiguousarray(velocity[a], dtype=np.float32).copy() for a in range(3)]
+        oracle_lib().ocx_flat_gradient(self.h, _p(pp, C.c_float), _p(u[0], C.c_float), _p(u[1], C.c_float), _p(u[2], C.c_float))
+        return pp, u
+
     def set_channel(self, prec, c, data):
         a = np.ascontiguousarray(data, dtype=np.float64).reshape(self.n * 512)
         oracle_lib().ocx_set_channel(self.h, prec, c, _p(a, C.c_double))
@@ -292,6 +300,7 @@ def ref_lib():
             "ref_set_channel": (None, [P, C.c_int, f32p]),
             "ref_get_channel": (None, [P, C.c_int, f32p]),
             "ref_rhs": (None, [P]),
+            "ref_add_gradient": (None, [P, C.c_int, C.c_int]),
             "ref_full_lap": (None, [P, C.c_int, C.c_int]),
             "ref_gs_sweep": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int]),
             "ref_residual_restrict": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -374,6 +383,14 @@ class RefHarness:
             self.set_channel(6 + a, velocity[a])
         ref_lib().ref_rhs(self.h)
         return self.get_channel(1)
+
+    def add_gradient(self, p, velocity):
+        """The reference's AddGradientToFaceCenters(grid, 0, 6): returns (p channel, u, v, w)."""
+        self.set_channel(0, p)
+        for a in range(3):
+            self.set_channel(6 + a, velocity[a])
+        ref_lib().ref_add_gradient(self.h, 0, 6)
+        return self.get_channel(0), [self.get_channel(6 + a) for a in range(3)]
 
     def full_lap(self, xc, yc):
         ref_lib().ref_full_lap(self.h, xc, yc)

@@ -197,6 +197,10 @@ void ref_rhs(void* h) {
     VelocityVolumeDivergenceOnLeafs(grid, Tile::u_channel, Tile::b_channel);
     cudaDeviceSynchronize();
 }
+void ref_add_gradient(void* h, int pc, int uc) {
+    AddGradientToFaceCenters(*((RefGrid*)h)->g, pc, uc);
+    cudaDeviceSynchronize();
+}
 void ref_full_lap(void* h, int xc, int yc) {
     FullNegativeLaplacian(*((RefGrid*)h)->g, xc, yc, false);
     cudaDeviceSynchronize();
