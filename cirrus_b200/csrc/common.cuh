@@ -71,7 +71,9 @@ struct Topo {
     const int* ghost_list;       // GHOST tile of each ghost slot
     const int* inst;             // n: instance of each tile
     const float* inst_h0;        // per instance: voxel size of level 0, stored in FP32 as the reference does
+    const float4* lconst;        // per instance x kLevelSlots levels: h, c1, c2, fast-path diagonal
 };
+constexpr int kLevelSlots = 16;
 
 __host__ __device__ inline float tile_h0(const Topo& tp, int tile) { return tp.inst_h0[tp.inst[tile]]; }
 // true when the tile's instance has finished (or takes no part in) the running solve

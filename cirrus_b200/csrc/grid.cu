@@ -12,6 +12,7 @@
 //   lists      LEAF (instance by instance), GHOST, LEAF|GHOST tiles; LEAF|NONLEAF tiles per level
 // The per-cell stencil masks fold NegativeLaplacianCoeff's tile-type and Neumann tests
 // (src/GMGSolver.cu:26-39) into one byte so the kernels never load neighbour cell types.
+#include "kernels.cuh"
 #include "solver_internal.hpp"
 #include "topology.hpp"
 
@@ -264,6 +265,17 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
     CK((cudaError_t)(upload(&g->d_inst, g_inst) ? cudaErrorMemoryAllocation : cudaSuccess));
     CK((cudaError_t)(upload(&g->d_inst_h0, g->inst_h0) ? cudaErrorMemoryAllocation : cudaSuccess));
     {
+        // level constants per instance and level, computed here with the device's IEEE float
+        // operations (the kernels would otherwise recompute them in every thread)
+        std::vector<float4> lc((size_t)K * kLevelSlots);
+        for (int i = 0; i < K; i++)
+            for (int l = 0; l < kLevelSlots; l++) {
+                const LevelConst<float> L(g->inst_h0[i], l);
+                lc[(size_t)i * kLevelSlots + l] = make_float4(L.h, L.c1, L.c2, L.dfast);
+            }
+        CK((cudaError_t)(upload(&g->d_lconst, lc) ? cudaErrorMemoryAllocation : cudaSuccess));
+    }
+    {
         // ghost bookkeeping of the fused Laplacian: slot of each GHOST tile, the ghost slot of the
         // GHOST child in each octant, and a 64-float partial-sum row per ghost
         std::vector<int> gslot(n, -1), gchild((size_t)n * 8, -1);
@@ -440,6 +452,7 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
     g->topo.ghost_list = g->d_ghost;
     g->topo.inst = g->d_inst;
     g->topo.inst_h0 = g->d_inst_h0;
+    g->topo.lconst = g->d_lconst;
     g->bytes = cells * kNumChannels * sizeof(float) + cells * 3 + sizeof(TileMeta) * n + sizeof(uint32_t) * n + sizeof(int) * nl +
                sizeof(int) * 22 * (size_t)n + cells * sizeof(float);
     *out = g;
@@ -457,6 +470,7 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_edge);
     cudaFree(g->d_inst);
     cudaFree(g->d_inst_h0);
+    cudaFree(g->d_lconst);
     cudaFree(g->d_ghost_tables);
     cudaFree(g->d_gacc);
     cudaFree(g->d_xpre);

@@ -87,11 +87,13 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const in
     for (int u = 0; u < NT; u++) {
         const int q = (blockIdx.x * NT + u) * TPB + g;
         tile[u] = q < n ? list[q] : 0;
-        act[u] = q < n && !tile_done(tp, S, tile[u]);
+        act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (act[u]) stage_async(X, nullptr, tp.mask_lap, tile[u], halo_nb(tp.meta, tile[u], t), t, st[u * TPB + g]);
+#pragma unroll
+    for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
     __syncthreads();
     bool ghost[NT];
@@ -102,7 +104,7 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const in
         TileStage& ts = st[u * TPB + g];
         const int packed = tp.meta[tile[u]].packed;
         ghost[u] = meta_type(packed) & GHOST_T;
-        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(packed));
+        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(packed));
         float out[4], dg[4];
         neg_lap4<float, false, false>(ts.xs, ts.hx, t, *reinterpret_cast<const uint32_t*>(ts.mask + t * 4), tp.fcls[tile[u]] & 0xfffu,
                                       L, out, dg);
@@ -184,18 +186,20 @@ __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __re
     for (int u = 0; u < NT; u++) {
         const int q = (blockIdx.x * NT + u) * TPB + g;
         tile[u] = q < n ? list[q] : 0;
-        act[u] = q < n && !tile_done(tp, S, tile[u]);
+        act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (act[u]) stage_async(X, R, tp.mask_mg, tile[u], halo_nb(tp.meta, tile[u], t), t, st[u * TPB + g]);
+#pragma unroll
+    for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         const TileStage& ts = st[u * TPB + g];
-        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(tp.meta[tile[u]].packed));
+        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ts.mask + t * 4);
         st4(X + (size_t)tile[u] * kTileCells + t * 4,
             colour_update(ts.xs, ts.hx, t, mask4, (tp.fcls[tile[u]] >> 12) & 0xfffu, L, ld4(ts.b + t * 4), color));
@@ -227,7 +231,7 @@ __global__ void __launch_bounds__(1024) k_gs_sequence(Topo tp, const int* __rest
             if (active) {
                 const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
                 const V4<float> b = ld4(R + (size_t)tile * kTileCells + t * 4);
-                const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
+                const LevelConst<float> L = tile_level_const(tp, tile, meta_level(m.packed));
                 st4(X + (size_t)tile * kTileCells + t * 4,
                     colour_update(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, b, color));
             }
@@ -254,18 +258,20 @@ __global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int fi
     for (int u = 0; u < NT; u++) {
         const int q = (blockIdx.x * NT + u) * TPB + g;
         tile[u] = first + (q < n ? q : 0);
-        act[u] = q < n && !tile_done(tp, S, tile[u]);
+        act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (act[u]) stage_async(X, RHS, tp.mask_mg, tile[u], halo_nb(tp.meta, tile[u], t), t, st[u * TPB + g]);
+#pragma unroll
+    for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         TileStage& ts = st[u * TPB + g];
-        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(tp.meta[tile[u]].packed));
+        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
         float ax[4], d[4];
         neg_lap4<float, false>(ts.xs, ts.hx, t, *reinterpret_cast<const uint32_t*>(ts.mask + t * 4),
                                (tp.fcls[tile[u]] >> 12) & 0xfffu, L, ax, d);

@@ -49,7 +49,8 @@ template <bool FUSED> __device__ __forceinline__ double fmadd(double a, double b
 // dfast: the diagonal of a cell with six 1/h^2 faces, summed and scaled as neg_lap4 does.
 template <class T> struct LevelConst {
     T h, c1, c2, dfast;
-    __device__ __forceinline__ LevelConst(T h0, int level) {
+    __device__ __forceinline__ explicit LevelConst(float4 v) : h(v.x), c1(v.y), c2(v.z), dfast(v.w) {}
+    __host__ __device__ __forceinline__ LevelConst(T h0, int level) {
         h = h0 / T(1 << level);
         const T ooh = T(1) / h;
         c1 = ooh * ooh;                  // (ooh*1 + x*0) * ooh
@@ -64,6 +65,13 @@ template <class T> struct LevelConst {
 // compiler never fuses the last product into a following addition).
 __device__ __forceinline__ float mul_h3(float s, float h) { return __fmul_rn(__fmul_rn(__fmul_rn(s, h), h), h); }
 __device__ __forceinline__ double mul_h3(double s, double h) { return __dmul_rn(__dmul_rn(__dmul_rn(s, h), h), h); }
+
+// The level constants of a tile from the per-instance table (the same values LevelConst's
+// constructor computes, precomputed once per grid).
+__device__ __forceinline__ LevelConst<float> tile_level_const(const Topo& tp, int tile, int level) {
+    const float4 v = tp.lconst[tp.inst[tile] * kLevelSlots + level];
+    return LevelConst<float>(v);
+}
 
 struct TileIdx {
     int i, j, k0;

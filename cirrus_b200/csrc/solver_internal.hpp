@@ -81,6 +81,7 @@ struct DevGrid {
     std::vector<std::vector<TileRun>> inst_runs;
     int* d_inst = nullptr;          // n: instance of each tile
     float* d_inst_h0 = nullptr;
+    float4* d_lconst = nullptr;     // per instance x kLevelSlots: level constants
 
     float* d_chbuf = nullptr;
     float* d_ch[kNumChannels] = {};

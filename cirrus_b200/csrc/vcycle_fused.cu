@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
     for (int u = 0; u < NT; u++) {
         const int q = (blockIdx.x * NT + u) * TPB + g;
         tile[u] = q < n ? list[q] : 0;
-        act[u] = q < n && !tile_done(tp, S, tile[u]);
+        act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
     // neighbour of this thread's x/y-face piece (t < 64) and z-face cell; GHOST neighbours count
     // as absent (their x is 0 on the way down)
@@ -126,6 +126,8 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
             }
         }
     }
+#pragma unroll
+    for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
     __syncthreads();
     // first colour (0) of the own cells and of the live neighbours' first layer, in place
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         PreStage& ps = st[u * TPB + g];
-        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(tp.meta[tile[u]].packed));
+        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
         const uint32_t cls = (tp.fcls[tile[u]] >> 12) & 0xfffu;
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ps.mask + t * 4);
         const V4<float> b = ld4(ps.b + t * 4);
@@ -188,7 +190,7 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         PreStage& ps = st[u * TPB + g];
-        const LevelConst<float> L(tile_h0(tp, tile[u]), meta_level(tp.meta[tile[u]].packed));
+        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
         st4(XP + (size_t)tile[u] * kTileCells + t * 4,
             colour_update(ps.xs, ps.hx, t, *reinterpret_cast<const uint32_t*>(ps.mask + t * 4), (tp.fcls[tile[u]] >> 12) & 0xfffu, L,
                           ld4(ps.b + t * 4), 1));
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first,
     if (!ghost) {
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
         const V4<float> b = ld4(RHS + (size_t)tile * kTileCells + t * 4);
-        const LevelConst<float> L(tile_h0(tp, tile), meta_level(m.packed));
+        const LevelConst<float> L = tile_level_const(tp, tile, meta_level(m.packed));
         o = colour_update(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, b, 1);
     }
     st4(Z + (size_t)tile * kTileCells + t * 4, o);
@@ -367,7 +369,6 @@ __global__ void __launch_bounds__(1024) k_bottom(Topo tp, const BottomInst* __re
     float* X = reinterpret_cast<float*>(T + nb);
     float* B = X + cells;
     uint16_t* CODE = reinterpret_cast<uint16_t*>(B + cells);
-    const float h0 = tp.inst_h0[inst];
     // cells is a multiple of 8: every region is 16-byte aligned and copied in 16-byte vectors
     for (int t = threadIdx.x; t < nb; t += blockDim.x) T[t] = tiles[bi.rec_off + t];
     for (int v = threadIdx.x; v < cells / 4; v += blockDim.x) {
@@ -391,7 +392,7 @@ __global__ void __launch_bounds__(1024) k_bottom(Topo tp, const BottomInst* __re
     __syncthreads();
     for (int ph = 0; ph < prog.nphase; ph++) {
         const int op = prog.op[ph], level = prog.level[ph];
-        const LevelConst<float> L(h0, level);
+        const LevelConst<float> L(tp.lconst[inst * kLevelSlots + level]);
         const int sy = bi.sy[level], sz = bi.sz[level], first = bi.first[level];
         if (op == 1) {
             // one colour of GaussSeidelGMG on the level's LEAF|NONLEAF tiles; items are the 256 cells
