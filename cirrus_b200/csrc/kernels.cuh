@@ -140,6 +140,17 @@ __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32
         }
         return;
     }
+    if ((mask4 & 0x3F3F3F3Fu) == 0u) {
+        // no coupled face on any of the four cells (e.g. inside a GHOST tile, whose ghost-ghost
+        // faces carry no coefficient): every product is 0, the sum stays +0, and so do the
+        // result and the diagonal (for finite values, the general path's bits)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            out[e] = T(0);
+            if (DIAG) diag[e] = T(0);
+        }
+        return;
+    }
     auto cross = [&](int f) -> T { return ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1; };
     const T cxm = ix.i == 0 ? cross(0) : L.c1;
     const T cxp = ix.i == 7 ? cross(1) : L.c1;

@@ -173,6 +173,52 @@ def ring(base: int = 2, fine: int = 6, seed: int = 0) -> Workload:
                                 f"box obstacle c=(.5,.5,1) half .1")
 
 
+def random_spheres(seed: int = 0) -> Workload:
+    """One instance of the batched configuration: effective size log-uniform over 64^3, 128^3,
+    256^3 (finest level 3-5), 1-4 levels of leaves, refinement in an 8-fine-cell band around 1-5
+    seeded spheres of radius U(0.05, 0.25); Neumann box walls with a Dirichlet top."""
+    rng = np.random.default_rng(0x5EED0000 + seed)
+    fine = int(rng.integers(3, 6))
+    depth = int(rng.integers(1, 5))
+    base = max(fine - depth + 1, 0)
+    k = int(rng.integers(1, 6))
+    centers = rng.uniform(0.2, 0.8, size=(k, 3))
+    radii = rng.uniform(0.05, 0.25, size=k)
+    band = 8 / float(8 << fine)
+    masks: list[np.ndarray | None] = [None] * 10
+    for l in range(fine):
+        lo, hi = _tile_boxes(l, (1, 1, 1), 1 / 8)
+        if l < base:
+            masks[l] = np.ones(lo.shape[:3], dtype=np.uint8)
+            continue
+        near = np.zeros(lo.shape[:3], dtype=bool)
+        for c, r in zip(centers, radii):
+            dmin2 = _box_point_dist2(lo, hi, c)
+            dmax2 = _box_far_dist2(lo, hi, c)
+            near |= (dmin2 <= (r + band) ** 2) & (dmax2 >= max(r - band, 0.0) ** 2)
+        masks[l] = near.astype(np.uint8)
+    eff = 8 << fine
+    return Workload(name=f"spheres{eff}_d{depth}_s{seed}", roots=[(0, 0, 0)], root_extent=(1, 1, 1), masks=masks, seed=seed,
+                    description=f"{eff}^3 effective, leaves at levels {base}-{fine}, {k} random spheres",
+                    meta={"fine": fine, "depth": depth, "spheres": k, "velocity": "stream"})
+
+
+def stream_velocity(tiles: np.ndarray, seed: int) -> np.ndarray:
+    """(3, n, 512) float32 N(0,1) lower-face velocities on LEAF tiles from one seeded stream in
+    all-tiles order (reproducible for a given tile list; faster than face_velocity)."""
+    n = tiles.shape[0]
+    out = np.zeros((3, n, 512), dtype=np.float32)
+    leaf = np.flatnonzero((tiles[:, 4] & LEAF) != 0)
+    rng = np.random.default_rng(0xF00D0000 + seed)
+    out[:, leaf] = rng.standard_normal((3, leaf.size, 512), dtype=np.float32)
+    return out
+
+
+def batch_of_spheres(count: int = 64, seed0: int = 0) -> list[Workload]:
+    """The batched configuration: `count` independent random_spheres instances."""
+    return [random_spheres(seed0 + i) for i in range(count)]
+
+
 WORKLOADS: dict[str, Callable[..., Workload]] = {
     "uniform128": lambda seed=0: uniform(4, seed),
     "sphere256": lambda seed=0: sphere(3, 5, seed),
@@ -244,22 +290,26 @@ def _splitmix(x: np.ndarray) -> np.ndarray:
 
 
 def face_velocity(tiles: np.ndarray, seed: int) -> np.ndarray:
-    """(3, n, 512) float32 N(0,1) lower-face velocities on LEAF tiles (0 elsewhere)."""
+    """(3, n, 512) float32 N(0,1) lower-face velocities on LEAF tiles (0 elsewhere); the value of
+    a face depends only on (seed, level, global cell, axis)."""
     n = tiles.shape[0]
+    out = np.zeros((3, n, 512), dtype=np.float32)
+    leaf = np.flatnonzero((tiles[:, 4] & LEAF) != 0)
+    m = leaf.size
+    if m == 0:
+        return out
     o = np.arange(512)
     loc = np.stack([o >> 6, (o >> 3) & 7, o & 7], axis=-1).astype(np.int64)
-    g = tiles[:, None, 1:4].astype(np.int64) * 8 + loc[None]
-    lev = np.broadcast_to(tiles[:, None, 0].astype(np.int64), (n, 512))
-    out = np.zeros((3, n, 512), dtype=np.float32)
-    leaf = (tiles[:, 4] & LEAF) != 0
+    g = tiles[leaf, None, 1:4].astype(np.int64) * 8 + loc[None]
+    lev = np.broadcast_to(tiles[leaf, None, 0].astype(np.int64), (m, 512))
     for axis in range(3):
-        k = _splitmix(np.full((n, 512), np.uint64(seed), dtype=np.uint64))
-        for comp in (lev, g[..., 0], g[..., 1], g[..., 2], np.full((n, 512), axis, dtype=np.int64)):
+        k = _splitmix(np.full((m, 512), np.uint64(seed), dtype=np.uint64))
+        for comp in (lev, g[..., 0], g[..., 1], g[..., 2], np.full((m, 512), axis, dtype=np.int64)):
             k = _splitmix(k ^ comp.astype(np.uint64))
         u1 = ((_splitmix(k) >> np.uint64(11)).astype(np.float64) + 0.5) * (1.0 / 9007199254740992.0)
         u2 = ((_splitmix(k ^ np.uint64(0x5851F42D4C957F2D)) >> np.uint64(11)).astype(np.float64)) * (1.0 / 9007199254740992.0)
         z = np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
-        out[axis] = np.where(leaf[:, None], z, 0.0).astype(np.float32)
+        out[axis, leaf] = z.astype(np.float32)
     return out
 
 
@@ -306,5 +356,5 @@ def build(w: Workload):
     topo.set_cell_types(leaf_cell_types(w, tiles, nbr6))
     topo.calc_cell_types_from_leafs()
     ct = topo.cell_types()
-    vel = face_velocity(tiles, w.seed)
+    vel = stream_velocity(tiles, w.seed) if w.meta.get("velocity") == "stream" else face_velocity(tiles, w.seed)
     return Built(w, tiles, nbr6, ct, vel, topo)
