@@ -227,6 +227,16 @@ class DeviceGrid:
         (results are unchanged by the choice); overwrites channels 2-5."""
         check(lib().cirrus_grid_autotune(self._h, reps, C.c_void_p(stream)), "cirrus_grid_autotune")
 
+    def set_launch_shape(self, shape: int, kernel: int = -1, level: int = -1) -> None:
+        """Set the launch shape (0..3) of one staged stencil kernel (KERNEL_*, -1: all) on one
+        level (-1: all); results are unchanged by the choice."""
+        check(lib().cirrus_grid_set_launch_shape(self._h, kernel, level, shape), "cirrus_grid_set_launch_shape")
+
+    def get_launch_shape(self, kernel: int, level: int = 0) -> int:
+        v = C.c_int(0)
+        check(lib().cirrus_grid_get_launch_shape(self._h, kernel, level, C.byref(v)), "cirrus_grid_get_launch_shape")
+        return v.value
+
     def bench_launch(self, kernel: int, level: int = 0, reps: int = 1, stream: int = 0) -> None:
         """Launch one solve kernel `reps` times on `stream` (for timing with the caller's events);
         overwrites channels 2-5."""
@@ -359,7 +369,7 @@ class GMGSolver:
         return r.iters, r.rel_residual
 
     def solve_batch(self, grid: DeviceGrid, active: Sequence[bool] | None = None, tolerances: Sequence[float] | None = None,
-                    stream: int = 0, **kw) -> list[tuple[int, float]]:
+                    pure_neumann: Sequence[bool] | None = None, stream: int = 0, **kw) -> list[tuple[int, float]]:
         """Solve every (active) instance of a batched grid in one graph launch; per-instance
         (iters, relative residual).  Each instance's bits do not depend on the rest of the batch."""
         p = self.params(**kw)
@@ -367,7 +377,8 @@ class GMGSolver:
         res = (SolveResult * k)()
         act = (C.c_int * k)(*[int(bool(a)) for a in active]) if active is not None else None
         tol = (C.c_double * k)(*tolerances) if tolerances is not None else None
-        check(lib().cirrus_gmg_solve_batch(grid.handle, C.byref(p), act, tol, C.c_void_p(stream), res), "cirrus_gmg_solve_batch")
+        pn = (C.c_int * k)(*[int(bool(x)) for x in pure_neumann]) if pure_neumann is not None else None
+        check(lib().cirrus_gmg_solve_batch(grid.handle, C.byref(p), act, tol, pn, C.c_void_p(stream), res), "cirrus_gmg_solve_batch")
         self.last_results = list(res)
         self.last_result = res[0]
         return [(r.iters, r.rel_residual) for r in res]

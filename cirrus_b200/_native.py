@@ -129,7 +129,7 @@ _PROTOS = {
     "cirrus_add_gradient_to_face_centers": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_solve_params_default": (None, [C.POINTER(SolveParams)]),
     "cirrus_gmg_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveResult)]),
-    "cirrus_gmg_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_int_p, c_f64_p, C.c_void_p,
+    "cirrus_gmg_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_int_p, c_f64_p, c_int_p, C.c_void_p,
                                          C.POINTER(SolveResult)]),
     "cirrus_gmg_solve_host": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p, C.POINTER(SolveResult)]),
     "cirrus_server_create": (C.c_int, [C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),
@@ -141,6 +141,8 @@ _PROTOS = {
     "cirrus_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), c_int_p, c_int_p,
                                       C.POINTER(C.c_longlong)]),
     "cirrus_grid_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "cirrus_grid_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "cirrus_grid_get_launch_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "cirrus_bench_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_true_residual": (C.c_int, [C.c_void_p, c_f32_p, c_f64_p, C.c_void_p]),
     "cirrus_grid_get_solution_f64": (C.c_int, [C.c_void_p, c_f64_p, C.c_void_p]),

@@ -38,6 +38,12 @@ float time_graph(F launch, int reps, cudaStream_t s) {
 
 }  // namespace
 
+void drop_graphs(DevGrid& g) {
+    // solve graphs captured with the previous shapes are rebuilt on the next solve
+    for (auto& kv : g.graphs) cudaGraphExecDestroy(kv.second.exec);
+    g.graphs.clear();
+}
+
 int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
     if (reps < 1) reps = 1;
     // timing runs on a private stream (the caller's may be the legacy default stream, which
@@ -72,12 +78,12 @@ int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
             pick(KS_PRESMOOTH, l, [&] { launch::presmooth(g, l, g.d_xpre, ap, nullptr, s); });
         if (l >= 1 && g.level_count[l] > 0)
             pick(KS_RESIDUAL, l, [&] { launch::residual_restrict(g, l, g.d_xpre, ap, tmp, 1.f, nullptr, s); });
+        if (l >= 1 && g.level_count[l] > 0 && g.bottom_level >= 0)
+            pick(KS_PROLONG, l, [&] { launch::prolong_sweep(g, l, z, g.d_xpre, ap, 1.f, nullptr, s); });
     }
     if (g.n_leafghost > 0) pick(KS_LAPLACIAN, 0, [&] { launch::laplacian_fused(g, p, tmp, nullptr, s); });
     g.launch_count = count0;
-    // solve graphs captured with the previous shapes are rebuilt on the next solve
-    for (auto& kv : g.graphs) cudaGraphExecDestroy(kv.second.exec);
-    g.graphs.clear();
+    drop_graphs(g);
     const bool ok = cudaStreamSynchronize(s) == cudaSuccess;
     cudaStreamDestroy(s);
     return ok ? 0 : 2;

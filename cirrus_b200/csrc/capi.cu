@@ -443,7 +443,8 @@ void cirrus_solve_params_default(cirrus_solve_params* p) {
 }
 
 cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_params* params, const int* active,
-                                     const double* tolerances, void* stream, cirrus_solve_result* results) {
+                                     const double* tolerances, const int* pure_neumann, void* stream,
+                                     cirrus_solve_result* results) {
     if (!grid || !params_ok(params) || !results) return CIRRUS_ERR_INVALID_ARGUMENT;
     const int K = grid->g->num_inst;
     if (tolerances)
@@ -456,6 +457,7 @@ cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_param
         for (int i = 0; i < K; i++) {
             req[i].active = active ? (active[i] ? 1 : 0) : 1;
             if (tolerances) req[i].tol = tolerances[i];
+            if (pure_neumann) req[i].pure_neumann = pure_neumann[i] ? 1 : 0;
         }
         std::vector<cirrus::SolveResult> r(K);
         if (p.precision != CIRRUS_PRECISION_MIXED_FP64) grid->g->x64_valid = false;
@@ -478,7 +480,7 @@ cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* par
     if (!grid || !params_ok(params) || !result) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] {
         std::vector<cirrus_solve_result> all(grid->g->num_inst);
-        cirrus_status st = cirrus_gmg_solve_batch(grid, params, nullptr, nullptr, stream, all.data());
+        cirrus_status st = cirrus_gmg_solve_batch(grid, params, nullptr, nullptr, nullptr, stream, all.data());
         if (st == CIRRUS_OK) *result = all[0];
         return st;
     });
@@ -499,6 +501,44 @@ cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params
 cirrus_status cirrus_grid_autotune(cirrus_grid* grid, int reps, void* stream) {
     if (!grid) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] { return map_rc(cirrus::autotune(*grid->g, S(stream), reps > 0 ? reps : 20, nullptr)); });
+}
+
+namespace {
+// CIRRUS_KERNEL_* of a kernel with launch shapes -> its row in DevGrid::shapes (-1: none)
+int shape_kind(int kernel) {
+    switch (kernel) {
+    case CIRRUS_KERNEL_LAPLACIAN: return cirrus::KS_LAPLACIAN;
+    case CIRRUS_KERNEL_GS_SWEEP: return cirrus::KS_GS_SWEEP;
+    case CIRRUS_KERNEL_PRESMOOTH: return cirrus::KS_PRESMOOTH;
+    case CIRRUS_KERNEL_PROLONG_SWEEP: return cirrus::KS_PROLONG;
+    case CIRRUS_KERNEL_RESIDUAL_RESTRICT: return cirrus::KS_RESIDUAL;
+    default: return -1;
+    }
+}
+}  // namespace
+
+cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape) {
+    if (!grid || shape < 0 || shape >= CIRRUS_NUM_LAUNCH_SHAPES || shape >= cirrus::kNumShapes) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    if (kernel != -1 && shape_kind(kernel) < 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (level < -1 || level >= g.num_layers) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        for (int k = 0; k < cirrus::KS_COUNT; k++) {
+            if (kernel != -1 && k != shape_kind(kernel)) continue;
+            for (int l = 0; l < g.num_layers; l++)
+                if (level == -1 || l == level) g.shapes[(size_t)k * g.num_layers + l] = (uint8_t)shape;
+        }
+        cirrus::drop_graphs(g);  // graphs captured with the previous shapes
+        return CIRRUS_OK;
+    });
+}
+
+cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int level, int* shape) {
+    if (!grid || !shape || shape_kind(kernel) < 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+    const auto& g = *grid->g;
+    if (level < 0 || level >= g.num_layers) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *shape = g.shape(shape_kind(kernel), level);
+    return CIRRUS_OK;
 }
 
 cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int reps, void* stream) {

@@ -113,13 +113,15 @@ template <class T, bool DIAG, bool FUSED = true>
 __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32_t mask4, uint32_t cls,
                                          const LevelConst<T>& L, T out[4], T diag[4]) {
     const TileIdx ix(t);
+    // each neighbour vector comes from the tile or from its halo: the address is selected, then
+    // one load issued
     const V4<T> xc = ld4(xs + t * 4);
-    const V4<T> xm = ix.i > 0 ? ld4(xs + (t - 16) * 4) : ld4(hx + 0 * 64 + ix.j * 8 + ix.k0);
-    const V4<T> xp = ix.i < 7 ? ld4(xs + (t + 16) * 4) : ld4(hx + 1 * 64 + ix.j * 8 + ix.k0);
-    const V4<T> ym = ix.j > 0 ? ld4(xs + (t - 2) * 4) : ld4(hx + 2 * 64 + ix.i * 8 + ix.k0);
-    const V4<T> yp = ix.j < 7 ? ld4(xs + (t + 2) * 4) : ld4(hx + 3 * 64 + ix.i * 8 + ix.k0);
-    const T zlo = ix.k0 > 0 ? xs[t * 4 - 1] : hx[4 * 64 + ix.i * 8 + ix.j];
-    const T zhi = ix.k0 < 4 ? xs[t * 4 + 4] : hx[5 * 64 + ix.i * 8 + ix.j];
+    const V4<T> xm = ld4(ix.i > 0 ? xs + (t - 16) * 4 : hx + 0 * 64 + ix.j * 8 + ix.k0);
+    const V4<T> xp = ld4(ix.i < 7 ? xs + (t + 16) * 4 : hx + 1 * 64 + ix.j * 8 + ix.k0);
+    const V4<T> ym = ld4(ix.j > 0 ? xs + (t - 2) * 4 : hx + 2 * 64 + ix.i * 8 + ix.k0);
+    const V4<T> yp = ld4(ix.j < 7 ? xs + (t + 2) * 4 : hx + 3 * 64 + ix.i * 8 + ix.k0);
+    const T zlo = *(ix.k0 > 0 ? xs + t * 4 - 1 : hx + 4 * 64 + ix.i * 8 + ix.j);
+    const T zhi = *(ix.k0 < 4 ? xs + t * 4 + 4 : hx + 5 * 64 + ix.i * 8 + ix.j);
     if (mask4 == 0x7F7F7F7Fu) {
         // the four cells are INTERIOR with six 1/h^2 faces: every coefficient is c1 (the same
         // operations as the general path below with a_f = c1)
@@ -230,12 +232,12 @@ __device__ __forceinline__ V4<float> colour_update(const float* xs, const float*
                                                    const LevelConst<float>& L, const V4<float>& b, int color) {
     const TileIdx ix(t);
     const V4<float> xc = ld4(xs + t * 4);
-    const V4<float> xm = ix.i > 0 ? ld4(xs + (t - 16) * 4) : ld4(hx + 0 * 64 + ix.j * 8 + ix.k0);
-    const V4<float> xp = ix.i < 7 ? ld4(xs + (t + 16) * 4) : ld4(hx + 1 * 64 + ix.j * 8 + ix.k0);
-    const V4<float> ym = ix.j > 0 ? ld4(xs + (t - 2) * 4) : ld4(hx + 2 * 64 + ix.i * 8 + ix.k0);
-    const V4<float> yp = ix.j < 7 ? ld4(xs + (t + 2) * 4) : ld4(hx + 3 * 64 + ix.i * 8 + ix.k0);
-    const float zlo = ix.k0 > 0 ? xs[t * 4 - 1] : hx[4 * 64 + ix.i * 8 + ix.j];
-    const float zhi = ix.k0 < 4 ? xs[t * 4 + 4] : hx[5 * 64 + ix.i * 8 + ix.j];
+    const V4<float> xm = ld4(ix.i > 0 ? xs + (t - 16) * 4 : hx + 0 * 64 + ix.j * 8 + ix.k0);
+    const V4<float> xp = ld4(ix.i < 7 ? xs + (t + 16) * 4 : hx + 1 * 64 + ix.j * 8 + ix.k0);
+    const V4<float> ym = ld4(ix.j > 0 ? xs + (t - 2) * 4 : hx + 2 * 64 + ix.i * 8 + ix.k0);
+    const V4<float> yp = ld4(ix.j < 7 ? xs + (t + 2) * 4 : hx + 3 * 64 + ix.i * 8 + ix.k0);
+    const float zlo = *(ix.k0 > 0 ? xs + t * 4 - 1 : hx + 4 * 64 + ix.i * 8 + ix.j);
+    const float zhi = *(ix.k0 < 4 ? xs + t * 4 + 4 : hx + 5 * 64 + ix.i * 8 + ix.j);
     const bool p = (color + ix.i + ix.j) & 1;
     const uint32_t mA = (mask4 >> (p ? 8 : 0)) & 0xffu, mB = (mask4 >> (p ? 24 : 16)) & 0xffu;
     const float A = gs_cell(p ? xc.v[1] : xc.v[0], p ? xm.v[1] : xm.v[0], p ? xp.v[1] : xp.v[0], p ? ym.v[1] : ym.v[0],
@@ -258,6 +260,10 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 

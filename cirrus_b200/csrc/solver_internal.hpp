@@ -273,6 +273,8 @@ int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s);
 // kernel and level (autotune.cu); overwrites the scratch channels 2-5.  report (optional) gets one
 // line per choice.
 int autotune(DevGrid& g, cudaStream_t s, int reps, std::string* report);
+// Destroys the grid's cached solve graphs (after a change of launch shapes).
+void drop_graphs(DevGrid& g);
 // Copy the last solution to the host in FP64 (num_tiles*512 doubles, pool order).
 int solution_f64(DevGrid& g, double* host, cudaStream_t s);
 

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
         nbf[u] = nbz[u] = -1;
         if (!act[u]) continue;
         PreStage& ps = st[u * TPB + g];
-        const TileMeta m = tp.meta[tile[u]];
+        const TileMeta& m = tp.meta[tile[u]];
         const size_t base = (size_t)tile[u] * kTileCells;
         cp_async16(ps.b + t * 4, RHS + base + t * 4);
         if (t < 32) cp_async16(ps.mask + t * 16, tp.mask_mg + base + t * 16);
@@ -198,94 +198,167 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
 }
 
 // ---------------------------------------------------------------------------- up: prolongation + first colour
-// Value of cell `off` of `tile` after ProlongateAndUpdate128 (src/GMGSolver.cu:345-376): parent
-// value by injection; GHOST: x = cx, others x = fma(prolong_coeff, cx, xpre); 0 off INTERIOR.
-__device__ __forceinline__ float prolongated(const Topo& tp, const float* __restrict__ Z, const float* __restrict__ XP, int tile,
-                                             const TileMeta& tm, int off, float prolong_coeff) {
-    if (!(tp.mask_mg[(size_t)tile * kTileCells + off] & kMaskInterior)) return 0.f;
-    float cx = 0.f;
-    if (tm.parent >= 0) {
-        const int oct = meta_octant(tm.packed);
-        cx = Z[(size_t)tm.parent * kTileCells + ((oct & 1) * 4 + (off >> 7)) * 64 + (((oct >> 1) & 1) * 4 + ((off >> 4) & 3)) * 8 +
-               ((oct >> 2) & 1) * 4 + ((off & 7) >> 1)];
-    }
-    return (meta_type(tm.packed) & GHOST_T) ? cx : fmaf(prolong_coeff, cx, XP[(size_t)tile * kTileCells + off]);
+// Staging area of the prolongation kernel: the tile's pre-smoothed x, right-hand side, mask and
+// its parent's octant block (4x4x4 coarse values); per face neighbour the pre-smoothed x and mask
+// of its first layer and the coarse values over it.  xs/hx receive the prolongated values.
+struct __align__(16) ProStage {
+    float xs[kTileCells];
+    float hx[6 * 64];
+    float xp[kTileCells];
+    float b[kTileCells];
+    float hxp[6 * 64];
+    float pblk[64];
+    float hpar[4 * 16 * 2 + 2 * 64];  // x/y faces: 2 coarse values per 4-cell run; z faces: 1 per cell
+    uint8_t mask[kTileCells];
+    uint8_t hmask[6 * 64];
+};
+
+// The coarse cell under fine cell `off` of a tile in octant `oct` of its parent.
+__device__ __forceinline__ int parent_cell(int oct, int off) {
+    return ((oct & 1) * 4 + (off >> 7)) * 64 + (((oct >> 1) & 1) * 4 + ((off >> 4) & 3)) * 8 + ((oct >> 2) & 1) * 4 + ((off & 7) >> 1);
 }
 
-// prolongated() for the four cells off4..off4+3 (off4 a multiple of 4: one run along k, whose
-// parent values are two consecutive cells).
-__device__ __forceinline__ V4<float> prolongated4(const Topo& tp, const float* __restrict__ Z, const float* __restrict__ XP, int tile,
-                                                  const TileMeta& tm, int off4, float prolong_coeff) {
-    const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + off4);
-    const bool ghost = meta_type(tm.packed) & GHOST_T;
-    float cx0 = 0.f, cx1 = 0.f;
-    if (tm.parent >= 0) {
-        const int oct = meta_octant(tm.packed);
-        const float2 c = *reinterpret_cast<const float2*>(
-            Z + (size_t)tm.parent * kTileCells + ((oct & 1) * 4 + (off4 >> 7)) * 64 + (((oct >> 1) & 1) * 4 + ((off4 >> 4) & 3)) * 8 +
-            ((oct >> 2) & 1) * 4 + ((off4 & 7) >> 1));
-        cx0 = c.x;
-        cx1 = c.y;
-    }
-    V4<float> xp = zero4<float>();
-    if (!ghost) xp = ld4(XP + (size_t)tile * kTileCells + off4);
-    V4<float> o;
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-        const float cx = e < 2 ? cx0 : cx1;
-        o.v[e] = ((mask4 >> (8 * e)) & kMaskInterior) ? (ghost ? cx : fmaf(prolong_coeff, cx, xp.v[e])) : 0.f;
-    }
-    return o;
+// prolongated() from staged values: mask byte mm, coarse value cx (0 without a parent), x.
+__device__ __forceinline__ float prolong_value(uint32_t mm, bool ghost, float cx, float x, float prolong_coeff) {
+    return (mm & kMaskInterior) ? (ghost ? cx : fmaf(prolong_coeff, cx, x)) : 0.f;
 }
 
 // Prolongation into every tile of one level; on mg tiles also the first colour (1) of
-// GaussSeidelGMG(1, 1).  Reads Z of the coarser level and XP of this level, writes Z of this level.
-template <int TPB>
+// GaussSeidelGMG(1, 1).  Reads Z of the coarser level and XP of this level, writes Z of this
+// level.  NT tiles per 128-thread group are staged with asynchronous copies.
+template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first, int n, float* Z, const float* __restrict__ XP,
                                                              const float* __restrict__ RHS, float prolong_coeff,
                                                              const Scalars* __restrict__ S) {
     pdl_entry();
-    __shared__ TileShared<float> sh[TPB];
+    extern __shared__ __align__(16) unsigned char pro_smem[];
+    ProStage* st = reinterpret_cast<ProStage*>(pro_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-    const int q = blockIdx.x * TPB + g;
-    const int tile = first + (q < n ? q : 0);
-    const bool active = q < n && !tile_done(tp, S, tile);
-    TileMeta m;
-    bool ghost = false;
-    if (active) {
-        m = tp.meta[tile];
-        ghost = meta_type(m.packed) & GHOST_T;
-        st4(sh[g].xs + t * 4, prolongated4(tp, Z, XP, tile, m, t * 4, prolong_coeff));
-        if (!ghost) {
-            if (t < 64) {
-                const int face = t >> 4, qq = t & 15;
-                const int nb = m.nb[face];
-                int off;
-                if (face == 0) off = 448 + qq * 4;
-                else if (face == 1) off = qq * 4;
-                else if (face == 2) off = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
-                else off = (qq >> 1) * 64 + (qq & 1) * 4;
-                st4(sh[g].hx + face * 64 + qq * 4, nb >= 0 ? prolongated4(tp, Z, XP, nb, tp.meta[nb], off, prolong_coeff) : zero4<float>());
+    // this thread's halo pieces: x/y-face run (t < 64) and z-face cell
+    const int fface = t >> 4, qq = t & 15;
+    int foff;
+    if (fface == 0) foff = 448 + qq * 4;
+    else if (fface == 1) foff = qq * 4;
+    else if (fface == 2) foff = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
+    else foff = (qq >> 1) * 64 + (qq & 1) * 4;
+    const int zface = 4 + (t >> 6), zc = t & 63;
+    const int zoff = (zc >> 3) * 64 + (zc & 7) * 8 + (zface == 4 ? 7 : 0);
+    int tile[NT];
+    bool act[NT], ghost[NT];
+    uint32_t hf[NT];  // bits: 0 f-neighbour, 1 f ghost, 2 f has parent, 3 z-neighbour, 4 z ghost, 5 z has parent, 6 own parent
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        const int q = (blockIdx.x * NT + u) * TPB + g;
+        tile[u] = first + (q < n ? q : 0);
+        act[u] = q < n;  // finished instances are dropped after the copies are issued
+        ghost[u] = false;
+        hf[u] = 0;
+        if (!act[u]) continue;
+        ProStage& ps = st[u * TPB + g];
+        const TileMeta& m = tp.meta[tile[u]];
+        ghost[u] = meta_type(m.packed) & GHOST_T;
+        const size_t base = (size_t)tile[u] * kTileCells;
+        if (t < 32) cp_async16(ps.mask + t * 16, tp.mask_mg + base + t * 16);
+        if (!ghost[u]) {
+            cp_async16(ps.xp + t * 4, XP + base + t * 4);
+            cp_async16(ps.b + t * 4, RHS + base + t * 4);
+        }
+        if (m.parent >= 0) {
+            hf[u] |= 64u;
+            if (t < 16) {
+                const int oct = meta_octant(m.packed);
+                cp_async16(ps.pblk + t * 4, Z + (size_t)m.parent * kTileCells + ((oct & 1) * 4 + (t >> 2)) * 64 +
+                                                (((oct >> 1) & 1) * 4 + (t & 3)) * 8 + ((oct >> 2) & 1) * 4);
             }
-            {
-                const int face = 4 + (t >> 6), c = t & 63;
-                const int nb = m.nb[face];
-                sh[g].hx[face * 64 + c] =
-                    nb >= 0 ? prolongated(tp, Z, XP, nb, tp.meta[nb], (c >> 3) * 64 + (c & 7) * 8 + (face == 4 ? 7 : 0), prolong_coeff)
-                            : 0.f;
+        }
+        if (ghost[u]) continue;  // a GHOST tile only takes the prolongation
+        if (t < 64) {
+            const int nb = m.nb[fface];
+            if (nb >= 0) {
+                const TileMeta nm = tp.meta[nb];
+                const bool ng = meta_type(nm.packed) & GHOST_T;
+                hf[u] |= 1u | (ng ? 2u : 0u);
+                const size_t nbase = (size_t)nb * kTileCells;
+                if (!ng) cp_async16(ps.hxp + fface * 64 + qq * 4, XP + nbase + foff);
+                cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + nbase + foff);
+                if (nm.parent >= 0) {
+                    hf[u] |= 4u;
+                    cp_async8(ps.hpar + (fface * 16 + qq) * 2, Z + (size_t)nm.parent * kTileCells + parent_cell(meta_octant(nm.packed), foff));
+                }
+            }
+        }
+        {
+            const int nb = m.nb[zface];
+            if (nb >= 0) {
+                const TileMeta nm = tp.meta[nb];
+                const bool ng = meta_type(nm.packed) & GHOST_T;
+                hf[u] |= 8u | (ng ? 16u : 0u);
+                const size_t nbase = (size_t)nb * kTileCells;
+                if (!ng) cp_async4(ps.hxp + zface * 64 + zc, XP + nbase + zoff);
+                ps.hmask[zface * 64 + zc] = tp.mask_mg[nbase + zoff];
+                if (nm.parent >= 0) {
+                    hf[u] |= 32u;
+                    cp_async4(ps.hpar + 128 + (zface - 4) * 64 + zc, Z + (size_t)nm.parent * kTileCells + parent_cell(meta_octant(nm.packed), zoff));
+                }
             }
         }
     }
+#pragma unroll
+    for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
+    cp_async_wait_all();
     __syncthreads();
-    if (!active) return;
-    V4<float> o = ld4(sh[g].xs + t * 4);
-    if (!ghost) {
-        const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_mg + (size_t)tile * kTileCells + t * 4);
-        const V4<float> b = ld4(RHS + (size_t)tile * kTileCells + t * 4);
-        const LevelConst<float> L = tile_level_const(tp, tile, meta_level(m.packed));
-        o = colour_update(sh[g].xs, sh[g].hx, t, mask4, (tp.fcls[tile] >> 12) & 0xfffu, L, b, 1);
+    // prolongated values of the tile and of its neighbours' first layer
+    const TileIdx ix(t);
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        if (!act[u]) continue;
+        ProStage& ps = st[u * TPB + g];
+        const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ps.mask + t * 4);
+        const bool par = hf[u] & 64u;
+        const float* pb = ps.pblk + (ix.i >> 1) * 16 + (ix.j >> 1) * 4 + (ix.k0 >> 1);
+        const float c0 = par ? pb[0] : 0.f, c1 = par ? pb[1] : 0.f;
+        const V4<float> xp = ghost[u] ? zero4<float>() : ld4(ps.xp + t * 4);
+        V4<float> o;
+#pragma unroll
+        for (int e = 0; e < 4; e++) o.v[e] = prolong_value((mask4 >> (8 * e)) & 0xffu, ghost[u], e < 2 ? c0 : c1, xp.v[e], prolong_coeff);
+        st4(ps.xs + t * 4, o);
+        if (ghost[u]) continue;
+        if (t < 64) {
+            V4<float> v = zero4<float>();
+            if (hf[u] & 1u) {
+                const bool ng = hf[u] & 2u;
+                const uint32_t nm4 = *reinterpret_cast<const uint32_t*>(ps.hmask + fface * 64 + qq * 4);
+                const float h0 = (hf[u] & 4u) ? ps.hpar[(fface * 16 + qq) * 2] : 0.f;
+                const float h1 = (hf[u] & 4u) ? ps.hpar[(fface * 16 + qq) * 2 + 1] : 0.f;
+                const V4<float> nxp = ng ? zero4<float>() : ld4(ps.hxp + fface * 64 + qq * 4);
+#pragma unroll
+                for (int e = 0; e < 4; e++) v.v[e] = prolong_value((nm4 >> (8 * e)) & 0xffu, ng, e < 2 ? h0 : h1, nxp.v[e], prolong_coeff);
+            }
+            st4(ps.hx + fface * 64 + qq * 4, v);
+        }
+        {
+            float v = 0.f;
+            if (hf[u] & 8u) {
+                const bool ng = hf[u] & 16u;
+                const float cx = (hf[u] & 32u) ? ps.hpar[128 + (zface - 4) * 64 + zc] : 0.f;
+                v = prolong_value(ps.hmask[zface * 64 + zc], ng, cx, ng ? 0.f : ps.hxp[zface * 64 + zc], prolong_coeff);
+            }
+            ps.hx[zface * 64 + zc] = v;
+        }
     }
-    st4(Z + (size_t)tile * kTileCells + t * 4, o);
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        if (!act[u]) continue;
+        ProStage& ps = st[u * TPB + g];
+        V4<float> o = ld4(ps.xs + t * 4);
+        if (!ghost[u]) {
+            const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
+            o = colour_update(ps.xs, ps.hx, t, *reinterpret_cast<const uint32_t*>(ps.mask + t * 4), (tp.fcls[tile[u]] >> 12) & 0xfffu, L,
+                              ld4(ps.b + t * 4), 1);
+        }
+        st4(Z + (size_t)tile[u] * kTileCells + t * 4, o);
+    }
 }
 
 // Right-hand sides of GHOST tiles to 0 (the V-cycle's initialisation of them, src/GMGSolver.cu:393-396).
@@ -486,13 +559,26 @@ void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const S
     }
 }
 
+template <int TPB, int NT>
+void prolong_shape(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
+                   cudaStream_t s) {
+    const int n = g.level_count[level];
+    const int per = TPB * NT;
+    launch_kernel(k_prolong_sweep<TPB, NT>, (n + per - 1) / per, 128 * TPB, sizeof(ProStage) * per, s, g.topo, g.level_first[level], n,
+                  Z, XP, RHS, prolong_coeff, S);
+}
+
 void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
                    cudaStream_t s) {
     const int n = g.level_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    launch_kernel(k_prolong_sweep<kTPB2>, (n + kTPB2 - 1) / kTPB2, 128 * kTPB2, 0, s, g.topo, g.level_first[level], n, Z, XP, RHS,
-                  prolong_coeff, S);
+    switch (g.shape(KS_PROLONG, level)) {
+    case 0: prolong_shape<2, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    case 1: prolong_shape<2, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    case 2: prolong_shape<1, 4>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    default: prolong_shape<1, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    }
 }
 
 void zero_ghost_tiles(const DevGrid& g, float* X, cudaStream_t s) {
@@ -532,6 +618,8 @@ bool bottom_supported(int coarsest_iters, int lb) {
 void init_kernel_attributes() {
     cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, kBottomSmemBudget);
     cudaFuncSetAttribute(k_presmooth<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PreStage) * 8);
+    cudaFuncSetAttribute(k_prolong_sweep<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ProStage) * 4);
+    cudaFuncSetAttribute(k_prolong_sweep<1, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ProStage) * 4);
 }
 
 }  // namespace launch

@@ -239,12 +239,14 @@ cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* par
 /* Solves every instance of a (batched) grid in one graph launch: one kernel per step for the whole
  * batch, per-instance CG scalars and stopping, the loop running until the last instance stops.
  * active (NULL = all): instances with 0 take no part and keep their channels; tolerances (NULL =
- * params->relative_tolerance): per-instance relative tolerance.  results: one per instance.  An
- * instance's result is bit-identical whatever else is in the batch (per-instance reductions
- * in a fixed order).  cirrus_gmg_solve on a batched grid solves all instances and reports
- * instance 0. */
+ * params->relative_tolerance): per-instance relative tolerance; pure_neumann (NULL =
+ * params->is_pure_neumann): per-instance projection of r to zero mean.  results: one per
+ * instance.  An instance's result is bit-identical whatever else is in the batch (per-instance
+ * reductions in a fixed order).  cirrus_gmg_solve on a batched grid solves all instances and
+ * reports instance 0. */
 cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_params* params, const int* active,
-                                     const double* tolerances, void* stream, cirrus_solve_result* results);
+                                     const double* tolerances, const int* pure_neumann, void* stream,
+                                     cirrus_solve_result* results);
 
 /* End-to-end variant for callers holding host arrays: copies b (num_tiles*512 floats, pinned or
  * pageable) to the device, solves, and copies x back into x_host. */
@@ -276,6 +278,16 @@ enum {
     CIRRUS_KERNEL_DOT = 6               /* whole-grid LEAF dot product                              */
 };
 cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int reps, void* stream);
+
+/* Launch shapes of the staged stencil kernels, as the autotuner sets them: kernel one of
+ * CIRRUS_KERNEL_LAPLACIAN / _GS_SWEEP / _PRESMOOTH / _PROLONG_SWEEP / _RESIDUAL_RESTRICT (or -1:
+ * all of them), level a level of the grid (or -1: all levels; the Laplacian has one entry,
+ * level 0), shape in [0, CIRRUS_NUM_LAUNCH_SHAPES).  Lets a caller reuse tuned shapes for grids
+ * of the same structure or pin one.  Shapes never change results.  No counterpart in the
+ * reference. */
+#define CIRRUS_NUM_LAUNCH_SHAPES 4
+cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape);
+cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int level, int* shape);
 
 /* FP64 true residual ||b - A x||/||b|| over INTERIOR cells of LEAF tiles for a given b (host,
  * num_tiles*512 floats) and the last solution (FP64 after a mixed-precision solve, else the

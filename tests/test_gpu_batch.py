@@ -7,7 +7,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from cirrus_b200 import DeviceGrid, GMGSolver, PRECISION_MIXED_FP64, workloads as W
+from cirrus_b200 import KERNEL_PROLONG_SWEEP, DeviceGrid, GMGSolver, PRECISION_MIXED_FP64, workloads as W
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -47,17 +47,10 @@ def test_batch_results_equal_alone(built_cache):
     for i, r in enumerate(rhs):
         g.set_channel_instance(i, 1, r)
     s = GMGSolver()
-    # per-instance pure-Neumann flags go through the shared parameter only when all agree; the
-    # mixed batch here is solved in two passes: Dirichlet instances, then the pure-Neumann one
-    act_d = [not p for p in pure]
-    res_d = s.solve_batch(g, active=act_d)
-    act_n = [bool(p) for p in pure]
-    for i, r in enumerate(rhs):
-        if act_n[i]:
-            g.set_channel_instance(i, 1, r)
-    res_n = s.solve_batch(g, active=act_n, is_pure_neumann=True)
+    # one launch for Dirichlet and pure-Neumann instances together (per-instance flags)
+    res = s.solve_batch(g, pure_neumann=pure)
     for i, b in enumerate(bs):
-        it, rel = (res_n if pure[i] else res_d)[i]
+        it, rel = res[i]
         ait, arel, ax = alone(b, rhs[i], GMGSolver(), pure[i])
         x = g.get_channel_instance(i, 0)
         print(f"{MIX[i]}: batch {it} iters {rel:.3e}; alone {ait} iters {arel:.3e}")
@@ -155,6 +148,30 @@ def test_autotune_changes_timing_not_results(built_cache):
     assert out[0][0] == out[1][0]
     for a, b in zip(out[0][1], out[1][1]):
         assert np.array_equal(bits(a), bits(b))
+    g.close()
+
+
+def test_every_launch_shape_gives_the_same_bits(built_cache):
+    """Each of the four launch shapes of the staged kernels (tiles per CTA x tiles in flight),
+    pinned for every kernel and level, gives the solve of the default shapes bit for bit."""
+    bs = [built_cache(n) for n in ["sphere64_small", "ring64_small"]]
+    rhs = [rhs_of(b) for b in bs]
+    g = DeviceGrid([b.topology for b in bs])
+    s = GMGSolver()
+    out = []
+    for shape in (None, 0, 1, 2, 3):
+        if shape is not None:
+            g.set_launch_shape(shape)
+            assert g.get_launch_shape(KERNEL_PROLONG_SWEEP, 1) == shape
+        for i, r in enumerate(rhs):
+            g.set_channel_instance(i, 1, r)
+            g.set_channel_instance(i, 0, np.zeros_like(r))
+        res = s.solve_batch(g)
+        out.append((res, [g.get_channel_instance(i, 0) for i in range(len(bs))]))
+    for res, xs in out[1:]:
+        assert res == out[0][0]
+        for a, b in zip(out[0][1], xs):
+            assert np.array_equal(bits(a), bits(b))
     g.close()
 
 
