@@ -81,7 +81,7 @@ int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
         if (l >= 1 && g.level_count[l] > 0 && g.bottom_level >= 0)
             pick(KS_PROLONG, l, [&] { launch::prolong_sweep(g, l, z, g.d_xpre, ap, 1.f, nullptr, s); });
     }
-    if (g.n_leafghost > 0) pick(KS_LAPLACIAN, 0, [&] { launch::laplacian_fused(g, p, tmp, nullptr, s); });
+    if (g.n_lapmain + g.n_lapitems > 0) pick(KS_LAPLACIAN, 0, [&] { launch::laplacian_fused(g, p, tmp, nullptr, s); });
     g.launch_count = count0;
     drop_graphs(g);
     const bool ok = cudaStreamSynchronize(s) == cudaSuccess;

@@ -187,7 +187,7 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
     }
 
     // ------------------------------------------------------------------ lists
-    std::vector<int> leaf, ghost, leafghost, mg;
+    std::vector<int> leaf, ghost, leafghost, mg, lapmain;
     std::vector<int> mg_off(num_layers, 0), mg_cnt(num_layers, 0), lfirst(num_layers, 0), lcnt(num_layers, 0);
     std::vector<int> inst_leaves(K, 0);
     std::vector<int64_t> inst_dof(K, 0);
@@ -289,10 +289,57 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
         CK(cudaMemcpy(g->d_ghost_tables, gslot.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(g->d_ghost_tables + n, gchild.data(), sizeof(int) * 8 * (size_t)n, cudaMemcpyHostToDevice));
         CK(cudaMalloc(&g->d_gacc, sizeof(float) * 64 * std::max<size_t>(ghost.size(), 1)));
+        CK(cudaMemset(g->d_gacc, 0, sizeof(float) * 64 * std::max<size_t>(ghost.size(), 1)));
+        // split of the fused Laplacian's GHOST tiles: a tile whose coupled cells (mask face bits)
+        // all lie on its faces, each coupled only across the tile faces it lies on, takes the
+        // face path with the set of those faces (none: its row stays 0); any other goes through
+        // the staged path with the LEAF tiles
+        std::vector<int4> lapitems;
+        int n_face = 0;
+        for (int t : leafghost) {
+            if (!(type[t] & GHOST_T)) {
+                lapmain.push_back(t);
+                continue;
+            }
+            uint32_t faces = 0;
+            bool outward = true;
+            for (int o = 0; o < kTileCells && outward; o++) {
+                const uint32_t bits = mlap[(size_t)t * kTileCells + o] & 0x3Fu;
+                const int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                const uint32_t on = (i == 0 ? 1u : 0u) | (i == 7 ? 2u : 0u) | (j == 0 ? 4u : 0u) | (j == 7 ? 8u : 0u) |
+                                    (k == 0 ? 16u : 0u) | (k == 7 ? 32u : 0u);
+                if (bits & ~on) outward = false;
+                faces |= bits;
+            }
+            if (!outward) {
+                lapmain.push_back(t);
+            } else if (faces) {
+                n_face++;
+                const int cf = (int)(faces | ((fcls[t] & 0xfffu) << 6)), lc = g_inst[t] * kLevelSlots + level[t];
+                for (int c = 0; c < 64; c++) {
+                    // coarse cell c covers fine cells 2*(c/16).., 2*((c/4)%4).., 2*(c%4)..
+                    const int ci = c / 16, cj = (c / 4) % 4, ck = c % 4;
+                    const uint32_t touch = (ci == 0 ? 1u : 0u) | (ci == 3 ? 2u : 0u) | (cj == 0 ? 4u : 0u) | (cj == 3 ? 8u : 0u) |
+                                           (ck == 0 ? 16u : 0u) | (ck == 3 ? 32u : 0u);
+                    if (touch & faces) lapitems.push_back(make_int4(t, (gslot[t] << 6) | c, cf, lc));
+                }
+            }
+        }
+        g->n_lapface = n_face;
+        g->n_lapitems = (int)lapitems.size();
+        if (!lapitems.empty()) {
+            if (ghost.size() >= (1u << 25)) {
+                if (err) *err = "too many GHOST tiles";
+                grid_destroy(g);
+                return 1;
+            }
+            CK(cudaMalloc(&g->d_lapitems, sizeof(int4) * lapitems.size()));
+            CK(cudaMemcpy(g->d_lapitems, lapitems.data(), sizeof(int4) * lapitems.size(), cudaMemcpyHostToDevice));
+        }
         CK(cudaMalloc(&g->d_xpre, sizeof(float) * kTileCells * (size_t)n));
         CK(cudaMemset(g->d_xpre, 0, sizeof(float) * kTileCells * (size_t)n));  // GHOST tiles stay 0
     }
-    const size_t nl = leaf.size() + ghost.size() + leafghost.size() + mg.size() + 1;
+    const size_t nl = leaf.size() + ghost.size() + leafghost.size() + mg.size() + lapmain.size() + 1;
     CK(cudaMalloc(&g->d_lists, sizeof(int) * nl));
     std::vector<int> lists;
     lists.reserve(nl);
@@ -300,12 +347,15 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
     lists.insert(lists.end(), ghost.begin(), ghost.end());
     lists.insert(lists.end(), leafghost.begin(), leafghost.end());
     lists.insert(lists.end(), mg.begin(), mg.end());
+    lists.insert(lists.end(), lapmain.begin(), lapmain.end());
     lists.push_back(0);
     CK(cudaMemcpy(g->d_lists, lists.data(), sizeof(int) * lists.size(), cudaMemcpyHostToDevice));
     g->d_leaf = g->d_lists;
     g->d_ghost = g->d_leaf + leaf.size();
     g->d_leafghost = g->d_ghost + ghost.size();
     g->d_mg = g->d_leafghost + leafghost.size();
+    g->d_lapmain = g->d_mg + mg.size();
+    g->n_lapmain = (int)lapmain.size();
 
     // ------------------------------------------------------------------ coarse-level boxes
     // Levels handled by the shared-memory kernel, one CTA per instance: the longest prefix of
@@ -473,6 +523,7 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_lconst);
     cudaFree(g->d_ghost_tables);
     cudaFree(g->d_gacc);
+    cudaFree(g->d_lapitems);
     cudaFree(g->d_xpre);
     cudaFree(g->d_bottom_tiles);
     cudaFree(g->d_bottom_code);

@@ -68,16 +68,107 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __r
     st4(Y + (size_t)tile * kTileCells + t * 4, o);
 }
 
+// Face path of the fused Laplacian: one coarse cell of a GHOST tile whose coupled cells all lie
+// on its faces and couple only outward.  Item: tile, ghost slot << 6 | coarse cell c, coupled
+// faces | face classes << 6, level-constant index.  Forms the cell's partial sum -- its 2x2x2
+// block of A p values in AccumulateToParents128's (ii,jj,kk) order -- computing A p only on
+// cells with coupled faces, each term from the neighbour's value across the face.  Every other
+// cell's A p is +0 in the full path, which also adds the zero-coefficient terms skipped here (as
+// +-0, which leaves finite sums unchanged).  All loads are issued before the arithmetic: the
+// block's own values, mask and type bytes (four 2-cell runs along k), then the neighbour values
+// across each coupled face it touches.
+__device__ __forceinline__ void ghost_face_sum(const Topo& tp, const float* __restrict__ X, int4 it, float* __restrict__ GACC) {
+    const int tile = it.x, c = it.y & 63;
+    const uint32_t faces = (uint32_t)it.z & 63u, cls = (uint32_t)it.z >> 6;
+    const int fi = c / 16 * 2, fj = (c / 4) % 4 * 2, fk = c % 4 * 2;
+    const size_t base = (size_t)tile * kTileCells;
+    const int o0 = fi * 64 + fj * 8 + fk;
+    float2 xo[4];
+    uint32_t mk[4], ck[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int o = o0 + (q >> 1) * 64 + (q & 1) * 8;
+        xo[q] = *reinterpret_cast<const float2*>(X + base + o);
+        mk[q] = *reinterpret_cast<const uint16_t*>(tp.mask_lap + base + o);
+        ck[q] = *reinterpret_cast<const uint16_t*>(tp.ctype + base + o);
+    }
+    const uint32_t touch = (fi == 0 ? 1u : 0u) | (fi == 6 ? 2u : 0u) | (fj == 0 ? 4u : 0u) | (fj == 6 ? 8u : 0u) | (fk == 0 ? 16u : 0u) |
+                           (fk == 6 ? 32u : 0u);
+    const uint32_t act = touch & faces;
+    const TileMeta& m = tp.meta[tile];
+    // nv[f][a*2+b]: the neighbour's value across face f for the block's cell (a, b) on that face,
+    // (a, b) = (jj, kk) on x faces, (ii, kk) on y faces, (ii, jj) on z faces
+    float nv[6][4];
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        const int nb = ((act >> f) & 1u) ? m.nb[f] : -1;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int a = q >> 1, b = q & 1;
+            int noff;
+            if (f == 0) noff = 7 * 64 + (fj + a) * 8 + fk + b;
+            else if (f == 1) noff = (fj + a) * 8 + fk + b;
+            else if (f == 2) noff = (fi + a) * 64 + 7 * 8 + fk + b;
+            else if (f == 3) noff = (fi + a) * 64 + fk + b;
+            else if (f == 4) noff = (fi + a) * 64 + (fj + b) * 8 + 7;
+            else noff = (fi + a) * 64 + (fj + b) * 8;
+            nv[f][q] = nb >= 0 ? X[(size_t)nb * kTileCells + noff] : 0.f;
+        }
+    }
+    const LevelConst<float> L(tp.lconst[it.w]);
+    float sum = 0.f;
+#pragma unroll
+    for (int ii = 0; ii < 2; ii++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int kk = 0; kk < 2; kk++) {
+                const int i = fi + ii, j = fj + jj, k = fk + kk;
+                const uint32_t on = (i == 0 ? 1u : 0u) | (i == 7 ? 2u : 0u) | (j == 0 ? 4u : 0u) | (j == 7 ? 8u : 0u) |
+                                    (k == 0 ? 16u : 0u) | (k == 7 ? 32u : 0u);
+                const int q = ii * 2 + jj;
+                const uint32_t mm = (mk[q] >> (8 * kk)) & 0xffu;
+                float v = 0.f;
+                if ((on & act) && (mm & 0x3Fu)) {
+                    const float x0 = kk ? xo[q].y : xo[q].x;
+                    float s = 0.f;
+#pragma unroll
+                    for (int f = 0; f < 6; f++) {
+                        if (!(mm & (1u << f))) continue;
+                        const float a = ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1;
+                        const float xf = nv[f][f < 2 ? jj * 2 + kk : (f < 4 ? ii * 2 + kk : ii * 2 + jj)];
+                        s = __fadd_rn(s, __fmul_rn(a, x0 - xf));
+                    }
+                    const float out = (mm & kMaskInterior) ? mul_h3(s, L.h) : 0.f;
+                    v = (((ck[q] >> (8 * kk)) & 0xffu) & (INTERIOR_C | DIRICHLET_C | NEUMANN_C)) ? out : 0.f;
+                }
+                sum += v;
+            }
+    GACC[(size_t)(it.y >> 6) * 64 + c] = sum;
+}
+
 // FullNegativeLaplacian in one launch over LEAF|GHOST tiles.  p on GHOST tiles is kept valid by
 // the kernels that write p (push_to_ghost_child), so no propagation pass runs; LEAF tiles write
 // A p; GHOST tiles write the 2x2x2 child sums of their A p (AccumulateToParents128's order) to a
-// per-ghost row, added to the parent's A p by the p.Ap reduction that follows.  Tiles are staged
-// with asynchronous copies, NT per 128-thread group.
+// per-ghost row, added to the parent's A p by the p.Ap reduction that follows.  The first
+// item_blocks CTAs take the face path, one thread per item of `items` (a coarse cell touching a
+// coupled face of a face-path GHOST tile); the others take `list` (LEAF tiles and GHOST tiles
+// coupled inside), staged with asynchronous copies, NT per 128-thread group.  Row entries in
+// neither are constant zeros (set when the grid is created).
 template <int TPB, int NT>
-__global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ X,
-                                                               float* __restrict__ Y, float* __restrict__ GACC,
-                                                               const Scalars* __restrict__ S) {
+__global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
+                                                               int nitems, int item_blocks,
+                                                               const float* __restrict__ X, float* __restrict__ Y,
+                                                               float* __restrict__ GACC, const Scalars* __restrict__ S) {
     pdl_entry();
+    if ((int)blockIdx.x < item_blocks) {
+        const int q = (int)blockIdx.x * (128 * TPB) + (int)threadIdx.x;
+        if (q >= nitems) return;
+        const int4 it = items[q];
+        if (S != nullptr && S[it.w / kLevelSlots].done) return;
+        ghost_face_sum(tp, X, it, GACC);
+        return;
+    }
     extern __shared__ __align__(16) unsigned char lap_smem[];
     TileStage* st = reinterpret_cast<TileStage*>(lap_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
@@ -85,7 +176,7 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const in
     bool act[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
-        const int q = (blockIdx.x * NT + u) * TPB + g;
+        const int q = (((int)blockIdx.x - item_blocks) * NT + u) * TPB + g;
         tile[u] = q < n ? list[q] : 0;
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
@@ -836,12 +927,13 @@ template void full_laplacian<double>(const DevGrid&, double*, double*, const Sca
 template <int TPB, int NT>
 void laplacian_shape(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s) {
     const int per = TPB * NT;
-    launch_kernel(k_laplacian_fused<TPB, NT>, (g.n_leafghost + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
-                  g.d_leafghost, g.n_leafghost, X, Y, g.d_gacc, S);
+    const int item_blocks = (g.n_lapitems + 128 * TPB - 1) / (128 * TPB);
+    launch_kernel(k_laplacian_fused<TPB, NT>, item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
+                  g.topo, g.d_lapmain, g.n_lapmain, g.d_lapitems, g.n_lapitems, item_blocks, X, Y, g.d_gacc, S);
 }
 
 void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s) {
-    if (g.n_leafghost == 0) return;
+    if (g.n_lapmain + g.n_lapitems == 0) return;
     ++g.launch_count;
     switch (g.shape(KS_LAPLACIAN, 0)) {
     case 0: laplacian_shape<2, 1>(g, X, Y, S, s); break;

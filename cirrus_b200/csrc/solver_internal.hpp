@@ -100,6 +100,13 @@ struct DevGrid {
     const int* d_leafghost = nullptr;
     const int* d_mg = nullptr;
     int n_leaf = 0, n_ghost = 0, n_leafghost = 0;
+    // fused Laplacian: LEAF tiles + GHOST tiles coupled inside (staged path); GHOST tiles coupled
+    // only outward across their faces (face path): per coarse cell touching a coupled face an
+    // item (tile, ghost slot << 6 | cell, coupled faces | face classes << 6, level-constant index)
+    const int* d_lapmain = nullptr;
+    int n_lapmain = 0;
+    int4* d_lapitems = nullptr;
+    int n_lapface = 0, n_lapitems = 0;
     std::vector<int> mg_offset, mg_count, level_first, level_count;
     std::vector<uint8_t> h_tile_type;
     std::vector<uint8_t> shapes;  // KS_COUNT x num_layers launch-shape choices
