@@ -180,9 +180,11 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const in
         tile[u] = q < n ? list[q] : 0;
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
+    TilePre pre[NT];
+    tile_pre(tp, tile, t, pre);
 #pragma unroll
     for (int u = 0; u < NT; u++)
-        if (act[u]) stage_async(X, nullptr, tp.mask_lap, tile[u], halo_nb(tp.meta, tile[u], t), t, st[u * TPB + g]);
+        if (act[u]) stage_async(X, nullptr, tp.mask_lap, tile[u], pre[u].nb, t, st[u * TPB + g]);
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
@@ -193,12 +195,11 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const in
         ghost[u] = false;
         if (!act[u]) continue;
         TileStage& ts = st[u * TPB + g];
-        const int packed = tp.meta[tile[u]].packed;
-        ghost[u] = meta_type(packed) & GHOST_T;
-        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(packed));
+        ghost[u] = meta_type(pre[u].packed) & GHOST_T;
+        const LevelConst<float> L(pre[u].lc);
         float out[4], dg[4];
-        neg_lap4<float, false, false>(ts.xs, ts.hx, t, *reinterpret_cast<const uint32_t*>(ts.mask + t * 4), tp.fcls[tile[u]] & 0xfffu,
-                                      L, out, dg);
+        neg_lap4<float, false, false>(ts.xs, ts.hx, t, *reinterpret_cast<const uint32_t*>(ts.mask + t * 4), pre[u].fcls & 0xfffu, L,
+                                      out, dg);
         if (ghost[u]) {
             const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + (size_t)tile[u] * kTileCells + t * 4);
 #pragma unroll
@@ -279,9 +280,11 @@ __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __re
         tile[u] = q < n ? list[q] : 0;
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
+    TilePre pre[NT];
+    tile_pre(tp, tile, t, pre);
 #pragma unroll
     for (int u = 0; u < NT; u++)
-        if (act[u]) stage_async(X, R, tp.mask_mg, tile[u], halo_nb(tp.meta, tile[u], t), t, st[u * TPB + g]);
+        if (act[u]) stage_async(X, R, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
@@ -290,10 +293,10 @@ __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __re
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         const TileStage& ts = st[u * TPB + g];
-        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
+        const LevelConst<float> L(pre[u].lc);
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ts.mask + t * 4);
         st4(X + (size_t)tile[u] * kTileCells + t * 4,
-            colour_update(ts.xs, ts.hx, t, mask4, (tp.fcls[tile[u]] >> 12) & 0xfffu, L, ld4(ts.b + t * 4), color));
+            colour_update(ts.xs, ts.hx, t, mask4, (pre[u].fcls >> 12) & 0xfffu, L, ld4(ts.b + t * 4), color));
     }
 }
 
@@ -351,9 +354,11 @@ __global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int fi
         tile[u] = first + (q < n ? q : 0);
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
+    TilePre pre[NT];
+    tile_pre(tp, tile, t, pre);
 #pragma unroll
     for (int u = 0; u < NT; u++)
-        if (act[u]) stage_async(X, RHS, tp.mask_mg, tile[u], halo_nb(tp.meta, tile[u], t), t, st[u * TPB + g]);
+        if (act[u]) stage_async(X, RHS, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
@@ -362,10 +367,10 @@ __global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int fi
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         TileStage& ts = st[u * TPB + g];
-        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
+        const LevelConst<float> L(pre[u].lc);
         float ax[4], d[4];
-        neg_lap4<float, false>(ts.xs, ts.hx, t, *reinterpret_cast<const uint32_t*>(ts.mask + t * 4),
-                               (tp.fcls[tile[u]] >> 12) & 0xfffu, L, ax, d);
+        neg_lap4<float, false>(ts.xs, ts.hx, t, *reinterpret_cast<const uint32_t*>(ts.mask + t * 4), (pre[u].fcls >> 12) & 0xfffu, L,
+                               ax, d);
         const V4<float> b = ld4(ts.b + t * 4);
         V4<float> r;
 #pragma unroll

@@ -288,6 +288,31 @@ __device__ __forceinline__ HaloNb halo_nb(const TileMeta* __restrict__ meta, int
     return h;
 }
 
+// Per-tile values a staged kernel needs besides the copied data: halo neighbours, packed
+// metadata, face classes and level constants.  Loaded for all of a group's tiles before any copy
+// is issued -- the copies are asm statements with a memory clobber, so loads written after one
+// are not moved ahead of it, and a load per tile between the copies would cost one memory round
+// trip per tile.
+struct TilePre {
+    HaloNb nb;
+    int packed;
+    uint32_t fcls;
+    float4 lc;
+};
+template <int NT>
+__device__ __forceinline__ void tile_pre(const Topo& tp, const int (&tile)[NT], int t, TilePre (&pre)[NT]) {
+    int inst[NT];
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        pre[u].nb = halo_nb(tp.meta, tile[u], t);
+        pre[u].packed = tp.meta[tile[u]].packed;
+        pre[u].fcls = tp.fcls[tile[u]];
+        inst[u] = tp.inst[tile[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < NT; u++) pre[u].lc = tp.lconst[inst[u] * kLevelSlots + meta_level(pre[u].packed)];
+}
+
 // Issue the copies of `tile` into st: channel X's values and face halos (0 for absent
 // neighbours), channel B (if given) and the mask bytes (if given).  Completed by
 // cp_async_wait_all + __syncthreads.

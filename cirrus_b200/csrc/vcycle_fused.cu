@@ -90,42 +90,53 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
     // neighbour of this thread's x/y-face piece (t < 64) and z-face cell; GHOST neighbours count
-    // as absent (their x is 0 on the way down)
-    int nbf[NT], nbz[NT];
+    // as absent (their x is 0 on the way down).  Metadata of all NT tiles is loaded before any
+    // copy is issued (see TilePre).
+    const int fface = t >> 4, qq = t & 15;
+    int foff;
+    if (fface == 0) foff = 448 + qq * 4;
+    else if (fface == 1) foff = qq * 4;
+    else if (fface == 2) foff = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
+    else foff = (qq >> 1) * 64 + (qq & 1) * 4;
+    const int zface = 4 + (t >> 6), zc = t & 63;
+    const int zoff = (zc >> 3) * 64 + (zc & 7) * 8 + (zface == 4 ? 7 : 0);
+    int nbf[NT], nbz[NT], inst[NT];
+    int packed[NT];
+    uint32_t fc[NT], nfc_f[NT], nfc_z[NT], zmb[NT];
+    float4 lc[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
-        nbf[u] = nbz[u] = -1;
+        const TileMeta& m = tp.meta[tile[u]];
+        packed[u] = m.packed;
+        const int nf = t < 64 ? m.nb[fface] : -1, nz = m.nb[zface];
+        nbf[u] = (act[u] && nf >= 0 && !meta_nb_ghost(m.packed, fface)) ? nf : -1;
+        nbz[u] = (act[u] && nz >= 0 && !meta_nb_ghost(m.packed, zface)) ? nz : -1;
+        fc[u] = tp.fcls[tile[u]];
+        inst[u] = tp.inst[tile[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        lc[u] = tp.lconst[inst[u] * kLevelSlots + meta_level(packed[u])];
+        nfc_f[u] = nbf[u] >= 0 ? tp.fcls[nbf[u]] : 0u;
+        nfc_z[u] = nbz[u] >= 0 ? tp.fcls[nbz[u]] : 0u;
+        zmb[u] = nbz[u] >= 0 ? tp.mask_mg[(size_t)nbz[u] * kTileCells + zoff] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         PreStage& ps = st[u * TPB + g];
-        const TileMeta& m = tp.meta[tile[u]];
         const size_t base = (size_t)tile[u] * kTileCells;
         cp_async16(ps.b + t * 4, RHS + base + t * 4);
         if (t < 32) cp_async16(ps.mask + t * 16, tp.mask_mg + base + t * 16);
-        if (t < 64) {
-            const int face = t >> 4, qq = t & 15;
-            int off;
-            if (face == 0) off = 448 + qq * 4;
-            else if (face == 1) off = qq * 4;
-            else if (face == 2) off = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
-            else off = (qq >> 1) * 64 + (qq & 1) * 4;
-            const int nb = m.nb[face];
-            if (nb >= 0 && !meta_nb_ghost(m.packed, face)) {
-                nbf[u] = nb;
-                cp_async16(ps.hx + face * 64 + qq * 4, RHS + (size_t)nb * kTileCells + off);
-                cp_async4(ps.hmask + face * 64 + qq * 4, tp.mask_mg + (size_t)nb * kTileCells + off);
-            }
+        if (nbf[u] >= 0) {
+            cp_async16(ps.hx + fface * 64 + qq * 4, RHS + (size_t)nbf[u] * kTileCells + foff);
+            cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + (size_t)nbf[u] * kTileCells + foff);
         }
-        {
-            const int face = 4 + (t >> 6), c = t & 63;
-            const int nb = m.nb[face];
-            if (nb >= 0 && !meta_nb_ghost(m.packed, face)) {
-                nbz[u] = nb;
-                const int off = (c >> 3) * 64 + (c & 7) * 8 + (face == 4 ? 7 : 0);
-                cp_async4(ps.hx + face * 64 + c, RHS + (size_t)nb * kTileCells + off);
-                ps.hmask[face * 64 + c] = tp.mask_mg[(size_t)nb * kTileCells + off];
-            }
-        }
+        if (nbz[u] >= 0) cp_async4(ps.hx + zface * 64 + zc, RHS + (size_t)nbz[u] * kTileCells + zoff);
     }
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (nbz[u] >= 0) st[u * TPB + g].hmask[zface * 64 + zc] = (uint8_t)zmb[u];
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
@@ -135,8 +146,8 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         PreStage& ps = st[u * TPB + g];
-        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
-        const uint32_t cls = (tp.fcls[tile[u]] >> 12) & 0xfffu;
+        const LevelConst<float> L(lc[u]);
+        const uint32_t cls = (fc[u] >> 12) & 0xfffu;
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ps.mask + t * 4);
         const V4<float> b = ld4(ps.b + t * 4);
         V4<float> x1;
@@ -150,18 +161,13 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
         }
         st4(ps.xs + t * 4, x1);
         if (t < 64) {
-            const int face = t >> 4, qq = t & 15;
+            const int face = fface;
             V4<float> v = zero4<float>();
             if (nbf[u] >= 0) {
                 const V4<float> nbb = ld4(ps.hx + face * 64 + qq * 4);
                 const uint32_t nm4 = *reinterpret_cast<const uint32_t*>(ps.hmask + face * 64 + qq * 4);
-                const uint32_t ncls = (tp.fcls[nbf[u]] >> 12) & 0xfffu;
-                int off;
-                if (face == 0) off = 448 + qq * 4;
-                else if (face == 1) off = qq * 4;
-                else if (face == 2) off = (qq >> 1) * 64 + 56 + (qq & 1) * 4;
-                else off = (qq >> 1) * 64 + (qq & 1) * 4;
-                const int ni = off >> 6, nj = (off >> 3) & 7, nk0 = off & 7;
+                const uint32_t ncls = (nfc_f[u] >> 12) & 0xfffu;
+                const int ni = foff >> 6, nj = (foff >> 3) & 7, nk0 = foff & 7;
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
                     const uint32_t mm = (nm4 >> (8 * e)) & 0xffu;
@@ -172,14 +178,14 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
             st4(ps.hx + face * 64 + qq * 4, v);
         }
         {
-            const int face = 4 + (t >> 6), c = t & 63;
+            const int face = zface, c = zc;
             float v = 0.f;
             if (nbz[u] >= 0) {
                 int i, j, k;
                 halo_cell_ijk(face, c, i, j, k);
                 const uint32_t mm = ps.hmask[face * 64 + c];
                 if (((i + j + k) & 1) == 0 && (mm & kMaskInterior))
-                    v = 0.f + (ps.hx[face * 64 + c] - 0.f) / cell_diag(i, j, k, mm, (tp.fcls[nbz[u]] >> 12) & 0xfffu, L);
+                    v = 0.f + (ps.hx[face * 64 + c] - 0.f) / cell_diag(i, j, k, mm, (nfc_z[u] >> 12) & 0xfffu, L);
             }
             ps.hx[face * 64 + c] = v;
         }
@@ -190,10 +196,9 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         PreStage& ps = st[u * TPB + g];
-        const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
         st4(XP + (size_t)tile[u] * kTileCells + t * 4,
-            colour_update(ps.xs, ps.hx, t, *reinterpret_cast<const uint32_t*>(ps.mask + t * 4), (tp.fcls[tile[u]] >> 12) & 0xfffu, L,
-                          ld4(ps.b + t * 4), 1));
+            colour_update(ps.xs, ps.hx, t, *reinterpret_cast<const uint32_t*>(ps.mask + t * 4), (fc[u] >> 12) & 0xfffu,
+                          LevelConst<float>(lc[u]), ld4(ps.b + t * 4), 1));
     }
 }
 
@@ -245,64 +250,85 @@ __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first,
     const int zoff = (zc >> 3) * 64 + (zc & 7) * 8 + (zface == 4 ? 7 : 0);
     int tile[NT];
     bool act[NT], ghost[NT];
-    uint32_t hf[NT];  // bits: 0 f-neighbour, 1 f ghost, 2 f has parent, 3 z-neighbour, 4 z ghost, 5 z has parent, 6 own parent
+    // hf bits: 0 f-neighbour, 1 f ghost, 2 f has parent, 3 z-neighbour, 4 z ghost, 5 z has parent,
+    // 6 own parent, 8-10 / 11-13 the f / z neighbour's octant
+    uint32_t hf[NT];
+    // metadata of all NT tiles and of their neighbours first, then the copies (see TilePre)
+    int packed[NT], parent[NT], nbf[NT], nbz[NT], inst[NT], fpar[NT], zpar[NT];
+    uint32_t fc[NT], zmb[NT];
+    float4 lc[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         const int q = (blockIdx.x * NT + u) * TPB + g;
         tile[u] = first + (q < n ? q : 0);
         act[u] = q < n;  // finished instances are dropped after the copies are issued
-        ghost[u] = false;
-        hf[u] = 0;
+        const TileMeta& m = tp.meta[tile[u]];
+        packed[u] = m.packed;
+        parent[u] = m.parent;
+        nbf[u] = t < 64 ? m.nb[fface] : -1;
+        nbz[u] = m.nb[zface];
+        fc[u] = tp.fcls[tile[u]];
+        inst[u] = tp.inst[tile[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        ghost[u] = meta_type(packed[u]) & GHOST_T;
+        lc[u] = tp.lconst[inst[u] * kLevelSlots + meta_level(packed[u])];
+        hf[u] = parent[u] >= 0 ? 64u : 0u;
+        if (!act[u] || ghost[u]) nbf[u] = nbz[u] = -1;  // a GHOST tile only takes the prolongation
+        fpar[u] = zpar[u] = -1;
+        zmb[u] = 0;
+        if (nbf[u] >= 0) {
+            const TileMeta& nm = tp.meta[nbf[u]];
+            const int np = nm.packed;
+            hf[u] |= 1u | ((meta_type(np) & GHOST_T) ? 2u : 0u);
+            if (nm.parent >= 0) {
+                hf[u] |= 4u | ((uint32_t)meta_octant(np) << 8);
+                fpar[u] = nm.parent;
+            }
+        }
+        if (nbz[u] >= 0) {
+            const TileMeta& nm = tp.meta[nbz[u]];
+            const int np = nm.packed;
+            hf[u] |= 8u | ((meta_type(np) & GHOST_T) ? 16u : 0u);
+            if (nm.parent >= 0) {
+                hf[u] |= 32u | ((uint32_t)meta_octant(np) << 11);
+                zpar[u] = nm.parent;
+            }
+            zmb[u] = tp.mask_mg[(size_t)nbz[u] * kTileCells + zoff];
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
         ProStage& ps = st[u * TPB + g];
-        const TileMeta& m = tp.meta[tile[u]];
-        ghost[u] = meta_type(m.packed) & GHOST_T;
         const size_t base = (size_t)tile[u] * kTileCells;
         if (t < 32) cp_async16(ps.mask + t * 16, tp.mask_mg + base + t * 16);
         if (!ghost[u]) {
             cp_async16(ps.xp + t * 4, XP + base + t * 4);
             cp_async16(ps.b + t * 4, RHS + base + t * 4);
         }
-        if (m.parent >= 0) {
-            hf[u] |= 64u;
-            if (t < 16) {
-                const int oct = meta_octant(m.packed);
-                cp_async16(ps.pblk + t * 4, Z + (size_t)m.parent * kTileCells + ((oct & 1) * 4 + (t >> 2)) * 64 +
-                                                (((oct >> 1) & 1) * 4 + (t & 3)) * 8 + ((oct >> 2) & 1) * 4);
-            }
+        if (parent[u] >= 0 && t < 16) {
+            const int oct = meta_octant(packed[u]);
+            cp_async16(ps.pblk + t * 4, Z + (size_t)parent[u] * kTileCells + ((oct & 1) * 4 + (t >> 2)) * 64 +
+                                            (((oct >> 1) & 1) * 4 + (t & 3)) * 8 + ((oct >> 2) & 1) * 4);
         }
-        if (ghost[u]) continue;  // a GHOST tile only takes the prolongation
-        if (t < 64) {
-            const int nb = m.nb[fface];
-            if (nb >= 0) {
-                const TileMeta nm = tp.meta[nb];
-                const bool ng = meta_type(nm.packed) & GHOST_T;
-                hf[u] |= 1u | (ng ? 2u : 0u);
-                const size_t nbase = (size_t)nb * kTileCells;
-                if (!ng) cp_async16(ps.hxp + fface * 64 + qq * 4, XP + nbase + foff);
-                cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + nbase + foff);
-                if (nm.parent >= 0) {
-                    hf[u] |= 4u;
-                    cp_async8(ps.hpar + (fface * 16 + qq) * 2, Z + (size_t)nm.parent * kTileCells + parent_cell(meta_octant(nm.packed), foff));
-                }
-            }
+        if (nbf[u] >= 0) {
+            const size_t nbase = (size_t)nbf[u] * kTileCells;
+            if (!(hf[u] & 2u)) cp_async16(ps.hxp + fface * 64 + qq * 4, XP + nbase + foff);
+            cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + nbase + foff);
+            if (fpar[u] >= 0)
+                cp_async8(ps.hpar + (fface * 16 + qq) * 2, Z + (size_t)fpar[u] * kTileCells + parent_cell((hf[u] >> 8) & 7u, foff));
         }
-        {
-            const int nb = m.nb[zface];
-            if (nb >= 0) {
-                const TileMeta nm = tp.meta[nb];
-                const bool ng = meta_type(nm.packed) & GHOST_T;
-                hf[u] |= 8u | (ng ? 16u : 0u);
-                const size_t nbase = (size_t)nb * kTileCells;
-                if (!ng) cp_async4(ps.hxp + zface * 64 + zc, XP + nbase + zoff);
-                ps.hmask[zface * 64 + zc] = tp.mask_mg[nbase + zoff];
-                if (nm.parent >= 0) {
-                    hf[u] |= 32u;
-                    cp_async4(ps.hpar + 128 + (zface - 4) * 64 + zc, Z + (size_t)nm.parent * kTileCells + parent_cell(meta_octant(nm.packed), zoff));
-                }
-            }
+        if (nbz[u] >= 0) {
+            if (!(hf[u] & 16u)) cp_async4(ps.hxp + zface * 64 + zc, XP + (size_t)nbz[u] * kTileCells + zoff);
+            if (zpar[u] >= 0)
+                cp_async4(ps.hpar + 128 + (zface - 4) * 64 + zc, Z + (size_t)zpar[u] * kTileCells + parent_cell((hf[u] >> 11) & 7u, zoff));
         }
     }
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (nbz[u] >= 0) st[u * TPB + g].hmask[zface * 64 + zc] = (uint8_t)zmb[u];
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
@@ -352,11 +378,9 @@ __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first,
         if (!act[u]) continue;
         ProStage& ps = st[u * TPB + g];
         V4<float> o = ld4(ps.xs + t * 4);
-        if (!ghost[u]) {
-            const LevelConst<float> L = tile_level_const(tp, tile[u], meta_level(tp.meta[tile[u]].packed));
-            o = colour_update(ps.xs, ps.hx, t, *reinterpret_cast<const uint32_t*>(ps.mask + t * 4), (tp.fcls[tile[u]] >> 12) & 0xfffu, L,
-                              ld4(ps.b + t * 4), 1);
-        }
+        if (!ghost[u])
+            o = colour_update(ps.xs, ps.hx, t, *reinterpret_cast<const uint32_t*>(ps.mask + t * 4), (fc[u] >> 12) & 0xfffu,
+                              LevelConst<float>(lc[u]), ld4(ps.b + t * 4), 1);
         st4(Z + (size_t)tile[u] * kTileCells + t * 4, o);
     }
 }
