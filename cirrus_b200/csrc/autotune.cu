@@ -77,7 +77,7 @@ int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
         if (g.mg_count[l] > 0 && g.bottom_level >= 0)
             pick(KS_PRESMOOTH, l, [&] { launch::presmooth(g, l, g.d_xpre, ap, nullptr, s); });
         if (l >= 1 && g.level_count[l] > 0)
-            pick(KS_RESIDUAL, l, [&] { launch::residual_restrict(g, l, g.d_xpre, ap, tmp, 1.f, nullptr, s); });
+            pick(KS_RESIDUAL, l, [&] { launch::residual_restrict(g, l, g.d_xpre, ap, tmp, 1.f, nullptr, s, true); });
         if (l >= 1 && g.level_count[l] > 0 && g.bottom_level >= 0)
             pick(KS_PROLONG, l, [&] { launch::prolong_sweep(g, l, z, g.d_xpre, ap, 1.f, nullptr, s); });
     }

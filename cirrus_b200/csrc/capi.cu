@@ -558,7 +558,7 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
         case CIRRUS_KERNEL_GS_SWEEP: cirrus::launch::gs_sweep(g, level, z, ap, i & 1, nullptr, s); break;
         case CIRRUS_KERNEL_PRESMOOTH: cirrus::launch::presmooth(g, level, g.d_xpre, ap, nullptr, s); break;
         case CIRRUS_KERNEL_PROLONG_SWEEP: cirrus::launch::prolong_sweep(g, level, z, g.d_xpre, ap, 1.f, nullptr, s); break;
-        case CIRRUS_KERNEL_RESIDUAL_RESTRICT: cirrus::launch::residual_restrict(g, level, g.d_xpre, ap, tmp, 1.f, nullptr, s); break;
+        case CIRRUS_KERNEL_RESIDUAL_RESTRICT: cirrus::launch::residual_restrict(g, level, g.d_xpre, ap, tmp, 1.f, nullptr, s, true); break;
         case CIRRUS_KERNEL_COARSE: cirrus::launch::bottom(g, g.bottom_level, 10, z, ap, 1.f, 1.f, nullptr, s); break;
         case CIRRUS_KERNEL_DOT: cirrus::launch::grid_dot(g, p, z, s); break;
         default: return CIRRUS_ERR_INVALID_ARGUMENT;

@@ -336,6 +336,45 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
             CK(cudaMalloc(&g->d_lapitems, sizeof(int4) * lapitems.size()));
             CK(cudaMemcpy(g->d_lapitems, lapitems.data(), sizeof(int4) * lapitems.size(), cudaMemcpyHostToDevice));
         }
+        // the same split for the residual + restriction of the fused V-cycle, per level, from the
+        // multigrid masks: face-path GHOST tiles give one item per coarse cell (every parent cell
+        // receives its += in both paths)
+        std::vector<int> rrmain;
+        std::vector<int4> rritems;
+        g->rr_off.assign(num_layers, 0);
+        g->rr_cnt.assign(num_layers, 0);
+        g->rri_off.assign(num_layers, 0);
+        g->rri_cnt.assign(num_layers, 0);
+        for (int l = 0; l < num_layers; l++) {
+            g->rr_off[l] = (int)rrmain.size();
+            g->rri_off[l] = (int)rritems.size();
+            for (int t = lfirst[l]; t < lfirst[l] + lcnt[l]; t++) {
+                bool face = (type[t] & GHOST_T) && par[t] >= 0;
+                uint32_t faces = 0;
+                for (int o = 0; o < kTileCells && face; o++) {
+                    const uint32_t bits = mmg[(size_t)t * kTileCells + o] & 0x3Fu;
+                    const int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                    const uint32_t on = (i == 0 ? 1u : 0u) | (i == 7 ? 2u : 0u) | (j == 0 ? 4u : 0u) | (j == 7 ? 8u : 0u) |
+                                        (k == 0 ? 16u : 0u) | (k == 7 ? 32u : 0u);
+                    if (bits & ~on) face = false;
+                    faces |= bits;
+                }
+                if (!face) {
+                    rrmain.push_back(t);
+                    continue;
+                }
+                const int oct = (meta[t].packed >> 16) & 7;
+                for (int c = 0; c < 64; c++)
+                    rritems.push_back(make_int4(t, c | (int)(faces << 6) | (int)(((fcls[t] >> 12) & 0xfffu) << 12) | (oct << 24), par[t],
+                                                g_inst[t] * kLevelSlots + level[t]));
+            }
+            g->rr_cnt[l] = (int)rrmain.size() - g->rr_off[l];
+            g->rri_cnt[l] = (int)rritems.size() - g->rri_off[l];
+        }
+        CK(cudaMalloc(&g->d_rrmain, sizeof(int) * std::max<size_t>(rrmain.size(), 1)));
+        if (!rrmain.empty()) CK(cudaMemcpy(g->d_rrmain, rrmain.data(), sizeof(int) * rrmain.size(), cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&g->d_rritems, sizeof(int4) * std::max<size_t>(rritems.size(), 1)));
+        if (!rritems.empty()) CK(cudaMemcpy(g->d_rritems, rritems.data(), sizeof(int4) * rritems.size(), cudaMemcpyHostToDevice));
         CK(cudaMalloc(&g->d_xpre, sizeof(float) * kTileCells * (size_t)n));
         CK(cudaMemset(g->d_xpre, 0, sizeof(float) * kTileCells * (size_t)n));  // GHOST tiles stay 0
     }
@@ -524,6 +563,8 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_ghost_tables);
     cudaFree(g->d_gacc);
     cudaFree(g->d_lapitems);
+    cudaFree(g->d_rrmain);
+    cudaFree(g->d_rritems);
     cudaFree(g->d_xpre);
     cudaFree(g->d_bottom_tiles);
     cudaFree(g->d_bottom_code);

@@ -335,14 +335,97 @@ __global__ void __launch_bounds__(1024) k_gs_sequence(Topo tp, const int* __rest
 }
 
 // ------------------------------------------------------------------ residual + restriction
+// Face path of the residual + restriction for one coarse cell of a GHOST tile whose x and
+// right-hand side are 0 (the fused V-cycle keeps them so) and whose coupled cells all lie on its
+// faces, coupled only outward.  Item: tile, coarse cell c | coupled faces << 6 | face classes <<
+// 12 | octant << 24, parent tile, level-constant index.  r = 0 - A x on the block's cells (A x
+// from the neighbours' values across coupled faces, fused as the full path rounds it; +0 on
+// uncoupled cells), summed in (ii,jj,kk) order and added to the parent cell.
+__device__ __forceinline__ void ghost_face_restrict(const Topo& tp, const float* __restrict__ X, int4 it, float* C) {
+    const int tile = it.x, c = it.y & 63;
+    const uint32_t faces = ((uint32_t)it.y >> 6) & 63u, cls = ((uint32_t)it.y >> 12) & 0xfffu;
+    const int oct = ((uint32_t)it.y >> 24) & 7u;
+    const int fi = c / 16 * 2, fj = (c / 4) % 4 * 2, fk = c % 4 * 2;
+    const uint32_t touch = (fi == 0 ? 1u : 0u) | (fi == 6 ? 2u : 0u) | (fj == 0 ? 4u : 0u) | (fj == 6 ? 8u : 0u) | (fk == 0 ? 16u : 0u) |
+                           (fk == 6 ? 32u : 0u);
+    const uint32_t act = touch & faces;
+    float sum = 0.f;
+    if (act) {
+        const size_t base = (size_t)tile * kTileCells;
+        const int o0 = fi * 64 + fj * 8 + fk;
+        uint32_t mk[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) mk[q] = *reinterpret_cast<const uint16_t*>(tp.mask_mg + base + o0 + (q >> 1) * 64 + (q & 1) * 8);
+        const TileMeta& m = tp.meta[tile];
+        float nv[6][4];
+#pragma unroll
+        for (int f = 0; f < 6; f++) {
+            const int nb = ((act >> f) & 1u) ? m.nb[f] : -1;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int a = q >> 1, b = q & 1;
+                int noff;
+                if (f == 0) noff = 7 * 64 + (fj + a) * 8 + fk + b;
+                else if (f == 1) noff = (fj + a) * 8 + fk + b;
+                else if (f == 2) noff = (fi + a) * 64 + 7 * 8 + fk + b;
+                else if (f == 3) noff = (fi + a) * 64 + fk + b;
+                else if (f == 4) noff = (fi + a) * 64 + (fj + b) * 8 + 7;
+                else noff = (fi + a) * 64 + (fj + b) * 8;
+                nv[f][q] = nb >= 0 ? X[(size_t)nb * kTileCells + noff] : 0.f;
+            }
+        }
+        const LevelConst<float> L(tp.lconst[it.w]);
+#pragma unroll
+        for (int ii = 0; ii < 2; ii++)
+#pragma unroll
+            for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+                for (int kk = 0; kk < 2; kk++) {
+                    const int i = fi + ii, j = fj + jj, k = fk + kk;
+                    const uint32_t on = (i == 0 ? 1u : 0u) | (i == 7 ? 2u : 0u) | (j == 0 ? 4u : 0u) | (j == 7 ? 8u : 0u) |
+                                        (k == 0 ? 16u : 0u) | (k == 7 ? 32u : 0u);
+                    const uint32_t mm = (mk[ii * 2 + jj] >> (8 * kk)) & 0xffu;
+                    float r = 0.f;
+                    if ((on & act) && (mm & 0x3Fu)) {
+                        float s = 0.f;
+#pragma unroll
+                        for (int f = 0; f < 6; f++) {
+                            if (!(mm & (1u << f))) continue;
+                            const float a = ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1;
+                            const float xf = nv[f][f < 2 ? jj * 2 + kk : (f < 4 ? ii * 2 + kk : ii * 2 + jj)];
+                            s = fmaf(a, 0.f - xf, s);
+                        }
+                        const float ax = (mm & kMaskInterior) ? s * L.h * L.h * L.h : 0.f;
+                        r = 0.f - ax;
+                    }
+                    sum += r;
+                }
+    } else {
+#pragma unroll
+        for (int e = 0; e < 8; e++) sum += 0.f;
+    }
+    C[(size_t)it.z * kTileCells + ((oct & 1) * 4 + fi / 2) * 64 + (((oct >> 1) & 1) * 4 + fj / 2) * 8 + ((oct >> 2) & 1) * 4 + fk / 2] += sum;
+}
+
 // ResidualAndRestrict128Kernel (src/GMGSolver.cu:284-339): r = rhs - A x on every cell of the
 // level's tiles; 2x2x2 sums go to the parent cell: GHOST tiles add, others overwrite
-// (times one_over_alpha).
+// (times one_over_alpha).  The staged path takes tiles list[0..n) (or first..first+n when list is
+// null); the first item_blocks CTAs take face-path GHOST cells (ghost_face_restrict), one per
+// thread.
 template <int TPB, int NT>
-__global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int first, int n, const float* __restrict__ X,
-                                                                 const float* RHS, float* C, float one_over_alpha,
-                                                                 const Scalars* __restrict__ S) {
+__global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int first, const int* __restrict__ list, int n,
+                                                                 const int4* __restrict__ items, int nitems, int item_blocks,
+                                                                 const float* __restrict__ X, const float* RHS, float* C,
+                                                                 float one_over_alpha, const Scalars* __restrict__ S) {
     pdl_entry();
+    if ((int)blockIdx.x < item_blocks) {
+        const int q = (int)blockIdx.x * (128 * TPB) + (int)threadIdx.x;
+        if (q >= nitems) return;
+        const int4 it = items[q];
+        if (S != nullptr && S[it.w / kLevelSlots].done) return;
+        ghost_face_restrict(tp, X, it, C);
+        return;
+    }
     extern __shared__ __align__(16) unsigned char rr_smem[];
     TileStage* st = reinterpret_cast<TileStage*>(rr_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
@@ -350,8 +433,9 @@ __global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int fi
     bool act[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
-        const int q = (blockIdx.x * NT + u) * TPB + g;
-        tile[u] = first + (q < n ? q : 0);
+        const int q = (((int)blockIdx.x - item_blocks) * NT + u) * TPB + g;
+        const int qq = q < n ? q : 0;
+        tile[u] = list ? list[qq] : first + qq;
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
     }
     TilePre pre[NT];
@@ -984,23 +1068,26 @@ void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t
 
 template <int TPB, int NT>
 void residual_shape(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha, const Scalars* S,
-                    cudaStream_t s) {
-    const int n = g.level_count[level];
+                    cudaStream_t s, bool ghosts_zero) {
     const int per = TPB * NT;
-    launch_kernel(k_residual_restrict<TPB, NT>, (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
-                  g.level_first[level], n, X, RHS, C, one_over_alpha, S);
+    const int* list = ghosts_zero ? g.d_rrmain + g.rr_off[level] : nullptr;
+    const int n = ghosts_zero ? g.rr_cnt[level] : g.level_count[level];
+    const int nitems = ghosts_zero ? g.rri_cnt[level] : 0;
+    const int4* items = ghosts_zero ? g.d_rritems + g.rri_off[level] : nullptr;
+    const int item_blocks = (nitems + 128 * TPB - 1) / (128 * TPB);
+    launch_kernel(k_residual_restrict<TPB, NT>, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
+                  g.level_first[level], list, n, items, nitems, item_blocks, X, RHS, C, one_over_alpha, S);
 }
 
 void residual_restrict(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha,
-                       const Scalars* S, cudaStream_t s) {
-    const int n = g.level_count[level];
-    if (n == 0) return;
+                       const Scalars* S, cudaStream_t s, bool ghosts_zero) {
+    if (g.level_count[level] == 0) return;
     ++g.launch_count;
     switch (g.shape(KS_RESIDUAL, level)) {
-    case 0: residual_shape<2, 1>(g, level, X, RHS, C, one_over_alpha, S, s); break;
-    case 1: residual_shape<2, 2>(g, level, X, RHS, C, one_over_alpha, S, s); break;
-    case 2: residual_shape<1, 4>(g, level, X, RHS, C, one_over_alpha, S, s); break;
-    default: residual_shape<2, 4>(g, level, X, RHS, C, one_over_alpha, S, s); break;
+    case 0: residual_shape<2, 1>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    case 1: residual_shape<2, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    case 2: residual_shape<1, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    default: residual_shape<2, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     }
 }
 

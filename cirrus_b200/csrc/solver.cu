@@ -72,7 +72,7 @@ void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, fl
     const int lb = g.bottom_level;
     for (int l = g.max_level; l > lb; l--) {
         launch::presmooth(g, l, g.d_xpre, RHS, S, s);
-        launch::residual_restrict(g, l, g.d_xpre, RHS, RHS, one_over_alpha, S, s);
+        launch::residual_restrict(g, l, g.d_xpre, RHS, RHS, one_over_alpha, S, s, true);
     }
     launch::bottom(g, lb, coarsest_iters, X, RHS, one_over_alpha, prolong_coeff, S, s);
     for (int l = lb + 1; l <= g.max_level; l++) {

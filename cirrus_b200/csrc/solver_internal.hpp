@@ -107,6 +107,13 @@ struct DevGrid {
     int n_lapmain = 0;
     int4* d_lapitems = nullptr;
     int n_lapface = 0, n_lapitems = 0;
+    // residual + restriction with GHOST x and right-hand sides 0: per level the tiles of the
+    // staged path (all but the face-path GHOST tiles) and one item per coarse cell of each
+    // face-path GHOST tile (tile, cell | coupled faces << 6 | face classes << 12 | octant << 24,
+    // parent tile, level-constant index)
+    std::vector<int> rr_off, rr_cnt, rri_off, rri_cnt;
+    int* d_rrmain = nullptr;
+    int4* d_rritems = nullptr;
     std::vector<int> mg_offset, mg_count, level_first, level_count;
     std::vector<uint8_t> h_tile_type;
     std::vector<uint8_t> shapes;  // KS_COUNT x num_layers launch-shape choices
@@ -186,8 +193,10 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
 void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s);
 void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t colors, int nsweeps, const Scalars* S,
                  cudaStream_t s);
+// ghosts_zero: GHOST tiles hold x = 0 and right-hand side 0 (the fused V-cycle), so the
+// face-path GHOST tiles of the level skip staging.
 void residual_restrict(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha,
-                       const Scalars* S, cudaStream_t s);
+                       const Scalars* S, cudaStream_t s, bool ghosts_zero = false);
 void prolongate(const DevGrid& g, int level, const float* CX, float* FX, float prolong_coeff, const Scalars* S, cudaStream_t s);
 void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const Scalars* S, cudaStream_t s);
 // Per-instance reduction over LEAF vectors with the fused elementwise work of `op`; the
