@@ -375,6 +375,34 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
         if (!rrmain.empty()) CK(cudaMemcpy(g->d_rrmain, rrmain.data(), sizeof(int) * rrmain.size(), cudaMemcpyHostToDevice));
         CK(cudaMalloc(&g->d_rritems, sizeof(int4) * std::max<size_t>(rritems.size(), 1)));
         if (!rritems.empty()) CK(cudaMemcpy(g->d_rritems, rritems.data(), sizeof(int4) * rritems.size(), cudaMemcpyHostToDevice));
+        // prolongation split: non-GHOST tiles per level, and the GHOST faces that a non-GHOST
+        // neighbour at the same level reads as its halo
+        std::vector<int> prmain;
+        std::vector<int4> pritems;
+        g->pr_off.assign(num_layers, 0);
+        g->pr_cnt.assign(num_layers, 0);
+        g->pri_off.assign(num_layers, 0);
+        g->pri_cnt.assign(num_layers, 0);
+        for (int l = 0; l < num_layers; l++) {
+            g->pr_off[l] = (int)prmain.size();
+            g->pri_off[l] = (int)pritems.size();
+            for (int t = lfirst[l]; t < lfirst[l] + lcnt[l]; t++) {
+                if (!(type[t] & GHOST_T)) {
+                    prmain.push_back(t);
+                    continue;
+                }
+                for (int f = 0; f < 6; f++) {
+                    const int nb = meta[t].nb[f];
+                    if (nb >= 0 && !(type[nb] & GHOST_T)) pritems.push_back(make_int4(t, f, par[t], (meta[t].packed >> 16) & 7));
+                }
+            }
+            g->pr_cnt[l] = (int)prmain.size() - g->pr_off[l];
+            g->pri_cnt[l] = (int)pritems.size() - g->pri_off[l];
+        }
+        CK(cudaMalloc(&g->d_prmain, sizeof(int) * std::max<size_t>(prmain.size(), 1)));
+        if (!prmain.empty()) CK(cudaMemcpy(g->d_prmain, prmain.data(), sizeof(int) * prmain.size(), cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&g->d_pritems, sizeof(int4) * std::max<size_t>(pritems.size(), 1)));
+        if (!pritems.empty()) CK(cudaMemcpy(g->d_pritems, pritems.data(), sizeof(int4) * pritems.size(), cudaMemcpyHostToDevice));
         CK(cudaMalloc(&g->d_xpre, sizeof(float) * kTileCells * (size_t)n));
         CK(cudaMemset(g->d_xpre, 0, sizeof(float) * kTileCells * (size_t)n));  // GHOST tiles stay 0
     }
@@ -565,6 +593,8 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_lapitems);
     cudaFree(g->d_rrmain);
     cudaFree(g->d_rritems);
+    cudaFree(g->d_prmain);
+    cudaFree(g->d_pritems);
     cudaFree(g->d_xpre);
     cudaFree(g->d_bottom_tiles);
     cudaFree(g->d_bottom_code);

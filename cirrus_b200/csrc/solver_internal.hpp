@@ -114,6 +114,11 @@ struct DevGrid {
     std::vector<int> rr_off, rr_cnt, rri_off, rri_cnt;
     int* d_rrmain = nullptr;
     int4* d_rritems = nullptr;
+    // prolongation of the fused V-cycle: per level the non-GHOST tiles (staged path) and one item
+    // per GHOST face towards a non-GHOST neighbour (tile, face, parent tile, octant)
+    std::vector<int> pr_off, pr_cnt, pri_off, pri_cnt;
+    int* d_prmain = nullptr;
+    int4* d_pritems = nullptr;
     std::vector<int> mg_offset, mg_count, level_first, level_count;
     std::vector<uint8_t> h_tile_type;
     std::vector<uint8_t> shapes;  // KS_COUNT x num_layers launch-shape choices

@@ -228,14 +228,45 @@ __device__ __forceinline__ float prolong_value(uint32_t mm, bool ghost, float cx
     return (mm & kMaskInterior) ? (ghost ? cx : fmaf(prolong_coeff, cx, x)) : 0.f;
 }
 
-// Prolongation into every tile of one level; on mg tiles also the first colour (1) of
-// GaussSeidelGMG(1, 1).  Reads Z of the coarser level and XP of this level, writes Z of this
-// level.  NT tiles per 128-thread group are staged with asynchronous copies.
+// Prolongation into one face layer of a GHOST tile (item: tile, face, parent tile, octant in the
+// parent), one thread per cell: x = the parent value on INTERIOR cells, 0 elsewhere.  A GHOST
+// tile's x is read only as the face halo of its non-GHOST neighbours at the same level (the
+// second colour sweep), so only the faces towards those are written.
+__device__ __forceinline__ void ghost_face_prolong(const Topo& tp, float* Z, int4 it, int c) {
+    const int a = c >> 3, b = c & 7;
+    int i, j, k;
+    switch (it.y) {
+        case 0: i = 0; j = a; k = b; break;
+        case 1: i = 7; j = a; k = b; break;
+        case 2: i = a; j = 0; k = b; break;
+        case 3: i = a; j = 7; k = b; break;
+        case 4: i = a; j = b; k = 0; break;
+        default: i = a; j = b; k = 7; break;
+    }
+    const int off = i * 64 + j * 8 + k;
+    const size_t base = (size_t)it.x * kTileCells;
+    const float cx = it.z >= 0 ? Z[(size_t)it.z * kTileCells + parent_cell(it.w, off)] : 0.f;
+    Z[base + off] = prolong_value(tp.mask_mg[base + off], true, cx, 0.f, 0.f);
+}
+
+// Prolongation into the tiles of one level; on non-GHOST tiles (list[0..n)) also the first
+// colour (1) of GaussSeidelGMG(1, 1), NT tiles per 128-thread group staged with asynchronous
+// copies; the first item_blocks CTAs prolongate GHOST face layers (ghost_face_prolong), two per
+// 128 threads.  Reads Z of the coarser level and XP of this level, writes Z of this level.
 template <int TPB, int NT>
-__global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first, int n, float* Z, const float* __restrict__ XP,
-                                                             const float* __restrict__ RHS, float prolong_coeff,
-                                                             const Scalars* __restrict__ S) {
+__global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, const int* __restrict__ list, int n,
+                                                             const int4* __restrict__ items, int nitems, int item_blocks, float* Z,
+                                                             const float* __restrict__ XP, const float* __restrict__ RHS,
+                                                             float prolong_coeff, const Scalars* __restrict__ S) {
     pdl_entry();
+    if ((int)blockIdx.x < item_blocks) {
+        const int q = (int)blockIdx.x * (2 * TPB) + ((int)threadIdx.x >> 6);
+        if (q >= nitems) return;
+        const int4 it = items[q];
+        if (tile_done(tp, S, it.x)) return;
+        ghost_face_prolong(tp, Z, it, threadIdx.x & 63);
+        return;
+    }
     extern __shared__ __align__(16) unsigned char pro_smem[];
     ProStage* st = reinterpret_cast<ProStage*>(pro_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
@@ -259,8 +290,8 @@ __global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, int first,
     float4 lc[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
-        const int q = (blockIdx.x * NT + u) * TPB + g;
-        tile[u] = first + (q < n ? q : 0);
+        const int q = (((int)blockIdx.x - item_blocks) * NT + u) * TPB + g;
+        tile[u] = list[q < n ? q : 0];
         act[u] = q < n;  // finished instances are dropped after the copies are issued
         const TileMeta& m = tp.meta[tile[u]];
         packed[u] = m.packed;
@@ -586,10 +617,11 @@ void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const S
 template <int TPB, int NT>
 void prolong_shape(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
                    cudaStream_t s) {
-    const int n = g.level_count[level];
+    const int n = g.pr_cnt[level], nitems = g.pri_cnt[level];
     const int per = TPB * NT;
-    launch_kernel(k_prolong_sweep<TPB, NT>, (n + per - 1) / per, 128 * TPB, sizeof(ProStage) * per, s, g.topo, g.level_first[level], n,
-                  Z, XP, RHS, prolong_coeff, S);
+    const int item_blocks = (nitems + 2 * TPB - 1) / (2 * TPB);
+    launch_kernel(k_prolong_sweep<TPB, NT>, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(ProStage) * per, s, g.topo,
+                  g.d_prmain + g.pr_off[level], n, g.d_pritems + g.pri_off[level], nitems, item_blocks, Z, XP, RHS, prolong_coeff, S);
 }
 
 void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
