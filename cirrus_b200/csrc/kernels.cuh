@@ -122,7 +122,12 @@ __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32
     const V4<T> yp = ld4(ix.j < 7 ? xs + (t + 2) * 4 : hx + 3 * 64 + ix.i * 8 + ix.k0);
     const T zlo = *(ix.k0 > 0 ? xs + t * 4 - 1 : hx + 4 * 64 + ix.i * 8 + ix.j);
     const T zhi = *(ix.k0 < 4 ? xs + t * 4 + 4 : hx + 5 * 64 + ix.i * 8 + ix.j);
-    if (mask4 == 0x7F7F7F7Fu) {
+    // The path is chosen per warp (a vote over the converged lanes), so a warp never runs two
+    // paths one after the other: each path gives a lane's cells the same bits (the general one
+    // with a_f = c1 on uniform cells, +0 on cells without coupled faces), so the choice only
+    // affects speed.
+    const unsigned lanes = __activemask();
+    if (__all_sync(lanes, mask4 == 0x7F7F7F7Fu)) {
         // the four cells are INTERIOR with six 1/h^2 faces: every coefficient is c1 (the same
         // operations as the general path below with a_f = c1)
 #pragma unroll
@@ -142,7 +147,7 @@ __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32
         }
         return;
     }
-    if ((mask4 & 0x3F3F3F3Fu) == 0u) {
+    if (__all_sync(lanes, (mask4 & 0x3F3F3F3Fu) == 0u)) {
         // no coupled face on any of the four cells (e.g. inside a GHOST tile, whose ghost-ghost
         // faces carry no coefficient): every product is 0, the sum stays +0, and so do the
         // result and the diagonal (for finite values, the general path's bits)
@@ -189,27 +194,37 @@ __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32
     }
 }
 
-// One Gauss-Seidel update x0 + (b - A x)/D of a single cell with mask byte m at local (i, j, k),
-// given its six neighbour values in face order: the operations of neg_lap4 + the sweep update.
+// Coefficients of the general stencil path for thread t's column of four cells: the x and y
+// faces of its (i, j) column and the outer z faces of its first and last cell (1/h^2 inside the
+// tile, the cross-face class's coefficient on a tile face).
+template <class T> struct FaceCoef {
+    T xm, xp, ym, yp, zlo, zhi;
+};
+template <class T>
+__device__ __forceinline__ FaceCoef<T> face_coef(const TileIdx& ix, uint32_t cls, const LevelConst<T>& L) {
+    auto cross = [&](int f) -> T { return ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1; };
+    FaceCoef<T> c;
+    c.xm = ix.i == 0 ? cross(0) : L.c1;
+    c.xp = ix.i == 7 ? cross(1) : L.c1;
+    c.ym = ix.j == 0 ? cross(2) : L.c1;
+    c.yp = ix.j == 7 ? cross(3) : L.c1;
+    c.zlo = ix.k0 == 0 ? cross(4) : L.c1;
+    c.zhi = ix.k0 == 4 ? cross(5) : L.c1;
+    return c;
+}
+
+// One Gauss-Seidel update x0 + (b - A x)/D of a single cell with mask byte m, given its six
+// neighbour values in face order and the coefficients of its x/y faces (C) and z faces (azl,
+// azr): the operations of neg_lap4 + the sweep update.  On a uniform cell (m = 0x7F, every
+// coefficient 1/h^2) it gives gs_cell_fast's bits.
 __device__ __forceinline__ float gs_cell(float x0, float xm, float xp, float ym, float yp, float zl, float zr, float b, uint32_t m,
-                                         int i, int j, int k, uint32_t cls, const LevelConst<float>& L) {
-    if (m == (uint32_t)kMaskFull) {
-        float s = 0.f;
-        s = fmaf(L.c1, x0 - xm, s);
-        s = fmaf(L.c1, x0 - xp, s);
-        s = fmaf(L.c1, x0 - ym, s);
-        s = fmaf(L.c1, x0 - yp, s);
-        s = fmaf(L.c1, x0 - zl, s);
-        s = fmaf(L.c1, x0 - zr, s);
-        return x0 + (b - mul_h3(s, L.h)) / L.dfast;
-    }
-    auto cross = [&](int f) -> float { return ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1; };
-    const float a0 = (m & 1u) ? (i == 0 ? cross(0) : L.c1) : 0.f;
-    const float a1 = (m & 2u) ? (i == 7 ? cross(1) : L.c1) : 0.f;
-    const float a2 = (m & 4u) ? (j == 0 ? cross(2) : L.c1) : 0.f;
-    const float a3 = (m & 8u) ? (j == 7 ? cross(3) : L.c1) : 0.f;
-    const float a4 = (m & 16u) ? (k == 0 ? cross(4) : L.c1) : 0.f;
-    const float a5 = (m & 32u) ? (k == 7 ? cross(5) : L.c1) : 0.f;
+                                         const FaceCoef<float>& C, float azl, float azr, const LevelConst<float>& L) {
+    const float a0 = (m & 1u) ? C.xm : 0.f;
+    const float a1 = (m & 2u) ? C.xp : 0.f;
+    const float a2 = (m & 4u) ? C.ym : 0.f;
+    const float a3 = (m & 8u) ? C.yp : 0.f;
+    const float a4 = (m & 16u) ? azl : 0.f;
+    const float a5 = (m & 32u) ? azr : 0.f;
     float s = 0.f;
     s = fmaf(a0, x0 - xm, s);
     s = fmaf(a1, x0 - xp, s);
@@ -217,17 +232,28 @@ __device__ __forceinline__ float gs_cell(float x0, float xm, float xp, float ym,
     s = fmaf(a3, x0 - yp, s);
     s = fmaf(a4, x0 - zl, s);
     s = fmaf(a5, x0 - zr, s);
-    const bool interior = m & kMaskInterior;
-    const float ax = interior ? s * L.h * L.h * L.h : 0.f;
     float d = 0.f;
     d = d + a0; d = d + a1; d = d + a2; d = d + a3; d = d + a4; d = d + a5;
-    const float dd = interior ? d * L.h * L.h * L.h : 0.f;
-    return x0 + (interior ? (b - ax) / dd : 0.f);
+    return x0 + ((m & kMaskInterior) ? (b - mul_h3(s, L.h)) / mul_h3(d, L.h) : 0.f);
+}
+// gs_cell on a uniform cell: every coefficient 1/h^2, the diagonal the level's constant.
+__device__ __forceinline__ float gs_cell_fast(float x0, float xm, float xp, float ym, float yp, float zl, float zr, float b,
+                                              const LevelConst<float>& L) {
+    float s = 0.f;
+    s = fmaf(L.c1, x0 - xm, s);
+    s = fmaf(L.c1, x0 - xp, s);
+    s = fmaf(L.c1, x0 - ym, s);
+    s = fmaf(L.c1, x0 - yp, s);
+    s = fmaf(L.c1, x0 - zl, s);
+    s = fmaf(L.c1, x0 - zr, s);
+    return x0 + (b - mul_h3(s, L.h)) / L.dfast;
 }
 
 // One colour of a red-black sweep on thread t's four cells: the two cells of colour `color`
 // (k0 is even, so they are e = p and p + 2 with p = (color + i + j) & 1) get the update, the
-// other two keep their values.  xs/hx: the tile and its halos in shared memory.
+// other two keep their values.  xs/hx: the tile and its halos in shared memory.  Uniform warps
+// (every lane's four cells uniform, by vote) take the fast form, the others the general one for
+// every lane: the same bits either way.
 __device__ __forceinline__ V4<float> colour_update(const float* xs, const float* hx, int t, uint32_t mask4, uint32_t cls,
                                                    const LevelConst<float>& L, const V4<float>& b, int color) {
     const TileIdx ix(t);
@@ -239,13 +265,26 @@ __device__ __forceinline__ V4<float> colour_update(const float* xs, const float*
     const float zlo = *(ix.k0 > 0 ? xs + t * 4 - 1 : hx + 4 * 64 + ix.i * 8 + ix.j);
     const float zhi = *(ix.k0 < 4 ? xs + t * 4 + 4 : hx + 5 * 64 + ix.i * 8 + ix.j);
     const bool p = (color + ix.i + ix.j) & 1;
-    const uint32_t mA = (mask4 >> (p ? 8 : 0)) & 0xffu, mB = (mask4 >> (p ? 24 : 16)) & 0xffu;
-    const float A = gs_cell(p ? xc.v[1] : xc.v[0], p ? xm.v[1] : xm.v[0], p ? xp.v[1] : xp.v[0], p ? ym.v[1] : ym.v[0],
-                            p ? yp.v[1] : yp.v[0], p ? xc.v[0] : zlo, p ? xc.v[2] : xc.v[1], p ? b.v[1] : b.v[0], mA, ix.i, ix.j,
-                            ix.k0 + (p ? 1 : 0), cls, L);
-    const float B = gs_cell(p ? xc.v[3] : xc.v[2], p ? xm.v[3] : xm.v[2], p ? xp.v[3] : xp.v[2], p ? ym.v[3] : ym.v[2],
-                            p ? yp.v[3] : yp.v[2], p ? xc.v[2] : xc.v[1], p ? zhi : xc.v[3], p ? b.v[3] : b.v[2], mB, ix.i, ix.j,
-                            ix.k0 + (p ? 3 : 2), cls, L);
+    // cell A = e p, cell B = e p + 2
+    const float x0A = p ? xc.v[1] : xc.v[0], x0B = p ? xc.v[3] : xc.v[2];
+    const float xmA = p ? xm.v[1] : xm.v[0], xmB = p ? xm.v[3] : xm.v[2];
+    const float xpA = p ? xp.v[1] : xp.v[0], xpB = p ? xp.v[3] : xp.v[2];
+    const float ymA = p ? ym.v[1] : ym.v[0], ymB = p ? ym.v[3] : ym.v[2];
+    const float ypA = p ? yp.v[1] : yp.v[0], ypB = p ? yp.v[3] : yp.v[2];
+    const float zlA = p ? xc.v[0] : zlo, zrA = p ? xc.v[2] : xc.v[1];
+    const float zlB = p ? xc.v[2] : xc.v[1], zrB = p ? zhi : xc.v[3];
+    const float bA = p ? b.v[1] : b.v[0], bB = p ? b.v[3] : b.v[2];
+    float A, B;
+    if (__all_sync(__activemask(), mask4 == 0x7F7F7F7Fu)) {
+        A = gs_cell_fast(x0A, xmA, xpA, ymA, ypA, zlA, zrA, bA, L);
+        B = gs_cell_fast(x0B, xmB, xpB, ymB, ypB, zlB, zrB, bB, L);
+    } else {
+        const FaceCoef<float> C = face_coef(ix, cls, L);
+        const uint32_t mA = (mask4 >> (p ? 8 : 0)) & 0xffu, mB = (mask4 >> (p ? 24 : 16)) & 0xffu;
+        // cell A is the column's first cell (outer z- face) when p = 0; B its last (z+) when p = 1
+        A = gs_cell(x0A, xmA, xpA, ymA, ypA, zlA, zrA, bA, mA, C, p ? L.c1 : C.zlo, L.c1, L);
+        B = gs_cell(x0B, xmB, xpB, ymB, ypB, zlB, zrB, bB, mB, C, L.c1, p ? C.zhi : L.c1, L);
+    }
     V4<float> o = xc;
     if (p) { o.v[1] = A; o.v[3] = B; } else { o.v[0] = A; o.v[2] = B; }
     return o;
