@@ -201,16 +201,60 @@ template <class T> struct FaceCoef {
     T xm, xp, ym, yp, zlo, zhi;
 };
 template <class T>
-__device__ __forceinline__ FaceCoef<T> face_coef(const TileIdx& ix, uint32_t cls, const LevelConst<T>& L) {
+__device__ __forceinline__ FaceCoef<T> face_coef(int i, int j, int k0, uint32_t cls, const LevelConst<T>& L) {
     auto cross = [&](int f) -> T { return ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1; };
     FaceCoef<T> c;
-    c.xm = ix.i == 0 ? cross(0) : L.c1;
-    c.xp = ix.i == 7 ? cross(1) : L.c1;
-    c.ym = ix.j == 0 ? cross(2) : L.c1;
-    c.yp = ix.j == 7 ? cross(3) : L.c1;
-    c.zlo = ix.k0 == 0 ? cross(4) : L.c1;
-    c.zhi = ix.k0 == 4 ? cross(5) : L.c1;
+    c.xm = i == 0 ? cross(0) : L.c1;
+    c.xp = i == 7 ? cross(1) : L.c1;
+    c.ym = j == 0 ? cross(2) : L.c1;
+    c.yp = j == 7 ? cross(3) : L.c1;
+    c.zlo = k0 == 0 ? cross(4) : L.c1;
+    c.zhi = k0 == 4 ? cross(5) : L.c1;
     return c;
+}
+template <class T>
+__device__ __forceinline__ FaceCoef<T> face_coef(const TileIdx& ix, uint32_t cls, const LevelConst<T>& L) {
+    return face_coef(ix.i, ix.j, ix.k0, cls, L);
+}
+
+// Diagonal h^3 * sum_f a_f of a cell with mask byte m (the sum in face order, as neg_lap4 forms
+// it; 0 off INTERIOR), x/y-face coefficients C and z-face coefficients azl, azr.  On a uniform
+// cell it equals the level's dfast bit for bit.
+__device__ __forceinline__ float diag_cell(uint32_t m, const FaceCoef<float>& C, float azl, float azr, const LevelConst<float>& L) {
+    const float a0 = (m & 1u) ? C.xm : 0.f;
+    const float a1 = (m & 2u) ? C.xp : 0.f;
+    const float a2 = (m & 4u) ? C.ym : 0.f;
+    const float a3 = (m & 8u) ? C.yp : 0.f;
+    const float a4 = (m & 16u) ? azl : 0.f;
+    const float a5 = (m & 32u) ? azr : 0.f;
+    float d = 0.f;
+    d = d + a0; d = d + a1; d = d + a2; d = d + a3; d = d + a4; d = d + a5;
+    return (m & kMaskInterior) ? mul_h3(d, L.h) : 0.f;
+}
+
+// First colour (0) of a red-black sweep from x = 0 on a 4-cell column run (i, j, k0..k0+3):
+// x = b/D on its two colour-0 cells (e = q, q + 2 with q = (i + j) & 1, k0 even), 0 elsewhere and
+// off INTERIOR.  The warp takes D = dfast when every lane's four cells are uniform (by vote),
+// else the general diagonal on every lane: the same bits either way.
+__device__ __forceinline__ V4<float> first_colour_run(int i, int j, int k0, uint32_t mask4, const V4<float>& b, uint32_t cls,
+                                                      const LevelConst<float>& L) {
+    const int q = (i + j) & 1;
+    const uint32_t mA = (mask4 >> (q ? 8 : 0)) & 0xffu, mB = (mask4 >> (q ? 24 : 16)) & 0xffu;
+    const float bA = q ? b.v[1] : b.v[0], bB = q ? b.v[3] : b.v[2];
+    float dA, dB;
+    if (__all_sync(__activemask(), mask4 == 0x7F7F7F7Fu)) {
+        dA = L.dfast;
+        dB = L.dfast;
+    } else {
+        const FaceCoef<float> C = face_coef(i, j, k0, cls, L);
+        dA = diag_cell(mA, C, q ? L.c1 : C.zlo, L.c1, L);
+        dB = diag_cell(mB, C, L.c1, q ? C.zhi : L.c1, L);
+    }
+    const float vA = (mA & kMaskInterior) ? 0.f + (bA - 0.f) / dA : 0.f;
+    const float vB = (mB & kMaskInterior) ? 0.f + (bB - 0.f) / dB : 0.f;
+    V4<float> o = zero4<float>();
+    if (q) { o.v[1] = vA; o.v[3] = vB; } else { o.v[0] = vA; o.v[2] = vB; }
+    return o;
 }
 
 // One Gauss-Seidel update x0 + (b - A x)/D of a single cell with mask byte m, given its six

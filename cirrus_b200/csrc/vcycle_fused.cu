@@ -149,31 +149,14 @@ __global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __r
         const LevelConst<float> L(lc[u]);
         const uint32_t cls = (fc[u] >> 12) & 0xfffu;
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ps.mask + t * 4);
-        const V4<float> b = ld4(ps.b + t * 4);
-        V4<float> x1;
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int k = ix.k0 + e;
-            const uint32_t mm = (mask4 >> (8 * e)) & 0xffu;
-            float v = 0.f;
-            if (((ix.i + ix.j + k) & 1) == 0 && (mm & kMaskInterior)) v = 0.f + (b.v[e] - 0.f) / cell_diag(ix.i, ix.j, k, mm, cls, L);
-            x1.v[e] = v;
-        }
-        st4(ps.xs + t * 4, x1);
+        st4(ps.xs + t * 4, first_colour_run(ix.i, ix.j, ix.k0, mask4, ld4(ps.b + t * 4), cls, L));
         if (t < 64) {
             const int face = fface;
             V4<float> v = zero4<float>();
             if (nbf[u] >= 0) {
-                const V4<float> nbb = ld4(ps.hx + face * 64 + qq * 4);
-                const uint32_t nm4 = *reinterpret_cast<const uint32_t*>(ps.hmask + face * 64 + qq * 4);
-                const uint32_t ncls = (nfc_f[u] >> 12) & 0xfffu;
                 const int ni = foff >> 6, nj = (foff >> 3) & 7, nk0 = foff & 7;
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const uint32_t mm = (nm4 >> (8 * e)) & 0xffu;
-                    if (((ni + nj + nk0 + e) & 1) == 0 && (mm & kMaskInterior))
-                        v.v[e] = 0.f + (nbb.v[e] - 0.f) / cell_diag(ni, nj, nk0 + e, mm, ncls, L);
-                }
+                v = first_colour_run(ni, nj, nk0, *reinterpret_cast<const uint32_t*>(ps.hmask + face * 64 + qq * 4),
+                                     ld4(ps.hx + face * 64 + qq * 4), (nfc_f[u] >> 12) & 0xfffu, L);
             }
             st4(ps.hx + face * 64 + qq * 4, v);
         }
