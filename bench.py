@@ -283,7 +283,7 @@ def run_serving(rank: int, built: dict, n_requests: int = 96, rates=(100.0, 400.
 def run_batch64(args) -> dict:
     """The batched configuration: 64 independent random-sphere instances (64^3-256^3 effective,
     1-4 levels) in one mixed-precision batched launch per step, each to a 1e-6 FP64 true relative
-    residual; autotuned launch shapes."""
+    residual; autotuned launch shapes and smoother sweep counts."""
     import torch
 
     from cirrus_b200 import B_CHANNEL, PRECISION_MIXED_FP64, TMP_CHANNEL, DeviceGrid, GMGSolver, workloads as W
@@ -298,12 +298,14 @@ def run_batch64(args) -> dict:
     g.copy_channel(TMP_CHANNEL, B_CHANNEL)
     stream = torch.cuda.current_stream()
     s = GMGSolver(precision=PRECISION_MIXED_FP64)
+    # smoother sweep counts from the sweep tuner (timed trial solves of this batch)
+    li, ci = s.autotune_sweeps(g, stream=stream.cuda_stream)
     times = []
     for i in range(args.warmup + args.steps):
         g.copy_channel(B_CHANNEL, TMP_CHANNEL, stream.cuda_stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        s.solve_batch(g, stream=stream.cuda_stream)
+        s.solve_batch(g, stream=stream.cuda_stream, level_iters=li, coarsest_iters=ci)
         e1.record(stream)
         torch.cuda.synchronize()
         if i >= args.warmup:
@@ -315,7 +317,8 @@ def run_batch64(args) -> dict:
     return {"value": round(value, 2), "unit": "solves/s", "instances": 64, "tiles": int(sum(b.tiles.shape[0] for b in bs)),
             "mdof_per_s": round(dof / 64 * value / 1e6, 1), "ms_per_batch": round(float(np.mean(times)), 3),
             "all_converged": all(r.status == 0 and r.true_rel_residual < 1e-6 for r in res),
-            "max_pcg_iters": int(max(r.iters for r in res)), "precision": "mixed, 1e-6 FP64 true residual"}
+            "max_pcg_iters": int(max(r.iters for r in res)), "precision": "mixed, 1e-6 FP64 true residual",
+            "sweeps": {"level_iters": li, "coarsest_iters": ci, "source": "sweep tuner"}}
 
 
 def cpu_baseline(b, rhs, budget_s: float = 10.0, max_solves: int = 5) -> dict:

@@ -383,6 +383,19 @@ class GMGSolver:
         self.last_result = res[0]
         return [(r.iters, r.rel_residual) for r in res]
 
+    def autotune_sweeps(self, grid: DeviceGrid, stream: int = 0, **kw) -> tuple[int, int]:
+        """Time this solver's batched solve of the grid's current right-hand sides for each
+        candidate (level_iters, coarsest_iters) and return the fastest pair that converged (pass
+        it back as solve_batch(..., level_iters=, coarsest_iters=)).  Sweep counts change the
+        iterates -- the reference's bits come only from (1, 10) -- so this is for the
+        mixed-precision solver, whose FP64 tolerance fixes the result.  b is restored; x and the
+        scratch channels are overwritten."""
+        p = self.params(**kw)
+        best = SolveParams()
+        check(lib().cirrus_grid_autotune_sweeps(grid.handle, C.byref(p), C.c_void_p(stream), C.byref(best)),
+              "cirrus_grid_autotune_sweeps")
+        return best.level_iters, best.coarsest_iters
+
     def solve_host(self, grid: DeviceGrid, b: np.ndarray, x_out: np.ndarray, stream: int = 0, **kw) -> tuple[int, float]:
         """End-to-end solve from host buffers (b in, x out; all-tiles order, 512 floats/tile)."""
         p = self.params(**kw)

@@ -5,6 +5,7 @@
 #include "solver_internal.hpp"
 
 #include <cstdio>
+#include <vector>
 
 namespace cirrus {
 
@@ -87,6 +88,79 @@ int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
     const bool ok = cudaStreamSynchronize(s) == cudaSuccess;
     cudaStreamDestroy(s);
     return ok ? 0 : 2;
+}
+
+// Sweep-count tuner: each candidate (level_iters, coarsest_iters) solves the grid's current
+// right-hand sides with `base` (precision, tolerance, flags), once to build its solve graph and
+// once timed with CUDA events on a private stream; the fastest candidate whose every instance
+// converged wins.  Sweep counts change the preconditioner (so the iterates), not the stopping
+// rule: a mixed-precision solve still ends at its FP64 tolerance.  b is restored after every
+// trial and at the end; x and the scratch channels keep the last trial's values.
+int autotune_sweeps(DevGrid& g, const SolveParams& base, cudaStream_t user, int* level_iters, int* coarsest_iters,
+                    std::string* report) {
+    static const int kCand[][2] = {{1, 2}, {1, 4}, {1, 6}, {1, 10}, {1, 16}, {1, 24}, {2, 10}};
+    *level_iters = base.level_iters;
+    *coarsest_iters = base.coarsest_iters;
+    if (cudaStreamSynchronize(user) != cudaSuccess) return 2;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return 2;
+    const size_t bytes = (size_t)g.n * kTileCells * sizeof(float);
+    float* bsave = nullptr;
+    if (cudaMalloc(&bsave, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamDestroy(s);
+        return 3;
+    }
+    cudaMemcpyAsync(bsave, g.d_ch[kChB], bytes, cudaMemcpyDeviceToDevice, s);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<SolveResult> r(g.num_inst);
+    float best = -1.f;
+    int rc = 0;
+    for (const auto& c : kCand) {
+        SolveParams p = base;
+        p.level_iters = c[0];
+        p.coarsest_iters = c[1];
+        p.warm_start = 0;
+        float ms = -1.f;
+        bool ok = true;
+        for (int rep = 0; rep < 2 && ok; rep++) {
+            cudaMemcpyAsync(g.d_ch[kChB], bsave, bytes, cudaMemcpyDeviceToDevice, s);
+            cudaEventRecord(e0, s);
+            rc = base.precision ? mixed_solve(g, p, s, r.data()) : pcg_solve(g, p, s, r.data());
+            cudaEventRecord(e1, s);
+            if (rc || cudaEventSynchronize(e1) != cudaSuccess) {
+                ok = false;
+                break;
+            }
+            for (const SolveResult& x : r) ok = ok && x.status == 0;
+            if (rep == 1) cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (rc) break;
+        if (report) {
+            char line[128];
+            std::snprintf(line, sizeof line, "level_iters %d coarsest_iters %d: %s %.3f ms\n", c[0], c[1], ok ? "converged" : "not converged",
+                          ms);
+            *report += line;
+        }
+        if (ok && ms > 0.f && (best < 0.f || ms < best)) {
+            best = ms;
+            *level_iters = c[0];
+            *coarsest_iters = c[1];
+        }
+    }
+    cudaMemcpyAsync(g.d_ch[kChB], bsave, bytes, cudaMemcpyDeviceToDevice, s);
+    const bool synced = cudaStreamSynchronize(s) == cudaSuccess;
+    cudaFree(bsave);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    drop_graphs(g);  // the trials' graphs; the next solve builds the one it needs
+    g.x64_valid = false;
+    if (rc) return rc;
+    if (!synced) return 2;
+    return best < 0.f ? 5 : 0;
 }
 
 }  // namespace cirrus

@@ -541,6 +541,21 @@ cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int le
     return CIRRUS_OK;
 }
 
+cirrus_status cirrus_grid_autotune_sweeps(cirrus_grid* grid, const cirrus_solve_params* params, void* stream,
+                                          cirrus_solve_params* best) {
+    if (!grid || !params_ok(params) || !best) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        cirrus::SolveParams p;
+        to_internal(params, &p);
+        int li = p.level_iters, ci = p.coarsest_iters;
+        const int rc = cirrus::autotune_sweeps(*grid->g, p, S(stream), &li, &ci, nullptr);
+        *best = *params;
+        best->level_iters = li;
+        best->coarsest_iters = ci;
+        return map_rc(rc);
+    });
+}
+
 cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int reps, void* stream) {
     if (!grid || reps < 0) return CIRRUS_ERR_INVALID_ARGUMENT;
     auto& g = *grid->g;

@@ -296,6 +296,10 @@ int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s);
 int autotune(DevGrid& g, cudaStream_t s, int reps, std::string* report);
 // Destroys the grid's cached solve graphs (after a change of launch shapes).
 void drop_graphs(DevGrid& g);
+// Fastest converging (level_iters, coarsest_iters) for `base` on the grid's current right-hand
+// sides (autotune.cu); 5 if no candidate converged (base's values are returned).
+int autotune_sweeps(DevGrid& g, const SolveParams& base, cudaStream_t s, int* level_iters, int* coarsest_iters,
+                    std::string* report);
 // Copy the last solution to the host in FP64 (num_tiles*512 doubles, pool order).
 int solution_f64(DevGrid& g, double* host, cudaStream_t s);
 

@@ -264,6 +264,19 @@ cirrus_status cirrus_grid_get_solution_f64(cirrus_grid* grid, double* host, void
  * kernels x levels x shapes) launches.  reps <= 0 picks 20. */
 cirrus_status cirrus_grid_autotune(cirrus_grid* grid, int reps, void* stream);
 
+/* Sweep-count tuner (no counterpart in the reference, which always runs the caller's
+ * level_iters and coarsest_iters): solves the grid's current right-hand sides (channel 1, every
+ * instance) with `params` -- its precision, tolerance and pure-Neumann flag -- once per candidate
+ * (level_iters, coarsest_iters) in {(1,2), (1,4), (1,6), (1,10), (1,16), (1,24), (2,10)}, first
+ * untimed (building that solve's graph) then timed, and writes to *best a copy of params with the
+ * fastest pair whose solves all converged (CIRRUS_ERR_NOT_CONVERGED and params' own pair if none
+ * did).  Sweep counts change the preconditioner and so the iterates: the reference's bits come
+ * only from (1, 10).  Meant for the mixed-precision solver, whose result is set by its FP64
+ * tolerance.  Channel 1 is restored; channels 0 and 2-5 keep the last trial's values.
+ * Synchronises `stream`; holds one channel of scratch device memory while it runs. */
+cirrus_status cirrus_grid_autotune_sweeps(cirrus_grid* grid, const cirrus_solve_params* params, void* stream,
+                                          cirrus_solve_params* best);
+
 /* Measurement hook: launches one kernel of the solve `reps` times back to back on `stream` (no
  * synchronisation), so a caller can time it with its own CUDA events on that stream.  Uses
  * channels 2-5 (the solve's scratch) and overwrites them.  level: the level of the per-level

@@ -175,6 +175,26 @@ def test_every_launch_shape_gives_the_same_bits(built_cache):
     g.close()
 
 
+def test_sweep_tuner_picks_a_converging_pair_and_keeps_b(built_cache):
+    """The sweep-count tuner returns one of its candidate (level_iters, coarsest_iters) pairs,
+    leaves the right-hand sides bit-identical, and the mixed-precision batched solve with that
+    pair reaches the FP64 tolerance on every instance."""
+    bs = [built_cache(n) for n in ["sphere64_small", "ring64_small"]]
+    rhs = [rhs_of(b) for b in bs]
+    g = DeviceGrid([b.topology for b in bs])
+    for i, r in enumerate(rhs):
+        g.set_channel_instance(i, 1, r)
+    s = GMGSolver(precision=PRECISION_MIXED_FP64)
+    li, ci = s.autotune_sweeps(g)
+    assert (li, ci) in {(1, 2), (1, 4), (1, 6), (1, 10), (1, 16), (1, 24), (2, 10)}
+    for i, r in enumerate(rhs):
+        assert np.array_equal(bits(g.get_channel_instance(i, 1)), bits(r))
+    s.solve_batch(g, level_iters=li, coarsest_iters=ci)
+    for r in s.last_results:
+        assert r.status == 0 and r.true_rel_residual < 1e-6
+    g.close()
+
+
 def test_batch_of_64_random_spheres():
     """The batched configuration: 64 independent instances (64^3-256^3 effective, 1-4 levels,
     1-5 random spheres each) in one mixed-precision batched launch; every instance reaches a 1e-6
