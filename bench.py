@@ -342,7 +342,8 @@ def cpu_baseline(b, rhs, budget_s: float = 10.0, max_solves: int = 5) -> dict:
 def run_ours(args, world, rank, local, pg):
     import torch
 
-    from cirrus_b200 import B_CHANNEL, KERNEL_LAPLACIAN, TMP_CHANNEL, GMGSolver
+    from cirrus_b200 import (B_CHANNEL, KERNEL_GS_SWEEP, KERNEL_LAPLACIAN, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP,
+                             KERNEL_RESIDUAL_RESTRICT, TMP_CHANNEL, GMGSolver)
 
     K = args.batch
     b, g = build_batch(args.workload, batch_seeds(rank, K))
@@ -428,6 +429,29 @@ def run_ours(args, world, rank, local, pg):
     achieved = lap_bytes / (lap_ms * 1e-3) / 1e9
     biter = b_iter_bytes(b.tiles)
 
+    # the V-cycle's stencil kernels at the finest level, each against the survey's bytes per cell
+    # of the reference kernels it performs (fusion-credited: the pre-smoother is two colour
+    # sweeps, the prolongation kernel a prolongation + update and one colour)
+    typ, lvl = b.tiles[:, 4], b.tiles[:, 0]
+    lmax = int(lvl.max())
+    n_mg = int((((typ & 3) != 0) & (lvl == lmax)).sum()) * K * 512
+    n_gh = int((((typ & 4) != 0) & (lvl == lmax)).sum()) * K * 512
+    stencil = []
+    for name, kern, nbytes in [("k_presmooth (2 colours from x = 0)", KERNEL_PRESMOOTH, 18 * n_mg),
+                               ("k_residual_restrict", KERNEL_RESIDUAL_RESTRICT, 9.5 * (n_mg + n_gh)),
+                               ("k_prolong_sweep (prolongation + 1 colour)", KERNEL_PROLONG_SWEEP, 9.5 * (n_mg + n_gh) + 9 * n_mg),
+                               ("k_gs_sweep (1 colour)", KERNEL_GS_SWEEP, 9 * n_mg)]:
+        g.bench_launch(kern, lmax, 4, stream=sh)
+        e0.record(stream)
+        g.bench_launch(kern, lmax, reps, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        us = e0.elapsed_time(e1) / reps * 1e3
+        gbs = nbytes / (us * 1e-6) / 1e9
+        stencil.append({"kernel": name, "level": lmax, "cells": n_mg, "algorithmic_bytes_per_launch": int(nbytes),
+                        "launch_us": round(us, 2), "achieved": round(gbs, 1), "unit": "GB/s", "frac": round(gbs / peaks["hbm_gbs"], 4)})
+    g.copy_channel(TMP_CHANNEL, B_CHANNEL, sh)  # the kernel launches overwrote channels 2-5, TMP held b
+
     # the mixed-precision batched solver (FP32 V-cycle and matvec, FP64 residual and defect
     # correction) to the same 1e-6 on the same batch, FP64 true residual checked per instance
     from cirrus_b200 import PRECISION_MIXED_FP64
@@ -509,6 +533,7 @@ def run_ours(args, world, rank, local, pg):
                      "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peaks["source"],
                      "algorithmic_bytes_per_launch": int(lap_bytes), "bytes_per_cell": LAP_BYTES_PER_CELL,
                      "launch_us": round(lap_ms * 1e3, 3), "traffic": LAP_TRAFFIC_PER_LAUNCH.get((args.workload, K))},
+        "stencil_kernels": stencil,
         "whole_solve_bandwidth": {"value": round(biter * sum(iters_seen) / (total_ms * 1e-3) / 1e9, 1), "unit": "GB/s per GPU",
                                   "fusion_credited": True, "bytes_per_iteration_per_instance": int(biter),
                                   "frac_of_peak": round(biter * sum(iters_seen) / (total_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)},
