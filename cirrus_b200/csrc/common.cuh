@@ -69,6 +69,8 @@ struct Topo {
     const int* ghost_slot;       // n: index of a GHOST tile in the ghost list, else -1
     const int* ghost_child;      // n x 8: ghost slot of the GHOST child in each octant, else -1
     const int* ghost_list;       // GHOST tile of each ghost slot
+    const uint8_t* ghost_faces;  // per ghost slot: faces other tiles read (bit f: toward a non-GHOST
+                                 // neighbour), bit 6: every cell is read
     const int* inst;             // n: instance of each tile
     const float* inst_h0;        // per instance: voxel size of level 0, stored in FP32 as the reference does
     const float4* lconst;        // per instance x kLevelSlots levels: h, c1, c2, fast-path diagonal

@@ -326,6 +326,25 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
             }
         }
         g->n_lapface = n_face;
+        {
+            // faces of each GHOST tile whose p other tiles read: those toward a non-GHOST
+            // neighbour (its halo, and the face path's own values); a GHOST tile on the staged
+            // Laplacian path is read whole
+            std::vector<uint8_t> gf(std::max<size_t>(ghost.size(), 1), 0);
+            for (size_t q = 0; q < ghost.size(); q++) {
+                const int t = ghost[q];
+                uint8_t f6 = 0;
+                for (int f = 0; f < 6; f++) {
+                    const int nb = meta[t].nb[f];
+                    if (nb >= 0 && !(type[nb] & GHOST_T)) f6 |= (uint8_t)(1u << f);
+                }
+                gf[q] = f6;
+            }
+            for (int t : lapmain)
+                if (type[t] & GHOST_T) gf[gslot[t]] = 0x40;
+            CK(cudaMalloc(&g->d_ghost_faces, gf.size()));
+            CK(cudaMemcpy(g->d_ghost_faces, gf.data(), gf.size(), cudaMemcpyHostToDevice));
+        }
         g->n_lapitems = (int)lapitems.size();
         if (!lapitems.empty()) {
             if (ghost.size() >= (1u << 25)) {
@@ -565,6 +584,7 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
     g->topo.fcls = g->d_fcls;
     g->topo.edge = g->d_edge;
     g->topo.ghost_slot = g->d_ghost_tables;
+    g->topo.ghost_faces = g->d_ghost_faces;
     g->topo.ghost_child = g->d_ghost_tables + n;
     g->topo.ghost_list = g->d_ghost;
     g->topo.inst = g->d_inst;
@@ -591,6 +611,7 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_ghost_tables);
     cudaFree(g->d_gacc);
     cudaFree(g->d_lapitems);
+    cudaFree(g->d_ghost_faces);
     cudaFree(g->d_rrmain);
     cudaFree(g->d_rritems);
     cudaFree(g->d_prmain);

@@ -726,11 +726,15 @@ __device__ __forceinline__ bool chunk_reduce_and_elect(double a, double b, doubl
 // octant holding the four cells (i, j, k0..k0+3) of vector qv of LEAF tile `tile`: the 2x2x2
 // children of each cell take its new value p where child and parent cell are INTERIOR, 0
 // elsewhere.  Every GHOST tile is the child of a LEAF tile, so the kernels that write p on LEAF
-// tiles keep p valid on all GHOST tiles and the Laplacian reads it there directly.
+// tiles keep p valid on the GHOST tiles and the fused Laplacian reads it there directly.  Only
+// the cells other tiles read are written: the faces towards non-GHOST neighbours (their halos and
+// the Laplacian's face path), or every cell of a GHOST tile on the staged path (ghost_faces).
 __device__ __forceinline__ void push_to_ghost_child(const Topo& tp, float* P, int tile, int qv, const V4<float>& p, uint32_t ct4) {
     const int i = qv >> 4, j = (qv >> 1) & 7, k0 = (qv & 1) * 4;
     const int gs = tp.ghost_child[(size_t)tile * 8 + ((i >> 2) | ((j >> 2) << 1) | ((k0 >> 2) << 2))];
     if (gs < 0) return;
+    const uint32_t faces = tp.ghost_faces[gs];
+    if (faces == 0) return;
     const int gt = tp.ghost_list[gs];
     float pv[4];
 #pragma unroll
@@ -739,16 +743,25 @@ __device__ __forceinline__ void push_to_ghost_child(const Topo& tp, float* P, in
     for (int di = 0; di < 2; di++)
 #pragma unroll
         for (int dj = 0; dj < 2; dj++) {
-            const size_t row = (size_t)gt * kTileCells + (2 * (i & 3) + di) * 64 + (2 * (j & 3) + dj) * 8;
-            const uint2 cc = *reinterpret_cast<const uint2*>(tp.ctype + row);
-            V4<float> lo, hi;
+            const int fi = 2 * (i & 3) + di, fj = 2 * (j & 3) + dj;
+            const size_t row = (size_t)gt * kTileCells + fi * 64 + fj * 8;
+            const bool whole = (faces & 0x40u) || ((faces & 1u) && fi == 0) || ((faces & 2u) && fi == 7) || ((faces & 4u) && fj == 0) ||
+                               ((faces & 8u) && fj == 7);
+            if (whole) {
+                const uint2 cc = *reinterpret_cast<const uint2*>(tp.ctype + row);
+                V4<float> lo, hi;
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                lo.v[k] = ((cc.x >> (8 * k)) & INTERIOR_C) ? pv[k >> 1] : 0.f;
-                hi.v[k] = ((cc.y >> (8 * k)) & INTERIOR_C) ? pv[2 + (k >> 1)] : 0.f;
+                for (int k = 0; k < 4; k++) {
+                    lo.v[k] = ((cc.x >> (8 * k)) & INTERIOR_C) ? pv[k >> 1] : 0.f;
+                    hi.v[k] = ((cc.y >> (8 * k)) & INTERIOR_C) ? pv[2 + (k >> 1)] : 0.f;
+                }
+                st4(P + row, lo);
+                st4(P + row + 4, hi);
+            } else {
+                // only the row's end cells can lie on a read face (z- at k = 0, z+ at k = 7)
+                if (faces & 16u) P[row] = (tp.ctype[row] & INTERIOR_C) ? pv[0] : 0.f;
+                if (faces & 32u) P[row + 7] = (tp.ctype[row + 7] & INTERIOR_C) ? pv[3] : 0.f;
             }
-            st4(P + row, lo);
-            st4(P + row + 4, hi);
         }
 }
 

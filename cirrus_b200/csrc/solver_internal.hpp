@@ -92,6 +92,7 @@ struct DevGrid {
     int* d_edge = nullptr;       // n x 12 same-level edge neighbours, -1 if absent
     int* d_ghost_tables = nullptr;  // ghost slot per tile (n) | ghost slot per child octant (n x 8)
     float* d_gacc = nullptr;        // per GHOST tile: 64 partial sums of its A p (fused Laplacian)
+    uint8_t* d_ghost_faces = nullptr;  // per GHOST tile: faces whose p other tiles read (Topo::ghost_faces)
     float* d_xpre = nullptr;        // n x 512: pre-smoothed x of the fused V-cycle (read by the upstroke)
     void** d_tile_ptrs = nullptr;  // optional external array-of-tiles storage (interop)
     int* d_lists = nullptr;
