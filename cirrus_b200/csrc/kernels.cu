@@ -1041,7 +1041,9 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
     case 0: laplacian_shape<2, 1>(g, X, Y, S, s); break;
     case 1: laplacian_shape<2, 2>(g, X, Y, S, s); break;
     case 2: laplacian_shape<1, 4>(g, X, Y, S, s); break;
-    default: laplacian_shape<2, 4>(g, X, Y, S, s); break;
+    case 3: laplacian_shape<2, 4>(g, X, Y, S, s); break;
+    case 4: laplacian_shape<1, 1>(g, X, Y, S, s); break;
+    default: laplacian_shape<1, 2>(g, X, Y, S, s); break;
     }
 }
 
@@ -1063,7 +1065,9 @@ void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, 
     case 0: gs_sweep_shape<2, 1>(g, level, X, R, color, S, s); break;
     case 1: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s); break;
     case 2: gs_sweep_shape<1, 4>(g, level, X, R, color, S, s); break;
-    default: gs_sweep_shape<2, 4>(g, level, X, R, color, S, s); break;
+    case 3: gs_sweep_shape<2, 4>(g, level, X, R, color, S, s); break;
+    case 4: gs_sweep_shape<1, 1>(g, level, X, R, color, S, s); break;
+    default: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s); break;
     }
 }
 
@@ -1100,7 +1104,9 @@ void residual_restrict(const DevGrid& g, int level, const float* X, const float*
     case 0: residual_shape<2, 1>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     case 1: residual_shape<2, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     case 2: residual_shape<1, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
-    default: residual_shape<2, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    case 3: residual_shape<2, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    case 4: residual_shape<1, 1>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    default: residual_shape<1, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     }
 }
 

@@ -593,7 +593,9 @@ void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const S
     case 0: presmooth_shape<2, 1>(g, level, XP, RHS, S, s); break;
     case 1: presmooth_shape<2, 2>(g, level, XP, RHS, S, s); break;
     case 2: presmooth_shape<1, 4>(g, level, XP, RHS, S, s); break;
-    default: presmooth_shape<2, 4>(g, level, XP, RHS, S, s); break;
+    case 3: presmooth_shape<2, 4>(g, level, XP, RHS, S, s); break;
+    case 4: presmooth_shape<1, 1>(g, level, XP, RHS, S, s); break;
+    default: presmooth_shape<1, 2>(g, level, XP, RHS, S, s); break;
     }
 }
 
@@ -616,7 +618,9 @@ void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const
     case 0: prolong_shape<2, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     case 1: prolong_shape<2, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     case 2: prolong_shape<1, 4>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
-    default: prolong_shape<1, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    case 3: prolong_shape<1, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    case 4: prolong_shape<1, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    default: prolong_shape<4, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     }
 }
 
