@@ -25,10 +25,15 @@ float time_graph(F launch, int reps, cudaStream_t s) {
         cudaEventCreate(&a);
         cudaEventCreate(&b);
         cudaGraphLaunch(exec, s);  // warm
-        cudaEventRecord(a, s);
-        cudaGraphLaunch(exec, s);
-        cudaEventRecord(b, s);
-        if (cudaEventSynchronize(b) == cudaSuccess) cudaEventElapsedTime(&ms, a, b);
+        // the best of three timed graph launches (transients on a shared GPU only add time)
+        for (int k = 0; k < 3; k++) {
+            cudaEventRecord(a, s);
+            cudaGraphLaunch(exec, s);
+            cudaEventRecord(b, s);
+            float t = -1.f;
+            if (cudaEventSynchronize(b) == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+            if (t > 0.f && (ms < 0.f || t < ms)) ms = t;
+        }
         cudaEventDestroy(a);
         cudaEventDestroy(b);
         cudaGraphExecDestroy(exec);

@@ -155,8 +155,8 @@ __device__ __forceinline__ void ghost_face_sum(const Topo& tp, const float* __re
 // coupled face of a face-path GHOST tile); the others take `list` (LEAF tiles and GHOST tiles
 // coupled inside), staged with asynchronous copies, NT per 128-thread group.  Row entries in
 // neither are constant zeros (set when the grid is created).
-template <int TPB, int NT>
-__global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
+template <int TPB, int NT, int MINB = 1>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
                                                                int nitems, int item_blocks,
                                                                const float* __restrict__ X, float* __restrict__ Y,
                                                                float* __restrict__ GACC, const Scalars* __restrict__ S) {
@@ -265,8 +265,8 @@ __global__ void __launch_bounds__(64) k_accumulate_ghosts(Topo tp, const int* __
 // x += (b - A x) / D on INTERIOR cells.
 // The tiles of a CTA are NT groups of TPB consecutive list entries, one 128-thread group per
 // tile, all staged with asynchronous copies before any is computed (NT tiles per group in flight).
-template <int TPB, int NT>
-__global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
+template <int TPB, int NT, int MINB = 1>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
                                                         const float* __restrict__ R, int color, const Scalars* __restrict__ S) {
     pdl_entry();
     extern __shared__ __align__(16) unsigned char gs_smem[];
@@ -412,8 +412,8 @@ __device__ __forceinline__ void ghost_face_restrict(const Topo& tp, const float*
 // (times one_over_alpha).  The staged path takes tiles list[0..n) (or first..first+n when list is
 // null); the first item_blocks CTAs take face-path GHOST cells (ghost_face_restrict), one per
 // thread.
-template <int TPB, int NT>
-__global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int first, const int* __restrict__ list, int n,
+template <int TPB, int NT, int MINB = 1>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_residual_restrict(Topo tp, int first, const int* __restrict__ list, int n,
                                                                  const int4* __restrict__ items, int nitems, int item_blocks,
                                                                  const float* __restrict__ X, const float* RHS, float* C,
                                                                  float one_over_alpha, const Scalars* __restrict__ S) {
@@ -1026,11 +1026,11 @@ template void propagate_ghosts<float>(const DevGrid&, float*, const Scalars*, cu
 template void full_laplacian<float>(const DevGrid&, float*, float*, const Scalars*, cudaStream_t);
 template void full_laplacian<double>(const DevGrid&, double*, double*, const Scalars*, cudaStream_t);
 
-template <int TPB, int NT>
+template <int TPB, int NT, int MINB = 1>
 void laplacian_shape(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s) {
     const int per = TPB * NT;
     const int item_blocks = (g.n_lapitems + 128 * TPB - 1) / (128 * TPB);
-    launch_kernel(k_laplacian_fused<TPB, NT>, item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
+    launch_kernel(k_laplacian_fused<TPB, NT, MINB>, item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
                   g.topo, g.d_lapmain, g.n_lapmain, g.d_lapitems, g.n_lapitems, item_blocks, X, Y, g.d_gacc, S);
 }
 
@@ -1043,17 +1043,18 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
     case 2: laplacian_shape<1, 4>(g, X, Y, S, s); break;
     case 3: laplacian_shape<2, 4>(g, X, Y, S, s); break;
     case 4: laplacian_shape<1, 1>(g, X, Y, S, s); break;
-    default: laplacian_shape<1, 2>(g, X, Y, S, s); break;
+    case 5: laplacian_shape<1, 2>(g, X, Y, S, s); break;
+    default: laplacian_shape<1, 1, 16>(g, X, Y, S, s); break;
     }
 }
 
 // Launch shapes of the staged kernels: TPB tiles per CTA side by side, NT tiles per 128-thread
 // group in flight.
-template <int TPB, int NT>
+template <int TPB, int NT, int MINB = 1>
 void gs_sweep_shape(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s) {
     const int n = g.mg_count[level];
     const int per = TPB * NT;
-    launch_kernel(k_gs_sweep<TPB, NT>, (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
+    launch_kernel(k_gs_sweep<TPB, NT, MINB>, (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
                   g.d_mg + g.mg_offset[level], n, X, R, color, S);
 }
 
@@ -1067,7 +1068,8 @@ void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, 
     case 2: gs_sweep_shape<1, 4>(g, level, X, R, color, S, s); break;
     case 3: gs_sweep_shape<2, 4>(g, level, X, R, color, S, s); break;
     case 4: gs_sweep_shape<1, 1>(g, level, X, R, color, S, s); break;
-    default: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s); break;
+    case 5: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s); break;
+    default: gs_sweep_shape<1, 1, 16>(g, level, X, R, color, S, s); break;
     }
 }
 
@@ -1083,7 +1085,7 @@ void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t
     for (int k = 0; k < nsweeps; k++) gs_sweep(g, level, X, R, (colors >> k) & 1, S, s);
 }
 
-template <int TPB, int NT>
+template <int TPB, int NT, int MINB = 1>
 void residual_shape(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha, const Scalars* S,
                     cudaStream_t s, bool ghosts_zero) {
     const int per = TPB * NT;
@@ -1092,7 +1094,7 @@ void residual_shape(const DevGrid& g, int level, const float* X, const float* RH
     const int nitems = ghosts_zero ? g.rri_cnt[level] : 0;
     const int4* items = ghosts_zero ? g.d_rritems + g.rri_off[level] : nullptr;
     const int item_blocks = (nitems + 128 * TPB - 1) / (128 * TPB);
-    launch_kernel(k_residual_restrict<TPB, NT>, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
+    launch_kernel(k_residual_restrict<TPB, NT, MINB>, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
                   g.level_first[level], list, n, items, nitems, item_blocks, X, RHS, C, one_over_alpha, S);
 }
 
@@ -1106,7 +1108,8 @@ void residual_restrict(const DevGrid& g, int level, const float* X, const float*
     case 2: residual_shape<1, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     case 3: residual_shape<2, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     case 4: residual_shape<1, 1>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
-    default: residual_shape<1, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    case 5: residual_shape<1, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    default: residual_shape<1, 1, 16>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     }
 }
 

@@ -73,8 +73,8 @@ struct __align__(16) PreStage {
 // GaussSeidelGMG(1, 0) on the mg tiles (LEAF|NONLEAF) of one level, x starting from 0; the
 // result goes to XP.  GHOST neighbours hold x = 0 on the way down (they are not smoothed).
 // NT tiles per 128-thread group are staged with asynchronous copies before any is computed.
-template <int TPB, int NT>
-__global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __restrict__ list, int n, float* XP,
+template <int TPB, int NT, int MINB = 1>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_presmooth(Topo tp, const int* __restrict__ list, int n, float* XP,
                                                          const float* __restrict__ RHS, const Scalars* __restrict__ S) {
     pdl_entry();
     extern __shared__ __align__(16) unsigned char pre_smem[];
@@ -236,8 +236,8 @@ __device__ __forceinline__ void ghost_face_prolong(const Topo& tp, float* Z, int
 // colour (1) of GaussSeidelGMG(1, 1), NT tiles per 128-thread group staged with asynchronous
 // copies; the first item_blocks CTAs prolongate GHOST face layers (ghost_face_prolong), two per
 // 128 threads.  Reads Z of the coarser level and XP of this level, writes Z of this level.
-template <int TPB, int NT>
-__global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, const int* __restrict__ list, int n,
+template <int TPB, int NT, int MINB = 1>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_prolong_sweep(Topo tp, const int* __restrict__ list, int n,
                                                              const int4* __restrict__ items, int nitems, int item_blocks, float* Z,
                                                              const float* __restrict__ XP, const float* __restrict__ RHS,
                                                              float prolong_coeff, const Scalars* __restrict__ S) {
@@ -577,11 +577,11 @@ namespace launch {
 
 constexpr int kTPB2 = 2;
 
-template <int TPB, int NT>
+template <int TPB, int NT, int MINB = 1>
 void presmooth_shape(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s) {
     const int n = g.mg_count[level];
     const int per = TPB * NT;
-    launch_kernel(k_presmooth<TPB, NT>, (n + per - 1) / per, 128 * TPB, sizeof(PreStage) * per, s, g.topo, g.d_mg + g.mg_offset[level], n,
+    launch_kernel(k_presmooth<TPB, NT, MINB>, (n + per - 1) / per, 128 * TPB, sizeof(PreStage) * per, s, g.topo, g.d_mg + g.mg_offset[level], n,
                   XP, RHS, S);
 }
 
@@ -595,17 +595,18 @@ void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const S
     case 2: presmooth_shape<1, 4>(g, level, XP, RHS, S, s); break;
     case 3: presmooth_shape<2, 4>(g, level, XP, RHS, S, s); break;
     case 4: presmooth_shape<1, 1>(g, level, XP, RHS, S, s); break;
-    default: presmooth_shape<1, 2>(g, level, XP, RHS, S, s); break;
+    case 5: presmooth_shape<1, 2>(g, level, XP, RHS, S, s); break;
+    default: presmooth_shape<1, 1, 16>(g, level, XP, RHS, S, s); break;
     }
 }
 
-template <int TPB, int NT>
+template <int TPB, int NT, int MINB = 1>
 void prolong_shape(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
                    cudaStream_t s) {
     const int n = g.pr_cnt[level], nitems = g.pri_cnt[level];
     const int per = TPB * NT;
     const int item_blocks = (nitems + 2 * TPB - 1) / (2 * TPB);
-    launch_kernel(k_prolong_sweep<TPB, NT>, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(ProStage) * per, s, g.topo,
+    launch_kernel(k_prolong_sweep<TPB, NT, MINB>, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(ProStage) * per, s, g.topo,
                   g.d_prmain + g.pr_off[level], n, g.d_pritems + g.pri_off[level], nitems, item_blocks, Z, XP, RHS, prolong_coeff, S);
 }
 
@@ -620,7 +621,8 @@ void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const
     case 2: prolong_shape<1, 4>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     case 3: prolong_shape<1, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     case 4: prolong_shape<1, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
-    default: prolong_shape<4, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    case 5: prolong_shape<4, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    default: prolong_shape<1, 1, 16>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     }
 }
 
