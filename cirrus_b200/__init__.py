@@ -228,7 +228,7 @@ class DeviceGrid:
         check(lib().cirrus_grid_autotune(self._h, reps, C.c_void_p(stream)), "cirrus_grid_autotune")
 
     def set_launch_shape(self, shape: int, kernel: int = -1, level: int = -1) -> None:
-        """Set the launch shape (0..6) of one staged stencil kernel (KERNEL_*, -1: all) on one
+        """Set the launch shape (0..7) of one staged stencil kernel (KERNEL_*, -1: all) on one
         level (-1: all); results are unchanged by the choice."""
         check(lib().cirrus_grid_set_launch_shape(self._h, kernel, level, shape), "cirrus_grid_set_launch_shape")
 

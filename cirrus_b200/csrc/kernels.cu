@@ -1044,7 +1044,8 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
     case 3: laplacian_shape<2, 4>(g, X, Y, S, s); break;
     case 4: laplacian_shape<1, 1>(g, X, Y, S, s); break;
     case 5: laplacian_shape<1, 2>(g, X, Y, S, s); break;
-    default: laplacian_shape<1, 1, 16>(g, X, Y, S, s); break;
+    case 6: laplacian_shape<1, 1, 16>(g, X, Y, S, s); break;
+    default: laplacian_shape<1, 1, 12>(g, X, Y, S, s); break;
     }
 }
 
@@ -1069,7 +1070,8 @@ void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, 
     case 3: gs_sweep_shape<2, 4>(g, level, X, R, color, S, s); break;
     case 4: gs_sweep_shape<1, 1>(g, level, X, R, color, S, s); break;
     case 5: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s); break;
-    default: gs_sweep_shape<1, 1, 16>(g, level, X, R, color, S, s); break;
+    case 6: gs_sweep_shape<1, 1, 16>(g, level, X, R, color, S, s); break;
+    default: gs_sweep_shape<1, 1, 12>(g, level, X, R, color, S, s); break;
     }
 }
 
@@ -1109,7 +1111,8 @@ void residual_restrict(const DevGrid& g, int level, const float* X, const float*
     case 3: residual_shape<2, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     case 4: residual_shape<1, 1>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     case 5: residual_shape<1, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
-    default: residual_shape<1, 1, 16>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    case 6: residual_shape<1, 1, 16>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    default: residual_shape<1, 1, 12>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     }
 }
 

@@ -56,7 +56,7 @@ struct GraphKey {
 // choice per kernel and level is made by the autotuner (autotune.cu) and is bit-neutral: every
 // shape computes each tile with the same operations.
 enum { KS_GS_SWEEP = 0, KS_PRESMOOTH = 1, KS_PROLONG = 2, KS_RESIDUAL = 3, KS_LAPLACIAN = 4, KS_COUNT = 5 };
-constexpr int kNumShapes = 7;
+constexpr int kNumShapes = 8;
 
 // A contiguous run of one instance's tiles inside the merged pool: tiles local..local+count of
 // the instance's all-tiles order are global..global+count (one run per level).

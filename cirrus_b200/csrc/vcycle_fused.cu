@@ -596,7 +596,8 @@ void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const S
     case 3: presmooth_shape<2, 4>(g, level, XP, RHS, S, s); break;
     case 4: presmooth_shape<1, 1>(g, level, XP, RHS, S, s); break;
     case 5: presmooth_shape<1, 2>(g, level, XP, RHS, S, s); break;
-    default: presmooth_shape<1, 1, 16>(g, level, XP, RHS, S, s); break;
+    case 6: presmooth_shape<1, 1, 16>(g, level, XP, RHS, S, s); break;
+    default: presmooth_shape<1, 1, 12>(g, level, XP, RHS, S, s); break;
     }
 }
 
@@ -622,7 +623,8 @@ void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const
     case 3: prolong_shape<1, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     case 4: prolong_shape<1, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     case 5: prolong_shape<4, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
-    default: prolong_shape<1, 1, 16>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    case 6: prolong_shape<1, 1, 16>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    default: prolong_shape<1, 1, 12>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     }
 }
 

@@ -298,7 +298,7 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
  * level 0), shape in [0, CIRRUS_NUM_LAUNCH_SHAPES).  Lets a caller reuse tuned shapes for grids
  * of the same structure or pin one.  Shapes never change results.  No counterpart in the
  * reference. */
-#define CIRRUS_NUM_LAUNCH_SHAPES 7
+#define CIRRUS_NUM_LAUNCH_SHAPES 8
 cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape);
 cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int level, int* shape);
 

@@ -152,14 +152,14 @@ def test_autotune_changes_timing_not_results(built_cache):
 
 
 def test_every_launch_shape_gives_the_same_bits(built_cache):
-    """Each of the seven launch shapes of the staged kernels (tiles per CTA x tiles in flight),
+    """Each of the eight launch shapes of the staged kernels (tiles per CTA x tiles in flight),
     pinned for every kernel and level, gives the solve of the default shapes bit for bit."""
     bs = [built_cache(n) for n in ["sphere64_small", "ring64_small"]]
     rhs = [rhs_of(b) for b in bs]
     g = DeviceGrid([b.topology for b in bs])
     s = GMGSolver()
     out = []
-    for shape in (None, 0, 1, 2, 3, 4, 5, 6):
+    for shape in (None, 0, 1, 2, 3, 4, 5, 6, 7):
         if shape is not None:
             g.set_launch_shape(shape)
             assert g.get_launch_shape(KERNEL_PROLONG_SWEEP, 1) == shape
