@@ -155,8 +155,8 @@ __device__ __forceinline__ void ghost_face_sum(const Topo& tp, const float* __re
 // coupled face of a face-path GHOST tile); the others take `list` (LEAF tiles and GHOST tiles
 // coupled inside), staged with asynchronous copies, NT per 128-thread group.  Row entries in
 // neither are constant zeros (set when the grid is created).
-template <int TPB, int NT, int MINB = 1>
-__global__ void __launch_bounds__(128 * TPB, MINB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
+template <int TPB, int NT>
+__device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
                                                                int nitems, int item_blocks,
                                                                const float* __restrict__ X, float* __restrict__ Y,
                                                                float* __restrict__ GACC, const Scalars* __restrict__ S) {
@@ -225,7 +225,26 @@ __global__ void __launch_bounds__(128 * TPB, MINB) k_laplacian_fused(Topo tp, co
 #pragma unroll
                 for (int kk = 0; kk < 2; kk++) sum += gsum[(fi + ii) * 64 + (fj + jj) * 8 + (fk + kk)];
         GACC[(size_t)tp.ghost_slot[tile[u]] * 64 + t] = sum;
-    }
+    }}
+template <int TPB, int NT>
+__global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
+                                                               int nitems, int item_blocks,
+                                                               const float* __restrict__ X, float* __restrict__ Y,
+                                                               float* __restrict__ GACC, const Scalars* __restrict__ S) {
+    k_laplacian_fused_body<TPB, NT>(tp, list, n, items, nitems, item_blocks, X, Y, GACC, S);
+}
+// the same kernel with at least MINB CTAs per SM (registers capped to fit)
+template <int TPB, int NT, int MINB>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_laplacian_fused_occ(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
+                                                               int nitems, int item_blocks,
+                                                               const float* __restrict__ X, float* __restrict__ Y,
+                                                               float* __restrict__ GACC, const Scalars* __restrict__ S) {
+    k_laplacian_fused_body<TPB, NT>(tp, list, n, items, nitems, item_blocks, X, Y, GACC, S);
+}
+template <int TPB, int NT, int MINB>
+constexpr auto k_laplacian_fused_shape() {
+    if constexpr (MINB == 0) return &k_laplacian_fused<TPB, NT>;
+    else return &k_laplacian_fused_occ<TPB, NT, MINB>;
 }
 
 // AccumulateToParents128Kernel on GHOST tiles, additive, coefficient 1, all cell types
@@ -265,8 +284,8 @@ __global__ void __launch_bounds__(64) k_accumulate_ghosts(Topo tp, const int* __
 // x += (b - A x) / D on INTERIOR cells.
 // The tiles of a CTA are NT groups of TPB consecutive list entries, one 128-thread group per
 // tile, all staged with asynchronous copies before any is computed (NT tiles per group in flight).
-template <int TPB, int NT, int MINB = 1>
-__global__ void __launch_bounds__(128 * TPB, MINB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
+template <int TPB, int NT>
+__device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__ list, int n, float* X,
                                                         const float* __restrict__ R, int color, const Scalars* __restrict__ S) {
     pdl_entry();
     extern __shared__ __align__(16) unsigned char gs_smem[];
@@ -297,7 +316,22 @@ __global__ void __launch_bounds__(128 * TPB, MINB) k_gs_sweep(Topo tp, const int
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ts.mask + t * 4);
         st4(X + (size_t)tile[u] * kTileCells + t * 4,
             colour_update(ts.xs, ts.hx, t, mask4, (pre[u].fcls >> 12) & 0xfffu, L, ld4(ts.b + t * 4), color));
-    }
+    }}
+template <int TPB, int NT>
+__global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
+                                                        const float* __restrict__ R, int color, const Scalars* __restrict__ S) {
+    k_gs_sweep_body<TPB, NT>(tp, list, n, X, R, color, S);
+}
+// the same kernel with at least MINB CTAs per SM (registers capped to fit)
+template <int TPB, int NT, int MINB>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_gs_sweep_occ(Topo tp, const int* __restrict__ list, int n, float* X,
+                                                        const float* __restrict__ R, int color, const Scalars* __restrict__ S) {
+    k_gs_sweep_body<TPB, NT>(tp, list, n, X, R, color, S);
+}
+template <int TPB, int NT, int MINB>
+constexpr auto k_gs_sweep_shape() {
+    if constexpr (MINB == 0) return &k_gs_sweep<TPB, NT>;
+    else return &k_gs_sweep_occ<TPB, NT, MINB>;
 }
 
 // A whole sequence of colour sweeps over a small level inside one CTA (used for the coarsest
@@ -412,8 +446,8 @@ __device__ __forceinline__ void ghost_face_restrict(const Topo& tp, const float*
 // (times one_over_alpha).  The staged path takes tiles list[0..n) (or first..first+n when list is
 // null); the first item_blocks CTAs take face-path GHOST cells (ghost_face_restrict), one per
 // thread.
-template <int TPB, int NT, int MINB = 1>
-__global__ void __launch_bounds__(128 * TPB, MINB) k_residual_restrict(Topo tp, int first, const int* __restrict__ list, int n,
+template <int TPB, int NT>
+__device__ __forceinline__ void k_residual_restrict_body(Topo tp, int first, const int* __restrict__ list, int n,
                                                                  const int4* __restrict__ items, int nitems, int item_blocks,
                                                                  const float* __restrict__ X, const float* RHS, float* C,
                                                                  float one_over_alpha, const Scalars* __restrict__ S) {
@@ -482,7 +516,26 @@ __global__ void __launch_bounds__(128 * TPB, MINB) k_residual_restrict(Topo tp, 
                            ((oct >> 2) & 1) * 4 + fk / 2;
         if (meta_type(m.packed) & GHOST_T) C[pid] += sum;
         else C[pid] = sum * one_over_alpha;
-    }
+    }}
+template <int TPB, int NT>
+__global__ void __launch_bounds__(128 * TPB) k_residual_restrict(Topo tp, int first, const int* __restrict__ list, int n,
+                                                                 const int4* __restrict__ items, int nitems, int item_blocks,
+                                                                 const float* __restrict__ X, const float* RHS, float* C,
+                                                                 float one_over_alpha, const Scalars* __restrict__ S) {
+    k_residual_restrict_body<TPB, NT>(tp, first, list, n, items, nitems, item_blocks, X, RHS, C, one_over_alpha, S);
+}
+// the same kernel with at least MINB CTAs per SM (registers capped to fit)
+template <int TPB, int NT, int MINB>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_residual_restrict_occ(Topo tp, int first, const int* __restrict__ list, int n,
+                                                                 const int4* __restrict__ items, int nitems, int item_blocks,
+                                                                 const float* __restrict__ X, const float* RHS, float* C,
+                                                                 float one_over_alpha, const Scalars* __restrict__ S) {
+    k_residual_restrict_body<TPB, NT>(tp, first, list, n, items, nitems, item_blocks, X, RHS, C, one_over_alpha, S);
+}
+template <int TPB, int NT, int MINB>
+constexpr auto k_residual_restrict_shape() {
+    if constexpr (MINB == 0) return &k_residual_restrict<TPB, NT>;
+    else return &k_residual_restrict_occ<TPB, NT, MINB>;
 }
 
 // ------------------------------------------------------------------ prolongation + update
@@ -1026,11 +1079,11 @@ template void propagate_ghosts<float>(const DevGrid&, float*, const Scalars*, cu
 template void full_laplacian<float>(const DevGrid&, float*, float*, const Scalars*, cudaStream_t);
 template void full_laplacian<double>(const DevGrid&, double*, double*, const Scalars*, cudaStream_t);
 
-template <int TPB, int NT, int MINB = 1>
+template <int TPB, int NT, int MINB = 0>
 void laplacian_shape(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s) {
     const int per = TPB * NT;
     const int item_blocks = (g.n_lapitems + 128 * TPB - 1) / (128 * TPB);
-    launch_kernel(k_laplacian_fused<TPB, NT, MINB>, item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
+    launch_kernel(k_laplacian_fused_shape<TPB, NT, MINB>(), item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
                   g.topo, g.d_lapmain, g.n_lapmain, g.d_lapitems, g.n_lapitems, item_blocks, X, Y, g.d_gacc, S);
 }
 
@@ -1051,11 +1104,11 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
 
 // Launch shapes of the staged kernels: TPB tiles per CTA side by side, NT tiles per 128-thread
 // group in flight.
-template <int TPB, int NT, int MINB = 1>
+template <int TPB, int NT, int MINB = 0>
 void gs_sweep_shape(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s) {
     const int n = g.mg_count[level];
     const int per = TPB * NT;
-    launch_kernel(k_gs_sweep<TPB, NT, MINB>, (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
+    launch_kernel(k_gs_sweep_shape<TPB, NT, MINB>(), (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
                   g.d_mg + g.mg_offset[level], n, X, R, color, S);
 }
 
@@ -1087,7 +1140,7 @@ void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t
     for (int k = 0; k < nsweeps; k++) gs_sweep(g, level, X, R, (colors >> k) & 1, S, s);
 }
 
-template <int TPB, int NT, int MINB = 1>
+template <int TPB, int NT, int MINB = 0>
 void residual_shape(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha, const Scalars* S,
                     cudaStream_t s, bool ghosts_zero) {
     const int per = TPB * NT;
@@ -1096,7 +1149,7 @@ void residual_shape(const DevGrid& g, int level, const float* X, const float* RH
     const int nitems = ghosts_zero ? g.rri_cnt[level] : 0;
     const int4* items = ghosts_zero ? g.d_rritems + g.rri_off[level] : nullptr;
     const int item_blocks = (nitems + 128 * TPB - 1) / (128 * TPB);
-    launch_kernel(k_residual_restrict<TPB, NT, MINB>, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
+    launch_kernel(k_residual_restrict_shape<TPB, NT, MINB>(), item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
                   g.level_first[level], list, n, items, nitems, item_blocks, X, RHS, C, one_over_alpha, S);
 }
 

@@ -73,8 +73,8 @@ struct __align__(16) PreStage {
 // GaussSeidelGMG(1, 0) on the mg tiles (LEAF|NONLEAF) of one level, x starting from 0; the
 // result goes to XP.  GHOST neighbours hold x = 0 on the way down (they are not smoothed).
 // NT tiles per 128-thread group are staged with asynchronous copies before any is computed.
-template <int TPB, int NT, int MINB = 1>
-__global__ void __launch_bounds__(128 * TPB, MINB) k_presmooth(Topo tp, const int* __restrict__ list, int n, float* XP,
+template <int TPB, int NT>
+__device__ __forceinline__ void k_presmooth_body(Topo tp, const int* __restrict__ list, int n, float* XP,
                                                          const float* __restrict__ RHS, const Scalars* __restrict__ S) {
     pdl_entry();
     extern __shared__ __align__(16) unsigned char pre_smem[];
@@ -182,7 +182,22 @@ __global__ void __launch_bounds__(128 * TPB, MINB) k_presmooth(Topo tp, const in
         st4(XP + (size_t)tile[u] * kTileCells + t * 4,
             colour_update(ps.xs, ps.hx, t, *reinterpret_cast<const uint32_t*>(ps.mask + t * 4), (fc[u] >> 12) & 0xfffu,
                           LevelConst<float>(lc[u]), ld4(ps.b + t * 4), 1));
-    }
+    }}
+template <int TPB, int NT>
+__global__ void __launch_bounds__(128 * TPB) k_presmooth(Topo tp, const int* __restrict__ list, int n, float* XP,
+                                                         const float* __restrict__ RHS, const Scalars* __restrict__ S) {
+    k_presmooth_body<TPB, NT>(tp, list, n, XP, RHS, S);
+}
+// the same kernel with at least MINB CTAs per SM (registers capped to fit)
+template <int TPB, int NT, int MINB>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_presmooth_occ(Topo tp, const int* __restrict__ list, int n, float* XP,
+                                                         const float* __restrict__ RHS, const Scalars* __restrict__ S) {
+    k_presmooth_body<TPB, NT>(tp, list, n, XP, RHS, S);
+}
+template <int TPB, int NT, int MINB>
+constexpr auto k_presmooth_shape() {
+    if constexpr (MINB == 0) return &k_presmooth<TPB, NT>;
+    else return &k_presmooth_occ<TPB, NT, MINB>;
 }
 
 // ---------------------------------------------------------------------------- up: prolongation + first colour
@@ -236,8 +251,8 @@ __device__ __forceinline__ void ghost_face_prolong(const Topo& tp, float* Z, int
 // colour (1) of GaussSeidelGMG(1, 1), NT tiles per 128-thread group staged with asynchronous
 // copies; the first item_blocks CTAs prolongate GHOST face layers (ghost_face_prolong), two per
 // 128 threads.  Reads Z of the coarser level and XP of this level, writes Z of this level.
-template <int TPB, int NT, int MINB = 1>
-__global__ void __launch_bounds__(128 * TPB, MINB) k_prolong_sweep(Topo tp, const int* __restrict__ list, int n,
+template <int TPB, int NT>
+__device__ __forceinline__ void k_prolong_sweep_body(Topo tp, const int* __restrict__ list, int n,
                                                              const int4* __restrict__ items, int nitems, int item_blocks, float* Z,
                                                              const float* __restrict__ XP, const float* __restrict__ RHS,
                                                              float prolong_coeff, const Scalars* __restrict__ S) {
@@ -396,7 +411,26 @@ __global__ void __launch_bounds__(128 * TPB, MINB) k_prolong_sweep(Topo tp, cons
             o = colour_update(ps.xs, ps.hx, t, *reinterpret_cast<const uint32_t*>(ps.mask + t * 4), (fc[u] >> 12) & 0xfffu,
                               LevelConst<float>(lc[u]), ld4(ps.b + t * 4), 1);
         st4(Z + (size_t)tile[u] * kTileCells + t * 4, o);
-    }
+    }}
+template <int TPB, int NT>
+__global__ void __launch_bounds__(128 * TPB) k_prolong_sweep(Topo tp, const int* __restrict__ list, int n,
+                                                             const int4* __restrict__ items, int nitems, int item_blocks, float* Z,
+                                                             const float* __restrict__ XP, const float* __restrict__ RHS,
+                                                             float prolong_coeff, const Scalars* __restrict__ S) {
+    k_prolong_sweep_body<TPB, NT>(tp, list, n, items, nitems, item_blocks, Z, XP, RHS, prolong_coeff, S);
+}
+// the same kernel with at least MINB CTAs per SM (registers capped to fit)
+template <int TPB, int NT, int MINB>
+__global__ void __launch_bounds__(128 * TPB, MINB) k_prolong_sweep_occ(Topo tp, const int* __restrict__ list, int n,
+                                                             const int4* __restrict__ items, int nitems, int item_blocks, float* Z,
+                                                             const float* __restrict__ XP, const float* __restrict__ RHS,
+                                                             float prolong_coeff, const Scalars* __restrict__ S) {
+    k_prolong_sweep_body<TPB, NT>(tp, list, n, items, nitems, item_blocks, Z, XP, RHS, prolong_coeff, S);
+}
+template <int TPB, int NT, int MINB>
+constexpr auto k_prolong_sweep_shape() {
+    if constexpr (MINB == 0) return &k_prolong_sweep<TPB, NT>;
+    else return &k_prolong_sweep_occ<TPB, NT, MINB>;
 }
 
 // Right-hand sides of GHOST tiles to 0 (the V-cycle's initialisation of them, src/GMGSolver.cu:393-396).
@@ -577,11 +611,11 @@ namespace launch {
 
 constexpr int kTPB2 = 2;
 
-template <int TPB, int NT, int MINB = 1>
+template <int TPB, int NT, int MINB = 0>
 void presmooth_shape(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s) {
     const int n = g.mg_count[level];
     const int per = TPB * NT;
-    launch_kernel(k_presmooth<TPB, NT, MINB>, (n + per - 1) / per, 128 * TPB, sizeof(PreStage) * per, s, g.topo, g.d_mg + g.mg_offset[level], n,
+    launch_kernel(k_presmooth_shape<TPB, NT, MINB>(), (n + per - 1) / per, 128 * TPB, sizeof(PreStage) * per, s, g.topo, g.d_mg + g.mg_offset[level], n,
                   XP, RHS, S);
 }
 
@@ -601,13 +635,13 @@ void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const S
     }
 }
 
-template <int TPB, int NT, int MINB = 1>
+template <int TPB, int NT, int MINB = 0>
 void prolong_shape(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
                    cudaStream_t s) {
     const int n = g.pr_cnt[level], nitems = g.pri_cnt[level];
     const int per = TPB * NT;
     const int item_blocks = (nitems + 2 * TPB - 1) / (2 * TPB);
-    launch_kernel(k_prolong_sweep<TPB, NT, MINB>, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(ProStage) * per, s, g.topo,
+    launch_kernel(k_prolong_sweep_shape<TPB, NT, MINB>(), item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(ProStage) * per, s, g.topo,
                   g.d_prmain + g.pr_off[level], n, g.d_pritems + g.pri_off[level], nitems, item_blocks, Z, XP, RHS, prolong_coeff, S);
 }
 
