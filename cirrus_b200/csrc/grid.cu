@@ -356,8 +356,8 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
             CK(cudaMemcpy(g->d_lapitems, lapitems.data(), sizeof(int4) * lapitems.size(), cudaMemcpyHostToDevice));
         }
         // the same split for the residual + restriction of the fused V-cycle, per level, from the
-        // multigrid masks: face-path GHOST tiles give one item per coarse cell (every parent cell
-        // receives its += in both paths)
+        // multigrid masks: face-path GHOST tiles give one item per coarse cell touching a coupled
+        // face
         std::vector<int> rrmain;
         std::vector<int4> rritems;
         g->rr_off.assign(num_layers, 0);
@@ -382,10 +382,17 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
                     rrmain.push_back(t);
                     continue;
                 }
+                // only the coarse cells touching a coupled face: the others' sums are +0, and the
+                // multigrid right-hand side copies of r are written without -0 under GHOST children
                 const int oct = (meta[t].packed >> 16) & 7;
-                for (int c = 0; c < 64; c++)
+                for (int c = 0; c < 64; c++) {
+                    const int ci = c / 16, cj = (c / 4) % 4, ck = c % 4;
+                    const uint32_t touch = (ci == 0 ? 1u : 0u) | (ci == 3 ? 2u : 0u) | (cj == 0 ? 4u : 0u) | (cj == 3 ? 8u : 0u) |
+                                           (ck == 0 ? 16u : 0u) | (ck == 3 ? 32u : 0u);
+                    if (!(touch & faces)) continue;
                     rritems.push_back(make_int4(t, c | (int)(faces << 6) | (int)(((fcls[t] >> 12) & 0xfffu) << 12) | (oct << 24), par[t],
                                                 g_inst[t] * kLevelSlots + level[t]));
+                }
             }
             g->rr_cnt[l] = (int)rrmain.size() - g->rr_off[l];
             g->rri_cnt[l] = (int)rritems.size() - g->rri_off[l];

@@ -818,6 +818,19 @@ __device__ __forceinline__ void push_to_ghost_child(const Topo& tp, float* P, in
         }
 }
 
+// The multigrid right-hand side copy of r for vector qv of LEAF tile `tile`.  Under a GHOST child
+// (a cell whose right-hand side the child's restriction adds to) -0 becomes +0: the reference
+// adds the child's 2x2x2 sum to every such cell, which turns -0 into +0 even where the sum is
+// +0, and the restriction's face path skips the cells whose sum is known to be +0.
+__device__ __forceinline__ V4<float> mg_rhs_copy(const Topo& tp, int tile, int qv, const V4<float>& r) {
+    const int i = qv >> 4, j = (qv >> 1) & 7, k0 = (qv & 1) * 4;
+    if (tp.ghost_child[(size_t)tile * 8 + ((i >> 2) | ((j >> 2) << 1) | ((k0 >> 2) << 2))] < 0) return r;
+    V4<float> c;
+#pragma unroll
+    for (int e = 0; e < 4; e++) c.v[e] = r.v[e] + 0.f;
+    return c;
+}
+
 // Per-instance reduction over the 4-cell vectors of LEAF tiles, one CTA per chunk (the chunk table
 // cuts every instance's leaf vectors into pieces of kChunkVecs).  OP selects the fused
 // elementwise work done while reducing:
@@ -851,7 +864,7 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
         } else if (OP == OP_INIT) {  // A = x, B = r, D = multigrid right-hand side (copy of r)
             st4(A + off, zero4<float>());
             const V4<float> r = ld4(B + off);
-            if (D) st4(D + off, r);
+            if (D) st4(D + off, mg_rhs_copy(tp, tile, v & 127, r));
             acc_a += dot4f(r, r);
         } else if (OP == OP_COPY_DOT) {  // A = z, B = r, C = p (also on the GHOST children)
             const V4<float> z = ld4(A + off);
@@ -871,7 +884,7 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
             }
             st4(A + off, x);
             st4(C + off, r);
-            st4(D + off, r);  // Ap is consumed; the channel now carries r as the multigrid right-hand side
+            st4(D + off, mg_rhs_copy(tp, tile, v & 127, r));  // Ap is consumed; the channel now carries r as the multigrid right-hand side
             acc_a += dot4f(r, r);
         } else if (OP == OP_PAP) {  // A = p, B = Ap, C = ghost partial sums: Ap += ghost sums; p.Ap
             const V4<float> p = ld4(A + off);
@@ -962,7 +975,7 @@ __global__ void __launch_bounds__(256) k_recenter(Topo tp, const int* __restrict
         for (int e = 0; e < 4; e++)
             if ((ct4 >> (8 * e)) & INTERIOR_C) r.v[e] = (float)((double)r.v[e] - mean);
         st4(R + off, r);
-        if (RC) st4(RC + off, r);
+        if (RC) st4(RC + off, mg_rhs_copy(tp, tile, (int)(v & 127), r));
     }
 }
 
