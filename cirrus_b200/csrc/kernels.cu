@@ -934,26 +934,28 @@ __global__ void __launch_bounds__(256) k_begin(Scalars* S, const InstParams* __r
 }
 
 // p = z + beta p on INTERIOR cells of LEAF tiles (src/GMGSolver.cu:642-653), per instance; the
-// GHOST children receive the new p (push_to_ghost_child).
+// GHOST children receive the new p (push_to_ghost_child).  One 128-thread group per tile, one
+// 4-cell vector per thread: the tile's values are loaded before its instance's state is read, so
+// the loads do not wait on that lookup.
 __global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict__ leaves, int nleaf, float* P,
                                                   const float* __restrict__ Z, const Scalars* S) {
     pdl_entry();
-    const size_t nv = (size_t)nleaf * 128;
-    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
-        const int tile = leaves[v >> 7];
-        const Scalars& Si = S[tp.inst[tile]];
-        if (Si.done) continue;
-        const float beta = (float)Si.beta;
-        const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
-        const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
-        V4<float> p = ld4(P + off);
-        const V4<float> z = ld4(Z + off);
+    const int q = (int)blockIdx.x * 2 + ((int)threadIdx.x >> 7);
+    if (q >= nleaf) return;
+    const int t = threadIdx.x & 127;
+    const int tile = leaves[q];
+    const size_t off = (size_t)tile * kTileCells + t * 4;
+    const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+    V4<float> p = ld4(P + off);
+    const V4<float> z = ld4(Z + off);
+    const Scalars& Si = S[tp.inst[tile]];
+    if (Si.done) return;
+    const float beta = (float)Si.beta;
 #pragma unroll
-        for (int e = 0; e < 4; e++)
-            if ((ct4 >> (8 * e)) & INTERIOR_C) p.v[e] = fmaf(beta, p.v[e], z.v[e]);
-        st4(P + off, p);
-        push_to_ghost_child(tp, P, tile, (int)(v & 127), p, ct4);
-    }
+    for (int e = 0; e < 4; e++)
+        if ((ct4 >> (8 * e)) & INTERIOR_C) p.v[e] = fmaf(beta, p.v[e], z.v[e]);
+    st4(P + off, p);
+    push_to_ghost_child(tp, P, tile, t, p, ct4);
 }
 
 // r -= mean on INTERIOR cells of LEAF tiles (ReCenterLeafVoxels, src/PoissonSolver.cu:356-368)
@@ -1249,8 +1251,9 @@ void begin_solve(const DevGrid& g, const SolveCtl& ctl, cudaStream_t s) {
 }
 
 void update_p(const DevGrid& g, float* P, const float* Z, cudaStream_t s) {
+    if (g.n_leaf == 0) return;
     ++g.launch_count;
-    launch_kernel(k_update_p, leaf_blocks(g), 256, 0, s, g.topo, g.d_leaf, g.n_leaf, P, Z, (const Scalars*)g.d_scalars);
+    launch_kernel(k_update_p, (g.n_leaf + 1) / 2, 256, 0, s, g.topo, g.d_leaf, g.n_leaf, P, Z, (const Scalars*)g.d_scalars);
 }
 
 void recenter(const DevGrid& g, float* R, float* RC, cudaStream_t s) {
