@@ -505,9 +505,11 @@ __global__ void __launch_bounds__(1024) k_bottom(Topo tp, const BottomInst* __re
     pdl_entry();
     extern __shared__ __align__(16) unsigned char bsm[];
     __shared__ BottomInst bi;
+    __shared__ float4 lcs[kBottomMaxLevels];  // the instance's level constants, read once
     const int inst = blockIdx.x;
     if (S && S[inst].done) return;
     if (threadIdx.x == 0) bi = insts[inst];
+    if (threadIdx.x < kBottomMaxLevels) lcs[threadIdx.x] = tp.lconst[inst * kLevelSlots + threadIdx.x];
     __syncthreads();
     const int nb = bi.nrec, cells = bi.cells;
     int4* T = reinterpret_cast<int4*>(bsm);  // base, parent-cell base, type | level << 8, tile
@@ -537,7 +539,7 @@ __global__ void __launch_bounds__(1024) k_bottom(Topo tp, const BottomInst* __re
     __syncthreads();
     for (int ph = 0; ph < prog.nphase; ph++) {
         const int op = prog.op[ph], level = prog.level[ph];
-        const LevelConst<float> L(tp.lconst[inst * kLevelSlots + level]);
+        const LevelConst<float> L(lcs[level]);
         const int sy = bi.sy[level], sz = bi.sz[level], first = bi.first[level];
         if (op == 1) {
             // one colour of GaussSeidelGMG on the level's LEAF|NONLEAF tiles; items are the 256 cells
