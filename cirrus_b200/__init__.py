@@ -177,6 +177,43 @@ class DeviceGrid:
         self.instance_tiles = [t.num_tiles for t in topos]
         self.tiles = topos[0].tiles() if len(topos) == 1 else None
 
+    @classmethod
+    def from_arrays(cls, h0: float, levels_log2_hash: Sequence[int], tiles5: np.ndarray, cell_types: np.ndarray,
+                    b: np.ndarray | None = None, x0: np.ndarray | None = None) -> "DeviceGrid":
+        """A device grid straight from a reference grid's arrays (cirrus_grid_create_from_desc):
+        tiles5 = (n, 5) int32 rows (level, x, y, z, type), level-major in the reference's order;
+        cell_types = (n, 512) uint8; optional b and x0 = (n, 512) float32."""
+        from ._native import GridDesc
+
+        t5 = np.ascontiguousarray(tiles5, dtype=np.int32)
+        n, L = t5.shape[0], len(levels_log2_hash)
+        counts = np.bincount(t5[:, 0], minlength=L).astype(np.int32)
+        coords = np.ascontiguousarray(t5[:, 1:4])
+        types = np.ascontiguousarray(t5[:, 4].astype(np.uint8))
+        ct = np.ascontiguousarray(cell_types, dtype=np.uint8)
+        log2 = (C.c_uint32 * L)(*levels_log2_hash)
+        d = GridDesc()
+        d.h0, d.num_layers, d.log2_hash = float(h0), L, log2
+        d.tiles_per_level = _ptr(counts, C.c_int32)
+        d.coords = _ptr(coords, C.c_int32)
+        d.types = _ptr(types, C.c_uint8)
+        d.cell_types = _ptr(ct, C.c_uint8)
+        keep = []
+        for name, arr in (("b", b), ("x0", x0)):
+            if arr is not None:
+                a = np.ascontiguousarray(arr, dtype=np.float32)
+                keep.append(a)
+                setattr(d, name, _ptr(a, C.c_float))
+        h = C.c_void_p()
+        check(lib().cirrus_grid_create_from_desc(C.byref(d), C.byref(h)), "cirrus_grid_create_from_desc")
+        self = cls.__new__(cls)
+        self._h = h
+        self.num_tiles = n
+        self.num_instances = 1
+        self.instance_tiles = [n]
+        self.tiles = t5
+        return self
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:

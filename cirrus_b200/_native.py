@@ -35,6 +35,20 @@ c_f64_p = C.POINTER(C.c_double)
 LEVEL_TARGET_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int)
 
 
+class GridDesc(C.Structure):
+    _fields_ = [
+        ("h0", C.c_double),
+        ("num_layers", C.c_int),
+        ("log2_hash", C.POINTER(C.c_uint32)),
+        ("tiles_per_level", C.POINTER(C.c_int32)),
+        ("coords", C.POINTER(C.c_int32)),
+        ("types", C.POINTER(C.c_uint8)),
+        ("cell_types", C.POINTER(C.c_uint8)),
+        ("b", C.POINTER(C.c_float)),
+        ("x0", C.POINTER(C.c_float)),
+    ]
+
+
 class SolveParams(C.Structure):
     _fields_ = [
         ("max_iters", C.c_int),
@@ -141,6 +155,7 @@ _PROTOS = {
     "cirrus_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), c_int_p, c_int_p,
                                       C.POINTER(C.c_longlong)]),
     "cirrus_grid_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "cirrus_grid_create_from_desc": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
     "cirrus_grid_autotune_sweeps": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveParams)]),
     "cirrus_grid_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "cirrus_grid_get_launch_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),

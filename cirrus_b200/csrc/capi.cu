@@ -227,6 +227,46 @@ cirrus_status cirrus_grid_create(const cirrus_topology* topo, cirrus_grid** out)
         return CIRRUS_OK;
     });
 }
+cirrus_status cirrus_grid_create_from_desc(const cirrus_grid_desc* d, cirrus_grid** out) {
+    if (!d || !out || d->num_layers <= 0 || !d->log2_hash || !d->tiles_per_level || !d->coords || !d->types || !d->cell_types)
+        return CIRRUS_ERR_INVALID_ARGUMENT;
+    long long n = 0;
+    for (int l = 0; l < d->num_layers; l++) {
+        if (d->tiles_per_level[l] < 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+        n += d->tiles_per_level[l];
+    }
+    if (n <= 0 || n > (1LL << 30)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    cirrus_topology* topo = nullptr;
+    cirrus_status st = cirrus_topology_create(d->num_layers, d->log2_hash, d->h0, &topo);
+    if (st != CIRRUS_OK) return st;
+    st = guard([&] {
+        std::vector<int32_t> t5((size_t)n * 5);
+        size_t q = 0;
+        for (int l = 0; l < d->num_layers; l++)
+            for (int k = 0; k < d->tiles_per_level[l]; k++, q++) {
+                t5[5 * q] = l;
+                t5[5 * q + 1] = d->coords[3 * q];
+                t5[5 * q + 2] = d->coords[3 * q + 1];
+                t5[5 * q + 3] = d->coords[3 * q + 2];
+                t5[5 * q + 4] = d->types[q];
+            }
+        cirrus_status r = cirrus_topology_import_tiles(topo, t5.data(), (int)n);
+        if (r == CIRRUS_OK) r = cirrus_topology_set_cell_types(topo, d->cell_types);
+        if (r == CIRRUS_OK) r = cirrus_grid_create(topo, out);
+        if (r == CIRRUS_OK && d->b) r = cirrus_grid_set_channel(*out, 1, d->b, nullptr);
+        if (r == CIRRUS_OK && d->x0) r = cirrus_grid_set_channel(*out, 0, d->x0, nullptr);
+        if (r == CIRRUS_OK && cudaStreamSynchronize(nullptr) != cudaSuccess) r = cuda_status();
+        if (r != CIRRUS_OK && *out) {
+            cirrus_grid_destroy(*out);
+            *out = nullptr;
+        }
+        return r;
+    });
+    cirrus_topology_destroy(topo);
+    return st;
+}
+
 cirrus_status cirrus_grid_create_batch(const cirrus_topology* const* topos, int count, cirrus_grid** out) {
     if (!topos || count <= 0 || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
     for (int i = 0; i < count; i++)

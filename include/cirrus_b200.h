@@ -112,6 +112,25 @@ cirrus_status cirrus_grid_instance_info(const cirrus_grid* grid, int instance, i
 cirrus_status cirrus_grid_set_channel_instance(cirrus_grid* grid, int instance, int channel, const float* host, void* stream);
 cirrus_status cirrus_grid_get_channel_instance(const cirrus_grid* grid, int instance, int channel, float* host, void* stream);
 void cirrus_grid_destroy(cirrus_grid* grid);
+/* Grid descriptor: a reference grid's content as plain arrays -- its tile list per level in the
+ * reference's compacted order (the dAllTiles order, src/HAGrid.h:538-556), tile types, cell types
+ * (CalcCellTypesFromLeafs applied, src/PoissonSolver.cu:7-61) and optionally b and x0.  The
+ * library builds its own neighbour, parent and child tables from the coordinates. */
+typedef struct cirrus_grid_desc {
+    double h0;                       /* voxel size of level 0 (HADeviceGrid's h0) */
+    int num_layers;
+    const uint32_t* log2_hash;       /* num_layers: log2 of each level's hash-table size */
+    const int32_t* tiles_per_level;  /* num_layers */
+    const int32_t* coords;           /* 3 int32 (x, y, z) per tile: level 0's tiles first */
+    const uint8_t* types;            /* per tile: CIRRUS_LEAF, CIRRUS_NONLEAF or CIRRUS_GHOST */
+    const uint8_t* cell_types;       /* 512 per tile */
+    const float* b;                  /* optional (NULL): 512 per tile, loaded into channel 1 */
+    const float* x0;                 /* optional (NULL): 512 per tile, loaded into channel 0 */
+} cirrus_grid_desc;
+/* One call from a descriptor to a device grid: cirrus_topology_create + _import_tiles +
+ * _set_cell_types + cirrus_grid_create (+ the channel uploads, synchronous).  Replaces building a
+ * HADeviceGrid tile by tile when the tiles already exist elsewhere. */
+cirrus_status cirrus_grid_create_from_desc(const cirrus_grid_desc* desc, cirrus_grid** out);
 cirrus_status cirrus_grid_num_tiles(const cirrus_grid* grid, int* num_tiles);
 /* Device bytes held by the grid. */
 cirrus_status cirrus_grid_device_bytes(const cirrus_grid* grid, size_t* bytes);
