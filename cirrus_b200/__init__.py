@@ -420,6 +420,15 @@ class GMGSolver:
         self.last_result = res[0]
         return [(r.iters, r.rel_residual) for r in res]
 
+    def damped_jacobi_solve(self, grid: DeviceGrid, verbose: bool = False, max_iters: int = 10, relative_tolerance: float = 1e-6,
+                            omega: float = 1.0, stream: int = 0) -> tuple[int, float]:
+        """GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x to channel 0;
+        returns (iterations, relative residual)."""
+        it, rel = C.c_int(), C.c_double()
+        check(lib().cirrus_damped_jacobi_solve(grid.handle, int(max_iters), float(relative_tolerance), float(omega), C.c_void_p(stream),
+                                               C.byref(it), C.byref(rel)), "cirrus_damped_jacobi_solve")
+        return it.value, rel.value
+
     def autotune_sweeps(self, grid: DeviceGrid, stream: int = 0, **kw) -> tuple[int, int]:
         """Time this solver's batched solve of the grid's current right-hand sides for each
         candidate (level_iters, coarsest_iters) and return the fastest pair that converged (pass

@@ -155,6 +155,8 @@ _PROTOS = {
     "cirrus_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), c_int_p, c_int_p,
                                       C.POINTER(C.c_longlong)]),
     "cirrus_grid_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "cirrus_damped_jacobi_solve": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_float, C.c_void_p, C.POINTER(C.c_int),
+                                             C.POINTER(C.c_double)]),
     "cirrus_grid_create_from_desc": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
     "cirrus_grid_autotune_sweeps": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveParams)]),
     "cirrus_grid_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),

@@ -581,6 +581,13 @@ cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int le
     return CIRRUS_OK;
 }
 
+cirrus_status cirrus_damped_jacobi_solve(cirrus_grid* grid, int max_iters, double relative_tolerance, float omega, void* stream,
+                                         int* iters, double* rel) {
+    if (!grid || !iters || !rel || max_iters < 0 || !(relative_tolerance >= 0)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (grid->g->num_inst != 1) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return map_rc(cirrus::damped_jacobi(*grid->g, max_iters, relative_tolerance, omega, S(stream), iters, rel)); });
+}
+
 cirrus_status cirrus_grid_autotune_sweeps(cirrus_grid* grid, const cirrus_solve_params* params, void* stream,
                                           cirrus_solve_params* best) {
     if (!grid || !params_ok(params) || !best) return CIRRUS_ERR_INVALID_ARGUMENT;

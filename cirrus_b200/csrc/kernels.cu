@@ -43,7 +43,9 @@ __global__ void __launch_bounds__(128) k_propagate_ghosts(Topo tp, const int* __
 // ------------------------------------------------------------------ Laplacian apply
 // NegativeLaplacianSameLevel128Kernel (src/GMGSolver.cu:145-194) on LEAF|GHOST tiles of all
 // levels with the tile types as stored (subtree level -1).
-template <class T, int TPB>
+// DIAG: the diagonal (the same sum over the face coefficients) instead of A x, as the
+// reference's calc_diag argument selects.
+template <class T, int TPB, bool DIAG = false>
 __global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __restrict__ list, int n, const T* __restrict__ X,
                                                          T* __restrict__ Y, const Scalars* __restrict__ S) {
     pdl_entry();
@@ -62,9 +64,10 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __r
     const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(tp.mask_lap + (size_t)tile * kTileCells + t * 4);
     const LevelConst<T> L((T)tile_h0(tp, tile), meta_level(m.packed));
     T out[4], dg[4];
-    neg_lap4<T, false, false>(sh[g].xs, sh[g].hx, t, mask4, tp.fcls[tile] & 0xfffu, L, out, dg);
+    neg_lap4<T, DIAG, false>(sh[g].xs, sh[g].hx, t, mask4, tp.fcls[tile] & 0xfffu, L, out, dg);
     V4<T> o;
-    o.v[0] = out[0]; o.v[1] = out[1]; o.v[2] = out[2]; o.v[3] = out[3];
+#pragma unroll
+    for (int e = 0; e < 4; e++) o.v[e] = DIAG ? dg[e] : out[e];
     st4(Y + (size_t)tile * kTileCells + t * 4, o);
 }
 
@@ -1072,11 +1075,15 @@ void propagate_ghosts(const DevGrid& g, T* X, const Scalars* S, cudaStream_t s) 
     launch_kernel(k_propagate_ghosts<T>, g.n_ghost, 128, 0, s, g.topo, g.d_ghost, g.n_ghost, X, S);
 }
 template <class T>
-void laplacian_tiles(const DevGrid& g, const T* X, T* Y, const Scalars* S, cudaStream_t s) {
+void laplacian_tiles(const DevGrid& g, const T* X, T* Y, const Scalars* S, cudaStream_t s, bool diag = false) {
     if (g.n_leafghost == 0) return;
     ++g.launch_count;
-    launch_kernel(k_laplacian<T, kTPB>, (g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.d_leafghost, g.n_leafghost,
-                  X, Y, S);
+    if (diag)
+        launch_kernel(k_laplacian<T, kTPB, true>, (g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.d_leafghost,
+                      g.n_leafghost, X, Y, S);
+    else
+        launch_kernel(k_laplacian<T, kTPB>, (g.n_leafghost + kTPB - 1) / kTPB, 128 * kTPB, 0, s, g.topo, g.d_leafghost,
+                      g.n_leafghost, X, Y, S);
 }
 template <class T>
 void accumulate_ghosts(const DevGrid& g, T* Y, const Scalars* S, cudaStream_t s) {
@@ -1089,6 +1096,13 @@ void full_laplacian(const DevGrid& g, T* X, T* Y, const Scalars* S, cudaStream_t
     propagate_ghosts<T>(g, X, S, s);
     laplacian_tiles<T>(g, X, Y, S, s);
     accumulate_ghosts<T>(g, Y, S, s);
+}
+// FullNegativeLaplacian(grid, x, D, calc_diag = true): x propagated to the GHOST tiles, the
+// diagonal of every LEAF|GHOST cell, the GHOST rows accumulated into their parents.
+void full_laplacian_diag(const DevGrid& g, float* X, float* D, cudaStream_t s) {
+    propagate_ghosts<float>(g, X, nullptr, s);
+    laplacian_tiles<float>(g, X, D, nullptr, s, true);
+    accumulate_ghosts<float>(g, D, nullptr, s);
 }
 template void propagate_ghosts<float>(const DevGrid&, float*, const Scalars*, cudaStream_t);
 template void full_laplacian<float>(const DevGrid&, float*, float*, const Scalars*, cudaStream_t);
@@ -1197,6 +1211,59 @@ void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const S
     if (blocks < 1) blocks = 1;
     ++g.launch_count;
     launch_kernel(k_vcycle_init, blocks, 256, 0, s, g.topo, g.n, X, RHS, F, S);
+}
+
+// dampedJacobiSolve's residual step (src/GMGSolver.cu:479-490): Ax = b - Ax on INTERIOR cells
+// of LEAF tiles (other cells keep A x).
+__global__ void __launch_bounds__(128) k_jacobi_residual(Topo tp, const int* __restrict__ leaves, int nleaf, const float* __restrict__ B,
+                                                         float* AX) {
+    pdl_entry();
+    const int q = blockIdx.x;
+    if (q >= nleaf) return;
+    const size_t off = (size_t)leaves[q] * kTileCells + threadIdx.x * 4;
+    const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+    const V4<float> b = ld4(B + off);
+    V4<float> ax = ld4(AX + off);
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+        if ((ct4 >> (8 * e)) & INTERIOR_C) ax.v[e] = b.v[e] - ax.v[e];
+    st4(AX + off, ax);
+}
+// dampedJacobiSolve's update (src/GMGSolver.cu:508-525): on INTERIOR cells of LEAF tiles
+// x += omega * r / D, or x = 0 where D is 0.
+__global__ void __launch_bounds__(128) k_jacobi_update(Topo tp, const int* __restrict__ leaves, int nleaf, float* X,
+                                                       const float* __restrict__ R, const float* __restrict__ D, float omega) {
+    pdl_entry();
+    const int q = blockIdx.x;
+    if (q >= nleaf) return;
+    const size_t off = (size_t)leaves[q] * kTileCells + threadIdx.x * 4;
+    const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+    const V4<float> r = ld4(R + off), d = ld4(D + off);
+    V4<float> x = ld4(X + off);
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+        if ((ct4 >> (8 * e)) & INTERIOR_C) x.v[e] = d.v[e] == 0.f ? 0.f : x.v[e] + __fdiv_rn(__fmul_rn(omega, r.v[e]), d.v[e]);
+    st4(X + off, x);
+}
+void jacobi_residual(const DevGrid& g, const float* B, float* AX, cudaStream_t s) {
+    if (g.n_leaf == 0) return;
+    ++g.launch_count;
+    launch_kernel(k_jacobi_residual, g.n_leaf, 128, 0, s, g.topo, g.d_leaf, g.n_leaf, B, AX);
+}
+void jacobi_update(const DevGrid& g, float* X, const float* R, const float* D, float omega, cudaStream_t s) {
+    if (g.n_leaf == 0) return;
+    ++g.launch_count;
+    launch_kernel(k_jacobi_update, g.n_leaf, 128, 0, s, g.topo, g.d_leaf, g.n_leaf, X, R, D, omega);
+}
+// a dot over an arbitrary tile list (the whole-grid reduction of cirrus_dot), result on the host
+double list_dot(const DevGrid& g, const float* A, const float* B, const int* list, int n, cudaStream_t s) {
+    if (n == 0) return 0.0;
+    ++g.launch_count;
+    k_leaf_dot<<<g.red_blocks, 256, 0, s>>>(list, n, A, B, g.d_dot, g.d_partials, g.d_counter);
+    double v = 0.0;
+    cudaMemcpyAsync(&v, &g.d_dot->gamma, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return v;
 }
 
 void init_stencil_attributes() {

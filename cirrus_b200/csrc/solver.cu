@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 
 namespace cirrus {
 
@@ -356,6 +357,31 @@ int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s) {
 // FP64 defect correction of every active instance: x64 accumulates FP32 PCG corrections e
 // solving A e = r, with r = b - A x64 formed in FP64 on the device; an instance stops when its
 // ||r||/||b|| < tol (FP64 true residual).  All instances still correcting share each inner solve.
+int damped_jacobi(DevGrid& g, int max_iters, double tol, float omega, cudaStream_t s, int* iters, double* rel) {
+    float *X = g.d_ch[kChX], *B = g.d_ch[kChB], *AX = g.d_ch[2], *D = g.d_ch[3];
+    cudaMemsetAsync(X, 0, (size_t)g.n * kTileCells * sizeof(float), s);  // x = 0 on LEAF|NONLEAF|GHOST tiles
+    const int n_mg = g.mg_offset.empty() ? 0 : g.mg_offset.back() + g.mg_count.back();
+    // ||b|| over LEAF|NONLEAF|GHOST tiles (src/GMGSolver.cu:467): the multigrid lists of all
+    // levels hold every LEAF and NONLEAF tile once
+    const double rhs_norm =
+        std::sqrt(launch::list_dot(g, B, B, g.d_mg, n_mg, s) + launch::list_dot(g, B, B, g.d_ghost, g.n_ghost, s));
+    const double threshold = std::max(tol * rhs_norm, std::numeric_limits<double>::min());
+    double res = rhs_norm;
+    int i = 0;
+    for (i = 0; i < max_iters; i++) {
+        launch::full_laplacian<float>(g, X, AX, nullptr, s);
+        launch::jacobi_residual(g, B, AX, s);
+        res = std::sqrt(launch::list_dot(g, AX, AX, g.d_leaf, g.n_leaf, s));
+        if (res < threshold) break;
+        launch::full_laplacian_diag(g, X, D, s);
+        launch::jacobi_update(g, X, AX, D, omega, s);
+    }
+    g.x64_valid = false;
+    *iters = i;
+    *rel = res / rhs_norm;
+    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : 2;
+}
+
 int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r, const InstRequest* req) {
     int rc = ensure_fp64(g);
     if (rc) return rc;

@@ -194,6 +194,13 @@ inline void launch_kernel(void (*k)(KArgs...), dim3 grid, dim3 block, size_t sme
 }
 // S (nullable): per-instance scalars; tiles of finished instances are skipped.
 template <class T> void full_laplacian(const DevGrid& g, T* X, T* Y, const Scalars* S, cudaStream_t s);
+// FullNegativeLaplacian with calc_diag: the diagonal of LEAF|GHOST cells, ghost rows accumulated.
+void full_laplacian_diag(const DevGrid& g, float* X, float* D, cudaStream_t s);
+// dampedJacobiSolve's residual (Ax = b - Ax) and update (x += omega r / D) on INTERIOR LEAF cells.
+void jacobi_residual(const DevGrid& g, const float* B, float* AX, cudaStream_t s);
+void jacobi_update(const DevGrid& g, float* X, const float* R, const float* D, float omega, cudaStream_t s);
+// Dot over the 4-cell vectors of the tiles in `list` (synchronises s; result on the host).
+double list_dot(const DevGrid& g, const float* A, const float* B, const int* list, int n, cudaStream_t s);
 // FullNegativeLaplacian as one launch; the ghost-to-parent sums are completed by OP_PAP.
 void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s);
 void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s);
@@ -288,6 +295,9 @@ struct InstRequest {
 int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r, const InstRequest* req = nullptr);
 // Mixed precision: FP64 defect correction around FP32 PCG solves.
 int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r, const InstRequest* req = nullptr);
+// GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x to channel 0,
+// channels 2 (residual) and 3 (diagonal) as the reference leaves them.  Single-instance grids.
+int damped_jacobi(DevGrid& g, int max_iters, double tol, float omega, cudaStream_t s, int* iters, double* rel);
 // FP64 true relative residual of the last solution of each instance against b (device FP32
 // channel): the FP64 x of a mixed-precision solve, else channel 0 widened to FP64.
 int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s);

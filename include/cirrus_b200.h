@@ -321,6 +321,15 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
 cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape);
 cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int level, int* shape);
 
+/* Replaces GMGSolver::dampedJacobiSolve(grid, verbose, max_iters, relative_tolerance, omega)
+ * (src/GMGSolver.cu:449-531; FluidEuler::project's commented-out alternative,
+ * src/FluidEuler.h:599): x = 0; per iteration r = b - A x on INTERIOR cells of LEAF tiles
+ * (channel 2), stop when ||r|| < relative_tolerance * ||b|| (||b|| over LEAF|NONLEAF|GHOST
+ * tiles), else D = the diagonal (channel 3) and x += omega * r / D.  b in channel 1, x to
+ * channel 0.  *iters and *rel: the reference's returned pair.  Grids of one instance. */
+cirrus_status cirrus_damped_jacobi_solve(cirrus_grid* grid, int max_iters, double relative_tolerance, float omega, void* stream,
+                                         int* iters, double* rel);
+
 /* FP64 true residual ||b - A x||/||b|| over INTERIOR cells of LEAF tiles for a given b (host,
  * num_tiles*512 floats) and the last solution (FP64 after a mixed-precision solve, else the
  * FP32 channel 0); one value per instance (rel holds num_instances doubles). */

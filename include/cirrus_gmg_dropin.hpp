@@ -71,6 +71,21 @@ public:
         return std::make_tuple(r.iters, sync_stride > 0 ? r.rel_residual : -1.0);
     }
 
+    /* GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x to channel 0,
+     * the last residual in channel 2 and the diagonal in channel 3 of LEAF|GHOST tiles (both
+     * channels keep their previous contents on NONLEAF tiles, as in the reference). */
+    std::tuple<int, double> dampedJacobiSolve(Grid& grid, bool verbose, int max_iters, double relative_tolerance, float omega) {
+        bind(grid);
+        for (int c : {1, 2, 3}) check(cirrus_grid_gather_tiles(cg_, c, channel_offset(c), nullptr), "gather");
+        int iters = 0;
+        double rel = 0.0;
+        check(cirrus_damped_jacobi_solve(cg_, max_iters, relative_tolerance, omega, nullptr, &iters, &rel), "cirrus_damped_jacobi_solve");
+        for (int c : {0, 2, 3}) check(cirrus_grid_scatter_tiles(cg_, c, channel_offset(c), nullptr), "scatter");
+        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cirrus_dropin: CUDA error");
+        if (verbose) std::printf("cirrus damped Jacobi: %d iterations, relative residual %.3e\n", iters, rel);
+        return std::make_tuple(iters, rel);
+    }
+
 private:
     using Info = typename std::decay<decltype(std::declval<Grid&>().hAllTiles[0])>::type;
     using Tile = typename std::decay<decltype(*std::declval<Info&>().mTilePtr)>::type;

@@ -445,6 +445,12 @@ struct Solver {
         lap_tiles(xc, yc, false);
         accumulate_ghosts(yc);
     }
+    // FullNegativeLaplacian(grid, x, y, calc_diag = true): the diagonal instead of A x
+    void full_lap_diag(int xc, int yc) {
+        propagate_ghosts(xc);
+        lap_tiles(xc, yc, true);
+        accumulate_ghosts(yc);
+    }
     // one red-black colour sweep on LEAF|NONLEAF tiles of 'level' (src/GMGSolver.cu:216-269)
     void gs_sweep(int level, int xc, int rc, int color) {
         Halo<T> H{f, C(xc), level};
@@ -565,6 +571,51 @@ struct Solver {
             }
         }
         return total;
+    }
+    // Dot over the tiles whose type is in `types` (same 4-cell FP32 partials widened to FP64)
+    double dot_types(int a, int b, uint8_t types) {
+        const T* A = C(a); const T* B = C(b);
+        double total = 0;
+        for (int t = 0; t < f.n; t++) {
+            if (!(f.type[t] & types)) continue;
+            for (int g = 0; g < 128; g++) {
+                const T* p = A + (size_t)t * NCELL + 4 * g;
+                const T* q = B + (size_t)t * NCELL + 4 * g;
+                T s = fmaT<T>(p[0], q[0], p[1] * q[1]);
+                s = fmaT<T>(p[2], q[2], s);
+                s = fmaT<T>(p[3], q[3], s);
+                total += (double)s;
+            }
+        }
+        return total;
+    }
+    // GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x in 0, the
+    // residual in 2 and the diagonal in 3.  Returns iterations; writes the relative residual.
+    int damped_jacobi(int max_iters, double tol, T omega, double& rel) {
+        T* x = C(0); const T* b = C(1); T* ax = C(2); const T* d = C(3);
+        for (int t = 0; t < f.n; t++)
+            if (f.type[t] & (LEAF | NONLEAF | GHOST))
+                for (int o = 0; o < NCELL; o++) x[(size_t)t * NCELL + o] = 0;
+        const double rhs_norm = std::sqrt(dot_types(1, 1, LEAF | NONLEAF | GHOST));
+        const double threshold = std::max(tol * rhs_norm, DBL_MIN);
+        double res = rhs_norm;
+        int i = 0;
+        for (i = 0; i < max_iters; i++) {
+            full_lap(0, 2);
+            leaf_cells([&](size_t id) { if (f.ctype[id] & INTERIOR) ax[id] = b[id] - ax[id]; });
+            res = std::sqrt(dot_types(2, 2, LEAF));
+            if (res < threshold) break;
+            full_lap_diag(0, 3);
+            leaf_cells([&](size_t id) {
+                if (!(f.ctype[id] & INTERIOR)) return;
+                if (d[id] == 0) { x[id] = 0; return; }
+                T q = omega * ax[id];  // no contraction: -ffp-contract=off
+                q = q / d[id];
+                x[id] = x[id] + q;
+            });
+        }
+        rel = res / rhs_norm;
+        return i;
     }
     // MeanAsync + ReCenterLeafVoxels (src/PoissonGrid.cu:231-325, src/PoissonSolver.cu:356-368)
     void recenter(int c) {
@@ -1028,6 +1079,11 @@ int ocx_solve(void* h, int prec, int max_iters, double tol, int level_iters, int
     if (hist_len) *hist_len = (int)hist.size();
     if (history) for (int i = 0; i < (int)hist.size() && i < hist_cap; i++) history[i] = hist[i];
     return it;
+}
+// GMGSolver::dampedJacobiSolve; b in channel 1, x out in channel 0.  Returns iterations.
+int ocx_damped_jacobi(void* h, int prec, int max_iters, double tol, double omega, double* rel) {
+    OCX* o = (OCX*)h;
+    return prec == 0 ? S32(o).damped_jacobi(max_iters, tol, (float)omega, *rel) : S64(o).damped_jacobi(max_iters, tol, omega, *rel);
 }
 int ocx_num_threads() { return omp_get_max_threads(); }
 void ocx_set_threads(int n) { omp_set_num_threads(n); }

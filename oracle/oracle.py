@@ -44,7 +44,7 @@ def build_ref(force: bool = False, reference_dir: str | None = None) -> Path | N
     ref = Path(reference_dir or os.environ.get("CIRRUS_REFERENCE_DIR", "/root/reference"))
     if not (ref / "src").is_dir():
         return REF_LIB if REF_LIB.exists() else None
-    deps = [HERE / "ref_harness.cu", HERE / "build_ref.sh"]
+    deps = [HERE / "ref_harness.cu", HERE / "build_ref.sh", *sorted((HERE.parent / "include").glob("*.h*"))]
     if force or not REF_LIB.exists() or any(REF_LIB.stat().st_mtime < d.stat().st_mtime for d in deps):
         env = dict(os.environ, CIRRUS_REFERENCE_DIR=str(ref))
         subprocess.run(["bash", str(HERE / "build_ref.sh")], check=True, capture_output=True, env=env)
@@ -107,6 +107,7 @@ def oracle_lib():
             "ocx_dot": (C.c_double, [P, C.c_int, C.c_int, C.c_int]),
             "ocx_solve": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p, f64p,
                                     C.c_int, C.POINTER(C.c_int)]),
+            "ocx_damped_jacobi": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_double, f64p]),
             "ocx_num_threads": (C.c_int, []),
             "ocx_set_threads": (None, [C.c_int]),
         }
@@ -258,6 +259,12 @@ class CpuOracle:
                                     int(pure_neumann), C.byref(rel), _p(hist, C.c_double), hist.size, C.byref(hl))
         return it, rel.value, hist[:hl.value].copy()
 
+    def damped_jacobi(self, prec, max_iters=10, tol=1e-6, omega=1.0):
+        """GMGSolver::dampedJacobiSolve restated: b in channel 1; returns (iterations, relative residual)."""
+        rel = C.c_double()
+        it = oracle_lib().ocx_damped_jacobi(self.h, prec, max_iters, tol, omega, C.byref(rel))
+        return it, rel.value
+
 
 def set_threads(n: int):
     oracle_lib().ocx_set_threads(n)
@@ -308,6 +315,8 @@ def ref_lib():
             "ref_vcycle": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
             "ref_dot": (C.c_double, [P, C.c_int, C.c_int]),
             "ref_solve": (C.c_int, [P, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p, f64p]),
+            "ref_damped_jacobi": (C.c_int, [P, C.c_int, C.c_double, C.c_float, f64p]),
+            "ref_damped_jacobi_dropin": (C.c_int, [P, C.c_int, C.c_double, C.c_float, f64p]),
             "ref_last_error": (C.c_int, []),
         }
         for k, (r, a) in protos.items():
@@ -416,3 +425,15 @@ class RefHarness:
         it = ref_lib().ref_solve(self.h, max_iters, tol, level_iters, coarsest_iters, sync_stride, int(pure_neumann),
                                  C.byref(rel), C.byref(ms))
         return it, rel.value, ms.value
+
+    def damped_jacobi(self, max_iters=10, tol=1e-6, omega=1.0):
+        """The reference's GMGSolver::dampedJacobiSolve: returns (iterations, relative residual)."""
+        rel = C.c_double()
+        it = ref_lib().ref_damped_jacobi(self.h, max_iters, tol, omega, C.byref(rel))
+        return it, rel.value
+
+    def damped_jacobi_dropin(self, max_iters=10, tol=1e-6, omega=1.0):
+        """The same call through the product's drop-in header on this reference grid."""
+        rel = C.c_double()
+        it = ref_lib().ref_damped_jacobi_dropin(self.h, max_iters, tol, omega, C.byref(rel))
+        return it, rel.value

@@ -255,6 +255,23 @@ int ref_solve_dropin(void* h, int max_iters, double tol, int level_iters, int co
     if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     return iters;
 }
+// GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531), and the same call through the drop-in
+int ref_damped_jacobi(void* h, int max_iters, double tol, float omega, double* rel) {
+    RefGrid* r = (RefGrid*)h;
+    if (!r->solver) r->solver = std::make_unique<GMGSolver>(1., 1.);
+    auto [iters, err] = r->solver->dampedJacobiSolve(*r->g, false, max_iters, tol, omega);
+    cudaDeviceSynchronize();
+    if (rel) *rel = err;
+    return iters;
+}
+int ref_damped_jacobi_dropin(void* h, int max_iters, double tol, float omega, double* rel) {
+    RefGrid* r = (RefGrid*)h;
+    if (!r->dropin) r->dropin = std::make_unique<cirrus_dropin::GMGSolver<HADeviceGrid<Tile>>>(1.f, 1.f);
+    auto [iters, err] = r->dropin->dampedJacobiSolve(*r->g, false, max_iters, tol, omega);
+    cudaDeviceSynchronize();
+    if (rel) *rel = err;
+    return iters;
+}
 int ref_last_error() { return (int)cudaGetLastError(); }
 
 }  // extern "C"

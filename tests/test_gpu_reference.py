@@ -153,3 +153,49 @@ def test_gradient_against_reference_and_oracle(name, built_cache, ref_ok):
         assert np.array_equal(bits(gu[a]), bits(ru[a])), f"axis {a}: product vs reference"
         assert np.array_equal(bits(ou[a]), bits(ru[a])), f"axis {a}: oracle vs reference"
     g.close()
+
+
+@pytest.mark.parametrize("name", ["uniform32_small", "sphere64_small", "ring64_small"])
+def test_damped_jacobi_against_reference_and_oracle(name, built_cache, ref_ok):
+    """GMGSolver::dampedJacobiSolve, the reference's other public solver: the product, the
+    reference build, the drop-in header on the reference grid and the CPU oracle take the same
+    number of iterations and leave x, the residual and the diagonal bit-identical on LEAF cells."""
+    b = built_cache(name)
+    w = b.workload
+    ref = O.RefHarness(w)
+    ref.calc_neighbors()
+    ref.set_ctypes(W.leaf_cell_types(w, b.tiles, b.nbr6))
+    ref.calc_cell_types()
+    ref.calc_neighbors()
+    g = DeviceGrid(b.topology)
+    for a in range(3):
+        g.set_channel(6 + a, b.velocity[a])
+    g.projection_rhs()
+    rhs = g.get_channel(1)
+    o = O.CpuOracle(b.tiles)
+    o.set_ctypes(b.ctypes)
+    leaf = (b.tiles[:, 4] & W.LEAF) != 0
+    omega = float(np.float32(2.0 / 3.0))
+    ref.set_channel(1, rhs)
+    _, rel5 = ref.damped_jacobi(5, 1e-9, omega)
+    for max_iters, tol in ((20, 1e-9), (100, rel5 * (1 + 1e-9))):
+        ref.set_channel(1, rhs)
+        rit, rrel = ref.damped_jacobi(max_iters, tol, omega)
+        rch = [ref.get_channel(c) for c in (0, 2, 3)]
+        g.set_channel(1, rhs)
+        it, rel = GMGSolver().damped_jacobi_solve(g, False, max_iters, tol, omega)
+        ch = [g.get_channel(c) for c in (0, 2, 3)]
+        o.set_channel_f32(1, rhs)
+        oit, orel = o.damped_jacobi(O.CpuOracle.FP32, max_iters, tol, omega)
+        och = [o.get_channel_f32(c) for c in (0, 2, 3)]
+        dit, drel = ref.damped_jacobi_dropin(max_iters, tol, omega)
+        dch = [ref.get_channel(c) for c in (0, 2, 3)]
+        print(f"{name} max_iters {max_iters}: iters {it}/{rit}/{oit}/{dit} rel {rel:.6e}/{rrel:.6e}/{orel:.6e}/{drel:.6e}")
+        assert it == rit == oit == dit
+        assert rit <= (4 if max_iters == 100 else 20)
+        for r in (rel, orel, drel):
+            assert abs(r - rrel) <= 1e-12 * rrel
+        for c, a, rr, ro, d in zip((0, 2, 3), ch, rch, och, dch):
+            assert np.array_equal(bits(a)[leaf], bits(rr)[leaf]), f"channel {c} vs reference"
+            assert np.array_equal(bits(ro)[leaf], bits(a)[leaf]), f"channel {c} vs oracle"
+            assert np.array_equal(bits(d)[leaf], bits(a)[leaf]), f"channel {c} drop-in"

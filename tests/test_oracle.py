@@ -108,3 +108,27 @@ def test_pure_neumann_converges(built_cache):
     f.set_channel_f32(1, f.rhs(b.velocity))
     it, rel, _ = f.solve(O.CpuOracle.FP32, 1000, 1e-6, pure_neumann=True)
     assert rel < 1e-6 and it < 200
+
+
+@pytest.mark.parametrize("name", ["uniform32_small", "sphere64_small", "ring64_small"])
+def test_damped_jacobi_restatement(name, built_cache):
+    """GMGSolver::dampedJacobiSolve restated: the FP32 mirror follows the FP64 restatement, the
+    residual falls, a tolerance reached early stops the loop, a zero b gives the reference's 0/0."""
+    b = built_cache(name)
+    f = oracle_for(b)
+    rhs = f.rhs(b.velocity)
+    omega = float(np.float32(2.0 / 3.0))
+    f.set_channel_f32(1, rhs)
+    it10, rel10 = f.damped_jacobi(O.CpuOracle.FP32, 10, 1e-9, omega)
+    it40, rel40 = f.damped_jacobi(O.CpuOracle.FP32, 40, 1e-9, omega)
+    assert (it10, it40) == (10, 40)
+    assert 0.0 < rel40 < rel10 < 1.0
+    f.set_channel(O.CpuOracle.FP64, 1, rhs.astype(np.float64))
+    it64, rel64 = f.damped_jacobi(O.CpuOracle.FP64, 40, 1e-9, omega)
+    assert it64 == 40 and abs(rel64 - rel40) <= 1e-4 * rel64
+    # the loop ends at the first residual under tolerance * ||b||: x after 9 updates here
+    it, rel = f.damped_jacobi(O.CpuOracle.FP32, 100, rel10 * (1 + 1e-9), omega)
+    assert it <= 9 and rel <= rel10 * (1 + 1e-9)
+    f.set_channel_f32(1, np.zeros((b.n, 512), np.float32))
+    it, rel = f.damped_jacobi(O.CpuOracle.FP32, 10, 1e-6, omega)
+    assert it == 0 and np.isnan(rel)
