@@ -293,9 +293,18 @@ class DeviceGrid:
         return p.value
 
     # operators ------------------------------------------------------------------------
-    def full_negative_laplacian(self, x_channel: int, Ax_channel: int, stream: int = 0) -> None:
-        check(lib().cirrus_full_negative_laplacian(self._h, x_channel, Ax_channel, C.c_void_p(stream)),
-              "cirrus_full_negative_laplacian")
+    def full_negative_laplacian(self, x_channel: int, Ax_channel: int, calc_diag: bool = False, stream: int = 0) -> None:
+        """FullNegativeLaplacian(grid, x_channel, Ax_channel, calc_diag) (src/GMGSolver.cu:203-213)."""
+        check(lib().cirrus_full_negative_laplacian_ex(self._h, x_channel, Ax_channel, int(bool(calc_diag)), C.c_void_p(stream)),
+              "cirrus_full_negative_laplacian_ex")
+
+    def negative_laplacian_same_level(self, tile_level: int, subtree_level: int, launch_tile_types: int, x_channel: int,
+                                      Ax_channel: int, calc_diag: bool = False, stream: int = 0) -> None:
+        """NegativeLaplacianSameLevel128 (src/GMGSolver.cu:145-201) on the tiles of `tile_level`
+        (-1: all tiles) whose subtreeType(subtree_level) is in `launch_tile_types`."""
+        check(lib().cirrus_negative_laplacian_same_level(self._h, tile_level, subtree_level, launch_tile_types, x_channel, Ax_channel,
+                                                         int(bool(calc_diag)), C.c_void_p(stream)),
+              "cirrus_negative_laplacian_same_level")
 
     def gauss_seidel_sweep(self, level: int, x_channel: int, rhs_channel: int, color: int, stream: int = 0) -> None:
         check(lib().cirrus_gauss_seidel_sweep(self._h, level, x_channel, rhs_channel, color, C.c_void_p(stream)),

@@ -131,6 +131,9 @@ _PROTOS = {
     "cirrus_grid_gather_tiles": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_void_p]),
     "cirrus_grid_scatter_tiles": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_void_p]),
     "cirrus_full_negative_laplacian": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "cirrus_full_negative_laplacian_ex": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "cirrus_negative_laplacian_same_level": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                       C.c_void_p]),
     "cirrus_gauss_seidel_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_residual_and_restrict": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "cirrus_prolongate_and_update": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),

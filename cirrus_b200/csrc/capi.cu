@@ -389,6 +389,23 @@ cirrus_status cirrus_full_negative_laplacian(cirrus_grid* grid, int x_channel, i
     cirrus::launch::full_laplacian<float>(g, g.d_ch[x_channel], g.d_ch[Ax_channel], nullptr, S(stream));
     return cuda_status();
 }
+cirrus_status cirrus_full_negative_laplacian_ex(cirrus_grid* grid, int x_channel, int Ax_channel, int calc_diag, void* stream) {
+    if (!calc_diag) return cirrus_full_negative_laplacian(grid, x_channel, Ax_channel, stream);
+    if (!grid || !channel_ok(x_channel) || !channel_ok(Ax_channel) || x_channel == Ax_channel) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    cirrus::launch::full_laplacian_diag(g, g.d_ch[x_channel], g.d_ch[Ax_channel], S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_negative_laplacian_same_level(cirrus_grid* grid, int tile_level, int subtree_level, int launch_tile_types,
+                                                   int x_channel, int Ax_channel, int calc_diag, void* stream) {
+    if (!grid || !channel_ok(x_channel) || !channel_ok(Ax_channel) || x_channel == Ax_channel) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    if (tile_level < -1 || tile_level >= (int)g.level_count.size() || subtree_level < -1 || (launch_tile_types & ~7) != 0)
+        return CIRRUS_ERR_INVALID_ARGUMENT;
+    cirrus::launch::laplacian_same_level(g, tile_level, subtree_level, (uint32_t)launch_tile_types, g.d_ch[x_channel],
+                                         g.d_ch[Ax_channel], calc_diag != 0, S(stream));
+    return cuda_status();
+}
 cirrus_status cirrus_gauss_seidel_sweep(cirrus_grid* grid, int level, int x_channel, int rhs_channel, int color, void* stream) {
     if (!grid || !channel_ok(x_channel) || !channel_ok(rhs_channel) || (color != 0 && color != 1)) return CIRRUS_ERR_INVALID_ARGUMENT;
     auto& g = *grid->g;

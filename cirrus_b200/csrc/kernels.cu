@@ -71,6 +71,44 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian(Topo tp, const int* __r
     st4(Y + (size_t)tile * kTileCells + t * 4, o);
 }
 
+// NegativeLaplacianSameLevel128 (src/GMGSolver.cu:145-201) over the pool tiles [first,
+// first + count): a tile whose subtreeType(subtree_level) -- NONLEAF counts as LEAF at its own
+// level -- is in `types` gets A x (or the diagonal) on all 512 cells; other tiles are not
+// written.  A tile at the subtree level sees its neighbours with the same rule (the multigrid
+// level context, mask_mg); a tile at any other level sees their plain types (the full-tree
+// context, mask_lap).  Products rounded before the add, as in the reference's kernel.
+template <int TPB, bool DIAG>
+__global__ void __launch_bounds__(128 * TPB) k_laplacian_same_level(Topo tp, int first, int count, int subtree_level,
+                                                                      uint32_t types, const float* __restrict__ X,
+                                                                      float* __restrict__ Y) {
+    pdl_entry();
+    __shared__ TileShared<float> sh[TPB];
+    const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
+    const int q = blockIdx.x * TPB + g;
+    const int tile = first + (q < count ? q : 0);
+    bool active = false, own_level = false;
+    TileMeta m;
+    if (q < count) {
+        m = tp.meta[tile];
+        own_level = meta_level(m.packed) == subtree_level;
+        const uint32_t type = (uint32_t)meta_type(m.packed);
+        active = ((own_level && type == NONLEAF_T ? (uint32_t)LEAF_T : type) & types) != 0;
+        if (active) stage_tile<float>(X, tile, m, t, sh[g]);
+    }
+    __syncthreads();
+    if (!active) return;
+    const uint8_t* masks = own_level ? tp.mask_mg : tp.mask_lap;
+    const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(masks + (size_t)tile * kTileCells + t * 4);
+    const uint32_t cls = (own_level ? tp.fcls[tile] >> 12 : tp.fcls[tile]) & 0xfffu;
+    const LevelConst<float> L((float)tile_h0(tp, tile), meta_level(m.packed));
+    float out[4], dg[4];
+    neg_lap4<float, DIAG, false>(sh[g].xs, sh[g].hx, t, mask4, cls, L, out, dg);
+    V4<float> o;
+#pragma unroll
+    for (int e = 0; e < 4; e++) o.v[e] = DIAG ? dg[e] : out[e];
+    st4(Y + (size_t)tile * kTileCells + t * 4, o);
+}
+
 // Face path of the fused Laplacian: one coarse cell of a GHOST tile whose coupled cells all lie
 // on its faces and couple only outward.  Item: tile, ghost slot << 6 | coarse cell c, coupled
 // faces | face classes << 6, level-constant index.  Forms the cell's partial sum -- its 2x2x2
@@ -1211,6 +1249,18 @@ void vcycle_init(const DevGrid& g, float* X, float* RHS, const float* F, const S
     if (blocks < 1) blocks = 1;
     ++g.launch_count;
     launch_kernel(k_vcycle_init, blocks, 256, 0, s, g.topo, g.n, X, RHS, F, S);
+}
+
+void laplacian_same_level(const DevGrid& g, int level, int subtree_level, uint32_t types, const float* X, float* Y, bool diag,
+                          cudaStream_t s) {
+    const int first = level < 0 ? 0 : g.level_first[level], count = level < 0 ? g.n : g.level_count[level];
+    if (count == 0) return;
+    ++g.launch_count;
+    const int blocks = (count + kTPB - 1) / kTPB;
+    if (diag)
+        launch_kernel(k_laplacian_same_level<kTPB, true>, blocks, 128 * kTPB, 0, s, g.topo, first, count, subtree_level, types, X, Y);
+    else
+        launch_kernel(k_laplacian_same_level<kTPB, false>, blocks, 128 * kTPB, 0, s, g.topo, first, count, subtree_level, types, X, Y);
 }
 
 // dampedJacobiSolve's residual step (src/GMGSolver.cu:479-490): Ax = b - Ax on INTERIOR cells

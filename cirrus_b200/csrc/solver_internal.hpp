@@ -196,6 +196,10 @@ inline void launch_kernel(void (*k)(KArgs...), dim3 grid, dim3 block, size_t sme
 template <class T> void full_laplacian(const DevGrid& g, T* X, T* Y, const Scalars* S, cudaStream_t s);
 // FullNegativeLaplacian with calc_diag: the diagonal of LEAF|GHOST cells, ghost rows accumulated.
 void full_laplacian_diag(const DevGrid& g, float* X, float* D, cudaStream_t s);
+// NegativeLaplacianSameLevel128 over the tiles of `level` (-1: all tiles) whose
+// subtreeType(subtree_level) is in `types`.
+void laplacian_same_level(const DevGrid& g, int level, int subtree_level, uint32_t types, const float* X, float* Y, bool diag,
+                          cudaStream_t s);
 // dampedJacobiSolve's residual (Ax = b - Ax) and update (x += omega r / D) on INTERIOR LEAF cells.
 void jacobi_residual(const DevGrid& g, const float* B, float* AX, cudaStream_t s);
 void jacobi_update(const DevGrid& g, float* X, const float* R, const float* D, float omega, cudaStream_t s);

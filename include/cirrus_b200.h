@@ -158,6 +158,19 @@ cirrus_status cirrus_grid_channel_ptr(cirrus_grid* grid, int channel, float** de
  * ---------------------------------------------------------------------------------------- */
 /* FullNegativeLaplacian(grid, x_channel, Ax_channel) (src/GMGSolver.cu:203-213). */
 cirrus_status cirrus_full_negative_laplacian(cirrus_grid* grid, int x_channel, int Ax_channel, void* stream);
+/* FullNegativeLaplacian(grid, x_channel, Ax_channel, calc_diag) with the reference's calc_diag
+ * argument (src/GMGSolver.h:13): calc_diag != 0 gives the diagonal of the same operator
+ * (GHOST rows accumulated into their parents as for A x). */
+cirrus_status cirrus_full_negative_laplacian_ex(cirrus_grid* grid, int x_channel, int Ax_channel, int calc_diag, void* stream);
+/* NegativeLaplacianSameLevel128(grid, tiles, n, subtree_level, launch_tile_types, x_channel,
+ * Ax_channel, calc_diag) (src/GMGSolver.h:7, src/GMGSolver.cu:145-201).  tile_level selects the
+ * tile array: -1 = all tiles (grid.dAllTiles), l >= 0 = the tiles of level l
+ * (grid.dTileArrays[l]).  A tile is computed when its subtreeType(subtree_level) -- NONLEAF at
+ * that level counts as LEAF -- is in launch_tile_types (CIRRUS_LEAF | CIRRUS_NONLEAF |
+ * CIRRUS_GHOST bits); it gets A x (or the diagonal) on all 512 cells, 0 on non-INTERIOR cells.
+ * No ghost propagation or accumulation (FullNegativeLaplacian adds those). */
+cirrus_status cirrus_negative_laplacian_same_level(cirrus_grid* grid, int tile_level, int subtree_level, int launch_tile_types,
+                                                   int x_channel, int Ax_channel, int calc_diag, void* stream);
 /* One red-black colour sweep on LEAF|NONLEAF tiles of `level`
  * (NegativeLaplacianAndGaussSeidelSameLevel128, src/GMGSolver.cu:216-274). */
 cirrus_status cirrus_gauss_seidel_sweep(cirrus_grid* grid, int level, int x_channel, int rhs_channel, int color, void* stream);

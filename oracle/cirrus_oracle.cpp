@@ -451,6 +451,19 @@ struct Solver {
         lap_tiles(xc, yc, true);
         accumulate_ghosts(yc);
     }
+    // NegativeLaplacianSameLevel128 (src/GMGSolver.cu:145-201): tiles of `tile_level` (-1: all)
+    // whose subtreeType(subtree_level) is in `types`; products rounded before the add
+    void lap_same_level(int tile_level, int subtree_level, uint8_t types, int xc, int yc, bool diag) {
+        Halo<T> H{f, C(xc), subtree_level};
+        T* y = C(yc);
+#pragma omp parallel for schedule(static)
+        for (int t = 0; t < f.n; t++) {
+            if (tile_level >= 0 && f.level[t] != tile_level) continue;
+            if (!(f.subtree_type(t, subtree_level) & types)) continue;
+            for (int o = 0; o < NCELL; o++)
+                y[(size_t)t * NCELL + o] = neg_lap<T>(H, t, o >> 6, (o >> 3) & 7, o & 7, diag, false);
+        }
+    }
     // one red-black colour sweep on LEAF|NONLEAF tiles of 'level' (src/GMGSolver.cu:216-269)
     void gs_sweep(int level, int xc, int rc, int color) {
         Halo<T> H{f, C(xc), level};
@@ -1046,6 +1059,15 @@ void ocx_get_channel_f32(void* h, int c, float* data) {
 void ocx_full_lap(void* h, int prec, int xc, int yc) {
     OCX* o = (OCX*)h;
     if (prec == 0) S32(o).full_lap(xc, yc); else S64(o).full_lap(xc, yc);
+}
+void ocx_full_lap_diag(void* h, int prec, int xc, int yc) {
+    OCX* o = (OCX*)h;
+    if (prec == 0) S32(o).full_lap_diag(xc, yc); else S64(o).full_lap_diag(xc, yc);
+}
+void ocx_lap_same_level(void* h, int prec, int tile_level, int subtree_level, int types, int xc, int yc, int diag) {
+    OCX* o = (OCX*)h;
+    if (prec == 0) S32(o).lap_same_level(tile_level, subtree_level, (uint8_t)types, xc, yc, diag != 0);
+    else S64(o).lap_same_level(tile_level, subtree_level, (uint8_t)types, xc, yc, diag != 0);
 }
 void ocx_gs_sweep(void* h, int prec, int level, int xc, int rc, int color) {
     OCX* o = (OCX*)h;

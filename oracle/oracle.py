@@ -100,6 +100,8 @@ def oracle_lib():
             "ocx_set_channel_f32": (None, [P, C.c_int, f32p]),
             "ocx_get_channel_f32": (None, [P, C.c_int, f32p]),
             "ocx_full_lap": (None, [P, C.c_int, C.c_int, C.c_int]),
+            "ocx_full_lap_diag": (None, [P, C.c_int, C.c_int, C.c_int]),
+            "ocx_lap_same_level": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
             "ocx_gs_sweep": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
             "ocx_residual_restrict": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
             "ocx_prolongate": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -236,6 +238,12 @@ class CpuOracle:
     def full_lap(self, prec, xc, yc):
         oracle_lib().ocx_full_lap(self.h, prec, xc, yc)
 
+    def full_lap_diag(self, prec, xc, yc):
+        oracle_lib().ocx_full_lap_diag(self.h, prec, xc, yc)
+
+    def lap_same_level(self, prec, tile_level, subtree_level, types, xc, yc, diag=False):
+        oracle_lib().ocx_lap_same_level(self.h, prec, tile_level, subtree_level, types, xc, yc, int(diag))
+
     def gs_sweep(self, prec, level, xc, rc, color):
         oracle_lib().ocx_gs_sweep(self.h, prec, level, xc, rc, color)
 
@@ -309,6 +317,8 @@ def ref_lib():
             "ref_rhs": (None, [P]),
             "ref_add_gradient": (None, [P, C.c_int, C.c_int]),
             "ref_full_lap": (None, [P, C.c_int, C.c_int]),
+            "ref_full_lap_ex": (None, [P, C.c_int, C.c_int, C.c_int]),
+            "ref_lap_same_level": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
             "ref_gs_sweep": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int]),
             "ref_residual_restrict": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int]),
             "ref_prolongate": (None, [P, C.c_int, C.c_int, C.c_int]),
@@ -403,6 +413,12 @@ class RefHarness:
 
     def full_lap(self, xc, yc):
         ref_lib().ref_full_lap(self.h, xc, yc)
+
+    def full_lap_ex(self, xc, yc, calc_diag):
+        ref_lib().ref_full_lap_ex(self.h, xc, yc, int(calc_diag))
+
+    def lap_same_level(self, tile_level, subtree_level, types, xc, yc, calc_diag=False):
+        ref_lib().ref_lap_same_level(self.h, tile_level, subtree_level, types, xc, yc, int(calc_diag))
 
     def gs_sweep(self, level, xc, rc, color):
         ref_lib().ref_gs_sweep(self.h, level, xc, rc, color)

@@ -205,6 +205,20 @@ void ref_full_lap(void* h, int xc, int yc) {
     FullNegativeLaplacian(*((RefGrid*)h)->g, xc, yc, false);
     cudaDeviceSynchronize();
 }
+void ref_full_lap_ex(void* h, int xc, int yc, int calc_diag) {
+    FullNegativeLaplacian(*((RefGrid*)h)->g, xc, yc, calc_diag != 0);
+    cudaDeviceSynchronize();
+}
+// NegativeLaplacianSameLevel128 on grid.dAllTiles (tile_level -1) or grid.dTileArrays[tile_level]
+void ref_lap_same_level(void* h, int tile_level, int subtree_level, int types, int xc, int yc, int calc_diag) {
+    auto& grid = *((RefGrid*)h)->g;
+    if (tile_level < 0)
+        NegativeLaplacianSameLevel128(grid, grid.dAllTiles, grid.dAllTiles.size(), subtree_level, (uint8_t)types, xc, yc, calc_diag != 0);
+    else
+        NegativeLaplacianSameLevel128(grid, grid.dTileArrays[tile_level], grid.hNumTiles[tile_level], subtree_level, (uint8_t)types, xc,
+                                      yc, calc_diag != 0);
+    cudaDeviceSynchronize();
+}
 void ref_gs_sweep(void* h, int level, int xc, int rc, int color) {
     auto& grid = *((RefGrid*)h)->g;
     NegativeLaplacianAndGaussSeidelSameLevel128(grid, grid.dTileArrays[level], grid.hNumTiles[level], level, LEAF | NONLEAF, xc, rc, color);

@@ -49,6 +49,42 @@ def test_full_laplacian_bitwise(name, built_cache):
     assert np.array_equal(bits(g.get_channel(2)), bits(f.get_channel_f32(2)))
 
 
+def same_level_cases(maxl):
+    """(tile_level, subtree_level, launch_tile_types, calc_diag) combinations the reference's
+    NegativeLaplacianSameLevel128 is called with, plus mixed-context ones."""
+    lg, all3 = W.LEAF | W.GHOST, W.LEAF | W.NONLEAF | W.GHOST
+    cases = [(-1, -1, lg, 0), (-1, -1, lg, 1), (-1, -1, all3, 0), (-1, min(2, maxl), all3, 0), (-1, maxl, W.NONLEAF, 1)]
+    for l in range(maxl + 1):
+        cases += [(l, l, W.LEAF | W.NONLEAF, 0), (l, l, W.LEAF | W.NONLEAF, 1), (l, l, W.GHOST, 0), (l, -1, all3, 1)]
+    return cases
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_laplacian_variants_bitwise(name, built_cache):
+    """FullNegativeLaplacian with calc_diag, and NegativeLaplacianSameLevel128 for every tile
+    array, subtree level and tile-type filter: computed tiles and untouched tiles bit for bit."""
+    b = built_cache(name)
+    g, f = setup(b)
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((b.n, 512)).astype(np.float32)
+    y0 = rng.standard_normal((b.n, 512)).astype(np.float32)
+    g.set_channel(2, x)
+    g.full_negative_laplacian(2, 3, calc_diag=True)
+    f.set_channel_f32(2, x)
+    f.full_lap_diag(O.CpuOracle.FP32, 2, 3)
+    lg = (b.tiles[:, 4] & (W.LEAF | W.GHOST)) != 0
+    assert np.array_equal(bits(g.get_channel(3))[lg], bits(f.get_channel_f32(3))[lg])
+    maxl = int(b.tiles[:, 0].max())
+    for case in same_level_cases(maxl):
+        g.set_channel(2, x)
+        g.set_channel(3, y0)
+        g.negative_laplacian_same_level(*case[:3], 2, 3, bool(case[3]))
+        f.set_channel_f32(2, x)
+        f.set_channel_f32(3, y0)
+        f.lap_same_level(O.CpuOracle.FP32, *case[:3], 2, 3, bool(case[3]))
+        assert np.array_equal(bits(g.get_channel(3)), bits(f.get_channel_f32(3))), case
+
+
 @pytest.mark.parametrize("name", NAMES)
 def test_level_operators_bitwise(name, built_cache):
     """GS colour sweeps, residual+restriction and prolongation on every level."""

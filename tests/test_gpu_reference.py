@@ -199,3 +199,37 @@ def test_damped_jacobi_against_reference_and_oracle(name, built_cache, ref_ok):
             assert np.array_equal(bits(a)[leaf], bits(rr)[leaf]), f"channel {c} vs reference"
             assert np.array_equal(bits(ro)[leaf], bits(a)[leaf]), f"channel {c} vs oracle"
             assert np.array_equal(bits(d)[leaf], bits(a)[leaf]), f"channel {c} drop-in"
+
+
+@pytest.mark.parametrize("name", ["uniform32_small", "sphere64_small", "ring64_small", "sphere256"])
+def test_laplacian_variants_against_reference(name, built_cache, ref_ok):
+    """FullNegativeLaplacian(calc_diag = true) and NegativeLaplacianSameLevel128 against the
+    reference's own kernels on its grid: same bits on every tile, computed or untouched."""
+    from test_gpu_kernels import same_level_cases
+
+    b = built_cache(name)
+    w = b.workload
+    ref = O.RefHarness(w)
+    ref.calc_neighbors()
+    ref.set_ctypes(W.leaf_cell_types(w, b.tiles, b.nbr6))
+    ref.calc_cell_types()
+    ref.calc_neighbors()
+    g = DeviceGrid(b.topology)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((b.n, 512)).astype(np.float32)
+    y0 = rng.standard_normal((b.n, 512)).astype(np.float32)
+    lg = (b.tiles[:, 4] & (W.LEAF | W.GHOST)) != 0
+    for diag in (False, True):
+        g.set_channel(2, x)
+        g.full_negative_laplacian(2, 3, calc_diag=diag)
+        ref.set_channel(2, x)
+        ref.full_lap_ex(2, 3, diag)
+        assert np.array_equal(bits(g.get_channel(3))[lg], bits(ref.get_channel(3))[lg]), diag
+    for case in same_level_cases(int(b.tiles[:, 0].max())):
+        g.set_channel(2, x)
+        g.set_channel(3, y0)
+        g.negative_laplacian_same_level(*case[:3], 2, 3, bool(case[3]))
+        ref.set_channel(2, x)
+        ref.set_channel(3, y0)
+        ref.lap_same_level(*case[:3], 2, 3, bool(case[3]))
+        assert np.array_equal(bits(g.get_channel(3)), bits(ref.get_channel(3))), case
