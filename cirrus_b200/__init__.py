@@ -460,6 +460,22 @@ class GMGSolver:
         self.last_result = r
         return r.iters, r.rel_residual
 
+    def solve_host_submit(self, grid: DeviceGrid, b: np.ndarray, x_out: np.ndarray, stream: int = 0, **kw) -> None:
+        """Asynchronous end-to-end solve: enqueues the copy of b, the solve and the copy of x into
+        x_out on `stream` and returns; solve_host_wait(grid) collects it.  Keep b and x_out
+        untouched until then (pinned arrays make the copies asynchronous)."""
+        p = self.params(**kw)
+        check(lib().cirrus_gmg_solve_host_submit(grid.handle, C.byref(p), _ptr(b, C.c_float), _ptr(x_out, C.c_float),
+                                                 C.c_void_p(stream)), "cirrus_gmg_solve_host_submit")
+        grid._inflight = (b, x_out)
+
+    def solve_host_wait(self, grid: DeviceGrid) -> list[tuple[int, float]]:
+        """Waits for the grid's submitted solve; (iterations, relative residual) per instance."""
+        res = (SolveResult * grid.num_instances)()
+        check(lib().cirrus_gmg_solve_host_wait(grid.handle, res), "cirrus_gmg_solve_host_wait")
+        grid._inflight = None
+        return [(r.iters, r.rel_residual) for r in res]
+
 
 class Server:
     """Serving loop: sessions (independent problems) with device-resident tile pools and warm-start

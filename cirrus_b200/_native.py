@@ -149,6 +149,8 @@ _PROTOS = {
     "cirrus_gmg_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_int_p, c_f64_p, c_int_p, C.c_void_p,
                                          C.POINTER(SolveResult)]),
     "cirrus_gmg_solve_host": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p, C.POINTER(SolveResult)]),
+    "cirrus_gmg_solve_host_submit": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p]),
+    "cirrus_gmg_solve_host_wait": (C.c_int, [C.c_void_p, C.POINTER(SolveResult)]),
     "cirrus_server_create": (C.c_int, [C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),
     "cirrus_server_destroy": (None, [C.c_void_p]),
     "cirrus_server_add_session": (C.c_int, [C.c_void_p, C.c_void_p, c_int_p]),

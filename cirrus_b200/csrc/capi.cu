@@ -15,6 +15,15 @@ struct cirrus_topology {
 };
 struct cirrus_grid {
     cirrus::DevGrid* g;
+    // the asynchronous end-to-end solve in flight (cirrus_gmg_solve_host_submit), if any
+    struct Pending {
+        bool active = false, collected = false;
+        cudaStream_t stream = nullptr;
+        cirrus::SolveParams p;
+        long long direct = -1;
+        int rc = 0;
+        std::vector<cirrus::SolveResult> r;
+    } pending;
 };
 struct cirrus_server {
     cirrus::Server* s;
@@ -316,6 +325,7 @@ cirrus_status cirrus_grid_get_channel_instance(const cirrus_grid* grid, int inst
 }
 void cirrus_grid_destroy(cirrus_grid* grid) {
     if (!grid) return;
+    if (grid->pending.active) cudaStreamSynchronize(grid->pending.stream);
     cirrus::grid_destroy(grid->g);
     delete grid;
 }
@@ -553,6 +563,62 @@ cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params
     if (st != CIRRUS_OK) return st;
     if (cudaMemcpyAsync(x_host, g.d_ch[cirrus::kChX], bytes, cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess) return cuda_status();
     return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
+}
+
+cirrus_status cirrus_gmg_solve_host_wait(cirrus_grid* grid, cirrus_solve_result* results) {
+    if (!grid || !results || !grid->pending.active) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& pd = grid->pending;
+    auto& g = *grid->g;
+    pd.active = false;
+    if (!pd.collected) {
+        if (cudaStreamSynchronize(pd.stream) != cudaSuccess) return cuda_status();
+        pd.r.assign(g.num_inst, cirrus::SolveResult());
+        cirrus::pcg_collect(g, pd.p, pd.direct, pd.r.data());
+    }
+    if (pd.rc) return map_rc(pd.rc);
+    for (int i = 0; i < g.num_inst; i++) {
+        results[i].iters = pd.r[i].iters;
+        results[i].outer_iters = pd.r[i].outer;
+        results[i].rel_residual = pd.r[i].rel;
+        results[i].true_rel_residual = pd.r[i].true_rel;
+        results[i].status = (int)map_rc(pd.r[i].status);
+        results[i].kernel_launches = pd.r[i].launches;
+    }
+    return CIRRUS_OK;
+}
+
+cirrus_status cirrus_gmg_solve_host_submit(cirrus_grid* grid, const cirrus_solve_params* params, const float* b_host, float* x_host,
+                                           void* stream) {
+    if (!grid || !params_ok(params) || !b_host || !x_host) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (grid->pending.active) {  // one solve in flight per grid: finish the previous one first
+        std::vector<cirrus_solve_result> prev(grid->g->num_inst);
+        cirrus_gmg_solve_host_wait(grid, prev.data());
+    }
+    return guard([&] {
+        auto& g = *grid->g;
+        auto& pd = grid->pending;
+        const size_t bytes = (size_t)g.n * cirrus::kTileCells * sizeof(float);
+        if (cudaMemcpyAsync(g.d_ch[cirrus::kChB], b_host, bytes, cudaMemcpyHostToDevice, S(stream)) != cudaSuccess) return cuda_status();
+        to_internal(params, &pd.p);
+        pd.stream = S(stream);
+        pd.direct = -1;
+        pd.rc = 0;
+        pd.collected = false;
+        if (pd.p.precision == CIRRUS_PRECISION_MIXED_FP64) {
+            // the outer refinement loop reads residuals on the host: runs to completion here
+            pd.r.assign(g.num_inst, cirrus::SolveResult());
+            pd.rc = cirrus::mixed_solve(g, pd.p, pd.stream, pd.r.data(), nullptr);
+            pd.collected = true;
+        } else {
+            g.x64_valid = false;
+            const int rc = cirrus::pcg_launch(g, pd.p, pd.stream, nullptr, &pd.direct);
+            if (rc) return map_rc(rc);
+        }
+        if (!pd.rc && cudaMemcpyAsync(x_host, g.d_ch[cirrus::kChX], bytes, cudaMemcpyDeviceToHost, pd.stream) != cudaSuccess)
+            return cuda_status();
+        pd.active = true;
+        return CIRRUS_OK;
+    });
 }
 
 cirrus_status cirrus_grid_autotune(cirrus_grid* grid, int reps, void* stream) {

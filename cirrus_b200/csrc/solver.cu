@@ -247,6 +247,19 @@ bool any_pure_neumann(const DevGrid& g) {
 }  // namespace
 
 int pcg_solve(DevGrid& g, const SolveParams& p0, cudaStream_t s, SolveResult* r, const InstRequest* req) {
+    long long direct = -1;
+    int rc = pcg_launch(g, p0, s, req, &direct);
+    if (rc) return rc;
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        g.last_error = std::string("solve: ") + cudaGetErrorString(e);
+        return 2;
+    }
+    pcg_collect(g, p0, direct, r);
+    return 0;
+}
+
+int pcg_launch(DevGrid& g, const SolveParams& p0, cudaStream_t s, const InstRequest* req, long long* direct_out) {
     upload_params(g, p0, req, s);
     SolveParams p = p0;
     p.pure_neumann = any_pure_neumann(g) ? 1 : 0;
@@ -285,17 +298,24 @@ int pcg_solve(DevGrid& g, const SolveParams& p0, cudaStream_t s, SolveResult* r,
         direct = g.launch_count - c0;
     }
     cudaMemcpyAsync(g.h_scalars, g.d_scalars, sizeof(Scalars) * g.num_inst, cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        g.last_error = std::string("solve: ") + cudaGetErrorString(e);
-        return 2;
+    *direct_out = direct;
+    return 0;
+}
+
+void pcg_collect(DevGrid& g, const SolveParams& p, long long direct, SolveResult* r) {
+    const DevGrid::SolveGraph* sgp = nullptr;
+    if (direct < 0) {
+        GraphKey key{0, p.level_iters, p.coarsest_iters, p.sync_stride, any_pure_neumann(g) ? 1 : 0, p.one_over_alpha,
+                     p.prolong_coeff, use_fused(g, p.level_iters, p.coarsest_iters) ? 1 : 0};
+        auto it = g.graphs.find(key);
+        if (it != g.graphs.end()) sgp = &it->second;
     }
     // bodies executed = the largest iteration count of the instances (each body advances every
     // iterating instance's counter once)
     int loops = 0;
     for (int k = 0; k < g.num_inst; k++)
         if (g.h_iparams[k].active) loops = std::max(loops, g.h_scalars[k].iter);
-    g.last_solve_launches = direct >= 0 ? direct : sg.prologue + (long long)loops * sg.body + sg.epilogue;
+    g.last_solve_launches = direct >= 0 ? direct : sgp ? sgp->prologue + (long long)loops * sgp->body + sgp->epilogue : 0;
     for (int k = 0; k < g.num_inst; k++) {
         const Scalars& S = g.h_scalars[k];
         SolveResult& o = r[k];
@@ -307,7 +327,6 @@ int pcg_solve(DevGrid& g, const SolveParams& p0, cudaStream_t s, SolveResult* r,
         if (!g.h_iparams[k].active) o.status = 0;
         o.launches = g.last_solve_launches;
     }
-    return 0;
 }
 
 namespace {

@@ -299,6 +299,12 @@ struct InstRequest {
 int pcg_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r, const InstRequest* req = nullptr);
 // Mixed precision: FP64 defect correction around FP32 PCG solves.
 int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r, const InstRequest* req = nullptr);
+// pcg_solve in two halves for asynchronous callers: pcg_launch enqueues the solve on s (the graph
+// launch, or direct launches with their per-iteration host checks, then the copy of the
+// instances' scalars into the pinned mirror); pcg_collect turns that mirror into results once s
+// has completed.  `direct` carries the direct path's launch count (-1: graph) from one to the other.
+int pcg_launch(DevGrid& g, const SolveParams& p, cudaStream_t s, const InstRequest* req, long long* direct);
+void pcg_collect(DevGrid& g, const SolveParams& p, long long direct, SolveResult* r);
 // GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x to channel 0,
 // channels 2 (residual) and 3 (diagonal) as the reference leaves them.  Single-instance grids.
 int damped_jacobi(DevGrid& g, int max_iters, double tol, float omega, cudaStream_t s, int* iters, double* rel);

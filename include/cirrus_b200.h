@@ -285,6 +285,19 @@ cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_param
 cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params* params, const float* b_host,
                                     float* x_host, void* stream, cirrus_solve_result* result);
 
+/* Asynchronous form of cirrus_gmg_solve_host for pipelines (no counterpart in the reference):
+ * enqueues on `stream` the copy of b_host to the device, the solve (one graph launch for every
+ * instance of the grid) and the copy of x into x_host, and returns without waiting.  Both host
+ * arrays must stay valid and untouched until cirrus_gmg_solve_host_wait returns; pinned memory
+ * makes the copies asynchronous.  cirrus_gmg_solve_host_wait synchronises the stream and writes
+ * one result per instance.  One solve in flight per grid (a second submit first waits for the
+ * previous one, discarding its results); to overlap one batch's transfers with another batch's
+ * solve, alternate between two grids of the same problems, each with its own stream.  Mixed
+ * precision runs to completion inside the submit (its outer loop reads residuals on the host). */
+cirrus_status cirrus_gmg_solve_host_submit(cirrus_grid* grid, const cirrus_solve_params* params, const float* b_host,
+                                           float* x_host, void* stream);
+cirrus_status cirrus_gmg_solve_host_wait(cirrus_grid* grid, cirrus_solve_result* results);
+
 /* The last solution in FP64 (num_tiles*512 doubles, all-tiles order): the FP64 iterate of a
  * mixed-precision solve, else channel 0 widened.  Channel 0 always holds its FP32 rounding. */
 cirrus_status cirrus_grid_get_solution_f64(cirrus_grid* grid, double* host, void* stream);
