@@ -74,6 +74,9 @@ struct Topo {
     const int* inst;             // n: instance of each tile
     const float* inst_h0;        // per instance: voxel size of level 0, stored in FP32 as the reference does
     const float4* lconst;        // per instance x kLevelSlots levels: h, c1, c2, fast-path diagonal
+    const int* leafslot;         // n: position s of a LEAF tile in the LEAF list, stored as s for a
+                                 // tile without GHOST children and as -2 - s for one with them; -1
+                                 // for every other tile
 };
 constexpr int kLevelSlots = 16;
 

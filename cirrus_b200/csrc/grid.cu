@@ -563,6 +563,32 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
         CK((cudaError_t)(upload(&g->d_chunks, chunks) ? cudaErrorMemoryAllocation : cudaSuccess));
         CK((cudaError_t)(upload(&g->d_inst_chunks, ich) ? cudaErrorMemoryAllocation : cudaSuccess));
     }
+    // LEAF slots (with the GHOST-children mark), per-instance LEAF ranges, bottom-level LEAF tiles
+    {
+        std::vector<int> slot(n, -1), bl;
+        for (size_t q = 0; q < leaf.size(); q++) {
+            const int t = leaf[q];
+            bool kids = false;
+            for (int o = 0; o < 8; o++) {
+                const int c = ch8[(size_t)t * 8 + o];
+                kids = kids || (c >= 0 && (type[c] & GHOST_T));
+            }
+            slot[t] = kids ? -2 - (int)q : (int)q;
+            if (level[t] <= g->bottom_level) bl.push_back(t);
+        }
+        std::vector<int2> lr(K);
+        int first = 0;
+        for (int i = 0; i < K; i++) {
+            lr[i] = make_int2(first, inst_leaves[i]);
+            first += inst_leaves[i];
+        }
+        CK((cudaError_t)(upload(&g->d_leafslot, slot) ? cudaErrorMemoryAllocation : cudaSuccess));
+        CK((cudaError_t)(upload(&g->d_inst_leafrange, lr) ? cudaErrorMemoryAllocation : cudaSuccess));
+        g->n_bottom_leaves = (int)bl.size();
+        bl.push_back(0);
+        CK((cudaError_t)(upload(&g->d_bottom_leaves, bl) ? cudaErrorMemoryAllocation : cudaSuccess));
+        CK(cudaMalloc(&g->d_wpart, sizeof(double) * 4 * std::max<size_t>(leaf.size(), 1)));
+    }
     CK(cudaMalloc(&g->d_partials, sizeof(double) * 2 * std::max(g->red_blocks, g->n_chunks)));
     CK(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CK(cudaMemset(g->d_counter, 0, sizeof(unsigned int) * 4));
@@ -597,6 +623,7 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
     g->topo.inst = g->d_inst;
     g->topo.inst_h0 = g->d_inst_h0;
     g->topo.lconst = g->d_lconst;
+    g->topo.leafslot = g->d_leafslot;
     g->bytes = cells * kNumChannels * sizeof(float) + cells * 3 + sizeof(TileMeta) * n + sizeof(uint32_t) * n + sizeof(int) * nl +
                sizeof(int) * 22 * (size_t)n + cells * sizeof(float);
     *out = g;
@@ -629,6 +656,10 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_bottom_inst);
     cudaFree(g->d_tile_ptrs);
     cudaFree(g->d_lists);
+    cudaFree(g->d_leafslot);
+    cudaFree(g->d_wpart);
+    cudaFree(g->d_inst_leafrange);
+    cudaFree(g->d_bottom_leaves);
     cudaFree(g->d_chunks);
     cudaFree(g->d_inst_chunks);
     cudaFree(g->d_partials);

@@ -325,9 +325,15 @@ __global__ void __launch_bounds__(64) k_accumulate_ghosts(Topo tp, const int* __
 // x += (b - A x) / D on INTERIOR cells.
 // The tiles of a CTA are NT groups of TPB consecutive list entries, one 128-thread group per
 // tile, all staged with asynchronous copies before any is computed (NT tiles per group in flight).
+// With RD (the PCG residual r) the sweep also forms, for every LEAF tile it updates, the partial
+// sums of the next r.z (DotAsync, src/GMGSolver.cu:636-640): per 32-thread quarter of the tile the
+// 4-cell FP32 products widened to FP64 and warp-summed, stored at WP[4 * LEAF slot + quarter].  A
+// LEAF tile's z is final after this sweep (finer levels only read it).  Its r is the staged
+// right-hand side unless GHOST children added their residuals to that copy; then r is read.
 template <int TPB, int NT>
 __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__ list, int n, float* X,
-                                                        const float* __restrict__ R, int color, const Scalars* __restrict__ S) {
+                                                        const float* __restrict__ R, int color, const Scalars* __restrict__ S,
+                                                        const float* __restrict__ RD, double* __restrict__ WP) {
     pdl_entry();
     extern __shared__ __align__(16) unsigned char gs_smem[];
     TileStage* st = reinterpret_cast<TileStage*>(gs_smem);
@@ -342,6 +348,9 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
     }
     TilePre pre[NT];
     tile_pre(tp, tile, t, pre);
+    int slot[NT];
+#pragma unroll
+    for (int u = 0; u < NT; u++) slot[u] = RD != nullptr && act[u] ? tp.leafslot[tile[u]] : -1;
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (act[u]) stage_async(X, R, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
@@ -355,19 +364,27 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
         const TileStage& ts = st[u * TPB + g];
         const LevelConst<float> L(pre[u].lc);
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ts.mask + t * 4);
-        st4(X + (size_t)tile[u] * kTileCells + t * 4,
-            colour_update(ts.xs, ts.hx, t, mask4, (pre[u].fcls >> 12) & 0xfffu, L, ld4(ts.b + t * 4), color));
+        const size_t off = (size_t)tile[u] * kTileCells + t * 4;
+        const V4<float> b = ld4(ts.b + t * 4);
+        const V4<float> z = colour_update(ts.xs, ts.hx, t, mask4, (pre[u].fcls >> 12) & 0xfffu, L, b, color);
+        st4(X + off, z);
+        if (slot[u] != -1) {  // uniform over the 128-thread group
+            const double d = warp_sum(dot4f(slot[u] >= 0 ? b : ld4(RD + off), z));
+            if ((t & 31) == 0) WP[4 * (size_t)(slot[u] >= 0 ? slot[u] : -2 - slot[u]) + (t >> 5)] = d;
+        }
     }}
 template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
-                                                        const float* __restrict__ R, int color, const Scalars* __restrict__ S) {
-    k_gs_sweep_body<TPB, NT>(tp, list, n, X, R, color, S);
+                                                        const float* __restrict__ R, int color, const Scalars* __restrict__ S,
+                                                        const float* __restrict__ RD, double* __restrict__ WP) {
+    k_gs_sweep_body<TPB, NT>(tp, list, n, X, R, color, S, RD, WP);
 }
 // the same kernel with at least MINB CTAs per SM (registers capped to fit)
 template <int TPB, int NT, int MINB>
 __global__ void __launch_bounds__(128 * TPB, MINB) k_gs_sweep_occ(Topo tp, const int* __restrict__ list, int n, float* X,
-                                                        const float* __restrict__ R, int color, const Scalars* __restrict__ S) {
-    k_gs_sweep_body<TPB, NT>(tp, list, n, X, R, color, S);
+                                                        const float* __restrict__ R, int color, const Scalars* __restrict__ S,
+                                                        const float* __restrict__ RD, double* __restrict__ WP) {
+    k_gs_sweep_body<TPB, NT>(tp, list, n, X, R, color, S, RD, WP);
 }
 template <int TPB, int NT, int MINB>
 constexpr auto k_gs_sweep_shape() {
@@ -633,19 +650,6 @@ __global__ void __launch_bounds__(256) k_vcycle_init(Topo tp, int n, float* X, f
 // CTA, and the last CTA to finish (ticket counter) sums the partials in a fixed order and runs
 // the epilogue on the scalar state.  Per 4-cell vector the FP32 products are formed as the
 // reference's Dot128Kernel does (src/PoissonGrid.cu:177-181) and widened to FP64.
-__device__ __forceinline__ double dot4f(const V4<float>& a, const V4<float>& b) {
-    float s = fmaf(a.v[0], b.v[0], a.v[1] * b.v[1]);
-    s = fmaf(a.v[2], b.v[2], s);
-    s = fmaf(a.v[3], b.v[3], s);
-    return (double)s;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-
 struct Double2 { double a, b; };
 
 // Block-reduce (a, b), publish the partial, return true in thread 0 of the last CTA with the
@@ -951,6 +955,50 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
     if (chunk_reduce_and_elect(acc_a, acc_b, partials, counters + inst, inst_chunks[inst], tot)) epilogue(epi, tot, Si, P, ctl, inst);
 }
 
+// The r.z partial sums of LEAF tiles that no fused colour sweep updates (those at the levels of
+// the shared-memory kernel): one 128-thread group per tile, per 32-thread quarter the warp sum of
+// the 4-cell products, stored at WP[4 * LEAF slot + quarter] as the colour sweep stores them.
+__global__ void __launch_bounds__(256) k_leaf_wpart(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ R,
+                                                    const float* __restrict__ Z, double* __restrict__ WP, const Scalars* S) {
+    pdl_entry();
+    const int q = (int)blockIdx.x * 2 + ((int)threadIdx.x >> 7);
+    if (q >= n) return;
+    const int t = threadIdx.x & 127;
+    const int tile = list[q];
+    if (tile_done(tp, S, tile)) return;
+    const size_t off = (size_t)tile * kTileCells + t * 4;
+    const double d = warp_sum(dot4f(ld4(R + off), ld4(Z + off)));
+    const int slot = tp.leafslot[tile];
+    if ((t & 31) == 0) WP[4 * (size_t)(slot >= 0 ? slot : -2 - slot) + (t >> 5)] = d;
+}
+
+// Per instance (one CTA each): the sum of the 4 partials of each of its LEAF tiles in LEAF-list
+// order (thread-strided, then warp trees, then the 8 warp sums in order), then the epilogue.  The
+// order is fixed and involves only the instance's own tiles.
+__global__ void __launch_bounds__(256) k_inst_wsum(const int2* __restrict__ ranges, const double* __restrict__ WP, Scalars* S,
+                                                   const InstParams* __restrict__ ip, SolveCtl ctl, int epi, int skip) {
+    pdl_entry();
+    __shared__ double ws[8];
+    const int inst = blockIdx.x;
+    Scalars* Si = S + inst;
+    const InstParams P = ip[inst];
+    if (!P.active || (skip == SKIP_DONE && Si->done)) return;
+    const int2 r = ranges[inst];
+    const double* w = WP + 4 * (size_t)r.x;
+    double acc = 0.0;
+#pragma unroll 8
+    for (int i = threadIdx.x; i < 4 * r.y; i += 256) acc += w[i];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) tot += ws[k];
+        epilogue(epi, Double2{tot, 0.0}, Si, P, ctl, inst);
+    }
+}
+
 // Start of a solve: per-instance scalars zeroed, instances outside the solve marked done, the
 // count of iterating instances set (0 ends the graph's loop at once).
 __global__ void __launch_bounds__(256) k_begin(Scalars* S, const InstParams* __restrict__ ip, int ninst, SolveCtl ctl) {
@@ -1172,26 +1220,28 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
 // Launch shapes of the staged kernels: TPB tiles per CTA side by side, NT tiles per 128-thread
 // group in flight.
 template <int TPB, int NT, int MINB = 0>
-void gs_sweep_shape(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s) {
+void gs_sweep_shape(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s,
+                    const float* RD) {
     const int n = g.mg_count[level];
     const int per = TPB * NT;
     launch_kernel(k_gs_sweep_shape<TPB, NT, MINB>(), (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
-                  g.d_mg + g.mg_offset[level], n, X, R, color, S);
+                  g.d_mg + g.mg_offset[level], n, X, R, color, S, RD, RD ? g.d_wpart : nullptr);
 }
 
-void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s) {
+void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s,
+              const float* RD) {
     const int n = g.mg_count[level];
     if (n == 0) return;
     ++g.launch_count;
     switch (g.shape(KS_GS_SWEEP, level)) {
-    case 0: gs_sweep_shape<2, 1>(g, level, X, R, color, S, s); break;
-    case 1: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s); break;
-    case 2: gs_sweep_shape<1, 4>(g, level, X, R, color, S, s); break;
-    case 3: gs_sweep_shape<2, 4>(g, level, X, R, color, S, s); break;
-    case 4: gs_sweep_shape<1, 1>(g, level, X, R, color, S, s); break;
-    case 5: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s); break;
-    case 6: gs_sweep_shape<1, 1, 16>(g, level, X, R, color, S, s); break;
-    default: gs_sweep_shape<1, 1, 12>(g, level, X, R, color, S, s); break;
+    case 0: gs_sweep_shape<2, 1>(g, level, X, R, color, S, s, RD); break;
+    case 1: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s, RD); break;
+    case 2: gs_sweep_shape<1, 4>(g, level, X, R, color, S, s, RD); break;
+    case 3: gs_sweep_shape<2, 4>(g, level, X, R, color, S, s, RD); break;
+    case 4: gs_sweep_shape<1, 1>(g, level, X, R, color, S, s, RD); break;
+    case 5: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s, RD); break;
+    case 6: gs_sweep_shape<1, 1, 16>(g, level, X, R, color, S, s, RD); break;
+    default: gs_sweep_shape<1, 1, 12>(g, level, X, R, color, S, s, RD); break;
     }
 }
 
@@ -1350,6 +1400,18 @@ void inst_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* 
     case OP_PAP: CIRRUS_INST_REDUCE(OP_PAP); break;
     }
 #undef CIRRUS_INST_REDUCE
+}
+
+void leaf_wpart(const DevGrid& g, const float* R, const float* Z, cudaStream_t s) {
+    if (g.n_bottom_leaves == 0) return;
+    ++g.launch_count;
+    launch_kernel(k_leaf_wpart, (g.n_bottom_leaves + 1) / 2, 256, 0, s, g.topo, g.d_bottom_leaves, g.n_bottom_leaves, R, Z, g.d_wpart,
+                  (const Scalars*)g.d_scalars);
+}
+void inst_wsum(const DevGrid& g, const SolveCtl& ctl, int epi, int skip, cudaStream_t s) {
+    ++g.launch_count;
+    launch_kernel(k_inst_wsum, g.num_inst, 256, 0, s, g.d_inst_leafrange, (const double*)g.d_wpart, g.d_scalars,
+                  (const InstParams*)g.d_iparams, ctl, epi, skip);
 }
 
 void grid_dot(const DevGrid& g, const float* A, const float* B, cudaStream_t s) {

@@ -437,4 +437,19 @@ __device__ __forceinline__ V4<T> stage_tile(const T* __restrict__ X, int tile, c
     return own;
 }
 
+// 4-cell dot product as the reference's Dot128Kernel forms it (src/PoissonGrid.cu:177-181): FP32
+// products and sums, widened to FP64.
+__device__ __forceinline__ double dot4f(const V4<float>& a, const V4<float>& b) {
+    float s = fmaf(a.v[0], b.v[0], a.v[1] * b.v[1]);
+    s = fmaf(a.v[2], b.v[2], s);
+    s = fmaf(a.v[3], b.v[3], s);
+    return (double)s;
+}
+// shuffle-down tree over a full warp; lane 0 holds the sum
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
 }  // namespace cirrus

@@ -69,7 +69,7 @@ bool use_fused(const DevGrid& g, int level_iters, int coarsest_iters) {
 }
 
 void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, float one_over_alpha, float prolong_coeff,
-                  const Scalars* S, cudaStream_t s) {
+                  const Scalars* S, cudaStream_t s, const float* dot_r) {
     const int lb = g.bottom_level;
     for (int l = g.max_level; l > lb; l--) {
         launch::presmooth(g, l, g.d_xpre, RHS, S, s);
@@ -78,8 +78,9 @@ void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, fl
     launch::bottom(g, lb, coarsest_iters, X, RHS, one_over_alpha, prolong_coeff, S, s);
     for (int l = lb + 1; l <= g.max_level; l++) {
         launch::prolong_sweep(g, l, X, g.d_xpre, RHS, prolong_coeff, S, s);
-        launch::gs_sweep(g, l, X, RHS, 0, S, s);
+        launch::gs_sweep(g, l, X, RHS, 0, S, s, dot_r);
     }
+    if (dot_r) launch::leaf_wpart(g, dot_r, X, s);
 }
 
 namespace {
@@ -90,10 +91,12 @@ struct Ch {
 Ch channels(const DevGrid& g) { return {g.d_ch[kChX], g.d_ch[kChR], g.d_ch[kChP], g.d_ch[kChAp], g.d_ch[kChZ]}; }
 
 // z <- M^-1 r with the fused kernels when level_iters == 1 (RHS already holds r on LEAF tiles).
-void precondition(const DevGrid& g, const SolveParams& p, cudaStream_t s) {
+// with_dot: the fused V-cycle also leaves the r.z partial sums in d_wpart (see k_gs_sweep_body).
+void precondition(const DevGrid& g, const SolveParams& p, cudaStream_t s, bool with_dot = false) {
     const Ch c = channels(g);
     const Scalars* S = g.d_scalars;
-    if (use_fused(g, p.level_iters, p.coarsest_iters)) vcycle_fused(g, c.z, c.ap, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, S, s);
+    if (use_fused(g, p.level_iters, p.coarsest_iters))
+        vcycle_fused(g, c.z, c.ap, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, S, s, with_dot ? c.r : nullptr);
     else vcycle(g, c.z, c.r, c.ap, p.level_iters, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, S, s);
 }
 
@@ -128,8 +131,13 @@ void record_body(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl, cu
         launch::inst_reduce(OP_MEAN, g, c.r, nullptr, nullptr, nullptr, ctl, EPI_MEAN, SKIP_DONE, s);
         launch::recenter(g, c.r, c.ap, s);
     }
-    precondition(g, p, s);
-    launch::inst_reduce(OP_DOT, g, c.r, c.z, nullptr, nullptr, ctl, EPI_BETA, SKIP_DONE, s);
+    if (use_fused(g, p.level_iters, p.coarsest_iters)) {
+        precondition(g, p, s, true);  // r.z partial sums formed by the V-cycle's last colour sweeps
+        launch::inst_wsum(g, ctl, EPI_BETA, SKIP_DONE, s);
+    } else {
+        precondition(g, p, s);
+        launch::inst_reduce(OP_DOT, g, c.r, c.z, nullptr, nullptr, ctl, EPI_BETA, SKIP_DONE, s);
+    }
     launch::update_p(g, c.p, c.z, s);
 }
 
