@@ -79,7 +79,8 @@ int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
         }
     };
     for (int l = lo; l <= g.max_level; l++) {
-        if (g.mg_count[l] > 0) pick(KS_GS_SWEEP, l, [&] { launch::gs_sweep(g, l, z, ap, 0, nullptr, s); });
+        // the colour sweep as the solve runs it: with the r.z tile parts (r taken from channel p here)
+        if (g.mg_count[l] > 0) pick(KS_GS_SWEEP, l, [&] { launch::gs_sweep(g, l, z, ap, 0, nullptr, s, p); });
         if (g.mg_count[l] > 0 && g.bottom_level >= 0)
             pick(KS_PRESMOOTH, l, [&] { launch::presmooth(g, l, g.d_xpre, ap, nullptr, s); });
         if (l >= 1 && g.level_count[l] > 0)
@@ -87,7 +88,7 @@ int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
         if (l >= 1 && g.level_count[l] > 0 && g.bottom_level >= 0)
             pick(KS_PROLONG, l, [&] { launch::prolong_sweep(g, l, z, g.d_xpre, ap, 1.f, nullptr, s); });
     }
-    if (g.n_lapmain + g.n_lapitems > 0) pick(KS_LAPLACIAN, 0, [&] { launch::laplacian_fused(g, p, tmp, nullptr, s); });
+    if (g.n_lapmain + g.n_lapitems > 0) pick(KS_LAPLACIAN, 0, [&] { launch::laplacian_fused(g, p, tmp, nullptr, s, true); });
     g.launch_count = count0;
     drop_graphs(g);
     const bool ok = cudaStreamSynchronize(s) == cudaSuccess;

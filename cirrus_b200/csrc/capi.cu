@@ -699,8 +699,8 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
     cudaStream_t s = S(stream);
     for (int i = 0; i < reps; i++) {
         switch (kernel) {
-        case CIRRUS_KERNEL_LAPLACIAN: cirrus::launch::laplacian_fused(g, p, tmp, nullptr, s); break;
-        case CIRRUS_KERNEL_GS_SWEEP: cirrus::launch::gs_sweep(g, level, z, ap, i & 1, nullptr, s); break;
+        case CIRRUS_KERNEL_LAPLACIAN: cirrus::launch::laplacian_fused(g, p, tmp, nullptr, s, true); break;
+        case CIRRUS_KERNEL_GS_SWEEP: cirrus::launch::gs_sweep(g, level, z, ap, i & 1, nullptr, s, p); break;
         case CIRRUS_KERNEL_PRESMOOTH: cirrus::launch::presmooth(g, level, g.d_xpre, ap, nullptr, s); break;
         case CIRRUS_KERNEL_PROLONG_SWEEP: cirrus::launch::prolong_sweep(g, level, z, g.d_xpre, ap, 1.f, nullptr, s); break;
         case CIRRUS_KERNEL_RESIDUAL_RESTRICT: cirrus::launch::residual_restrict(g, level, g.d_xpre, ap, tmp, 1.f, nullptr, s, true); break;

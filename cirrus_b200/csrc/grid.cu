@@ -565,7 +565,7 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
     }
     // LEAF slots (with the GHOST-children mark), per-instance LEAF ranges, bottom-level LEAF tiles
     {
-        std::vector<int> slot(n, -1), bl;
+        std::vector<int> slot(n, -1), bl, gp;
         for (size_t q = 0; q < leaf.size(); q++) {
             const int t = leaf[q];
             bool kids = false;
@@ -574,6 +574,7 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
                 kids = kids || (c >= 0 && (type[c] & GHOST_T));
             }
             slot[t] = kids ? -2 - (int)q : (int)q;
+            if (kids) gp.push_back(t);
             if (level[t] <= g->bottom_level) bl.push_back(t);
         }
         std::vector<int2> lr(K);
@@ -587,7 +588,10 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
         g->n_bottom_leaves = (int)bl.size();
         bl.push_back(0);
         CK((cudaError_t)(upload(&g->d_bottom_leaves, bl) ? cudaErrorMemoryAllocation : cudaSuccess));
-        CK(cudaMalloc(&g->d_wpart, sizeof(double) * 4 * std::max<size_t>(leaf.size(), 1)));
+        g->n_gpar_leaves = (int)gp.size();
+        gp.push_back(0);
+        CK((cudaError_t)(upload(&g->d_gpar_leaves, gp) ? cudaErrorMemoryAllocation : cudaSuccess));
+        CK(cudaMalloc(&g->d_wpart, sizeof(double) * std::max<size_t>(leaf.size(), 1)));
     }
     CK(cudaMalloc(&g->d_partials, sizeof(double) * 2 * std::max(g->red_blocks, g->n_chunks)));
     CK(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
@@ -660,6 +664,7 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_wpart);
     cudaFree(g->d_inst_leafrange);
     cudaFree(g->d_bottom_leaves);
+    cudaFree(g->d_gpar_leaves);
     cudaFree(g->d_chunks);
     cudaFree(g->d_inst_chunks);
     cudaFree(g->d_partials);

@@ -196,11 +196,15 @@ __device__ __forceinline__ void ghost_face_sum(const Topo& tp, const float* __re
 // coupled face of a face-path GHOST tile); the others take `list` (LEAF tiles and GHOST tiles
 // coupled inside), staged with asynchronous copies, NT per 128-thread group.  Row entries in
 // neither are constant zeros (set when the grid is created).
+// With WP the launch also stores, for every LEAF tile without GHOST children (whose A p is final
+// here), the tile's part of p.Ap (tile_part_sum of the threads' 4-cell FP32 products) at
+// WP[LEAF slot]; k_pap_ghost forms those of the other LEAF tiles.
 template <int TPB, int NT>
 __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
                                                                int nitems, int item_blocks,
                                                                const float* __restrict__ X, float* __restrict__ Y,
-                                                               float* __restrict__ GACC, const Scalars* __restrict__ S) {
+                                                               float* __restrict__ GACC, const Scalars* __restrict__ S,
+                                                               double* __restrict__ WP) {
     pdl_entry();
     if ((int)blockIdx.x < item_blocks) {
         const int q = (int)blockIdx.x * (128 * TPB) + (int)threadIdx.x;
@@ -225,7 +229,10 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
     tile_pre(tp, tile, t, pre);
 #pragma unroll
     for (int u = 0; u < NT; u++)
-        if (act[u]) stage_async(X, nullptr, tp.mask_lap, tile[u], pre[u].nb, t, st[u * TPB + g]);
+        if (act[u]) {
+            stage_async(X, nullptr, tp.mask_lap, tile[u], pre[u].nb, t, st[u * TPB + g]);
+            if (WP != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
+        }
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
@@ -249,10 +256,22 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
             V4<float> o;
             o.v[0] = out[0]; o.v[1] = out[1]; o.v[2] = out[2]; o.v[3] = out[3];
             st4(Y + (size_t)tile[u] * kTileCells + t * 4, o);
+            // the thread's p.Ap term, in its own (already read) mask bytes
+            if (WP != nullptr && ts.aux[0] >= 0) reinterpret_cast<float*>(ts.mask)[t] = dot4f32(ld4(ts.xs + t * 4), o);
         }
     }
     __syncthreads();
-    if (t >= 64) return;
+    if (t >= 64) {
+        if (WP == nullptr || t >= 96) return;
+#pragma unroll
+        for (int u = 0; u < NT; u++) {  // warp 2 of each group sums its LEAF tiles' terms
+            const TileStage& ts = st[u * TPB + g];
+            if (!act[u] || ghost[u] || ts.aux[0] < 0) continue;
+            const double d = tile_part_sum(reinterpret_cast<const float*>(ts.mask), t - 64);
+            if (t == 64) WP[ts.aux[0]] = d;
+        }
+        return;
+    }
     const int fi = t / 16 * 2, fj = (t / 4) % 4 * 2, fk = t % 4 * 2;
 #pragma unroll
     for (int u = 0; u < NT; u++) {
@@ -271,16 +290,18 @@ template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
                                                                int nitems, int item_blocks,
                                                                const float* __restrict__ X, float* __restrict__ Y,
-                                                               float* __restrict__ GACC, const Scalars* __restrict__ S) {
-    k_laplacian_fused_body<TPB, NT>(tp, list, n, items, nitems, item_blocks, X, Y, GACC, S);
+                                                               float* __restrict__ GACC, const Scalars* __restrict__ S,
+                                                               double* __restrict__ WP) {
+    k_laplacian_fused_body<TPB, NT>(tp, list, n, items, nitems, item_blocks, X, Y, GACC, S, WP);
 }
 // the same kernel with at least MINB CTAs per SM (registers capped to fit)
 template <int TPB, int NT, int MINB>
 __global__ void __launch_bounds__(128 * TPB, MINB) k_laplacian_fused_occ(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
                                                                int nitems, int item_blocks,
                                                                const float* __restrict__ X, float* __restrict__ Y,
-                                                               float* __restrict__ GACC, const Scalars* __restrict__ S) {
-    k_laplacian_fused_body<TPB, NT>(tp, list, n, items, nitems, item_blocks, X, Y, GACC, S);
+                                                               float* __restrict__ GACC, const Scalars* __restrict__ S,
+                                                               double* __restrict__ WP) {
+    k_laplacian_fused_body<TPB, NT>(tp, list, n, items, nitems, item_blocks, X, Y, GACC, S, WP);
 }
 template <int TPB, int NT, int MINB>
 constexpr auto k_laplacian_fused_shape() {
@@ -325,11 +346,11 @@ __global__ void __launch_bounds__(64) k_accumulate_ghosts(Topo tp, const int* __
 // x += (b - A x) / D on INTERIOR cells.
 // The tiles of a CTA are NT groups of TPB consecutive list entries, one 128-thread group per
 // tile, all staged with asynchronous copies before any is computed (NT tiles per group in flight).
-// With RD (the PCG residual r) the sweep also forms, for every LEAF tile it updates, the partial
-// sums of the next r.z (DotAsync, src/GMGSolver.cu:636-640): per 32-thread quarter of the tile the
-// 4-cell FP32 products widened to FP64 and warp-summed, stored at WP[4 * LEAF slot + quarter].  A
-// LEAF tile's z is final after this sweep (finer levels only read it).  Its r is the staged
-// right-hand side unless GHOST children added their residuals to that copy; then r is read.
+// With RD (the PCG residual r) the sweep also forms, for every LEAF tile it updates, the tile's
+// part of the next r.z (DotAsync, src/GMGSolver.cu:636-640) and stores it at WP[LEAF slot]; the
+// tile part is tile_part_sum of the threads' 4-cell FP32 products.  A LEAF tile's z is final
+// after this sweep (finer levels only read it).  Its r is the staged right-hand side unless GHOST
+// children added their residuals to that copy; then r is read.
 template <int TPB, int NT>
 __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__ list, int n, float* X,
                                                         const float* __restrict__ R, int color, const Scalars* __restrict__ S,
@@ -348,12 +369,12 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
     }
     TilePre pre[NT];
     tile_pre(tp, tile, t, pre);
-    int slot[NT];
-#pragma unroll
-    for (int u = 0; u < NT; u++) slot[u] = RD != nullptr && act[u] ? tp.leafslot[tile[u]] : -1;
 #pragma unroll
     for (int u = 0; u < NT; u++)
-        if (act[u]) stage_async(X, R, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
+        if (act[u]) {
+            stage_async(X, R, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
+            if (RD != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
+        }
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
@@ -361,17 +382,28 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
-        const TileStage& ts = st[u * TPB + g];
+        TileStage& ts = st[u * TPB + g];
         const LevelConst<float> L(pre[u].lc);
         const uint32_t mask4 = *reinterpret_cast<const uint32_t*>(ts.mask + t * 4);
         const size_t off = (size_t)tile[u] * kTileCells + t * 4;
         const V4<float> b = ld4(ts.b + t * 4);
         const V4<float> z = colour_update(ts.xs, ts.hx, t, mask4, (pre[u].fcls >> 12) & 0xfffu, L, b, color);
         st4(X + off, z);
-        if (slot[u] != -1) {  // uniform over the 128-thread group
-            const double d = warp_sum(dot4f(slot[u] >= 0 ? b : ld4(RD + off), z));
-            if ((t & 31) == 0) WP[4 * (size_t)(slot[u] >= 0 ? slot[u] : -2 - slot[u]) + (t >> 5)] = d;
+        if (RD != nullptr) {  // the thread's term, in its own (already read) mask bytes
+            const int sl = ts.aux[0];
+            if (sl != -1) reinterpret_cast<float*>(ts.mask)[t] = dot4f32(sl >= 0 ? b : ld4(RD + off), z);
         }
+    }
+    if (RD == nullptr) return;
+    __syncthreads();
+    if (t >= 32) return;
+#pragma unroll
+    for (int u = 0; u < NT; u++) {  // warp 0 of each group sums its tiles' terms
+        const TileStage& ts = st[u * TPB + g];
+        const int sl = ts.aux[0];
+        if (!act[u] || sl == -1) continue;
+        const double d = tile_part_sum(reinterpret_cast<const float*>(ts.mask), t);
+        if (t == 0) WP[sl >= 0 ? sl : -2 - sl] = d;
     }}
 template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
@@ -955,26 +987,63 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
     if (chunk_reduce_and_elect(acc_a, acc_b, partials, counters + inst, inst_chunks[inst], tot)) epilogue(epi, tot, Si, P, ctl, inst);
 }
 
-// The r.z partial sums of LEAF tiles that no fused colour sweep updates (those at the levels of
-// the shared-memory kernel): one 128-thread group per tile, per 32-thread quarter the warp sum of
-// the 4-cell products, stored at WP[4 * LEAF slot + quarter] as the colour sweep stores them.
+// The r.z tile parts of LEAF tiles that no fused colour sweep updates (those at the levels of the
+// shared-memory kernel), formed as the colour sweep forms them: one warp per tile, lane l taking
+// the 4-cell vectors l, l+32, l+64, l+96.
 __global__ void __launch_bounds__(256) k_leaf_wpart(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ R,
                                                     const float* __restrict__ Z, double* __restrict__ WP, const Scalars* S) {
     pdl_entry();
-    const int q = (int)blockIdx.x * 2 + ((int)threadIdx.x >> 7);
+    const int q = (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5);
     if (q >= n) return;
-    const int t = threadIdx.x & 127;
+    const int l = threadIdx.x & 31;
     const int tile = list[q];
     if (tile_done(tp, S, tile)) return;
-    const size_t off = (size_t)tile * kTileCells + t * 4;
-    const double d = warp_sum(dot4f(ld4(R + off), ld4(Z + off)));
+    const size_t base = (size_t)tile * kTileCells + l * 4;
+    float term[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) term[k] = dot4f32(ld4(R + base + 128 * k), ld4(Z + base + 128 * k));
+    const double d = lane_part_sum(term);
     const int slot = tp.leafslot[tile];
-    if ((t & 31) == 0) WP[4 * (size_t)(slot >= 0 ? slot : -2 - slot) + (t >> 5)] = d;
+    if (l == 0) WP[slot >= 0 ? slot : -2 - slot] = d;
 }
 
-// Per instance (one CTA each): the sum of the 4 partials of each of its LEAF tiles in LEAF-list
-// order (thread-strided, then warp trees, then the 8 warp sums in order), then the epilogue.  The
-// order is fixed and involves only the instance's own tiles.
+// The p.Ap tile parts of the LEAF tiles with GHOST children: their A p first receives the
+// children's 2x2x2 sums (the rows the fused Laplacian left in GACC, added in AccumulateToParents's
+// way: Ap + sum), then the part is formed as the Laplacian forms it: one warp per tile, lane l
+// taking the 4-cell vectors l, l+32, l+64, l+96.
+__global__ void __launch_bounds__(256) k_pap_ghost(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ P,
+                                                   float* AP, const float* __restrict__ GACC, double* __restrict__ WP,
+                                                   const Scalars* S) {
+    pdl_entry();
+    const int q = (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5);
+    if (q >= n) return;
+    const int l = threadIdx.x & 31;
+    const int tile = list[q];
+    if (tile_done(tp, S, tile)) return;
+    float term[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int qv = l + 32 * k;
+        const size_t off = (size_t)tile * kTileCells + qv * 4;
+        const V4<float> p = ld4(P + off);
+        V4<float> ap = ld4(AP + off);
+        const int i = qv >> 4, j = (qv >> 1) & 7, k0 = (qv & 1) * 4;
+        const int gs = tp.ghost_child[(size_t)tile * 8 + ((i >> 2) | ((j >> 2) << 1) | ((k0 >> 2) << 2))];
+        if (gs >= 0) {
+            const float* row = GACC + (size_t)gs * 64 + (i & 3) * 16 + (j & 3) * 4 + (k0 & 3);
+#pragma unroll
+            for (int e = 0; e < 4; e++) ap.v[e] = ap.v[e] + row[e];
+            st4(AP + off, ap);
+        }
+        term[k] = dot4f32(p, ap);
+    }
+    const double d = lane_part_sum(term);
+    if (l == 0) WP[-2 - tp.leafslot[tile]] = d;
+}
+
+// Per instance (one CTA each): the sum of its LEAF tiles' parts in LEAF-list order (thread-strided,
+// warp trees, then the 8 warp sums in order), then the epilogue.  The order is fixed and involves
+// only the instance's own tiles.
 __global__ void __launch_bounds__(256) k_inst_wsum(const int2* __restrict__ ranges, const double* __restrict__ WP, Scalars* S,
                                                    const InstParams* __restrict__ ip, SolveCtl ctl, int epi, int skip) {
     pdl_entry();
@@ -984,10 +1053,10 @@ __global__ void __launch_bounds__(256) k_inst_wsum(const int2* __restrict__ rang
     const InstParams P = ip[inst];
     if (!P.active || (skip == SKIP_DONE && Si->done)) return;
     const int2 r = ranges[inst];
-    const double* w = WP + 4 * (size_t)r.x;
+    const double* w = WP + r.x;
     double acc = 0.0;
-#pragma unroll 8
-    for (int i = threadIdx.x; i < 4 * r.y; i += 256) acc += w[i];
+#pragma unroll 4
+    for (int i = threadIdx.x; i < r.y; i += 256) acc += w[i];
     acc = warp_sum(acc);
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
     __syncthreads();
@@ -1195,26 +1264,33 @@ template void full_laplacian<float>(const DevGrid&, float*, float*, const Scalar
 template void full_laplacian<double>(const DevGrid&, double*, double*, const Scalars*, cudaStream_t);
 
 template <int TPB, int NT, int MINB = 0>
-void laplacian_shape(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s) {
+void laplacian_shape(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s, double* WP) {
     const int per = TPB * NT;
     const int item_blocks = (g.n_lapitems + 128 * TPB - 1) / (128 * TPB);
     launch_kernel(k_laplacian_fused_shape<TPB, NT, MINB>(), item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
-                  g.topo, g.d_lapmain, g.n_lapmain, g.d_lapitems, g.n_lapitems, item_blocks, X, Y, g.d_gacc, S);
+                  g.topo, g.d_lapmain, g.n_lapmain, g.d_lapitems, g.n_lapitems, item_blocks, X, Y, g.d_gacc, S, WP);
 }
 
-void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s) {
+void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s, bool with_pap) {
     if (g.n_lapmain + g.n_lapitems == 0) return;
     ++g.launch_count;
+    double* WP = with_pap ? g.d_wpart : nullptr;
     switch (g.shape(KS_LAPLACIAN, 0)) {
-    case 0: laplacian_shape<2, 1>(g, X, Y, S, s); break;
-    case 1: laplacian_shape<2, 2>(g, X, Y, S, s); break;
-    case 2: laplacian_shape<1, 4>(g, X, Y, S, s); break;
-    case 3: laplacian_shape<2, 4>(g, X, Y, S, s); break;
-    case 4: laplacian_shape<1, 1>(g, X, Y, S, s); break;
-    case 5: laplacian_shape<1, 2>(g, X, Y, S, s); break;
-    case 6: laplacian_shape<1, 1, 16>(g, X, Y, S, s); break;
-    default: laplacian_shape<1, 1, 12>(g, X, Y, S, s); break;
+    case 0: laplacian_shape<2, 1>(g, X, Y, S, s, WP); break;
+    case 1: laplacian_shape<2, 2>(g, X, Y, S, s, WP); break;
+    case 2: laplacian_shape<1, 4>(g, X, Y, S, s, WP); break;
+    case 3: laplacian_shape<2, 4>(g, X, Y, S, s, WP); break;
+    case 4: laplacian_shape<1, 1>(g, X, Y, S, s, WP); break;
+    case 5: laplacian_shape<1, 2>(g, X, Y, S, s, WP); break;
+    case 6: laplacian_shape<1, 1, 16>(g, X, Y, S, s, WP); break;
+    default: laplacian_shape<1, 1, 12>(g, X, Y, S, s, WP); break;
     }
+}
+void pap_ghost(const DevGrid& g, const float* P, float* AP, cudaStream_t s) {
+    if (g.n_gpar_leaves == 0) return;
+    ++g.launch_count;
+    launch_kernel(k_pap_ghost, (g.n_gpar_leaves + 7) / 8, 256, 0, s, g.topo, g.d_gpar_leaves, g.n_gpar_leaves, P, AP,
+                  (const float*)g.d_gacc, g.d_wpart, (const Scalars*)g.d_scalars);
 }
 
 // Launch shapes of the staged kernels: TPB tiles per CTA side by side, NT tiles per 128-thread
@@ -1405,7 +1481,7 @@ void inst_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* 
 void leaf_wpart(const DevGrid& g, const float* R, const float* Z, cudaStream_t s) {
     if (g.n_bottom_leaves == 0) return;
     ++g.launch_count;
-    launch_kernel(k_leaf_wpart, (g.n_bottom_leaves + 1) / 2, 256, 0, s, g.topo, g.d_bottom_leaves, g.n_bottom_leaves, R, Z, g.d_wpart,
+    launch_kernel(k_leaf_wpart, (g.n_bottom_leaves + 7) / 8, 256, 0, s, g.topo, g.d_bottom_leaves, g.n_bottom_leaves, R, Z, g.d_wpart,
                   (const Scalars*)g.d_scalars);
 }
 void inst_wsum(const DevGrid& g, const SolveCtl& ctl, int epi, int skip, cudaStream_t s) {

@@ -357,6 +357,7 @@ struct __align__(16) TileStage {
     float hx[6 * 64];
     float b[kTileCells];
     uint8_t mask[kTileCells];
+    int aux[4];  // per-tile word copied with the tile (the LEAF slot, for the kernels that form dot partials)
 };
 
 // Neighbour tiles whose halo cells thread t copies: face t>>4 (threads 0..63, 16-byte pieces of
@@ -439,17 +440,32 @@ __device__ __forceinline__ V4<T> stage_tile(const T* __restrict__ X, int tile, c
 
 // 4-cell dot product as the reference's Dot128Kernel forms it (src/PoissonGrid.cu:177-181): FP32
 // products and sums, widened to FP64.
-__device__ __forceinline__ double dot4f(const V4<float>& a, const V4<float>& b) {
+__device__ __forceinline__ float dot4f32(const V4<float>& a, const V4<float>& b) {
     float s = fmaf(a.v[0], b.v[0], a.v[1] * b.v[1]);
     s = fmaf(a.v[2], b.v[2], s);
-    s = fmaf(a.v[3], b.v[3], s);
-    return (double)s;
+    return fmaf(a.v[3], b.v[3], s);
 }
+__device__ __forceinline__ double dot4f(const V4<float>& a, const V4<float>& b) { return (double)dot4f32(a, b); }
 // shuffle-down tree over a full warp; lane 0 holds the sum
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
+}
+// A tile's part of a dot product from its 128 per-vector FP32 terms (vector v's term held by lane
+// v % 32 as term[v / 32]): each lane adds its four terms in FP64 in order, then a warp tree.  All
+// 32 lanes of the warp take part; lane 0 holds the result.
+__device__ __forceinline__ double lane_part_sum(const float term[4]) {
+    double d = (double)term[0];
+    d += (double)term[1];
+    d += (double)term[2];
+    d += (double)term[3];
+    return warp_sum(d);
+}
+// the same from terms laid out by vector in shared memory (terms[v], v = 0..127), lane = l
+__device__ __forceinline__ double tile_part_sum(const float* terms, int l) {
+    const float term[4] = {terms[l], terms[l + 32], terms[l + 64], terms[l + 96]};
+    return lane_part_sum(term);
 }
 
 }  // namespace cirrus

@@ -91,7 +91,7 @@ struct Ch {
 Ch channels(const DevGrid& g) { return {g.d_ch[kChX], g.d_ch[kChR], g.d_ch[kChP], g.d_ch[kChAp], g.d_ch[kChZ]}; }
 
 // z <- M^-1 r with the fused kernels when level_iters == 1 (RHS already holds r on LEAF tiles).
-// with_dot: the fused V-cycle also leaves the r.z partial sums in d_wpart (see k_gs_sweep_body).
+// with_dot: the fused V-cycle also leaves the r.z tile parts in d_wpart (see k_gs_sweep_body).
 void precondition(const DevGrid& g, const SolveParams& p, cudaStream_t s, bool with_dot = false) {
     const Ch c = channels(g);
     const Scalars* S = g.d_scalars;
@@ -120,8 +120,11 @@ void record_prologue(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl
 void record_body(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl, cudaStream_t s) {
     const Ch c = channels(g);
     if (use_fused(g, p.level_iters, p.coarsest_iters)) {
-        launch::laplacian_fused(g, c.p, c.ap, g.d_scalars, s);
-        launch::inst_reduce(OP_PAP, g, c.p, c.ap, g.d_gacc, nullptr, ctl, EPI_ALPHA, SKIP_DONE, s);
+        // p.Ap tile parts: from the Laplacian for LEAF tiles without GHOST children, from
+        // pap_ghost (after adding the children's sums to Ap) for the others
+        launch::laplacian_fused(g, c.p, c.ap, g.d_scalars, s, true);
+        launch::pap_ghost(g, c.p, c.ap, s);
+        launch::inst_wsum(g, ctl, EPI_ALPHA, SKIP_DONE, s);
     } else {
         launch::full_laplacian<float>(g, c.p, c.ap, g.d_scalars, s);
         launch::inst_reduce(OP_DOT, g, c.p, c.ap, nullptr, nullptr, ctl, EPI_ALPHA, SKIP_DONE, s);
@@ -132,7 +135,7 @@ void record_body(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl, cu
         launch::recenter(g, c.r, c.ap, s);
     }
     if (use_fused(g, p.level_iters, p.coarsest_iters)) {
-        precondition(g, p, s, true);  // r.z partial sums formed by the V-cycle's last colour sweeps
+        precondition(g, p, s, true);  // r.z tile parts formed by the V-cycle's last colour sweeps
         launch::inst_wsum(g, ctl, EPI_BETA, SKIP_DONE, s);
     } else {
         precondition(g, p, s);

@@ -134,14 +134,17 @@ struct DevGrid {
 
     // per-instance reductions: chunk table (instance, first vector, end vector) and per instance
     // (first chunk, chunk count)
-    // per-tile partial sums of the PCG dot products formed inside the V-cycle's last colour sweep:
-    // 4 per LEAF tile (one per 32-thread quarter), in LEAF-list order; per instance its first
-    // LEAF slot and count; the LEAF tiles at the shared-memory kernel's levels (summed apart)
+    // per-tile parts of the PCG dot products formed by the stencil kernels (the fused Laplacian for
+    // p.Ap, the V-cycle's last colour sweeps for r.z): one FP64 value per LEAF tile in LEAF-list
+    // order; per instance its first LEAF slot and count; the LEAF tiles at the shared-memory
+    // kernel's levels (their r.z parts formed apart)
     int* d_leafslot = nullptr;
     double* d_wpart = nullptr;
     int2* d_inst_leafrange = nullptr;
     int* d_bottom_leaves = nullptr;
     int n_bottom_leaves = 0;
+    int* d_gpar_leaves = nullptr;  // LEAF tiles with GHOST children
+    int n_gpar_leaves = 0;
     int n_chunks = 0;
     int4* d_chunks = nullptr;
     int2* d_inst_chunks = nullptr;
@@ -214,13 +217,16 @@ void jacobi_update(const DevGrid& g, float* X, const float* R, const float* D, f
 // Dot over the 4-cell vectors of the tiles in `list` (synchronises s; result on the host).
 double list_dot(const DevGrid& g, const float* A, const float* B, const int* list, int n, cudaStream_t s);
 // FullNegativeLaplacian as one launch; the ghost-to-parent sums are completed by OP_PAP.
-void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s);
-// RD: with the PCG residual r, also store the r.z partial sums of the level's LEAF tiles (d_wpart)
+// with_pap: also store the p.Ap tile parts of LEAF tiles without GHOST children (d_wpart)
+void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s, bool with_pap = false);
+// Ap += GHOST children's sums on the LEAF tiles that have them, and their p.Ap tile parts
+void pap_ghost(const DevGrid& g, const float* P, float* AP, cudaStream_t s);
+// RD: with the PCG residual r, also store the r.z tile parts of the level's LEAF tiles (d_wpart)
 void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s,
               const float* RD = nullptr);
-// r.z partial sums (d_wpart) of the LEAF tiles at the shared-memory kernel's levels
+// r.z tile parts (d_wpart) of the LEAF tiles at the shared-memory kernel's levels
 void leaf_wpart(const DevGrid& g, const float* R, const float* Z, cudaStream_t s);
-// per instance: the sum of its LEAF tiles' partials in d_wpart (fixed order), then the epilogue
+// per instance: the sum of its LEAF tiles' parts in d_wpart (fixed order), then the epilogue
 void inst_wsum(const DevGrid& g, const SolveCtl& ctl, int epi, int skip, cudaStream_t s);
 void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t colors, int nsweeps, const Scalars* S,
                  cudaStream_t s);
@@ -282,8 +288,8 @@ void vcycle(const DevGrid& g, float* X, const float* F, float* RHS, int level_it
             float prolong_coeff, const Scalars* S, cudaStream_t s);
 // The same V-cycle with fused kernels (level_iters == 1).  Precondition: RHS holds f on LEAF
 // tiles (the PCG kernels that write r maintain this) and 0 on GHOST tiles; X needs no
-// initialisation.  dot_r (the PCG residual r, optional): also leave the r.z partial sums of every
-// LEAF tile in d_wpart for inst_wsum.
+// initialisation.  dot_r (the PCG residual r, optional): also leave the r.z part of every LEAF
+// tile in d_wpart for inst_wsum.
 void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, float one_over_alpha, float prolong_coeff,
                   const Scalars* S, cudaStream_t s, const float* dot_r = nullptr);
 bool use_fused(const DevGrid& g, int level_iters, int coarsest_iters);

@@ -327,8 +327,10 @@ cirrus_status cirrus_grid_autotune_sweeps(cirrus_grid* grid, const cirrus_solve_
  * channels 2-5 (the solve's scratch) and overwrites them.  level: the level of the per-level
  * kernels (ignored by the others).  No counterpart in the reference. */
 enum {
-    CIRRUS_KERNEL_LAPLACIAN = 0,        /* fused FullNegativeLaplacian over LEAF|GHOST tiles        */
-    CIRRUS_KERNEL_GS_SWEEP = 1,         /* one red-black colour sweep of a level                    */
+    CIRRUS_KERNEL_LAPLACIAN = 0,        /* fused FullNegativeLaplacian over LEAF|GHOST tiles, with
+                                           the p.Ap tile parts it forms in the solve                */
+    CIRRUS_KERNEL_GS_SWEEP = 1,         /* one red-black colour sweep of a level, with the r.z tile
+                                           parts it forms in the solve                              */
     CIRRUS_KERNEL_PRESMOOTH = 2,        /* two-colour pre-smoothing from x = 0 of a level           */
     CIRRUS_KERNEL_PROLONG_SWEEP = 3,    /* prolongation + first post-smoothing colour of a level    */
     CIRRUS_KERNEL_RESIDUAL_RESTRICT = 4,/* residual and restriction of a level                      */
