@@ -914,7 +914,8 @@ __device__ __forceinline__ V4<float> mg_rhs_copy(const Topo& tp, int tile, int q
 //   OP_DOT       a.b                                  (Dot)
 //   OP_INIT      x = 0; D = r; r.r                    (Fill + Dot, src/GMGSolver.cu:537-542)
 //   OP_COPY_DOT  p = z; z.r                           (Copy + DotAsync, :564-568)
-//   OP_XR        x += a p, r -= a Ap (INTERIOR); D = r; r.r  (:587-612)
+//   OP_XR        r -= a Ap (INTERIOR); D = r; r.r      (:587-612; its x += a p is applied by k_update_p,
+//                which reads p anyway, and after the loop by k_x_final)
 //   OP_MEAN      (sum of 4 values, 2*#INTERIOR)       (MeanAsync, src/PoissonGrid.cu:231-325)
 //   OP_PAP       Ap += ghost partial sums (C); p.Ap    (the tail of the fused Laplacian + Dot)
 // skip: SKIP_DONE leaves out finished instances, SKIP_INACTIVE only those outside the solve;
@@ -948,18 +949,13 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
             st4(C + off, z);
             push_to_ghost_child(tp, C, tile, v & 127, z, *reinterpret_cast<const uint32_t*>(tp.ctype + off));
             acc_a += dot4f(z, ld4(B + off));
-        } else if (OP == OP_XR) {  // A = x, B = p, C = r, D = Ap
+        } else if (OP == OP_XR) {  // C = r, D = Ap
             const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
-            V4<float> x = ld4(A + off), r = ld4(C + off);
-            const V4<float> p = ld4(B + off), ap = ld4(D + off);
+            V4<float> r = ld4(C + off);
+            const V4<float> ap = ld4(D + off);
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
-                if ((ct4 >> (8 * e)) & INTERIOR_C) {
-                    x.v[e] = fmaf(alpha, p.v[e], x.v[e]);
-                    r.v[e] = fmaf(-alpha, ap.v[e], r.v[e]);
-                }
-            }
-            st4(A + off, x);
+            for (int e = 0; e < 4; e++)
+                if ((ct4 >> (8 * e)) & INTERIOR_C) r.v[e] = fmaf(-alpha, ap.v[e], r.v[e]);
             st4(C + off, r);
             st4(D + off, mg_rhs_copy(tp, tile, v & 127, r));  // Ap is consumed; the channel now carries r as the multigrid right-hand side
             acc_a += dot4f(r, r);
@@ -1091,12 +1087,13 @@ __global__ void __launch_bounds__(256) k_begin(Scalars* S, const InstParams* __r
     }
 }
 
-// p = z + beta p on INTERIOR cells of LEAF tiles (src/GMGSolver.cu:642-653), per instance; the
-// GHOST children receive the new p (push_to_ghost_child).  One 128-thread group per tile, one
-// 4-cell vector per thread: the tile's values are loaded before its instance's state is read, so
-// the loads do not wait on that lookup.
+// x += alpha p, then p = z + beta p on INTERIOR cells of LEAF tiles (src/GMGSolver.cu:587-600 and
+// 642-653), per instance still iterating: the x update of this iteration, taken out of the x/r
+// pass so that p is read once; the GHOST children receive the new p (push_to_ghost_child).  One
+// 128-thread group per tile, one 4-cell vector per thread: the tile's values are loaded before
+// its instance's state is read, so the loads do not wait on that lookup.
 __global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict__ leaves, int nleaf, float* P,
-                                                  const float* __restrict__ Z, const Scalars* S) {
+                                                  const float* __restrict__ Z, float* X, const Scalars* S) {
     pdl_entry();
     const int q = (int)blockIdx.x * 2 + ((int)threadIdx.x >> 7);
     if (q >= nleaf) return;
@@ -1104,16 +1101,42 @@ __global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict
     const int tile = leaves[q];
     const size_t off = (size_t)tile * kTileCells + t * 4;
     const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
-    V4<float> p = ld4(P + off);
+    V4<float> p = ld4(P + off), x = ld4(X + off);
     const V4<float> z = ld4(Z + off);
     const Scalars& Si = S[tp.inst[tile]];
     if (Si.done) return;
-    const float beta = (float)Si.beta;
+    const float alpha = (float)Si.alpha, beta = (float)Si.beta;
 #pragma unroll
     for (int e = 0; e < 4; e++)
-        if ((ct4 >> (8 * e)) & INTERIOR_C) p.v[e] = fmaf(beta, p.v[e], z.v[e]);
+        if ((ct4 >> (8 * e)) & INTERIOR_C) {
+            x.v[e] = fmaf(alpha, p.v[e], x.v[e]);
+            p.v[e] = fmaf(beta, p.v[e], z.v[e]);
+        }
+    st4(X + off, x);
     st4(P + off, p);
     push_to_ghost_child(tp, P, tile, t, p, ct4);
+}
+
+// After the loop: the last iteration's x += alpha p (its k_update_p did not run: the instance
+// stopped in that iteration's x/r pass) for every instance that iterated at least once.
+__global__ void __launch_bounds__(256) k_x_final(Topo tp, const int* __restrict__ leaves, int nleaf, float* X,
+                                                 const float* __restrict__ P, const Scalars* S) {
+    pdl_entry();
+    const int q = (int)blockIdx.x * 2 + ((int)threadIdx.x >> 7);
+    if (q >= nleaf) return;
+    const int t = threadIdx.x & 127;
+    const int tile = leaves[q];
+    const Scalars& Si = S[tp.inst[tile]];
+    if (Si.iter == 0) return;
+    const size_t off = (size_t)tile * kTileCells + t * 4;
+    const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+    V4<float> x = ld4(X + off);
+    const V4<float> p = ld4(P + off);
+    const float alpha = (float)Si.alpha;
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+        if ((ct4 >> (8 * e)) & INTERIOR_C) x.v[e] = fmaf(alpha, p.v[e], x.v[e]);
+    st4(X + off, x);
 }
 
 // r -= mean on INTERIOR cells of LEAF tiles (ReCenterLeafVoxels, src/PoissonSolver.cu:356-368)
@@ -1505,10 +1528,15 @@ void begin_solve(const DevGrid& g, const SolveCtl& ctl, cudaStream_t s) {
     launch_kernel(k_begin, 1, 256, 0, s, g.d_scalars, g.d_iparams, g.num_inst, ctl);
 }
 
-void update_p(const DevGrid& g, float* P, const float* Z, cudaStream_t s) {
+void update_p(const DevGrid& g, float* P, const float* Z, float* X, cudaStream_t s) {
     if (g.n_leaf == 0) return;
     ++g.launch_count;
-    launch_kernel(k_update_p, (g.n_leaf + 1) / 2, 256, 0, s, g.topo, g.d_leaf, g.n_leaf, P, Z, (const Scalars*)g.d_scalars);
+    launch_kernel(k_update_p, (g.n_leaf + 1) / 2, 256, 0, s, g.topo, g.d_leaf, g.n_leaf, P, Z, X, (const Scalars*)g.d_scalars);
+}
+void x_final(const DevGrid& g, float* X, const float* P, cudaStream_t s) {
+    if (g.n_leaf == 0) return;
+    ++g.launch_count;
+    launch_kernel(k_x_final, (g.n_leaf + 1) / 2, 256, 0, s, g.topo, g.d_leaf, g.n_leaf, X, P, (const Scalars*)g.d_scalars);
 }
 
 void recenter(const DevGrid& g, float* R, float* RC, cudaStream_t s) {

@@ -141,11 +141,12 @@ void record_body(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl, cu
         precondition(g, p, s);
         launch::inst_reduce(OP_DOT, g, c.r, c.z, nullptr, nullptr, ctl, EPI_BETA, SKIP_DONE, s);
     }
-    launch::update_p(g, c.p, c.z, s);
+    launch::update_p(g, c.p, c.z, c.x, s);
 }
 
 void record_epilogue(const DevGrid& g, const SolveCtl& ctl, cudaStream_t s) {
     const Ch c = channels(g);
+    launch::x_final(g, c.x, c.p, s);
     launch::inst_reduce(OP_DOT, g, c.r, c.r, nullptr, nullptr, ctl, EPI_FINAL, SKIP_INACTIVE, s);
 }
 

@@ -248,7 +248,10 @@ void leaf_dot_raw(const float* A, const float* B, const int* leaves, int nleaf, 
                   unsigned int* counter, Scalars* S, cudaStream_t s);
 // Sets up the per-instance scalars of a solve from g.d_iparams.
 void begin_solve(const DevGrid& g, const SolveCtl& ctl, cudaStream_t s);
-void update_p(const DevGrid& g, float* P, const float* Z, cudaStream_t s);
+// x += alpha p and p = z + beta p (instances still iterating), p pushed to GHOST children
+void update_p(const DevGrid& g, float* P, const float* Z, float* X, cudaStream_t s);
+// the last iteration's x += alpha p, after the loop
+void x_final(const DevGrid& g, float* X, const float* P, cudaStream_t s);
 void recenter(const DevGrid& g, float* R, float* RC, cudaStream_t s);
 void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s);
 void accumulate_correction(const DevGrid& g, double* X64, float* E, cudaStream_t s);
