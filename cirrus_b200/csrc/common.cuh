@@ -44,7 +44,8 @@ constexpr int kMaskFull = 0x7F;
 // gamma, beta, alpha, gamma_old, fp, mean, count as 7 device doubles, src/GMGSolver.h:22-30).
 struct Scalars {
     double rhs2, thr2, gamma, gamma_old, beta, alpha, fp, res2, mean, rel;
-    int iter, iters, done, converged, nonfinite, pad;
+    int iter, iters, done, converged, nonfinite;
+    int capped;  // reached max_iters unconverged; pure Neumann: stops after this iteration's recentring
 };
 
 // Per-instance parameters of one solve of a (batched) grid, written by the host before each solve.

@@ -775,10 +775,21 @@ __device__ void epilogue(int which, const Double2& tot, Scalars* S, const InstPa
                 return;
             }
         }
-        if (i + 1 >= P.max_iters) finish(S, c);
+        if (i + 1 >= P.max_iters) {
+            // the reference's loop runs its last iteration to the end: a pure-Neumann r is
+            // recentred before the loop exits, so such an instance stops at EPI_BETA
+            if (P.pure_neumann) S->capped = 1;
+            else finish(S, c);
+        }
         break;
     }
-    case EPI_BETA: S->gamma_old = S->gamma; S->gamma = tot.a; S->beta = tot.a / S->gamma_old; break;
+    case EPI_BETA:
+        if (S->capped) {  // the iteration cap of a pure-Neumann instance (EPI_CHECK)
+            finish(S, c);
+            return;
+        }
+        S->gamma_old = S->gamma; S->gamma = tot.a; S->beta = tot.a / S->gamma_old;
+        break;
     case EPI_MEAN: S->mean = tot.a / tot.b; break;
     case EPI_FINAL:
         if (!S->converged && !S->nonfinite) {

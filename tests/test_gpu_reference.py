@@ -233,3 +233,33 @@ def test_laplacian_variants_against_reference(name, built_cache, ref_ok):
         ref.set_channel(3, y0)
         ref.lap_same_level(*case[:3], 2, 3, bool(case[3]))
         assert np.array_equal(bits(g.get_channel(3)), bits(ref.get_channel(3))), case
+
+
+@pytest.mark.parametrize("name", ["sphere64_small", "sphere64_neumann_small"])
+def test_stopping_rules_against_reference(name, built_cache, ref_ok):
+    """GMGSolver::solve's stopping rules (src/GMGSolver.cu:546-551, 612-628, 660-665): an iteration
+    cap reached before convergence, no convergence checks at all (sync_stride 0: max_iters
+    iterations, relative residual -1), and checks every third iteration -- same iteration count,
+    same returned residual, and the pressure of the reference build."""
+    b = built_cache(name)
+    w = b.workload
+    ref = O.RefHarness(w)
+    ref.calc_neighbors()
+    ref.set_ctypes(W.leaf_cell_types(w, b.tiles, b.nbr6))
+    ref.calc_cell_types()
+    ref.calc_neighbors()
+    rhs = ref.rhs(b.velocity)
+    g = DeviceGrid(b.topology)
+    leaf = (b.tiles[:, 4] & W.LEAF) != 0
+    for max_iters, sync_stride in ((3, 1), (5, 0), (1000, 3)):
+        ref.set_channel(1, rhs)
+        rit, rrel, _ = ref.solve(max_iters, 1e-6, 1, 10, sync_stride, w.pure_neumann)
+        g.set_channel(1, rhs)
+        it, rel = GMGSolver().solve(g, False, max_iters, 1e-6, 1, 10, sync_stride, w.pure_neumann)
+        x, rx = g.get_channel(0), ref.get_channel(0)
+        same = float((bits(x)[leaf] == bits(rx)[leaf]).mean())
+        print(f"{name} max_iters {max_iters} sync_stride {sync_stride}: iters {it}/{rit} rel {rel:.6e}/{rrel:.6e} "
+              f"x bitwise {same:.4f}")
+        assert it == rit
+        assert rel == rrel if sync_stride <= 0 else abs(rel - rrel) <= 1e-9 * abs(rrel)
+        assert rel_l2(x, rx, leaf) <= 1e-6
