@@ -132,3 +132,45 @@ def test_damped_jacobi_restatement(name, built_cache):
     f.set_channel_f32(1, np.zeros((b.n, 512), np.float32))
     it, rel = f.damped_jacobi(O.CpuOracle.FP32, 10, 1e-6, omega)
     assert it == 0 and np.isnan(rel)
+
+
+@pytest.mark.parametrize("name", ["sphere64_small", "ring64_small"])
+def test_same_level_laplacian_restatement(name, built_cache):
+    """NegativeLaplacianSameLevel128 restated, tied to the pinned FullNegativeLaplacian: on x with
+    GHOST values already propagated, the same-level operator over all tiles, subtree -1, LEAF|GHOST
+    gives FullNegativeLaplacian's result on every tile that receives no GHOST sums; other tiles
+    and filters leave the target untouched; the diagonal variant is positive on INTERIOR cells."""
+    b = built_cache(name)
+    f = oracle_for(b)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((b.n, 512)).astype(np.float32)
+    f.set_channel_f32(2, x)
+    f.full_lap(O.CpuOracle.FP32, 2, 3)  # also propagates x to the GHOST tiles of channel 2
+    full = f.get_channel_f32(3)
+    y0 = rng.standard_normal((b.n, 512)).astype(np.float32)
+    f.set_channel_f32(4, y0)
+    f.lap_same_level(O.CpuOracle.FP32, -1, -1, W.LEAF | W.GHOST, 2, 4)
+    same = f.get_channel_f32(4)
+    typ, lvl = b.tiles[:, 4], b.tiles[:, 0]
+    lg = (typ & (W.LEAF | W.GHOST)) != 0
+    coords = {tuple(int(v) for v in r[:4]): i for i, r in enumerate(b.tiles)}
+    gparent = np.zeros(b.n, bool)
+    for r in b.tiles[(typ & W.GHOST) != 0]:
+        p = coords.get((int(r[0]) - 1, int(r[1]) // 2, int(r[2]) // 2, int(r[3]) // 2))
+        if p is not None:
+            gparent[p] = True
+    keep = lg & ~gparent
+    assert keep.any() and np.array_equal(same[keep].view(np.uint32), full[keep].view(np.uint32))
+    assert np.array_equal(same[~lg].view(np.uint32), y0[~lg].view(np.uint32))
+    for l in range(int(lvl.max()) + 1):
+        f.set_channel_f32(4, y0)
+        f.lap_same_level(O.CpuOracle.FP32, l, l, W.GHOST, 2, 4)
+        out = f.get_channel_f32(4)
+        untouched = ~((lvl == l) & ((typ & W.GHOST) != 0))
+        assert np.array_equal(out[untouched].view(np.uint32), y0[untouched].view(np.uint32))
+    f.set_channel_f32(4, y0)
+    f.lap_same_level(O.CpuOracle.FP32, -1, -1, W.LEAF, 2, 4, diag=True)
+    d = f.get_channel_f32(4)
+    leaf = (typ & W.LEAF) != 0
+    interior = (b.ctypes & W.INTERIOR) != 0
+    assert np.all(d[leaf][interior[leaf]] > 0)
