@@ -262,14 +262,18 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
     }
     __syncthreads();
     if (t >= 64) {
-        if (WP == nullptr || t >= 96) return;
+        // warps 2 and 3 of each group sum the LEAF tiles' terms, each 16-lane half one tile:
+        // u = 2 * (warp - 2) + half
+        const int u = 2 * ((t - 64) >> 5) + ((t >> 4) & 1);
+        if (WP == nullptr || 2 * ((t - 64) >> 5) >= NT) return;  // whole warps
+        bool ok = false;
 #pragma unroll
-        for (int u = 0; u < NT; u++) {  // warp 2 of each group sums its LEAF tiles' terms
-            const TileStage& ts = st[u * TPB + g];
-            if (!act[u] || ghost[u] || ts.aux[0] < 0) continue;
-            const double d = tile_part_sum(reinterpret_cast<const float*>(ts.mask), t - 64);
-            if (t == 64) WP[ts.aux[0]] = d;
-        }
+        for (int k = 0; k < NT; k++)
+            if (k == u) ok = act[k] && !ghost[k];
+        const TileStage& ts = st[(u < NT ? u : 0) * TPB + g];
+        const int sl = ts.aux[0];
+        const double d = tile_part_sum(reinterpret_cast<const float*>(ts.mask), t & 15);
+        if (ok && u < NT && sl >= 0 && (t & 15) == 0) WP[sl] = d;
         return;
     }
     const int fi = t / 16 * 2, fj = (t / 4) % 4 * 2, fk = t % 4 * 2;
@@ -396,15 +400,18 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
     }
     if (RD == nullptr) return;
     __syncthreads();
-    if (t >= 32) return;
+    // warps 0 and 1 of each group sum the terms, each 16-lane half one tile: u = 2 * warp + half
+    const int u = 2 * (t >> 5) + ((t >> 4) & 1);
+    if (t >= 64 || 2 * (t >> 5) >= NT) return;  // whole warps
+    bool ok = false;
 #pragma unroll
-    for (int u = 0; u < NT; u++) {  // warp 0 of each group sums its tiles' terms
-        const TileStage& ts = st[u * TPB + g];
-        const int sl = ts.aux[0];
-        if (!act[u] || sl == -1) continue;
-        const double d = tile_part_sum(reinterpret_cast<const float*>(ts.mask), t);
-        if (t == 0) WP[sl >= 0 ? sl : -2 - sl] = d;
-    }}
+    for (int k = 0; k < NT; k++)
+        if (k == u) ok = act[k];
+    const TileStage& ts = st[(u < NT ? u : 0) * TPB + g];
+    const int sl = ts.aux[0];
+    const double d = tile_part_sum(reinterpret_cast<const float*>(ts.mask), t & 15);
+    if (ok && u < NT && sl != -1 && (t & 15) == 0) WP[sl >= 0 ? sl : -2 - sl] = d;
+}
 template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_gs_sweep(Topo tp, const int* __restrict__ list, int n, float* X,
                                                         const float* __restrict__ R, int color, const Scalars* __restrict__ S,
@@ -995,42 +1002,44 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
 }
 
 // The r.z tile parts of LEAF tiles that no fused colour sweep updates (those at the levels of the
-// shared-memory kernel), formed as the colour sweep forms them: one warp per tile, lane l taking
-// the 4-cell vectors l, l+32, l+64, l+96.
+// shared-memory kernel), formed as the colour sweep forms them: 16 lanes per tile, lane j taking
+// the 4-cell vectors j, j+16, ..., j+112.
 __global__ void __launch_bounds__(256) k_leaf_wpart(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ R,
                                                     const float* __restrict__ Z, double* __restrict__ WP, const Scalars* S) {
     pdl_entry();
-    const int q = (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5);
-    if (q >= n) return;
-    const int l = threadIdx.x & 31;
-    const int tile = list[q];
-    if (tile_done(tp, S, tile)) return;
-    const size_t base = (size_t)tile * kTileCells + l * 4;
-    float term[4];
+    const int w = (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5);
+    if (2 * w >= n) return;  // whole warps
+    const int j = threadIdx.x & 15;
+    const int q = 2 * w + ((threadIdx.x >> 4) & 1);
+    const int tile = list[q < n ? q : 2 * w];
+    const bool ok = q < n && !tile_done(tp, S, tile);
+    const size_t base = (size_t)tile * kTileCells + j * 4;
+    float term[8];
 #pragma unroll
-    for (int k = 0; k < 4; k++) term[k] = dot4f32(ld4(R + base + 128 * k), ld4(Z + base + 128 * k));
-    const double d = lane_part_sum(term);
+    for (int k = 0; k < 8; k++) term[k] = dot4f32(ld4(R + base + 64 * k), ld4(Z + base + 64 * k));
+    const double d = half_part_sum(term);
     const int slot = tp.leafslot[tile];
-    if (l == 0) WP[slot >= 0 ? slot : -2 - slot] = d;
+    if (ok && j == 0) WP[slot >= 0 ? slot : -2 - slot] = d;
 }
 
 // The p.Ap tile parts of the LEAF tiles with GHOST children: their A p first receives the
 // children's 2x2x2 sums (the rows the fused Laplacian left in GACC, added in AccumulateToParents's
-// way: Ap + sum), then the part is formed as the Laplacian forms it: one warp per tile, lane l
-// taking the 4-cell vectors l, l+32, l+64, l+96.
+// way: Ap + sum), then the part is formed as the Laplacian forms it: 16 lanes per tile, lane j
+// taking the 4-cell vectors j, j+16, ..., j+112.
 __global__ void __launch_bounds__(256) k_pap_ghost(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ P,
                                                    float* AP, const float* __restrict__ GACC, double* __restrict__ WP,
                                                    const Scalars* S) {
     pdl_entry();
-    const int q = (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5);
-    if (q >= n) return;
-    const int l = threadIdx.x & 31;
-    const int tile = list[q];
-    if (tile_done(tp, S, tile)) return;
-    float term[4];
+    const int w = (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5);
+    if (2 * w >= n) return;  // whole warps
+    const int j = threadIdx.x & 15;
+    const int q = 2 * w + ((threadIdx.x >> 4) & 1);
+    const int tile = list[q < n ? q : 2 * w];
+    const bool ok = q < n && !tile_done(tp, S, tile);
+    float term[8];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int qv = l + 32 * k;
+    for (int k = 0; k < 8; k++) {
+        const int qv = j + 16 * k;
         const size_t off = (size_t)tile * kTileCells + qv * 4;
         const V4<float> p = ld4(P + off);
         V4<float> ap = ld4(AP + off);
@@ -1040,12 +1049,12 @@ __global__ void __launch_bounds__(256) k_pap_ghost(Topo tp, const int* __restric
             const float* row = GACC + (size_t)gs * 64 + (i & 3) * 16 + (j & 3) * 4 + (k0 & 3);
 #pragma unroll
             for (int e = 0; e < 4; e++) ap.v[e] = ap.v[e] + row[e];
-            st4(AP + off, ap);
+            if (ok) st4(AP + off, ap);
         }
         term[k] = dot4f32(p, ap);
     }
-    const double d = lane_part_sum(term);
-    if (l == 0) WP[-2 - tp.leafslot[tile]] = d;
+    const double d = half_part_sum(term);
+    if (ok && j == 0) WP[-2 - tp.leafslot[tile]] = d;
 }
 
 // Per instance (one CTA each): the sum of its LEAF tiles' parts in LEAF-list order (thread-strided,
@@ -1323,7 +1332,7 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
 void pap_ghost(const DevGrid& g, const float* P, float* AP, cudaStream_t s) {
     if (g.n_gpar_leaves == 0) return;
     ++g.launch_count;
-    launch_kernel(k_pap_ghost, (g.n_gpar_leaves + 7) / 8, 256, 0, s, g.topo, g.d_gpar_leaves, g.n_gpar_leaves, P, AP,
+    launch_kernel(k_pap_ghost, (g.n_gpar_leaves + 15) / 16, 256, 0, s, g.topo, g.d_gpar_leaves, g.n_gpar_leaves, P, AP,
                   (const float*)g.d_gacc, g.d_wpart, (const Scalars*)g.d_scalars);
 }
 
@@ -1515,7 +1524,7 @@ void inst_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* 
 void leaf_wpart(const DevGrid& g, const float* R, const float* Z, cudaStream_t s) {
     if (g.n_bottom_leaves == 0) return;
     ++g.launch_count;
-    launch_kernel(k_leaf_wpart, (g.n_bottom_leaves + 7) / 8, 256, 0, s, g.topo, g.d_bottom_leaves, g.n_bottom_leaves, R, Z, g.d_wpart,
+    launch_kernel(k_leaf_wpart, (g.n_bottom_leaves + 15) / 16, 256, 0, s, g.topo, g.d_bottom_leaves, g.n_bottom_leaves, R, Z, g.d_wpart,
                   (const Scalars*)g.d_scalars);
 }
 void inst_wsum(const DevGrid& g, const SolveCtl& ctl, int epi, int skip, cudaStream_t s) {

@@ -452,20 +452,25 @@ __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
 }
-// A tile's part of a dot product from its 128 per-vector FP32 terms (vector v's term held by lane
-// v % 32 as term[v / 32]): each lane adds its four terms in FP64 in order, then a warp tree.  All
-// 32 lanes of the warp take part; lane 0 holds the result.
-__device__ __forceinline__ double lane_part_sum(const float term[4]) {
+// A tile's part of a dot product from its 128 per-vector FP32 terms, formed by 16 lanes: lane j
+// (0..15) adds the terms of vectors j, j+16, ..., j+112 in FP64 in that order (term[k] = vector
+// j + 16k), then a 4-level shuffle tree over the 16 lanes.  Both 16-lane halves of the warp take
+// part (each its own tile, or a discarded one); lane 0 of each half holds its tile's part.  The
+// order is the same in every kernel and launch shape.
+__device__ __forceinline__ double half_part_sum(const float term[8]) {
     double d = (double)term[0];
-    d += (double)term[1];
-    d += (double)term[2];
-    d += (double)term[3];
-    return warp_sum(d);
+#pragma unroll
+    for (int k = 1; k < 8; k++) d += (double)term[k];
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o, 16);
+    return d;
 }
-// the same from terms laid out by vector in shared memory (terms[v], v = 0..127), lane = l
-__device__ __forceinline__ double tile_part_sum(const float* terms, int l) {
-    const float term[4] = {terms[l], terms[l + 32], terms[l + 64], terms[l + 96]};
-    return lane_part_sum(term);
+// the same from terms laid out by vector in shared memory (terms[v], v = 0..127), lane j = 0..15
+__device__ __forceinline__ double tile_part_sum(const float* terms, int j) {
+    float term[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) term[k] = terms[j + 16 * k];
+    return half_part_sum(term);
 }
 
 }  // namespace cirrus
