@@ -62,6 +62,12 @@ def test_invalid_arguments_are_rejected_without_a_device():
     assert lib.cirrus_topology_create(0, bad, 0.125, C.byref(h)) == 1
     assert lib.cirrus_gmg_solve(None, None, None, None) == 1
     assert lib.cirrus_grid_create(None, C.byref(h)) == 1
+    it, rel = C.c_int(), C.c_double()
+    assert lib.cirrus_damped_jacobi_solve(None, 10, 1e-6, 1.0, None, C.byref(it), C.byref(rel)) == 1
+    assert lib.cirrus_full_negative_laplacian_ex(None, 2, 3, 1, None) == 1
+    assert lib.cirrus_negative_laplacian_same_level(None, -1, -1, 5, 2, 3, 0, None) == 1
+    assert lib.cirrus_gmg_solve_host_submit(None, None, None, None, None) == 1
+    assert lib.cirrus_gmg_solve_host_wait(None, None) == 1
 
 
 def test_library_is_built_for_sm100a():
