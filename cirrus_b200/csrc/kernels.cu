@@ -935,7 +935,6 @@ __device__ __forceinline__ V4<float> mg_rhs_copy(const Topo& tp, int tile, int q
 //   OP_XR        r -= a Ap (INTERIOR); D = r; r.r      (:587-612; its x += a p is applied by k_update_p,
 //                which reads p anyway, and after the loop by k_x_final)
 //   OP_MEAN      (sum of 4 values, 2*#INTERIOR)       (MeanAsync, src/PoissonGrid.cu:231-325)
-//   OP_PAP       Ap += ghost partial sums (C); p.Ap    (the tail of the fused Laplacian + Dot)
 // skip: SKIP_DONE leaves out finished instances, SKIP_INACTIVE only those outside the solve;
 // OP_MEAN also leaves out instances that are not pure Neumann.
 template <int OP>
@@ -977,19 +976,6 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
             st4(C + off, r);
             st4(D + off, mg_rhs_copy(tp, tile, v & 127, r));  // Ap is consumed; the channel now carries r as the multigrid right-hand side
             acc_a += dot4f(r, r);
-        } else if (OP == OP_PAP) {  // A = p, B = Ap, C = ghost partial sums: Ap += ghost sums; p.Ap
-            const V4<float> p = ld4(A + off);
-            V4<float> ap = ld4(B + off);
-            const int qv = v & 127;
-            const int i = qv >> 4, j = (qv >> 1) & 7, k0 = (qv & 1) * 4;
-            const int gs = tp.ghost_child[(size_t)tile * 8 + ((i >> 2) | ((j >> 2) << 1) | ((k0 >> 2) << 2))];
-            if (gs >= 0) {
-                const float* row = C + (size_t)gs * 64 + (i & 3) * 16 + (j & 3) * 4 + (k0 & 3);
-#pragma unroll
-                for (int e = 0; e < 4; e++) ap.v[e] = ap.v[e] + row[e];
-                st4(B + off, ap);
-            }
-            acc_a += dot4f(p, ap);
         } else if (OP == OP_MEAN) {  // A = channel
             const V4<float> a = ld4(A + off);
             acc_a += (double)(a.v[0] + a.v[1] + a.v[2] + a.v[3]);
@@ -1516,7 +1502,6 @@ void inst_reduce(int op, const DevGrid& g, float* A, float* B, float* C, float* 
     case OP_COPY_DOT: CIRRUS_INST_REDUCE(OP_COPY_DOT); break;
     case OP_XR: CIRRUS_INST_REDUCE(OP_XR); break;
     case OP_MEAN: CIRRUS_INST_REDUCE(OP_MEAN); break;
-    case OP_PAP: CIRRUS_INST_REDUCE(OP_PAP); break;
     }
 #undef CIRRUS_INST_REDUCE
 }

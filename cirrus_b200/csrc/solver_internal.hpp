@@ -36,7 +36,7 @@ struct BottomInst {
     int first[kBottomMaxLevels], cnt[kBottomMaxLevels], sy[kBottomMaxLevels], sz[kBottomMaxLevels];
 };
 
-enum { OP_DOT = 0, OP_INIT = 1, OP_COPY_DOT = 2, OP_XR = 3, OP_MEAN = 4, OP_PAP = 5 };
+enum { OP_DOT = 0, OP_INIT = 1, OP_COPY_DOT = 2, OP_XR = 3, OP_MEAN = 4 };
 enum { SKIP_INACTIVE = 0, SKIP_DONE = 1 };  // which instances a reduction leaves out
 constexpr int kChunkVecs = 1024;            // 4-cell vectors per reduction chunk (one CTA)
 enum { EPI_NONE = -1, EPI_INIT = 0, EPI_GAMMA = 1, EPI_ALPHA = 2, EPI_CHECK = 3, EPI_BETA = 4, EPI_MEAN = 5, EPI_FINAL = 6 };
@@ -216,7 +216,7 @@ void jacobi_residual(const DevGrid& g, const float* B, float* AX, cudaStream_t s
 void jacobi_update(const DevGrid& g, float* X, const float* R, const float* D, float omega, cudaStream_t s);
 // Dot over the 4-cell vectors of the tiles in `list` (synchronises s; result on the host).
 double list_dot(const DevGrid& g, const float* A, const float* B, const int* list, int n, cudaStream_t s);
-// FullNegativeLaplacian as one launch; the ghost-to-parent sums are completed by OP_PAP.
+// FullNegativeLaplacian as one launch; the ghost-to-parent sums are completed by pap_ghost.
 // with_pap: also store the p.Ap tile parts of LEAF tiles without GHOST children (d_wpart)
 void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s, bool with_pap = false);
 // Ap += GHOST children's sums on the LEAF tiles that have them, and their p.Ap tile parts
