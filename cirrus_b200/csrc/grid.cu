@@ -629,7 +629,8 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
     g->topo.lconst = g->d_lconst;
     g->topo.leafslot = g->d_leafslot;
     g->bytes = cells * kNumChannels * sizeof(float) + cells * 3 + sizeof(TileMeta) * n + sizeof(uint32_t) * n + sizeof(int) * nl +
-               sizeof(int) * 22 * (size_t)n + cells * sizeof(float);
+               sizeof(int) * 22 * (size_t)n + cells * sizeof(float) +
+               sizeof(int) * ((size_t)n + g->n_bottom_leaves + g->n_gpar_leaves) + sizeof(double) * leaf.size();
     *out = g;
     return 0;
 }
