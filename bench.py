@@ -93,6 +93,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-batch64", action="store_true", help="skip the 64-instance random-spheres batch")
+    ap.add_argument("--no-side-configs", action="store_true", help="skip the uniform128 / sphere256 single-solve lines")
     return ap.parse_args()
 
 
@@ -564,12 +565,7 @@ def run_ours(args, world, rank, local, pg):
         "vs_baseline": None,
         "dtype": "f32 (fp64 CG scalars)",
         "data": "synthetic (seeded face velocities, divergence right-hand side)",
-        "config": {"workload": f"{args.workload} x{K} batch", "instances_per_step": K, "tiles_per_instance": int(b.tiles.shape[0]),
-                   "dof_per_instance": int(dof),
-                   "effective_resolution": "512x512x1024" if args.workload == "ring512" else args.workload,
-                   "levels": f"leaves {int(b.tiles[(b.tiles[:, 4] & 1) != 0, 0].min())}-{maxl}",
-                   "tolerance": 1e-6, "stopping_rule": "recursive ||r||/||b|| < tol per instance, checked every iteration",
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+        "config": bench_config(args.workload, K, b.tiles, b.ctypes, world),
         "mdof_per_s": round(dof * value / 1e6, 2),
         "iters_per_solve": int(statistics.median(iters_seen)),
         "latency_ms": {"single_p50": round(float(np.percentile(lat, 50)), 4), "single_p99": round(float(np.percentile(lat, 99)), 4),
@@ -605,6 +601,34 @@ def run_ours(args, world, rank, local, pg):
         "clocks": clocks,
     }
     g1.close()
+    if not args.no_side_configs:
+        # the other configurations, one instance per solve as the reference arm runs them (C1:
+        # uniform 128^3; C2: 3-level sphere, 256^3 effective), plain FP32 to 1e-6, device-timed
+        out["side_configs"] = {}
+        for name in SIDE_CONFIGS:
+            sb, sg = build_batch(name, [0])
+            sg.autotune()
+            sg.copy_channel(TMP_CHANNEL, B_CHANNEL)
+            ts, its = [], []
+            for i in range(args.warmup + args.steps):
+                sg.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                it, rel = solver.solve(sg, stream=sh)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                if not rel < 1e-6:
+                    raise RuntimeError(f"{name}: solve did not converge: rel {rel}")
+                if i >= args.warmup:
+                    ts.append(e0.elapsed_time(e1))
+                    its.append(it)
+            sv = 1e3 / float(np.mean(ts))
+            out["side_configs"][name] = {"solves_per_s": round(sv, 3), "mdof_per_s": round(sg.dof * sv / 1e6, 2),
+                                         "tiles": int(sb.tiles.shape[0]), "dof": int(sg.dof), "iters": int(statistics.median(its)),
+                                         "p50_ms": round(float(np.percentile(ts, 50)), 4)}
+            sg.close()
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         rhs1 = rhs[: b.tiles.shape[0]] if K == 1 else g.get_channel_instance(0, TMP_CHANNEL)
         cb = cpu_baseline(b, rhs1)
@@ -621,7 +645,49 @@ def run_ours(args, world, rank, local, pg):
     return out
 
 
+def bench_config(workload: str, K: int, tiles: np.ndarray, ctypes: np.ndarray, world: int) -> dict:
+    """The `config` of both arms' lines: the same dict for the same workload, batch and ranks."""
+    leaf = (tiles[:, 4] & 1) != 0
+    dof = int(((ctypes[leaf] & 2) != 0).sum())
+    maxl = int(tiles[:, 0].max())
+    return {"workload": f"{workload} x{K} batch", "instances_per_step": K, "tiles_per_instance": int(tiles.shape[0]),
+            "dof_per_instance": dof,
+            "effective_resolution": "512x512x1024" if workload == "ring512" else workload,
+            "levels": f"leaves {int(tiles[leaf, 0].min())}-{maxl}",
+            "tolerance": 1e-6, "stopping_rule": "recursive ||r||/||b|| < tol per instance, checked every iteration",
+            "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"}
+
+
+# the other configurations measured beside the headline one: one instance per solve (C1, C2)
+SIDE_CONFIGS = ["uniform128", "sphere256"]
+
+
+def ref_instance(name: str, seed: int):
+    """A reference grid of workload `name` built by the reference's own code (oracle/_ref):
+    tiles and neighbours from its IterativeRefine and CalculateNeighborTiles, the leaf cell-type
+    rule from the workload definition (numpy), CalcCellTypesFromLeafs by the reference."""
+    from oracle import oracle as O
+
+    from cirrus_b200 import workloads as W  # workload geometry and seeded velocities (numpy only)
+
+    w = W.make(name, seed=seed)
+    ref = O.RefHarness(w)
+    tiles = ref.tiles()
+    ref.calc_neighbors()
+    nbr6 = ref.neighbors()
+    ref.set_ctypes(W.leaf_cell_types(w, tiles, nbr6))
+    ref.calc_cell_types()
+    ref.calc_neighbors()
+    return w, ref, tiles, ref.ctypes()
+
+
 def run_reference(args, world, rank, local, pg):
+    """The reference's own CUDA build (oracle/_ref/libcirrus_ref.so, which links nothing of this
+    project) on the same workload and batch as the product arm: each step solves the same K
+    instances (velocity seeds rank*K + i) one after another through the reference's stock
+    GMGSolver::solve, each timed as FluidEuler::project times it (src/FluidEuler.h:595-601: host
+    clock around the call, device synchronised on both sides); the right-hand side of each
+    instance is loaded and L2 flushed before its solve, outside the timed call."""
     from oracle import oracle as O
 
     if not O.ref_available():
@@ -630,56 +696,80 @@ def run_reference(args, world, rank, local, pg):
 
     from cirrus_b200 import workloads as W
 
-    w = W.make(args.workload, seed=rank)
-    b = W.build(w)
-    ref = O.RefHarness(w)
-    ref.calc_neighbors()
-    ref.set_ctypes(W.leaf_cell_types(w, b.tiles, b.nbr6))
-    ref.calc_cell_types()
-    ref.calc_neighbors()
-    rhs = ref.rhs(b.velocity)
+    K = args.batch
+    w, ref, tiles, ct = ref_instance(args.workload, batch_seeds(rank, K)[0])
+    rhs = [ref.rhs(W.face_velocity(tiles, sd)) for sd in batch_seeds(rank, K)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    times, iters = [], []
+    solve_ms, iters = [], []
 
-    def one():
-        ref.set_channel(1, rhs)
-        flush.zero_()
-        torch.cuda.synchronize()
-        it, rel, ms = ref.solve(1000, 1e-6, 1, 10, 1, w.pure_neumann)
-        iters.append(it)
-        return ms
+    def one_step():
+        total = 0.0
+        for b in rhs:
+            ref.set_channel(1, b)
+            flush.zero_()
+            torch.cuda.synchronize()
+            it, rel, ms = ref.solve(1000, 1e-6, 1, 10, 1, w.pure_neumann)
+            if not rel < 1e-6:
+                raise RuntimeError(f"reference solve did not converge: rel {rel}")
+            iters.append(it)
+            solve_ms.append(ms)
+            total += ms
+        return total
 
     for _ in range(args.warmup):
-        one()
+        one_step()
     iters.clear()
+    solve_ms.clear()
     clk = Clocks(local)
     if rank == 0:
         clk.start()
-    if pg is not None:
-        pg.barrier()
-    times = [one() for _ in range(args.steps)]
+    times = [one_step() for _ in range(args.steps)]
     clocks = clk.stop() if rank == 0 else None
-    total = barrier_max(pg, sum(times))
-    n = args.steps * world
+    total = sum(times)
+    n = args.steps * world * K
     value = n / (total * 1e-3)
-    leaf = (b.tiles[:, 4] & 1) != 0
-    dof = int(((b.ctypes[leaf] & 2) != 0).sum())
-    return {
+    cfg = bench_config(args.workload, K, tiles, ct, world)
+    out = {
         "impl": "reference",
         "metric": "Poisson solves/s to 1e-6 relative residual (GMG-PCG, reference arithmetic)",
         "value": round(value, 3), "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total / args.steps, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (fp64 CG scalars)", "data": "synthetic (seeded face velocities, divergence right-hand side)",
-        "config": {"workload": args.workload, "tiles": int(b.tiles.shape[0]), "dof": dof, "tolerance": 1e-6,
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
-        "mdof_per_s": round(dof * value / 1e6, 2), "iters_per_solve": int(statistics.median(iters)),
-        "latency_ms": {"p50": round(float(np.percentile(times, 50)), 4), "p99": round(float(np.percentile(times, 99)), 4)},
+        "config": cfg,
+        "mdof_per_s": round(cfg["dof_per_instance"] * value / 1e6, 2), "iters_per_solve": int(statistics.median(iters)),
+        "latency_ms": {"single_p50": round(float(np.percentile(solve_ms, 50)), 4),
+                       "single_p99": round(float(np.percentile(solve_ms, 99)), 4),
+                       "batch_p50": round(float(np.percentile(times, 50)), 4), "batch_p99": round(float(np.percentile(times, 99)), 4)},
+        "single_solves_per_s": round(1e3 / float(np.mean(solve_ms)), 3),
         "e2e": {"value": round(value, 3), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": round(value, 3), "unit": "solves/s", "cores": 1, "kind": "reference",
-                         "sample": f"the reference's own CUDA build of GMGSolver::solve (oracle/_ref) on this GPU, "
-                                   f"one host thread, {args.steps} full solves timed like FluidEuler::project"},
+                         "sample": f"the reference's own CUDA build of GMGSolver::solve (oracle/_ref) on this GPU, one host "
+                                   f"thread, {args.steps} steps of {K} full solves, each timed like FluidEuler::project"},
         "clocks": clocks,
     }
+    del ref
+    if not args.no_side_configs:
+        out["side_configs"] = {}
+        for name in SIDE_CONFIGS:
+            sw, sref, st, sct = ref_instance(name, 0)
+            srhs = sref.rhs(W.face_velocity(st, 0))
+            ms_list, its = [], []
+            for i in range(args.warmup + args.steps):
+                sref.set_channel(1, srhs)
+                flush.zero_()
+                torch.cuda.synchronize()
+                it, rel, ms = sref.solve(1000, 1e-6, 1, 10, 1, sw.pure_neumann)
+                if i >= args.warmup:
+                    ms_list.append(ms)
+                    its.append(it)
+            leaf = (st[:, 4] & 1) != 0
+            dof = int(((sct[leaf] & 2) != 0).sum())
+            sv = 1e3 / float(np.mean(ms_list))
+            out["side_configs"][name] = {"solves_per_s": round(sv, 3), "mdof_per_s": round(dof * sv / 1e6, 2), "tiles": int(st.shape[0]),
+                                         "dof": dof, "iters": int(statistics.median(its)),
+                                         "p50_ms": round(float(np.percentile(ms_list, 50)), 4)}
+            del sref
+    return out
 
 
 def main():

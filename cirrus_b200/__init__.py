@@ -274,6 +274,11 @@ class DeviceGrid:
         check(lib().cirrus_grid_get_launch_shape(self._h, kernel, level, C.byref(v)), "cirrus_grid_get_launch_shape")
         return v.value
 
+    def set_launch_mode(self, direct: bool) -> None:
+        """direct=False (default): each solve is one CUDA graph launch; direct=True: the same
+        kernels launched one by one from the host (visible to launch tracers).  Same bits."""
+        check(lib().cirrus_grid_set_launch_mode(self._h, 1 if direct else 0), "cirrus_grid_set_launch_mode")
+
     def bench_launch(self, kernel: int, level: int = 0, reps: int = 1, stream: int = 0) -> None:
         """Launch one solve kernel `reps` times on `stream` (for timing with the caller's events);
         overwrites channels 2-5."""

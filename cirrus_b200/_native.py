@@ -130,6 +130,11 @@ _PROTOS = {
     "cirrus_grid_set_tile_pointers": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "cirrus_grid_gather_tiles": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_void_p]),
     "cirrus_grid_scatter_tiles": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_void_p]),
+    "cirrus_grid_compare_tile_cell_types": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.POINTER(C.c_int),
+                                                       C.POINTER(C.c_uint8)]),
+    "cirrus_gather_tile_bytes": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_size_t, C.POINTER(C.c_uint8), C.c_void_p]),
+    "cirrus_grid_set_launch_mode": (C.c_int, [C.c_void_p, C.c_int]),
+    "cirrus_grid_get_launch_mode": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "cirrus_full_negative_laplacian": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_full_negative_laplacian_ex": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "cirrus_negative_laplacian_same_level": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

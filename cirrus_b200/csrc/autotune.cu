@@ -63,7 +63,7 @@ int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
     auto pick = [&](int kind, int level, auto&& launch) {
         float best = 0.f;
         int best_shape = g.shape(kind, level);
-        for (int sh = 0; sh < kNumShapes; sh++) {
+        for (int sh = 0; sh < num_shapes(kind); sh++) {
             g.shapes[(size_t)kind * g.num_layers + level] = (uint8_t)sh;
             const float ms = time_graph(launch, reps, s);
             if (ms > 0.f && (best == 0.f || ms < best)) {

@@ -386,6 +386,44 @@ cirrus_status cirrus_grid_scatter_tiles(cirrus_grid* grid, int channel, size_t b
     cirrus::launch::scatter_tiles(*grid->g, channel, byte_offset, S(stream));
     return cuda_status();
 }
+cirrus_status cirrus_grid_compare_tile_cell_types(cirrus_grid* grid, size_t byte_offset, void* stream, int* changed,
+                                                 uint8_t* host_types) {
+    if (!grid || !changed || (byte_offset & 3u)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    if (!g.d_tile_ptrs) return CIRRUS_ERR_STATE;
+    const size_t cells = (size_t)g.n * cirrus::kTileCells;
+    if (!g.d_ct_gather) {
+        if (cudaMalloc(&g.d_ct_gather, cells) != cudaSuccess) return cuda_status();
+        if (cudaMalloc(&g.d_ct_flag, sizeof(unsigned int)) != cudaSuccess) return cuda_status();
+        g.bytes += cells + sizeof(unsigned int);
+    }
+    cirrus::launch::compare_tile_cell_types(g, byte_offset, S(stream));
+    unsigned int flag = 0;
+    if (cudaMemcpyAsync(&flag, g.d_ct_flag, sizeof(flag), cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess) return cuda_status();
+    if (cudaStreamSynchronize(S(stream)) != cudaSuccess) return cuda_status();
+    *changed = flag ? 1 : 0;
+    if (flag && host_types &&
+        cudaMemcpyAsync(host_types, g.d_ct_gather, cells, cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess)
+        return cuda_status();
+    return cudaStreamSynchronize(S(stream)) == cudaSuccess ? CIRRUS_OK : cuda_status();
+}
+cirrus_status cirrus_gather_tile_bytes(const void* const* tile_ptrs, int num_tiles, size_t byte_offset, uint8_t* host_out,
+                                       void* stream) {
+    if (!tile_ptrs || num_tiles <= 0 || !host_out || (byte_offset & 3u)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < num_tiles; i++)
+        if (!tile_ptrs[i] || (reinterpret_cast<uintptr_t>(tile_ptrs[i]) & 3u)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return map_rc(cirrus::gather_tile_bytes(tile_ptrs, num_tiles, byte_offset, host_out, S(stream)));
+}
+cirrus_status cirrus_grid_set_launch_mode(cirrus_grid* grid, int mode) {
+    if (!grid || (mode != CIRRUS_LAUNCH_GRAPH && mode != CIRRUS_LAUNCH_DIRECT)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    grid->g->launch_mode = mode;
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_grid_get_launch_mode(const cirrus_grid* grid, int* mode) {
+    if (!grid || !mode) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *mode = grid->g->launch_mode;
+    return CIRRUS_OK;
+}
 cirrus_status cirrus_grid_channel_ptr(cirrus_grid* grid, int channel, float** device_ptr) {
     if (!grid || !device_ptr || !channel_ok(channel)) return CIRRUS_ERR_INVALID_ARGUMENT;
     *device_ptr = grid->g->d_ch[channel];
@@ -641,9 +679,11 @@ int shape_kind(int kernel) {
 }  // namespace
 
 cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape) {
-    if (!grid || shape < 0 || shape >= CIRRUS_NUM_LAUNCH_SHAPES || shape >= cirrus::kNumShapes) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (!grid || shape < 0 || shape >= CIRRUS_NUM_LAUNCH_SHAPES) return CIRRUS_ERR_INVALID_ARGUMENT;
     auto& g = *grid->g;
     if (kernel != -1 && shape_kind(kernel) < 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+    // shapes past the common eight exist for the Laplacian only
+    if (shape >= (kernel == -1 ? cirrus::kNumShapes : cirrus::num_shapes(shape_kind(kernel)))) return CIRRUS_ERR_INVALID_ARGUMENT;
     if (level < -1 || level >= g.num_layers) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] {
         for (int k = 0; k < cirrus::KS_COUNT; k++) {

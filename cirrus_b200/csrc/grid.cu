@@ -542,6 +542,11 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
         launch::init_kernel_attributes();
         launch::init_stencil_attributes();
         g->shapes.assign((size_t)KS_COUNT * num_layers, 1);
+        init_tile_map_cache(*g);
+        CK(cudaMalloc(&g->d_err, sizeof(unsigned int)));
+        CK(cudaMemset(g->d_err, 0, sizeof(unsigned int)));
+        CK(cudaMallocHost(&g->h_err, sizeof(unsigned int)));
+        *g->h_err = 0;
     }
 
     // ------------------------------------------------------------------ per-instance reductions
@@ -660,6 +665,11 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_bottom_code);
     cudaFree(g->d_bottom_inst);
     cudaFree(g->d_tile_ptrs);
+    cudaFree(g->d_ct_gather);
+    cudaFree(g->d_err);
+    if (g->h_err) cudaFreeHost(g->h_err);
+    free_tile_map_cache(*g);
+    cudaFree(g->d_ct_flag);
     cudaFree(g->d_lists);
     cudaFree(g->d_leafslot);
     cudaFree(g->d_wpart);
@@ -682,6 +692,8 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_ax64);
     cudaFree(g->d_r64);
     cudaFree(g->d_norm);
+    cudaFree(g->d_msum);
+    cudaFree(g->d_dofd);
     cudaFree(g->d_bsave);
     delete g;
 }

@@ -109,85 +109,6 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian_same_level(Topo tp, int
     st4(Y + (size_t)tile * kTileCells + t * 4, o);
 }
 
-// Face path of the fused Laplacian: one coarse cell of a GHOST tile whose coupled cells all lie
-// on its faces and couple only outward.  Item: tile, ghost slot << 6 | coarse cell c, coupled
-// faces | face classes << 6, level-constant index.  Forms the cell's partial sum -- its 2x2x2
-// block of A p values in AccumulateToParents128's (ii,jj,kk) order -- computing A p only on
-// cells with coupled faces, each term from the neighbour's value across the face.  Every other
-// cell's A p is +0 in the full path, which also adds the zero-coefficient terms skipped here (as
-// +-0, which leaves finite sums unchanged).  All loads are issued before the arithmetic: the
-// block's own values, mask and type bytes (four 2-cell runs along k), then the neighbour values
-// across each coupled face it touches.
-__device__ __forceinline__ void ghost_face_sum(const Topo& tp, const float* __restrict__ X, int4 it, float* __restrict__ GACC) {
-    const int tile = it.x, c = it.y & 63;
-    const uint32_t faces = (uint32_t)it.z & 63u, cls = (uint32_t)it.z >> 6;
-    const int fi = c / 16 * 2, fj = (c / 4) % 4 * 2, fk = c % 4 * 2;
-    const size_t base = (size_t)tile * kTileCells;
-    const int o0 = fi * 64 + fj * 8 + fk;
-    float2 xo[4];
-    uint32_t mk[4], ck[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int o = o0 + (q >> 1) * 64 + (q & 1) * 8;
-        xo[q] = *reinterpret_cast<const float2*>(X + base + o);
-        mk[q] = *reinterpret_cast<const uint16_t*>(tp.mask_lap + base + o);
-        ck[q] = *reinterpret_cast<const uint16_t*>(tp.ctype + base + o);
-    }
-    const uint32_t touch = (fi == 0 ? 1u : 0u) | (fi == 6 ? 2u : 0u) | (fj == 0 ? 4u : 0u) | (fj == 6 ? 8u : 0u) | (fk == 0 ? 16u : 0u) |
-                           (fk == 6 ? 32u : 0u);
-    const uint32_t act = touch & faces;
-    const TileMeta& m = tp.meta[tile];
-    // nv[f][a*2+b]: the neighbour's value across face f for the block's cell (a, b) on that face,
-    // (a, b) = (jj, kk) on x faces, (ii, kk) on y faces, (ii, jj) on z faces
-    float nv[6][4];
-#pragma unroll
-    for (int f = 0; f < 6; f++) {
-        const int nb = ((act >> f) & 1u) ? m.nb[f] : -1;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int a = q >> 1, b = q & 1;
-            int noff;
-            if (f == 0) noff = 7 * 64 + (fj + a) * 8 + fk + b;
-            else if (f == 1) noff = (fj + a) * 8 + fk + b;
-            else if (f == 2) noff = (fi + a) * 64 + 7 * 8 + fk + b;
-            else if (f == 3) noff = (fi + a) * 64 + fk + b;
-            else if (f == 4) noff = (fi + a) * 64 + (fj + b) * 8 + 7;
-            else noff = (fi + a) * 64 + (fj + b) * 8;
-            nv[f][q] = nb >= 0 ? X[(size_t)nb * kTileCells + noff] : 0.f;
-        }
-    }
-    const LevelConst<float> L(tp.lconst[it.w]);
-    float sum = 0.f;
-#pragma unroll
-    for (int ii = 0; ii < 2; ii++)
-#pragma unroll
-        for (int jj = 0; jj < 2; jj++)
-#pragma unroll
-            for (int kk = 0; kk < 2; kk++) {
-                const int i = fi + ii, j = fj + jj, k = fk + kk;
-                const uint32_t on = (i == 0 ? 1u : 0u) | (i == 7 ? 2u : 0u) | (j == 0 ? 4u : 0u) | (j == 7 ? 8u : 0u) |
-                                    (k == 0 ? 16u : 0u) | (k == 7 ? 32u : 0u);
-                const int q = ii * 2 + jj;
-                const uint32_t mm = (mk[q] >> (8 * kk)) & 0xffu;
-                float v = 0.f;
-                if ((on & act) && (mm & 0x3Fu)) {
-                    const float x0 = kk ? xo[q].y : xo[q].x;
-                    float s = 0.f;
-#pragma unroll
-                    for (int f = 0; f < 6; f++) {
-                        if (!(mm & (1u << f))) continue;
-                        const float a = ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1;
-                        const float xf = nv[f][f < 2 ? jj * 2 + kk : (f < 4 ? ii * 2 + kk : ii * 2 + jj)];
-                        s = __fadd_rn(s, __fmul_rn(a, x0 - xf));
-                    }
-                    const float out = (mm & kMaskInterior) ? mul_h3(s, L.h) : 0.f;
-                    v = (((ck[q] >> (8 * kk)) & 0xffu) & (INTERIOR_C | DIRICHLET_C | NEUMANN_C)) ? out : 0.f;
-                }
-                sum += v;
-            }
-    GACC[(size_t)(it.y >> 6) * 64 + c] = sum;
-}
-
 // FullNegativeLaplacian in one launch over LEAF|GHOST tiles.  p on GHOST tiles is kept valid by
 // the kernels that write p (push_to_ghost_child), so no propagation pass runs; LEAF tiles write
 // A p; GHOST tiles write the 2x2x2 child sums of their A p (AccumulateToParents128's order) to a
@@ -205,6 +126,8 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
                                                                const float* __restrict__ X, float* __restrict__ Y,
                                                                float* __restrict__ GACC, const Scalars* __restrict__ S,
                                                                double* __restrict__ WP) {
+    // the dot-part tail below gives tile u to 16-lane half (u & 1) of warp 2 + (u >> 1): NT <= 4
+    static_assert(NT >= 1 && NT <= 4, "k_laplacian_fused: the tile-part tail covers at most 4 tiles per group");
     pdl_entry();
     if ((int)blockIdx.x < item_blocks) {
         const int q = (int)blockIdx.x * (128 * TPB) + (int)threadIdx.x;
@@ -359,6 +282,8 @@ template <int TPB, int NT>
 __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__ list, int n, float* X,
                                                         const float* __restrict__ R, int color, const Scalars* __restrict__ S,
                                                         const float* __restrict__ RD, double* __restrict__ WP) {
+    // the dot-part tail gives tile u to 16-lane half (u & 1) of warp 2 + (u >> 1): NT <= 4
+    static_assert(NT >= 1 && NT <= 4, "k_gs_sweep: the tile-part tail covers at most 4 tiles per group");
     pdl_entry();
     extern __shared__ __align__(16) unsigned char gs_smem[];
     TileStage* st = reinterpret_cast<TileStage*>(gs_smem);
@@ -1195,6 +1120,34 @@ __global__ void __launch_bounds__(256) k_residual64(Topo tp, const int* __restri
     }
 }
 
+// Pure-Neumann instances of the FP64 defect correction: the residual's component along A's null
+// space (the constant on INTERIOR cells of LEAF tiles) is removed -- r -= sum(r)/count on INTERIOR
+// cells, sum over the instance's LEAF cells (r is 0 off INTERIOR), count its INTERIOR cells --
+// and the FP32 copy refreshed.  Other instances are left alone.
+__global__ void __launch_bounds__(256) k_sub_mean64(Topo tp, const int* __restrict__ leaves, int nleaf, double* R64, float* R32,
+                                                    const double* __restrict__ sums, const double* __restrict__ counts,
+                                                    const InstParams* __restrict__ ip) {
+    pdl_entry();
+    const size_t nv = (size_t)nleaf * 128;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+        const int tile = leaves[v >> 7];
+        const int inst = tp.inst[tile];
+        if (!ip[inst].active || !ip[inst].pure_neumann || !(counts[inst] > 0.0)) continue;
+        const double mean = sums[inst] / counts[inst];
+        const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
+        const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+        V4<double> r = ld4(R64 + off);
+        V4<float> r32;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            if ((ct4 >> (8 * e)) & INTERIOR_C) r.v[e] -= mean;
+            r32.v[e] = (float)r.v[e];
+        }
+        st4(R64 + off, r);
+        st4(R32 + off, r32);
+    }
+}
+
 // x64 += e (FP32 correction) on INTERIOR cells of LEAF tiles of the active instances.
 __global__ void __launch_bounds__(256) k_accumulate_correction(Topo tp, const int* __restrict__ leaves, int nleaf, double* X64,
                                                                float* E, const InstParams* __restrict__ ip) {
@@ -1215,17 +1168,21 @@ __global__ void __launch_bounds__(256) k_accumulate_correction(Topo tp, const in
 }
 
 // Per-instance FP64 sum of squares of a leaf channel (FP64 A, or FP32 B32 widened) into
-// out[instance], chunked like k_inst_reduce (every instance, active or not).
+// out[instance], chunked like k_inst_reduce (every instance, active or not).  plain_sum: the sum of
+// the FP64 values themselves instead (A only).
 __global__ void __launch_bounds__(256) k_inst_norm64(const int* __restrict__ leaves, const int4* __restrict__ chunks,
                                                      const int2* __restrict__ inst_chunks, const double* __restrict__ A,
                                                      const float* __restrict__ B32, double* partials, unsigned int* counters,
-                                                     double* out) {
+                                                     double* out, int plain_sum) {
     pdl_entry();
     const int4 ch = chunks[blockIdx.x];
     double acc = 0.0;
     for (int v = ch.y + threadIdx.x; v < ch.z; v += blockDim.x) {
         const size_t off = (size_t)leaves[v >> 7] * kTileCells + (v & 127) * 4;
-        if (A) {
+        if (A && plain_sum) {
+            const V4<double> a = ld4(A + off);
+            acc += a.v[0] + a.v[1] + a.v[2] + a.v[3];
+        } else if (A) {
             const V4<double> a = ld4(A + off);
             acc += a.v[0] * a.v[0] + a.v[1] * a.v[1] + a.v[2] * a.v[2] + a.v[3] * a.v[3];
         } else {
@@ -1304,7 +1261,10 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
     if (g.n_lapmain + g.n_lapitems == 0) return;
     ++g.launch_count;
     double* WP = with_pap ? g.d_wpart : nullptr;
-    switch (g.shape(KS_LAPLACIAN, 0)) {
+    const int shape = g.shape(KS_LAPLACIAN, 0);
+    // shapes 8..11: the TMA-staged pipeline (the cp.async shape 1 if X's tensor maps cannot be made)
+    if (shape >= kNumShapes && laplacian_tma(g, shape - kNumShapes, X, Y, S, s, with_pap)) return;
+    switch (shape) {
     case 0: laplacian_shape<2, 1>(g, X, Y, S, s, WP); break;
     case 1: laplacian_shape<2, 2>(g, X, Y, S, s, WP); break;
     case 2: laplacian_shape<1, 4>(g, X, Y, S, s, WP); break;
@@ -1559,10 +1519,15 @@ void accumulate_correction(const DevGrid& g, double* X64, float* E, cudaStream_t
     launch_kernel(k_accumulate_correction, leaf_blocks(g), 256, 0, s, g.topo, g.d_leaf, g.n_leaf, X64, E,
                   (const InstParams*)g.d_iparams);
 }
-void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s) {
+void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s, bool plain_sum) {
     ++g.launch_count;
     launch_kernel(k_inst_norm64, g.n_chunks, 256, 0, s, (const int*)g.d_leaf, (const int4*)g.d_chunks, (const int2*)g.d_inst_chunks, A,
-                  B32, g.d_partials, g.d_counters, out);
+                  B32, g.d_partials, g.d_counters, out, plain_sum ? 1 : 0);
+}
+void sub_mean64(const DevGrid& g, double* R64, float* R32, const double* sums, const double* counts, cudaStream_t s) {
+    ++g.launch_count;
+    launch_kernel(k_sub_mean64, leaf_blocks(g), 256, 0, s, g.topo, g.d_leaf, g.n_leaf, R64, R32, sums, counts,
+                  (const InstParams*)g.d_iparams);
 }
 void widen(const DevGrid& g, const float* a, double* b, size_t n, cudaStream_t s) {
     ++g.launch_count;

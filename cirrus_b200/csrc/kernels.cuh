@@ -106,22 +106,24 @@ __device__ __forceinline__ void load_halo(const T* __restrict__ X, const TileMet
 }
 
 // Negative Laplacian of the four cells of thread t, times h^3, for INTERIOR cells (0 elsewhere).
-// xs = tile values in shared memory (512), hx = halos, mask4 = the four mask bytes, cls = the
-// 12-bit cross-face class field of the context.  DIAG additionally returns the diagonal;
-// FUSED selects the rounding of the stencil sum (see fmadd).
+// xs = tile values in shared memory (512); the six face halos: hxm/hxp (x-/x+, [j*8 + k]),
+// hym/hyp (y-/y+, [i*8 + k]), hzm/hzp (z-/z+: the value of column (i, j) at [(i*8 + j)*zs]);
+// mask4 = the four mask bytes, cls = the 12-bit cross-face class field of the context.  DIAG
+// additionally returns the diagonal; FUSED selects the rounding of the stencil sum (see fmadd).
 template <class T, bool DIAG, bool FUSED = true>
-__device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32_t mask4, uint32_t cls,
-                                         const LevelConst<T>& L, T out[4], T diag[4]) {
+__device__ __forceinline__ void neg_lap4v(const T* xs, const T* hxm, const T* hxp, const T* hym, const T* hyp, const T* hzm,
+                                          const T* hzp, int zs, int t, uint32_t mask4, uint32_t cls, const LevelConst<T>& L,
+                                          T out[4], T diag[4]) {
     const TileIdx ix(t);
     // each neighbour vector comes from the tile or from its halo: the address is selected, then
     // one load issued
     const V4<T> xc = ld4(xs + t * 4);
-    const V4<T> xm = ld4(ix.i > 0 ? xs + (t - 16) * 4 : hx + 0 * 64 + ix.j * 8 + ix.k0);
-    const V4<T> xp = ld4(ix.i < 7 ? xs + (t + 16) * 4 : hx + 1 * 64 + ix.j * 8 + ix.k0);
-    const V4<T> ym = ld4(ix.j > 0 ? xs + (t - 2) * 4 : hx + 2 * 64 + ix.i * 8 + ix.k0);
-    const V4<T> yp = ld4(ix.j < 7 ? xs + (t + 2) * 4 : hx + 3 * 64 + ix.i * 8 + ix.k0);
-    const T zlo = *(ix.k0 > 0 ? xs + t * 4 - 1 : hx + 4 * 64 + ix.i * 8 + ix.j);
-    const T zhi = *(ix.k0 < 4 ? xs + t * 4 + 4 : hx + 5 * 64 + ix.i * 8 + ix.j);
+    const V4<T> xm = ld4(ix.i > 0 ? xs + (t - 16) * 4 : hxm + ix.j * 8 + ix.k0);
+    const V4<T> xp = ld4(ix.i < 7 ? xs + (t + 16) * 4 : hxp + ix.j * 8 + ix.k0);
+    const V4<T> ym = ld4(ix.j > 0 ? xs + (t - 2) * 4 : hym + ix.i * 8 + ix.k0);
+    const V4<T> yp = ld4(ix.j < 7 ? xs + (t + 2) * 4 : hyp + ix.i * 8 + ix.k0);
+    const T zlo = *(ix.k0 > 0 ? xs + t * 4 - 1 : hzm + (ix.i * 8 + ix.j) * zs);
+    const T zhi = *(ix.k0 < 4 ? xs + t * 4 + 4 : hzp + (ix.i * 8 + ix.j) * zs);
     // The path is chosen per warp (a vote over the converged lanes), so a warp never runs two
     // paths one after the other: each path gives a lane's cells the same bits (the general one
     // with a_f = c1 on uniform cells, +0 on cells without coupled faces), so the choice only
@@ -192,6 +194,13 @@ __device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32
             diag[e] = interior ? d * L.h * L.h * L.h : T(0);
         }
     }
+}
+
+// neg_lap4v with the halos of hx[6][64] (face order x-, x+, y-, y+, z-, z+).
+template <class T, bool DIAG, bool FUSED = true>
+__device__ __forceinline__ void neg_lap4(const T* xs, const T* hx, int t, uint32_t mask4, uint32_t cls, const LevelConst<T>& L,
+                                         T out[4], T diag[4]) {
+    neg_lap4v<T, DIAG, FUSED>(xs, hx, hx + 64, hx + 128, hx + 192, hx + 256, hx + 320, 1, t, mask4, cls, L, out, diag);
 }
 
 // Coefficients of the general stencil path for thread t's column of four cells: the x and y
@@ -471,6 +480,85 @@ __device__ __forceinline__ double tile_part_sum(const float* terms, int j) {
 #pragma unroll
     for (int k = 0; k < 8; k++) term[k] = terms[j + 16 * k];
     return half_part_sum(term);
+}
+
+// Face path of the fused Laplacian: one coarse cell of a GHOST tile whose coupled cells all lie
+// on its faces and couple only outward.  Item: tile, ghost slot << 6 | coarse cell c, coupled
+// faces | face classes << 6, level-constant index.  Forms the cell's partial sum -- its 2x2x2
+// block of A p values in AccumulateToParents128's (ii,jj,kk) order -- computing A p only on
+// cells with coupled faces, each term from the neighbour's value across the face.  Every other
+// cell's A p is +0 in the full path, which also adds the zero-coefficient terms skipped here (as
+// +-0, which leaves finite sums unchanged).  All loads are issued before the arithmetic: the
+// block's own values, mask and type bytes (four 2-cell runs along k), then the neighbour values
+// across each coupled face it touches.
+__device__ __forceinline__ void ghost_face_sum(const Topo& tp, const float* __restrict__ X, int4 it, float* __restrict__ GACC) {
+    const int tile = it.x, c = it.y & 63;
+    const uint32_t faces = (uint32_t)it.z & 63u, cls = (uint32_t)it.z >> 6;
+    const int fi = c / 16 * 2, fj = (c / 4) % 4 * 2, fk = c % 4 * 2;
+    const size_t base = (size_t)tile * kTileCells;
+    const int o0 = fi * 64 + fj * 8 + fk;
+    float2 xo[4];
+    uint32_t mk[4], ck[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int o = o0 + (q >> 1) * 64 + (q & 1) * 8;
+        xo[q] = *reinterpret_cast<const float2*>(X + base + o);
+        mk[q] = *reinterpret_cast<const uint16_t*>(tp.mask_lap + base + o);
+        ck[q] = *reinterpret_cast<const uint16_t*>(tp.ctype + base + o);
+    }
+    const uint32_t touch = (fi == 0 ? 1u : 0u) | (fi == 6 ? 2u : 0u) | (fj == 0 ? 4u : 0u) | (fj == 6 ? 8u : 0u) | (fk == 0 ? 16u : 0u) |
+                           (fk == 6 ? 32u : 0u);
+    const uint32_t act = touch & faces;
+    const TileMeta& m = tp.meta[tile];
+    // nv[f][a*2+b]: the neighbour's value across face f for the block's cell (a, b) on that face,
+    // (a, b) = (jj, kk) on x faces, (ii, kk) on y faces, (ii, jj) on z faces
+    float nv[6][4];
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        const int nb = ((act >> f) & 1u) ? m.nb[f] : -1;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int a = q >> 1, b = q & 1;
+            int noff;
+            if (f == 0) noff = 7 * 64 + (fj + a) * 8 + fk + b;
+            else if (f == 1) noff = (fj + a) * 8 + fk + b;
+            else if (f == 2) noff = (fi + a) * 64 + 7 * 8 + fk + b;
+            else if (f == 3) noff = (fi + a) * 64 + fk + b;
+            else if (f == 4) noff = (fi + a) * 64 + (fj + b) * 8 + 7;
+            else noff = (fi + a) * 64 + (fj + b) * 8;
+            nv[f][q] = nb >= 0 ? X[(size_t)nb * kTileCells + noff] : 0.f;
+        }
+    }
+    const LevelConst<float> L(tp.lconst[it.w]);
+    float sum = 0.f;
+#pragma unroll
+    for (int ii = 0; ii < 2; ii++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int kk = 0; kk < 2; kk++) {
+                const int i = fi + ii, j = fj + jj, k = fk + kk;
+                const uint32_t on = (i == 0 ? 1u : 0u) | (i == 7 ? 2u : 0u) | (j == 0 ? 4u : 0u) | (j == 7 ? 8u : 0u) |
+                                    (k == 0 ? 16u : 0u) | (k == 7 ? 32u : 0u);
+                const int q = ii * 2 + jj;
+                const uint32_t mm = (mk[q] >> (8 * kk)) & 0xffu;
+                float v = 0.f;
+                if ((on & act) && (mm & 0x3Fu)) {
+                    const float x0 = kk ? xo[q].y : xo[q].x;
+                    float s = 0.f;
+#pragma unroll
+                    for (int f = 0; f < 6; f++) {
+                        if (!(mm & (1u << f))) continue;
+                        const float a = ((cls >> (2 * f)) & 3u) == 2u ? L.c2 : L.c1;
+                        const float xf = nv[f][f < 2 ? jj * 2 + kk : (f < 4 ? ii * 2 + kk : ii * 2 + jj)];
+                        s = __fadd_rn(s, __fmul_rn(a, x0 - xf));
+                    }
+                    const float out = (mm & kMaskInterior) ? mul_h3(s, L.h) : 0.f;
+                    v = (((ck[q] >> (8 * kk)) & 0xffu) & (INTERIOR_C | DIRICHLET_C | NEUMANN_C)) ? out : 0.f;
+                }
+                sum += v;
+            }
+    GACC[(size_t)(it.y >> 6) * 64 + c] = sum;
 }
 
 }  // namespace cirrus

@@ -4,7 +4,10 @@
 // its last pressure stay resident on the device between its solves; each solve after the first
 // starts from that pressure (FP64 defect correction from the warm start).  When a session must be
 // made resident and the budget is spent, idle sessions are evicted least recently used first,
-// their pressure kept on the host for the next warm start.  No counterpart in the reference.
+// their pressure kept on the host for the next warm start.  Victims are chosen under the
+// scheduler lock, but their pressure copy and pool release (a device synchronisation) run on the
+// evicting worker's stream after the lock is dropped, so other slots keep scheduling meanwhile.
+// No counterpart in the reference.
 #include "serve.hpp"
 
 #include "solver_internal.hpp"
@@ -61,7 +64,7 @@ int Server::close_session(int id) {
     it->second.closing = true;
     // wait until no request of the session is running or queued
     cv_.wait(lk, [&] {
-        if (it->second.busy) return false;
+        if (it->second.busy || it->second.evicting) return false;
         for (const Request& r : pending_)
             if (r.session == id) return false;
         return true;
@@ -114,12 +117,13 @@ void Server::stats(size_t* resident, size_t* peak, int* resident_sessions, int* 
 }
 
 // Under the lock: the first queued request that can start now.  Its session must be idle; if it
-// is not resident, the bytes it needs must fit after evicting idle sessions (which are then
-// evicted).  A session larger than the whole budget fails its requests at once.
-bool Server::take_runnable(Request& r, bool& need_create) {
+// is not resident, the bytes it needs must fit after evicting idle sessions (chosen here, least
+// recently used first, and released by the caller outside the lock).  A session larger than the
+// whole budget fails its requests at once.
+bool Server::take_runnable(Request& r, bool& need_create, std::vector<Victim>& victims) {
     for (auto it = pending_.begin(); it != pending_.end(); ++it) {
         Session& s = sessions_[it->session];
-        if (s.busy) continue;
+        if (s.busy || s.evicting) continue;
         if (s.grid) {
             need_create = false;
         } else {
@@ -132,19 +136,13 @@ bool Server::take_runnable(Request& r, bool& need_create) {
                 done_.push_back(c);
                 pending_.erase(it);
                 cv_.notify_all();
-                return take_runnable(r, need_create);
+                return take_runnable(r, need_create, victims);
             }
             size_t freeable = 0;
             for (auto& kv : sessions_)
                 if (kv.second.grid && !kv.second.busy) freeable += kv.second.bytes;
             if (used_ + s.estimate > budget_ + freeable) continue;
-            // evict idle sessions, least recently used first, until the new one fits
-            while (used_ + s.estimate > budget_) {
-                Session* lru = nullptr;
-                for (auto& kv : sessions_)
-                    if (kv.second.grid && !kv.second.busy && (!lru || kv.second.last_used < lru->last_used)) lru = &kv.second;
-                if (!lru) break;
-                evict(*lru);
+            while (used_ + s.estimate > budget_ && pick_lru(victims, &s)) {
             }
             used_ += s.estimate;  // reserved now, corrected to the grid's bytes after its first solve
             s.bytes = s.estimate;
@@ -159,16 +157,48 @@ bool Server::take_runnable(Request& r, bool& need_create) {
     return false;
 }
 
-void Server::evict(Session& s) {
-    const size_t cells = (size_t)s.grid->n * kTileCells;
-    s.x_saved.resize(cells);
-    cudaMemcpy(s.x_saved.data(), s.grid->d_ch[kChX], cells * sizeof(float), cudaMemcpyDeviceToHost);
-    s.has_saved = true;
-    grid_destroy(s.grid);
+// Under the lock: detach the least recently used idle resident session (other than `keep`) as a
+// victim; its bytes count as freed from now on.  False if there is none.
+bool Server::pick_lru(std::vector<Victim>& victims, const Session* keep) {
+    Session* lru = nullptr;
+    for (auto& kv : sessions_) {
+        Session& c = kv.second;
+        if (&c != keep && c.grid && !c.busy && !c.evicting && (!lru || c.last_used < lru->last_used)) lru = &c;
+    }
+    if (!lru) return false;
+    choose_victim(*lru, victims);
+    return true;
+}
+
+void Server::choose_victim(Session& s, std::vector<Victim>& victims) {
+    victims.push_back({&s, s.grid});
     s.grid = nullptr;
+    s.evicting = true;
     used_ -= s.bytes;
     s.bytes = 0;
     evictions_++;
+}
+
+// Outside the lock: save each victim's pressure to the host (for its next warm start) and free
+// its pool; then mark it evicted.
+void Server::finish_evictions(std::vector<Victim>& victims, cudaStream_t stream) {
+    if (victims.empty()) return;
+    for (Victim& v : victims) {
+        const size_t cells = (size_t)v.grid->n * kTileCells;
+        v.s->x_saved.resize(cells);
+        cudaMemcpyAsync(v.s->x_saved.data(), v.grid->d_ch[kChX], cells * sizeof(float), cudaMemcpyDeviceToHost, stream);
+        cudaStreamSynchronize(stream);
+        grid_destroy(v.grid);
+    }
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (Victim& v : victims) {
+            v.s->has_saved = true;
+            v.s->evicting = false;
+        }
+    }
+    victims.clear();
+    cv_.notify_all();
 }
 
 void Server::worker(int slot) {
@@ -182,16 +212,18 @@ void Server::worker(int slot) {
         Request r;
         bool need_create = false, got = false;
         Session* s = nullptr;
+        std::vector<Victim> victims;
         {
             std::unique_lock<std::mutex> lk(mu_);
             cv_.wait(lk, [&] {
                 if (stop_) return true;
-                got = take_runnable(r, need_create);
+                got = take_runnable(r, need_create, victims);
                 return got;
             });
             if (!got) break;
             s = &sessions_[r.session];
         }
+        finish_evictions(victims, stream);  // before the new pool is allocated
         Completion c{};
         c.ticket = r.ticket;
         c.session = r.session;
@@ -238,6 +270,10 @@ void Server::worker(int slot) {
                 s->bytes = s->grid->bytes;
                 used_ += s->bytes;
                 peak_ = std::max(peak_, used_);
+                // the pool's real size (FP64 buffers, graphs) can exceed the reservation: evict
+                // idle sessions until the resident bytes fit the budget again
+                while (used_ > budget_ && pick_lru(victims, s)) {
+                }
             } else {
                 used_ -= s->bytes;  // creation failed: release the reservation
                 s->bytes = 0;
@@ -248,6 +284,7 @@ void Server::worker(int slot) {
             done_.push_back(c);
         }
         cv_.notify_all();
+        finish_evictions(victims, stream);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

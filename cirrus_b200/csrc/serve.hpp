@@ -48,12 +48,21 @@ private:
         DevGrid* grid = nullptr;
         size_t estimate = 0, bytes = 0;
         bool busy = false, closing = false, has_saved = false;
+        bool evicting = false;  // chosen for eviction: its pressure is being saved, its pool freed
         std::vector<float> x_saved;
         long long solves = 0;
         uint64_t last_used = 0;
     };
-    bool take_runnable(Request& r, bool& need_create);
-    void evict(Session& s);
+    // a session chosen for eviction under the lock; its pressure is copied out and its pool freed
+    // outside the lock (finish_evictions)
+    struct Victim {
+        Session* s;
+        DevGrid* grid;
+    };
+    bool take_runnable(Request& r, bool& need_create, std::vector<Victim>& victims);
+    void choose_victim(Session& s, std::vector<Victim>& victims);
+    bool pick_lru(std::vector<Victim>& victims, const Session* keep);
+    void finish_evictions(std::vector<Victim>& victims, cudaStream_t stream);
     void worker(int slot);
 
     size_t budget_, used_ = 0, peak_ = 0;

@@ -278,7 +278,7 @@ int pcg_launch(DevGrid& g, const SolveParams& p0, cudaStream_t s, const InstRequ
     GraphKey key{0, p.level_iters, p.coarsest_iters, p.sync_stride, p.pure_neumann, p.one_over_alpha, p.prolong_coeff,
                  use_fused(g, p.level_iters, p.coarsest_iters) ? 1 : 0};
     DevGrid::SolveGraph sg;
-    if (graphs_enabled()) {
+    if (graphs_enabled() && g.launch_mode == 0) {
         auto it = g.graphs.find(key);
         if (it != g.graphs.end()) sg = it->second;
         else {
@@ -310,6 +310,8 @@ int pcg_launch(DevGrid& g, const SolveParams& p0, cudaStream_t s, const InstRequ
         direct = g.launch_count - c0;
     }
     cudaMemcpyAsync(g.h_scalars, g.d_scalars, sizeof(Scalars) * g.num_inst, cudaMemcpyDeviceToHost, s);
+    // a kernel whose bounded wait gave up (a stage that never filled) leaves a flag; read with the scalars
+    cudaMemcpyAsync(g.h_err, g.d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
     *direct_out = direct;
     return 0;
 }
@@ -328,6 +330,12 @@ void pcg_collect(DevGrid& g, const SolveParams& p, long long direct, SolveResult
     for (int k = 0; k < g.num_inst; k++)
         if (g.h_iparams[k].active) loops = std::max(loops, g.h_scalars[k].iter);
     g.last_solve_launches = direct >= 0 ? direct : sgp ? sgp->prologue + (long long)loops * sgp->body + sgp->epilogue : 0;
+    const bool wait_failed = *g.h_err != 0;
+    if (wait_failed) {
+        g.last_error = "a staged kernel gave up waiting for its copies (bounded wait)";
+        *g.h_err = 0;
+        cudaMemset(g.d_err, 0, sizeof(unsigned int));
+    }
     for (int k = 0; k < g.num_inst; k++) {
         const Scalars& S = g.h_scalars[k];
         SolveResult& o = r[k];
@@ -337,6 +345,7 @@ void pcg_collect(DevGrid& g, const SolveParams& p, long long direct, SolveResult
         o.status = S.nonfinite ? 6 : (S.converged ? 0 : 5);
         if (p.sync_stride <= 0) o.status = 0;
         if (!g.h_iparams[k].active) o.status = 0;
+        if (wait_failed) o.status = 2;
         o.launches = g.last_solve_launches;
     }
 }
@@ -351,7 +360,11 @@ int ensure_fp64(DevGrid& g) {
     if (cudaMalloc(&g.d_bsave, cells * sizeof(float)) != cudaSuccess) return 3;
     cudaMemset(g.d_x64, 0, cells * sizeof(double));
     cudaMemset(g.d_ax64, 0, cells * sizeof(double));
-    g.bytes += cells * (3 * sizeof(double) + sizeof(float));
+    if (cudaMalloc(&g.d_msum, sizeof(double) * g.num_inst) != cudaSuccess) return 3;
+    if (cudaMalloc(&g.d_dofd, sizeof(double) * g.num_inst) != cudaSuccess) return 3;
+    std::vector<double> dofd(g.inst_dof.begin(), g.inst_dof.end());
+    if (cudaMemcpy(g.d_dofd, dofd.data(), sizeof(double) * g.num_inst, cudaMemcpyHostToDevice) != cudaSuccess) return 2;
+    g.bytes += cells * (3 * sizeof(double) + sizeof(float)) + 2 * sizeof(double) * g.num_inst;
     return 0;
 }
 
@@ -362,8 +375,11 @@ void read_norms(DevGrid& g, std::vector<double>& out, cudaStream_t s) {
     cudaStreamSynchronize(s);
 }
 
-void set_active(DevGrid& g, const std::vector<uint8_t>& active, cudaStream_t s) {
-    for (int i = 0; i < g.num_inst; i++) g.h_iparams[i].active = active[i];
+void set_active(DevGrid& g, const std::vector<uint8_t>& active, cudaStream_t s, const std::vector<uint8_t>* pure = nullptr) {
+    for (int i = 0; i < g.num_inst; i++) {
+        g.h_iparams[i].active = active[i];
+        if (pure) g.h_iparams[i].pure_neumann = (*pure)[i];
+    }
     cudaMemcpyAsync(g.d_iparams, g.h_iparams, sizeof(InstParams) * g.num_inst, cudaMemcpyHostToDevice, s);
 }
 }  // namespace
@@ -388,6 +404,9 @@ int true_residual(DevGrid& g, const float* d_b, double* rel, cudaStream_t s) {
 // FP64 defect correction of every active instance: x64 accumulates FP32 PCG corrections e
 // solving A e = r, with r = b - A x64 formed in FP64 on the device; an instance stops when its
 // ||r||/||b|| < tol (FP64 true residual).  All instances still correcting share each inner solve.
+// A pure-Neumann instance's r is projected off A's null space (its mean over INTERIOR cells of
+// LEAF tiles removed) before the norm and the inner solve, which also recentres as the
+// reference's does; ||b|| is the unprojected norm, as the reference's rhs_norm2.
 int damped_jacobi(DevGrid& g, int max_iters, double tol, float omega, cudaStream_t s, int* iters, double* rel) {
     float *X = g.d_ch[kChX], *B = g.d_ch[kChB], *AX = g.d_ch[2], *D = g.d_ch[3];
     cudaMemsetAsync(X, 0, (size_t)g.n * kTileCells * sizeof(float), s);  // x = 0 on LEAF|NONLEAF|GHOST tiles
@@ -420,11 +439,14 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
     const size_t cells = (size_t)g.n * kTileCells;
     const long long own0 = g.launch_count;
     long long inner_recorded = 0, inner_executed = 0;
-    std::vector<uint8_t> want(K), active(K);
+    std::vector<uint8_t> want(K), active(K), pure(K);
     std::vector<double> tol(K);
+    bool any_pure = false;
     for (int i = 0; i < K; i++) {
         want[i] = req ? (req[i].active ? 1 : 0) : 1;
         tol[i] = (req && req[i].tol >= 0) ? req[i].tol : p.tol;
+        pure[i] = (req && req[i].pure_neumann >= 0) ? (req[i].pure_neumann ? 1 : 0) : (p.pure_neumann ? 1 : 0);
+        any_pure = any_pure || (want[i] && pure[i]);
         r[i] = SolveResult();
         r[i].status = want[i] ? 5 : 0;
     }
@@ -444,9 +466,13 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
     }
     std::vector<double> rel(K, 1.0);
     for (int k = 0; k <= p.max_outer; k++) {
-        set_active(g, active, s);
+        set_active(g, active, s, &pure);
         launch::full_laplacian<double>(g, g.d_x64, g.d_ax64, nullptr, s);
         launch::residual64(g, g.d_bsave, g.d_ax64, g.d_r64, g.d_ch[kChB], s);
+        if (any_pure) {
+            launch::norm64(g, g.d_r64, nullptr, g.d_msum, s, true);
+            launch::sub_mean64(g, g.d_r64, g.d_ch[kChB], g.d_msum, g.d_dofd, s);
+        }
         launch::norm64(g, g.d_r64, nullptr, g.d_norm, s);
         read_norms(g, rr, s);
         bool any = false;
@@ -464,6 +490,7 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
             tau = std::min(0.1, std::max(p.inner_tol, tau));
             inner[i].active = 1;
             inner[i].tol = tau;
+            inner[i].pure_neumann = pure[i];
             any = true;
         }
         if (!any) break;

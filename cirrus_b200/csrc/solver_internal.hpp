@@ -57,6 +57,10 @@ struct GraphKey {
 // shape computes each tile with the same operations.
 enum { KS_GS_SWEEP = 0, KS_PRESMOOTH = 1, KS_PROLONG = 2, KS_RESIDUAL = 3, KS_LAPLACIAN = 4, KS_COUNT = 5 };
 constexpr int kNumShapes = 8;
+// the Laplacian has four more: the TMA-staged pipeline (lap_tma.cu) with (consumer groups, stages)
+// = (2, 8), (4, 8), (2, 12), (1, 6)
+constexpr int kNumLapShapes = 12;
+inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kNumShapes; }
 
 // A contiguous run of one instance's tiles inside the merged pool: tiles local..local+count of
 // the instance's all-tiles order are global..global+count (one run per level).
@@ -95,6 +99,12 @@ struct DevGrid {
     uint8_t* d_ghost_faces = nullptr;  // per GHOST tile: faces whose p other tiles read (Topo::ghost_faces)
     float* d_xpre = nullptr;        // n x 512: pre-smoothed x of the fused V-cycle (read by the upstroke)
     void** d_tile_ptrs = nullptr;  // optional external array-of-tiles storage (interop)
+    uint8_t* d_ct_gather = nullptr;       // n x 512 cell types gathered from the external tiles
+    unsigned int* d_ct_flag = nullptr;    // set when a gathered cell type differs from the pool's
+    int launch_mode = 0;                  // 0: solves run as one CUDA graph; 1: direct launches
+    void* tile_map_cache = nullptr;       // tensor maps of the channel buffers (lap_tma.cu)
+    unsigned int* d_err = nullptr;        // set by a kernel whose bounded wait gave up (0 otherwise)
+    unsigned int* h_err = nullptr;        // pinned mirror, read back after each solve
     int* d_lists = nullptr;
     const int* d_leaf = nullptr;   // LEAF tiles, instance by instance, each in its all-tiles order
     const int* d_ghost = nullptr;
@@ -165,6 +175,8 @@ struct DevGrid {
     double* d_ax64 = nullptr;
     double* d_r64 = nullptr;
     double* d_norm = nullptr;      // per instance
+    double* d_msum = nullptr;      // per instance: sum of the FP64 residual (pure-Neumann projection)
+    double* d_dofd = nullptr;      // per instance: INTERIOR cells of LEAF tiles, as doubles
     float* d_bsave = nullptr;
     bool x64_valid = false;      // the last solve was mixed precision: d_x64 holds its FP64 x
 
@@ -219,6 +231,10 @@ double list_dot(const DevGrid& g, const float* A, const float* B, const int* lis
 // FullNegativeLaplacian as one launch; the ghost-to-parent sums are completed by pap_ghost.
 // with_pap: also store the p.Ap tile parts of LEAF tiles without GHOST children (d_wpart)
 void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s, bool with_pap = false);
+// The same with the staged tiles moved by bulk asynchronous copies through a stage ring
+// (lap_tma.cu); variant 0..3 = (consumer groups, stages) (2, 8), (4, 8), (2, 12), (1, 6).  False
+// (nothing launched) when the tensor maps of X cannot be made.
+bool laplacian_tma(const DevGrid& g, int variant, const float* X, float* Y, const Scalars* S, cudaStream_t s, bool with_pap);
 // Ap += GHOST children's sums on the LEAF tiles that have them, and their p.Ap tile parts
 void pap_ghost(const DevGrid& g, const float* P, float* AP, cudaStream_t s);
 // RD: with the PCG residual r, also store the r.z tile parts of the level's LEAF tiles (d_wpart)
@@ -255,8 +271,10 @@ void x_final(const DevGrid& g, float* X, const float* P, cudaStream_t s);
 void recenter(const DevGrid& g, float* R, float* RC, cudaStream_t s);
 void residual64(const DevGrid& g, const float* B, const double* AX, double* R64, float* R32, cudaStream_t s);
 void accumulate_correction(const DevGrid& g, double* X64, float* E, cudaStream_t s);
-// per-instance FP64 sums of squares into out[instance] (A, or B32 widened)
-void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s);
+// per-instance FP64 sums of squares into out[instance] (A, or B32 widened); plain_sum: sums of A
+void norm64(const DevGrid& g, const double* A, const float* B32, double* out, cudaStream_t s, bool plain_sum = false);
+// pure-Neumann active instances: R64 -= sums/counts on INTERIOR cells of LEAF tiles, R32 refreshed
+void sub_mean64(const DevGrid& g, double* R64, float* R32, const double* sums, const double* counts, cudaStream_t s);
 void widen(const DevGrid& g, const float* a, double* b, size_t n, cudaStream_t s);
 void narrow(const DevGrid& g, const double* a, float* b, size_t n, cudaStream_t s);
 // right-hand side construction (rhs.cu)
@@ -283,7 +301,18 @@ void init_stencil_attributes();
 // array-of-tiles interop (interop.cu)
 void gather_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream_t s);
 void scatter_tiles(const DevGrid& g, int channel, size_t byte_offset, cudaStream_t s);
+// the 512 cell-type bytes at tile_ptr + byte_offset of every tile into d_ct_gather, and
+// *d_ct_flag |= 1 where one differs from the pool's cell types (flag cleared first on s)
+void compare_tile_cell_types(const DevGrid& g, size_t byte_offset, cudaStream_t s);
 }  // namespace launch
+
+// tensor-map cache of the TMA-staged kernels (lap_tma.cu)
+void init_tile_map_cache(DevGrid& g);
+void free_tile_map_cache(DevGrid& g);
+
+// 512 bytes at tile_ptrs[i] + byte_offset of n device tiles into host_out, through temporary
+// device buffers (interop.cu); synchronises s.  0, or 2 (CUDA error) / 3 (out of memory).
+int gather_tile_bytes(const void* const* tile_ptrs, int n, size_t byte_offset, uint8_t* host_out, cudaStream_t s);
 
 // V-cycle with the reference's schedule (src/GMGSolver.cu:383-447), one launch per kernel of the
 // reference (any level_iters).

@@ -148,6 +148,23 @@ cirrus_status cirrus_grid_set_tile_pointers(cirrus_grid* grid, const void* const
  * c * 736 * 4 bytes (src/PoissonTile.h:39,51). */
 cirrus_status cirrus_grid_gather_tiles(cirrus_grid* grid, int channel, size_t byte_offset, void* stream);
 cirrus_status cirrus_grid_scatter_tiles(cirrus_grid* grid, int channel, size_t byte_offset, void* stream);
+/* Array-of-tiles cell types: copies the 512 cell-type bytes at tile_ptr + byte_offset of every
+ * registered tile (the reference's PoissonTile<float>::mCellType, src/PoissonTile.h:54) into a
+ * device buffer of the grid and compares them, on the device, with the cell types the grid was
+ * built from.  *changed = 1 if any byte differs, else 0.  When it differs and host_types is not
+ * NULL, the gathered types (num_tiles*512 bytes, all-tiles order) are copied to host_types, ready
+ * for cirrus_topology_set_cell_types and a rebuild of the grid (the stencil masks derive from
+ * them).  byte_offset must be a multiple of 4.  Synchronises `stream`.  The reference rewrites
+ * mCellType every step (CalcCellTypesFromLeafs, src/FluidEuler.h:934) without changing tiles, so
+ * a caller that keeps a grid across steps checks this before each solve. */
+cirrus_status cirrus_grid_compare_tile_cell_types(cirrus_grid* grid, size_t byte_offset, void* stream, int* changed,
+                                                 uint8_t* host_types);
+/* The 512 bytes at tile_ptrs[i] + byte_offset of num_tiles device tiles (e.g. every tile's
+ * mCellType) into host_out (num_tiles*512 bytes), with one gather kernel and one copy through
+ * temporary device buffers, instead of a copy per tile.  byte_offset a multiple of 4, tile
+ * pointers 4-byte aligned.  Synchronises `stream`. */
+cirrus_status cirrus_gather_tile_bytes(const void* const* tile_ptrs, int num_tiles, size_t byte_offset, uint8_t* host_out,
+                                       void* stream);
 /* Device-to-device copy of a whole channel, ordered on `stream` (asynchronous). */
 cirrus_status cirrus_grid_copy_channel(cirrus_grid* grid, int dst_channel, int src_channel, void* stream);
 /* Device pointer of a channel (num_tiles*512 floats), for zero-copy integration. */
@@ -202,6 +219,8 @@ cirrus_status cirrus_dot(cirrus_grid* grid, int a_channel, int b_channel, double
  * CIRRUS_ERR_INVALID_ARGUMENT, doing nothing, when that exceeds CIRRUS_NOALLOC_MAX_BLOCKS
  * (only on devices with more than 256 SMs).  The first call on each device looks up the
  * scratch address (cudaGetSymbolAddress); make it before any stream capture on that device.
+ * The address is kept for the life of the process: after cudaDeviceReset (or any reset of the
+ * device's primary context) it is stale, so do not call this function on that device again.
  * Calls that can overlap on one device (several host threads, or streams not ordered with each
  * other) share the scratch and race: serialise them.  Calls from one host thread never overlap,
  * since each returns only after its stream is synchronised. */
@@ -257,6 +276,16 @@ typedef struct cirrus_solve_result {
     int status;                 /* cirrus_status of the solve */
     long long kernel_launches;  /* CUDA kernels the solve executed on the device */
 } cirrus_solve_result;
+
+/* How a grid's solves reach the GPU (no counterpart in the reference, which launches every kernel
+ * from the host and reads the residual back each iteration).  CIRRUS_LAUNCH_GRAPH (the default):
+ * the whole PCG loop is one CUDA graph with a device-side while node, captured on first use per
+ * parameter set.  CIRRUS_LAUNCH_DIRECT: the same kernels launched one by one from the host, which
+ * reads the per-instance scalars after each iteration -- for profilers and launch tracers that do
+ * not follow kernels inside conditional graph nodes.  Results are bit-identical in both modes. */
+enum { CIRRUS_LAUNCH_GRAPH = 0, CIRRUS_LAUNCH_DIRECT = 1 };
+cirrus_status cirrus_grid_set_launch_mode(cirrus_grid* grid, int mode);
+cirrus_status cirrus_grid_get_launch_mode(const cirrus_grid* grid, int* mode);
 
 /* Fills params with the reference call site's values (src/FluidEuler.h:591-598). */
 void cirrus_solve_params_default(cirrus_solve_params* params);
@@ -342,10 +371,12 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
 /* Launch shapes of the staged stencil kernels, as the autotuner sets them: kernel one of
  * CIRRUS_KERNEL_LAPLACIAN / _GS_SWEEP / _PRESMOOTH / _PROLONG_SWEEP / _RESIDUAL_RESTRICT (or -1:
  * all of them), level a level of the grid (or -1: all levels; the Laplacian has one entry,
- * level 0), shape in [0, CIRRUS_NUM_LAUNCH_SHAPES).  Lets a caller reuse tuned shapes for grids
- * of the same structure or pin one.  Shapes never change results.  No counterpart in the
- * reference. */
-#define CIRRUS_NUM_LAUNCH_SHAPES 8
+ * level 0), shape in [0, 8) for every kernel; the Laplacian also takes 8..11, its TMA-staged
+ * pipeline (persistent CTAs, one producer warp issuing bulk tensor copies of each tile and its
+ * halos into a ring of shared-memory stages, 1-4 consumer groups).  Lets a caller reuse tuned
+ * shapes for grids of the same structure or pin one.  Shapes never change results.  No
+ * counterpart in the reference. */
+#define CIRRUS_NUM_LAUNCH_SHAPES 12
 cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape);
 cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int level, int* shape);
 

@@ -8,12 +8,24 @@
  *   auto [iters, err] = solver.solve(grid, false, 1000, 1e-6, 1, 10, 1, mIsPureNeumann);
  *
  * Same preconditions and results as the reference: b in channel 1 of LEAF tiles, x written to
- * channel 0, channel 1 left holding the final residual.  The first solve on a grid (and the first
- * after its tiles change) imports the tile list and cell types and builds the device tile pool;
- * every solve then moves channels between the reference's tiles and the pool with device
- * gather/scatter kernels (no host copies) and runs the whole PCG as one CUDA graph.
+ * channel 0, channel 1 left holding the final residual.
+ *
+ * FluidEuler::project constructs a fresh solver object for every projection, so the device
+ * state does not live in the object: a process-wide registry keeps, per grid object, the tile
+ * pool built from it (topology tables, stencil masks, the captured solve graph).  A solve
+ *   1. compares the grid's tile list (tile pointers, levels, coordinates, types) with the bound
+ *      one and rebuilds the pool when it differs (a refined or coarsened grid);
+ *   2. gathers every tile's mCellType on the device and compares it with the pool's (one kernel,
+ *      1 byte per cell, and a 4-byte read-back): CalcCellTypesFromLeafs rewrites the cell types
+ *      every step (src/FluidEuler.h:934) and can move NEUMANN/DIRICHLET cells without changing
+ *      tiles, and the stencil masks derive from them, so a change rebuilds the pool's masks from
+ *      the gathered types;
+ *   3. gathers b, solves (one CUDA graph launch) and scatters x and r back, on the device.
+ * A pool stays bound until release(grid) or release_all(); its memory is about 60 bytes per cell.
  * Template parameter Grid needs: hAllTiles (host array of infos with mTileCoord, mTilePtr,
  * mLevel, mType), hLog2Hashes, mNumLayers, mH0; its Tile needs mData[c][...] and mCellType[512].
+ * Calls for one grid are serialised by the registry; the reference's solve is not re-entrant
+ * for a grid either.
  */
 #ifndef CIRRUS_GMG_DROPIN_HPP
 #define CIRRUS_GMG_DROPIN_HPP
@@ -25,6 +37,9 @@
 #include <cstddef>
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <tuple>
@@ -38,20 +53,93 @@ inline void check(cirrus_status s, const char* what) {
     if (s != CIRRUS_OK) throw std::runtime_error(std::string(what) + ": " + cirrus_status_string(s));
 }
 
+namespace detail {
+
+// The device pool bound to one grid object, with the tile list it was built from.
+struct Binding {
+    std::vector<const void*> ptrs;
+    std::vector<int32_t> tiles5;  // level, x, y, z, type per tile (all-tiles order)
+    std::vector<uint8_t> ctypes;  // host staging of gathered cell types (num_tiles*512)
+    int num_layers = 0;
+    std::vector<uint32_t> log2;
+    double h0 = 0;
+    cirrus_topology* topo = nullptr;
+    cirrus_grid* cg = nullptr;
+    std::mutex mu;  // one solve at a time per grid
+    ~Binding() { drop(); }
+    void drop() {
+        if (cg) cirrus_grid_destroy(cg);
+        if (topo) cirrus_topology_destroy(topo);
+        cg = nullptr;
+        topo = nullptr;
+    }
+};
+
+struct Registry {
+    std::mutex mu;
+    std::map<const void*, std::shared_ptr<Binding>> by_grid;
+};
+// Never destroyed: a static destructor would free device memory after the CUDA runtime may
+// already have shut down at process exit.  release_all() frees the pools explicitly.
+inline Registry& registry() {
+    static Registry* r = new Registry();
+    return *r;
+}
+
+}  // namespace detail
+
+// Frees the device pool bound to `grid` (if any).  Call it before a grid object is destroyed
+// when its memory matters; a later solve on the same object rebuilds the pool.
+template <class Grid>
+void release(const Grid& grid) {
+    auto& reg = detail::registry();
+    std::shared_ptr<detail::Binding> b;
+    {
+        std::lock_guard<std::mutex> lk(reg.mu);
+        auto it = reg.by_grid.find(static_cast<const void*>(&grid));
+        if (it == reg.by_grid.end()) return;
+        b = it->second;
+        reg.by_grid.erase(it);
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->drop();
+}
+// Frees every bound pool.
+inline void release_all() {
+    auto& reg = detail::registry();
+    std::map<const void*, std::shared_ptr<detail::Binding>> all;
+    {
+        std::lock_guard<std::mutex> lk(reg.mu);
+        all.swap(reg.by_grid);
+    }
+    for (auto& kv : all) {
+        std::lock_guard<std::mutex> lk(kv.second->mu);
+        kv.second->drop();
+    }
+}
+// Number of grids with a bound pool.
+inline int bound_grids() {
+    auto& reg = detail::registry();
+    std::lock_guard<std::mutex> lk(reg.mu);
+    return (int)reg.by_grid.size();
+}
+
 template <class Grid>
 class GMGSolver {
 public:
     explicit GMGSolver(float one_over_alpha = 1.f, float prolong_coeff = 1.f)
         : one_over_alpha_(one_over_alpha), prolong_coeff_(prolong_coeff) {}
-    ~GMGSolver() { release(); }
     GMGSolver(const GMGSolver&) = delete;
     GMGSolver& operator=(const GMGSolver&) = delete;
 
     /* GMGSolver::solve (src/GMGSolver.cu:531-666): returns (iterations, relative residual). */
     std::tuple<int, double> solve(Grid& grid, bool verbose, int max_iters, double relative_tolerance, int level_iters,
                                   int coarsest_iters, int sync_stride, bool is_pure_neumann) {
-        bind(grid);
-        check(cirrus_grid_gather_tiles(cg_, 1, channel_offset(1), nullptr), "gather b");
+        std::shared_ptr<detail::Binding> b = binding(grid);
+        std::lock_guard<std::mutex> lk(b->mu);
+        bind(grid, *b);
+        cirrus_grid* cg = b->cg;
+        check(cirrus_grid_gather_tiles(cg, 1, channel_offset(1), nullptr), "gather b");
         cirrus_solve_params p;
         cirrus_solve_params_default(&p);
         p.max_iters = max_iters;
@@ -63,9 +151,9 @@ public:
         p.one_over_alpha = one_over_alpha_;
         p.prolong_coeff = prolong_coeff_;
         cirrus_solve_result r;
-        check(cirrus_gmg_solve(cg_, &p, nullptr, &r), "cirrus_gmg_solve");
-        check(cirrus_grid_scatter_tiles(cg_, 0, channel_offset(0), nullptr), "scatter x");
-        check(cirrus_grid_scatter_tiles(cg_, 1, channel_offset(1), nullptr), "scatter r");
+        check(cirrus_gmg_solve(cg, &p, nullptr, &r), "cirrus_gmg_solve");
+        check(cirrus_grid_scatter_tiles(cg, 0, channel_offset(0), nullptr), "scatter x");
+        check(cirrus_grid_scatter_tiles(cg, 1, channel_offset(1), nullptr), "scatter r");
         if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cirrus_dropin: CUDA error");
         if (verbose) std::printf("cirrus GMG-PCG: %d iterations, relative residual %.3e\n", r.iters, r.rel_residual);
         return std::make_tuple(r.iters, sync_stride > 0 ? r.rel_residual : -1.0);
@@ -75,12 +163,15 @@ public:
      * the last residual in channel 2 and the diagonal in channel 3 of LEAF|GHOST tiles (both
      * channels keep their previous contents on NONLEAF tiles, as in the reference). */
     std::tuple<int, double> dampedJacobiSolve(Grid& grid, bool verbose, int max_iters, double relative_tolerance, float omega) {
-        bind(grid);
-        for (int c : {1, 2, 3}) check(cirrus_grid_gather_tiles(cg_, c, channel_offset(c), nullptr), "gather");
+        std::shared_ptr<detail::Binding> b = binding(grid);
+        std::lock_guard<std::mutex> lk(b->mu);
+        bind(grid, *b);
+        cirrus_grid* cg = b->cg;
+        for (int c : {1, 2, 3}) check(cirrus_grid_gather_tiles(cg, c, channel_offset(c), nullptr), "gather");
         int iters = 0;
         double rel = 0.0;
-        check(cirrus_damped_jacobi_solve(cg_, max_iters, relative_tolerance, omega, nullptr, &iters, &rel), "cirrus_damped_jacobi_solve");
-        for (int c : {0, 2, 3}) check(cirrus_grid_scatter_tiles(cg_, c, channel_offset(c), nullptr), "scatter");
+        check(cirrus_damped_jacobi_solve(cg, max_iters, relative_tolerance, omega, nullptr, &iters, &rel), "cirrus_damped_jacobi_solve");
+        for (int c : {0, 2, 3}) check(cirrus_grid_scatter_tiles(cg, c, channel_offset(c), nullptr), "scatter");
         if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cirrus_dropin: CUDA error");
         if (verbose) std::printf("cirrus damped Jacobi: %d iterations, relative residual %.3e\n", iters, rel);
         return std::make_tuple(iters, rel);
@@ -98,57 +189,66 @@ private:
         return base + (size_t)c * sizeof(((Tile*)nullptr)->mData[0]);
     }
     static size_t types_offset() {
-        static Tile probe;
-        return (size_t)((const char*)&probe.mCellType[0] - (const char*)&probe);
+        static const size_t off = [] {
+            static Tile probe;
+            return (size_t)((const char*)&probe.mCellType[0] - (const char*)&probe);
+        }();
+        return off;
     }
 
-    void release() {
-        if (cg_) cirrus_grid_destroy(cg_);
-        if (topo_) cirrus_topology_destroy(topo_);
-        cg_ = nullptr;
-        topo_ = nullptr;
-        ptrs_.clear();
-        types_.clear();
+    static std::shared_ptr<detail::Binding> binding(Grid& grid) {
+        auto& reg = detail::registry();
+        std::lock_guard<std::mutex> lk(reg.mu);
+        auto& slot = reg.by_grid[static_cast<const void*>(&grid)];
+        if (!slot) slot = std::make_shared<detail::Binding>();
+        return slot;
     }
 
-    void bind(Grid& grid) {
+    // Builds the topology and the device pool from the bound tile list and the cell types in
+    // b.ctypes (all tiles, as the reference's CalcCellTypesFromLeafs left them).
+    static void build_pool(detail::Binding& b) {
+        b.drop();
+        const int n = (int)b.ptrs.size();
+        check(cirrus_topology_create(b.num_layers, b.log2.data(), b.h0, &b.topo), "topology");
+        check(cirrus_topology_import_tiles(b.topo, b.tiles5.data(), n), "import tiles");
+        check(cirrus_topology_set_cell_types(b.topo, b.ctypes.data()), "cell types");
+        check(cirrus_grid_create(b.topo, &b.cg), "grid");
+        check(cirrus_grid_set_tile_pointers(b.cg, b.ptrs.data()), "tile pointers");
+    }
+
+    static void bind(Grid& grid, detail::Binding& b) {
+        if (grid.hAllTiles.empty()) throw std::runtime_error("cirrus_dropin: grid has no tiles");
         const size_t n = grid.hAllTiles.size();
         std::vector<const void*> ptrs(n);
-        std::vector<uint8_t> types(n);
-        for (size_t i = 0; i < n; i++) {
-            ptrs[i] = grid.hAllTiles[i].mTilePtr;
-            types[i] = grid.hAllTiles[i].mType;
-        }
-        if (cg_ && ptrs == ptrs_ && types == types_) return;  // same tiles: reuse the pool
-        release();
-        std::vector<uint32_t> log2(grid.hLog2Hashes.begin(), grid.hLog2Hashes.end());
-        check(cirrus_topology_create((int)grid.mNumLayers, log2.data(), (double)grid.mH0, &topo_), "topology");
         std::vector<int32_t> t5(5 * n);
         for (size_t i = 0; i < n; i++) {
             const auto& info = grid.hAllTiles[i];
+            ptrs[i] = info.mTilePtr;
             t5[5 * i] = info.mLevel;
             t5[5 * i + 1] = info.mTileCoord[0];
             t5[5 * i + 2] = info.mTileCoord[1];
             t5[5 * i + 3] = info.mTileCoord[2];
             t5[5 * i + 4] = info.mType;
         }
-        check(cirrus_topology_import_tiles(topo_, t5.data(), (int)n), "import tiles");
-        std::vector<uint8_t> ct(512 * n);
-        for (size_t i = 0; i < n; i++)
-            if (cudaMemcpy(ct.data() + 512 * i, (const char*)ptrs[i] + types_offset(), 512, cudaMemcpyDeviceToHost) != cudaSuccess)
-                throw std::runtime_error("cirrus_dropin: reading cell types");
-        check(cirrus_topology_set_cell_types(topo_, ct.data()), "cell types");
-        check(cirrus_grid_create(topo_, &cg_), "grid");
-        check(cirrus_grid_set_tile_pointers(cg_, ptrs.data()), "tile pointers");
-        ptrs_ = std::move(ptrs);
-        types_ = std::move(types);
+        if (!b.cg || ptrs != b.ptrs || t5 != b.tiles5 || (int)grid.mNumLayers != b.num_layers || (double)grid.mH0 != b.h0) {
+            // new or changed tile list: read the cell types (one gather kernel, one copy) and
+            // build the pool from them
+            b.ptrs = std::move(ptrs);
+            b.tiles5 = std::move(t5);
+            b.num_layers = (int)grid.mNumLayers;
+            b.log2.assign(grid.hLog2Hashes.begin(), grid.hLog2Hashes.end());
+            b.h0 = (double)grid.mH0;
+            b.ctypes.resize(512 * n);
+            check(cirrus_gather_tile_bytes(b.ptrs.data(), (int)n, types_offset(), b.ctypes.data(), nullptr), "read cell types");
+            build_pool(b);
+            return;
+        }
+        int changed = 0;
+        check(cirrus_grid_compare_tile_cell_types(b.cg, types_offset(), nullptr, &changed, b.ctypes.data()), "cell types");
+        if (changed) build_pool(b);
     }
 
     float one_over_alpha_, prolong_coeff_;
-    cirrus_topology* topo_ = nullptr;
-    cirrus_grid* cg_ = nullptr;
-    std::vector<const void*> ptrs_;
-    std::vector<uint8_t> types_;
 };
 
 }  // namespace cirrus_dropin

@@ -3,7 +3,10 @@
 * `CpuOracle`: oracle/cirrus_oracle.cpp, the CPU restatement of the reference algorithm
   (FP32 mirror of the reference arithmetic, and FP64).
 * `RefHarness`: oracle/_ref/libcirrus_ref.so, the reference's own CUDA sources compiled by
-  oracle/build_ref.sh around oracle/ref_harness.cu (needs a GPU to run).
+  oracle/build_ref.sh around oracle/ref_harness.cu (needs a GPU to run).  It links nothing of
+  the product.
+* `RefHarness.solve_dropin` / `damped_jacobi_dropin`: oracle/_ref/libcirrus_ref_dropin.so, the
+  product's drop-in header run on a reference grid (loads the product library; tests only).
 
 Only tests/, __graft_entry__.smoke() and bench.py's reference/CPU-baseline legs import this
 module; the product path never does.
@@ -20,6 +23,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "_build" / "libcirrus_oracle.so"
 REF_LIB = HERE / "_ref" / "libcirrus_ref.so"
+REF_DROPIN_LIB = HERE / "_ref" / "libcirrus_ref_dropin.so"
 
 P = C.c_void_p
 i32p = C.POINTER(C.c_int32)
@@ -41,11 +45,15 @@ def build_oracle(force: bool = False) -> Path:
 
 def build_ref(force: bool = False, reference_dir: str | None = None) -> Path | None:
     """Compile the reference harness when the reference tree is present; returns None otherwise."""
-    ref = Path(reference_dir or os.environ.get("CIRRUS_REFERENCE_DIR", "/root/reference"))
+    # the reference tree: an explicit argument, CIRRUS_REFERENCE_DIR, else `reference` beside
+    # this repository
+    ref = Path(reference_dir or os.environ.get("CIRRUS_REFERENCE_DIR", str(HERE.parent.parent / "reference")))
     if not (ref / "src").is_dir():
         return REF_LIB if REF_LIB.exists() else None
-    deps = [HERE / "ref_harness.cu", HERE / "build_ref.sh", *sorted((HERE.parent / "include").glob("*.h*"))]
-    if force or not REF_LIB.exists() or any(REF_LIB.stat().st_mtime < d.stat().st_mtime for d in deps):
+    deps = [HERE / "ref_harness.cu", HERE / "ref_dropin_harness.cu", HERE / "build_ref.sh",
+            *sorted((HERE.parent / "include").glob("*.h*"))]
+    outs = [REF_LIB, REF_DROPIN_LIB]
+    if force or not all(o.exists() for o in outs) or any(o.stat().st_mtime < d.stat().st_mtime for o in outs for d in deps):
         env = dict(os.environ, CIRRUS_REFERENCE_DIR=str(ref))
         subprocess.run(["bash", str(HERE / "build_ref.sh")], check=True, capture_output=True, env=env)
     return REF_LIB
@@ -303,6 +311,7 @@ def ref_lib():
             "ref_set_tile": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
             "ref_compress_sync_spawn": (None, [P]),
             "ref_iterative_refine": (None, [P, C.POINTER(u8p), C.POINTER(C.c_int), C.c_int]),
+            "ref_grid": (P, [P]),
             "ref_num_tiles": (C.c_int, [P]),
             "ref_max_level": (C.c_int, [P]),
             "ref_tiles": (None, [P, i32p]),
@@ -326,7 +335,6 @@ def ref_lib():
             "ref_dot": (C.c_double, [P, C.c_int, C.c_int]),
             "ref_solve": (C.c_int, [P, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p, f64p]),
             "ref_damped_jacobi": (C.c_int, [P, C.c_int, C.c_double, C.c_float, f64p]),
-            "ref_damped_jacobi_dropin": (C.c_int, [P, C.c_int, C.c_double, C.c_float, f64p]),
             "ref_last_error": (C.c_int, []),
         }
         for k, (r, a) in protos.items():
@@ -335,6 +343,31 @@ def ref_lib():
             f.argtypes = a
         _RLIB = L
     return _RLIB
+
+
+_RDLIB = None
+
+
+def ref_dropin_lib():
+    """oracle/_ref/libcirrus_ref_dropin.so (loads libcirrus_ref.so and the product library)."""
+    global _RDLIB
+    if _RDLIB is None:
+        if not REF_DROPIN_LIB.exists():
+            raise FileNotFoundError(f"{REF_DROPIN_LIB} not built (oracle/build_ref.sh)")
+        ref_lib()
+        L = C.CDLL(str(REF_DROPIN_LIB))
+        protos = {
+            "refdrop_solve": (C.c_int, [P, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p, f64p]),
+            "refdrop_damped_jacobi": (C.c_int, [P, C.c_int, C.c_double, C.c_float, f64p]),
+            "refdrop_bound_grids": (C.c_int, []),
+            "refdrop_release_all": (None, []),
+        }
+        for k, (r, a) in protos.items():
+            f = getattr(L, k)
+            f.restype = r
+            f.argtypes = a
+        _RDLIB = L
+    return _RDLIB
 
 
 class RefHarness:
@@ -448,8 +481,22 @@ class RefHarness:
         it = ref_lib().ref_damped_jacobi(self.h, max_iters, tol, omega, C.byref(rel))
         return it, rel.value
 
+    def solve_dropin(self, max_iters=1000, tol=1e-6, level_iters=1, coarsest_iters=10, sync_stride=1, pure_neumann=False):
+        """GMGSolver::solve through the product's drop-in header on this reference grid, with a
+        fresh solver object per call as FluidEuler::project constructs one: (iterations,
+        relative residual, host-clock milliseconds of the call)."""
+        rel = C.c_double()
+        ms = C.c_double()
+        it = ref_dropin_lib().refdrop_solve(self.h, max_iters, tol, level_iters, coarsest_iters, sync_stride, int(pure_neumann),
+                                            C.byref(rel), C.byref(ms))
+        if it < 0:
+            raise RuntimeError("drop-in solve failed")
+        return it, rel.value, ms.value
+
     def damped_jacobi_dropin(self, max_iters=10, tol=1e-6, omega=1.0):
         """The same call through the product's drop-in header on this reference grid."""
         rel = C.c_double()
-        it = ref_lib().ref_damped_jacobi_dropin(self.h, max_iters, tol, omega, C.byref(rel))
+        it = ref_dropin_lib().refdrop_damped_jacobi(self.h, max_iters, tol, omega, C.byref(rel))
+        if it < 0:
+            raise RuntimeError("drop-in damped Jacobi failed")
         return it, rel.value

@@ -2,7 +2,10 @@
 // TEST INFRASTRUCTURE ONLY: it is compiled together with the reference's unmodified sources
 // (src/GMGSolver.cu, src/PoissonSolver.cu, src/PoissonGrid.cu, src/HAGrid.cu,
 // common/Common.cpp) by oracle/build_ref.sh into oracle/_ref/libcirrus_ref.so, and is loaded
-// only by tests/, the fixture generator in tests/golden/ and bench.py's reference arm.
+// only by tests/, the fixture generator in tests/golden/ and bench.py's reference arm.  The
+// library contains nothing of this project's solver and links none of its libraries; the
+// product's drop-in header is exercised on these grids by oracle/ref_dropin_harness.cu, a
+// separate library that only tests load.
 //
 // It drives the reference through its public functions exactly as FluidEuler does
 // (src/FluidEuler.h:413-447 grid construction, :464 IterativeRefine, :581-612 project), with
@@ -12,9 +15,6 @@
 
 #include "GMGSolver.h"
 #include "PoissonSolver.h"
-
-// the product's header-only drop-in, exercised against the reference grid it is meant for
-#include "cirrus_gmg_dropin.hpp"
 
 #include <chrono>
 #include <cstddef>
@@ -34,7 +34,6 @@ namespace {
 struct RefGrid {
     std::unique_ptr<HADeviceGrid<Tile>> g;
     std::unique_ptr<GMGSolver> solver;
-    std::unique_ptr<cirrus_dropin::GMGSolver<HADeviceGrid<Tile>>> dropin;
 };
 
 __global__ void GatherChannelKernel(HATileInfo<Tile>* tiles, int c, float* out) {
@@ -71,7 +70,6 @@ void* ref_create(int num_layers, const uint32_t* log2hash, double h0) {
 }
 void ref_destroy(void* h) {
     RefGrid* r = (RefGrid*)h;
-    r->dropin.reset();
     r->solver.reset();
     r->g.reset();
     delete r;
@@ -115,6 +113,8 @@ void ref_iterative_refine(void* h, const uint8_t* const* masks, const int* dims,
     IterativeRefine(grid, level_target, false);
     cudaDeviceSynchronize();
 }
+// The reference grid object itself (HADeviceGrid<Tile>*), for harnesses that run other code on it.
+void* ref_grid(void* h) { return ((RefGrid*)h)->g.get(); }
 int ref_num_tiles(void* h) { return (int)((RefGrid*)h)->g->hAllTiles.size(); }
 int ref_max_level(void* h) { return ((RefGrid*)h)->g->mMaxLevel; }
 void ref_tiles(void* h, int* out) {
@@ -254,34 +254,11 @@ int ref_solve(void* h, int max_iters, double tol, int level_iters, int coarsest_
     if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     return iters;
 }
-// The same call through the product's drop-in (include/cirrus_gmg_dropin.hpp) on the same
-// reference grid: what FluidEuler::project would run after switching solver classes.
-int ref_solve_dropin(void* h, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann,
-                     double* rel, double* ms) {
-    RefGrid* r = (RefGrid*)h;
-    if (!r->dropin) r->dropin = std::make_unique<cirrus_dropin::GMGSolver<HADeviceGrid<Tile>>>(1.f, 1.f);
-    cudaDeviceSynchronize();
-    auto t0 = std::chrono::high_resolution_clock::now();
-    auto [iters, err] = r->dropin->solve(*r->g, false, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0);
-    cudaDeviceSynchronize();
-    auto t1 = std::chrono::high_resolution_clock::now();
-    if (rel) *rel = err;
-    if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-    return iters;
-}
-// GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531), and the same call through the drop-in
+// GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531)
 int ref_damped_jacobi(void* h, int max_iters, double tol, float omega, double* rel) {
     RefGrid* r = (RefGrid*)h;
     if (!r->solver) r->solver = std::make_unique<GMGSolver>(1., 1.);
     auto [iters, err] = r->solver->dampedJacobiSolve(*r->g, false, max_iters, tol, omega);
-    cudaDeviceSynchronize();
-    if (rel) *rel = err;
-    return iters;
-}
-int ref_damped_jacobi_dropin(void* h, int max_iters, double tol, float omega, double* rel) {
-    RefGrid* r = (RefGrid*)h;
-    if (!r->dropin) r->dropin = std::make_unique<cirrus_dropin::GMGSolver<HADeviceGrid<Tile>>>(1.f, 1.f);
-    auto [iters, err] = r->dropin->dampedJacobiSolve(*r->g, false, max_iters, tol, omega);
     cudaDeviceSynchronize();
     if (rel) *rel = err;
     return iters;

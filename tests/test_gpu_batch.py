@@ -7,7 +7,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from cirrus_b200 import KERNEL_PROLONG_SWEEP, DeviceGrid, GMGSolver, PRECISION_MIXED_FP64, workloads as W
+from cirrus_b200 import KERNEL_LAPLACIAN, KERNEL_PROLONG_SWEEP, DeviceGrid, GMGSolver, PRECISION_MIXED_FP64, workloads as W
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -172,6 +172,33 @@ def test_every_launch_shape_gives_the_same_bits(built_cache):
         assert res == out[0][0]
         for a, b in zip(out[0][1], xs):
             assert np.array_equal(bits(a), bits(b))
+    g.close()
+
+
+@pytest.mark.parametrize("names", [["sphere64_small", "ring64_small"], ["ring512"], ["ring512"] * 4])
+def test_tma_laplacian_shapes_give_the_same_bits(built_cache, names):
+    """The Laplacian's TMA-staged pipeline (shapes 8-11: one producer warp issuing bulk tensor
+    copies of each tile, its halos and masks into a ring of shared-memory stages, 1-4 consumer
+    groups) inside the solve -- A p of every LEAF tile, the GHOST rows, the p.Ap tile parts --
+    gives the iterations and pressure of the cp.async-staged shape bit for bit."""
+    bs = [built_cache(n) for n in names]
+    rhs = [rhs_of(b) for b in bs]
+    g = DeviceGrid([b.topology for b in bs])
+    s = GMGSolver()
+    out = []
+    for shape in (1, 8, 9, 10, 11):
+        g.set_launch_shape(shape, KERNEL_LAPLACIAN)
+        assert g.get_launch_shape(KERNEL_LAPLACIAN, 0) == shape
+        for i, r in enumerate(rhs):
+            g.set_channel_instance(i, 1, r)
+            g.set_channel_instance(i, 0, np.zeros_like(r))
+        res = s.solve_batch(g)
+        assert all(r.status == 0 for r in s.last_results), shape
+        out.append((res, [g.get_channel_instance(i, 0) for i in range(len(bs))]))
+    for k, (res, xs) in enumerate(out[1:]):
+        assert res == out[0][0], k + 8
+        for a, b in zip(out[0][1], xs):
+            assert np.array_equal(bits(a), bits(b)), k + 8
     g.close()
 
 

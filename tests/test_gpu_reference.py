@@ -83,36 +83,92 @@ def test_against_reference(name, built_cache, ref_ok):
     assert err <= 1e-5
 
 
-@pytest.mark.parametrize("name", ["sphere64_small", "ring64_small", "ring512"])
-def test_dropin_in_reference_grid(name, built_cache, ref_ok):
-    """include/cirrus_gmg_dropin.hpp on the reference's own HADeviceGrid: what FluidEuler::project
-    runs after switching the solver class -- same iterations, same pressure and residual channels."""
-    import ctypes as C
-
-    b = built_cache(name)
+def _ref_grid(b):
     w = b.workload
     ref = O.RefHarness(w)
     ref.calc_neighbors()
     ref.set_ctypes(W.leaf_cell_types(w, b.tiles, b.nbr6))
     ref.calc_cell_types()
     ref.calc_neighbors()
-    rhs = ref.rhs(b.velocity)
-    it, rel, _ = ref.solve(1000, 1e-6, 1, 10, 1, w.pure_neumann)
+    return ref
+
+
+def _ref_then_dropin(ref, velocity, pure_neumann):
+    """The reference's own solve, then the drop-in (fresh solver object, as FluidEuler::project
+    constructs one per call) on the same grid and right-hand side: both results."""
+    rhs = ref.rhs(velocity)
+    it, rel, _ = ref.solve(1000, 1e-6, 1, 10, 1, pure_neumann)
     x_ref, r_ref = ref.get_channel(0), ref.get_channel(1)
     ref.set_channel(1, rhs)
     ref.set_channel(0, np.zeros_like(rhs))
-    L = O.ref_lib()
-    L.ref_solve_dropin.restype = C.c_int
-    L.ref_solve_dropin.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
-                                   C.POINTER(C.c_double), C.POINTER(C.c_double)]
-    drel, dms = C.c_double(), C.c_double()
-    dit = L.ref_solve_dropin(ref.h, 1000, 1e-6, 1, 10, 1, int(w.pure_neumann), C.byref(drel), C.byref(dms))
-    x_d, r_d = ref.get_channel(0), ref.get_channel(1)
+    dit, drel, dms = ref.solve_dropin(1000, 1e-6, 1, 10, 1, pure_neumann)
+    return (it, rel, x_ref, r_ref), (dit, drel, ref.get_channel(0), ref.get_channel(1), dms)
+
+
+@pytest.mark.parametrize("name", ["sphere64_small", "ring64_small", "ring512"])
+def test_dropin_in_reference_grid(name, built_cache, ref_ok):
+    """include/cirrus_gmg_dropin.hpp on the reference's own HADeviceGrid: what FluidEuler::project
+    runs after switching the solver class -- same iterations, same pressure and residual channels,
+    with a fresh solver object per call (the bound pool is found in the drop-in's registry)."""
+    b = built_cache(name)
+    w = b.workload
+    ref = _ref_grid(b)
     leaf = (b.tiles[:, 4] & W.LEAF) != 0
-    print(f"{name}: reference {it} iters {rel:.3e}; drop-in {dit} iters {drel.value:.3e} ({dms.value:.2f} ms incl. first bind)")
-    assert dit == it and drel.value == rel
-    assert np.array_equal(bits(x_d)[leaf], bits(x_ref)[leaf])
-    assert np.array_equal(bits(r_d)[leaf], bits(r_ref)[leaf])
+    for call in range(2):
+        (it, rel, x_ref, r_ref), (dit, drel, x_d, r_d, dms) = _ref_then_dropin(ref, b.velocity, w.pure_neumann)
+        print(f"{name} call {call}: reference {it} iters {rel:.3e}; drop-in {dit} iters {drel:.3e} ({dms:.2f} ms)")
+        assert dit == it and drel == rel
+        assert np.array_equal(bits(x_d)[leaf], bits(x_ref)[leaf])
+        assert np.array_equal(bits(r_d)[leaf], bits(r_ref)[leaf])
+
+
+@pytest.mark.parametrize("name", ["sphere64_small", "ring512"])
+def test_dropin_follows_cell_type_changes(name, built_cache, ref_ok):
+    """CalcCellTypesFromLeafs rewrites the cell types every step (src/FluidEuler.h:934) without
+    changing tiles.  Between solves on the same tiles, a block of INTERIOR cells becomes NEUMANN
+    (an obstacle appears), then INTERIOR again: each time the drop-in, a fresh solver object per
+    call, gives the reference's iterations and bits, so it never solves with stale masks."""
+    b = built_cache(name)
+    w = b.workload
+    ref = _ref_grid(b)
+    leaf = (b.tiles[:, 4] & W.LEAF) != 0
+    base = W.leaf_cell_types(w, b.tiles, b.nbr6)
+    # a 4x4x4 block of INTERIOR cells in the LEAF tile nearest the middle of the LEAF list
+    cand = [t for t in np.flatnonzero(leaf) if (base[t].reshape(8, 8, 8)[2:6, 2:6, 2:6] == W.INTERIOR).all()]
+    assert cand
+    t = cand[len(cand) // 2]
+    moved = base.copy()
+    blk = moved[t].reshape(8, 8, 8)
+    blk[2:6, 2:6, 2:6] = W.NEUMANN
+    iters = []
+    for ct in (base, moved, base):
+        ref.set_ctypes(ct)
+        ref.calc_cell_types()
+        (it, rel, x_ref, r_ref), (dit, drel, x_d, r_d, _) = _ref_then_dropin(ref, b.velocity, w.pure_neumann)
+        assert dit == it and drel == rel
+        assert np.array_equal(bits(x_d)[leaf], bits(x_ref)[leaf])
+        assert np.array_equal(bits(r_d)[leaf], bits(r_ref)[leaf])
+        iters.append(it)
+        # the obstacle's cells carry no pressure in the moved case
+        assert (x_ref[t].reshape(8, 8, 8)[2:6, 2:6, 2:6] == 0).all() == (ct is moved)
+    print(f"{name}: iterations {iters} (tile {t} block NEUMANN in the second solve)")
+
+
+def test_dropin_registry_rebinds_on_new_tiles(built_cache, ref_ok):
+    """Two reference grids solved alternately through fresh drop-in objects: each keeps its own
+    pool in the registry and gives the reference's bits; release_all frees both."""
+    bs = [built_cache("sphere64_small"), built_cache("ring64_small")]
+    refs = [_ref_grid(b) for b in bs]
+    O.ref_dropin_lib().refdrop_release_all()
+    for _ in range(2):
+        for b, ref in zip(bs, refs):
+            leaf = (b.tiles[:, 4] & W.LEAF) != 0
+            (it, rel, x_ref, _), (dit, drel, x_d, _, _) = _ref_then_dropin(ref, b.velocity, b.workload.pure_neumann)
+            assert dit == it and drel == rel
+            assert np.array_equal(bits(x_d)[leaf], bits(x_ref)[leaf])
+    assert O.ref_dropin_lib().refdrop_bound_grids() == 2
+    O.ref_dropin_lib().refdrop_release_all()
+    assert O.ref_dropin_lib().refdrop_bound_grids() == 0
 
 
 @pytest.mark.parametrize("name", ["uniform32_small", "sphere64_small", "sphere64_neumann_small", "ring64_small", "ring512"])
@@ -162,11 +218,7 @@ def test_damped_jacobi_against_reference_and_oracle(name, built_cache, ref_ok):
     number of iterations and leave x, the residual and the diagonal bit-identical on LEAF cells."""
     b = built_cache(name)
     w = b.workload
-    ref = O.RefHarness(w)
-    ref.calc_neighbors()
-    ref.set_ctypes(W.leaf_cell_types(w, b.tiles, b.nbr6))
-    ref.calc_cell_types()
-    ref.calc_neighbors()
+    ref = _ref_grid(b)
     g = DeviceGrid(b.topology)
     for a in range(3):
         g.set_channel(6 + a, b.velocity[a])
@@ -263,3 +315,30 @@ def test_stopping_rules_against_reference(name, built_cache, ref_ok):
         assert it == rit
         assert rel == rrel if sync_stride <= 0 else abs(rel - rrel) <= 1e-9 * abs(rrel)
         assert rel_l2(x, rx, leaf) <= 1e-6
+
+
+def test_dropin_time_at_call_site(built_cache, ref_ok):
+    """The drop-in's cost where FluidEuler::project pays it: ring512, one solve per call, a fresh
+    solver object per call (src/FluidEuler.h:591), host clock around the call as the reference
+    times it (src/FluidEuler.h:595-601).  The first call binds the grid (reads the cell types,
+    builds the pool and the graph); later calls find the pool in the registry and only check the
+    cell types on the device.  Prints the reference's time beside it."""
+    b = built_cache("ring512")
+    w = b.workload
+    ref = _ref_grid(b)
+    rhs = ref.rhs(b.velocity)
+    O.ref_dropin_lib().refdrop_release_all()
+    ref_ms, drop_ms = [], []
+    for i in range(6):
+        ref.set_channel(1, rhs)
+        it, rel, ms = ref.solve(1000, 1e-6, 1, 10, 1, w.pure_neumann)
+        ref_ms.append(ms)
+        ref.set_channel(1, rhs)
+        dit, drel, dms = ref.solve_dropin(1000, 1e-6, 1, 10, 1, w.pure_neumann)
+        drop_ms.append(dms)
+        assert dit == it and drel == rel
+    print(f"ring512 at the call site: reference {np.median(ref_ms[1:]):.2f} ms per solve; drop-in first call (bind) "
+          f"{drop_ms[0]:.2f} ms, later calls median {np.median(drop_ms[1:]):.2f} ms "
+          f"({np.median(ref_ms[1:]) / np.median(drop_ms[1:]):.2f}x)")
+    O.ref_dropin_lib().refdrop_release_all()
+    assert np.median(drop_ms[1:]) < np.median(ref_ms[1:])
