@@ -25,12 +25,12 @@ from typing import Callable, Sequence
 
 import numpy as np
 
-from ._native import (CirrusError, Completion, LEVEL_TARGET_FN, SolveParams, SolveResult, check, lib)
+from ._native import (CirrusError, Completion, LEVEL_TARGET_FN, SolveParams, SolveResult, check, lib, loaded_lib)
 
 __all__ = [
     "LEAF", "NONLEAF", "GHOST", "DIRICHLET", "INTERIOR", "NEUMANN",
     "X_CHANNEL", "B_CHANNEL", "R_CHANNEL", "P_CHANNEL", "AP_CHANNEL", "Z_CHANNEL", "TMP_CHANNEL", "U_CHANNEL",
-    "FLUID_EULER_LOG2_HASH", "Topology", "DeviceGrid", "GMGSolver", "CirrusError", "lib",
+    "FLUID_EULER_LOG2_HASH", "Topology", "DeviceGrid", "GMGSolver", "Holder", "CirrusError", "lib",
 ]
 
 LEAF, NONLEAF, GHOST = 1, 2, 4
@@ -61,8 +61,9 @@ class Topology:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().cirrus_topology_destroy(h)
+        L = loaded_lib()
+        if h is not None and h.value and L is not None:
+            L.cirrus_topology_destroy(h)
             self._h = None
 
     @property
@@ -216,8 +217,9 @@ class DeviceGrid:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().cirrus_grid_destroy(h)
+        L = loaded_lib()
+        if h is not None and h.value and L is not None:
+            L.cirrus_grid_destroy(h)
             self._h = None
 
     def close(self):
@@ -496,8 +498,9 @@ class Server:
 
     def close(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib().cirrus_server_destroy(h)
+        L = loaded_lib()
+        if h is not None and h.value and L is not None:
+            L.cirrus_server_destroy(h)
             self._h = None
         self._live.clear()
 
@@ -546,3 +549,82 @@ class Server:
         check(lib().cirrus_server_stats(self._h, C.byref(r), C.byref(pk), C.byref(rs), C.byref(pd), C.byref(e)), "cirrus_server_stats")
         return {"resident_bytes": r.value, "peak_bytes": pk.value, "resident_sessions": rs.value, "pending": pd.value,
                 "evictions": e.value}
+
+
+class Holder:
+    """A tile-holder file in memory: the reference's checkpoint / interchange format of a grid's
+    tiles (IOFunc::WriteHAHostTileHolderToFile / ReadHAHostTileHolderFromFile,
+    src/PoissonIOFunc.cu:38-121).  Tiles are listed level by level in file order."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+
+    @classmethod
+    def read(cls, path: str) -> "Holder":
+        h = C.c_void_p()
+        check(lib().cirrus_holder_read(str(path).encode(), C.byref(h)), "cirrus_holder_read")
+        return cls(h)
+
+    @classmethod
+    def from_grid(cls, topology: Topology, grid: DeviceGrid, tile_types: int = LEAF | NONLEAF | GHOST) -> "Holder":
+        """getHostTileHolder(tile_types): the grid's tiles of those types with channels 0..8 and
+        cell types (synchronous)."""
+        h = C.c_void_p()
+        check(lib().cirrus_holder_from_grid(topology.handle, grid.handle, int(tile_types), C.byref(h)), "cirrus_holder_from_grid")
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        L = loaded_lib()
+        if h is not None and h.value and L is not None:
+            L.cirrus_holder_destroy(h)
+            self._h = None
+
+    def write(self, path: str) -> None:
+        check(lib().cirrus_holder_write(self._h, str(path).encode()), "cirrus_holder_write")
+
+    def info(self) -> dict:
+        h0, nl, ml, nt = C.c_double(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().cirrus_holder_info(self._h, C.byref(h0), C.byref(nl), C.byref(ml), C.byref(nt)), "cirrus_holder_info")
+        return {"h0": h0.value, "num_layers": nl.value, "max_level": ml.value, "num_tiles": nt.value}
+
+    @property
+    def num_tiles(self) -> int:
+        return self.info()["num_tiles"]
+
+    def tiles(self) -> np.ndarray:
+        out = np.empty((self.num_tiles, 5), dtype=np.int32)
+        check(lib().cirrus_holder_tiles(self._h, _ptr(out, C.c_int32)), "cirrus_holder_tiles")
+        return out
+
+    def cell_types(self) -> np.ndarray:
+        out = np.empty((self.num_tiles, 512), dtype=np.uint8)
+        check(lib().cirrus_holder_cell_types(self._h, _ptr(out, C.c_uint8)), "cirrus_holder_cell_types")
+        return out
+
+    def channel(self, c: int) -> np.ndarray:
+        out = np.empty((self.num_tiles, 512), dtype=np.float32)
+        check(lib().cirrus_holder_channel(self._h, int(c), _ptr(out, C.c_float)), "cirrus_holder_channel")
+        return out
+
+    def to_topology(self, levels_log2_hash: Sequence[int] = FLUID_EULER_LOG2_HASH) -> tuple[Topology, np.ndarray]:
+        """setTilesFromHolder + compressHost into a new Topology; also returns each holder tile's
+        index in the topology's all-tiles order."""
+        nl = len(levels_log2_hash)
+        arr = (C.c_uint32 * nl)(*levels_log2_hash)
+        order = np.empty(self.num_tiles, dtype=np.int32)
+        h = C.c_void_p()
+        check(lib().cirrus_topology_from_holder(self._h, arr, nl, C.byref(h), _ptr(order, C.c_int32)), "cirrus_topology_from_holder")
+        t = Topology.__new__(Topology)
+        t.num_layers = nl
+        t.h0 = self.info()["h0"]
+        t._h = h
+        return t, order
+
+    def load_into(self, grid: DeviceGrid, order: np.ndarray, channels: Sequence[int] = (0,), stream: int = 0) -> None:
+        """Copy the holder's channels into the grid's tiles at `order` (from to_topology)."""
+        mask = 0
+        for c in channels:
+            mask |= 1 << int(c)
+        o = np.ascontiguousarray(order, dtype=np.int32)
+        check(lib().cirrus_grid_load_holder(grid.handle, self._h, _ptr(o, C.c_int32), mask, C.c_void_p(stream)), "cirrus_grid_load_holder")

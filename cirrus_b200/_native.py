@@ -133,6 +133,17 @@ _PROTOS = {
     "cirrus_grid_compare_tile_cell_types": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.POINTER(C.c_int),
                                                        C.POINTER(C.c_uint8)]),
     "cirrus_gather_tile_bytes": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_size_t, C.POINTER(C.c_uint8), C.c_void_p]),
+    "cirrus_holder_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "cirrus_holder_write": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "cirrus_holder_destroy": (None, [C.c_void_p]),
+    "cirrus_holder_info": (C.c_int, [C.c_void_p, c_f64_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "cirrus_holder_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "cirrus_holder_cell_types": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "cirrus_holder_channel": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
+    "cirrus_topology_from_holder": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_int, C.POINTER(C.c_void_p),
+                                              C.POINTER(C.c_int32)]),
+    "cirrus_holder_from_grid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "cirrus_grid_load_holder": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.c_uint32, C.c_void_p]),
     "cirrus_grid_set_launch_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "cirrus_grid_get_launch_mode": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "cirrus_full_negative_laplacian": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
@@ -203,6 +214,12 @@ def lib():
             fn.argtypes = args
         _LIB = handle
         return _LIB
+
+
+def loaded_lib():
+    """The native library if it is loaded, else None (for finalizers: during interpreter shutdown
+    module globals may already be cleared, and nothing should be loaded then)."""
+    return _LIB
 
 
 def check(status: int, func: str) -> None:

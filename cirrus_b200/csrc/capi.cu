@@ -1,10 +1,12 @@
 // C ABI (include/cirrus_b200.h).  Every entry point validates its arguments, maps internal
 // failures to cirrus_status and never lets an exception cross the boundary.
 #include "../../include/cirrus_b200.h"
+#include "holder.hpp"
 #include "serve.hpp"
 #include "solver_internal.hpp"
 #include "topology.hpp"
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -839,3 +841,156 @@ cirrus_status cirrus_server_stats(cirrus_server* server, size_t* resident_bytes,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- tile-holder files
+struct cirrus_holder {
+    cirrus::Holder h;
+};
+
+cirrus_status cirrus_holder_read(const char* path, cirrus_holder** out) {
+    if (!path || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        auto* h = new cirrus_holder();
+        std::string err;
+        if (cirrus::holder_read(path, &h->h, &err)) {
+            delete h;
+            return CIRRUS_ERR_INVALID_ARGUMENT;
+        }
+        *out = h;
+        return CIRRUS_OK;
+    });
+}
+cirrus_status cirrus_holder_write(const cirrus_holder* holder, const char* path) {
+    if (!holder || !path) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        std::string err;
+        return cirrus::holder_write(holder->h, path, &err) ? CIRRUS_ERR_INVALID_ARGUMENT : CIRRUS_OK;
+    });
+}
+void cirrus_holder_destroy(cirrus_holder* holder) { delete holder; }
+cirrus_status cirrus_holder_info(const cirrus_holder* holder, double* h0, int* num_layers, int* max_level, int* num_tiles) {
+    if (!holder) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (h0) *h0 = (double)holder->h.h0;
+    if (num_layers) *num_layers = holder->h.num_layers;
+    if (max_level) *max_level = holder->h.max_level;
+    if (num_tiles) *num_tiles = holder->h.num_tiles();
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_holder_tiles(const cirrus_holder* holder, int32_t* tiles5) {
+    if (!holder || !tiles5) return CIRRUS_ERR_INVALID_ARGUMENT;
+    size_t i = 0;
+    for (const cirrus::HolderInfo* t : holder->h.ordered()) {
+        tiles5[5 * i] = t->level;
+        tiles5[5 * i + 1] = t->x;
+        tiles5[5 * i + 2] = t->y;
+        tiles5[5 * i + 3] = t->z;
+        tiles5[5 * i + 4] = t->type;
+        i++;
+    }
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_holder_cell_types(const cirrus_holder* holder, uint8_t* out) {
+    if (!holder || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    size_t i = 0;
+    for (const cirrus::HolderInfo* t : holder->h.ordered()) {
+        if (t->record >= 0) std::memcpy(out + i * cirrus::kTileCells, holder->h.types_of((int)t->record), cirrus::kTileCells);
+        else std::memset(out + i * cirrus::kTileCells, 0, cirrus::kTileCells);
+        i++;
+    }
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_holder_channel(const cirrus_holder* holder, int channel, float* out) {
+    if (!holder || !out || channel < 0 || channel >= cirrus::kRecordChannels) return CIRRUS_ERR_INVALID_ARGUMENT;
+    size_t i = 0;
+    for (const cirrus::HolderInfo* t : holder->h.ordered()) {
+        if (t->record >= 0)
+            std::memcpy(out + i * cirrus::kTileCells, holder->h.channel_of((int)t->record, channel), sizeof(float) * cirrus::kTileCells);
+        else std::memset(out + i * cirrus::kTileCells, 0, sizeof(float) * cirrus::kTileCells);
+        i++;
+    }
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_topology_from_holder(const cirrus_holder* holder, const uint32_t* log2_hash, int num_layers, cirrus_topology** out,
+                                          int32_t* order) {
+    if (!holder || !log2_hash || !out || num_layers <= 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        cirrus::Topology* t = nullptr;
+        std::vector<int32_t> ord;
+        std::string err;
+        const int rc = cirrus::holder_to_topology(holder->h, log2_hash, num_layers, &t, &ord, &err);
+        if (rc) return map_rc(rc);
+        auto* topo = new cirrus_topology();
+        topo->t = t;
+        if (order) std::copy(ord.begin(), ord.end(), order);
+        *out = topo;
+        return CIRRUS_OK;
+    });
+}
+cirrus_status cirrus_holder_from_grid(const cirrus_topology* topo, const cirrus_grid* grid, int tile_types, cirrus_holder** out) {
+    if (!topo || !grid || !out || grid->g->num_inst != 1 || (tile_types & ~7) || !tile_types) return CIRRUS_ERR_INVALID_ARGUMENT;
+    const auto& g = *grid->g;
+    if (topo->t->num_tiles() != g.n) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        const size_t cells = (size_t)g.n * cirrus::kTileCells;
+        std::vector<float> ch(cells * cirrus::kNumChannels);
+        std::vector<uint8_t> ct(cells);
+        if (cudaMemcpy(ch.data(), g.d_chbuf, ch.size() * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) return cuda_status();
+        if (cudaMemcpy(ct.data(), g.topo.ctype, cells, cudaMemcpyDeviceToHost) != cudaSuccess) return cuda_status();
+        std::vector<int32_t> t5((size_t)g.n * 5);
+        topo->t->tiles(t5.data());
+        auto* h = new cirrus_holder();
+        cirrus::Holder& H = h->h;
+        H.h0 = (float)topo->t->h0();
+        H.num_layers = topo->t->num_layers();
+        H.max_level = topo->t->max_level();
+        H.levels.assign(H.num_layers, {});
+        int nrec = 0;
+        for (int i = 0; i < g.n; i++) nrec += (t5[5 * i + 4] & tile_types) ? 1 : 0;
+        H.records.assign((size_t)nrec * cirrus::kRecordBytes, 0);
+        int r = 0;
+        for (int i = 0; i < g.n; i++) {  // getHostTileHolder: level by level, all-tiles order
+            if (!(t5[5 * i + 4] & tile_types)) continue;
+            cirrus::HolderInfo info;
+            info.level = t5[5 * i];
+            info.x = t5[5 * i + 1];
+            info.y = t5[5 * i + 2];
+            info.z = t5[5 * i + 3];
+            info.type = (uint8_t)t5[5 * i + 4];
+            info.record = r;
+            for (int c = 0; c < cirrus::kNumChannels; c++)
+                std::memcpy(H.channel_of(r, c), ch.data() + (size_t)c * cells + (size_t)i * cirrus::kTileCells,
+                            sizeof(float) * cirrus::kTileCells);
+            std::memcpy(H.types_of(r), ct.data() + (size_t)i * cirrus::kTileCells, cirrus::kTileCells);
+            H.levels[info.level].push_back(info);
+            r++;
+        }
+        *out = h;
+        return CIRRUS_OK;
+    });
+}
+cirrus_status cirrus_grid_load_holder(cirrus_grid* grid, const cirrus_holder* holder, const int32_t* order, uint32_t channel_mask,
+                                      void* stream) {
+    if (!grid || !holder || !order || grid->g->num_inst != 1 || (channel_mask >> cirrus::kNumChannels)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    return guard([&] {
+        const auto tiles = holder->h.ordered();
+        for (size_t i = 0; i < tiles.size(); i++)
+            if (order[i] < 0 || order[i] >= g.n) return CIRRUS_ERR_INVALID_ARGUMENT;
+        std::vector<float> buf((size_t)g.n * cirrus::kTileCells);
+        for (int c = 0; c < cirrus::kNumChannels; c++) {
+            if (!(channel_mask & (1u << c))) continue;
+            if (cudaMemcpyAsync(buf.data(), g.d_ch[c], buf.size() * sizeof(float), cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess ||
+                cudaStreamSynchronize(S(stream)) != cudaSuccess)
+                return cuda_status();
+            for (size_t i = 0; i < tiles.size(); i++)
+                if (tiles[i]->record >= 0)
+                    std::memcpy(buf.data() + (size_t)order[i] * cirrus::kTileCells, holder->h.channel_of((int)tiles[i]->record, c),
+                                sizeof(float) * cirrus::kTileCells);
+            if (cudaMemcpyAsync(g.d_ch[c], buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice, S(stream)) != cudaSuccess ||
+                cudaStreamSynchronize(S(stream)) != cudaSuccess)
+                return cuda_status();
+        }
+        g.x64_valid = false;
+        return CIRRUS_OK;
+    });
+}

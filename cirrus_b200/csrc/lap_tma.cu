@@ -16,7 +16,8 @@
 //     bits), write A p, form the p.Ap tile parts or the GHOST rows, and hand the stage back
 //     through its `empty` barrier.
 // Every wait is bounded: a barrier that never completes sets a bit in `err` and the thread stops.
-// The face-path GHOST tiles are processed by the first item_blocks CTAs as in k_laplacian_fused.
+// The face-path GHOST tiles (k_laplacian_fused's item CTAs) are taken by all threads of the
+// persistent CTAs once their staged tiles are done.
 // Single-GPU code: all copies read this GPU's own memory; none uses cluster multicast.
 #include "kernels.cuh"
 #include "solver_internal.hpp"
@@ -83,28 +84,25 @@ __device__ __forceinline__ PMeta pmeta_shfl(const PMeta& m, int src) {
 }
 
 template <int G, int S>
+__device__ __forceinline__ void consume(unsigned char* smem, uint64_t* full, uint64_t* empty, const Topo& tp, float* __restrict__ Y,
+                                        float* __restrict__ GACC, const Scalars* __restrict__ Sc, double* __restrict__ WP,
+                                        unsigned int* __restrict__ err, int count);
+
+template <int G, int S>
 __global__ void __launch_bounds__(128 * G + 32) k_laplacian_tma(const __grid_constant__ TileMaps maps, Topo tp,
                                                                const int* __restrict__ list, int n, const int4* __restrict__ items,
-                                                               int nitems, int item_blocks, const float* __restrict__ X,
+                                                               int nitems, const float* __restrict__ X,
                                                                float* __restrict__ Y, float* __restrict__ GACC,
                                                                const Scalars* __restrict__ Sc, double* __restrict__ WP,
                                                                unsigned int* __restrict__ err) {
     static_assert(G >= 1 && G <= 4 && S >= G && S % G == 0, "stage ring: S a multiple of the consumer groups");
     constexpr int kThreads = 128 * G + 32;
     pdl_entry();
-    if ((int)blockIdx.x < item_blocks) {
-        const int q = (int)blockIdx.x * kThreads + (int)threadIdx.x;
-        if (q >= nitems) return;
-        const int4 it = items[q];
-        if (Sc != nullptr && Sc[it.w / kLevelSlots].done) return;
-        ghost_face_sum(tp, X, it, GACC);
-        return;
-    }
     extern __shared__ unsigned char lt_smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(lt_smem_raw) + 127) & ~uintptr_t(127));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * kStageBytes);
     uint64_t* empty = full + S;
-    const int cta = (int)blockIdx.x - item_blocks, ncta = (int)gridDim.x - item_blocks;
+    const int cta = (int)blockIdx.x, ncta = (int)gridDim.x;
     const int count = n > cta ? (n - cta + ncta - 1) / ncta : 0;
     if (threadIdx.x == 0) {
         for (int i = 0; i < S; i++) {
@@ -161,9 +159,24 @@ __global__ void __launch_bounds__(128 * G + 32) k_laplacian_tma(const __grid_con
             }
             cur = nxt;
         }
-        return;
+    } else {
+        consume<G, S>(smem, full, empty, tp, Y, GACC, Sc, WP, err, count);
     }
-    // -------------------------------------------------------------------- consumer groups
+    // ------------------------------------------------- the face path, after the CTA's staged tiles
+    // every thread of the CTA takes items cta*kThreads + tid, then strides over the grid
+    for (int q = cta * kThreads + (int)threadIdx.x; q < nitems; q += ncta * kThreads) {
+        const int4 it = items[q];
+        if (Sc != nullptr && Sc[it.w / kLevelSlots].done) continue;
+        ghost_face_sum(tp, X, it, GACC);
+    }
+}
+
+// The consumer groups of k_laplacian_tma: group grp takes stages k = grp, grp + G, ...
+template <int G, int S>
+__device__ __forceinline__ void consume(unsigned char* smem, uint64_t* full, uint64_t* empty, const Topo& tp, float* __restrict__ Y,
+                                        float* __restrict__ GACC, const Scalars* __restrict__ Sc, double* __restrict__ WP,
+                                        unsigned int* __restrict__ err, int count) {
+    const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
     const int grp = warp >> 2, t = (int)threadIdx.x & 127;
     for (int k = grp; k < count; k += G) {
         const int s = k % S;
@@ -285,16 +298,19 @@ bool laplacian_tma_shape(const DevGrid& g, const float* X, float* Y, const Scala
     constexpr int threads = 128 * G + 32;
     constexpr size_t smem = tma_smem_bytes<G, S>();
     static int occ = [] {
+        // all of the SM's unified L1/shared storage as shared memory, so the occupancy the grid is
+        // sized for is the one the launch gets (the default carveout may hold fewer stage rings)
         cudaFuncSetAttribute(k_laplacian_tma<G, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_laplacian_tma<G, S>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         int o = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_laplacian_tma<G, S>, threads, smem) != cudaSuccess) o = 1;
         return o > 0 ? o : 1;
     }();
-    const int item_blocks = (g.n_lapitems + threads - 1) / threads;
-    const int want = (g.n_lapmain + G - 1) / G;
-    const int ncta = g.n_lapmain > 0 ? std::max(1, std::min(g.sm_count * occ, want)) : 0;
-    launch::launch_kernel(k_laplacian_tma<G, S>, item_blocks + ncta, threads, smem, s, *maps, g.topo, g.d_lapmain, g.n_lapmain,
-                  g.d_lapitems, g.n_lapitems, item_blocks, X, Y, g.d_gacc, Sc, WP, g.d_err);
+    // persistent: one wave of CTAs (fewer when there are few tiles and items)
+    const int want = std::max((g.n_lapmain + G - 1) / G, (g.n_lapitems + threads - 1) / threads);
+    const int ncta = std::max(1, std::min(g.sm_count * occ, want));
+    launch::launch_kernel(k_laplacian_tma<G, S>, ncta, threads, smem, s, *maps, g.topo, g.d_lapmain, g.n_lapmain, g.d_lapitems,
+                          g.n_lapitems, X, Y, g.d_gacc, Sc, WP, g.d_err);
     return true;
 }
 
@@ -314,7 +330,7 @@ bool laplacian_tma(const DevGrid& g, int variant, const float* X, float* Y, cons
     double* WP = with_pap ? g.d_wpart : nullptr;
     switch (variant) {
     case 0: return laplacian_tma_shape<2, 8>(g, X, Y, S, s, WP);
-    case 1: return laplacian_tma_shape<4, 8>(g, X, Y, S, s, WP);
+    case 1: return laplacian_tma_shape<4, 16>(g, X, Y, S, s, WP);
     case 2: return laplacian_tma_shape<2, 12>(g, X, Y, S, s, WP);
     default: return laplacian_tma_shape<1, 6>(g, X, Y, S, s, WP);
     }

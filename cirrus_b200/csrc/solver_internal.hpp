@@ -58,7 +58,7 @@ struct GraphKey {
 enum { KS_GS_SWEEP = 0, KS_PRESMOOTH = 1, KS_PROLONG = 2, KS_RESIDUAL = 3, KS_LAPLACIAN = 4, KS_COUNT = 5 };
 constexpr int kNumShapes = 8;
 // the Laplacian has four more: the TMA-staged pipeline (lap_tma.cu) with (consumer groups, stages)
-// = (2, 8), (4, 8), (2, 12), (1, 6)
+// = (2, 8), (4, 16), (2, 12), (1, 6)
 constexpr int kNumLapShapes = 12;
 inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kNumShapes; }
 
@@ -232,7 +232,7 @@ double list_dot(const DevGrid& g, const float* A, const float* B, const int* lis
 // with_pap: also store the p.Ap tile parts of LEAF tiles without GHOST children (d_wpart)
 void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s, bool with_pap = false);
 // The same with the staged tiles moved by bulk asynchronous copies through a stage ring
-// (lap_tma.cu); variant 0..3 = (consumer groups, stages) (2, 8), (4, 8), (2, 12), (1, 6).  False
+// (lap_tma.cu); variant 0..3 = (consumer groups, stages) (2, 8), (4, 16), (2, 12), (1, 6).  False
 // (nothing launched) when the tensor maps of X cannot be made.
 bool laplacian_tma(const DevGrid& g, int variant, const float* X, float* Y, const Scalars* S, cudaStream_t s, bool with_pap);
 // Ap += GHOST children's sums on the LEAF tiles that have them, and their p.Ap tile parts

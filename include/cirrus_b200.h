@@ -395,6 +395,48 @@ cirrus_status cirrus_damped_jacobi_solve(cirrus_grid* grid, int max_iters, doubl
 cirrus_status cirrus_true_residual(cirrus_grid* grid, const float* b_host, double* rel, void* stream);
 
 /* ------------------------------------------------------------------------------------------
+ * Tile-holder files: the reference's on-disk form of a grid's tiles, its checkpoint, warm-start
+ * and interchange format (IOFunc::WriteHAHostTileHolderToFile / ReadHAHostTileHolderFromFile,
+ * src/PoissonIOFunc.cu:38-121, over HAHostTileHolder<PoissonTile<float>>, src/HAGrid.h:74-92).
+ * The file holds h0, the layer count and the finest level, the raw 33104-byte PoissonTile<float>
+ * records (11 channels of 736 floats, neighbour infos, 512 cell types, flags) and per level the
+ * tile infos (coordinates, level, type, record index).  Files written here are read by the
+ * reference's reader and the other way round.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct cirrus_holder cirrus_holder;
+
+/* Reads a holder file (ReadHAHostTileHolderFromFile); CIRRUS_ERR_INVALID_ARGUMENT if it cannot be
+ * opened or is truncated or inconsistent. */
+cirrus_status cirrus_holder_read(const char* path, cirrus_holder** out);
+/* Writes a holder file (WriteHAHostTileHolderToFile). */
+cirrus_status cirrus_holder_write(const cirrus_holder* holder, const char* path);
+void cirrus_holder_destroy(cirrus_holder* holder);
+/* Any output may be NULL.  num_tiles counts the tile infos of all levels. */
+cirrus_status cirrus_holder_info(const cirrus_holder* holder, double* h0, int* num_layers, int* max_level, int* num_tiles);
+/* The holder's tiles level by level, each level in file order: level, x, y, z, type (5 int32). */
+cirrus_status cirrus_holder_tiles(const cirrus_holder* holder, int32_t* tiles5);
+/* Cell types (num_tiles*512 bytes) and one channel (0..10; num_tiles*512 floats, the first 512
+ * of the record's 736), in the order of cirrus_holder_tiles. */
+cirrus_status cirrus_holder_cell_types(const cirrus_holder* holder, uint8_t* out);
+cirrus_status cirrus_holder_channel(const cirrus_holder* holder, int channel, float* out);
+/* HADeviceGrid(h0, log2_hash) + setTilesFromHolder + compressHost (src/HAGrid.h:316-331, 491-561):
+ * a topology of the holder's tiles, inserted level by level in file order into hash tables of the
+ * given sizes, then compressed; cell types from the records.  order (optional, num_tiles int32)
+ * receives each holder tile's index in the topology's all-tiles order. */
+cirrus_status cirrus_topology_from_holder(const cirrus_holder* holder, const uint32_t* log2_hash, int num_layers, cirrus_topology** out,
+                                          int32_t* order);
+/* HADeviceGrid::getHostTileHolder(tile_types) (src/HAGrid.h:433-462) of a single-instance grid
+ * and the topology it was created from: the tiles whose type is in tile_types, level by level in
+ * all-tiles order, with channels 0..8 and the cell types copied from the device (channels 9, 10,
+ * the neighbour infos and the flags zero).  Synchronous. */
+cirrus_status cirrus_holder_from_grid(const cirrus_topology* topo, const cirrus_grid* grid, int tile_types, cirrus_holder** out);
+/* Copies the holder's channels selected by channel_mask (bit c: channel c, 0..8) into the grid's
+ * tiles at order[i] (from cirrus_topology_from_holder); other tiles keep their values.  A warm
+ * start: load channel 0 and solve in mixed precision with warm_start = 1.  Synchronous. */
+cirrus_status cirrus_grid_load_holder(cirrus_grid* grid, const cirrus_holder* holder, const int32_t* order, uint32_t channel_mask,
+                                      void* stream);
+
+/* ------------------------------------------------------------------------------------------
  * Serving loop (no counterpart in the reference): independent problems ("sessions") whose
  * solves arrive over time run concurrently on `slots` worker slots (one host thread and one
  * CUDA stream each, so their kernels overlap on the GPU), admitted against an HBM budget.  A

@@ -336,6 +336,9 @@ def ref_lib():
             "ref_solve": (C.c_int, [P, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p, f64p]),
             "ref_damped_jacobi": (C.c_int, [P, C.c_int, C.c_double, C.c_float, f64p]),
             "ref_last_error": (C.c_int, []),
+            "ref_tile_layout": (None, [C.POINTER(C.c_longlong)]),
+            "ref_write_holder": (C.c_int, [P, C.c_int, C.c_char_p]),
+            "ref_read_holder": (P, [C.c_char_p, C.c_int, C.POINTER(C.c_uint32)]),
         }
         for k, (r, a) in protos.items():
             f = getattr(L, k)
@@ -370,8 +373,36 @@ def ref_dropin_lib():
     return _RDLIB
 
 
+def ref_tile_layout() -> dict:
+    """sizeof / offsets of the reference's PoissonTile<float> as compiled (no GPU needed)."""
+    a = (C.c_longlong * 11)()
+    ref_lib().ref_tile_layout(a)
+    keys = ["sizeof_tile", "data", "neighbors", "cell_type", "interest", "locked", "status", "serial", "sizeof_info",
+            "sizeof_T", "chnlsize"]
+    return dict(zip(keys, list(a)))
+
+
 class RefHarness:
     """The reference's HADeviceGrid driven through its own functions (GPU)."""
+
+    @classmethod
+    def from_holder(cls, path, log2_hash):
+        """A reference grid read from a tile-holder file (its reader, setTilesFromHolder,
+        compressHost, syncHostAndDevice)."""
+        arr = (C.c_uint32 * len(log2_hash))(*log2_hash)
+        h = ref_lib().ref_read_holder(str(path).encode(), len(log2_hash), arr)
+        if not h:
+            raise RuntimeError(f"reference could not read holder {path}")
+        self = cls.__new__(cls)
+        self.num_layers = len(log2_hash)
+        self.h = h
+        self.n = ref_lib().ref_num_tiles(h)
+        return self
+
+    def write_holder(self, path, tile_types=7):
+        """getHostTileHolder(tile_types) written with the reference's file layout."""
+        if ref_lib().ref_write_holder(self.h, int(tile_types), str(path).encode()) != 0:
+            raise RuntimeError(f"reference could not write holder {path}")
 
     def __init__(self, w):
         L = ref_lib()

@@ -18,6 +18,7 @@
 
 #include <chrono>
 #include <cstddef>
+#include <cstdio>
 #include <map>
 #include <memory>
 
@@ -264,5 +265,93 @@ int ref_damped_jacobi(void* h, int max_iters, double tol, float omega, double* r
     return iters;
 }
 int ref_last_error() { return (int)cudaGetLastError(); }
+
+// Layout of the reference's PoissonTile<float> and HATileInfo as this compiler lays them out --
+// what a tile-holder file's records are: sizeof(Tile), offsets of mData, mNeighbors, mCellType,
+// mIsInterestArea, mIsLockedRefine, mStatus, mSerialIdx, sizeof(HATileInfo), sizeof(T), CHNLSIZE.
+void ref_tile_layout(long long* out) {
+    out[0] = (long long)sizeof(Tile);
+    out[1] = (long long)offsetof(Tile, mData);
+    out[2] = (long long)offsetof(Tile, mNeighbors);
+    out[3] = (long long)offsetof(Tile, mCellType);
+    out[4] = (long long)offsetof(Tile, mIsInterestArea);
+    out[5] = (long long)offsetof(Tile, mIsLockedRefine);
+    out[6] = (long long)offsetof(Tile, mStatus);
+    out[7] = (long long)offsetof(Tile, mSerialIdx);
+    out[8] = (long long)sizeof(HATileInfo<Tile>);
+    out[9] = (long long)sizeof(T);
+    out[10] = (long long)Tile::CHNLSIZE;
+}
+
+// The tile-holder writer and reader (IOFunc::WriteHAHostTileHolderToFile /
+// ReadHAHostTileHolderFromFile, src/PoissonIOFunc.cu:38-121), restated here because
+// PoissonIOFunc.cu needs libraries absent from this image.  They run on the reference's own
+// HAHostTileHolder, filled by getHostTileHolder (src/HAGrid.h:433-462) and consumed by
+// setTilesFromHolder (src/HAGrid.h:316-331): header fields, the raw tile records, then per level
+// the infos with each tile's record index.
+int ref_write_holder(void* h, int tile_types, const char* path) {
+    auto& grid = *((RefGrid*)h)->g;
+    auto holder = grid.getHostTileHolder((uint8_t)tile_types);
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) return 1;
+    std::fwrite(&holder->mH0, sizeof(holder->mH0), 1, f);
+    std::fwrite(&holder->mNumLayers, sizeof(holder->mNumLayers), 1, f);
+    std::fwrite(&holder->mMaxLevel, sizeof(holder->mMaxLevel), 1, f);
+    const size_t ntiles = holder->mHostTiles.size();
+    std::fwrite(&ntiles, sizeof(ntiles), 1, f);
+    if (ntiles) std::fwrite(holder->mHostTiles.data(), sizeof(Tile), ntiles, f);
+    const size_t nlev = holder->mHostLevels.size();
+    std::fwrite(&nlev, sizeof(nlev), 1, f);
+    for (const auto& lv : holder->mHostLevels) {
+        const size_t cnt = lv.size();
+        std::fwrite(&cnt, sizeof(cnt), 1, f);
+        for (const auto& info : lv) {
+            std::fwrite(&info.mTileCoord, sizeof(info.mTileCoord), 1, f);
+            std::fwrite(&info.mLevel, sizeof(info.mLevel), 1, f);
+            std::fwrite(&info.mType, sizeof(info.mType), 1, f);
+            const intptr_t idx = info.mTilePtr ? (intptr_t)(info.mTilePtr - holder->mHostTiles.data()) : (intptr_t)-1;
+            std::fwrite(&idx, sizeof(idx), 1, f);
+        }
+    }
+    return std::fclose(f) == 0 ? 0 : 1;
+}
+// A new reference grid (hash sizes log2hash) filled from a holder file: read, setTilesFromHolder,
+// compressHost, syncHostAndDevice.  NULL if the file cannot be read.
+void* ref_read_holder(const char* path, int num_layers, const uint32_t* log2hash) {
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) return nullptr;
+    HAHostTileHolder<Tile> holder;
+    bool ok = std::fread(&holder.mH0, sizeof(holder.mH0), 1, f) == 1 && std::fread(&holder.mNumLayers, sizeof(holder.mNumLayers), 1, f) == 1 &&
+              std::fread(&holder.mMaxLevel, sizeof(holder.mMaxLevel), 1, f) == 1;
+    size_t ntiles = 0, nlev = 0;
+    ok = ok && std::fread(&ntiles, sizeof(ntiles), 1, f) == 1;
+    if (ok) {
+        holder.mHostTiles.resize(ntiles);
+        ok = ntiles == 0 || std::fread(holder.mHostTiles.data(), sizeof(Tile), ntiles, f) == ntiles;
+    }
+    ok = ok && std::fread(&nlev, sizeof(nlev), 1, f) == 1;
+    if (ok) holder.mHostLevels.resize(nlev);
+    for (size_t l = 0; ok && l < nlev; l++) {
+        size_t cnt = 0;
+        ok = std::fread(&cnt, sizeof(cnt), 1, f) == 1;
+        if (ok) holder.mHostLevels[l].resize(cnt);
+        for (size_t i = 0; ok && i < cnt; i++) {
+            auto& info = holder.mHostLevels[l][i];
+            intptr_t idx = -1;
+            ok = std::fread(&info.mTileCoord, sizeof(info.mTileCoord), 1, f) == 1 && std::fread(&info.mLevel, sizeof(info.mLevel), 1, f) == 1 &&
+                 std::fread(&info.mType, sizeof(info.mType), 1, f) == 1 && std::fread(&idx, sizeof(idx), 1, f) == 1;
+            info.mTilePtr = (ok && idx >= 0 && (size_t)idx < ntiles) ? &holder.mHostTiles[idx] : nullptr;
+        }
+    }
+    std::fclose(f);
+    if (!ok || holder.mNumLayers != num_layers) return nullptr;
+    thrust::host_vector<uint32_t> l2(log2hash, log2hash + num_layers);
+    RefGrid* r = new RefGrid();
+    r->g = std::make_unique<HADeviceGrid<Tile>>(holder.mH0, l2);
+    r->g->setTilesFromHolder(holder);
+    r->g->compressHost(false);
+    r->g->syncHostAndDevice();
+    return r;
+}
 
 }  // extern "C"

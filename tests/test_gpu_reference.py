@@ -117,7 +117,7 @@ def test_dropin_in_reference_grid(name, built_cache, ref_ok):
     for call in range(2):
         (it, rel, x_ref, r_ref), (dit, drel, x_d, r_d, dms) = _ref_then_dropin(ref, b.velocity, w.pure_neumann)
         print(f"{name} call {call}: reference {it} iters {rel:.3e}; drop-in {dit} iters {drel:.3e} ({dms:.2f} ms)")
-        assert dit == it and drel == rel
+        assert dit == it and abs(drel - rel) <= 1e-12 * rel  # FP64 sums in another order; x and r bitwise below
         assert np.array_equal(bits(x_d)[leaf], bits(x_ref)[leaf])
         assert np.array_equal(bits(r_d)[leaf], bits(r_ref)[leaf])
 
@@ -145,7 +145,7 @@ def test_dropin_follows_cell_type_changes(name, built_cache, ref_ok):
         ref.set_ctypes(ct)
         ref.calc_cell_types()
         (it, rel, x_ref, r_ref), (dit, drel, x_d, r_d, _) = _ref_then_dropin(ref, b.velocity, w.pure_neumann)
-        assert dit == it and drel == rel
+        assert dit == it and abs(drel - rel) <= 1e-12 * rel  # FP64 sums in another order; x and r bitwise below
         assert np.array_equal(bits(x_d)[leaf], bits(x_ref)[leaf])
         assert np.array_equal(bits(r_d)[leaf], bits(r_ref)[leaf])
         iters.append(it)
@@ -164,7 +164,7 @@ def test_dropin_registry_rebinds_on_new_tiles(built_cache, ref_ok):
         for b, ref in zip(bs, refs):
             leaf = (b.tiles[:, 4] & W.LEAF) != 0
             (it, rel, x_ref, _), (dit, drel, x_d, _, _) = _ref_then_dropin(ref, b.velocity, b.workload.pure_neumann)
-            assert dit == it and drel == rel
+            assert dit == it and abs(drel - rel) <= 1e-12 * rel  # FP64 sums in another order; x and r bitwise below
             assert np.array_equal(bits(x_d)[leaf], bits(x_ref)[leaf])
     assert O.ref_dropin_lib().refdrop_bound_grids() == 2
     O.ref_dropin_lib().refdrop_release_all()
@@ -336,7 +336,7 @@ def test_dropin_time_at_call_site(built_cache, ref_ok):
         ref.set_channel(1, rhs)
         dit, drel, dms = ref.solve_dropin(1000, 1e-6, 1, 10, 1, w.pure_neumann)
         drop_ms.append(dms)
-        assert dit == it and drel == rel
+        assert dit == it and abs(drel - rel) <= 1e-12 * rel  # FP64 sums in another order; x and r bitwise below
     print(f"ring512 at the call site: reference {np.median(ref_ms[1:]):.2f} ms per solve; drop-in first call (bind) "
           f"{drop_ms[0]:.2f} ms, later calls median {np.median(drop_ms[1:]):.2f} ms "
           f"({np.median(ref_ms[1:]) / np.median(drop_ms[1:]):.2f}x)")
