@@ -30,7 +30,7 @@ from ._native import (CirrusError, Completion, LEVEL_TARGET_FN, SolveParams, Sol
 __all__ = [
     "LEAF", "NONLEAF", "GHOST", "DIRICHLET", "INTERIOR", "NEUMANN",
     "X_CHANNEL", "B_CHANNEL", "R_CHANNEL", "P_CHANNEL", "AP_CHANNEL", "Z_CHANNEL", "TMP_CHANNEL", "U_CHANNEL",
-    "FLUID_EULER_LOG2_HASH", "Topology", "DeviceGrid", "GMGSolver", "Holder", "CirrusError", "lib",
+    "FLUID_EULER_LOG2_HASH", "Topology", "DeviceTopology", "DeviceGrid", "GMGSolver", "Holder", "CirrusError", "lib",
 ]
 
 LEAF, NONLEAF, GHOST = 1, 2, 4
@@ -381,7 +381,7 @@ class GMGSolver:
     """Geometric-multigrid-preconditioned CG (the reference's GMGSolver, src/GMGSolver.h:17-52)."""
 
     def __init__(self, one_over_alpha: float = 1.0, prolong_coeff: float = 1.0, precision: int = PRECISION_FP32,
-                 inner_tolerance: float = 1e-5, max_outer_iters: int = 20, warm_start: bool = False):
+                 inner_tolerance: float = 1e-7, max_outer_iters: int = 20, warm_start: bool = False):
         self.one_over_alpha = one_over_alpha
         self.prolong_coeff = prolong_coeff
         self.precision = precision
@@ -518,7 +518,7 @@ class Server:
         self._topos.pop(session, None)
 
     def submit(self, session: int, b: np.ndarray, x_out: np.ndarray, relative_tolerance: float = 1e-6,
-               max_iters: int = 1000, inner_tolerance: float = 1e-5) -> int:
+               max_iters: int = 1000, inner_tolerance: float = 1e-7) -> int:
         p = SolveParams()
         lib().cirrus_solve_params_default(C.byref(p))
         p.relative_tolerance = relative_tolerance
@@ -628,3 +628,105 @@ class Holder:
             mask |= 1 << int(c)
         o = np.ascontiguousarray(order, dtype=np.int32)
         check(lib().cirrus_grid_load_holder(grid.handle, self._h, _ptr(o, C.c_int32), mask, C.c_void_p(stream)), "cirrus_grid_load_holder")
+
+
+class DeviceTopology:
+    """The octree construction on the GPU (RefineLeafsOneStep, CoarsenStep, SpawnGhostTiles,
+    compressHost/syncHostAndDevice, CalcCellTypesFromLeafs): tables, statuses and cell types in
+    device memory, bit-exact with Topology and the reference."""
+
+    def __init__(self, h0: float = 1.0 / 8, levels_log2_hash: Sequence[int] = FLUID_EULER_LOG2_HASH):
+        self.num_layers = len(levels_log2_hash)
+        self.h0 = float(h0)
+        self.log2_hash = tuple(levels_log2_hash)
+        arr = (C.c_uint32 * self.num_layers)(*levels_log2_hash)
+        h = C.c_void_p()
+        check(lib().cirrus_dtopology_create(self.num_layers, arr, self.h0, C.byref(h)), "cirrus_dtopology_create")
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        L = loaded_lib()
+        if h is not None and h.value and L is not None:
+            L.cirrus_dtopology_destroy(h)
+            self._h = None
+
+    def set_tiles(self, level: int, coords: np.ndarray, types) -> None:
+        xyz = np.ascontiguousarray(coords, dtype=np.int32).reshape(-1, 3)
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(types, dtype=np.uint8), (xyz.shape[0],)))
+        check(lib().cirrus_dtopology_set_tiles(self._h, level, _ptr(xyz, C.c_int32), _ptr(t, C.c_uint8), xyz.shape[0]),
+              "cirrus_dtopology_set_tiles")
+
+    def compress(self) -> None:
+        check(lib().cirrus_dtopology_compress(self._h), "cirrus_dtopology_compress")
+
+    def spawn_ghost_tiles(self) -> None:
+        check(lib().cirrus_dtopology_spawn_ghost_tiles(self._h), "cirrus_dtopology_spawn_ghost_tiles")
+
+    def refine_leafs_one_step(self, masks) -> list[int]:
+        keep, ptrs, dims = _mask_args(masks, self.num_layers)
+        out = (C.c_int * self.num_layers)()
+        check(lib().cirrus_dtopology_refine_leafs_one_step(self._h, ptrs, dims, out), "cirrus_dtopology_refine_leafs_one_step")
+        del keep
+        return list(out)
+
+    def iterative_refine(self, masks) -> None:
+        keep, ptrs, dims = _mask_args(masks, self.num_layers)
+        check(lib().cirrus_dtopology_iterative_refine(self._h, ptrs, dims), "cirrus_dtopology_iterative_refine")
+        del keep
+
+    def coarsen_step(self, masks) -> list[int]:
+        """CoarsenStep: a LEAF tile whose mask entry is set has target level - 1."""
+        keep, ptrs, dims = _mask_args(masks, self.num_layers)
+        out = (C.c_int * self.num_layers)()
+        check(lib().cirrus_dtopology_coarsen_step(self._h, ptrs, dims, out), "cirrus_dtopology_coarsen_step")
+        del keep
+        return list(out)
+
+    def set_cell_types(self, ctypes: np.ndarray) -> None:
+        a = np.ascontiguousarray(ctypes, dtype=np.uint8).reshape(self.num_tiles, 512)
+        check(lib().cirrus_dtopology_set_cell_types(self._h, _ptr(a, C.c_uint8)), "cirrus_dtopology_set_cell_types")
+
+    def calc_cell_types_from_leafs(self) -> None:
+        check(lib().cirrus_dtopology_calc_cell_types_from_leafs(self._h), "cirrus_dtopology_calc_cell_types_from_leafs")
+
+    @property
+    def num_tiles(self) -> int:
+        n = C.c_int()
+        check(lib().cirrus_dtopology_num_tiles(self._h, C.byref(n)), "cirrus_dtopology_num_tiles")
+        return n.value
+
+    @property
+    def max_level(self) -> int:
+        n = C.c_int()
+        check(lib().cirrus_dtopology_max_level(self._h, C.byref(n)), "cirrus_dtopology_max_level")
+        return n.value
+
+    def tiles(self) -> np.ndarray:
+        out = np.empty((self.num_tiles, 5), dtype=np.int32)
+        check(lib().cirrus_dtopology_tiles(self._h, _ptr(out, C.c_int32)), "cirrus_dtopology_tiles")
+        return out
+
+    def hash_slots(self) -> np.ndarray:
+        out = np.empty(self.num_tiles, dtype=np.int32)
+        check(lib().cirrus_dtopology_hash_slots(self._h, _ptr(out, C.c_int32)), "cirrus_dtopology_hash_slots")
+        return out
+
+    def cell_types(self) -> np.ndarray:
+        out = np.empty((self.num_tiles, 512), dtype=np.uint8)
+        check(lib().cirrus_dtopology_cell_types(self._h, _ptr(out, C.c_uint8)), "cirrus_dtopology_cell_types")
+        return out
+
+    def statuses(self) -> np.ndarray:
+        out = np.empty(self.num_tiles, dtype=np.int32)
+        check(lib().cirrus_dtopology_statuses(self._h, _ptr(out, C.c_int32)), "cirrus_dtopology_statuses")
+        return out
+
+    def to_topology(self) -> Topology:
+        h = C.c_void_p()
+        check(lib().cirrus_dtopology_to_topology(self._h, C.byref(h)), "cirrus_dtopology_to_topology")
+        t = Topology.__new__(Topology)
+        t.num_layers = self.num_layers
+        t.h0 = self.h0
+        t._h = h
+        return t

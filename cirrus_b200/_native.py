@@ -144,6 +144,24 @@ _PROTOS = {
                                               C.POINTER(C.c_int32)]),
     "cirrus_holder_from_grid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "cirrus_grid_load_holder": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.c_uint32, C.c_void_p]),
+    "cirrus_dtopology_create": (C.c_int, [C.c_int, C.POINTER(C.c_uint32), C.c_double, C.POINTER(C.c_void_p)]),
+    "cirrus_dtopology_destroy": (None, [C.c_void_p]),
+    "cirrus_dtopology_set_tiles": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.c_int]),
+    "cirrus_dtopology_compress": (C.c_int, [C.c_void_p]),
+    "cirrus_dtopology_spawn_ghost_tiles": (C.c_int, [C.c_void_p]),
+    "cirrus_dtopology_refine_leafs_one_step": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_int),
+                                                         C.POINTER(C.c_int)]),
+    "cirrus_dtopology_iterative_refine": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_int)]),
+    "cirrus_dtopology_coarsen_step": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "cirrus_dtopology_set_cell_types": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "cirrus_dtopology_calc_cell_types_from_leafs": (C.c_int, [C.c_void_p]),
+    "cirrus_dtopology_num_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "cirrus_dtopology_max_level": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "cirrus_dtopology_tiles": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "cirrus_dtopology_hash_slots": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "cirrus_dtopology_cell_types": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "cirrus_dtopology_statuses": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "cirrus_dtopology_to_topology": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "cirrus_grid_set_launch_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "cirrus_grid_get_launch_mode": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "cirrus_full_negative_laplacian": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),

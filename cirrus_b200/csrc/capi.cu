@@ -1,6 +1,7 @@
 // C ABI (include/cirrus_b200.h).  Every entry point validates its arguments, maps internal
 // failures to cirrus_status and never lets an exception cross the boundary.
 #include "../../include/cirrus_b200.h"
+#include "dtopo.hpp"
 #include "holder.hpp"
 #include "serve.hpp"
 #include "solver_internal.hpp"
@@ -545,7 +546,7 @@ void cirrus_solve_params_default(cirrus_solve_params* p) {
     p->prolong_coeff = 1.f;
     p->precision = CIRRUS_PRECISION_FP32;
     p->warm_start = 0;
-    p->inner_tolerance = 1e-5;
+    p->inner_tolerance = 1e-7;
     p->max_outer_iters = 20;
 }
 
@@ -992,5 +993,146 @@ cirrus_status cirrus_grid_load_holder(cirrus_grid* grid, const cirrus_holder* ho
         }
         g.x64_valid = false;
         return CIRRUS_OK;
+    });
+}
+
+// ---------------------------------------------------------------- device-resident topology
+struct cirrus_dtopology {
+    cirrus::DevTopology* t;
+};
+
+namespace {
+int dt_masks(const cirrus_dtopology* dt, const uint8_t* const* masks, const int* dims, std::vector<const uint8_t*>& m,
+             std::vector<int>& d) {
+    const int nl = dt->t->num_layers();
+    m.assign(masks, masks + nl);
+    d.assign(dims, dims + 3 * nl);
+    return 0;
+}
+cirrus_status dt_status(cirrus::DevTopology* t, int rc) { return rc == 0 ? CIRRUS_OK : map_rc(rc); }
+}  // namespace
+
+cirrus_status cirrus_dtopology_create(int num_layers, const uint32_t* log2_hash, double h0, cirrus_dtopology** out) {
+    if (num_layers <= 0 || num_layers > 32 || !log2_hash || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    for (int l = 0; l < num_layers; l++)
+        if (log2_hash[l] < 1 || log2_hash[l] > 26) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        auto* t = new cirrus::DevTopology(num_layers, log2_hash, h0);
+        if (!t->last_error.empty()) {
+            delete t;
+            return CIRRUS_ERR_OUT_OF_MEMORY;
+        }
+        *out = new cirrus_dtopology{t};
+        return CIRRUS_OK;
+    });
+}
+void cirrus_dtopology_destroy(cirrus_dtopology* dt) {
+    if (!dt) return;
+    delete dt->t;
+    delete dt;
+}
+cirrus_status cirrus_dtopology_set_tiles(cirrus_dtopology* dt, int level, const int32_t* xyz, const uint8_t* types, int n) {
+    if (!dt || (n > 0 && (!xyz || !types)) || n < 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < n; i++)
+        if (types[i] != CIRRUS_LEAF && types[i] != CIRRUS_NONLEAF && types[i] != CIRRUS_GHOST) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return dt_status(dt->t, dt->t->set_tiles(level, xyz, types, n)); });
+}
+cirrus_status cirrus_dtopology_compress(cirrus_dtopology* dt) {
+    if (!dt) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return dt_status(dt->t, dt->t->compress_and_sync()); });
+}
+cirrus_status cirrus_dtopology_spawn_ghost_tiles(cirrus_dtopology* dt) {
+    if (!dt) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return dt_status(dt->t, dt->t->spawn_ghost_tiles()); });
+}
+cirrus_status cirrus_dtopology_refine_leafs_one_step(cirrus_dtopology* dt, const uint8_t* const* masks, const int* dims,
+                                                     int* refined_per_level) {
+    if (!dt || !masks || !dims) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        std::vector<const uint8_t*> m;
+        std::vector<int> d, c;
+        dt_masks(dt, masks, dims, m, d);
+        const int rc = dt->t->refine_leafs_one_step(m, d, &c);
+        if (rc == 0 && refined_per_level) std::copy(c.begin(), c.end(), refined_per_level);
+        return dt_status(dt->t, rc);
+    });
+}
+cirrus_status cirrus_dtopology_iterative_refine(cirrus_dtopology* dt, const uint8_t* const* masks, const int* dims) {
+    if (!dt || !masks || !dims) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        std::vector<const uint8_t*> m;
+        std::vector<int> d;
+        dt_masks(dt, masks, dims, m, d);
+        return dt_status(dt->t, dt->t->iterative_refine(m, d));
+    });
+}
+cirrus_status cirrus_dtopology_coarsen_step(cirrus_dtopology* dt, const uint8_t* const* masks, const int* dims, int* deleted_per_level) {
+    if (!dt || !masks || !dims) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        std::vector<const uint8_t*> m;
+        std::vector<int> d, c;
+        dt_masks(dt, masks, dims, m, d);
+        const int rc = dt->t->coarsen_step(m, d, &c);
+        if (rc == 0 && deleted_per_level) std::copy(c.begin(), c.end(), deleted_per_level);
+        return dt_status(dt->t, rc);
+    });
+}
+cirrus_status cirrus_dtopology_set_cell_types(cirrus_dtopology* dt, const uint8_t* ctypes) {
+    if (!dt || !ctypes) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return dt_status(dt->t, dt->t->set_cell_types(ctypes)); });
+}
+cirrus_status cirrus_dtopology_calc_cell_types_from_leafs(cirrus_dtopology* dt) {
+    if (!dt) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return dt_status(dt->t, dt->t->calc_cell_types_from_leafs()); });
+}
+cirrus_status cirrus_dtopology_num_tiles(const cirrus_dtopology* dt, int* num_tiles) {
+    if (!dt || !num_tiles) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *num_tiles = dt->t->num_tiles();
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_dtopology_max_level(const cirrus_dtopology* dt, int* max_level) {
+    if (!dt || !max_level) return CIRRUS_ERR_INVALID_ARGUMENT;
+    *max_level = dt->t->max_level();
+    return CIRRUS_OK;
+}
+cirrus_status cirrus_dtopology_tiles(const cirrus_dtopology* dt, int32_t* out5) {
+    if (!dt || !out5) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return dt_status(dt->t, dt->t->tiles(out5)); });
+}
+cirrus_status cirrus_dtopology_hash_slots(const cirrus_dtopology* dt, int32_t* out) {
+    if (!dt || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return dt_status(dt->t, dt->t->hash_slots(out)); });
+}
+cirrus_status cirrus_dtopology_cell_types(const cirrus_dtopology* dt, uint8_t* out) {
+    if (!dt || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return dt_status(dt->t, dt->t->cell_types(out)); });
+}
+cirrus_status cirrus_dtopology_statuses(const cirrus_dtopology* dt, int32_t* out) {
+    if (!dt || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] { return dt_status(dt->t, dt->t->statuses(out)); });
+}
+cirrus_status cirrus_dtopology_to_topology(const cirrus_dtopology* dt, cirrus_topology** out) {
+    if (!dt || !out) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        const int n = dt->t->num_tiles();
+        if (n <= 0) return CIRRUS_ERR_STATE;
+        std::vector<int32_t> t5((size_t)n * 5);
+        std::vector<uint8_t> ct((size_t)n * cirrus::kTileCells);
+        int rc = dt->t->tiles(t5.data());
+        if (!rc) rc = dt->t->cell_types(ct.data());
+        if (rc) return map_rc(rc);
+        cirrus_topology* topo = nullptr;
+        cirrus_status st = CIRRUS_OK;
+        {
+            auto* t = new cirrus::Topology(dt->t->num_layers(), dt->t->log2_hash(), dt->t->h0());
+            if (!t->import_tiles(t5.data(), n)) {
+                delete t;
+                return CIRRUS_ERR_TOPOLOGY;
+            }
+            t->set_cell_types(ct.data());
+            topo = new cirrus_topology{t};
+        }
+        *out = topo;
+        return st;
     });
 }

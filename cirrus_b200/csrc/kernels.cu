@@ -1107,7 +1107,7 @@ __global__ void __launch_bounds__(256) k_residual64(Topo tp, const int* __restri
         const size_t off = (size_t)tile * kTileCells + (v & 127) * 4;
         const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
         const V4<float> b = ld4(B + off);
-        const V4<double> ax = ld4(AX + off);
+        const V4<double> ax = AX ? ld4(AX + off) : zero4<double>();  // AX null: x = 0
         V4<double> r;
         V4<float> r32;
 #pragma unroll

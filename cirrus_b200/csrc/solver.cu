@@ -467,8 +467,10 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
     std::vector<double> rel(K, 1.0);
     for (int k = 0; k <= p.max_outer; k++) {
         set_active(g, active, s, &pure);
-        launch::full_laplacian<double>(g, g.d_x64, g.d_ax64, nullptr, s);
-        launch::residual64(g, g.d_bsave, g.d_ax64, g.d_r64, g.d_ch[kChB], s);
+        // from x = 0 the first residual is b itself: no FP64 Laplacian
+        const bool cold = k == 0 && !p.warm_start;
+        if (!cold) launch::full_laplacian<double>(g, g.d_x64, g.d_ax64, nullptr, s);
+        launch::residual64(g, g.d_bsave, cold ? nullptr : g.d_ax64, g.d_r64, g.d_ch[kChB], s);
         if (any_pure) {
             launch::norm64(g, g.d_r64, nullptr, g.d_msum, s, true);
             launch::sub_mean64(g, g.d_r64, g.d_ch[kChB], g.d_msum, g.d_dofd, s);

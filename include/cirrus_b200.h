@@ -94,6 +94,48 @@ cirrus_status cirrus_topology_calc_cell_types_from_leafs(cirrus_topology* topo);
 cirrus_status cirrus_topology_neighbor_tiles(const cirrus_topology* topo, int32_t* out6);
 
 /* ------------------------------------------------------------------------------------------
+ * Device-resident topology: the same octree construction on the GPU.  The reference rebuilds
+ * its grid every step with device kernels for the per-tile decisions and host loops for the
+ * hash-table edits, one cudaMalloc per new tile (RefineLeafsOneStep and CoarsenStep,
+ * src/PoissonGrid.h:35-314; SpawnGhostTiles, src/PoissonGrid.cu:30-60; compressHost /
+ * syncHostAndDevice, src/HAGrid.h:491-561; CalcCellTypesFromLeafs, src/PoissonSolver.cu:7-61).
+ * Here the tables, tile statuses and cell types stay in device memory: decisions are parallel
+ * kernels, the order-dependent table edits (linear-probing insertion, removeTileHost's
+ * backward-shift deletion) are applied in the reference's order by one warp, and the host reads
+ * back only per-level counts.  Tile order (hash-slot order), statuses and cell types are those of
+ * the host topology and of the reference.  Level targets come as dense per-level masks (as
+ * cirrus_topology_iterative_refine_masks): refine when mask != 0 (target = level + 1); for
+ * CoarsenStep a LEAF tile with mask != 0 has target level - 1.  Calls synchronise the device.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct cirrus_dtopology cirrus_dtopology;
+
+cirrus_status cirrus_dtopology_create(int num_layers, const uint32_t* log2_hash, double h0, cirrus_dtopology** out);
+void cirrus_dtopology_destroy(cirrus_dtopology* topo);
+/* setTileHost(level, (x, y, z), blank tile, type) for n tiles of one level, in order. */
+cirrus_status cirrus_dtopology_set_tiles(cirrus_dtopology* topo, int level, const int32_t* xyz, const uint8_t* types, int n);
+cirrus_status cirrus_dtopology_compress(cirrus_dtopology* topo);
+cirrus_status cirrus_dtopology_spawn_ghost_tiles(cirrus_dtopology* topo);
+cirrus_status cirrus_dtopology_refine_leafs_one_step(cirrus_dtopology* topo, const uint8_t* const* masks, const int* dims,
+                                                     int* refined_per_level);
+cirrus_status cirrus_dtopology_iterative_refine(cirrus_dtopology* topo, const uint8_t* const* masks, const int* dims);
+cirrus_status cirrus_dtopology_coarsen_step(cirrus_dtopology* topo, const uint8_t* const* masks, const int* dims,
+                                            int* deleted_per_level);
+/* Cell types of all tiles in all-tiles order (num_tiles*512 bytes). */
+cirrus_status cirrus_dtopology_set_cell_types(cirrus_dtopology* topo, const uint8_t* ctypes);
+cirrus_status cirrus_dtopology_calc_cell_types_from_leafs(cirrus_dtopology* topo);
+cirrus_status cirrus_dtopology_num_tiles(const cirrus_dtopology* topo, int* num_tiles);
+cirrus_status cirrus_dtopology_max_level(const cirrus_dtopology* topo, int* max_level);
+/* Exports in all-tiles order: tiles (level, x, y, z, type), hash slots, cell types, status words
+ * (the reference's mStatus: REFINE 1, DELETE 2, COARSEN 4). */
+cirrus_status cirrus_dtopology_tiles(const cirrus_dtopology* topo, int32_t* out5);
+cirrus_status cirrus_dtopology_hash_slots(const cirrus_dtopology* topo, int32_t* out);
+cirrus_status cirrus_dtopology_cell_types(const cirrus_dtopology* topo, uint8_t* ctypes);
+cirrus_status cirrus_dtopology_statuses(const cirrus_dtopology* topo, int32_t* out);
+/* A host topology holding the device topology's tiles (in its order) and cell types, from which
+ * cirrus_grid_create builds the solver's tile pool. */
+cirrus_status cirrus_dtopology_to_topology(const cirrus_dtopology* topo, cirrus_topology** out);
+
+/* ------------------------------------------------------------------------------------------
  * Device grid: the tile pool resident in HBM (SoA channels, int32 topology tables).
  * ---------------------------------------------------------------------------------------- */
 typedef struct cirrus_grid cirrus_grid;
@@ -263,7 +305,9 @@ typedef struct cirrus_solve_params {
     int precision;              /* CIRRUS_PRECISION_* */
     int warm_start;             /* mixed mode: start from the x channel instead of 0 */
     double inner_tolerance;     /* mixed mode: the tightest relative tolerance an FP32 inner solve
-                                   is asked for (each targets max(this, 0.5*tol/current residual)) */
+                                   is asked for (each targets max(this, 0.5*tol/current residual));
+                                   default 1e-7: the inner solves stop on FP32's recursive residual,
+                                   which keeps falling, so a 1e-6 solve takes one inner solve */
     int max_outer_iters;        /* mixed mode: cap on defect-correction steps */
 } cirrus_solve_params;
 

@@ -337,6 +337,10 @@ def ref_lib():
             "ref_damped_jacobi": (C.c_int, [P, C.c_int, C.c_double, C.c_float, f64p]),
             "ref_last_error": (C.c_int, []),
             "ref_tile_layout": (None, [C.POINTER(C.c_longlong)]),
+            "ref_refine_one_step": (None, [P, C.POINTER(u8p), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
+            "ref_spawn_ghosts": (None, [P]),
+            "ref_coarsen_step": (None, [P, C.POINTER(u8p), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
+            "ref_statuses": (None, [P, i32p]),
             "ref_write_holder": (C.c_int, [P, C.c_int, C.c_char_p]),
             "ref_read_holder": (P, [C.c_char_p, C.c_int, C.POINTER(C.c_uint32)]),
         }
@@ -398,6 +402,46 @@ class RefHarness:
         self.h = h
         self.n = ref_lib().ref_num_tiles(h)
         return self
+
+    @classmethod
+    def roots(cls, w):
+        """A reference grid holding only the workload's root tiles, compressed, synced and with
+        ghosts spawned (src/FluidEuler.h:437-447), not yet refined."""
+        L = ref_lib()
+        self = cls.__new__(cls)
+        self.num_layers = len(w.log2_hash)
+        arr = (C.c_uint32 * self.num_layers)(*w.log2_hash)
+        self.h = L.ref_create(self.num_layers, arr, w.h0)
+        for r in w.roots:
+            L.ref_set_tile(self.h, 0, r[0], r[1], r[2], 1)
+        L.ref_compress_sync_spawn(self.h)
+        self.n = L.ref_num_tiles(self.h)
+        return self
+
+    def refine_one_step(self, masks):
+        keep, ptrs, dims = _mask_args(masks, self.num_layers)
+        out = (C.c_int * self.num_layers)()
+        ref_lib().ref_refine_one_step(self.h, ptrs, dims, self.num_layers, out)
+        del keep
+        self.n = ref_lib().ref_num_tiles(self.h)
+        return list(out)
+
+    def spawn_ghosts(self):
+        ref_lib().ref_spawn_ghosts(self.h)
+        self.n = ref_lib().ref_num_tiles(self.h)
+
+    def coarsen_step(self, masks):
+        keep, ptrs, dims = _mask_args(masks, self.num_layers)
+        out = (C.c_int * self.num_layers)()
+        ref_lib().ref_coarsen_step(self.h, ptrs, dims, self.num_layers, out)
+        del keep
+        self.n = ref_lib().ref_num_tiles(self.h)
+        return list(out)
+
+    def statuses(self):
+        out = np.empty(self.n, dtype=np.int32)
+        ref_lib().ref_statuses(self.h, _p(out, C.c_int32))
+        return out
 
     def write_holder(self, path, tile_types=7):
         """getHostTileHolder(tile_types) written with the reference's file layout."""

@@ -85,34 +85,91 @@ void ref_compress_sync_spawn(void* h) {
     grid.syncHostAndDevice();
     SpawnGhostTiles(grid, false);
 }
+// Dense per-level masks on the device, for level-target lambdas.
+struct DeviceMasks {
+    std::vector<thrust::device_vector<uint8_t>> dm;
+    thrust::device_vector<const uint8_t*> dptr;
+    thrust::device_vector<int> ddims;
+    DeviceMasks(const uint8_t* const* masks, const int* dims, int num_levels) : dm(num_levels) {
+        thrust::host_vector<const uint8_t*> hp(num_levels, nullptr);
+        thrust::host_vector<int> hd(3 * num_levels, 0);
+        for (int l = 0; l < num_levels; l++) {
+            hd[3 * l] = dims[3 * l]; hd[3 * l + 1] = dims[3 * l + 1]; hd[3 * l + 2] = dims[3 * l + 2];
+            size_t n = (size_t)dims[3 * l] * dims[3 * l + 1] * dims[3 * l + 2];
+            if (masks[l] && n > 0) {
+                dm[l] = thrust::device_vector<uint8_t>(masks[l], masks[l] + n);
+                hp[l] = thrust::raw_pointer_cast(dm[l].data());
+            }
+        }
+        dptr = hp;
+        ddims = hd;
+    }
+    const uint8_t* const* ptrs() const { return thrust::raw_pointer_cast(dptr.data()); }
+    const int* dims() const { return thrust::raw_pointer_cast(ddims.data()); }
+};
+__host__ __device__ inline bool mask_hit(const uint8_t* const* mp, const int* dp, int nl, int l, int x, int y, int z) {
+    if (l >= nl || mp[l] == nullptr) return false;
+    if (x < 0 || y < 0 || z < 0 || x >= dp[3 * l] || y >= dp[3 * l + 1] || z >= dp[3 * l + 2]) return false;
+    return mp[l][((size_t)x * dp[3 * l + 1] + y) * dp[3 * l + 2] + z] != 0;
+}
+
 // IterativeRefine with level_target(tile) = level + mask[level][tile], masks dense per level.
 void ref_iterative_refine(void* h, const uint8_t* const* masks, const int* dims, int num_levels) {
     auto& grid = *((RefGrid*)h)->g;
-    std::vector<thrust::device_vector<uint8_t>> dm(num_levels);
-    thrust::host_vector<const uint8_t*> hp(num_levels, nullptr);
-    thrust::host_vector<int> hd(3 * num_levels, 0);
-    for (int l = 0; l < num_levels; l++) {
-        hd[3 * l] = dims[3 * l]; hd[3 * l + 1] = dims[3 * l + 1]; hd[3 * l + 2] = dims[3 * l + 2];
-        size_t n = (size_t)dims[3 * l] * dims[3 * l + 1] * dims[3 * l + 2];
-        if (masks[l] && n > 0) {
-            dm[l] = thrust::device_vector<uint8_t>(masks[l], masks[l] + n);
-            hp[l] = thrust::raw_pointer_cast(dm[l].data());
-        }
-    }
-    thrust::device_vector<const uint8_t*> dptr = hp;
-    thrust::device_vector<int> ddims = hd;
-    const uint8_t* const* mp = thrust::raw_pointer_cast(dptr.data());
-    const int* dp = thrust::raw_pointer_cast(ddims.data());
+    DeviceMasks m(masks, dims, num_levels);
+    const uint8_t* const* mp = m.ptrs();
+    const int* dp = m.dims();
     int nl = num_levels;
     auto level_target = [mp, dp, nl] __device__(const HATileAccessor<Tile>& acc, HATileInfo<Tile>& info) -> int {
         int l = info.mLevel;
-        if (l >= nl || mp[l] == nullptr) return l;
-        int x = info.mTileCoord[0], y = info.mTileCoord[1], z = info.mTileCoord[2];
-        if (x < 0 || y < 0 || z < 0 || x >= dp[3 * l] || y >= dp[3 * l + 1] || z >= dp[3 * l + 2]) return l;
-        return mp[l][((size_t)x * dp[3 * l + 1] + y) * dp[3 * l + 2] + z] ? l + 1 : l;
+        return mask_hit(mp, dp, nl, l, info.mTileCoord[0], info.mTileCoord[1], info.mTileCoord[2]) ? l + 1 : l;
     };
     IterativeRefine(grid, level_target, false);
     cudaDeviceSynchronize();
+}
+// RefineLeafsOneStep alone (no ghost spawning), the same level targets; refined tiles per level.
+void ref_refine_one_step(void* h, const uint8_t* const* masks, const int* dims, int num_levels, int* counts) {
+    auto& grid = *((RefGrid*)h)->g;
+    DeviceMasks m(masks, dims, num_levels);
+    const uint8_t* const* mp = m.ptrs();
+    const int* dp = m.dims();
+    int nl = num_levels;
+    auto level_target = [mp, dp, nl] __device__(const HATileAccessor<Tile>& acc, HATileInfo<Tile>& info) -> int {
+        int l = info.mLevel;
+        return mask_hit(mp, dp, nl, l, info.mTileCoord[0], info.mTileCoord[1], info.mTileCoord[2]) ? l + 1 : l;
+    };
+    auto c = RefineLeafsOneStep(grid, level_target, false);
+    cudaDeviceSynchronize();
+    for (size_t i = 0; i < c.size(); i++) counts[i] = c[i];
+}
+void ref_spawn_ghosts(void* h) {
+    SpawnGhostTiles(*((RefGrid*)h)->g, false);
+    cudaDeviceSynchronize();
+}
+// CoarsenStep (src/PoissonGrid.h:164-314) with level_target(tile) = level - mask[level][tile];
+// deleted tiles per level.
+void ref_coarsen_step(void* h, const uint8_t* const* masks, const int* dims, int num_levels, int* deleted) {
+    auto& grid = *((RefGrid*)h)->g;
+    DeviceMasks m(masks, dims, num_levels);
+    const uint8_t* const* mp = m.ptrs();
+    const int* dp = m.dims();
+    int nl = num_levels;
+    auto level_target = [mp, dp, nl] __device__(const HATileAccessor<Tile>& acc, HATileInfo<Tile>& info) -> int {
+        int l = info.mLevel;
+        return mask_hit(mp, dp, nl, l, info.mTileCoord[0], info.mTileCoord[1], info.mTileCoord[2]) ? l - 1 : l;
+    };
+    auto c = CoarsenStep(grid, level_target, false);
+    cudaDeviceSynchronize();
+    for (size_t i = 0; i < c.size(); i++) deleted[i] = c[i];
+}
+// mStatus of every tile, all-tiles order
+void ref_statuses(void* h, int* out) {
+    auto& grid = *((RefGrid*)h)->g;
+    for (size_t i = 0; i < grid.hAllTiles.size(); i++) {
+        int st = 0;
+        cudaMemcpy(&st, (const char*)grid.hAllTiles[i].mTilePtr + offsetof(Tile, mStatus), sizeof(int), cudaMemcpyDeviceToHost);
+        out[i] = st;
+    }
 }
 // The reference grid object itself (HADeviceGrid<Tile>*), for harnesses that run other code on it.
 void* ref_grid(void* h) { return ((RefGrid*)h)->g.get(); }
