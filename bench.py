@@ -94,6 +94,10 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-batch64", action="store_true", help="skip the 64-instance random-spheres batch")
     ap.add_argument("--no-side-configs", action="store_true", help="skip the uniform128 / sphere256 single-solve lines")
+    ap.add_argument("--profile-kernels", action="store_true",
+                    help="for a profiler: launch each staged stencil kernel once at the finest level (NVTX range "
+                         "'kernels'), then one batched solve with direct kernel launches (NVTX range 'solve'); no timing")
+    ap.add_argument("--lap-shape", type=int, default=-1, help="pin the Laplacian's launch shape (0-11) after autotuning")
     return ap.parse_args()
 
 
@@ -207,45 +211,46 @@ def build_batch(name: str, seeds: list[int]):
     return b, g
 
 
-SERVE_WORKLOADS = ["ring512", "sphere256", "uniform128", "ring64_small", "sphere64_small", "uniform32_small"]
+SERVE_SESSIONS = 16
 
 
-def run_serving(rank: int, built: dict, n_requests: int = 96, rates=(100.0, 400.0), slots: int = 8) -> dict:
-    """Serving loop under Poisson arrivals: sessions of six sizes (32^3 ... 512x512x1024 effective),
-    each request the next right-hand side of its session (a 1e-3 relative change, as from the next
-    time step), warm-started from the session's previous pressure, mixed precision to 1e-6.
-    Reported per arrival rate: throughput and p50/p99 latency (arrival to completion), against
-    the same arrival stream served one at a time by plain FP32 cold solves (service times
-    measured, queueing computed from them)."""
+def run_serving(rank: int, n_requests: int = 96, rates=(100.0, 400.0), slots: int = 8) -> dict:
+    """Serving loop under Poisson arrivals over 16 sessions (independent problems) with effective
+    sizes log-uniform over 32^3 - 512^3, 1-5 levels of leaves, each refined around a seeded
+    sphere or vortex ring (workloads.random_session); each request is the next right-hand side of
+    its session (a 1e-3 relative change, as from the next time step), warm-started from the
+    session's previous pressure, mixed precision to 1e-6.  Reported per arrival rate: throughput
+    and p50/p99 latency (arrival to completion), against the same arrival stream served one at a
+    time by plain FP32 cold solves (service times measured, queueing computed from them)."""
     import torch
 
     from cirrus_b200 import B_CHANNEL, DeviceGrid, GMGSolver, Server, workloads as W
 
-    base = {}
-    for name in SERVE_WORKLOADS:
-        b = built.get(name) or W.build(W.make(name, rank))
-        built[name] = b
+    base = []
+    for w in W.serving_sessions(SERVE_SESSIONS, seed0=1000 * rank):
+        b = W.build(w)
         g = DeviceGrid(b.topology)
         for a in range(3):
             g.set_channel(6 + a, b.velocity[a])
         g.projection_rhs()
-        base[name] = (b, g.get_channel(B_CHANNEL))
+        base.append((b, g.get_channel(B_CHANNEL)))
         g.close()
+    out = {"sessions": {b.workload.name: {"tiles": int(b.tiles.shape[0]), "dof": b.dof()} for b, _ in base}, "slots": slots,
+           "requests": n_requests, "precision": "mixed (FP32 V-cycle, FP64 defect correction), warm start", "tolerance": 1e-6,
+           "rates": []}
     rng = np.random.default_rng(1000 + rank)
-    out = {"sessions": {n: int(base[n][0].tiles.shape[0]) for n in SERVE_WORKLOADS}, "slots": slots, "requests": n_requests,
-           "precision": "mixed (FP32 V-cycle, FP64 defect correction), warm start", "tolerance": 1e-6, "rates": []}
     for rate in rates:
-        picks = rng.integers(0, len(SERVE_WORKLOADS), n_requests)
+        picks = rng.integers(0, len(base), n_requests)
         arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
-        bs = [(base[SERVE_WORKLOADS[k]][1] * (1 + np.float32(1e-3) * rng.standard_normal(base[SERVE_WORKLOADS[k]][1].shape)
-                                              .astype(np.float32))).astype(np.float32) for k in picks]
+        bs = [(base[k][1] * (1 + np.float32(1e-3) * rng.standard_normal(base[k][1].shape).astype(np.float32))).astype(np.float32)
+              for k in picks]
         srv = Server(40 << 30, slots)
-        sids = {n: srv.add_session(base[n][0].topology) for n in SERVE_WORKLOADS}
-        warm = [np.zeros_like(base[n][1]) for n in SERVE_WORKLOADS]
-        for n, x in zip(SERVE_WORKLOADS, warm):  # each session has solved once before the stream starts
-            srv.submit(sids[n], base[n][1], x)
+        sids = [srv.add_session(b.topology) for b, _ in base]
+        warm = [np.zeros_like(r) for _, r in base]
+        for k, x in enumerate(warm):  # each session has solved once before the stream starts
+            srv.submit(sids[k], base[k][1], x)
         got = 0
-        while got < len(SERVE_WORKLOADS):
+        while got < len(base):
             got += len(srv.poll(wait_ms=1000))
         xs = [np.zeros_like(x) for x in bs]
         t0 = time.perf_counter()
@@ -255,7 +260,7 @@ def run_serving(rank: int, built: dict, n_requests: int = 96, rates=(100.0, 400.
                 for c in srv.poll(wait_ms=0):
                     done[c["ticket"]] = c
                 time.sleep(0.0002)
-            sub[srv.submit(sids[SERVE_WORKLOADS[picks[i]]], bs[i], xs[i])] = i
+            sub[srv.submit(sids[picks[i]], bs[i], xs[i])] = i
         while len(done) < n_requests:
             for c in srv.poll(wait_ms=1000):
                 done[c["ticket"]] = c
@@ -265,12 +270,12 @@ def run_serving(rank: int, built: dict, n_requests: int = 96, rates=(100.0, 400.
         lat = np.array([done[t]["latency_ms"] for t in sub])
         ok = all(done[t]["status"] == 0 and done[t]["rel_residual"] < 1e-6 for t in sub)
         # the same stream one at a time: plain FP32 solves from x = 0 (service times on the GPU)
-        grids = {n: DeviceGrid(base[n][0].topology) for n in SERVE_WORKLOADS}
+        grids = [DeviceGrid(b.topology) for b, _ in base]
         solver = GMGSolver()
         stream = torch.cuda.current_stream()
         svc = []
         for i in range(n_requests):
-            g = grids[SERVE_WORKLOADS[picks[i]]]
+            g = grids[picks[i]]
             g.set_channel(B_CHANNEL, bs[i])
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -278,7 +283,7 @@ def run_serving(rank: int, built: dict, n_requests: int = 96, rates=(100.0, 400.
             e1.record(stream)
             torch.cuda.synchronize()
             svc.append(e0.elapsed_time(e1))
-        for g in grids.values():
+        for g in grids:
             g.close()
         finish, lat1 = 0.0, []
         for i in range(n_requests):
@@ -638,8 +643,8 @@ def run_ours(args, world, rank, local, pg):
                                          f"PCG iterations each) by the CPU oracle (FP32 mirror of the reference "
                                          f"arithmetic, OpenMP), {cb['seconds']:.1f} s wall"}
     g.close()
-    if rank == 0 and not args.no_serve and args.workload == "ring512":
-        out["serving"] = run_serving(rank, {"ring512": b})
+    if rank == 0 and not args.no_serve:
+        out["serving"] = run_serving(rank)
     if rank == 0 and not args.no_batch64:
         out["batch64_spheres"] = run_batch64(args)
     return out
@@ -772,8 +777,48 @@ def run_reference(args, world, rank, local, pg):
     return out
 
 
+def profile_kernels(args):
+    """The launches a profiler captures: the workload's batch built and autotuned as the bench does,
+    then inside NVTX range 'kernels' the fused Laplacian and the four V-cycle stencil kernels at the
+    finest level once each, and inside NVTX range 'solve' one batched solve launched kernel by kernel
+    (a CUDA graph with a conditional node is not followed by every profiler)."""
+    import torch
+
+    from cirrus_b200 import (B_CHANNEL, KERNEL_GS_SWEEP, KERNEL_LAPLACIAN, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP,
+                             KERNEL_RESIDUAL_RESTRICT, TMP_CHANNEL, GMGSolver)
+
+    b, g = build_batch(args.workload, batch_seeds(0, args.batch))
+    g.autotune()
+    if args.lap_shape >= 0:
+        g.set_launch_shape(args.lap_shape, KERNEL_LAPLACIAN)
+    g.copy_channel(TMP_CHANNEL, B_CHANNEL)
+    sh = torch.cuda.current_stream().cuda_stream
+    lmax = int(b.tiles[:, 0].max())
+    g.copy_channel(2, B_CHANNEL, sh)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("kernels")
+    g.bench_launch(KERNEL_LAPLACIAN, 0, 1, stream=sh)
+    for kern in (KERNEL_PRESMOOTH, KERNEL_RESIDUAL_RESTRICT, KERNEL_PROLONG_SWEEP, KERNEL_GS_SWEEP):
+        g.bench_launch(kern, lmax, 1, stream=sh)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    g.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
+    g.set_launch_mode(True)
+    torch.cuda.nvtx.range_push("solve")
+    GMGSolver().solve_batch(g, stream=sh)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    g.close()
+
+
 def main():
     args = parse()
+    if args.profile_kernels:
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        profile_kernels(args)
+        return
     if args.impl == "reference":
         # the reference arm runs on rank 0 only; other ranks exit without work or collectives
         if int(os.environ.get("RANK", "0")) != 0:

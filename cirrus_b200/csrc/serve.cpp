@@ -269,11 +269,11 @@ void Server::worker(int slot) {
                 used_ -= s->bytes;
                 s->bytes = s->grid->bytes;
                 used_ += s->bytes;
-                peak_ = std::max(peak_, used_);
                 // the pool's real size (FP64 buffers, graphs) can exceed the reservation: evict
                 // idle sessions until the resident bytes fit the budget again
                 while (used_ > budget_ && pick_lru(victims, s)) {
                 }
+                peak_ = std::max(peak_, used_);
             } else {
                 used_ -= s->bytes;  // creation failed: release the reservation
                 s->bytes = 0;

@@ -203,6 +203,49 @@ def random_spheres(seed: int = 0) -> Workload:
                     meta={"fine": fine, "depth": depth, "spheres": k, "velocity": "stream"})
 
 
+def random_session(seed: int = 0) -> Workload:
+    """One problem of the serving configuration: effective size log-uniform over 32^3 - 512^3
+    (finest level 2-6, the exponent drawn uniformly), 1-5 levels of leaves, refinement around a
+    seeded sphere (band of 8 fine cells) or a seeded vortex ring (the ring's 10%-vorticity tube);
+    Neumann box walls with a Dirichlet top, unit cube.  The number of levels is at least fine - 3,
+    so no level is refined uniformly beyond 128^3 (keeps every session within a few GB)."""
+    rng = np.random.default_rng(0xC5C50000 + seed)
+    fine = int(np.floor(rng.uniform(2.0, 7.0)))  # 8 << fine effective cells: 32 ... 512, log-uniform
+    depth = int(rng.integers(max(1, fine - 3), min(5, fine + 1) + 1))
+    base = fine - depth + 1
+    kind = "sphere" if rng.random() < 0.5 else "ring"
+    eff = 8 << fine
+    if kind == "sphere":
+        c = rng.uniform(0.3, 0.7, size=3)
+        r = float(rng.uniform(0.1, 0.25))
+        band = 8 / float(eff)
+        masks: list[np.ndarray | None] = [None] * 10
+        for l in range(fine):
+            lo, hi = _tile_boxes(l, (1, 1, 1), 1 / 8)
+            if l < base:
+                masks[l] = np.ones(lo.shape[:3], dtype=np.uint8)
+                continue
+            dmin2 = _box_point_dist2(lo, hi, c)
+            dmax2 = _box_far_dist2(lo, hi, c)
+            masks[l] = ((dmin2 <= (r + band) ** 2) & (dmax2 >= max(r - band, 0.0) ** 2)).astype(np.uint8)
+        obstacle = sphere_obstacle(c, r)
+        desc = f"sphere c={np.round(c, 3).tolist()} r={r:.3f}"
+    else:
+        c = (float(rng.uniform(0.35, 0.65)), float(rng.uniform(0.35, 0.65)), float(rng.uniform(0.3, 0.7)))
+        major = float(rng.uniform(0.1, 0.2))
+        masks = ring_masks(base, fine, c, major, 0.02, 0.1, extent=(1, 1, 1))
+        obstacle = None
+        desc = f"vortex ring c={np.round(c, 3).tolist()} R={major:.3f}"
+    return Workload(name=f"session{eff}_d{depth}_{kind}_s{seed}", roots=[(0, 0, 0)], root_extent=(1, 1, 1), masks=masks,
+                    obstacle=obstacle, seed=seed, description=f"{eff}^3 effective, leaves at levels {base}-{fine}, {desc}",
+                    meta={"fine": fine, "depth": depth, "kind": kind, "velocity": "stream"})
+
+
+def serving_sessions(count: int = 16, seed0: int = 0) -> list[Workload]:
+    """The serving configuration's problems: `count` independent random_session instances."""
+    return [random_session(seed0 + i) for i in range(count)]
+
+
 def stream_velocity(tiles: np.ndarray, seed: int) -> np.ndarray:
     """(3, n, 512) float32 N(0,1) lower-face velocities on LEAF tiles from one seeded stream in
     all-tiles order (reproducible for a given tile list; faster than face_velocity)."""

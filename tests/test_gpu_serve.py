@@ -8,7 +8,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from cirrus_b200 import DeviceGrid, Server
+from cirrus_b200 import DeviceGrid, Server, workloads as W
 
 pytestmark = pytest.mark.gpu
 
@@ -30,11 +30,11 @@ def estimate(b):
     return b.tiles.shape[0] * (512 * (10 * 4 + 3 * 8 + 4 + 3) + 512) + (4 << 20)
 
 
-def requests(built_cache):
-    """Two solves per session: b, then a perturbed b (the second starts warm)."""
+def requests(built_cache, sessions=None):
+    """Two solves per session: b, then a perturbed b (the second starts warm).  sessions: built
+    workloads (default: NAMES)."""
     out = []
-    for n in NAMES:
-        b = built_cache(n)
+    for b in sessions or [built_cache(n) for n in NAMES]:
         r0 = rhs_of(b)
         rng = np.random.default_rng(len(out))
         # the next right-hand side of the same problem, as from the next time step: 1e-3 relative change
@@ -73,8 +73,13 @@ def run(reqs, slots, budget, together, deadline_s=120.0):
     return res, stats
 
 
-def test_serve_same_alone_and_in_mix_with_warm_starts(built_cache):
-    reqs = requests(built_cache)
+@pytest.mark.parametrize("mix", ["fixed", "random_sessions"])
+def test_serve_same_alone_and_in_mix_with_warm_starts(built_cache, mix):
+    """fixed: three small named workloads; random_sessions: four problems of the serving
+    configuration's generator (sizes log-uniform 32^3-512^3, 1-5 levels, sphere or vortex-ring
+    refinement; the small draws, seeds 1, 2, 3 and 9)."""
+    sessions = None if mix == "fixed" else [W.build(W.random_session(s)) for s in (1, 2, 3, 9)]
+    reqs = requests(built_cache, sessions)
     alone, _ = run(reqs, 1, BUDGET_OK, together=False)
     mix, st = run(reqs, 4, BUDGET_OK, together=True)
     for key, (c, x) in alone.items():
