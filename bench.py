@@ -219,9 +219,11 @@ def run_serving(rank: int, n_requests: int = 96, rates=(100.0, 400.0), slots: in
     sizes log-uniform over 32^3 - 512^3, 1-5 levels of leaves, each refined around a seeded
     sphere or vortex ring (workloads.random_session); each request is the next right-hand side of
     its session (a 1e-3 relative change, as from the next time step), warm-started from the
-    session's previous pressure, mixed precision to 1e-6.  Reported per arrival rate: throughput
-    and p50/p99 latency (arrival to completion), against the same arrival stream served one at a
-    time by plain FP32 cold solves (service times measured, queueing computed from them)."""
+    session's previous pressure, mixed precision to 1e-6.  Sessions of similar size share batched
+    pools and waiting requests are merged into one launch per pool (continuous batching).  Reported
+    per arrival rate: throughput, p50/p99 latency (arrival to completion) and requests per launch,
+    against the same arrival stream served one at a time by plain FP32 cold solves (service times
+    measured, queueing computed from them)."""
     import torch
 
     from cirrus_b200 import B_CHANNEL, DeviceGrid, GMGSolver, Server, workloads as W
@@ -291,6 +293,7 @@ def run_serving(rank: int, n_requests: int = 96, rates=(100.0, 400.0), slots: in
             lat1.append(finish - arrivals[i] * 1e3)
         out["rates"].append({
             "arrival_rate_rps": rate, "throughput_rps": round(n_requests / span, 2),
+            "launches": st["launches"], "requests_per_launch": round(st["requests"] / max(st["launches"], 1), 2),
             "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
             "all_converged": ok, "peak_resident_gb": round(st["peak_bytes"] / 2**30, 3),
             "one_at_a_time_fp32": {"throughput_rps": round(n_requests / (finish / 1e3), 2),
@@ -330,6 +333,9 @@ def run_batch64(args) -> dict:
         if i >= args.warmup:
             times.append(e0.elapsed_time(e1))
     res = list(s.last_results)
+    from cirrus_b200 import KERNEL_LAPLACIAN
+
+    lap_shape = g.get_launch_shape(KERNEL_LAPLACIAN, 0)  # 8-11: the TMA-staged pipeline
     dof = sum(g.instance_dof(i) for i in range(64))
     g.close()
     value = 64 * len(times) / (sum(times) * 1e-3)
@@ -337,7 +343,8 @@ def run_batch64(args) -> dict:
             "mdof_per_s": round(dof / 64 * value / 1e6, 1), "ms_per_batch": round(float(np.mean(times)), 3),
             "all_converged": all(r.status == 0 and r.true_rel_residual < 1e-6 for r in res),
             "max_pcg_iters": int(max(r.iters for r in res)), "precision": "mixed, 1e-6 FP64 true residual",
-            "sweeps": {"level_iters": li, "coarsest_iters": ci, "source": "sweep tuner"}}
+            "sweeps": {"level_iters": li, "coarsest_iters": ci, "source": "sweep tuner"},
+            "laplacian_launch_shape": lap_shape}
 
 
 def cpu_baseline(b, rhs, budget_s: float = 10.0, max_solves: int = 5) -> dict:
@@ -598,6 +605,7 @@ def run_ours(args, world, rank, local, pg):
                                          "note": "adds the p.Ap dot the launch forms for LEAF tiles without GHOST children "
                                                  "(8 B per cell: the reference's separate Dot pass over p and Ap)"}},
         "stencil_kernels": stencil,
+        "laplacian_launch_shape": g.get_launch_shape(KERNEL_LAPLACIAN, 0),
         "whole_solve_bandwidth": {"value": round(biter * sum(iters_seen) / (total_ms * 1e-3) / 1e9, 1), "unit": "GB/s per GPU",
                                   "fusion_credited": True, "bytes_per_iteration_per_instance": int(biter),
                                   "frac_of_peak": round(biter * sum(iters_seen) / (total_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)},

@@ -485,13 +485,15 @@ class GMGSolver:
 
 
 class Server:
-    """Serving loop: sessions (independent problems) with device-resident tile pools and warm-start
-    pressure; solves submitted as they arrive run concurrently on `slots` slots, admitted against
-    an HBM budget (idle sessions evicted least recently used first)."""
+    """Serving loop with continuous batching: sessions (independent problems) of similar size share
+    a batched device tile pool; requests that arrive while a pool is busy are merged into its next
+    launch (one mixed-precision batched solve, each request warm-started from its session's last
+    pressure); `slots` launches run concurrently; pools admitted against an HBM budget (idle pools
+    evicted least recently used first).  pool_size 1 keeps every session in a pool of its own."""
 
-    def __init__(self, hbm_budget_bytes: int, slots: int = 4):
+    def __init__(self, hbm_budget_bytes: int, slots: int = 4, pool_size: int = 8):
         h = C.c_void_p()
-        check(lib().cirrus_server_create(int(hbm_budget_bytes), int(slots), C.byref(h)), "cirrus_server_create")
+        check(lib().cirrus_server_create_ex(int(hbm_budget_bytes), int(slots), int(pool_size), C.byref(h)), "cirrus_server_create_ex")
         self._h = h
         self._topos = {}
         self._live = {}  # ticket -> (b, x) kept alive until the completion is polled
@@ -547,8 +549,10 @@ class Server:
         r, pk, e = C.c_size_t(), C.c_size_t(), C.c_longlong()
         rs, pd = C.c_int(), C.c_int()
         check(lib().cirrus_server_stats(self._h, C.byref(r), C.byref(pk), C.byref(rs), C.byref(pd), C.byref(e)), "cirrus_server_stats")
+        nb, nr = C.c_longlong(), C.c_longlong()
+        check(lib().cirrus_server_batch_stats(self._h, C.byref(nb), C.byref(nr)), "cirrus_server_batch_stats")
         return {"resident_bytes": r.value, "peak_bytes": pk.value, "resident_sessions": rs.value, "pending": pd.value,
-                "evictions": e.value}
+                "evictions": e.value, "launches": nb.value, "requests": nr.value}
 
 
 class Holder:

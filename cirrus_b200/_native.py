@@ -89,6 +89,7 @@ class Completion(C.Structure):
         ("rel_residual", C.c_double),
         ("latency_ms", C.c_double),
         ("device_ms", C.c_double),
+        ("batch", C.c_int),
     ]
 
 
@@ -162,6 +163,8 @@ _PROTOS = {
     "cirrus_dtopology_cell_types": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
     "cirrus_dtopology_statuses": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "cirrus_dtopology_to_topology": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "cirrus_server_create_ex": (C.c_int, [C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "cirrus_server_batch_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "cirrus_grid_set_launch_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "cirrus_grid_get_launch_mode": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "cirrus_full_negative_laplacian": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),

@@ -774,17 +774,26 @@ cirrus_status cirrus_true_residual(cirrus_grid* grid, const float* b_host, doubl
 }
 
 // ---------------------------------------------------------------- serving loop
-cirrus_status cirrus_server_create(size_t hbm_budget_bytes, int slots, cirrus_server** out) {
-    if (!out || slots < 1 || slots > 64 || hbm_budget_bytes == 0) return CIRRUS_ERR_INVALID_ARGUMENT;
+cirrus_status cirrus_server_create_ex(size_t hbm_budget_bytes, int slots, int pool_size, cirrus_server** out) {
+    if (!out || slots < 1 || slots > 64 || hbm_budget_bytes == 0 || pool_size < 1 || pool_size > 1024) return CIRRUS_ERR_INVALID_ARGUMENT;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
         return CIRRUS_ERR_NO_DEVICE;
     }
     return guard([&] {
-        *out = new cirrus_server{new cirrus::Server(hbm_budget_bytes, slots)};
+        *out = new cirrus_server{new cirrus::Server(hbm_budget_bytes, slots, pool_size)};
         return CIRRUS_OK;
     });
+}
+cirrus_status cirrus_server_create(size_t hbm_budget_bytes, int slots, cirrus_server** out) {
+    return cirrus_server_create_ex(hbm_budget_bytes, slots, 8, out);
+}
+cirrus_status cirrus_server_batch_stats(cirrus_server* server, long long* launches, long long* requests) {
+    if (!server) return CIRRUS_ERR_INVALID_ARGUMENT;
+    if (launches) *launches = server->s->batches();
+    if (requests) *requests = server->s->merged_requests();
+    return CIRRUS_OK;
 }
 void cirrus_server_destroy(cirrus_server* server) {
     if (!server) return;
@@ -828,6 +837,7 @@ cirrus_status cirrus_server_poll(cirrus_server* server, cirrus_completion* out, 
             c.rel_residual = v[i].rel;
             c.latency_ms = v[i].latency_ms;
             c.device_ms = v[i].device_ms;
+            c.batch = v[i].batch;
         }
         *count = (int)v.size();
         return CIRRUS_OK;

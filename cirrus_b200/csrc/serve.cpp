@@ -1,13 +1,17 @@
-// Serving loop: solves of independent problems ("sessions") submitted as they arrive, run
-// concurrently on a fixed number of slots (one worker thread and one CUDA stream per slot, so the
-// GPU overlaps the solves' kernels), admitted against an HBM budget.  A session's tile pool and
-// its last pressure stay resident on the device between its solves; each solve after the first
-// starts from that pressure (FP64 defect correction from the warm start).  When a session must be
-// made resident and the budget is spent, idle sessions are evicted least recently used first,
-// their pressure kept on the host for the next warm start.  Victims are chosen under the
-// scheduler lock, but their pressure copy and pool release (a device synchronisation) run on the
-// evicting worker's stream after the lock is dropped, so other slots keep scheduling meanwhile.
-// No counterpart in the reference.
+// Serving loop with continuous batching: solves of independent problems ("sessions") are
+// submitted as they arrive; sessions of similar size share one batched tile pool (a DevGrid of
+// several instances, sessions of one size class grouped in registration order up to a tile cap;
+// the largest sessions alone), and every launch
+// takes, for the pool it serves, the oldest waiting request of each of its sessions -- requests
+// that arrived while the pool was busy join the next launch of that pool, whichever sessions
+// they come from.  Each launch is one mixed-precision batched solve (FP32 V-cycle, FP64 defect
+// correction) with only the requested instances active; per-instance results do not depend on
+// the others in the launch, so a request's pressure is the same alone and in any mix.  A fixed
+// number of slots (one worker thread and one CUDA stream each) runs launches of different pools
+// concurrently on the GPU.  Pools are admitted against an HBM budget; idle pools are evicted
+// least recently used first, their sessions' pressures kept on the host for the next warm start.
+// Victims are chosen under the scheduler lock; their pressure copies and pool releases run on the
+// evicting worker's stream after the lock is dropped.  No counterpart in the reference.
 #include "serve.hpp"
 
 #include "solver_internal.hpp"
@@ -15,6 +19,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <set>
 
 namespace cirrus {
 
@@ -22,6 +27,19 @@ namespace {
 double now_ms() {
     using namespace std::chrono;
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+// channel `c` of one instance of a batched grid <-> a host array in that instance's own order
+bool instance_copy(const DevGrid& g, int inst, int c, float* host, bool to_device, cudaStream_t s) {
+    for (const TileRun& r : g.inst_runs[inst]) {
+        float* d = g.d_ch[c] + (size_t)r.global * kTileCells;
+        float* h = host + (size_t)r.local * kTileCells;
+        const size_t bytes = (size_t)r.count * kTileCells * sizeof(float);
+        const cudaError_t e = to_device ? cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s)
+                                        : cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) return false;
+    }
+    return true;
 }
 }  // namespace
 
@@ -32,7 +50,12 @@ size_t Server::estimate_bytes(const Topology& t) {
     return tiles * (kTileCells * (10 * sizeof(float) + 3 * sizeof(double) + sizeof(float) + 3) + 512) + (size_t)(4 << 20);
 }
 
-Server::Server(size_t budget, int slots) : budget_(budget) {
+// Size classes of the pools: a launch over a pool costs about as long as its largest member's
+// solve, so only sessions of similar size are merged, and a session of kSoloTiles tiles or more
+// (whose solve fills the GPU by itself) gets a pool of its own.
+int Server::size_class(size_t tiles) { return tiles < 256 ? 0 : tiles < 1024 ? 1 : tiles < kSoloTiles ? 2 : 3; }
+
+Server::Server(size_t budget, int slots, int pool_size) : budget_(budget), pool_size_(std::max(1, pool_size)) {
     cudaGetDevice(&device_);
     for (int i = 0; i < slots; i++) workers_.emplace_back([this, i] { worker(i); });
 }
@@ -44,8 +67,8 @@ Server::~Server() {
     }
     cv_.notify_all();
     for (auto& w : workers_) w.join();
-    for (auto& kv : sessions_)
-        if (kv.second.grid) grid_destroy(kv.second.grid);
+    for (Pool& p : pools_)
+        if (p.grid) grid_destroy(p.grid);
 }
 
 int Server::add_session(const Topology* topo) {
@@ -54,6 +77,24 @@ int Server::add_session(const Topology* topo) {
     Session& s = sessions_[id];
     s.topo = topo;
     s.estimate = estimate_bytes(*topo);
+    const int cls = size_class((size_t)topo->num_tiles());
+    int p = -1;
+    for (size_t i = 0; i < pools_.size(); i++)
+        if (!pools_[i].sealed && pools_[i].size_class == cls && cls < 3 && (int)pools_[i].members.size() < pool_size_ &&
+            pools_[i].tiles + (size_t)topo->num_tiles() <= kPoolTiles) {
+            p = (int)i;
+            break;
+        }
+    if (p < 0) {
+        pools_.emplace_back();
+        p = (int)pools_.size() - 1;
+        pools_[p].size_class = cls;
+    }
+    s.pool = p;
+    s.member = (int)pools_[p].members.size();
+    pools_[p].members.push_back(id);
+    pools_[p].estimate += s.estimate;
+    pools_[p].tiles += (size_t)topo->num_tiles();
     return id;
 }
 
@@ -64,16 +105,23 @@ int Server::close_session(int id) {
     it->second.closing = true;
     // wait until no request of the session is running or queued
     cv_.wait(lk, [&] {
-        if (it->second.busy || it->second.evicting) return false;
+        if (it->second.running) return false;
         for (const Request& r : pending_)
             if (r.session == id) return false;
         return true;
     });
-    if (it->second.grid) {
-        grid_destroy(it->second.grid);
-        used_ -= it->second.bytes;
-    }
+    const int p = it->second.pool;
     sessions_.erase(it);
+    // the last session of a pool frees its device state
+    bool any = false;
+    for (int m : pools_[p].members) any = any || sessions_.count(m);
+    cv_.wait(lk, [&] { return !pools_[p].busy && !pools_[p].evicting; });
+    if (!any && pools_[p].grid) {
+        grid_destroy(pools_[p].grid);
+        pools_[p].grid = nullptr;
+        used_ -= pools_[p].bytes;
+        pools_[p].bytes = 0;
+    }
     cv_.notify_all();
     return 0;
 }
@@ -110,24 +158,23 @@ void Server::stats(size_t* resident, size_t* peak, int* resident_sessions, int* 
     if (peak) *peak = peak_;
     if (resident_sessions) {
         int c = 0;
-        for (auto& kv : sessions_) c += kv.second.grid != nullptr;
+        for (auto& kv : sessions_) c += pools_[kv.second.pool].grid != nullptr;
         *resident_sessions = c;
     }
     if (pending) *pending = (int)pending_.size();
 }
 
-// Under the lock: the first queued request that can start now.  Its session must be idle; if it
-// is not resident, the bytes it needs must fit after evicting idle sessions (chosen here, least
-// recently used first, and released by the caller outside the lock).  A session larger than the
-// whole budget fails its requests at once.
-bool Server::take_runnable(Request& r, bool& need_create, std::vector<Victim>& victims) {
+// Under the lock: the pool of the oldest queued request that can run now, with the oldest queued
+// request of each of its sessions.  The pool must be idle; if it is not resident, its bytes must
+// fit after evicting idle pools (chosen here, least recently used first, released by the caller
+// outside the lock).  A pool larger than the whole budget fails its requests at once.
+bool Server::take_runnable(Batch& b, std::vector<Victim>& victims) {
     for (auto it = pending_.begin(); it != pending_.end(); ++it) {
-        Session& s = sessions_[it->session];
-        if (s.busy || s.evicting) continue;
-        if (s.grid) {
-            need_create = false;
-        } else {
-            if (s.estimate > budget_) {
+        const int pi = sessions_[it->session].pool;
+        Pool& P = pools_[pi];
+        if (P.busy || P.evicting) continue;
+        if (!P.grid) {
+            if (P.estimate > budget_) {
                 Completion c{};
                 c.ticket = it->ticket;
                 c.session = it->session;
@@ -136,66 +183,88 @@ bool Server::take_runnable(Request& r, bool& need_create, std::vector<Victim>& v
                 done_.push_back(c);
                 pending_.erase(it);
                 cv_.notify_all();
-                return take_runnable(r, need_create, victims);
+                return take_runnable(b, victims);
             }
             size_t freeable = 0;
-            for (auto& kv : sessions_)
-                if (kv.second.grid && !kv.second.busy) freeable += kv.second.bytes;
-            if (used_ + s.estimate > budget_ + freeable) continue;
-            while (used_ + s.estimate > budget_ && pick_lru(victims, &s)) {
+            for (const Pool& q : pools_)
+                if (q.grid && !q.busy) freeable += q.bytes;
+            if (used_ + P.estimate > budget_ + freeable) continue;
+            while (used_ + P.estimate > budget_ && pick_lru(victims, pi)) {
             }
-            used_ += s.estimate;  // reserved now, corrected to the grid's bytes after its first solve
-            s.bytes = s.estimate;
+            used_ += P.estimate;  // reserved now, corrected to the grid's bytes after the launch
+            P.bytes = P.estimate;
             peak_ = std::max(peak_, used_);
-            need_create = true;
+            b.need_create = true;
+        } else {
+            b.need_create = false;
         }
-        s.busy = true;
-        r = *it;
-        pending_.erase(it);
+        P.busy = true;
+        P.sealed = true;
+        b.pool = pi;
+        b.reqs.clear();
+        std::set<int> taken;
+        for (auto jt = pending_.begin(); jt != pending_.end();) {
+            if (sessions_[jt->session].pool == pi && taken.insert(jt->session).second) {
+                b.reqs.push_back(*jt);
+                sessions_[jt->session].running = true;
+                jt = pending_.erase(jt);
+            } else {
+                ++jt;
+            }
+        }
         return true;
     }
     return false;
 }
 
-// Under the lock: detach the least recently used idle resident session (other than `keep`) as a
+// Under the lock: detach the least recently used idle resident pool (other than keep_pool) as a
 // victim; its bytes count as freed from now on.  False if there is none.
-bool Server::pick_lru(std::vector<Victim>& victims, const Session* keep) {
-    Session* lru = nullptr;
-    for (auto& kv : sessions_) {
-        Session& c = kv.second;
-        if (&c != keep && c.grid && !c.busy && !c.evicting && (!lru || c.last_used < lru->last_used)) lru = &c;
+bool Server::pick_lru(std::vector<Victim>& victims, int keep_pool) {
+    int lru = -1;
+    for (size_t i = 0; i < pools_.size(); i++) {
+        const Pool& q = pools_[i];
+        if ((int)i != keep_pool && q.grid && !q.busy && !q.evicting && (lru < 0 || q.last_used < pools_[lru].last_used)) lru = (int)i;
     }
-    if (!lru) return false;
-    choose_victim(*lru, victims);
+    if (lru < 0) return false;
+    Pool& q = pools_[lru];
+    victims.push_back({lru, q.grid});
+    q.grid = nullptr;
+    q.evicting = true;
+    used_ -= q.bytes;
+    q.bytes = 0;
+    evictions_++;
     return true;
 }
 
-void Server::choose_victim(Session& s, std::vector<Victim>& victims) {
-    victims.push_back({&s, s.grid});
-    s.grid = nullptr;
-    s.evicting = true;
-    used_ -= s.bytes;
-    s.bytes = 0;
-    evictions_++;
-}
-
-// Outside the lock: save each victim's pressure to the host (for its next warm start) and free
-// its pool; then mark it evicted.
+// Outside the lock: save every live session's pressure of each victim pool to the host (for its
+// next warm start) and free the pool; then mark it evicted.
 void Server::finish_evictions(std::vector<Victim>& victims, cudaStream_t stream) {
     if (victims.empty()) return;
     for (Victim& v : victims) {
-        const size_t cells = (size_t)v.grid->n * kTileCells;
-        v.s->x_saved.resize(cells);
-        cudaMemcpyAsync(v.s->x_saved.data(), v.grid->d_ch[kChX], cells * sizeof(float), cudaMemcpyDeviceToHost, stream);
-        cudaStreamSynchronize(stream);
+        std::vector<std::pair<int, int>> live;  // (session, member)
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (int m : pools_[v.pool].members) {
+                auto it = sessions_.find(m);
+                if (it != sessions_.end()) live.push_back({m, it->second.member});
+            }
+        }
+        for (auto& sm : live) {
+            std::vector<float> x((size_t)v.grid->inst_tiles[sm.second] * kTileCells);
+            instance_copy(*v.grid, sm.second, kChX, x.data(), false, stream);
+            cudaStreamSynchronize(stream);
+            std::lock_guard<std::mutex> lk(mu_);
+            auto it = sessions_.find(sm.first);
+            if (it != sessions_.end()) {
+                it->second.x_saved = std::move(x);
+                it->second.has_saved = true;
+            }
+        }
         grid_destroy(v.grid);
     }
     {
         std::lock_guard<std::mutex> lk(mu_);
-        for (Victim& v : victims) {
-            v.s->has_saved = true;
-            v.s->evicting = false;
-        }
+        for (Victim& v : victims) pools_[v.pool].evicting = false;
     }
     victims.clear();
     cv_.notify_all();
@@ -209,79 +278,121 @@ void Server::worker(int slot) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     for (;;) {
-        Request r;
-        bool need_create = false, got = false;
-        Session* s = nullptr;
+        Batch b;
         std::vector<Victim> victims;
+        bool got = false;
+        std::vector<const Topology*> topos;        // per instance of the pool
+        std::vector<std::vector<float>> restore;   // saved pressures per instance (pool re-created)
+        std::vector<int> req_member;               // instance of each request
+        Pool* P = nullptr;
         {
             std::unique_lock<std::mutex> lk(mu_);
             cv_.wait(lk, [&] {
                 if (stop_) return true;
-                got = take_runnable(r, need_create, victims);
+                got = take_runnable(b, victims);
                 return got;
             });
             if (!got) break;
-            s = &sessions_[r.session];
+            P = &pools_[b.pool];
+            restore.resize(P->members.size());
+            for (size_t i = 0; i < P->members.size(); i++) {
+                auto it = sessions_.find(P->members[i]);
+                topos.push_back(it != sessions_.end() ? it->second.topo : nullptr);
+                if (b.need_create && it != sessions_.end() && it->second.has_saved) restore[i] = it->second.x_saved;
+            }
+            for (const Request& r : b.reqs) req_member.push_back(sessions_[r.session].member);
+            batches_++;
+            merged_ += (long long)b.reqs.size();
         }
         finish_evictions(victims, stream);  // before the new pool is allocated
-        Completion c{};
-        c.ticket = r.ticket;
-        c.session = r.session;
-        c.slot = slot;
         int rc = 0;
-        if (need_create) {
+        if (b.need_create) {
+            // a session closed before its pool was created keeps its instance, sized by a live
+            // member's topology (it is never active)
+            const Topology* any = nullptr;
+            for (const Topology* t : topos)
+                if (t) any = t;
+            for (auto& t : topos)
+                if (!t) t = any;
             std::string err;
             DevGrid* g = nullptr;
-            rc = grid_create({s->topo}, &g, &err);
+            rc = any ? grid_create(topos, &g, &err) : 1;
             if (rc == 0) {
-                s->grid = g;
-                if (s->has_saved)
-                    cudaMemcpyAsync(g->d_ch[kChX], s->x_saved.data(), s->x_saved.size() * sizeof(float), cudaMemcpyHostToDevice,
-                                    stream);
+                P->grid = g;
+                for (size_t i = 0; i < restore.size(); i++)
+                    if (!restore[i].empty()) instance_copy(*g, (int)i, kChX, restore[i].data(), true, stream);
             }
         }
-        SolveResult res;
+        std::vector<SolveResult> res;
+        double device_ms = 0.0;
         if (rc == 0) {
-            DevGrid& g = *s->grid;
-            const size_t bytes = (size_t)g.n * kTileCells * sizeof(float);
+            DevGrid& g = *P->grid;
             cudaEventRecord(e0, stream);
-            cudaMemcpyAsync(g.d_ch[kChB], r.b, bytes, cudaMemcpyHostToDevice, stream);
-            SolveParams p = r.params;
+            std::vector<InstRequest> inst(g.num_inst);
+            for (InstRequest& q : inst) q.active = 0;
+            for (size_t k = 0; k < b.reqs.size(); k++) {
+                const Request& r = b.reqs[k];
+                const int m = req_member[k];
+                if (!instance_copy(g, m, kChB, const_cast<float*>(r.b), true, stream)) rc = 2;
+                inst[m].active = 1;
+                inst[m].tol = r.params.tol;
+                inst[m].pure_neumann = r.params.pure_neumann;
+            }
+            // the pool's instances hold their sessions' last pressures (0 before a first solve,
+            // the saved one after an eviction): every solve starts from them
+            SolveParams p = b.reqs.front().params;
             p.precision = 1;
-            p.warm_start = (s->solves > 0 || s->has_saved) ? 1 : 0;
-            rc = mixed_solve(g, p, stream, &res, nullptr);
-            if (rc == 0 && r.x) cudaMemcpyAsync(r.x, g.d_ch[kChX], bytes, cudaMemcpyDeviceToHost, stream);
+            p.warm_start = 1;
+            res.resize(g.num_inst);
+            if (rc == 0) rc = mixed_solve(g, p, stream, res.data(), inst.data());
+            for (size_t k = 0; rc == 0 && k < b.reqs.size(); k++)
+                if (b.reqs[k].x && !instance_copy(g, req_member[k], kChX, b.reqs[k].x, false, stream)) rc = 2;
             cudaEventRecord(e1, stream);
             if (cudaStreamSynchronize(stream) != cudaSuccess) rc = 2;
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            c.device_ms = ms;
+            device_ms = ms;
         }
-        c.status = rc ? rc : res.status;
-        c.iters = res.iters;
-        c.outer = res.outer;
-        c.rel = res.true_rel;
         {
             std::lock_guard<std::mutex> lk(mu_);
-            c.latency_ms = now_ms() - r.t_submit;
-            c.warm = s->solves > 0 || s->has_saved;
-            if (s->grid) {
-                used_ -= s->bytes;
-                s->bytes = s->grid->bytes;
-                used_ += s->bytes;
+            const double t = now_ms();
+            for (size_t k = 0; k < b.reqs.size(); k++) {
+                const Request& r = b.reqs[k];
+                Session& s = sessions_[r.session];
+                Completion c{};
+                c.ticket = r.ticket;
+                c.session = r.session;
+                c.slot = slot;
+                c.batch = (int)b.reqs.size();
+                const SolveResult* sr = (rc == 0 && !res.empty()) ? &res[req_member[k]] : nullptr;
+                c.status = sr ? sr->status : rc;
+                if (sr) {
+                    c.iters = sr->iters;
+                    c.outer = sr->outer;
+                    c.rel = sr->true_rel;
+                }
+                c.latency_ms = t - r.t_submit;
+                c.device_ms = device_ms;
+                c.warm = s.solves > 0 || s.has_saved;
+                s.solves++;
+                s.running = false;
+                done_.push_back(c);
+            }
+            if (P->grid) {
+                used_ -= P->bytes;
+                P->bytes = P->grid->bytes;
+                used_ += P->bytes;
                 // the pool's real size (FP64 buffers, graphs) can exceed the reservation: evict
-                // idle sessions until the resident bytes fit the budget again
-                while (used_ > budget_ && pick_lru(victims, s)) {
+                // idle pools until the resident bytes fit the budget again
+                while (used_ > budget_ && pick_lru(victims, b.pool)) {
                 }
                 peak_ = std::max(peak_, used_);
             } else {
-                used_ -= s->bytes;  // creation failed: release the reservation
-                s->bytes = 0;
+                used_ -= P->bytes;  // creation failed: release the reservation
+                P->bytes = 0;
             }
-            s->solves++;
-            s->busy = false;
-            s->last_used = ++clock_;
-            done_.push_back(c);
+            P->busy = false;
+            P->last_used = ++clock_;
         }
         cv_.notify_all();
         finish_evictions(victims, stream);

@@ -481,14 +481,19 @@ cirrus_status cirrus_grid_load_holder(cirrus_grid* grid, const cirrus_holder* ho
                                       void* stream);
 
 /* ------------------------------------------------------------------------------------------
- * Serving loop (no counterpart in the reference): independent problems ("sessions") whose
- * solves arrive over time run concurrently on `slots` worker slots (one host thread and one
- * CUDA stream each, so their kernels overlap on the GPU), admitted against an HBM budget.  A
- * session's tile pool and last pressure stay on the device between its solves, and every solve
- * after its first starts from that pressure (mixed precision: FP64 defect correction from the
- * warm start to params->relative_tolerance).  Idle sessions are evicted least recently used
- * first when a new one needs the memory; their pressure is kept on the host for the next warm
- * start.  A session's solves run one at a time, in submission order.
+ * Serving loop with continuous batching (no counterpart in the reference): independent problems
+ * ("sessions") whose solves arrive over time.  Sessions of similar size (classes of < 256,
+ * < 1024 and < 4096 tiles) registered together share one batched tile pool of up to `pool_size`
+ * instances and 8192 tiles; a session of 4096 tiles or more has a pool of its own (its solve fills
+ * the GPU by itself).  Each launch serves one pool and takes the oldest waiting request of each
+ * of its sessions, so requests that arrive while a pool is busy are merged into its next launch
+ * -- one mixed-precision batched solve (FP64 defect correction from the session's previous
+ * pressure to params->relative_tolerance) with the other instances inactive.  Per-instance
+ * results do not depend on which other requests share the launch.  `slots` worker threads, each
+ * with its own CUDA stream, run launches of different pools concurrently.  Pools are admitted
+ * against an HBM budget; idle pools are evicted least recently used first, their sessions'
+ * pressures kept on the host for the next warm start.  A session's solves run one at a time, in
+ * submission order.
  * ---------------------------------------------------------------------------------------- */
 typedef struct cirrus_server cirrus_server;
 
@@ -502,15 +507,22 @@ typedef struct cirrus_completion {
     int warm;                 /* 1 if the solve started from the session's previous pressure */
     double rel_residual;      /* FP64 true relative residual */
     double latency_ms;        /* submission to completion (host clock) */
-    double device_ms;         /* the solve on its stream, b upload to x download (CUDA events) */
+    double device_ms;         /* its launch on the stream, b uploads to x downloads (CUDA events) */
+    int batch;                /* requests solved together in that launch */
 } cirrus_completion;
 
-/* hbm_budget_bytes: device memory the sessions' state may occupy; slots: concurrent solves. */
+/* hbm_budget_bytes: device memory the pools may occupy; slots: concurrent launches; pool_size:
+ * sessions per batched pool (1: every session in a pool of its own, no merging).
+ * cirrus_server_create uses pool_size 8. */
+cirrus_status cirrus_server_create_ex(size_t hbm_budget_bytes, int slots, int pool_size, cirrus_server** out);
 cirrus_status cirrus_server_create(size_t hbm_budget_bytes, int slots, cirrus_server** out);
+/* Launches run so far and the requests they carried (requests / launches = mean batch). */
+cirrus_status cirrus_server_batch_stats(cirrus_server* server, long long* launches, long long* requests);
 /* Finishes running solves, drops queued ones, frees every session's device state. */
 void cirrus_server_destroy(cirrus_server* server);
-/* Registers a problem (a finalised topology, which must outlive the session); no device memory
- * is taken until its first solve is admitted. */
+/* Registers a problem (a finalised topology, which must stay valid while the server exists: its
+ * pool may be re-created from it after an eviction); no device memory is taken until its pool is
+ * first admitted. */
 cirrus_status cirrus_server_add_session(cirrus_server* server, const cirrus_topology* topo, int* session);
 /* Waits for the session's queued and running solves, then frees its device state. */
 cirrus_status cirrus_server_close_session(cirrus_server* server, int session);

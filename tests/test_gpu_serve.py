@@ -43,11 +43,11 @@ def requests(built_cache, sessions=None):
     return out
 
 
-def run(reqs, slots, budget, together, deadline_s=120.0):
+def run(reqs, slots, budget, together, deadline_s=120.0, pool_size=8):
     import time
 
     t_end = time.monotonic() + deadline_s
-    srv = Server(budget, slots)
+    srv = Server(budget, slots, pool_size)
     sids = [srv.add_session(b.topology) for b, _ in reqs]
     xs, done = {}, {}
     order = [(s, k) for k in range(2) for s in range(len(reqs))]  # interleaved sessions
@@ -99,7 +99,9 @@ def test_serve_budget_admission_evicts_and_keeps_results(built_cache):
     reqs = requests(built_cache)
     ref, _ = run(reqs, 2, BUDGET_OK, together=True)
     budget = max(estimate(b) for b, _ in reqs) + (1 << 20)  # room for one session at a time
-    tight, st = run(reqs, 2, budget, together=True)
+    # one session per pool, so that the budget admits one pool at a time; the results are those
+    # of the shared pools above
+    tight, st = run(reqs, 2, budget, together=True, pool_size=1)
     assert st["peak_bytes"] <= budget and st["evictions"] > 0
     for key, (c, x) in ref.items():
         c2, x2 = tight[key]
@@ -117,3 +119,28 @@ def test_serve_refuses_a_session_larger_than_the_budget(built_cache):
     c = srv.poll(wait_ms=5000)
     srv.close()
     assert len(c) == 1 and c[0]["ticket"] == t and c[0]["status"] == 7
+
+
+def test_serve_merges_waiting_requests_into_one_launch(built_cache):
+    """Requests of several sessions queued while their shared pool is busy are solved in one
+    batched launch (fewer launches than requests, each completion reporting its batch), with the
+    bits of each request solved alone."""
+    sessions = [W.build(W.random_session(s)) for s in (1, 2, 3, 9)]
+    reqs = requests(built_cache, sessions)
+    alone, _ = run(reqs, 1, BUDGET_OK, together=False)
+    srv = Server(BUDGET_OK, 1, 8)
+    sids = [srv.add_session(b.topology) for b, _ in reqs]
+    xs, done = {}, {}
+    for s, (b, rhs) in enumerate(reqs):  # every session's first solve queued at once
+        x = np.zeros_like(rhs[0])
+        xs[srv.submit(sids[s], rhs[0], x)] = (s, x)
+    while len(done) < len(reqs):
+        for c in srv.poll(wait_ms=1000):
+            done[c["ticket"]] = c
+    st = srv.stats()
+    srv.close()
+    assert st["requests"] == len(reqs) and st["launches"] < len(reqs)
+    assert max(c["batch"] for c in done.values()) > 1
+    for t, (s, x) in xs.items():
+        assert done[t]["status"] == 0
+        assert np.array_equal(x.view(np.uint32), alone[(s, 0)][1].view(np.uint32))
