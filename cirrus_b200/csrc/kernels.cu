@@ -1262,6 +1262,11 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
     ++g.launch_count;
     double* WP = with_pap ? g.d_wpart : nullptr;
     const int shape = g.shape(KS_LAPLACIAN, 0);
+    // shapes 12..15: eight cells per thread
+    if (shape >= kFirstLap8Shape) {
+        laplacian8(g, shape - kFirstLap8Shape, X, Y, S, s, WP);
+        return;
+    }
     // shapes 8..11: the TMA-staged pipeline (the cp.async shape 1 if X's tensor maps cannot be made)
     if (shape >= kNumShapes && laplacian_tma(g, shape - kNumShapes, X, Y, S, s, with_pap)) return;
     switch (shape) {

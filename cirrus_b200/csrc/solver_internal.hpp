@@ -57,9 +57,10 @@ struct GraphKey {
 // shape computes each tile with the same operations.
 enum { KS_GS_SWEEP = 0, KS_PRESMOOTH = 1, KS_PROLONG = 2, KS_RESIDUAL = 3, KS_LAPLACIAN = 4, KS_COUNT = 5 };
 constexpr int kNumShapes = 8;
-// the Laplacian has four more: the TMA-staged pipeline (lap_tma.cu) with (consumer groups, stages)
-// = (2, 8), (4, 16), (2, 12), (1, 6)
-constexpr int kNumLapShapes = 12;
+// the Laplacian has eight more: 8..11 the TMA-staged pipeline (lap_tma.cu) with (consumer groups,
+// stages) = (2, 8), (4, 16), (2, 12), (1, 6); 12..15 eight cells per thread (lap8.cu)
+constexpr int kNumLapShapes = 16;
+constexpr int kFirstLap8Shape = 12;
 inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kNumShapes; }
 
 // A contiguous run of one instance's tiles inside the merged pool: tiles local..local+count of
@@ -235,6 +236,10 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
 // (lap_tma.cu); variant 0..3 = (consumer groups, stages) (2, 8), (4, 16), (2, 12), (1, 6).  False
 // (nothing launched) when the tensor maps of X cannot be made.
 bool laplacian_tma(const DevGrid& g, int variant, const float* X, float* Y, const Scalars* S, cudaStream_t s, bool with_pap);
+// The same with a column of eight cells per thread (lap8.cu); variant 0..3 = (tile groups per
+// CTA, tiles in flight per group) (2, 2), (4, 1), (1, 4), (2, 2) with at least 7 CTAs per SM.
+// WP: as laplacian_fused's.
+void laplacian8(const DevGrid& g, int variant, const float* X, float* Y, const Scalars* S, cudaStream_t s, double* WP);
 // Ap += GHOST children's sums on the LEAF tiles that have them, and their p.Ap tile parts
 void pap_ghost(const DevGrid& g, const float* P, float* AP, cudaStream_t s);
 // RD: with the PCG residual r, also store the r.z tile parts of the level's LEAF tiles (d_wpart)

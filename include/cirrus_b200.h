@@ -417,10 +417,11 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
  * all of them), level a level of the grid (or -1: all levels; the Laplacian has one entry,
  * level 0), shape in [0, 8) for every kernel; the Laplacian also takes 8..11, its TMA-staged
  * pipeline (persistent CTAs, one producer warp issuing bulk tensor copies of each tile and its
- * halos into a ring of shared-memory stages, 1-4 consumer groups).  Lets a caller reuse tuned
+ * halos into a ring of shared-memory stages, 1-4 consumer groups), and 12..15, a column of eight
+ * cells per thread (64 threads per tile).  Lets a caller reuse tuned
  * shapes for grids of the same structure or pin one.  Shapes never change results.  No
  * counterpart in the reference. */
-#define CIRRUS_NUM_LAUNCH_SHAPES 12
+#define CIRRUS_NUM_LAUNCH_SHAPES 16
 cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape);
 cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int level, int* shape);
 

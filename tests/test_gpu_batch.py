@@ -176,17 +176,19 @@ def test_every_launch_shape_gives_the_same_bits(built_cache):
 
 
 @pytest.mark.parametrize("names", [["sphere64_small", "ring64_small"], ["ring512"], ["ring512"] * 4])
-def test_tma_laplacian_shapes_give_the_same_bits(built_cache, names):
+def test_tma_and_column_laplacian_shapes_give_the_same_bits(built_cache, names):
     """The Laplacian's TMA-staged pipeline (shapes 8-11: one producer warp issuing bulk tensor
     copies of each tile, its halos and masks into a ring of shared-memory stages, 1-4 consumer
-    groups) inside the solve -- A p of every LEAF tile, the GHOST rows, the p.Ap tile parts --
-    gives the iterations and pressure of the cp.async-staged shape bit for bit."""
+    groups) and its eight-cells-per-thread layout (shapes 12-15: 64 threads per tile) inside the
+    solve -- A p of every LEAF tile, the GHOST rows, the p.Ap tile parts -- give the iterations and
+    pressure of the cp.async-staged 4-cell shape bit for bit."""
     bs = [built_cache(n) for n in names]
     rhs = [rhs_of(b) for b in bs]
     g = DeviceGrid([b.topology for b in bs])
     s = GMGSolver()
     out = []
-    for shape in (1, 8, 9, 10, 11):
+    shapes = (1, 8, 9, 10, 11, 12, 13, 14, 15)
+    for shape in shapes:
         g.set_launch_shape(shape, KERNEL_LAPLACIAN)
         assert g.get_launch_shape(KERNEL_LAPLACIAN, 0) == shape
         for i, r in enumerate(rhs):
@@ -195,10 +197,10 @@ def test_tma_laplacian_shapes_give_the_same_bits(built_cache, names):
         res = s.solve_batch(g)
         assert all(r.status == 0 for r in s.last_results), shape
         out.append((res, [g.get_channel_instance(i, 0) for i in range(len(bs))]))
-    for k, (res, xs) in enumerate(out[1:]):
-        assert res == out[0][0], k + 8
+    for shape, (res, xs) in zip(shapes[1:], out[1:]):
+        assert res == out[0][0], shape
         for a, b in zip(out[0][1], xs):
-            assert np.array_equal(bits(a), bits(b)), k + 8
+            assert np.array_equal(bits(a), bits(b)), shape
     g.close()
 
 
