@@ -30,7 +30,7 @@ from ._native import (CirrusError, Completion, LEVEL_TARGET_FN, SolveParams, Sol
 __all__ = [
     "LEAF", "NONLEAF", "GHOST", "DIRICHLET", "INTERIOR", "NEUMANN",
     "X_CHANNEL", "B_CHANNEL", "R_CHANNEL", "P_CHANNEL", "AP_CHANNEL", "Z_CHANNEL", "TMP_CHANNEL", "U_CHANNEL",
-    "FLUID_EULER_LOG2_HASH", "Topology", "DeviceTopology", "DeviceGrid", "GMGSolver", "Holder", "CirrusError", "lib",
+    "FLUID_EULER_LOG2_HASH", "Topology", "DeviceTopology", "DeviceGrid", "GMGSolver", "AMGSolver", "Holder", "CirrusError", "lib",
 ]
 
 LEAF, NONLEAF, GHOST = 1, 2, 4
@@ -482,6 +482,64 @@ class GMGSolver:
         check(lib().cirrus_gmg_solve_host_wait(grid.handle, res), "cirrus_gmg_solve_host_wait")
         grid._inflight = None
         return [(r.iters, r.rel_residual) for r in res]
+
+
+class AMGSolver(GMGSolver):
+    """The AMG variant (the reference's AMGSolver, src/AMGSolver.h:20-53): explicit per-cell face
+    coefficients with coarse levels formed from the children, its own V-cycle, and GMGSolver's
+    PCG around it.  prepare_types_and_coeffs(grid) first (after every change of the cell types);
+    solve() then takes b in channel 1 and leaves x in channel 0, using channels 3 and 5 as the
+    V-cycle's scratch.  The coefficients live apart from the grid's channels."""
+
+    def prepare_types_and_coeffs(self, grid: DeviceGrid, stream: int = 0) -> None:
+        """AMGSolver::prepareTypesAndCoeffs (src/AMGSolver.cu:717-720)."""
+        check(lib().cirrus_amg_prepare(grid.handle, float(self.one_over_alpha), C.c_void_p(stream)), "cirrus_amg_prepare")
+
+    def coefficients(self, grid: DeviceGrid, stream: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        """((4, n, 512) FP32: x-, y-, z- face off-diagonals and the diagonal; (n, 512) AMG cell types)."""
+        n = grid.num_tiles
+        co = np.empty((4, n, 512), dtype=np.float32)
+        ty = np.empty((n, 512), dtype=np.uint8)
+        check(lib().cirrus_amg_coefficients(grid.handle, _ptr(co, C.c_float), _ptr(ty, C.c_uint8), C.c_void_p(stream)),
+              "cirrus_amg_coefficients")
+        return co, ty
+
+    def vcycle(self, grid: DeviceGrid, x_channel: int = Z_CHANNEL, f_channel: int = R_CHANNEL, tmp_channel: int = AP_CHANNEL,
+               rhs_channel: int = TMP_CHANNEL, level_iters: int = 1, coarsest_iters: int = 10, stream: int = 0) -> None:
+        """VCycleAMG (src/AMGSolver.cu:610-715)."""
+        check(lib().cirrus_amg_vcycle(grid.handle, x_channel, f_channel, tmp_channel, rhs_channel, level_iters, coarsest_iters,
+                                      float(self.one_over_alpha), float(self.prolong_coeff), C.c_void_p(stream)), "cirrus_amg_vcycle")
+
+    def solve(self, grid: DeviceGrid, verbose: bool = False, max_iters: int = 1000, relative_tolerance: float = 1e-6,
+              level_iters: int = 1, coarsest_iters: int = 10, sync_stride: int = 1, is_pure_neumann: bool = False,
+              stream: int = 0) -> tuple[int, float]:
+        """AMGSolver::solve (src/AMGSolver.cu:722-853); returns (iters, relative residual)."""
+        p = self.params(max_iters, relative_tolerance, level_iters, coarsest_iters, sync_stride, is_pure_neumann)
+        r = SolveResult()
+        check(lib().cirrus_amg_solve(grid.handle, C.byref(p), C.c_void_p(stream), C.byref(r)), "cirrus_amg_solve")
+        self.last_result = r
+        if verbose:
+            print(f"AMG-PCG: {r.iters} iters, relative residual {r.rel_residual:.3e}, status {r.status}")
+        return r.iters, r.rel_residual
+
+    def solve_batch(self, grid: DeviceGrid, active: Sequence[bool] | None = None, tolerances: Sequence[float] | None = None,
+                    pure_neumann: Sequence[bool] | None = None, stream: int = 0, **kw) -> list[tuple[int, float]]:
+        p = self.params(**kw)
+        k = grid.num_instances
+        res = (SolveResult * k)()
+        act = (C.c_int * k)(*[int(bool(a)) for a in active]) if active is not None else None
+        tol = (C.c_double * k)(*tolerances) if tolerances is not None else None
+        pn = (C.c_int * k)(*[int(bool(x)) for x in pure_neumann]) if pure_neumann is not None else None
+        check(lib().cirrus_amg_solve_batch(grid.handle, C.byref(p), act, tol, pn, C.c_void_p(stream), res), "cirrus_amg_solve_batch")
+        self.last_results = list(res)
+        self.last_result = res[0]
+        return [(r.iters, r.rel_residual) for r in res]
+
+    def solve_host(self, *a, **kw):
+        raise NotImplementedError("AMGSolver: solve from device channels (solve / solve_batch)")
+
+    def solve_host_submit(self, *a, **kw):
+        raise NotImplementedError("AMGSolver: solve from device channels (solve / solve_batch)")
 
 
 class Server:

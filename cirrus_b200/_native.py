@@ -186,6 +186,13 @@ _PROTOS = {
     "cirrus_gmg_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_int_p, c_f64_p, c_int_p, C.c_void_p,
                                          C.POINTER(SolveResult)]),
     "cirrus_gmg_solve_host": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p, C.POINTER(SolveResult)]),
+    "cirrus_amg_prepare": (C.c_int, [C.c_void_p, C.c_float, C.c_void_p]),
+    "cirrus_amg_coefficients": (C.c_int, [C.c_void_p, c_f32_p, C.POINTER(C.c_uint8), C.c_void_p]),
+    "cirrus_amg_vcycle": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                    C.c_void_p]),
+    "cirrus_amg_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveResult)]),
+    "cirrus_amg_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_int_p, c_f64_p, c_int_p, C.c_void_p,
+                                         C.POINTER(SolveResult)]),
     "cirrus_gmg_solve_host_submit": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), c_f32_p, c_f32_p, C.c_void_p]),
     "cirrus_gmg_solve_host_wait": (C.c_int, [C.c_void_p, C.POINTER(SolveResult)]),
     "cirrus_server_create": (C.c_int, [C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),

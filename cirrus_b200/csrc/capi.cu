@@ -550,9 +550,10 @@ void cirrus_solve_params_default(cirrus_solve_params* p) {
     p->max_outer_iters = 20;
 }
 
-cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_params* params, const int* active,
-                                     const double* tolerances, const int* pure_neumann, void* stream,
-                                     cirrus_solve_result* results) {
+namespace {
+// the batched solve with the GMG (0) or the AMG (1) preconditioner
+cirrus_status solve_batch_with(int preconditioner, cirrus_grid* grid, const cirrus_solve_params* params, const int* active,
+                               const double* tolerances, const int* pure_neumann, void* stream, cirrus_solve_result* results) {
     if (!grid || !params_ok(params) || !results) return CIRRUS_ERR_INVALID_ARGUMENT;
     const int K = grid->g->num_inst;
     if (tolerances)
@@ -561,6 +562,7 @@ cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_param
     return guard([&] {
         cirrus::SolveParams p;
         to_internal(params, &p);
+        p.preconditioner = preconditioner;
         std::vector<cirrus::InstRequest> req(K);
         for (int i = 0; i < K; i++) {
             req[i].active = active ? (active[i] ? 1 : 0) : 1;
@@ -583,12 +585,61 @@ cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_param
         return CIRRUS_OK;
     });
 }
+}  // namespace
+
+cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_params* params, const int* active,
+                                     const double* tolerances, const int* pure_neumann, void* stream,
+                                     cirrus_solve_result* results) {
+    return solve_batch_with(0, grid, params, active, tolerances, pure_neumann, stream, results);
+}
 
 cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream, cirrus_solve_result* result) {
     if (!grid || !params_ok(params) || !result) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] {
         std::vector<cirrus_solve_result> all(grid->g->num_inst);
         cirrus_status st = cirrus_gmg_solve_batch(grid, params, nullptr, nullptr, nullptr, stream, all.data());
+        if (st == CIRRUS_OK) *result = all[0];
+        return st;
+    });
+}
+
+cirrus_status cirrus_amg_prepare(cirrus_grid* grid, float one_over_alpha, void* stream) {
+    if (!grid || !(one_over_alpha == one_over_alpha)) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        const int rc = cirrus::amg_prepare(*grid->g, one_over_alpha, S(stream));
+        return rc ? map_rc(rc) : cuda_status();
+    });
+}
+cirrus_status cirrus_amg_coefficients(cirrus_grid* grid, float* coeffs, uint8_t* types, void* stream) {
+    if (!grid) return CIRRUS_ERR_INVALID_ARGUMENT;
+    const int rc = cirrus::amg_download(*grid->g, coeffs, types, S(stream));
+    return rc == 1 ? CIRRUS_ERR_STATE : map_rc(rc);
+}
+cirrus_status cirrus_amg_vcycle(cirrus_grid* grid, int x_channel, int f_channel, int tmp_channel, int rhs_channel, int level_iters,
+                                int coarsest_iters, float one_over_alpha, float prolong_coeff, void* stream) {
+    if (!grid || !channel_ok(x_channel) || !channel_ok(f_channel) || !channel_ok(tmp_channel) || !channel_ok(rhs_channel) ||
+        level_iters < 0 || coarsest_iters < 0)
+        return CIRRUS_ERR_INVALID_ARGUMENT;
+    const int ch[4] = {x_channel, f_channel, tmp_channel, rhs_channel};
+    for (int a = 0; a < 4; a++)
+        for (int b = a + 1; b < 4; b++)
+            if (ch[a] == ch[b]) return CIRRUS_ERR_INVALID_ARGUMENT;
+    auto& g = *grid->g;
+    if (!g.amg_ready) return CIRRUS_ERR_STATE;
+    cirrus::vcycle_amg(g, g.d_ch[x_channel], g.d_ch[f_channel], g.d_ch[tmp_channel], g.d_ch[rhs_channel], level_iters, coarsest_iters,
+                       one_over_alpha, prolong_coeff, nullptr, S(stream));
+    return cuda_status();
+}
+cirrus_status cirrus_amg_solve_batch(cirrus_grid* grid, const cirrus_solve_params* params, const int* active, const double* tolerances,
+                                     const int* pure_neumann, void* stream, cirrus_solve_result* results) {
+    if (grid && !grid->g->amg_ready) return CIRRUS_ERR_STATE;
+    return solve_batch_with(1, grid, params, active, tolerances, pure_neumann, stream, results);
+}
+cirrus_status cirrus_amg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream, cirrus_solve_result* result) {
+    if (!grid || !params_ok(params) || !result) return CIRRUS_ERR_INVALID_ARGUMENT;
+    return guard([&] {
+        std::vector<cirrus_solve_result> all(grid->g->num_inst);
+        cirrus_status st = cirrus_amg_solve_batch(grid, params, nullptr, nullptr, nullptr, stream, all.data());
         if (st == CIRRUS_OK) *result = all[0];
         return st;
     });

@@ -695,6 +695,8 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_msum);
     cudaFree(g->d_dofd);
     cudaFree(g->d_bsave);
+    cudaFree(g->d_amg);
+    cudaFree(g->d_amg_ct);
     delete g;
 }
 

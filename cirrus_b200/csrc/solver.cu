@@ -85,6 +85,11 @@ void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, fl
 
 namespace {
 
+// the fused GMG V-cycle applies (the AMG preconditioner always runs its own V-cycle)
+bool fused(const DevGrid& g, const SolveParams& p) {
+    return p.preconditioner == 0 && use_fused(g, p.level_iters, p.coarsest_iters);
+}
+
 struct Ch {
     float *x, *r, *p, *ap, *z;
 };
@@ -95,7 +100,9 @@ Ch channels(const DevGrid& g) { return {g.d_ch[kChX], g.d_ch[kChR], g.d_ch[kChP]
 void precondition(const DevGrid& g, const SolveParams& p, cudaStream_t s, bool with_dot = false) {
     const Ch c = channels(g);
     const Scalars* S = g.d_scalars;
-    if (use_fused(g, p.level_iters, p.coarsest_iters))
+    if (p.preconditioner == 1)  // AMGSolver::solve's VCycleAMG(z, r, tmp = Ap, rhs = tmp channel)
+        vcycle_amg(g, c.z, c.r, c.ap, g.d_ch[kChTmp], p.level_iters, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, S, s);
+    else if (fused(g, p))
         vcycle_fused(g, c.z, c.ap, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, S, s, with_dot ? c.r : nullptr);
     else vcycle(g, c.z, c.r, c.ap, p.level_iters, p.coarsest_iters, p.one_over_alpha, p.prolong_coeff, S, s);
 }
@@ -106,7 +113,7 @@ void record_prologue(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl
     launch::begin_solve(g, ctl, s);
     // the fused V-cycle reads GHOST right-hand sides (channel Ap) as stored: 0; nothing in the
     // fused iteration writes them
-    if (use_fused(g, p.level_iters, p.coarsest_iters)) launch::zero_ghost_tiles(g, c.ap, s);
+    if (fused(g, p)) launch::zero_ghost_tiles(g, c.ap, s);
     launch::inst_reduce(OP_INIT, g, c.x, c.r, nullptr, c.ap, ctl, EPI_INIT, SKIP_INACTIVE, s);
     if (p.pure_neumann) {
         launch::inst_reduce(OP_MEAN, g, c.r, nullptr, nullptr, nullptr, ctl, EPI_MEAN, SKIP_DONE, s);
@@ -119,7 +126,7 @@ void record_prologue(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl
 // One PCG iteration, src/GMGSolver.cu:573-653
 void record_body(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl, cudaStream_t s) {
     const Ch c = channels(g);
-    if (use_fused(g, p.level_iters, p.coarsest_iters)) {
+    if (fused(g, p)) {
         // p.Ap tile parts: from the Laplacian for LEAF tiles without GHOST children, from
         // pap_ghost (after adding the children's sums to Ap) for the others
         launch::laplacian_fused(g, c.p, c.ap, g.d_scalars, s, true);
@@ -134,7 +141,7 @@ void record_body(const DevGrid& g, const SolveParams& p, const SolveCtl& ctl, cu
         launch::inst_reduce(OP_MEAN, g, c.r, nullptr, nullptr, nullptr, ctl, EPI_MEAN, SKIP_DONE, s);
         launch::recenter(g, c.r, c.ap, s);
     }
-    if (use_fused(g, p.level_iters, p.coarsest_iters)) {
+    if (fused(g, p)) {
         precondition(g, p, s, true);  // r.z tile parts formed by the V-cycle's last colour sweeps
         launch::inst_wsum(g, ctl, EPI_BETA, SKIP_DONE, s);
     } else {
@@ -272,11 +279,15 @@ int pcg_solve(DevGrid& g, const SolveParams& p0, cudaStream_t s, SolveResult* r,
 }
 
 int pcg_launch(DevGrid& g, const SolveParams& p0, cudaStream_t s, const InstRequest* req, long long* direct_out) {
+    if (p0.preconditioner == 1 && !g.amg_ready) {
+        g.last_error = "AMG solve before its coefficients were prepared (amg_prepare)";
+        return 1;
+    }
     upload_params(g, p0, req, s);
     SolveParams p = p0;
     p.pure_neumann = any_pure_neumann(g) ? 1 : 0;
     GraphKey key{0, p.level_iters, p.coarsest_iters, p.sync_stride, p.pure_neumann, p.one_over_alpha, p.prolong_coeff,
-                 use_fused(g, p.level_iters, p.coarsest_iters) ? 1 : 0};
+                 fused(g, p) ? 1 : 0, p.preconditioner};
     DevGrid::SolveGraph sg;
     if (graphs_enabled() && g.launch_mode == 0) {
         auto it = g.graphs.find(key);
@@ -320,7 +331,7 @@ void pcg_collect(DevGrid& g, const SolveParams& p, long long direct, SolveResult
     const DevGrid::SolveGraph* sgp = nullptr;
     if (direct < 0) {
         GraphKey key{0, p.level_iters, p.coarsest_iters, p.sync_stride, any_pure_neumann(g) ? 1 : 0, p.one_over_alpha,
-                     p.prolong_coeff, use_fused(g, p.level_iters, p.coarsest_iters) ? 1 : 0};
+                     p.prolong_coeff, fused(g, p) ? 1 : 0, p.preconditioner};
         auto it = g.graphs.find(key);
         if (it != g.graphs.end()) sgp = &it->second;
     }

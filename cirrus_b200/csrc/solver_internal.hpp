@@ -45,10 +45,11 @@ struct GraphKey {
     int max_iters, level_iters, coarsest_iters, sync_stride, pure_neumann;
     float one_over_alpha, prolong_coeff;
     int fused;
+    int preconditioner;
     bool operator<(const GraphKey& o) const {
-        return std::tie(max_iters, level_iters, coarsest_iters, sync_stride, pure_neumann, one_over_alpha, prolong_coeff, fused) <
-               std::tie(o.max_iters, o.level_iters, o.coarsest_iters, o.sync_stride, o.pure_neumann, o.one_over_alpha,
-                        o.prolong_coeff, o.fused);
+        return std::tie(max_iters, level_iters, coarsest_iters, sync_stride, pure_neumann, one_over_alpha, prolong_coeff, fused,
+                        preconditioner) < std::tie(o.max_iters, o.level_iters, o.coarsest_iters, o.sync_stride, o.pure_neumann,
+                                                   o.one_over_alpha, o.prolong_coeff, o.fused, o.preconditioner);
     }
 };
 
@@ -61,7 +62,9 @@ constexpr int kNumShapes = 8;
 // stages) = (2, 8), (4, 16), (2, 12), (1, 6); 12..15 eight cells per thread (lap8.cu)
 constexpr int kNumLapShapes = 16;
 constexpr int kFirstLap8Shape = 12;
-inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kNumShapes; }
+// the colour sweep has four more: 8..11 eight cells per thread (gs8.cu)
+constexpr int kNumGsShapes = 12;
+inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kind == KS_GS_SWEEP ? kNumGsShapes : kNumShapes; }
 
 // A contiguous run of one instance's tiles inside the merged pool: tiles local..local+count of
 // the instance's all-tiles order are global..global+count (one run per level).
@@ -181,6 +184,12 @@ struct DevGrid {
     float* d_bsave = nullptr;
     bool x64_valid = false;      // the last solve was mixed precision: d_x64 holds its FP64 x
 
+    // AMG variant (amg.cu): 4 planes of n*512 coefficients (x-, y-, z- face off-diagonals,
+    // diagonal) and the AMG cell types, allocated by the first amg_prepare
+    float* d_amg = nullptr;
+    uint8_t* d_amg_ct = nullptr;
+    bool amg_ready = false;
+
     struct SolveGraph {
         cudaGraphExec_t exec = nullptr;
         long long prologue = 0, body = 0, epilogue = 0;  // kernel launches per section
@@ -240,6 +249,10 @@ bool laplacian_tma(const DevGrid& g, int variant, const float* X, float* Y, cons
 // CTA, tiles in flight per group) (2, 2), (4, 1), (1, 4), (2, 2) with at least 7 CTAs per SM.
 // WP: as laplacian_fused's.
 void laplacian8(const DevGrid& g, int variant, const float* X, float* Y, const Scalars* S, cudaStream_t s, double* WP);
+// gs_sweep with a column of eight cells per thread (gs8.cu); variant 0..3 = (tile groups per CTA,
+// tiles in flight per group) (2, 2), (4, 1), (1, 4), (2, 1)
+void gs_sweep8(const DevGrid& g, int variant, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s,
+               const float* RD);
 // Ap += GHOST children's sums on the LEAF tiles that have them, and their p.Ap tile parts
 void pap_ghost(const DevGrid& g, const float* P, float* AP, cudaStream_t s);
 // RD: with the PCG residual r, also store the r.z tile parts of the level's LEAF tiles (d_wpart)
@@ -331,7 +344,18 @@ void vcycle_fused(const DevGrid& g, float* X, float* RHS, int coarsest_iters, fl
                   const Scalars* S, cudaStream_t s, const float* dot_r = nullptr);
 bool use_fused(const DevGrid& g, int level_iters, int coarsest_iters);
 
+// AMG variant (amg.cu).  AMGSolver::prepareTypesAndCoeffs (src/AMGSolver.cu:717-720): the AMG
+// cell types and coefficients of every tile.  0, 2 (CUDA error) or 3 (out of memory).
+int amg_prepare(DevGrid& g, float one_over_alpha, cudaStream_t s);
+// the 4 coefficient planes (4 * n * 512 floats) and the AMG cell types (n * 512), either may be
+// null; synchronises s.  1 when amg_prepare has not run.
+int amg_download(const DevGrid& g, float* coeffs, uint8_t* types, cudaStream_t s);
+// VCycleAMG(grid, x, f, tmp, rhs, ...) (src/AMGSolver.cu:610-715), after amg_prepare
+void vcycle_amg(const DevGrid& g, float* X, const float* F, float* TMP, float* RHS, int level_iters, int coarsest_iters,
+                float one_over_alpha, float prolong_coeff, const Scalars* S, cudaStream_t s);
+
 struct SolveParams {
+    int preconditioner = 0;  // 0: the GMG V-cycle (GMGSolver); 1: the AMG V-cycle (AMGSolver, amg_prepare first)
     int max_iters = 1000;
     double tol = 1e-6;
     int level_iters = 1, coarsest_iters = 10, sync_stride = 1, pure_neumann = 0;

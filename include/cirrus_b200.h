@@ -353,6 +353,35 @@ cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_param
                                      const double* tolerances, const int* pure_neumann, void* stream,
                                      cirrus_solve_result* results);
 
+/* ------------------------------------------------------------------------------------------
+ * AMG variant of the preconditioner: replaces AMGSolver (src/AMGSolver.h:20-53).  Explicit
+ * per-cell face coefficients (CalculateAMGCoefficients, src/AMGSolver.cu:37-108), coarse-level
+ * coefficients and cell types formed from the children (CoarsenTypesAndAMGCoeffs, :110-204), the
+ * V-cycle on them (VCycleAMG, :610-715) and GMGSolver::solve's PCG around it
+ * (AMGSolver::solve, :722-853).  The reference keeps the coefficients in four tile channels and
+ * rewrites the NONLEAF cell types in place; here both live in separate device planes, so the
+ * grid's channels and cell types are untouched.  The reference's AMG file does not build in this
+ * project's environment, so these results are checked against a CPU restatement only.
+ * ---------------------------------------------------------------------------------------- */
+/* AMGSolver::prepareTypesAndCoeffs (src/AMGSolver.cu:717-720); one_over_alpha as the
+ * AMGSolver constructor's (1).  Required before the other AMG calls (CIRRUS_ERR_STATE). */
+cirrus_status cirrus_amg_prepare(cirrus_grid* grid, float one_over_alpha, void* stream);
+/* The prepared coefficients: coeffs (optional) 4 * num_tiles * 512 floats (the off-diagonal
+ * coefficient of each cell's x-, y- and z- face, then the diagonal, each plane in all-tiles
+ * order); types (optional) num_tiles * 512 AMG cell types.  Synchronises `stream`. */
+cirrus_status cirrus_amg_coefficients(cirrus_grid* grid, float* coeffs, uint8_t* types, void* stream);
+/* VCycleAMG(grid, x, f, tmp, rhs, level_iters, coarsest_iters, one_over_alpha, prolong_coeff)
+ * (src/AMGSolver.cu:610-715); the four channels must differ. */
+cirrus_status cirrus_amg_vcycle(cirrus_grid* grid, int x_channel, int f_channel, int tmp_channel, int rhs_channel, int level_iters,
+                                int coarsest_iters, float one_over_alpha, float prolong_coeff, void* stream);
+/* AMGSolver::solve(grid, verbose, max_iters, relative_tolerance, level_iters, coarsest_iters,
+ * sync_stride, is_pure_neumann) (src/AMGSolver.cu:722-853): b in channel 1, x to channel 0, the
+ * V-cycle using channels 3 and 5 as its scratch; params->one_over_alpha / prolong_coeff are the
+ * AMGSolver's.  Precision, graphs and batches as cirrus_gmg_solve / _batch. */
+cirrus_status cirrus_amg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream, cirrus_solve_result* result);
+cirrus_status cirrus_amg_solve_batch(cirrus_grid* grid, const cirrus_solve_params* params, const int* active, const double* tolerances,
+                                     const int* pure_neumann, void* stream, cirrus_solve_result* results);
+
 /* End-to-end variant for callers holding host arrays: copies b (num_tiles*512 floats, pinned or
  * pageable) to the device, solves, and copies x back into x_host. */
 cirrus_status cirrus_gmg_solve_host(cirrus_grid* grid, const cirrus_solve_params* params, const float* b_host,
@@ -418,7 +447,8 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
  * level 0), shape in [0, 8) for every kernel; the Laplacian also takes 8..11, its TMA-staged
  * pipeline (persistent CTAs, one producer warp issuing bulk tensor copies of each tile and its
  * halos into a ring of shared-memory stages, 1-4 consumer groups), and 12..15, a column of eight
- * cells per thread (64 threads per tile).  Lets a caller reuse tuned
+ * cells per thread (64 threads per tile); the Gauss-Seidel colour sweep also takes 8..11, eight
+ * cells per thread.  Lets a caller reuse tuned
  * shapes for grids of the same structure or pin one.  Shapes never change results.  No
  * counterpart in the reference. */
 #define CIRRUS_NUM_LAUNCH_SHAPES 16

@@ -34,6 +34,8 @@
 //   Dot / Mean / ReCenter     src/PoissonGrid.cu:165-325, src/PoissonSolver.cu:356-368
 //   Divergence (RHS)          src/PoissonSolver.cu:66-142, PoissonGrid.cu:635-661, 721-755
 //   face clearing             src/FluidEuler.cu:43-60, src/PoissonGrid.h:451-489
+//   AMG variant               src/AMGSolver.cu:16-204, 231-250, 540-853 (parity unpinned:
+//                             that file does not build here; see the AMG section)
 
 #include <cstdint>
 #include <cstring>
@@ -699,6 +701,313 @@ struct Solver {
         rel = -1;
         return i;
     }
+
+    // ================================================================ AMG variant (src/AMGSolver.cu)
+    // Parity of this section is unpinned: the reference's AMGSolver.cu does not build here (it
+    // includes VTK and Eigen headers through PoissonIOFunc.h and FMParticles.h), so this
+    // restatement is checked only against the product's kernels, not against reference output.
+    // The FP32 mirror follows the reference's source with nvcc's contraction of a*b+c into one
+    // fused multiply-add, as in the GMG kernels above.
+    std::vector<T> amg_c[4];       // per cell: off-diagonal coefficient of its x-, y-, z- face; diagonal
+    std::vector<uint8_t> amg_ct;   // cell types after CoarsenTypesAndAMGCoeffs (NONLEAF cells rewritten)
+
+    // NegativeLaplacianCoeff of the AMG file (src/AMGSolver.cu:16-35): 1/h^2 between LEAF cells,
+    // (1/(1.5h))/h between a LEAF and a GHOST cell, 0 otherwise or next to a NEUMANN cell
+    static T amg_coeff(T h, uint8_t tt0, uint8_t tt1, uint8_t ct0, uint8_t ct1) {
+        const int both = ((tt0 & LEAF) && (tt1 & LEAF)) ? 1 : 0;
+        const int olog = (((tt0 & LEAF) && (tt1 & GHOST)) || ((tt0 & GHOST) && (tt1 & LEAF))) ? 1 : 0;
+        // one of the two products is an exact 0, so no contraction changes the sum
+        const T odh = ((T)1 / h) * (T)both + ((T)1 / ((T)1.5 * h)) * (T)olog;
+        const bool nm = (ct0 & NEUMANN) || (ct1 & NEUMANN);
+        return nm ? (T)0 : odh / h;
+    }
+    // a cell's same-level neighbour across (axis, sgn): tile and offset, -1 when its tile is absent
+    int amg_nb(int t, int i, int j, int k, int axis, int sgn, int& off) const {
+        int c[3] = {i, j, k};
+        c[axis] += sgn;
+        if (c[axis] >= 0 && c[axis] <= 7) { off = loff(c[0], c[1], c[2]); return t; }
+        const int nb = f.nbr[(size_t)t * 6 + (sgn < 0 ? axis : axis + 3)];
+        c[axis] &= 7;
+        off = loff(c[0], c[1], c[2]);
+        return nb;
+    }
+    // AMGSolver::prepareTypesAndCoeffs = CoarsenTypesAndAMGCoeffs (src/AMGSolver.cu:110-204)
+    void amg_prepare(T one_over_alpha) {
+        const size_t cells = (size_t)f.n * NCELL;
+        for (auto& c : amg_c) c.assign(cells, (T)0);
+        amg_ct = f.ctype;
+        // step 1: GHOST cells take their parent cell's type (DIRICHLET without one)
+        for (int t = 0; t < f.n; t++) {
+            if (!(f.type[t] & GHOST)) continue;
+            for (int o = 0; o < NCELL; o++) {
+                const int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                int po;
+                const int p = f.find_voxel(f.level[t] - 1, (f.cx[t] * 8 + i) >> 1, (f.cy[t] * 8 + j) >> 1, (f.cz[t] * 8 + k) >> 1, po);
+                amg_ct[(size_t)t * NCELL + o] = p < 0 ? DIRICHLET : f.ctype[(size_t)p * NCELL + po];
+            }
+        }
+        // step 2: CalculateAMGCoefficients on LEAF|GHOST tiles (src/AMGSolver.cu:40-108)
+#pragma omp parallel for schedule(static)
+        for (int t = 0; t < f.n; t++) {
+            if (!(f.type[t] & (LEAF | GHOST))) continue;
+            const T h = voxel_size<T>(f.level[t]);
+            const uint8_t tt0 = f.type[t];
+            for (int o = 0; o < NCELL; o++) {
+                const int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                const size_t id = (size_t)t * NCELL + o;
+                const uint8_t ct0 = amg_ct[id];
+                T diag = 0, off[3] = {0, 0, 0};
+                for (int axis = 0; axis < 3; axis++)
+                    for (int sgn = -1; sgn <= 1; sgn += 2) {
+                        int no;
+                        const int nb = amg_nb(t, i, j, k, axis, sgn, no);
+                        uint8_t tt1 = tt0, ct1 = DIRICHLET;
+                        if (nb >= 0) { tt1 = f.type[nb]; ct1 = amg_ct[(size_t)nb * NCELL + no]; }
+                        const T c = amg_coeff(h, tt0, tt1, ct0, ct1) * h * h * h;
+                        if (sgn == -1 && ct1 == INTERIOR) off[axis] = -c;
+                        diag = diag + c;
+                    }
+                for (int axis = 0; axis < 3; axis++) amg_c[axis][id] = ct0 == INTERIOR ? off[axis] : (T)0;
+                amg_c[3][id] = ct0 == INTERIOR ? diag : (T)0;
+            }
+        }
+        // step 3: NONLEAF|LEAF tiles fine-first from their children (src/AMGSolver.cu:138-203)
+        for (int l = f.num_layers - 1; l >= 0; l--) {
+            const auto& tl = f.by_level[l];
+#pragma omp parallel for schedule(static)
+            for (int q = 0; q < (int)tl.size(); q++) {
+                const int t = tl[q];
+                if (!(f.type[t] & (LEAF | NONLEAF))) continue;
+                for (int o = 0; o < NCELL; o++) {
+                    const int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                    const int gx = f.cx[t] * 8 + i, gy = f.cy[t] * 8 + j, gz = f.cz[t] * 8 + k;
+                    int interior_cnt = 0;
+                    bool has_ghost_child = false;
+                    T cod[3][8];
+                    T diag_sum = 0;
+                    for (int ci = 0; ci < 2; ci++)
+                        for (int cj = 0; cj < 2; cj++)
+                            for (int ck = 0; ck < 2; ck++) {
+                                const int b = ci * 4 + cj * 2 + ck;
+                                int co;
+                                const int c = f.find_voxel(l + 1, gx * 2 + ci, gy * 2 + cj, gz * 2 + ck, co);
+                                if (c >= 0) {
+                                    if (f.type[c] == GHOST) has_ghost_child = true;
+                                    const size_t cid = (size_t)c * NCELL + co;
+                                    diag_sum = diag_sum + amg_c[3][cid];
+                                    interior_cnt += amg_ct[cid] == INTERIOR ? 1 : 0;
+                                    for (int a = 0; a < 3; a++) cod[a][b] = amg_c[a][cid];
+                                } else {
+                                    for (int a = 0; a < 3; a++) cod[a][b] = 0;
+                                }
+                            }
+                    T offs[3] = {0, 0, 0};
+                    for (int ci = 0; ci < 2; ci++)
+                        for (int cj = 0; cj < 2; cj++)
+                            for (int ck = 0; ck < 2; ck++) {
+                                const int b = ci * 4 + cj * 2 + ck;
+                                if (ci == 0) offs[0] = offs[0] + cod[0][b];
+                                if (ci == 1) diag_sum = fmaT<T>((T)2, cod[0][b], diag_sum);
+                                if (cj == 0) offs[1] = offs[1] + cod[1][b];
+                                if (cj == 1) diag_sum = fmaT<T>((T)2, cod[1][b], diag_sum);
+                                if (ck == 0) offs[2] = offs[2] + cod[2][b];
+                                if (ck == 1) diag_sum = fmaT<T>((T)2, cod[2][b], diag_sum);
+                            }
+                    const size_t id = (size_t)t * NCELL + o;
+                    if (f.type[t] == NONLEAF) {
+                        amg_ct[id] = interior_cnt > 0 ? INTERIOR : DIRICHLET;
+                        for (int a = 0; a < 3; a++) amg_c[a][id] = offs[a] * one_over_alpha;
+                        amg_c[3][id] = diag_sum * one_over_alpha;
+                    }
+                    if (f.type[t] == LEAF && has_ghost_child) {
+                        for (int a = 0; a < 3; a++) amg_c[a][id] = amg_c[a][id] + offs[a];
+                        amg_c[3][id] = amg_c[3][id] + diag_sum;
+                    }
+                }
+            }
+        }
+    }
+    // AMGLaplacianTileData::negativeLapSameLevel (src/AMGSolver.cu:231-250): x0 * diag plus, per
+    // face in (axis, -/+) order, the off-diagonal coefficient stored at the face's upper cell
+    // times the neighbour's x (0 across an absent tile); products fused into the sum.
+    T amg_lap(const T* x, int t, int i, int j, int k) const {
+        const size_t id = (size_t)t * NCELL + loff(i, j, k);
+        T sum = x[id] * amg_c[3][id];
+        for (int axis = 0; axis < 3; axis++)
+            for (int sgn = -1; sgn <= 1; sgn += 2) {
+                int no;
+                const int nb = amg_nb(t, i, j, k, axis, sgn, no);
+                const T xn = nb >= 0 ? x[(size_t)nb * NCELL + no] : (T)0;
+                T off;
+                if (sgn < 0) off = amg_c[axis][id];
+                else off = nb >= 0 ? amg_c[axis][(size_t)nb * NCELL + no] : (T)0;
+                sum = fmaT<T>(off, xn, sum);
+            }
+        return sum;
+    }
+    // NegativeLaplacianAndGaussSeidelSameLevel128Kernel (src/AMGSolver.cu:540-578) on the
+    // LEAF|NONLEAF tiles of `level`, cells of one colour
+    void amg_gs_sweep(int level, int xc, int rc, int color) {
+        T* x = C(xc);
+        const T* r = C(rc);
+        const auto& tl = f.by_level[level];
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < (int)tl.size(); q++) {
+            const int t = tl[q];
+            if (!(f.type[t] & (LEAF | NONLEAF))) continue;
+            for (int o = 0; o < NCELL; o++) {
+                const int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                if ((i + j + k) % 2 != color) continue;
+                const size_t id = (size_t)t * NCELL + o;
+                const T Ax = amg_lap(x, t, i, j, k);
+                const T dx = (amg_ct[id] & INTERIOR) ? (r[id] - Ax) / amg_c[3][id] : (T)0;
+                x[id] = x[id] + dx;
+            }
+        }
+    }
+    void amg_gauss_seidel(int iters, int order, int level, int xc, int rc) {  // src/AMGSolver.cu:598-606
+        for (int it = 0; it < iters; it++) {
+            amg_gs_sweep(level, xc, rc, order);
+            amg_gs_sweep(level, xc, rc, 1 - order);
+        }
+    }
+    // the downstroke's residual and restriction to level - 1 (src/AMGSolver.cu:640-656):
+    // tmp = rhs - A x on INTERIOR cells of the level's tiles (0 elsewhere); NONLEAF tiles of the
+    // coarser level: Restrict (src/PoissonSolver.cu:292-319); its LEAF tiles: f plus their GHOST
+    // children's residuals (Copy + AccumulateToParents, src/PoissonGrid.cu:721-755); its GHOST
+    // tiles: 0 (Fill)
+    void amg_residual_restrict(int level, int xc, int fc, int tmpc, int rhsc, T one_over_alpha) {
+        const T* x = C(xc);
+        const T* fv = C(fc);
+        T* tmp = C(tmpc);
+        T* rhs = C(rhsc);
+        const auto& tl = f.by_level[level];
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < (int)tl.size(); q++) {
+            const int t = tl[q];
+            for (int o = 0; o < NCELL; o++) {
+                const size_t id = (size_t)t * NCELL + o;
+                tmp[id] = amg_ct[id] == INTERIOR ? rhs[id] - amg_lap(x, t, o >> 6, (o >> 3) & 7, o & 7) : (T)0;
+            }
+        }
+        const auto& cl = f.by_level[level - 1];
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < (int)cl.size(); q++) {
+            const int t = cl[q];
+            const uint8_t tt = f.type[t];
+            const bool has_child0 = f.find(level, f.cx[t] * 2, f.cy[t] * 2, f.cz[t] * 2) >= 0;
+            for (int o = 0; o < NCELL; o++) {
+                const int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                const int gx = f.cx[t] * 8 + i, gy = f.cy[t] * 8 + j, gz = f.cz[t] * 8 + k;
+                const size_t id = (size_t)t * NCELL + o;
+                const uint8_t ct = amg_ct[id];
+                auto child_sum = [&](uint8_t child_types) {
+                    T sum = 0;
+                    for (int s = 0; s < 8; s++) {  // childIndexToOffset: x fastest
+                        int co;
+                        const int c = f.find_voxel(level, gx * 2 + (s & 1), gy * 2 + ((s >> 1) & 1), gz * 2 + ((s >> 2) & 1), co);
+                        if (c < 0) continue;
+                        const size_t cid = (size_t)c * NCELL + co;
+                        if (amg_ct[cid] & child_types) sum = sum + tmp[cid];
+                    }
+                    return sum;
+                };
+                if (tt == NONLEAF) {
+                    if (!(ct & INTERIOR)) rhs[id] = 0;
+                    if (!has_child0) continue;
+                    rhs[id] = child_sum(INTERIOR) * one_over_alpha;
+                } else if (tt == LEAF) {
+                    if (!(ct & (INTERIOR | DIRICHLET | NEUMANN))) continue;
+                    rhs[id] = fv[id];
+                    rhs[id] = fmaT<T>(child_sum(INTERIOR | DIRICHLET | NEUMANN), (T)1, rhs[id]);
+                } else if (tt == GHOST) {
+                    if (ct & (INTERIOR | DIRICHLET | NEUMANN)) rhs[id] = 0;
+                }
+            }
+        }
+    }
+    // ProlongateAndUpdate128 (src/GMGSolver.cu:345-380) with the AMG's cell types
+    void amg_prolongate(int level, int cxc, int fxc, T prolong_coeff) {
+        const auto& tl = f.by_level[level];
+        T* fx = C(fxc);
+        const T* cxv = C(cxc);
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < (int)tl.size(); q++) {
+            const int t = tl[q];
+            for (int o = 0; o < NCELL; o++) {
+                const int i = o >> 6, j = (o >> 3) & 7, k = o & 7;
+                int po;
+                const int p = f.find_voxel(level - 1, (f.cx[t] * 8 + i) >> 1, (f.cy[t] * 8 + j) >> 1, (f.cz[t] * 8 + k) >> 1, po);
+                const T c = (p < 0) ? (T)0 : cxv[(size_t)p * NCELL + po];
+                const size_t id = (size_t)t * NCELL + o;
+                const bool interior = amg_ct[id] & INTERIOR;
+                if (f.type[t] & GHOST) fx[id] = interior ? c : (T)0;
+                else fx[id] = interior ? fmaT<T>(prolong_coeff, c, fx[id]) : (T)0;
+            }
+        }
+    }
+    // VCycleAMG (src/AMGSolver.cu:610-715)
+    void amg_vcycle(int xc, int fc, int tmpc, int rhsc, int level_iters, int coarsest_iters, T one_over_alpha, T prolong_coeff) {
+        T* x = C(xc); T* rhs = C(rhsc); const T* fv = C(fc);
+#pragma omp parallel for schedule(static)
+        for (int t = 0; t < f.n; t++) {
+            for (int o = 0; o < NCELL; o++) {
+                const size_t id = (size_t)t * NCELL + o;
+                x[id] = 0;
+                rhs[id] = (f.type[t] & GHOST) ? (T)0 : fv[id];
+            }
+        }
+        for (int l = f.max_level; l > 0; l--) {
+            amg_gauss_seidel(level_iters, 0, l, xc, rhsc);
+            amg_residual_restrict(l, xc, fc, tmpc, rhsc, one_over_alpha);
+        }
+        amg_gauss_seidel(coarsest_iters / 2, 0, 0, xc, rhsc);
+        amg_gauss_seidel(coarsest_iters / 2, 1, 0, xc, rhsc);
+        for (int l = 1; l <= f.max_level; l++) {
+            amg_prolongate(l, xc, xc, prolong_coeff);
+            amg_gauss_seidel(level_iters, 1, l, xc, rhsc);
+        }
+    }
+    // AMGSolver::solve (src/AMGSolver.cu:722-853): GMGSolver::solve's PCG with VCycleAMG(z, r,
+    // tmp = Ap, rhs = scratch) as the preconditioner
+    int amg_solve(int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, bool pure_neumann,
+                  T one_over_alpha, T prolong_coeff, double& rel) {
+        T* x = C(0); T* r = C(1); T* p = C(2); T* Ap = C(3); T* z = C(4);
+        leaf_cells([&](size_t id) { x[id] = 0; });
+        double rhs2 = 0, thr2 = 0;
+        if (sync_stride > 0) {
+            rhs2 = dot(1, 1);
+            if (rhs2 == 0.0) { rel = 0; return 0; }
+            thr2 = std::max(tol * tol * rhs2, DBL_MIN);
+        }
+        if (pure_neumann) recenter(1);
+        amg_vcycle(4, 1, 3, 5, level_iters, coarsest_iters, one_over_alpha, prolong_coeff);
+        leaf_cells([&](size_t id) { p[id] = z[id]; });
+        double gamma = dot(4, 1);
+        int i = 0;
+        for (i = 0; i < max_iters; i++) {
+            full_lap(2, 3);
+            double fp = dot(2, 3);
+            double alpha = gamma / fp;
+            T a = (T)alpha;
+            leaf_cells([&](size_t id) { if (f.ctype[id] & INTERIOR) x[id] = fmaT<T>(a, p[id], x[id]); });
+            leaf_cells([&](size_t id) { if (f.ctype[id] & INTERIOR) r[id] = fmaT<T>(-a, Ap[id], r[id]); });
+            if (sync_stride > 0 && (i + 1) % sync_stride == 0) {
+                double res2 = dot(1, 1);
+                if (res2 < thr2) { rel = std::sqrt(res2 / rhs2); return i + 1; }
+            }
+            if (pure_neumann) recenter(1);
+            amg_vcycle(4, 1, 3, 5, level_iters, coarsest_iters, one_over_alpha, prolong_coeff);
+            double gamma_old = gamma;
+            gamma = dot(1, 4);
+            double beta = gamma / gamma_old;
+            T bb = (T)beta;
+            leaf_cells([&](size_t id) { if (f.ctype[id] & INTERIOR) p[id] = fmaT<T>(bb, p[id], z[id]); });
+        }
+        if (sync_stride > 0) { rel = std::sqrt(dot(1, 1) / rhs2); return i; }
+        rel = -1;
+        return i;
+    }
 };
 
 // ---------------------------------------------------------------- RHS construction
@@ -1106,6 +1415,37 @@ int ocx_solve(void* h, int prec, int max_iters, double tol, int level_iters, int
 int ocx_damped_jacobi(void* h, int prec, int max_iters, double tol, double omega, double* rel) {
     OCX* o = (OCX*)h;
     return prec == 0 ? S32(o).damped_jacobi(max_iters, tol, (float)omega, *rel) : S64(o).damped_jacobi(max_iters, tol, omega, *rel);
+}
+// AMG variant (src/AMGSolver.cu): coefficients and cell types, one V-cycle, the PCG solve
+void ocx_amg_prepare(void* h, int prec, double one_over_alpha) {
+    OCX* o = (OCX*)h;
+    if (prec == 0) S32(o).amg_prepare((float)one_over_alpha); else S64(o).amg_prepare(one_over_alpha);
+}
+// coefficient k (0..2 off-diagonal x/y/z, 3 diagonal) of every cell; the AMG cell types
+void ocx_amg_coeffs(void* h, int prec, int k, double* out) {
+    OCX* o = (OCX*)h;
+    size_t n = (size_t)o->f.n * NCELL;
+    if (prec == 0) { auto& s = S32(o); for (size_t i = 0; i < n; i++) out[i] = s.amg_c[k][i]; }
+    else { auto& s = S64(o); for (size_t i = 0; i < n; i++) out[i] = s.amg_c[k][i]; }
+}
+void ocx_amg_types(void* h, int prec, uint8_t* out) {
+    OCX* o = (OCX*)h;
+    const auto& v = prec == 0 ? S32(o).amg_ct : S64(o).amg_ct;
+    std::memcpy(out, v.data(), v.size());
+}
+void ocx_amg_vcycle(void* h, int prec, int xc, int fc, int tmpc, int rhsc, int level_iters, int coarsest_iters, double one_over_alpha,
+                    double prolong_coeff) {
+    OCX* o = (OCX*)h;
+    if (prec == 0) S32(o).amg_vcycle(xc, fc, tmpc, rhsc, level_iters, coarsest_iters, (float)one_over_alpha, (float)prolong_coeff);
+    else S64(o).amg_vcycle(xc, fc, tmpc, rhsc, level_iters, coarsest_iters, one_over_alpha, prolong_coeff);
+}
+int ocx_amg_solve(void* h, int prec, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann,
+                  double one_over_alpha, double prolong_coeff, double* rel) {
+    OCX* o = (OCX*)h;
+    return prec == 0 ? S32(o).amg_solve(max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0, (float)one_over_alpha,
+                                         (float)prolong_coeff, *rel)
+                     : S64(o).amg_solve(max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0, one_over_alpha,
+                                        prolong_coeff, *rel);
 }
 int ocx_num_threads() { return omp_get_max_threads(); }
 void ocx_set_threads(int n) { omp_set_num_threads(n); }

@@ -118,6 +118,12 @@ def oracle_lib():
             "ocx_solve": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p, f64p,
                                     C.c_int, C.POINTER(C.c_int)]),
             "ocx_damped_jacobi": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_double, f64p]),
+            "ocx_amg_prepare": (None, [P, C.c_int, C.c_double]),
+            "ocx_amg_coeffs": (None, [P, C.c_int, C.c_int, f64p]),
+            "ocx_amg_types": (None, [P, C.c_int, u8p]),
+            "ocx_amg_vcycle": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]),
+            "ocx_amg_solve": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                        f64p]),
             "ocx_num_threads": (C.c_int, []),
             "ocx_set_threads": (None, [C.c_int]),
         }
@@ -279,6 +285,34 @@ class CpuOracle:
         """GMGSolver::dampedJacobiSolve restated: b in channel 1; returns (iterations, relative residual)."""
         rel = C.c_double()
         it = oracle_lib().ocx_damped_jacobi(self.h, prec, max_iters, tol, omega, C.byref(rel))
+        return it, rel.value
+
+
+    # AMG variant (src/AMGSolver.cu), parity unpinned: the reference's AMG file does not build here
+    def amg_prepare(self, prec, one_over_alpha=1.0):
+        oracle_lib().ocx_amg_prepare(self.h, prec, one_over_alpha)
+
+    def amg_coefficients(self, prec):
+        """(4, n, 512): off-diagonal coefficients of the x-, y-, z- faces and the diagonal."""
+        out = np.empty((4, self.n, 512), dtype=np.float64)
+        for k in range(4):
+            oracle_lib().ocx_amg_coeffs(self.h, prec, k, _p(out[k], C.c_double))
+        return out
+
+    def amg_types(self, prec):
+        out = np.empty((self.n, 512), dtype=np.uint8)
+        oracle_lib().ocx_amg_types(self.h, prec, _p(out, C.c_uint8))
+        return out
+
+    def amg_vcycle(self, prec, xc=4, fc=1, tmpc=3, rhsc=5, level_iters=1, coarsest_iters=10, one_over_alpha=1.0, prolong_coeff=1.0):
+        oracle_lib().ocx_amg_vcycle(self.h, prec, xc, fc, tmpc, rhsc, level_iters, coarsest_iters, one_over_alpha, prolong_coeff)
+
+    def amg_solve(self, prec, max_iters=1000, tol=1e-6, level_iters=1, coarsest_iters=10, sync_stride=1, pure_neumann=False,
+                  one_over_alpha=1.0, prolong_coeff=1.0):
+        """AMGSolver::solve restated (after amg_prepare): b in channel 1, x to channel 0."""
+        rel = C.c_double()
+        it = oracle_lib().ocx_amg_solve(self.h, prec, max_iters, tol, level_iters, coarsest_iters, sync_stride, int(pure_neumann),
+                                        one_over_alpha, prolong_coeff, C.byref(rel))
         return it, rel.value
 
 

@@ -1,0 +1,130 @@
+"""The AMG variant on the GPU (AMGSolver, src/AMGSolver.cu) against the CPU restatement's FP32
+mirror, bit for bit: the prepared coefficients and cell types, one V-cycle, and the whole
+AMG-preconditioned CG (iterations and pressure); a batch against its instances solved alone; the
+state error before preparation; FP64 defect correction to 1e-8.  Parity with the reference itself
+is unpinned (its AMG file does not build in this environment)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cirrus_b200 import AMGSolver, CirrusError, DeviceGrid, PRECISION_MIXED_FP64, workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FP32 = O.CpuOracle.FP32
+NAMES = ["uniform32_small", "sphere64_small", "ring64_small", "uniform128", "ring512"]
+
+
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+def setup(b):
+    g = DeviceGrid(b.topology)
+    for a in range(3):
+        g.set_channel(6 + a, b.velocity[a])
+    g.projection_rhs()
+    f = O.CpuOracle(b.tiles)
+    f.set_ctypes(b.ctypes)
+    return g, f
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_amg_coefficients_bitwise(name, built_cache):
+    b = built_cache(name)
+    g, f = setup(b)
+    s = AMGSolver()
+    s.prepare_types_and_coeffs(g)
+    co, ty = s.coefficients(g)
+    f.amg_prepare(FP32)
+    assert np.array_equal(ty, f.amg_types(FP32))
+    ref = f.amg_coefficients(FP32).astype(np.float32)
+    for k in range(4):
+        assert np.array_equal(bits(co[k]), bits(ref[k])), k
+    g.close()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_amg_vcycle_bitwise(name, built_cache):
+    b = built_cache(name)
+    g, f = setup(b)
+    rhs = g.get_channel(1)
+    s = AMGSolver()
+    s.prepare_types_and_coeffs(g)
+    s.vcycle(g, 4, 1, 3, 5, 1, 10)
+    f.set_channel_f32(1, rhs)
+    f.amg_prepare(FP32)
+    f.amg_vcycle(FP32, 4, 1, 3, 5, 1, 10)
+    assert np.array_equal(bits(g.get_channel(4)), bits(f.get_channel_f32(4)))
+    assert np.array_equal(bits(g.get_channel(5)), bits(f.get_channel_f32(5)))
+    g.close()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_amg_solve_bitwise(name, built_cache):
+    b = built_cache(name)
+    g, f = setup(b)
+    rhs = g.get_channel(1)
+    pn = b.workload.pure_neumann
+    s = AMGSolver()
+    s.prepare_types_and_coeffs(g)
+    it, rel = s.solve(g, is_pure_neumann=pn)
+    f.set_channel_f32(1, rhs)
+    f.amg_prepare(FP32)
+    it_o, rel_o = f.amg_solve(FP32, pure_neumann=pn)
+    print(f"{name}: AMG-PCG {it} iterations, rel {rel:.3e}")
+    assert it == it_o and rel < 1e-6
+    assert abs(rel - rel_o) <= 1e-12 * rel_o
+    leaf = (b.tiles[:, 4] & W.LEAF) != 0
+    assert np.array_equal(bits(g.get_channel(0))[leaf], bits(f.get_channel_f32(0))[leaf])
+    g.close()
+
+
+def test_amg_batch_matches_instances_alone(built_cache):
+    bs = [built_cache(n) for n in ["sphere64_small", "ring64_small", "uniform32_small"]]
+    rhs = []
+    for b in bs:
+        g, _ = setup(b)
+        rhs.append(g.get_channel(1))
+        g.close()
+    s = AMGSolver()
+    alone = []
+    for b, r in zip(bs, rhs):
+        g = DeviceGrid(b.topology)
+        g.set_channel(1, r)
+        s.prepare_types_and_coeffs(g)
+        alone.append((s.solve(g, is_pure_neumann=b.workload.pure_neumann), g.get_channel(0)))
+        g.close()
+    g = DeviceGrid([b.topology for b in bs])
+    for i, r in enumerate(rhs):
+        g.set_channel_instance(i, 1, r)
+    s.prepare_types_and_coeffs(g)
+    res = s.solve_batch(g, pure_neumann=[b.workload.pure_neumann for b in bs])
+    for i, ((it_rel, x), r) in enumerate(zip(alone, res)):
+        assert r[0] == it_rel[0]
+        assert np.array_equal(bits(g.get_channel_instance(i, 0)), bits(x))
+    g.close()
+
+
+def test_amg_needs_prepare(built_cache):
+    b = built_cache("sphere64_small")
+    g, _ = setup(b)
+    with pytest.raises(CirrusError):
+        AMGSolver().solve(g)
+    with pytest.raises(CirrusError):
+        AMGSolver().vcycle(g)
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["sphere64_small", "ring512"])
+def test_amg_mixed_precision_reaches_1e8(name, built_cache):
+    b = built_cache(name)
+    g, _ = setup(b)
+    s = AMGSolver(precision=PRECISION_MIXED_FP64)
+    s.prepare_types_and_coeffs(g)
+    it, rel = s.solve(g, relative_tolerance=1e-8, is_pure_neumann=b.workload.pure_neumann)
+    print(f"{name}: mixed AMG {it} iterations, {s.last_result.outer_iters} outer, FP64 true residual {rel:.2e}")
+    assert s.last_result.status == 0 and rel < 1e-8
+    g.close()
