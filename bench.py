@@ -369,7 +369,7 @@ def run_ours(args, world, rank, local, pg):
     import torch
 
     from cirrus_b200 import (B_CHANNEL, KERNEL_GS_SWEEP, KERNEL_LAPLACIAN, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP,
-                             KERNEL_RESIDUAL_RESTRICT, TMP_CHANNEL, DeviceGrid, GMGSolver)
+                             KERNEL_RESIDUAL_RESTRICT, TMP_CHANNEL, U_CHANNEL, DeviceGrid, GMGSolver)
 
     K = args.batch
     b, g = build_batch(args.workload, batch_seeds(rank, K))
@@ -563,6 +563,38 @@ def run_ours(args, world, rank, local, pg):
     if max(r.true_rel_residual for r in tres) >= 1e-6:
         raise RuntimeError("sweep-tuned mixed-precision solve did not reach 1e-6")
 
+    # the AMG variant (AMGSolver: explicit coefficients, coarse levels from the children) on the
+    # same batch, FP32 to the same 1e-6
+    from cirrus_b200 import AMGSolver
+
+    asolver = AMGSolver()
+    # its V-cycle uses channel 5 (which holds b between steps here) as scratch: b waits in channel 6
+    g.copy_channel(U_CHANNEL, TMP_CHANNEL, sh)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    asolver.prepare_types_and_coeffs(g, stream=sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    amg_prepare_ms = e0.elapsed_time(e1)
+    atimes, ares = [], []
+    for i in range(args.warmup + args.steps):
+        g.copy_channel(B_CHANNEL, U_CHANNEL, sh)
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        asolver.solve_batch(g, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            atimes.append(e0.elapsed_time(e1))
+            ares = list(asolver.last_results)
+    amg_total = barrier_max(pg, sum(atimes))
+    g.copy_channel(TMP_CHANNEL, U_CHANNEL, sh)
+    if not all(r.status == 0 for r in ares):
+        raise RuntimeError("AMG solve did not converge")
+
     # one instance alone (batch of one): latency
     b1, g1 = build_batch(args.workload, [rank * K])
     g1.autotune()
@@ -613,6 +645,10 @@ def run_ours(args, world, rank, local, pg):
                                             "sweeps": {"level_iters": tli, "coarsest_iters": tci, "source": "sweep tuner"},
                                             "pcg_iters_per_solve": int(statistics.median(r.iters for r in tres)),
                                             "max_true_rel_residual": float(max(r.true_rel_residual for r in tres))}},
+        "amg_variant": {"value": round(args.steps * world * K / (amg_total * 1e-3), 3), "unit": "solves/s",
+                        "solver": "AMGSolver (explicit face coefficients, coarse levels from the children), FP32 to 1e-6",
+                        "pcg_iters_per_solve": int(statistics.median(r.iters for r in ares)),
+                        "prepare_ms": round(amg_prepare_ms, 3)},
         "gpu_launches": int(sum(launches)),
         "e2e": {"value": round(n / (e2e_total * 1e-3), 3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(rhs.nbytes), "d2h_bytes_per_step": int(rhs.nbytes),

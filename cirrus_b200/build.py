@@ -23,7 +23,7 @@ INCLUDE = PKG.parent / "include"
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", *GENCODE, "-Xcompiler", "-fPIC,-fopenmp,-O3",
               "-I", str(CSRC), "-I", str(INCLUDE)]
-SOURCES = ["topology.cpp", "grid.cu", "kernels.cu", "lap_tma.cu", "lap8.cu", "gs8.cu", "amg.cu", "vcycle_fused.cu", "rhs.cu", "interop.cu", "solver.cu", "capi.cu", "noalloc.cu", "autotune.cu", "serve.cpp", "holder.cpp", "dtopo.cu"]
+SOURCES = ["topology.cpp", "grid.cu", "kernels.cu", "lap_tma.cu", "lap8.cu", "amg.cu", "vcycle_fused.cu", "rhs.cu", "interop.cu", "solver.cu", "capi.cu", "noalloc.cu", "autotune.cu", "serve.cpp", "holder.cpp", "dtopo.cu"]
 
 
 def nvcc() -> str:

@@ -1303,12 +1303,7 @@ void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, 
     const int n = g.mg_count[level];
     if (n == 0) return;
     ++g.launch_count;
-    const int shape = g.shape(KS_GS_SWEEP, level);
-    if (shape >= kNumShapes) {  // 8..11: eight cells per thread
-        gs_sweep8(g, shape - kNumShapes, level, X, R, color, S, s, RD);
-        return;
-    }
-    switch (shape) {
+    switch (g.shape(KS_GS_SWEEP, level)) {
     case 0: gs_sweep_shape<2, 1>(g, level, X, R, color, S, s, RD); break;
     case 1: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s, RD); break;
     case 2: gs_sweep_shape<1, 4>(g, level, X, R, color, S, s, RD); break;

@@ -62,9 +62,7 @@ constexpr int kNumShapes = 8;
 // stages) = (2, 8), (4, 16), (2, 12), (1, 6); 12..15 eight cells per thread (lap8.cu)
 constexpr int kNumLapShapes = 16;
 constexpr int kFirstLap8Shape = 12;
-// the colour sweep has four more: 8..11 eight cells per thread (gs8.cu)
-constexpr int kNumGsShapes = 12;
-inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kind == KS_GS_SWEEP ? kNumGsShapes : kNumShapes; }
+inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kNumShapes; }
 
 // A contiguous run of one instance's tiles inside the merged pool: tiles local..local+count of
 // the instance's all-tiles order are global..global+count (one run per level).
@@ -249,10 +247,6 @@ bool laplacian_tma(const DevGrid& g, int variant, const float* X, float* Y, cons
 // CTA, tiles in flight per group) (2, 2), (4, 1), (1, 4), (2, 2) with at least 7 CTAs per SM.
 // WP: as laplacian_fused's.
 void laplacian8(const DevGrid& g, int variant, const float* X, float* Y, const Scalars* S, cudaStream_t s, double* WP);
-// gs_sweep with a column of eight cells per thread (gs8.cu); variant 0..3 = (tile groups per CTA,
-// tiles in flight per group) (2, 2), (4, 1), (1, 4), (2, 1)
-void gs_sweep8(const DevGrid& g, int variant, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s,
-               const float* RD);
 // Ap += GHOST children's sums on the LEAF tiles that have them, and their p.Ap tile parts
 void pap_ghost(const DevGrid& g, const float* P, float* AP, cudaStream_t s);
 // RD: with the PCG residual r, also store the r.z tile parts of the level's LEAF tiles (d_wpart)

@@ -447,8 +447,7 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
  * level 0), shape in [0, 8) for every kernel; the Laplacian also takes 8..11, its TMA-staged
  * pipeline (persistent CTAs, one producer warp issuing bulk tensor copies of each tile and its
  * halos into a ring of shared-memory stages, 1-4 consumer groups), and 12..15, a column of eight
- * cells per thread (64 threads per tile); the Gauss-Seidel colour sweep also takes 8..11, eight
- * cells per thread.  Lets a caller reuse tuned
+ * cells per thread (64 threads per tile).  Lets a caller reuse tuned
  * shapes for grids of the same structure or pin one.  Shapes never change results.  No
  * counterpart in the reference. */
 #define CIRRUS_NUM_LAUNCH_SHAPES 16
