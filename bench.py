@@ -365,6 +365,58 @@ def cpu_baseline(b, rhs, budget_s: float = 10.0, max_solves: int = 5) -> dict:
     return {"seconds": dt, "threads": O.num_threads(), "solves": solves, "iters": its}
 
 
+# PoissonTile<float> as the reference's grid holds it in device memory: 33,104-byte records,
+# channel c at float offset 736 c, the 512 cell-type bytes at byte 32,576 (the layout the
+# tile-holder files use too)
+TILE_RECORD_BYTES, TILE_CHANNEL_STRIDE, TILE_CELLTYPE_OFFSET = 33104, 736, 32576
+
+
+def dropin_call_site(args, g1, ctypes_host, sh) -> dict:
+    """The drop-in's work at FluidEuler::project's call site (src/FluidEuler.h:591-601), one
+    instance: the reference keeps its tiles as separate device records, and a fresh solver object
+    per projection compares their cell types with the bound pool's on the device, gathers b from
+    the records, solves, and scatters x and the residual back (the C ABI calls
+    include/cirrus_gmg_dropin.hpp makes after its first bind), timed with the host clock around the
+    whole call as FluidEuler::project times the solve."""
+    import ctypes as C
+    import torch
+
+    from cirrus_b200 import B_CHANNEL, GMGSolver, lib
+
+    n = g1.num_tiles
+    rec = torch.zeros(n * TILE_RECORD_BYTES, dtype=torch.uint8, device="cuda")
+    f32 = rec.view(torch.float32).view(n, TILE_RECORD_BYTES // 4)
+    b = torch.from_numpy(g1.get_channel(B_CHANNEL)).cuda()
+    f32[:, TILE_CHANNEL_STRIDE:TILE_CHANNEL_STRIDE + 512] = b
+    ct = torch.from_numpy(np.ascontiguousarray(ctypes_host, dtype=np.uint8).reshape(n, 512)).cuda()
+    rec.view(n, TILE_RECORD_BYTES)[:, TILE_CELLTYPE_OFFSET:TILE_CELLTYPE_OFFSET + 512] = ct
+    base = rec.data_ptr()
+    ptrs = (C.c_void_p * n)(*[base + i * TILE_RECORD_BYTES for i in range(n)])
+    L = lib()
+    assert L.cirrus_grid_set_tile_pointers(g1.handle, ptrs) == 0
+    solver = GMGSolver()
+    changed = C.c_int()
+    times = []
+    torch.cuda.synchronize()
+    for i in range(args.warmup + args.steps):
+        f32[:, TILE_CHANNEL_STRIDE:TILE_CHANNEL_STRIDE + 512] = b  # the reference's next right-hand side
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        assert L.cirrus_grid_compare_tile_cell_types(g1.handle, TILE_CELLTYPE_OFFSET, C.c_void_p(sh), C.byref(changed), None) == 0
+        assert L.cirrus_grid_gather_tiles(g1.handle, 1, TILE_CHANNEL_STRIDE * 4, C.c_void_p(sh)) == 0
+        solver.solve(g1, stream=sh)
+        assert L.cirrus_grid_scatter_tiles(g1.handle, 0, 0, C.c_void_p(sh)) == 0
+        assert L.cirrus_grid_scatter_tiles(g1.handle, 1, TILE_CHANNEL_STRIDE * 4, C.c_void_p(sh)) == 0
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            times.append((time.perf_counter() - t0) * 1e3)
+        assert changed.value == 0
+    return {"value": round(1e3 / float(np.mean(times)), 3), "unit": "solves/s", "p50_ms": round(float(np.percentile(times, 50)), 4),
+            "api": "cirrus_grid_compare_tile_cell_types + cirrus_grid_gather_tiles + cirrus_gmg_solve + cirrus_grid_scatter_tiles x2 "
+                   "on tiles held as separate PoissonTile<float> device records (one instance, host clock around the call)",
+            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4}
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
 
@@ -611,6 +663,7 @@ def run_ours(args, world, rank, local, pg):
         torch.cuda.synchronize()
         if i >= args.warmup:
             lat.append(e0.elapsed_time(e1))
+    dropin = dropin_call_site(args, g1, b1.ctypes, sh)
 
     n = args.steps * world * K
     value = n / (total_ms * 1e-3)
@@ -635,6 +688,7 @@ def run_ours(args, world, rank, local, pg):
         "latency_ms": {"single_p50": round(float(np.percentile(lat, 50)), 4), "single_p99": round(float(np.percentile(lat, 99)), 4),
                        "batch_p50": round(float(np.percentile(times, 50)), 4), "batch_p99": round(float(np.percentile(times, 99)), 4)},
         "single_solves_per_s": round(1e3 / float(np.mean(lat)), 3),
+        "dropin_e2e": dropin,
         "mixed_precision": {"value": round(args.steps * world * K / (mixed_total * 1e-3), 3), "unit": "solves/s",
                             "precision": "FP32 V-cycle + matvec, FP64 residual and defect correction",
                             "tolerance": "1e-6 FP64 true relative residual per instance",

@@ -78,6 +78,8 @@ struct Topo {
     const int* leafslot;         // n: position s of a LEAF tile in the LEAF list, stored as s for a
                                  // tile without GHOST children and as -2 - s for one with them; -1
                                  // for every other tile
+    int pf;                      // per launch: the staged kernels also prefetch into L2 the tiles pf
+                                 // list entries ahead of their own (0: no prefetching)
 };
 constexpr int kLevelSlots = 16;
 

@@ -3,6 +3,7 @@
 #include "kernels.cuh"
 #include "solver_internal.hpp"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -120,6 +121,8 @@ __global__ void __launch_bounds__(128 * TPB) k_laplacian_same_level(Topo tp, int
 // With WP the launch also stores, for every LEAF tile without GHOST children (whose A p is final
 // here), the tile's part of p.Ap (tile_part_sum of the threads' 4-cell FP32 products) at
 // WP[LEAF slot]; k_pap_ghost forms those of the other LEAF tiles.
+// tp.pf > 0: thread 0 of each group also prefetches into L2 the values and mask bytes of the
+// tiles pf list entries ahead (the tiles a CTA about one resident wave later stages).
 template <int TPB, int NT>
 __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
                                                                int nitems, int item_blocks,
@@ -140,13 +143,14 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
     extern __shared__ __align__(16) unsigned char lap_smem[];
     TileStage* st = reinterpret_cast<TileStage*>(lap_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-    int tile[NT];
+    int tile[NT], ptile[NT];
     bool act[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         const int q = (((int)blockIdx.x - item_blocks) * NT + u) * TPB + g;
         tile[u] = q < n ? list[q] : 0;
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
+        ptile[u] = (tp.pf > 0 && t == 0 && q + tp.pf < n) ? list[q + tp.pf] : -1;
     }
     TilePre pre[NT];
     tile_pre(tp, tile, t, pre);
@@ -155,6 +159,12 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
         if (act[u]) {
             stage_async(X, nullptr, tp.mask_lap, tile[u], pre[u].nb, t, st[u * TPB + g]);
             if (WP != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
+        }
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (ptile[u] >= 0) {
+            prefetch_l2(X + (size_t)ptile[u] * kTileCells, kTileCells * sizeof(float));
+            prefetch_l2(tp.mask_lap + (size_t)ptile[u] * kTileCells, kTileCells);
         }
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
@@ -288,13 +298,14 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
     extern __shared__ __align__(16) unsigned char gs_smem[];
     TileStage* st = reinterpret_cast<TileStage*>(gs_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-    int tile[NT];
+    int tile[NT], ptile[NT];
     bool act[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         const int q = (blockIdx.x * NT + u) * TPB + g;
         tile[u] = q < n ? list[q] : 0;
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
+        ptile[u] = (tp.pf > 0 && t == 0 && q + tp.pf < n) ? list[q + tp.pf] : -1;
     }
     TilePre pre[NT];
     tile_pre(tp, tile, t, pre);
@@ -303,6 +314,13 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
         if (act[u]) {
             stage_async(X, R, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
             if (RD != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
+        }
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (ptile[u] >= 0) {
+            prefetch_l2(X + (size_t)ptile[u] * kTileCells, kTileCells * sizeof(float));
+            prefetch_l2(R + (size_t)ptile[u] * kTileCells, kTileCells * sizeof(float));
+            prefetch_l2(tp.mask_mg + (size_t)ptile[u] * kTileCells, kTileCells);
         }
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
@@ -485,7 +503,7 @@ __device__ __forceinline__ void k_residual_restrict_body(Topo tp, int first, con
     extern __shared__ __align__(16) unsigned char rr_smem[];
     TileStage* st = reinterpret_cast<TileStage*>(rr_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
-    int tile[NT];
+    int tile[NT], ptile[NT];
     bool act[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
@@ -493,12 +511,20 @@ __device__ __forceinline__ void k_residual_restrict_body(Topo tp, int first, con
         const int qq = q < n ? q : 0;
         tile[u] = list ? list[qq] : first + qq;
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
+        ptile[u] = (tp.pf > 0 && t == 0 && q + tp.pf < n) ? (list ? list[q + tp.pf] : first + q + tp.pf) : -1;
     }
     TilePre pre[NT];
     tile_pre(tp, tile, t, pre);
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (act[u]) stage_async(X, RHS, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (ptile[u] >= 0) {
+            prefetch_l2(X + (size_t)ptile[u] * kTileCells, kTileCells * sizeof(float));
+            prefetch_l2(RHS + (size_t)ptile[u] * kTileCells, kTileCells * sizeof(float));
+            prefetch_l2(tp.mask_mg + (size_t)ptile[u] * kTileCells, kTileCells);
+        }
 #pragma unroll
     for (int u = 0; u < NT; u++) act[u] = act[u] && !tile_done(tp, S, tile[u]);
     cp_async_wait_all();
@@ -1249,12 +1275,16 @@ template void propagate_ghosts<float>(const DevGrid&, float*, const Scalars*, cu
 template void full_laplacian<float>(const DevGrid&, float*, float*, const Scalars*, cudaStream_t);
 template void full_laplacian<double>(const DevGrid&, double*, double*, const Scalars*, cudaStream_t);
 
+// prefetch: stage the tiles of a CTA about one resident wave later into L2 (pf > 0, see
+// k_laplacian_fused_body): pf = the list entries the CTAs resident at once cover.
 template <int TPB, int NT, int MINB = 0>
-void laplacian_shape(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s, double* WP) {
+void laplacian_shape(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s, double* WP, bool prefetch = false) {
     const int per = TPB * NT;
     const int item_blocks = (g.n_lapitems + 128 * TPB - 1) / (128 * TPB);
-    launch_kernel(k_laplacian_fused_shape<TPB, NT, MINB>(), item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
-                  g.topo, g.d_lapmain, g.n_lapmain, g.d_lapitems, g.n_lapitems, item_blocks, X, Y, g.d_gacc, S, WP);
+    const auto k = k_laplacian_fused_shape<TPB, NT, MINB>();
+    launch_kernel(k, item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
+                  prefetch_topo(g, k, 128 * TPB, sizeof(TileStage) * per, per, prefetch), g.d_lapmain, g.n_lapmain, g.d_lapitems,
+                  g.n_lapitems, item_blocks, X, Y, g.d_gacc, S, WP);
 }
 
 void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* S, cudaStream_t s, bool with_pap) {
@@ -1263,12 +1293,12 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
     double* WP = with_pap ? g.d_wpart : nullptr;
     const int shape = g.shape(KS_LAPLACIAN, 0);
     // shapes 12..15: eight cells per thread
-    if (shape >= kFirstLap8Shape) {
+    if (shape >= kFirstLap8Shape && shape < kFirstLap8Shape + 4) {
         laplacian8(g, shape - kFirstLap8Shape, X, Y, S, s, WP);
         return;
     }
     // shapes 8..11: the TMA-staged pipeline (the cp.async shape 1 if X's tensor maps cannot be made)
-    if (shape >= kNumShapes && laplacian_tma(g, shape - kNumShapes, X, Y, S, s, with_pap)) return;
+    if (shape >= kFirstTmaShape && shape < kFirstLap8Shape && laplacian_tma(g, shape - kFirstTmaShape, X, Y, S, s, with_pap)) return;
     switch (shape) {
     case 0: laplacian_shape<2, 1>(g, X, Y, S, s, WP); break;
     case 1: laplacian_shape<2, 2>(g, X, Y, S, s, WP); break;
@@ -1277,7 +1307,13 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
     case 4: laplacian_shape<1, 1>(g, X, Y, S, s, WP); break;
     case 5: laplacian_shape<1, 2>(g, X, Y, S, s, WP); break;
     case 6: laplacian_shape<1, 1, 16>(g, X, Y, S, s, WP); break;
-    default: laplacian_shape<1, 1, 12>(g, X, Y, S, s, WP); break;
+    case 7: laplacian_shape<1, 1, 12>(g, X, Y, S, s, WP); break;
+    // 16..19: shapes 2, 3, 5, 1 with L2 prefetching one resident wave ahead
+    case 16: laplacian_shape<1, 4>(g, X, Y, S, s, WP, true); break;
+    case 17: laplacian_shape<2, 4>(g, X, Y, S, s, WP, true); break;
+    case 18: laplacian_shape<1, 2>(g, X, Y, S, s, WP, true); break;
+    case 19: laplacian_shape<2, 2>(g, X, Y, S, s, WP, true); break;
+    default: laplacian_shape<2, 2>(g, X, Y, S, s, WP); break;  // shape 1 (the TMA shapes without tensor maps)
     }
 }
 void pap_ghost(const DevGrid& g, const float* P, float* AP, cudaStream_t s) {
@@ -1291,11 +1327,13 @@ void pap_ghost(const DevGrid& g, const float* P, float* AP, cudaStream_t s) {
 // group in flight.
 template <int TPB, int NT, int MINB = 0>
 void gs_sweep_shape(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s,
-                    const float* RD) {
+                    const float* RD, bool prefetch = false) {
     const int n = g.mg_count[level];
     const int per = TPB * NT;
-    launch_kernel(k_gs_sweep_shape<TPB, NT, MINB>(), (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
-                  g.d_mg + g.mg_offset[level], n, X, R, color, S, RD, RD ? g.d_wpart : nullptr);
+    const auto k = k_gs_sweep_shape<TPB, NT, MINB>();
+    launch_kernel(k, (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
+                  prefetch_topo(g, k, 128 * TPB, sizeof(TileStage) * per, per, prefetch), g.d_mg + g.mg_offset[level], n, X, R, color,
+                  S, RD, RD ? g.d_wpart : nullptr);
 }
 
 void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, const Scalars* S, cudaStream_t s,
@@ -1311,7 +1349,12 @@ void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, 
     case 4: gs_sweep_shape<1, 1>(g, level, X, R, color, S, s, RD); break;
     case 5: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s, RD); break;
     case 6: gs_sweep_shape<1, 1, 16>(g, level, X, R, color, S, s, RD); break;
-    default: gs_sweep_shape<1, 1, 12>(g, level, X, R, color, S, s, RD); break;
+    case 7: gs_sweep_shape<1, 1, 12>(g, level, X, R, color, S, s, RD); break;
+    // 8..11: shapes 2, 5, 6, 1 prefetching later CTAs' tiles into L2
+    case 8: gs_sweep_shape<1, 4>(g, level, X, R, color, S, s, RD, true); break;
+    case 9: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s, RD, true); break;
+    case 10: gs_sweep_shape<1, 1, 16>(g, level, X, R, color, S, s, RD, true); break;
+    default: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s, RD, true); break;
     }
 }
 
@@ -1329,15 +1372,17 @@ void gs_sequence(const DevGrid& g, int level, float* X, const float* R, uint32_t
 
 template <int TPB, int NT, int MINB = 0>
 void residual_shape(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha, const Scalars* S,
-                    cudaStream_t s, bool ghosts_zero) {
+                    cudaStream_t s, bool ghosts_zero, bool prefetch = false) {
     const int per = TPB * NT;
     const int* list = ghosts_zero ? g.d_rrmain + g.rr_off[level] : nullptr;
     const int n = ghosts_zero ? g.rr_cnt[level] : g.level_count[level];
     const int nitems = ghosts_zero ? g.rri_cnt[level] : 0;
     const int4* items = ghosts_zero ? g.d_rritems + g.rri_off[level] : nullptr;
     const int item_blocks = (nitems + 128 * TPB - 1) / (128 * TPB);
-    launch_kernel(k_residual_restrict_shape<TPB, NT, MINB>(), item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s, g.topo,
-                  g.level_first[level], list, n, items, nitems, item_blocks, X, RHS, C, one_over_alpha, S);
+    const auto k = k_residual_restrict_shape<TPB, NT, MINB>();
+    launch_kernel(k, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
+                  prefetch_topo(g, k, 128 * TPB, sizeof(TileStage) * per, per, prefetch), g.level_first[level], list, n, items, nitems,
+                  item_blocks, X, RHS, C, one_over_alpha, S);
 }
 
 void residual_restrict(const DevGrid& g, int level, const float* X, const float* RHS, float* C, float one_over_alpha,
@@ -1352,7 +1397,12 @@ void residual_restrict(const DevGrid& g, int level, const float* X, const float*
     case 4: residual_shape<1, 1>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     case 5: residual_shape<1, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
     case 6: residual_shape<1, 1, 16>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
-    default: residual_shape<1, 1, 12>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    case 7: residual_shape<1, 1, 12>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero); break;
+    // 8..11: shapes 2, 5, 6, 1 prefetching later CTAs' tiles into L2
+    case 8: residual_shape<1, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
+    case 9: residual_shape<1, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
+    case 10: residual_shape<1, 1, 16>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
+    default: residual_shape<2, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
     }
 }
 

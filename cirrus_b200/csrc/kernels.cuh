@@ -357,6 +357,12 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+// Bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned) at `p` into L2, without waiting
+// and without a destination: a hint that raises the number of bytes in flight for tiles a later
+// CTA of the same launch will stage.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Staging area of one tile: its values, face halos, a second channel (right-hand side) and the

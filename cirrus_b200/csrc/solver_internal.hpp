@@ -57,10 +57,14 @@ struct GraphKey {
 // choice per kernel and level is made by the autotuner (autotune.cu) and is bit-neutral: every
 // shape computes each tile with the same operations.
 enum { KS_GS_SWEEP = 0, KS_PRESMOOTH = 1, KS_PROLONG = 2, KS_RESIDUAL = 3, KS_LAPLACIAN = 4, KS_COUNT = 5 };
-constexpr int kNumShapes = 8;
-// the Laplacian has eight more: 8..11 the TMA-staged pipeline (lap_tma.cu) with (consumer groups,
-// stages) = (2, 8), (4, 16), (2, 12), (1, 6); 12..15 eight cells per thread (lap8.cu)
-constexpr int kNumLapShapes = 16;
+// shapes 0..7: (tiles per CTA, tiles in flight per group, minimum CTAs per SM); 8..11 four of
+// them prefetching the tiles of CTAs one resident wave ahead into L2
+constexpr int kNumShapes = 12;
+// the Laplacian's 8..11 are instead the TMA-staged pipeline (lap_tma.cu) with (consumer groups,
+// stages) = (2, 8), (4, 16), (2, 12), (1, 6); then 12..15 eight cells per thread (lap8.cu), 16..19
+// shapes 2, 3, 5, 1 prefetching into L2 the tiles of CTAs one resident wave ahead
+constexpr int kNumLapShapes = 20;
+constexpr int kFirstTmaShape = 8;
 constexpr int kFirstLap8Shape = 12;
 inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kNumShapes; }
 
@@ -222,6 +226,20 @@ inline void launch_kernel(void (*k)(KArgs...), dim3 grid, dim3 block, size_t sme
     cfg.attrs = attr;
     cfg.numAttrs = pdl_enabled() ? 1 : 0;
     cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+// The grid's kernel view for one launch of a staged kernel k (threads per CTA, dynamic shared
+// memory, list entries per CTA): with prefetch, tp.pf = the list entries the CTAs resident at once
+// cover, so each CTA prefetches into L2 the tiles of the CTA one resident wave later.
+template <class K>
+inline Topo prefetch_topo(const DevGrid& g, K k, int threads, size_t smem, int per_cta, bool prefetch) {
+    Topo tp = g.topo;
+    tp.pf = 0;
+    if (prefetch) {
+        int resident = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k, threads, smem);
+        tp.pf = (resident > 0 ? resident : 1) * g.sm_count * per_cta;
+    }
+    return tp;
 }
 // S (nullable): per-instance scalars; tiles of finished instances are skipped.
 template <class T> void full_laplacian(const DevGrid& g, T* X, T* Y, const Scalars* S, cudaStream_t s);

@@ -81,13 +81,14 @@ __device__ __forceinline__ void k_presmooth_body(Topo tp, const int* __restrict_
     PreStage* st = reinterpret_cast<PreStage*>(pre_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     const TileIdx ix(t);
-    int tile[NT];
+    int tile[NT], ptile[NT];
     bool act[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         const int q = (blockIdx.x * NT + u) * TPB + g;
         tile[u] = q < n ? list[q] : 0;
         act[u] = q < n;  // finished instances are dropped after the copies are issued (reading them is harmless)
+        ptile[u] = (tp.pf > 0 && t == 0 && q + tp.pf < n) ? list[q + tp.pf] : -1;
     }
     // neighbour of this thread's x/y-face piece (t < 64) and z-face cell; GHOST neighbours count
     // as absent (their x is 0 on the way down).  Metadata of all NT tiles is loaded before any
@@ -134,6 +135,12 @@ __device__ __forceinline__ void k_presmooth_body(Topo tp, const int* __restrict_
         }
         if (nbz[u] >= 0) cp_async4(ps.hx + zface * 64 + zc, RHS + (size_t)nbz[u] * kTileCells + zoff);
     }
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (ptile[u] >= 0) {
+            prefetch_l2(RHS + (size_t)ptile[u] * kTileCells, kTileCells * sizeof(float));
+            prefetch_l2(tp.mask_mg + (size_t)ptile[u] * kTileCells, kTileCells);
+        }
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (nbz[u] >= 0) st[u * TPB + g].hmask[zface * 64 + zc] = (uint8_t)zmb[u];
@@ -286,11 +293,13 @@ __device__ __forceinline__ void k_prolong_sweep_body(Topo tp, const int* __restr
     int packed[NT], parent[NT], nbf[NT], nbz[NT], inst[NT], fpar[NT], zpar[NT];
     uint32_t fc[NT], zmb[NT];
     float4 lc[NT];
+    int ptile[NT];
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         const int q = (((int)blockIdx.x - item_blocks) * NT + u) * TPB + g;
         tile[u] = list[q < n ? q : 0];
         act[u] = q < n;  // finished instances are dropped after the copies are issued
+        ptile[u] = (tp.pf > 0 && t == 0 && q + tp.pf < n) ? list[q + tp.pf] : -1;
         const TileMeta& m = tp.meta[tile[u]];
         packed[u] = m.packed;
         parent[u] = m.parent;
@@ -355,6 +364,13 @@ __device__ __forceinline__ void k_prolong_sweep_body(Topo tp, const int* __restr
                 cp_async4(ps.hpar + 128 + (zface - 4) * 64 + zc, Z + (size_t)zpar[u] * kTileCells + parent_cell((hf[u] >> 11) & 7u, zoff));
         }
     }
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (ptile[u] >= 0) {
+            prefetch_l2(XP + (size_t)ptile[u] * kTileCells, kTileCells * sizeof(float));
+            prefetch_l2(RHS + (size_t)ptile[u] * kTileCells, kTileCells * sizeof(float));
+            prefetch_l2(tp.mask_mg + (size_t)ptile[u] * kTileCells, kTileCells);
+        }
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (nbz[u] >= 0) st[u * TPB + g].hmask[zface * 64 + zc] = (uint8_t)zmb[u];
@@ -614,11 +630,12 @@ namespace launch {
 constexpr int kTPB2 = 2;
 
 template <int TPB, int NT, int MINB = 0>
-void presmooth_shape(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s) {
+void presmooth_shape(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s, bool prefetch = false) {
     const int n = g.mg_count[level];
     const int per = TPB * NT;
-    launch_kernel(k_presmooth_shape<TPB, NT, MINB>(), (n + per - 1) / per, 128 * TPB, sizeof(PreStage) * per, s, g.topo, g.d_mg + g.mg_offset[level], n,
-                  XP, RHS, S);
+    const auto k = k_presmooth_shape<TPB, NT, MINB>();
+    launch_kernel(k, (n + per - 1) / per, 128 * TPB, sizeof(PreStage) * per, s,
+                  prefetch_topo(g, k, 128 * TPB, sizeof(PreStage) * per, per, prefetch), g.d_mg + g.mg_offset[level], n, XP, RHS, S);
 }
 
 void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const Scalars* S, cudaStream_t s) {
@@ -633,18 +650,25 @@ void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const S
     case 4: presmooth_shape<1, 1>(g, level, XP, RHS, S, s); break;
     case 5: presmooth_shape<1, 2>(g, level, XP, RHS, S, s); break;
     case 6: presmooth_shape<1, 1, 16>(g, level, XP, RHS, S, s); break;
-    default: presmooth_shape<1, 1, 12>(g, level, XP, RHS, S, s); break;
+    case 7: presmooth_shape<1, 1, 12>(g, level, XP, RHS, S, s); break;
+    // 8..11: shapes 2, 5, 6, 1 prefetching later CTAs' tiles into L2
+    case 8: presmooth_shape<1, 4>(g, level, XP, RHS, S, s, true); break;
+    case 9: presmooth_shape<1, 2>(g, level, XP, RHS, S, s, true); break;
+    case 10: presmooth_shape<1, 1, 16>(g, level, XP, RHS, S, s, true); break;
+    default: presmooth_shape<2, 2>(g, level, XP, RHS, S, s, true); break;
     }
 }
 
 template <int TPB, int NT, int MINB = 0>
 void prolong_shape(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
-                   cudaStream_t s) {
+                   cudaStream_t s, bool prefetch = false) {
     const int n = g.pr_cnt[level], nitems = g.pri_cnt[level];
     const int per = TPB * NT;
     const int item_blocks = (nitems + 2 * TPB - 1) / (2 * TPB);
-    launch_kernel(k_prolong_sweep_shape<TPB, NT, MINB>(), item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(ProStage) * per, s, g.topo,
-                  g.d_prmain + g.pr_off[level], n, g.d_pritems + g.pri_off[level], nitems, item_blocks, Z, XP, RHS, prolong_coeff, S);
+    const auto k = k_prolong_sweep_shape<TPB, NT, MINB>();
+    launch_kernel(k, item_blocks + (n + per - 1) / per, 128 * TPB, sizeof(ProStage) * per, s,
+                  prefetch_topo(g, k, 128 * TPB, sizeof(ProStage) * per, per, prefetch), g.d_prmain + g.pr_off[level], n,
+                  g.d_pritems + g.pri_off[level], nitems, item_blocks, Z, XP, RHS, prolong_coeff, S);
 }
 
 void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const float* RHS, float prolong_coeff, const Scalars* S,
@@ -660,7 +684,12 @@ void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const
     case 4: prolong_shape<1, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     case 5: prolong_shape<4, 1>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
     case 6: prolong_shape<1, 1, 16>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
-    default: prolong_shape<1, 1, 12>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    case 7: prolong_shape<1, 1, 12>(g, level, Z, XP, RHS, prolong_coeff, S, s); break;
+    // 8..11: shapes 2, 3, 6, 1 prefetching later CTAs' tiles into L2
+    case 8: prolong_shape<1, 4>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
+    case 9: prolong_shape<1, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
+    case 10: prolong_shape<1, 1, 16>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
+    default: prolong_shape<2, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
     }
 }
 

@@ -444,13 +444,15 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
 /* Launch shapes of the staged stencil kernels, as the autotuner sets them: kernel one of
  * CIRRUS_KERNEL_LAPLACIAN / _GS_SWEEP / _PRESMOOTH / _PROLONG_SWEEP / _RESIDUAL_RESTRICT (or -1:
  * all of them), level a level of the grid (or -1: all levels; the Laplacian has one entry,
- * level 0), shape in [0, 8) for every kernel; the Laplacian also takes 8..11, its TMA-staged
+ * level 0), shape in [0, 12) for every kernel (8..11: four of the shapes 0..7 also prefetching into
+ * L2 the tiles of the CTAs one resident wave later); the Laplacian's 8..11 are instead its TMA-staged
  * pipeline (persistent CTAs, one producer warp issuing bulk tensor copies of each tile and its
  * halos into a ring of shared-memory stages, 1-4 consumer groups), and 12..15, a column of eight
- * cells per thread (64 threads per tile).  Lets a caller reuse tuned
+ * cells per thread (64 threads per tile), and 16..19, shapes 2, 3, 5 and 1 prefetching the tiles of
+ * CTAs one resident wave ahead into L2.  Lets a caller reuse tuned
  * shapes for grids of the same structure or pin one.  Shapes never change results.  No
  * counterpart in the reference. */
-#define CIRRUS_NUM_LAUNCH_SHAPES 16
+#define CIRRUS_NUM_LAUNCH_SHAPES 20
 cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape);
 cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int level, int* shape);
 

@@ -7,7 +7,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from cirrus_b200 import KERNEL_LAPLACIAN, KERNEL_PROLONG_SWEEP, DeviceGrid, GMGSolver, PRECISION_MIXED_FP64, workloads as W
+from cirrus_b200 import KERNEL_GS_SWEEP, KERNEL_LAPLACIAN, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP, KERNEL_RESIDUAL_RESTRICT, DeviceGrid, GMGSolver, PRECISION_MIXED_FP64, workloads as W
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -152,7 +152,7 @@ def test_autotune_changes_timing_not_results(built_cache):
 
 
 def test_every_launch_shape_gives_the_same_bits(built_cache):
-    """Each of the eight launch shapes of the staged kernels (tiles per CTA x tiles in flight),
+    """Each of the eight plain launch shapes of the staged kernels (tiles per CTA x tiles in flight),
     pinned for every kernel and level, gives the solve of the default shapes bit for bit."""
     bs = [built_cache(n) for n in ["sphere64_small", "ring64_small"]]
     rhs = [rhs_of(b) for b in bs]
@@ -179,7 +179,8 @@ def test_every_launch_shape_gives_the_same_bits(built_cache):
 def test_tma_and_column_laplacian_shapes_give_the_same_bits(built_cache, names):
     """The Laplacian's TMA-staged pipeline (shapes 8-11: one producer warp issuing bulk tensor
     copies of each tile, its halos and masks into a ring of shared-memory stages, 1-4 consumer
-    groups) and its eight-cells-per-thread layout (shapes 12-15: 64 threads per tile) inside the
+    groups), its eight-cells-per-thread layout (shapes 12-15: 64 threads per tile) and the
+    4-cell shapes that prefetch later CTAs' tiles into L2 (shapes 16-19) inside the
     solve -- A p of every LEAF tile, the GHOST rows, the p.Ap tile parts -- give the iterations and
     pressure of the cp.async-staged 4-cell shape bit for bit."""
     bs = [built_cache(n) for n in names]
@@ -187,10 +188,38 @@ def test_tma_and_column_laplacian_shapes_give_the_same_bits(built_cache, names):
     g = DeviceGrid([b.topology for b in bs])
     s = GMGSolver()
     out = []
-    shapes = (1, 8, 9, 10, 11, 12, 13, 14, 15)
+    shapes = (1, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19)
     for shape in shapes:
         g.set_launch_shape(shape, KERNEL_LAPLACIAN)
         assert g.get_launch_shape(KERNEL_LAPLACIAN, 0) == shape
+        for i, r in enumerate(rhs):
+            g.set_channel_instance(i, 1, r)
+            g.set_channel_instance(i, 0, np.zeros_like(r))
+        res = s.solve_batch(g)
+        assert all(r.status == 0 for r in s.last_results), shape
+        out.append((res, [g.get_channel_instance(i, 0) for i in range(len(bs))]))
+    for shape, (res, xs) in zip(shapes[1:], out[1:]):
+        assert res == out[0][0], shape
+        for a, b in zip(out[0][1], xs):
+            assert np.array_equal(bits(a), bits(b)), shape
+    g.close()
+
+
+@pytest.mark.parametrize("kernel", [KERNEL_GS_SWEEP, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP, KERNEL_RESIDUAL_RESTRICT])
+@pytest.mark.parametrize("names", [["sphere64_small", "ring64_small"], ["ring512"] * 2])
+def test_prefetching_stencil_shapes_give_the_same_bits(built_cache, names, kernel):
+    """The V-cycle's staged kernels in the shapes that prefetch later CTAs' tiles into L2 (8-11),
+    pinned at every level, give the iterations and pressure of shape 1 bit for bit."""
+    bs = [built_cache(n) for n in names]
+    rhs = [rhs_of(b) for b in bs]
+    g = DeviceGrid([b.topology for b in bs])
+    s = GMGSolver()
+    out = []
+    shapes = (1, 8, 9, 10, 11)
+    for shape in shapes:
+        for lvl in range(int(max(int(b.tiles[:, 0].max()) for b in bs)) + 1):
+            g.set_launch_shape(shape, kernel, lvl)
+        assert g.get_launch_shape(kernel, 1) == shape
         for i, r in enumerate(rhs):
             g.set_channel_instance(i, 1, r)
             g.set_channel_instance(i, 0, np.zeros_like(r))
