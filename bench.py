@@ -97,7 +97,10 @@ def parse():
     ap.add_argument("--profile-kernels", action="store_true",
                     help="for a profiler: launch each staged stencil kernel once at the finest level (NVTX range "
                          "'kernels'), then one batched solve with direct kernel launches (NVTX range 'solve'); no timing")
-    ap.add_argument("--lap-shape", type=int, default=-1, help="pin the Laplacian's launch shape (0-11) after autotuning")
+    ap.add_argument("--lap-shape", type=int, default=-1, help="pin the Laplacian's launch shape (0-19) after autotuning")
+    ap.add_argument("--shape-sweep", action="store_true",
+                    help="time every launch shape of the fused Laplacian and of the four V-cycle stencil kernels at the "
+                         "finest level (warm, CUDA events, 40 back-to-back launches, best of 3); one JSON line")
     return ap.parse_args()
 
 
@@ -933,8 +936,53 @@ def profile_kernels(args):
     g.close()
 
 
+def shape_sweep(args) -> dict:
+    """Per staged kernel and launch shape, the warm time of one launch over the workload's batch:
+    the data the autotuner chooses from (shapes never change results)."""
+    import torch
+
+    from cirrus_b200 import (KERNEL_GS_SWEEP, KERNEL_LAPLACIAN, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP, KERNEL_RESIDUAL_RESTRICT,
+                             lib)
+
+    b, g = build_batch(args.workload, batch_seeds(0, args.batch))
+    rng = np.random.default_rng(0)
+    for c in (2, 3, 4):  # the channels the kernels read in cirrus_bench_launch
+        g.set_channel(c, rng.standard_normal((g.num_tiles, 512)).astype(np.float32))
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    lmax = int(b.tiles[:, 0].max())
+    out = {"workload": args.workload, "instances": args.batch, "level": lmax, "unit": "us per launch", "kernels": {}}
+    for name, kern, level in (("k_laplacian_fused", KERNEL_LAPLACIAN, 0), ("k_gs_sweep", KERNEL_GS_SWEEP, lmax),
+                              ("k_presmooth", KERNEL_PRESMOOTH, lmax), ("k_prolong_sweep", KERNEL_PROLONG_SWEEP, lmax),
+                              ("k_residual_restrict", KERNEL_RESIDUAL_RESTRICT, lmax)):
+        res = {}
+        shape = 0
+        while lib().cirrus_grid_set_launch_shape(g.handle, kern, level, shape) == 0:
+            g.bench_launch(kern, level, 4, stream=sh)
+            ts = []
+            for _ in range(3):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                g.bench_launch(kern, level, 40, stream=sh)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1) / 40 * 1e3)
+            res[str(shape)] = round(min(ts), 2)
+            shape += 1
+        out["kernels"][name] = res
+    g.close()
+    return out
+
+
 def main():
     args = parse()
+    if args.shape_sweep:
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps(shape_sweep(args)), flush=True)
+        return
     if args.profile_kernels:
         import torch
 

@@ -498,8 +498,11 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
             if (rel[i] < tol[i]) { r[i].status = 0; active[i] = 0; continue; }
             if (k == p.max_outer) { active[i] = 0; continue; }
             // each inner FP32 solve targets the defect that leaves the outer residual just under
-            // tol, but never tighter than inner_tol (where FP32 stalls) nor looser than 0.1
-            double tau = 0.5 * tol[i] / rel[i];
+            // tol (0.9 of it: the FP32 recursive residual the inner solve stops on stays within a
+            // few percent of the true one at these tolerances, and an outer step that falls short
+            // costs one more short inner solve), but never tighter than inner_tol (where FP32
+            // stalls) nor looser than 0.1
+            double tau = 0.9 * tol[i] / rel[i];
             tau = std::min(0.1, std::max(p.inner_tol, tau));
             inner[i].active = 1;
             inner[i].tol = tau;

@@ -305,7 +305,7 @@ typedef struct cirrus_solve_params {
     int precision;              /* CIRRUS_PRECISION_* */
     int warm_start;             /* mixed mode: start from the x channel instead of 0 */
     double inner_tolerance;     /* mixed mode: the tightest relative tolerance an FP32 inner solve
-                                   is asked for (each targets max(this, 0.5*tol/current residual));
+                                   is asked for (each targets max(this, 0.9*tol/current residual));
                                    default 1e-7: the inner solves stop on FP32's recursive residual,
                                    which keeps falling, so a 1e-6 solve takes one inner solve */
     int max_outer_iters;        /* mixed mode: cap on defect-correction steps */

@@ -26,6 +26,8 @@
  * mLevel, mType), hLog2Hashes, mNumLayers, mH0; its Tile needs mData[c][...] and mCellType[512].
  * Calls for one grid are serialised by the registry; the reference's solve is not re-entrant
  * for a grid either.
+ *
+ * cirrus_dropin::AMGSolver<Grid> (below) replaces the reference's AMGSolver on the same registry.
  */
 #ifndef CIRRUS_GMG_DROPIN_HPP
 #define CIRRUS_GMG_DROPIN_HPP
@@ -65,6 +67,7 @@ struct Binding {
     double h0 = 0;
     cirrus_topology* topo = nullptr;
     cirrus_grid* cg = nullptr;
+    bool amg_ready = false;  // the AMG coefficients of this pool are prepared (AMGSolver)
     std::mutex mu;  // one solve at a time per grid
     ~Binding() { drop(); }
     void drop() {
@@ -72,6 +75,7 @@ struct Binding {
         if (topo) cirrus_topology_destroy(topo);
         cg = nullptr;
         topo = nullptr;
+        amg_ready = false;
     }
 };
 
@@ -124,60 +128,11 @@ inline int bound_grids() {
     return (int)reg.by_grid.size();
 }
 
+namespace detail {
+// Tile layout, registry lookup and (re)binding of a reference grid type, shared by the solver
+// classes below.
 template <class Grid>
-class GMGSolver {
-public:
-    explicit GMGSolver(float one_over_alpha = 1.f, float prolong_coeff = 1.f)
-        : one_over_alpha_(one_over_alpha), prolong_coeff_(prolong_coeff) {}
-    GMGSolver(const GMGSolver&) = delete;
-    GMGSolver& operator=(const GMGSolver&) = delete;
-
-    /* GMGSolver::solve (src/GMGSolver.cu:531-666): returns (iterations, relative residual). */
-    std::tuple<int, double> solve(Grid& grid, bool verbose, int max_iters, double relative_tolerance, int level_iters,
-                                  int coarsest_iters, int sync_stride, bool is_pure_neumann) {
-        std::shared_ptr<detail::Binding> b = binding(grid);
-        std::lock_guard<std::mutex> lk(b->mu);
-        bind(grid, *b);
-        cirrus_grid* cg = b->cg;
-        check(cirrus_grid_gather_tiles(cg, 1, channel_offset(1), nullptr), "gather b");
-        cirrus_solve_params p;
-        cirrus_solve_params_default(&p);
-        p.max_iters = max_iters;
-        p.relative_tolerance = relative_tolerance;
-        p.level_iters = level_iters;
-        p.coarsest_iters = coarsest_iters;
-        p.sync_stride = sync_stride;
-        p.is_pure_neumann = is_pure_neumann ? 1 : 0;
-        p.one_over_alpha = one_over_alpha_;
-        p.prolong_coeff = prolong_coeff_;
-        cirrus_solve_result r;
-        check(cirrus_gmg_solve(cg, &p, nullptr, &r), "cirrus_gmg_solve");
-        check(cirrus_grid_scatter_tiles(cg, 0, channel_offset(0), nullptr), "scatter x");
-        check(cirrus_grid_scatter_tiles(cg, 1, channel_offset(1), nullptr), "scatter r");
-        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cirrus_dropin: CUDA error");
-        if (verbose) std::printf("cirrus GMG-PCG: %d iterations, relative residual %.3e\n", r.iters, r.rel_residual);
-        return std::make_tuple(r.iters, sync_stride > 0 ? r.rel_residual : -1.0);
-    }
-
-    /* GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x to channel 0,
-     * the last residual in channel 2 and the diagonal in channel 3 of LEAF|GHOST tiles (both
-     * channels keep their previous contents on NONLEAF tiles, as in the reference). */
-    std::tuple<int, double> dampedJacobiSolve(Grid& grid, bool verbose, int max_iters, double relative_tolerance, float omega) {
-        std::shared_ptr<detail::Binding> b = binding(grid);
-        std::lock_guard<std::mutex> lk(b->mu);
-        bind(grid, *b);
-        cirrus_grid* cg = b->cg;
-        for (int c : {1, 2, 3}) check(cirrus_grid_gather_tiles(cg, c, channel_offset(c), nullptr), "gather");
-        int iters = 0;
-        double rel = 0.0;
-        check(cirrus_damped_jacobi_solve(cg, max_iters, relative_tolerance, omega, nullptr, &iters, &rel), "cirrus_damped_jacobi_solve");
-        for (int c : {0, 2, 3}) check(cirrus_grid_scatter_tiles(cg, c, channel_offset(c), nullptr), "scatter");
-        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cirrus_dropin: CUDA error");
-        if (verbose) std::printf("cirrus damped Jacobi: %d iterations, relative residual %.3e\n", iters, rel);
-        return std::make_tuple(iters, rel);
-    }
-
-private:
+struct Access {
     using Info = typename std::decay<decltype(std::declval<Grid&>().hAllTiles[0])>::type;
     using Tile = typename std::decay<decltype(*std::declval<Info&>().mTilePtr)>::type;
 
@@ -248,7 +203,124 @@ private:
         if (changed) build_pool(b);
     }
 
+};
+}  // namespace detail
+
+template <class Grid>
+class GMGSolver {
+public:
+    explicit GMGSolver(float one_over_alpha = 1.f, float prolong_coeff = 1.f)
+        : one_over_alpha_(one_over_alpha), prolong_coeff_(prolong_coeff) {}
+    GMGSolver(const GMGSolver&) = delete;
+    GMGSolver& operator=(const GMGSolver&) = delete;
+
+    /* GMGSolver::solve (src/GMGSolver.cu:531-666): returns (iterations, relative residual). */
+    std::tuple<int, double> solve(Grid& grid, bool verbose, int max_iters, double relative_tolerance, int level_iters,
+                                  int coarsest_iters, int sync_stride, bool is_pure_neumann) {
+        using A = detail::Access<Grid>;
+        std::shared_ptr<detail::Binding> b = A::binding(grid);
+        std::lock_guard<std::mutex> lk(b->mu);
+        A::bind(grid, *b);
+        cirrus_grid* cg = b->cg;
+        check(cirrus_grid_gather_tiles(cg, 1, A::channel_offset(1), nullptr), "gather b");
+        cirrus_solve_params p;
+        cirrus_solve_params_default(&p);
+        p.max_iters = max_iters;
+        p.relative_tolerance = relative_tolerance;
+        p.level_iters = level_iters;
+        p.coarsest_iters = coarsest_iters;
+        p.sync_stride = sync_stride;
+        p.is_pure_neumann = is_pure_neumann ? 1 : 0;
+        p.one_over_alpha = one_over_alpha_;
+        p.prolong_coeff = prolong_coeff_;
+        cirrus_solve_result r;
+        check(cirrus_gmg_solve(cg, &p, nullptr, &r), "cirrus_gmg_solve");
+        check(cirrus_grid_scatter_tiles(cg, 0, A::channel_offset(0), nullptr), "scatter x");
+        check(cirrus_grid_scatter_tiles(cg, 1, A::channel_offset(1), nullptr), "scatter r");
+        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cirrus_dropin: CUDA error");
+        if (verbose) std::printf("cirrus GMG-PCG: %d iterations, relative residual %.3e\n", r.iters, r.rel_residual);
+        return std::make_tuple(r.iters, sync_stride > 0 ? r.rel_residual : -1.0);
+    }
+
+    /* GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x to channel 0,
+     * the last residual in channel 2 and the diagonal in channel 3 of LEAF|GHOST tiles (both
+     * channels keep their previous contents on NONLEAF tiles, as in the reference). */
+    std::tuple<int, double> dampedJacobiSolve(Grid& grid, bool verbose, int max_iters, double relative_tolerance, float omega) {
+        using A = detail::Access<Grid>;
+        std::shared_ptr<detail::Binding> b = A::binding(grid);
+        std::lock_guard<std::mutex> lk(b->mu);
+        A::bind(grid, *b);
+        cirrus_grid* cg = b->cg;
+        for (int c : {1, 2, 3}) check(cirrus_grid_gather_tiles(cg, c, A::channel_offset(c), nullptr), "gather");
+        int iters = 0;
+        double rel = 0.0;
+        check(cirrus_damped_jacobi_solve(cg, max_iters, relative_tolerance, omega, nullptr, &iters, &rel), "cirrus_damped_jacobi_solve");
+        for (int c : {0, 2, 3}) check(cirrus_grid_scatter_tiles(cg, c, A::channel_offset(c), nullptr), "scatter");
+        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cirrus_dropin: CUDA error");
+        if (verbose) std::printf("cirrus damped Jacobi: %d iterations, relative residual %.3e\n", iters, rel);
+        return std::make_tuple(iters, rel);
+    }
+
+private:
     float one_over_alpha_, prolong_coeff_;
+};
+
+/* Drop-in for the reference's AMGSolver (src/AMGSolver.h:20-53; AMGSolver.cu:717-853) on the same
+ * registry of bound pools: prepareTypesAndCoeffs(grid) forms the AMG cell types and coefficients
+ * on the device pool (cirrus_amg_prepare), solve(...) runs the AMG-preconditioned CG
+ * (cirrus_amg_solve) with b gathered from channel 1 and x / the final residual scattered to
+ * channels 0 / 1.  The reference writes the coefficients into tile channels coeff_channel..+3
+ * and rewrites NONLEAF cell types in place; here both stay on the device pool (the tiles'
+ * channels other than 0 and 1 and their cell types are not written), so coeff_channel is kept
+ * only for the signature.  A solve after the pool was rebuilt (new tiles or cell types) without
+ * a new prepareTypesAndCoeffs throws, where the reference would use stale coefficients. */
+template <class Grid>
+class AMGSolver {
+public:
+    explicit AMGSolver(int coeff_channel, float one_over_alpha = 1.f, float prolong_coeff = 1.f)
+        : coeff_channel(coeff_channel), one_over_alpha(one_over_alpha), prolong_coeff(prolong_coeff) {}
+    AMGSolver(const AMGSolver&) = delete;
+    AMGSolver& operator=(const AMGSolver&) = delete;
+
+    void prepareTypesAndCoeffs(Grid& grid) {
+        using A = detail::Access<Grid>;
+        std::shared_ptr<detail::Binding> b = A::binding(grid);
+        std::lock_guard<std::mutex> lk(b->mu);
+        A::bind(grid, *b);
+        check(cirrus_amg_prepare(b->cg, one_over_alpha, nullptr), "cirrus_amg_prepare");
+        b->amg_ready = true;
+    }
+
+    std::tuple<int, double> solve(Grid& grid, bool verbose, int max_iters, double relative_tolerance, int level_iters,
+                                  int coarsest_iters, int sync_stride, bool is_pure_neumann) {
+        using A = detail::Access<Grid>;
+        std::shared_ptr<detail::Binding> b = A::binding(grid);
+        std::lock_guard<std::mutex> lk(b->mu);
+        A::bind(grid, *b);
+        if (!b->amg_ready) throw std::runtime_error("cirrus_dropin::AMGSolver: prepareTypesAndCoeffs first (the tiles or cell types changed)");
+        cirrus_grid* cg = b->cg;
+        check(cirrus_grid_gather_tiles(cg, 1, A::channel_offset(1), nullptr), "gather b");
+        cirrus_solve_params p;
+        cirrus_solve_params_default(&p);
+        p.max_iters = max_iters;
+        p.relative_tolerance = relative_tolerance;
+        p.level_iters = level_iters;
+        p.coarsest_iters = coarsest_iters;
+        p.sync_stride = sync_stride;
+        p.is_pure_neumann = is_pure_neumann ? 1 : 0;
+        p.one_over_alpha = one_over_alpha;
+        p.prolong_coeff = prolong_coeff;
+        cirrus_solve_result r;
+        check(cirrus_amg_solve(cg, &p, nullptr, &r), "cirrus_amg_solve");
+        check(cirrus_grid_scatter_tiles(cg, 0, A::channel_offset(0), nullptr), "scatter x");
+        check(cirrus_grid_scatter_tiles(cg, 1, A::channel_offset(1), nullptr), "scatter r");
+        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cirrus_dropin: CUDA error");
+        if (verbose) std::printf("cirrus AMG-PCG: %d iterations, relative residual %.3e\n", r.iters, r.rel_residual);
+        return std::make_tuple(r.iters, sync_stride > 0 ? r.rel_residual : -1.0);
+    }
+
+    int coeff_channel;
+    float one_over_alpha, prolong_coeff;
 };
 
 }  // namespace cirrus_dropin

@@ -400,6 +400,7 @@ def ref_dropin_lib():
         protos = {
             "refdrop_solve": (C.c_int, [P, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p, f64p]),
             "refdrop_damped_jacobi": (C.c_int, [P, C.c_int, C.c_double, C.c_float, f64p]),
+            "refdrop_amg_solve": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p]),
             "refdrop_bound_grids": (C.c_int, []),
             "refdrop_release_all": (None, []),
         }
@@ -601,6 +602,16 @@ class RefHarness:
         if it < 0:
             raise RuntimeError("drop-in solve failed")
         return it, rel.value, ms.value
+
+    def amg_solve_dropin(self, prepare=True, max_iters=1000, tol=1e-6, level_iters=1, coarsest_iters=10, sync_stride=1,
+                         pure_neumann=False):
+        """AMGSolver through the product's drop-in header on this reference grid (fresh object;
+        prepareTypesAndCoeffs first when `prepare`): (iterations, relative residual), or None when
+        the drop-in raised (e.g. a solve without preparation for the bound pool)."""
+        rel = C.c_double()
+        it = ref_dropin_lib().refdrop_amg_solve(self.h, int(prepare), max_iters, tol, level_iters, coarsest_iters, sync_stride,
+                                                int(pure_neumann), C.byref(rel))
+        return None if it < 0 else (it, rel.value)
 
     def damped_jacobi_dropin(self, max_iters=10, tol=1e-6, omega=1.0):
         """The same call through the product's drop-in header on this reference grid."""

@@ -57,6 +57,26 @@ int refdrop_damped_jacobi(void* h, int max_iters, double tol, float omega, doubl
     return iters;
 }
 
+// The AMG drop-in on the reference grid: prepareTypesAndCoeffs (prepare != 0) then solve, fresh
+// object per call.  Returns iterations, -1 on an exception (message on stderr).
+int refdrop_amg_solve(void* h, int prepare, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
+                      int pure_neumann, double* rel) {
+    auto& grid = *static_cast<HADeviceGrid<Tile>*>(ref_grid(h));
+    int iters = -1;
+    double err = 0.0;
+    try {
+        cirrus_dropin::AMGSolver<HADeviceGrid<Tile>> solver(6, 1.f, 1.f);
+        if (prepare) solver.prepareTypesAndCoeffs(grid);
+        std::tie(iters, err) = solver.solve(grid, false, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "refdrop_amg_solve: %s\n", e.what());
+        return -1;
+    }
+    cudaDeviceSynchronize();
+    if (rel) *rel = err;
+    return iters;
+}
+
 // Bound device pools held by the drop-in's process-wide registry.
 int refdrop_bound_grids() { return cirrus_dropin::bound_grids(); }
 void refdrop_release_all() { cirrus_dropin::release_all(); }

@@ -13,7 +13,7 @@ from cirrus_b200 import workloads as W
 from oracle import oracle as O
 
 FP32, FP64 = O.CpuOracle.FP32, O.CpuOracle.FP64
-NAMES = ["uniform32_small", "sphere64_small", "ring64_small"]
+NAMES = ["uniform32_small", "sphere64_small", "ring64_small", "sphere64_neumann_small"]
 
 
 def oracle_for(b):

@@ -342,3 +342,44 @@ def test_dropin_time_at_call_site(built_cache, ref_ok):
           f"({np.median(ref_ms[1:]) / np.median(drop_ms[1:]):.2f}x)")
     O.ref_dropin_lib().refdrop_release_all()
     assert np.median(drop_ms[1:]) < np.median(ref_ms[1:])
+
+
+@pytest.mark.parametrize("name", ["sphere64_small", "ring512"])
+def test_amg_dropin_in_reference_grid(name, built_cache, ref_ok):
+    """The drop-in's AMGSolver on the reference's own grid (fresh object per call:
+    prepareTypesAndCoeffs, then solve) gives the product's AMGSolver iterations and pressure bit for
+    bit on the same right-hand side; after the cell types change, a solve without a new
+    preparation is refused (the bound pool was rebuilt), and a prepared one matches again."""
+    from cirrus_b200 import AMGSolver, DeviceGrid
+
+    b = built_cache(name)
+    w = b.workload
+    ref = _ref_grid(b)
+    leaf = (b.tiles[:, 4] & W.LEAF) != 0
+    rhs = ref.rhs(b.velocity)
+    ref.set_channel(1, rhs)
+    ref.set_channel(0, np.zeros_like(rhs))
+    got = ref.amg_solve_dropin(True, 1000, 1e-6, 1, 10, 1, w.pure_neumann)
+    assert got is not None
+    g = DeviceGrid(b.topology)
+    g.set_channel(1, rhs)
+    s = AMGSolver()
+    s.prepare_types_and_coeffs(g)
+    it, rel = s.solve(g, is_pure_neumann=w.pure_neumann)
+    print(f"{name}: AMG drop-in {got[0]} iters {got[1]:.3e}; product {it} iters {rel:.3e}")
+    assert got[0] == it and abs(got[1] - rel) <= 1e-12 * rel
+    assert np.array_equal(bits(ref.get_channel(0))[leaf], bits(g.get_channel(0))[leaf])
+    g.close()
+    # a block of cells turned NEUMANN: the pool is rebuilt on the next call, which needs a new preparation
+    base = W.leaf_cell_types(w, b.tiles, b.nbr6)
+    cand = [t for t in np.flatnonzero(leaf) if (base[t].reshape(8, 8, 8)[2:6, 2:6, 2:6] == W.INTERIOR).all()]
+    moved = base.copy()
+    moved[cand[len(cand) // 2]].reshape(8, 8, 8)[2:6, 2:6, 2:6] = W.NEUMANN
+    ref.set_ctypes(moved)
+    ref.calc_cell_types()
+    ref.set_channel(1, rhs)
+    assert ref.amg_solve_dropin(False, 1000, 1e-6, 1, 10, 1, w.pure_neumann) is None
+    ref.set_channel(1, rhs)
+    ref.set_channel(0, np.zeros_like(rhs))
+    got2 = ref.amg_solve_dropin(True, 1000, 1e-6, 1, 10, 1, w.pure_neumann)
+    assert got2 is not None and got2[1] < 1e-6
