@@ -377,9 +377,9 @@ def test_amg_dropin_in_reference_grid(name, built_cache, ref_ok):
     moved[cand[len(cand) // 2]].reshape(8, 8, 8)[2:6, 2:6, 2:6] = W.NEUMANN
     ref.set_ctypes(moved)
     ref.calc_cell_types()
-    ref.set_channel(1, rhs)
+    rhs2 = ref.rhs(b.velocity)  # the right-hand side of the new cell types
     assert ref.amg_solve_dropin(False, 1000, 1e-6, 1, 10, 1, w.pure_neumann) is None
-    ref.set_channel(1, rhs)
-    ref.set_channel(0, np.zeros_like(rhs))
+    ref.set_channel(1, rhs2)
+    ref.set_channel(0, np.zeros_like(rhs2))
     got2 = ref.amg_solve_dropin(True, 1000, 1e-6, 1, 10, 1, w.pure_neumann)
     assert got2 is not None and got2[1] < 1e-6
