@@ -10,11 +10,15 @@
 // Storage: four FP32 planes of n*512 (off-diagonal coefficient of each cell's x-, y-, z- face,
 // then the diagonal) and a byte plane of AMG cell types (the grid's cell types with GHOST cells
 // re-derived from their parents and NONLEAF cells rewritten by the coarsening), allocated on the
-// first prepare.  All kernels take one 128-thread CTA per tile; thread t owns the cells 4t..4t+3
-// (column (t >> 4, (t >> 1) & 7), k = 4 (t & 1) .. +3).  Tiles of finished instances are
-// skipped (per-instance scalars S), so the V-cycle runs inside batched solves too.
+// first prepare.  The kernels take one 128-thread CTA per tile, thread t owning the cells
+// 4t..4t+3 (column (t >> 4, (t >> 1) & 7), k = 4 (t & 1) .. +3); the coarsest level's sweeps run
+// as one CTA per instance looping over its tiles (k_amg_gs_sequence).  Tiles of finished
+// instances are skipped (per-instance scalars S), so the V-cycle runs inside batched solves too.
 #include "kernels.cuh"
 #include "solver_internal.hpp"
+
+#include <algorithm>
+#include <vector>
 
 namespace cirrus {
 
@@ -194,6 +198,25 @@ __device__ __forceinline__ float amg_lap(const TileShared<float>& sh, const floa
 // NegativeLaplacianAndGaussSeidelSameLevel128Kernel (src/AMGSolver.cu:540-578) on the LEAF|NONLEAF
 // tiles of one level: cells of colour (i+j+k)%2 == color get x + (b - A x)/D where INTERIOR, x + 0
 // elsewhere.
+// The colour update of thread t's four cells of a staged tile (see k_amg_gs).
+__device__ __forceinline__ void amg_gs_cells(const TileShared<float>& sh, const float* __restrict__ C, size_t plane, int tile, const TileMeta& m,
+                                             int t, float* X, const float* __restrict__ RHS, const uint8_t* __restrict__ act, int color) {
+    const TileIdx ix(t);
+    const size_t base = (size_t)tile * kTileCells;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int k = ix.k0 + e;
+        if (((ix.i + ix.j + k) & 1) != color) continue;
+        const int c = cell_of(ix.i, ix.j, k);
+        float delta = 0.f;
+        if (act[base + c] & INTERIOR_C) {
+            const float ax = amg_lap(sh, C, plane, base, m, ix.i, ix.j, k);
+            delta = __fdiv_rn(RHS[base + c] - ax, C[3 * plane + base + c]);
+        }
+        X[base + c] = sh.xs[c] + delta;
+    }
+}
+
 __global__ void __launch_bounds__(128) k_amg_gs(Topo tp, const int* __restrict__ list, int n, float* X, const float* __restrict__ RHS,
                                                 const uint8_t* __restrict__ act, const float* __restrict__ C, size_t plane, int color,
                                                 const Scalars* __restrict__ S) {
@@ -209,19 +232,39 @@ __global__ void __launch_bounds__(128) k_amg_gs(Topo tp, const int* __restrict__
     }
     __syncthreads();
     if (!active) return;
-    const TileIdx ix(t);
-    const size_t base = (size_t)tile * kTileCells;
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-        const int k = ix.k0 + e;
-        if (((ix.i + ix.j + k) & 1) != color) continue;
-        const int c = cell_of(ix.i, ix.j, k);
-        float delta = 0.f;
-        if (act[base + c] & INTERIOR_C) {
-            const float ax = amg_lap(sh, C, plane, base, m, ix.i, ix.j, k);
-            delta = __fdiv_rn(RHS[base + c] - ax, C[3 * plane + base + c]);
+    amg_gs_cells(sh, C, plane, tile, m, t, X, RHS, act, color);
+}
+
+// A sequence of colour sweeps (bit s of `colors` = the colour of sweep s) over one level's
+// LEAF|NONLEAF tiles, one CTA per instance: CTA i takes the list entries ranges[i] = (first, count)
+// -- one instance's tiles, coupled to no other instance's -- in rounds of blockDim/128 tiles, and
+// a __syncthreads makes each round's global writes visible to the next round's halo loads.  A
+// colour's cells never neighbour each other, so updating a sweep's tiles round by round gives
+// the bits of one launch per sweep.
+__global__ void __launch_bounds__(1024) k_amg_gs_sequence(Topo tp, const int* __restrict__ list, const int2* __restrict__ ranges,
+                                                          float* X, const float* __restrict__ RHS, const uint8_t* __restrict__ act,
+                                                          const float* __restrict__ C, size_t plane, uint32_t colors, int nsweeps,
+                                                          const Scalars* __restrict__ S) {
+    pdl_entry();
+    __shared__ TileShared<float> sh[8];
+    const int2 r = ranges[blockIdx.x];
+    const int groups = blockDim.x >> 7;
+    const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
+    for (int s = 0; s < nsweeps; s++) {
+        const int color = (colors >> s) & 1;
+        for (int base = 0; base < r.y; base += groups) {
+            const int q = base + g;
+            const int tile = q < r.y ? list[r.x + q] : 0;
+            const bool active = q < r.y && !tile_done(tp, S, tile);
+            TileMeta m;
+            if (active) {
+                m = tp.meta[tile];
+                stage_tile<float>(X, tile, m, t, sh[g]);
+            }
+            __syncthreads();
+            if (active) amg_gs_cells(sh[g], C, plane, tile, m, t, X, RHS, act, color);
+            __syncthreads();
         }
-        X[base + c] = sh.xs[c] + delta;
     }
 }
 
@@ -352,6 +395,33 @@ int amg_prepare(DevGrid& g, float one_over_alpha, cudaStream_t s) {
                                                            one_over_alpha);
     g.launch_count += 2 + g.max_level + 1;
     if (cudaGetLastError() != cudaSuccess) return 2;
+    // per instance, its entries of the level-0 LEAF|NONLEAF list (the list is instance by
+    // instance): the coarsest level's sweeps run as one CTA per instance
+    if (!g.d_amg_l0 && g.mg_count[0] > 0) {
+        // from the host tables: the level-0 list holds the level's LEAF|NONLEAF tiles in pool
+        // order, and each instance's tiles of a level are one run of the pool
+        std::vector<int> inst(g.n, -1);
+        for (int i = 0; i < g.num_inst; i++)
+            for (const TileRun& r : g.inst_runs[i])
+                for (int t = r.global; t < r.global + r.count; t++) inst[t] = i;
+        std::vector<int2> ranges(g.num_inst, int2{0, 0});
+        bool contiguous = true;
+        int q = 0;
+        for (int t = g.level_first[0]; t < g.level_first[0] + g.level_count[0]; t++) {
+            if (!(g.h_tile_type[t] & (LEAF_T | NONLEAF_T))) continue;
+            int2& r = ranges[inst[t]];
+            if (r.y == 0) r.x = q;
+            else if (r.x + r.y != q) contiguous = false;
+            r.y++;
+            q++;
+        }
+        if (q != g.mg_count[0]) contiguous = false;
+        g.amg_l0_max = 0;
+        if (contiguous)  // (else the sweeps take one launch each)
+            for (const int2& r : ranges) g.amg_l0_max = std::max(g.amg_l0_max, (int)r.y);
+        if (cudaMalloc(&g.d_amg_l0, sizeof(int2) * g.num_inst) != cudaSuccess) return 3;
+        if (cudaMemcpy(g.d_amg_l0, ranges.data(), sizeof(int2) * g.num_inst, cudaMemcpyHostToDevice) != cudaSuccess) return 2;
+    }
     g.amg_ready = true;
     return 0;
 }
@@ -384,8 +454,26 @@ void vcycle_amg(const DevGrid& g, float* X, const float* F, float* TMP, float* R
                                   g.level_count[l - 1], F, (const float*)TMP, RHS, (const uint8_t*)g.d_amg_ct, one_over_alpha, S);
         }
     }
-    amg_gauss_seidel(g, coarsest_iters / 2, 0, 0, X, RHS, S, s);
-    amg_gauss_seidel(g, coarsest_iters / 2, 1, 0, X, RHS, S, s);
+    // level 0: GaussSeidelAMG(ci/2, 0) + GaussSeidelAMG(ci/2, 1), as one sequence per instance
+    // where every instance's level-0 tiles fit one CTA's rounds, else one launch per sweep
+    if (g.d_amg_l0 && g.amg_l0_max > 0 && g.mg_count[0] > 0) {
+        std::vector<int> cols;
+        for (int it = 0; it < coarsest_iters / 2; it++) { cols.push_back(0); cols.push_back(1); }
+        for (int it = 0; it < coarsest_iters / 2; it++) { cols.push_back(1); cols.push_back(0); }
+        const int threads = 128 * std::min(8, g.amg_l0_max);
+        for (size_t c0 = 0; c0 < cols.size(); c0 += 32) {
+            uint32_t colors = 0;
+            const int ns = (int)std::min<size_t>(32, cols.size() - c0);
+            for (int k = 0; k < ns; k++) colors |= (uint32_t)cols[c0 + k] << k;
+            ++g.launch_count;
+            launch::launch_kernel(k_amg_gs_sequence, g.num_inst, threads, 0, s, g.topo, (const int*)(g.d_mg + g.mg_offset[0]),
+                                  (const int2*)g.d_amg_l0, X, (const float*)RHS, (const uint8_t*)g.d_amg_ct, (const float*)g.d_amg, plane,
+                                  colors, ns, S);
+        }
+    } else {
+        amg_gauss_seidel(g, coarsest_iters / 2, 0, 0, X, RHS, S, s);
+        amg_gauss_seidel(g, coarsest_iters / 2, 1, 0, X, RHS, S, s);
+    }
     for (int l = 1; l <= g.max_level; l++) {
         if (g.level_count[l] > 0) {
             ++g.launch_count;

@@ -697,6 +697,7 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_bsave);
     cudaFree(g->d_amg);
     cudaFree(g->d_amg_ct);
+    cudaFree(g->d_amg_l0);
     delete g;
 }
 

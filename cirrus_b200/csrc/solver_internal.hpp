@@ -190,6 +190,8 @@ struct DevGrid {
     // diagonal) and the AMG cell types, allocated by the first amg_prepare
     float* d_amg = nullptr;
     uint8_t* d_amg_ct = nullptr;
+    int2* d_amg_l0 = nullptr;  // per instance: (first entry, count) of its level-0 LEAF|NONLEAF tiles
+    int amg_l0_max = 0;        // the largest count
     bool amg_ready = false;
 
     struct SolveGraph {
