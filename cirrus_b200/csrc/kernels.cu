@@ -129,8 +129,8 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
                                                                const float* __restrict__ X, float* __restrict__ Y,
                                                                float* __restrict__ GACC, const Scalars* __restrict__ S,
                                                                double* __restrict__ WP) {
-    // the dot-part tail below gives tile u to 16-lane half (u & 1) of warp 2 + (u >> 1): NT <= 4
-    static_assert(NT >= 1 && NT <= 4, "k_laplacian_fused: the tile-part tail covers at most 4 tiles per group");
+    // the dot-part tail below gives tile u to 16-lane half (u & 1) of warp u >> 1: NT <= 8
+    static_assert(NT >= 1 && NT <= 8, "k_laplacian_fused: the tile-part tail covers at most 8 tiles per group");
     pdl_entry();
     if ((int)blockIdx.x < item_blocks) {
         const int q = (int)blockIdx.x * (128 * TPB) + (int)threadIdx.x;
@@ -141,7 +141,7 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
         return;
     }
     extern __shared__ __align__(16) unsigned char lap_smem[];
-    TileStage* st = reinterpret_cast<TileStage*>(lap_smem);
+    LapStage* st = reinterpret_cast<LapStage*>(lap_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     int tile[NT], ptile[NT];
     bool act[NT];
@@ -175,16 +175,40 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
     for (int u = 0; u < NT; u++) {
         ghost[u] = false;
         if (!act[u]) continue;
-        TileStage& ts = st[u * TPB + g];
+        LapStage& ts = st[u * TPB + g];
         ghost[u] = meta_type(pre[u].packed) & GHOST_T;
         const LevelConst<float> L(pre[u].lc);
         float out[4], dg[4];
         neg_lap4<float, false, false>(ts.xs, ts.hx, t, *reinterpret_cast<const uint32_t*>(ts.mask + t * 4), pre[u].fcls & 0xfffu, L,
                                       out, dg);
         if (ghost[u]) {
+            // the GHOST row: each coarse cell's 2x2x2 sum of the typed cells' A p, in
+            // AccumulateToParents128's (ii, jj, kk) order.  The thread holds (ii, jj) = (0, 0) of
+            // the coarse cells over its cells' pairs (kk = 0, 1); the threads t ^ 2 (jj = 1),
+            // t ^ 16 (ii = 1) and t ^ 18 hold the others -- in the same warp.
             const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + (size_t)tile[u] * kTileCells + t * 4);
+            float a[4], bj[4], bi[4], bij[4];
 #pragma unroll
-            for (int e = 0; e < 4; e++) ts.b[t * 4 + e] = ((ct4 >> (8 * e)) & (INTERIOR_C | DIRICHLET_C | NEUMANN_C)) ? out[e] : 0.f;
+            for (int e = 0; e < 4; e++) a[e] = ((ct4 >> (8 * e)) & (INTERIOR_C | DIRICHLET_C | NEUMANN_C)) ? out[e] : 0.f;
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                bj[e] = __shfl_xor_sync(0xffffffffu, a[e], 2);
+                bi[e] = __shfl_xor_sync(0xffffffffu, a[e], 16);
+                bij[e] = __shfl_xor_sync(0xffffffffu, a[e], 18);
+            }
+            const TileIdx ix(t);
+            if (((ix.i | ix.j) & 1) == 0) {
+                const size_t row = (size_t)tp.ghost_slot[tile[u]] * 64;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    float sum = 0.f;
+                    sum += a[2 * h]; sum += a[2 * h + 1];
+                    sum += bj[2 * h]; sum += bj[2 * h + 1];
+                    sum += bi[2 * h]; sum += bi[2 * h + 1];
+                    sum += bij[2 * h]; sum += bij[2 * h + 1];
+                    GACC[row + (ix.i >> 1) * 16 + (ix.j >> 1) * 4 + ((ix.k0 + 2 * h) >> 1)] = sum;
+                }
+            }
         } else {
             V4<float> o;
             o.v[0] = out[0]; o.v[1] = out[1]; o.v[2] = out[2]; o.v[3] = out[3];
@@ -193,36 +217,20 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
             if (WP != nullptr && ts.aux[0] >= 0) reinterpret_cast<float*>(ts.mask)[t] = dot4f32(ld4(ts.xs + t * 4), o);
         }
     }
+    if (WP == nullptr) return;
     __syncthreads();
-    if (t >= 64) {
-        // warps 2 and 3 of each group sum the LEAF tiles' terms, each 16-lane half one tile:
-        // u = 2 * (warp - 2) + half
-        const int u = 2 * ((t - 64) >> 5) + ((t >> 4) & 1);
-        if (WP == nullptr || 2 * ((t - 64) >> 5) >= NT) return;  // whole warps
-        bool ok = false;
+    // warp w of each group sums the LEAF tiles' terms of tiles u = 2w (lanes 0..15) and 2w + 1 (16..31)
+    if (2 * (t >> 5) >= NT) return;  // whole warps
+    const int u = 2 * (t >> 5) + ((t >> 4) & 1);
+    bool ok = false;
 #pragma unroll
-        for (int k = 0; k < NT; k++)
-            if (k == u) ok = act[k] && !ghost[k];
-        const TileStage& ts = st[(u < NT ? u : 0) * TPB + g];
-        const int sl = ts.aux[0];
-        const double d = tile_part_sum(reinterpret_cast<const float*>(ts.mask), t & 15);
-        if (ok && u < NT && sl >= 0 && (t & 15) == 0) WP[sl] = d;
-        return;
-    }
-    const int fi = t / 16 * 2, fj = (t / 4) % 4 * 2, fk = t % 4 * 2;
-#pragma unroll
-    for (int u = 0; u < NT; u++) {
-        if (!act[u] || !ghost[u]) continue;
-        const float* gsum = st[u * TPB + g].b;
-        float sum = 0.f;
-#pragma unroll
-        for (int ii = 0; ii < 2; ii++)
-#pragma unroll
-            for (int jj = 0; jj < 2; jj++)
-#pragma unroll
-                for (int kk = 0; kk < 2; kk++) sum += gsum[(fi + ii) * 64 + (fj + jj) * 8 + (fk + kk)];
-        GACC[(size_t)tp.ghost_slot[tile[u]] * 64 + t] = sum;
-    }}
+    for (int k = 0; k < NT; k++)
+        if (k == u) ok = act[k] && !ghost[k];
+    const LapStage& ts = st[(u < NT ? u : 0) * TPB + g];
+    const int sl = ts.aux[0];
+    const double d = tile_part_sum(reinterpret_cast<const float*>(ts.mask), t & 15);
+    if (ok && u < NT && sl >= 0 && (t & 15) == 0) WP[sl] = d;
+}
 template <int TPB, int NT>
 __global__ void __launch_bounds__(128 * TPB) k_laplacian_fused(Topo tp, const int* __restrict__ list, int n, const int4* __restrict__ items,
                                                                int nitems, int item_blocks,
@@ -1282,8 +1290,8 @@ void laplacian_shape(const DevGrid& g, const float* X, float* Y, const Scalars* 
     const int per = TPB * NT;
     const int item_blocks = (g.n_lapitems + 128 * TPB - 1) / (128 * TPB);
     const auto k = k_laplacian_fused_shape<TPB, NT, MINB>();
-    launch_kernel(k, item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(TileStage) * per, s,
-                  prefetch_topo(g, k, 128 * TPB, sizeof(TileStage) * per, per, prefetch), g.d_lapmain, g.n_lapmain, g.d_lapitems,
+    launch_kernel(k, item_blocks + (g.n_lapmain + per - 1) / per, 128 * TPB, sizeof(LapStage) * per, s,
+                  prefetch_topo(g, k, 128 * TPB, sizeof(LapStage) * per, per, prefetch), g.d_lapmain, g.n_lapmain, g.d_lapitems,
                   g.n_lapitems, item_blocks, X, Y, g.d_gacc, S, WP);
 }
 
@@ -1490,7 +1498,7 @@ void init_stencil_attributes() {
     static std::once_flag once;
     std::call_once(once, [] {
     cudaFuncSetAttribute(k_gs_sweep<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
-    cudaFuncSetAttribute(k_laplacian_fused<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
+    cudaFuncSetAttribute(k_laplacian_fused<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LapStage) * 8);
     cudaFuncSetAttribute(k_residual_restrict<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
     });
 }

@@ -368,11 +368,20 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Staging area of one tile: its values, face halos, a second channel (right-hand side) and the
 // stencil mask bytes.
 struct __align__(16) TileStage {
+    static constexpr bool kHasB = true;
     float xs[kTileCells];
     float hx[6 * 64];
     float b[kTileCells];
     uint8_t mask[kTileCells];
     int aux[4];  // per-tile word copied with the tile (the LEAF slot, for the kernels that form dot partials)
+};
+// The same without the second channel: the fused Laplacian's staging area (4 KB per tile).
+struct __align__(16) LapStage {
+    static constexpr bool kHasB = false;
+    float xs[kTileCells];
+    float hx[6 * 64];
+    uint8_t mask[kTileCells];
+    int aux[4];
 };
 
 // Neighbour tiles whose halo cells thread t copies: face t>>4 (threads 0..63, 16-byte pieces of
@@ -415,11 +424,14 @@ __device__ __forceinline__ void tile_pre(const Topo& tp, const int (&tile)[NT], 
 // Issue the copies of `tile` into st: channel X's values and face halos (0 for absent
 // neighbours), channel B (if given) and the mask bytes (if given).  Completed by
 // cp_async_wait_all + __syncthreads.
+template <class Stage>
 __device__ __forceinline__ void stage_async(const float* __restrict__ X, const float* __restrict__ B, const uint8_t* __restrict__ mask,
-                                            int tile, HaloNb nb, int t, TileStage& st) {
+                                            int tile, HaloNb nb, int t, Stage& st) {
     const size_t base = (size_t)tile * kTileCells;
     cp_async16(st.xs + t * 4, X + base + t * 4);
-    if (B) cp_async16(st.b + t * 4, B + base + t * 4);
+    if constexpr (Stage::kHasB) {
+        if (B) cp_async16(st.b + t * 4, B + base + t * 4);
+    }
     if (mask && t < 32) cp_async16(st.mask + t * 16, mask + base + t * 16);
     if (t < 64) {
         const int face = t >> 4, q = t & 15;
