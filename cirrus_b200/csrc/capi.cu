@@ -737,7 +737,8 @@ cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int le
     auto& g = *grid->g;
     if (kernel != -1 && shape_kind(kernel) < 0) return CIRRUS_ERR_INVALID_ARGUMENT;
     // shapes past the common eight exist for the Laplacian only
-    if (shape >= (kernel == -1 ? cirrus::kNumShapes : cirrus::num_shapes(shape_kind(kernel)))) return CIRRUS_ERR_INVALID_ARGUMENT;
+    // kernel -1 (all kernels): the shapes every kernel shares, 0..7
+    if (shape >= (kernel == -1 ? cirrus::kCommonShapes : cirrus::num_shapes(shape_kind(kernel)))) return CIRRUS_ERR_INVALID_ARGUMENT;
     if (level < -1 || level >= g.num_layers) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] {
         for (int k = 0; k < cirrus::KS_COUNT; k++) {

@@ -1362,7 +1362,11 @@ void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, 
     case 8: gs_sweep_shape<1, 4>(g, level, X, R, color, S, s, RD, true); break;
     case 9: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s, RD, true); break;
     case 10: gs_sweep_shape<1, 1, 16>(g, level, X, R, color, S, s, RD, true); break;
-    default: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s, RD, true); break;
+    case 11: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s, RD, true); break;
+    // 12, 13: two or four tiles in flight per group with registers capped for 12 or 8 CTAs per SM,
+    // prefetching
+    case 12: gs_sweep_shape<1, 2, 12>(g, level, X, R, color, S, s, RD, true); break;
+    default: gs_sweep_shape<1, 4, 8>(g, level, X, R, color, S, s, RD, true); break;
     }
 }
 
@@ -1410,7 +1414,9 @@ void residual_restrict(const DevGrid& g, int level, const float* X, const float*
     case 8: residual_shape<1, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
     case 9: residual_shape<1, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
     case 10: residual_shape<1, 1, 16>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
-    default: residual_shape<2, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
+    case 11: residual_shape<2, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
+    case 12: residual_shape<1, 2, 12>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
+    default: residual_shape<1, 4, 8>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
     }
 }
 
