@@ -1321,6 +1321,9 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
     case 17: laplacian_shape<2, 4>(g, X, Y, S, s, WP, true); break;
     case 18: laplacian_shape<1, 2>(g, X, Y, S, s, WP, true); break;
     case 19: laplacian_shape<2, 2>(g, X, Y, S, s, WP, true); break;
+    // 20: shape 2 prefetching with registers capped for 8 CTAs per SM (and the shared-memory
+    // carveout that fits them)
+    case 20: laplacian_shape<1, 4, 8>(g, X, Y, S, s, WP, true); break;
     default: laplacian_shape<2, 2>(g, X, Y, S, s, WP); break;  // shape 1 (the TMA shapes without tensor maps)
     }
 }
@@ -1505,6 +1508,7 @@ void init_stencil_attributes() {
     std::call_once(once, [] {
     cudaFuncSetAttribute(k_gs_sweep<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
     cudaFuncSetAttribute(k_laplacian_fused<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LapStage) * 8);
+    cudaFuncSetAttribute(k_laplacian_fused_occ<1, 4, 8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_residual_restrict<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
     });
 }

@@ -64,8 +64,9 @@ constexpr int kNumShapes = 14;
 constexpr int kCommonShapes = 8;
 // the Laplacian's 8..11 are instead the TMA-staged pipeline (lap_tma.cu) with (consumer groups,
 // stages) = (2, 8), (4, 16), (2, 12), (1, 6); then 12..15 eight cells per thread (lap8.cu), 16..19
-// shapes 2, 3, 5, 1 prefetching into L2 the tiles of CTAs one resident wave ahead
-constexpr int kNumLapShapes = 20;
+// shapes 2, 3, 5, 1 prefetching into L2 the tiles of CTAs one resident wave ahead; 20 shape 2
+// prefetching with registers capped for 8 CTAs per SM
+constexpr int kNumLapShapes = 21;
 constexpr int kFirstTmaShape = 8;
 constexpr int kFirstLap8Shape = 12;
 inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kNumShapes; }

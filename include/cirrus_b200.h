@@ -450,10 +450,11 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
  * group, registers capped for 12 or 8 CTAs per SM).  The Laplacian adds 8..11, its TMA-staged
  * pipeline (persistent CTAs, one producer warp issuing bulk tensor copies of each tile and its
  * halos into a ring of shared-memory stages, 1-4 consumer groups), 12..15, a column of eight cells
- * per thread (64 threads per tile), and 16..19, shapes 2, 3, 5 and 1 prefetching into L2.  Lets a
+ * per thread (64 threads per tile), 16..19, shapes 2, 3, 5 and 1 prefetching into L2, and 20,
+ * shape 2 prefetching with registers capped for 8 CTAs per SM.  Lets a
  * caller reuse tuned shapes for grids of the same structure or pin one.  Shapes never change
  * results.  No counterpart in the reference. */
-#define CIRRUS_NUM_LAUNCH_SHAPES 20
+#define CIRRUS_NUM_LAUNCH_SHAPES 21
 cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape);
 cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int level, int* shape);
 

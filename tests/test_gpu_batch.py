@@ -188,7 +188,7 @@ def test_tma_and_column_laplacian_shapes_give_the_same_bits(built_cache, names):
     g = DeviceGrid([b.topology for b in bs])
     s = GMGSolver()
     out = []
-    shapes = (1, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19)
+    shapes = (1, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20)
     for shape in shapes:
         g.set_launch_shape(shape, KERNEL_LAPLACIAN)
         assert g.get_launch_shape(KERNEL_LAPLACIAN, 0) == shape
