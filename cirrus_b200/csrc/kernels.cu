@@ -1321,9 +1321,6 @@ void laplacian_fused(const DevGrid& g, const float* X, float* Y, const Scalars* 
     case 17: laplacian_shape<2, 4>(g, X, Y, S, s, WP, true); break;
     case 18: laplacian_shape<1, 2>(g, X, Y, S, s, WP, true); break;
     case 19: laplacian_shape<2, 2>(g, X, Y, S, s, WP, true); break;
-    // 20: shape 2 prefetching with registers capped for 8 CTAs per SM (and the shared-memory
-    // carveout that fits them)
-    case 20: laplacian_shape<1, 4, 8>(g, X, Y, S, s, WP, true); break;
     default: laplacian_shape<2, 2>(g, X, Y, S, s, WP); break;  // shape 1 (the TMA shapes without tensor maps)
     }
 }
@@ -1365,11 +1362,7 @@ void gs_sweep(const DevGrid& g, int level, float* X, const float* R, int color, 
     case 8: gs_sweep_shape<1, 4>(g, level, X, R, color, S, s, RD, true); break;
     case 9: gs_sweep_shape<1, 2>(g, level, X, R, color, S, s, RD, true); break;
     case 10: gs_sweep_shape<1, 1, 16>(g, level, X, R, color, S, s, RD, true); break;
-    case 11: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s, RD, true); break;
-    // 12, 13: two or four tiles in flight per group with registers capped for 12 or 8 CTAs per SM,
-    // prefetching
-    case 12: gs_sweep_shape<1, 2, 12>(g, level, X, R, color, S, s, RD, true); break;
-    default: gs_sweep_shape<1, 4, 8>(g, level, X, R, color, S, s, RD, true); break;
+    default: gs_sweep_shape<2, 2>(g, level, X, R, color, S, s, RD, true); break;
     }
 }
 
@@ -1417,9 +1410,7 @@ void residual_restrict(const DevGrid& g, int level, const float* X, const float*
     case 8: residual_shape<1, 4>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
     case 9: residual_shape<1, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
     case 10: residual_shape<1, 1, 16>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
-    case 11: residual_shape<2, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
-    case 12: residual_shape<1, 2, 12>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
-    default: residual_shape<1, 4, 8>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
+    default: residual_shape<2, 2>(g, level, X, RHS, C, one_over_alpha, S, s, ghosts_zero, true); break;
     }
 }
 
@@ -1508,7 +1499,6 @@ void init_stencil_attributes() {
     std::call_once(once, [] {
     cudaFuncSetAttribute(k_gs_sweep<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
     cudaFuncSetAttribute(k_laplacian_fused<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LapStage) * 8);
-    cudaFuncSetAttribute(k_laplacian_fused_occ<1, 4, 8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_residual_restrict<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileStage) * 8);
     });
 }

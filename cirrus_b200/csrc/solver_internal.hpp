@@ -58,15 +58,13 @@ struct GraphKey {
 // shape computes each tile with the same operations.
 enum { KS_GS_SWEEP = 0, KS_PRESMOOTH = 1, KS_PROLONG = 2, KS_RESIDUAL = 3, KS_LAPLACIAN = 4, KS_COUNT = 5 };
 // shapes 0..7: (tiles per CTA, tiles in flight per group, minimum CTAs per SM); 8..11 four of
-// them prefetching the tiles of CTAs one resident wave ahead into L2; 12, 13 prefetching with two
-// or four tiles per group and registers capped for 12 or 8 CTAs per SM
-constexpr int kNumShapes = 14;
+// them prefetching the tiles of CTAs one resident wave ahead into L2
+constexpr int kNumShapes = 12;
 constexpr int kCommonShapes = 8;
 // the Laplacian's 8..11 are instead the TMA-staged pipeline (lap_tma.cu) with (consumer groups,
 // stages) = (2, 8), (4, 16), (2, 12), (1, 6); then 12..15 eight cells per thread (lap8.cu), 16..19
-// shapes 2, 3, 5, 1 prefetching into L2 the tiles of CTAs one resident wave ahead; 20 shape 2
-// prefetching with registers capped for 8 CTAs per SM
-constexpr int kNumLapShapes = 21;
+// shapes 2, 3, 5, 1 prefetching into L2 the tiles of CTAs one resident wave ahead
+constexpr int kNumLapShapes = 20;
 constexpr int kFirstTmaShape = 8;
 constexpr int kFirstLap8Shape = 12;
 inline int num_shapes(int kind) { return kind == KS_LAPLACIAN ? kNumLapShapes : kNumShapes; }

@@ -655,11 +655,7 @@ void presmooth(const DevGrid& g, int level, float* XP, const float* RHS, const S
     case 8: presmooth_shape<1, 4>(g, level, XP, RHS, S, s, true); break;
     case 9: presmooth_shape<1, 2>(g, level, XP, RHS, S, s, true); break;
     case 10: presmooth_shape<1, 1, 16>(g, level, XP, RHS, S, s, true); break;
-    case 11: presmooth_shape<2, 2>(g, level, XP, RHS, S, s, true); break;
-    // 12, 13: two or four tiles in flight per group with registers capped for 12 or 8 CTAs per SM,
-    // prefetching
-    case 12: presmooth_shape<1, 2, 12>(g, level, XP, RHS, S, s, true); break;
-    default: presmooth_shape<1, 4, 8>(g, level, XP, RHS, S, s, true); break;
+    default: presmooth_shape<2, 2>(g, level, XP, RHS, S, s, true); break;
     }
 }
 
@@ -693,9 +689,7 @@ void prolong_sweep(const DevGrid& g, int level, float* Z, const float* XP, const
     case 8: prolong_shape<1, 4>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
     case 9: prolong_shape<1, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
     case 10: prolong_shape<1, 1, 16>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
-    case 11: prolong_shape<2, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
-    case 12: prolong_shape<1, 2, 12>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
-    default: prolong_shape<1, 4, 8>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
+    default: prolong_shape<2, 2>(g, level, Z, XP, RHS, prolong_coeff, S, s, true); break;
     }
 }
 

@@ -446,15 +446,13 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
  * all of them, shapes 0..7 only), level a level of the grid (or -1: all levels; the Laplacian
  * has one entry, level 0).  Shapes 0..7 (tiles per CTA, tiles in flight per thread group, minimum CTAs per SM)
  * exist for every kernel.  The V-cycle kernels add 8..11 (four of them also prefetching into L2
- * the tiles of the CTAs one resident wave later) and 12, 13 (prefetching, two or four tiles per
- * group, registers capped for 12 or 8 CTAs per SM).  The Laplacian adds 8..11, its TMA-staged
+ * the tiles of the CTAs one resident wave later).  The Laplacian adds 8..11, its TMA-staged
  * pipeline (persistent CTAs, one producer warp issuing bulk tensor copies of each tile and its
  * halos into a ring of shared-memory stages, 1-4 consumer groups), 12..15, a column of eight cells
- * per thread (64 threads per tile), 16..19, shapes 2, 3, 5 and 1 prefetching into L2, and 20,
- * shape 2 prefetching with registers capped for 8 CTAs per SM.  Lets a
+ * per thread (64 threads per tile), and 16..19, shapes 2, 3, 5 and 1 prefetching into L2.  Lets a
  * caller reuse tuned shapes for grids of the same structure or pin one.  Shapes never change
  * results.  No counterpart in the reference. */
-#define CIRRUS_NUM_LAUNCH_SHAPES 21
+#define CIRRUS_NUM_LAUNCH_SHAPES 20
 cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape);
 cirrus_status cirrus_grid_get_launch_shape(cirrus_grid* grid, int kernel, int level, int* shape);
 
