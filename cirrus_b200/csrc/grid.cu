@@ -477,7 +477,9 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
                         lo[a] = std::min(lo[a], t5[5 * t + 1 + a]);
                         hi[a] = std::max(hi[a], t5[5 * t + 1 + a]);
                     }
-                const long long ex = 8LL * (hi[0] - lo[0] + 1) + 2, ey = 8LL * (hi[1] - lo[1] + 1) + 2, ez = 8LL * (hi[2] - lo[2] + 1) + 2;
+                // z rows carry two unused cells after the halo: a row stride of 4 mod 8 floats puts
+                // the 32 cells of one colour that a warp sweeps (8 rows x 4) in 32 different banks
+                const long long ex = 8LL * (hi[0] - lo[0] + 1) + 2, ey = 8LL * (hi[1] - lo[1] + 1) + 2, ez = 8LL * (hi[2] - lo[2] + 1) + 4;
                 if (ex > (1 << 15) || ey > (1 << 15) || ez > (1 << 15)) break;
                 const long long c = ex * ey * ez;
                 if (launch::bottom_smem_bytes(acc + c + 8, tiles + icnt[i][l]) > (size_t)launch::kBottomSmemBudget) break;

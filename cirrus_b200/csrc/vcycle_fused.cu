@@ -508,6 +508,58 @@ __device__ __forceinline__ float box_neglap(const float* X, int q, uint32_t code
     return interior ? s * L.h * L.h * L.h : 0.f;
 }
 
+// One cell of a sweep colour with its stencil coefficients, diagonal and right-hand side held in
+// registers over a run of sweeps on one level (the level's right-hand side and codes do not change
+// during the run): what box_neglap<true> and the sweep update derive from the codes every sweep.
+struct SweepCell {
+    int q;  // box index; -1: no cell (GHOST tile or beyond the colour's items)
+    float a[6], d, b;
+    bool interior;
+};
+__device__ __forceinline__ void sweep_cell_load(SweepCell& c, const int4* T, const float* B, const uint16_t* CODE, int first, int it,
+                                                int n, int color, int sy, int sz, const LevelConst<float>& L) {
+    c.q = -1;
+    if (it >= n) return;
+    const int4 r = T[first + (it >> 8)];
+    if (r.z & GHOST_T) return;
+    const int u = it & 255;
+    const int i = u >> 5, j = (u >> 2) & 7, k = ((u & 3) << 1) | ((i + j + color) & 1);
+    c.q = r.x + i * sy + j * sz + k;
+    const uint32_t code = CODE[c.q];
+    c.b = B[c.q];
+    c.interior = code & kMaskInterior;
+    if ((code & 0x1FFFu) == (uint32_t)kMaskFull) {
+#pragma unroll
+        for (int f = 0; f < 6; f++) c.a[f] = L.c1;
+        c.d = L.dfast;
+        return;
+    }
+    float d = 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        c.a[f] = ((code >> f) & 1u) ? (((code >> (7 + f)) & 1u) ? L.c2 : L.c1) : 0.f;
+        d = d + c.a[f];
+    }
+    c.d = c.interior ? mul_h3(d, L.h) : 0.f;
+}
+// the sweep update of box_neglap<true> + X += (B - Ax) / D with the cached terms: the same
+// operations in the same order
+__device__ __forceinline__ void sweep_cell_update(const SweepCell& c, float* X, int sy, int sz, const LevelConst<float>& L) {
+    if (c.q < 0) return;
+    const int q = c.q;
+    const float x0 = X[q];
+    const float xm = X[q - sy], xp = X[q + sy], ym = X[q - sz], yp = X[q + sz], zm = X[q - 1], zp = X[q + 1];
+    float s = 0.f;
+    s = fmaf(c.a[0], x0 - xm, s);
+    s = fmaf(c.a[1], x0 - xp, s);
+    s = fmaf(c.a[2], x0 - ym, s);
+    s = fmaf(c.a[3], x0 - yp, s);
+    s = fmaf(c.a[4], x0 - zm, s);
+    s = fmaf(c.a[5], x0 - zp, s);
+    const float ax = c.interior ? mul_h3(s, L.h) : 0.f;
+    X[q] = x0 + (c.interior ? (c.b - ax) / c.d : 0.f);
+}
+
 namespace launch {
 size_t bottom_smem_bytes(long long cells, int tiles) {
     return (size_t)tiles * sizeof(int4) + (size_t)cells * (2 * sizeof(float) + sizeof(uint16_t)) + 16;
@@ -557,6 +609,22 @@ __global__ void __launch_bounds__(1024) k_bottom(Topo tp, const BottomInst* __re
         const int op = prog.op[ph], level = prog.level[ph];
         const LevelConst<float> L(lcs[level]);
         const int sy = bi.sy[level], sz = bi.sz[level], first = bi.first[level];
+        if (op == 1 && bi.cnt[level] * 256 <= (int)blockDim.x && ph + 1 < prog.nphase && prog.op[ph + 1] == 1 &&
+            prog.level[ph + 1] == level) {
+            // a run of sweeps on a level whose colours have at most one cell per thread (the
+            // coarsest level's coarsest_iters sweeps): each thread keeps its cell of either colour
+            SweepCell cell[2];
+            const int n = bi.cnt[level] * 256;
+            sweep_cell_load(cell[0], T, B, CODE, first, threadIdx.x, n, 0, sy, sz, L);
+            sweep_cell_load(cell[1], T, B, CODE, first, threadIdx.x, n, 1, sy, sz, L);
+            for (; ph < prog.nphase && prog.op[ph] == 1 && prog.level[ph] == level; ph++) {
+                if (prog.color[ph] & 1) sweep_cell_update(cell[1], X, sy, sz, L);
+                else sweep_cell_update(cell[0], X, sy, sz, L);
+                __syncthreads();
+            }
+            ph--;
+            continue;
+        }
         if (op == 1) {
             // one colour of GaussSeidelGMG on the level's LEAF|NONLEAF tiles; items are the 256 cells
             // of the colour (a warp covers one (tile, i) plane), whose neighbours all have the other colour
