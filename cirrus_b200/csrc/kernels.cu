@@ -131,8 +131,9 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
                                                                double* __restrict__ WP) {
     // the dot-part tail below gives tile u to 16-lane half (u & 1) of warp u >> 1: NT <= 8
     static_assert(NT >= 1 && NT <= 8, "k_laplacian_fused: the tile-part tail covers at most 8 tiles per group");
-    pdl_entry();
+    pdl_trigger();
     if ((int)blockIdx.x < item_blocks) {
+        pdl_wait();
         const int q = (int)blockIdx.x * (128 * TPB) + (int)threadIdx.x;
         if (q >= nitems) return;
         const int4 it = items[q];
@@ -157,9 +158,13 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (act[u]) {
-            stage_async(X, nullptr, tp.mask_lap, tile[u], pre[u].nb, t, st[u * TPB + g]);
+            stage_mask_async(tp.mask_lap, tile[u], t, st[u * TPB + g]);
             if (WP != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
         }
+    pdl_wait();
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (act[u]) stage_async(X, nullptr, nullptr, tile[u], pre[u].nb, t, st[u * TPB + g]);
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (ptile[u] >= 0) {
@@ -302,7 +307,7 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
                                                         const float* __restrict__ RD, double* __restrict__ WP) {
     // the dot-part tail gives tile u to 16-lane half (u & 1) of warp 2 + (u >> 1): NT <= 4
     static_assert(NT >= 1 && NT <= 4, "k_gs_sweep: the tile-part tail covers at most 4 tiles per group");
-    pdl_entry();
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char gs_smem[];
     TileStage* st = reinterpret_cast<TileStage*>(gs_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
@@ -320,9 +325,13 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (act[u]) {
-            stage_async(X, R, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
+            stage_mask_async(tp.mask_mg, tile[u], t, st[u * TPB + g]);
             if (RD != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
         }
+    pdl_wait();
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (act[u]) stage_async(X, R, nullptr, tile[u], pre[u].nb, t, st[u * TPB + g]);
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (ptile[u] >= 0) {
@@ -499,8 +508,9 @@ __device__ __forceinline__ void k_residual_restrict_body(Topo tp, int first, con
                                                                  const int4* __restrict__ items, int nitems, int item_blocks,
                                                                  const float* __restrict__ X, const float* RHS, float* C,
                                                                  float one_over_alpha, const Scalars* __restrict__ S) {
-    pdl_entry();
+    pdl_trigger();
     if ((int)blockIdx.x < item_blocks) {
+        pdl_wait();
         const int q = (int)blockIdx.x * (128 * TPB) + (int)threadIdx.x;
         if (q >= nitems) return;
         const int4 it = items[q];
@@ -525,7 +535,11 @@ __device__ __forceinline__ void k_residual_restrict_body(Topo tp, int first, con
     tile_pre(tp, tile, t, pre);
 #pragma unroll
     for (int u = 0; u < NT; u++)
-        if (act[u]) stage_async(X, RHS, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
+        if (act[u]) stage_mask_async(tp.mask_mg, tile[u], t, st[u * TPB + g]);
+    pdl_wait();
+#pragma unroll
+    for (int u = 0; u < NT; u++)
+        if (act[u]) stage_async(X, RHS, nullptr, tile[u], pre[u].nb, t, st[u * TPB + g]);
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (ptile[u] >= 0) {

@@ -76,7 +76,7 @@ struct __align__(16) PreStage {
 template <int TPB, int NT>
 __device__ __forceinline__ void k_presmooth_body(Topo tp, const int* __restrict__ list, int n, float* XP,
                                                          const float* __restrict__ RHS, const Scalars* __restrict__ S) {
-    pdl_entry();
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char pre_smem[];
     PreStage* st = reinterpret_cast<PreStage*>(pre_smem);
     const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
@@ -127,12 +127,17 @@ __device__ __forceinline__ void k_presmooth_body(Topo tp, const int* __restrict_
         if (!act[u]) continue;
         PreStage& ps = st[u * TPB + g];
         const size_t base = (size_t)tile[u] * kTileCells;
-        cp_async16(ps.b + t * 4, RHS + base + t * 4);
         if (t < 32) cp_async16(ps.mask + t * 16, tp.mask_mg + base + t * 16);
-        if (nbf[u] >= 0) {
-            cp_async16(ps.hx + fface * 64 + qq * 4, RHS + (size_t)nbf[u] * kTileCells + foff);
-            cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + (size_t)nbf[u] * kTileCells + foff);
-        }
+        if (nbf[u] >= 0) cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + (size_t)nbf[u] * kTileCells + foff);
+    }
+    pdl_wait();
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        if (!act[u]) continue;
+        PreStage& ps = st[u * TPB + g];
+        const size_t base = (size_t)tile[u] * kTileCells;
+        cp_async16(ps.b + t * 4, RHS + base + t * 4);
+        if (nbf[u] >= 0) cp_async16(ps.hx + fface * 64 + qq * 4, RHS + (size_t)nbf[u] * kTileCells + foff);
         if (nbz[u] >= 0) cp_async4(ps.hx + zface * 64 + zc, RHS + (size_t)nbz[u] * kTileCells + zoff);
     }
 #pragma unroll
@@ -263,8 +268,9 @@ __device__ __forceinline__ void k_prolong_sweep_body(Topo tp, const int* __restr
                                                              const int4* __restrict__ items, int nitems, int item_blocks, float* Z,
                                                              const float* __restrict__ XP, const float* __restrict__ RHS,
                                                              float prolong_coeff, const Scalars* __restrict__ S) {
-    pdl_entry();
+    pdl_trigger();
     if ((int)blockIdx.x < item_blocks) {
+        pdl_wait();
         const int q = (int)blockIdx.x * (2 * TPB) + ((int)threadIdx.x >> 6);
         if (q >= nitems) return;
         const int4 it = items[q];
@@ -342,6 +348,14 @@ __device__ __forceinline__ void k_prolong_sweep_body(Topo tp, const int* __restr
         ProStage& ps = st[u * TPB + g];
         const size_t base = (size_t)tile[u] * kTileCells;
         if (t < 32) cp_async16(ps.mask + t * 16, tp.mask_mg + base + t * 16);
+        if (nbf[u] >= 0) cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + (size_t)nbf[u] * kTileCells + foff);
+    }
+    pdl_wait();
+#pragma unroll
+    for (int u = 0; u < NT; u++) {
+        if (!act[u]) continue;
+        ProStage& ps = st[u * TPB + g];
+        const size_t base = (size_t)tile[u] * kTileCells;
         if (!ghost[u]) {
             cp_async16(ps.xp + t * 4, XP + base + t * 4);
             cp_async16(ps.b + t * 4, RHS + base + t * 4);
@@ -354,7 +368,6 @@ __device__ __forceinline__ void k_prolong_sweep_body(Topo tp, const int* __restr
         if (nbf[u] >= 0) {
             const size_t nbase = (size_t)nbf[u] * kTileCells;
             if (!(hf[u] & 2u)) cp_async16(ps.hxp + fface * 64 + qq * 4, XP + nbase + foff);
-            cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + nbase + foff);
             if (fpar[u] >= 0)
                 cp_async8(ps.hpar + (fface * 16 + qq) * 2, Z + (size_t)fpar[u] * kTileCells + parent_cell((hf[u] >> 8) & 7u, foff));
         }
@@ -570,12 +583,13 @@ __global__ void __launch_bounds__(1024) k_bottom(Topo tp, const BottomInst* __re
                                                  const uint16_t* __restrict__ codes, float* Z, const float* __restrict__ RHS,
                                                  float one_over_alpha, float prolong_coeff, BottomProgram prog,
                                                  const Scalars* __restrict__ S) {
-    pdl_entry();
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char bsm[];
     __shared__ BottomInst bi;
     __shared__ float4 lcs[kBottomMaxLevels];  // the instance's level constants, read once
     const int inst = blockIdx.x;
-    if (S && S[inst].done) return;
+    // the boxes' records, codes and zeroed x / right-hand sides come from the topology: set up
+    // before pdl_wait
     if (threadIdx.x == 0) bi = insts[inst];
     if (threadIdx.x < kBottomMaxLevels) lcs[threadIdx.x] = tp.lconst[inst * kLevelSlots + threadIdx.x];
     __syncthreads();
@@ -593,6 +607,8 @@ __global__ void __launch_bounds__(1024) k_bottom(Topo tp, const BottomInst* __re
     for (int v = threadIdx.x; v < cells / 8; v += blockDim.x)
         reinterpret_cast<uint4*>(CODE)[v] = reinterpret_cast<const uint4*>(codes + bi.code_off)[v];
     __syncthreads();
+    pdl_wait();
+    if (S && S[inst].done) return;
     // right-hand sides of the non-GHOST tiles (GHOST right-hand sides are 0); a tile row of 8
     // cells is contiguous in its box
     for (int v = threadIdx.x; v < nb * 128; v += blockDim.x) {
