@@ -915,8 +915,9 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
                                                      const int2* __restrict__ inst_chunks, float* A, float* B, float* C, float* D,
                                                      Scalars* S, const InstParams* __restrict__ ip, SolveCtl ctl, int epi,
                                                      double* partials, unsigned int* counters, int skip) {
-    pdl_entry();
-    const int4 ch = chunks[blockIdx.x];
+    pdl_trigger();
+    const int4 ch = chunks[blockIdx.x];  // topology: read before pdl_wait
+    pdl_wait();
     const int inst = ch.x;
     Scalars* Si = S + inst;
     const InstParams P = ip[inst];
@@ -965,12 +966,16 @@ __global__ void __launch_bounds__(256) k_inst_reduce(Topo tp, const int* __restr
 // the 4-cell vectors j, j+16, ..., j+112.
 __global__ void __launch_bounds__(256) k_leaf_wpart(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ R,
                                                     const float* __restrict__ Z, double* __restrict__ WP, const Scalars* S) {
-    pdl_entry();
+    pdl_trigger();
     const int w = (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5);
-    if (2 * w >= n) return;  // whole warps
+    if (2 * w >= n) {  // whole warps
+        pdl_wait();
+        return;
+    }
     const int j = threadIdx.x & 15;
     const int q = 2 * w + ((threadIdx.x >> 4) & 1);
-    const int tile = list[q < n ? q : 2 * w];
+    const int tile = list[q < n ? q : 2 * w];  // topology: read before pdl_wait
+    pdl_wait();
     const bool ok = q < n && !tile_done(tp, S, tile);
     const size_t base = (size_t)tile * kTileCells + j * 4;
     float term[8];
@@ -988,12 +993,16 @@ __global__ void __launch_bounds__(256) k_leaf_wpart(Topo tp, const int* __restri
 __global__ void __launch_bounds__(256) k_pap_ghost(Topo tp, const int* __restrict__ list, int n, const float* __restrict__ P,
                                                    float* AP, const float* __restrict__ GACC, double* __restrict__ WP,
                                                    const Scalars* S) {
-    pdl_entry();
+    pdl_trigger();
     const int w = (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5);
-    if (2 * w >= n) return;  // whole warps
+    if (2 * w >= n) {  // whole warps
+        pdl_wait();
+        return;
+    }
     const int j = threadIdx.x & 15;
     const int q = 2 * w + ((threadIdx.x >> 4) & 1);
-    const int tile = list[q < n ? q : 2 * w];
+    const int tile = list[q < n ? q : 2 * w];  // topology: read before pdl_wait
+    pdl_wait();
     const bool ok = q < n && !tile_done(tp, S, tile);
     float term[8];
 #pragma unroll
@@ -1021,13 +1030,14 @@ __global__ void __launch_bounds__(256) k_pap_ghost(Topo tp, const int* __restric
 // only the instance's own tiles.
 __global__ void __launch_bounds__(256) k_inst_wsum(const int2* __restrict__ ranges, const double* __restrict__ WP, Scalars* S,
                                                    const InstParams* __restrict__ ip, SolveCtl ctl, int epi, int skip) {
-    pdl_entry();
+    pdl_trigger();
     __shared__ double ws[8];
     const int inst = blockIdx.x;
+    const int2 r = ranges[inst];  // topology: read before pdl_wait
+    pdl_wait();
     Scalars* Si = S + inst;
     const InstParams P = ip[inst];
     if (!P.active || (skip == SKIP_DONE && Si->done)) return;
-    const int2 r = ranges[inst];
     const double* w = WP + r.x;
     double acc = 0.0;
 #pragma unroll 4
@@ -1073,16 +1083,21 @@ __global__ void __launch_bounds__(256) k_begin(Scalars* S, const InstParams* __r
 // its instance's state is read, so the loads do not wait on that lookup.
 __global__ void __launch_bounds__(256) k_update_p(Topo tp, const int* __restrict__ leaves, int nleaf, float* P,
                                                   const float* __restrict__ Z, float* X, const Scalars* S) {
-    pdl_entry();
+    pdl_trigger();
     const int q = (int)blockIdx.x * 2 + ((int)threadIdx.x >> 7);
-    if (q >= nleaf) return;
+    if (q >= nleaf) {
+        pdl_wait();
+        return;
+    }
     const int t = threadIdx.x & 127;
-    const int tile = leaves[q];
+    const int tile = leaves[q];  // topology: read before pdl_wait
     const size_t off = (size_t)tile * kTileCells + t * 4;
     const uint32_t ct4 = *reinterpret_cast<const uint32_t*>(tp.ctype + off);
+    const int inst = tp.inst[tile];
+    pdl_wait();
     V4<float> p = ld4(P + off), x = ld4(X + off);
     const V4<float> z = ld4(Z + off);
-    const Scalars& Si = S[tp.inst[tile]];
+    const Scalars& Si = S[inst];
     if (Si.done) return;
     const float alpha = (float)Si.alpha, beta = (float)Si.beta;
 #pragma unroll
