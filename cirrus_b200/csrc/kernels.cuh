@@ -20,16 +20,17 @@ namespace cirrus {
 // serialisation (launch_kernel), so a kernel's CTAs may be scheduled while its predecessor is
 // still running.  Every kernel first allows its own successor to be scheduled, then waits until
 // its predecessor grid has completed and that grid's memory operations are visible, before it
-// reads or writes anything; so results are those of plain stream order.  Without the launch
-// attribute both instructions return at once.
+// reads or writes any data a kernel writes; so results are those of plain stream order.
+// Without the launch attribute both instructions return at once.
 __device__ __forceinline__ void pdl_entry() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     asm volatile("griddepcontrol.wait;" ::: "memory");
 }
-// The same two steps apart, for the stencil kernels: between them a kernel reads only the grid's
-// topology (tile lists, metadata, coefficient classes, level constants, stencil masks), which is
-// written once when the grid is created and never by a kernel, and writes only its own shared
-// memory -- so that part overlaps the predecessor's tail without changing any result.
+// The same two steps apart, for the stencil, coarse-level and vector kernels: between them a
+// kernel reads only the grid's topology (tile lists, metadata, coefficient classes, level
+// constants, stencil masks, chunk and range tables, coarse-level boxes), which is written once
+// when the grid is created and never by a kernel, and writes only its own shared memory -- so
+// that part overlaps the predecessor's tail without changing any result.
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
