@@ -215,7 +215,8 @@ namespace launch {
 bool pdl_enabled();
 // Launches kernel k on stream s with programmatic stream serialisation: the kernel may be
 // scheduled while its predecessor finishes; the kernel itself waits for the predecessor's
-// completion (pdl_entry) before touching memory.
+// completion (pdl_entry, or pdl_wait after its topology loads) before touching data that a
+// kernel writes.
 template <class... KArgs, class... Args>
 inline void launch_kernel(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
     cudaLaunchConfig_t cfg = {};
