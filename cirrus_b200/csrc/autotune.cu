@@ -48,7 +48,8 @@ float time_graph(F launch, int reps, cudaStream_t s) {
 // launches each bound by its own latency (one instance or a few): there, timing a kernel alone in
 // back-to-back launches measures overlapped throughput, not its place in the chain.  Candidates:
 // the per-kernel picks; each of the eight common shapes for every kernel; then, per kernel kind,
-// each of its shapes on all its levels.  Each is timed as a fixed-length solve (8 PCG iterations
+// each of its shapes on all its levels; then, level by level from the finest, each shape of each
+// V-cycle kernel.  Each is timed as a fixed-length solve (8 PCG iterations
 // of the grid's own right-hand sides, graph-launched, best of 3) and kept if it gains more than
 // 0.5 %.  b and x are saved first and restored after; a grid whose right-hand sides end a solve
 // early (zero or non-finite) is left as tuned.
@@ -109,6 +110,18 @@ static void refine_by_solve(DevGrid& g, cudaStream_t s) {
                 consider(cand);
             }
         }
+        // then the V-cycle kernels level by level, finest first
+        const int lo = g.bottom_level + 1;
+        for (int l = g.max_level; l >= lo; l--)
+            for (int kind : {KS_GS_SWEEP, KS_PRESMOOTH, KS_PROLONG, KS_RESIDUAL}) {
+                const std::vector<uint8_t> base = kept;
+                for (int sh = 0; sh < num_shapes(kind); sh++) {
+                    if (sh == base[(size_t)kind * g.num_layers + l]) continue;
+                    std::vector<uint8_t> cand = base;
+                    cand[(size_t)kind * g.num_layers + l] = (uint8_t)sh;
+                    consider(cand);
+                }
+            }
     }
     g.shapes = kept;
     cudaMemcpyAsync(g.d_ch[kChB], bsave, bytes, cudaMemcpyDeviceToDevice, s);

@@ -409,11 +409,12 @@ cirrus_status cirrus_grid_get_solution_f64(cirrus_grid* grid, double* host, void
  * and keeps the fastest for the following solves.  On grids of at most 16,384 tiles (one
  * instance or a few, where a solve is a chain of latency-bound launches) it then refines the
  * choice with whole solves: 8-iteration solves of the grid's own right-hand sides (channel 1),
- * trying the eight common shapes for every kernel and, per kernel, each shape on all its levels;
- * b and x are restored afterwards (skipped when the right-hand sides end a solve at once).
- * Shapes never change results.  Overwrites channels 2-5 (the solve's scratch); synchronises
- * `stream`; takes about reps x (number of kernels x levels x shapes) launches plus, on small
- * grids, about 60 short solves.  reps <= 0 picks 20. */
+ * trying the eight common shapes for every kernel, per kernel each shape on all its levels, then
+ * per V-cycle kernel and level each shape (about 1-2 s for one ring512 instance); b and x are
+ * restored afterwards (skipped when the right-hand sides end a solve at once).  Shapes never
+ * change results.  Overwrites channels 2-5 (the solve's scratch); synchronises `stream`; takes
+ * about reps x (number of kernels x levels x shapes) launches plus, on small grids, a few hundred
+ * short solves.  reps <= 0 picks 20. */
 cirrus_status cirrus_grid_autotune(cirrus_grid* grid, int reps, void* stream);
 
 /* Sweep-count tuner (no counterpart in the reference, which always runs the caller's
