@@ -53,7 +53,6 @@ float time_graph(F launch, int reps, cudaStream_t s) {
 // of the grid's own right-hand sides, graph-launched, best of 3) and kept if it gains more than
 // 0.5 %.  b and x are saved first and restored after; a grid whose right-hand sides end a solve
 // early (zero or non-finite) is left as tuned.
-constexpr int kSolveRefineTiles = 16384;
 static void refine_by_solve(DevGrid& g, cudaStream_t s) {
     const size_t bytes = (size_t)g.n * kTileCells * sizeof(float);
     float *bsave = nullptr, *xsave = nullptr;
@@ -178,7 +177,7 @@ int autotune(DevGrid& g, cudaStream_t user, int reps, std::string* report) {
             pick(KS_PROLONG, l, [&] { launch::prolong_sweep(g, l, z, g.d_xpre, ap, 1.f, nullptr, s); });
     }
     if (g.n_lapmain + g.n_lapitems > 0) pick(KS_LAPLACIAN, 0, [&] { launch::laplacian_fused(g, p, tmp, nullptr, s, true); });
-    if (g.n <= kSolveRefineTiles && g.bottom_level >= 0) refine_by_solve(g, s);
+    if (g.n <= kSmallGridTiles && g.bottom_level >= 0) refine_by_solve(g, s);
     g.launch_count = count0;
     drop_graphs(g);
     const bool ok = cudaStreamSynchronize(s) == cudaSuccess;

@@ -61,6 +61,10 @@ enum { KS_GS_SWEEP = 0, KS_PRESMOOTH = 1, KS_PROLONG = 2, KS_RESIDUAL = 3, KS_LA
 // them prefetching the tiles of CTAs one resident wave ahead into L2
 constexpr int kNumShapes = 12;
 constexpr int kCommonShapes = 8;
+// Grids of at most this many tiles (one instance or a few) are chains of latency-bound launches:
+// they start with one tile per 128-thread CTA (shape 4) rather than shape 1, and the autotuner
+// refines their shapes with whole solves.
+constexpr int kSmallGridTiles = 16384;
 // the Laplacian's 8..11 are instead the TMA-staged pipeline (lap_tma.cu) with (consumer groups,
 // stages) = (2, 8), (4, 16), (2, 12), (1, 6); then 12..15 eight cells per thread (lap8.cu), 16..19
 // shapes 2, 3, 5, 1 prefetching into L2 the tiles of CTAs one resident wave ahead
