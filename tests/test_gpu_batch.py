@@ -151,6 +151,35 @@ def test_autotune_changes_timing_not_results(built_cache):
     g.close()
 
 
+def test_autotune_whole_solve_refinement_restores_b_and_x(built_cache):
+    """On a small grid the autotuner also times whole solves of the grid's own right-hand sides;
+    it leaves channel 1 (b) and channel 0 (x) as it found them, picks only valid shapes, and the
+    solve after tuning gives the untuned solve's bits."""
+    b = built_cache("ring512")
+    rhs = rhs_of(b)
+    g = DeviceGrid(b.topology)
+    assert g.get_launch_shape(KERNEL_GS_SWEEP, 6) == 4  # the untuned shape of a small grid
+    s = GMGSolver()
+    g.set_channel(1, rhs)
+    it0, rel0 = s.solve(g)
+    x0 = g.get_channel(0)
+    g.set_channel(1, rhs)
+    x_marker = np.arange(x0.size, dtype=np.float32).reshape(x0.shape)
+    g.set_channel(0, x_marker)
+    g.autotune(reps=3)
+    assert np.array_equal(bits(g.get_channel(1)), bits(rhs))
+    assert np.array_equal(bits(g.get_channel(0)), bits(x_marker))
+    for k in (KERNEL_GS_SWEEP, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP, KERNEL_RESIDUAL_RESTRICT):
+        for lv in range(2, 7):
+            assert 0 <= g.get_launch_shape(k, lv) < 12
+    assert 0 <= g.get_launch_shape(KERNEL_LAPLACIAN, 0) < 20
+    g.set_channel(0, np.zeros_like(x0))  # the solve writes x on LEAF tiles only; start as the first did
+    it1, rel1 = s.solve(g)
+    assert (it1, rel1) == (it0, rel0)
+    assert np.array_equal(bits(g.get_channel(0)), bits(x0))
+    g.close()
+
+
 def test_every_launch_shape_gives_the_same_bits(built_cache):
     """Each of the eight plain launch shapes of the staged kernels (tiles per CTA x tiles in flight),
     pinned for every kernel and level, gives the solve of the default shapes bit for bit."""
