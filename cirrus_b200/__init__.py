@@ -436,6 +436,23 @@ class GMGSolver:
         self.last_result = res[0]
         return [(r.iters, r.rel_residual) for r in res]
 
+    def solve_grids(self, grids: Sequence[DeviceGrid], stream: int = 0, **kw) -> list[list[tuple[int, float]]]:
+        """Solve every instance of several distinct grids at once, each grid's solve on a stream of
+        its own (the grids' kernels share the GPU); per grid, per instance (iters, relative
+        residual), each bit-identical to that grid's solve_batch."""
+        p = self.params(**kw)
+        counts = [g.num_instances for g in grids]
+        res = (SolveResult * sum(counts))()
+        hs = (C.c_void_p * len(grids))(*[g.handle.value for g in grids])
+        check(lib().cirrus_gmg_solve_grids(hs, len(grids), C.byref(p), C.c_void_p(stream), res), "cirrus_gmg_solve_grids")
+        self.last_results = list(res)
+        self.last_result = res[0]
+        out, o = [], 0
+        for c in counts:
+            out.append([(r.iters, r.rel_residual) for r in res[o:o + c]])
+            o += c
+        return out
+
     def damped_jacobi_solve(self, grid: DeviceGrid, verbose: bool = False, max_iters: int = 10, relative_tolerance: float = 1e-6,
                             omega: float = 1.0, stream: int = 0) -> tuple[int, float]:
         """GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x to channel 0;

@@ -593,6 +593,37 @@ cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_param
     return solve_batch_with(0, grid, params, active, tolerances, pure_neumann, stream, results);
 }
 
+cirrus_status cirrus_gmg_solve_grids(cirrus_grid* const* grids, int count, const cirrus_solve_params* params, void* stream,
+                                     cirrus_solve_result* results) {
+    if (!grids || count <= 0 || !params_ok(params) || !results) return CIRRUS_ERR_INVALID_ARGUMENT;
+    std::vector<cirrus::DevGrid*> gs(count);
+    for (int k = 0; k < count; k++) {
+        if (!grids[k]) return CIRRUS_ERR_INVALID_ARGUMENT;
+        gs[k] = grids[k]->g;
+        for (int j = 0; j < k; j++)
+            if (gs[j] == gs[k]) return CIRRUS_ERR_INVALID_ARGUMENT;  // one solve in flight per grid
+    }
+    return guard([&] {
+        cirrus::SolveParams p;
+        to_internal(params, &p);
+        std::vector<std::vector<cirrus::SolveResult>> r;
+        const int rc = cirrus::solve_grids(gs, p, S(stream), r);
+        if (rc) return map_rc(rc);
+        int o = 0;
+        for (int k = 0; k < count; k++)
+            for (const cirrus::SolveResult& x : r[k]) {
+                results[o].iters = x.iters;
+                results[o].outer_iters = x.outer;
+                results[o].rel_residual = x.rel;
+                results[o].true_rel_residual = x.true_rel;
+                results[o].status = (int)map_rc(x.status);
+                results[o].kernel_launches = x.launches;
+                o++;
+            }
+        return CIRRUS_OK;
+    });
+}
+
 cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream, cirrus_solve_result* result) {
     if (!grid || !params_ok(params) || !result) return CIRRUS_ERR_INVALID_ARGUMENT;
     return guard([&] {

@@ -670,6 +670,8 @@ void grid_destroy(DevGrid* g) {
     cudaFree(g->d_ct_gather);
     cudaFree(g->d_err);
     if (g->h_err) cudaFreeHost(g->h_err);
+    if (g->side_stream) cudaStreamDestroy(g->side_stream);
+    if (g->side_join) cudaEventDestroy(g->side_join);
     free_tile_map_cache(*g);
     cudaFree(g->d_ct_flag);
     cudaFree(g->d_lists);

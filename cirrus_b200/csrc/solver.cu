@@ -278,6 +278,55 @@ int pcg_solve(DevGrid& g, const SolveParams& p0, cudaStream_t s, SolveResult* r,
     return 0;
 }
 
+int solve_grids(const std::vector<DevGrid*>& grids, const SolveParams& p, cudaStream_t s, std::vector<std::vector<SolveResult>>& r) {
+    r.assign(grids.size(), {});
+    for (size_t k = 0; k < grids.size(); k++) r[k].resize(grids[k]->num_inst);
+    if (p.precision != 0) {
+        for (size_t k = 0; k < grids.size(); k++) {
+            const int rc = mixed_solve(*grids[k], p, s, r[k].data());
+            if (rc) return rc;
+        }
+        return 0;
+    }
+    cudaEvent_t fork = nullptr;
+    if (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess) return 2;
+    cudaEventRecord(fork, s);
+    std::vector<long long> direct(grids.size(), -1);
+    int rc = 0;
+    size_t launched = 0;
+    for (; launched < grids.size(); launched++) {
+        DevGrid& g = *grids[launched];
+        if (!g.side_stream && cudaStreamCreateWithFlags(&g.side_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            g.side_stream = nullptr;
+            rc = 2;
+            break;
+        }
+        if (!g.side_join && cudaEventCreateWithFlags(&g.side_join, cudaEventDisableTiming) != cudaSuccess) {
+            g.side_join = nullptr;
+            rc = 2;
+            break;
+        }
+        g.x64_valid = false;
+        cudaStreamWaitEvent(g.side_stream, fork, 0);
+        rc = pcg_launch(g, p, g.side_stream, nullptr, &direct[launched]);
+        cudaEventRecord(g.side_join, g.side_stream);
+        cudaStreamWaitEvent(s, g.side_join, 0);
+        if (rc) {
+            launched++;
+            break;
+        }
+    }
+    const cudaError_t e = cudaStreamSynchronize(s);
+    cudaEventDestroy(fork);
+    if (rc) return rc;
+    if (e != cudaSuccess) {
+        grids[0]->last_error = std::string("solve: ") + cudaGetErrorString(e);
+        return 2;
+    }
+    for (size_t k = 0; k < grids.size(); k++) pcg_collect(*grids[k], p, direct[k], r[k].data());
+    return 0;
+}
+
 int pcg_launch(DevGrid& g, const SolveParams& p0, cudaStream_t s, const InstRequest* req, long long* direct_out) {
     if (p0.preconditioner == 1 && !g.amg_ready) {
         g.last_error = "AMG solve before its coefficients were prepared (amg_prepare)";

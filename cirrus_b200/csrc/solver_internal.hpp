@@ -116,6 +116,9 @@ struct DevGrid {
     void* tile_map_cache = nullptr;       // tensor maps of the channel buffers (lap_tma.cu)
     unsigned int* d_err = nullptr;        // set by a kernel whose bounded wait gave up (0 otherwise)
     unsigned int* h_err = nullptr;        // pinned mirror, read back after each solve
+    // the grid's own stream and join event for solves of several grids at once (created on first use)
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t side_join = nullptr;
     int* d_lists = nullptr;
     const int* d_leaf = nullptr;   // LEAF tiles, instance by instance, each in its all-tiles order
     const int* d_ghost = nullptr;
@@ -407,6 +410,10 @@ int mixed_solve(DevGrid& g, const SolveParams& p, cudaStream_t s, SolveResult* r
 // has completed.  `direct` carries the direct path's launch count (-1: graph) from one to the other.
 int pcg_launch(DevGrid& g, const SolveParams& p, cudaStream_t s, const InstRequest* req, long long* direct);
 void pcg_collect(DevGrid& g, const SolveParams& p, long long direct, SolveResult* r);
+// Plain FP32 solves of several grids at once: each grid's solve is launched on the grid's own
+// stream, forked from s after s's pending work and joined back into s; results per grid, in grid
+// order.  Mixed precision runs the grids one after another on s.
+int solve_grids(const std::vector<DevGrid*>& grids, const SolveParams& p, cudaStream_t s, std::vector<std::vector<SolveResult>>& r);
 // GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x to channel 0,
 // channels 2 (residual) and 3 (diagonal) as the reference leaves them.  Single-instance grids.
 int damped_jacobi(DevGrid& g, int max_iters, double tol, float omega, cudaStream_t s, int* iters, double* rel);

@@ -7,7 +7,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from cirrus_b200 import KERNEL_GS_SWEEP, KERNEL_LAPLACIAN, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP, KERNEL_RESIDUAL_RESTRICT, DeviceGrid, GMGSolver, PRECISION_MIXED_FP64, workloads as W
+from cirrus_b200 import KERNEL_GS_SWEEP, KERNEL_LAPLACIAN, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP, KERNEL_RESIDUAL_RESTRICT, CirrusError, DeviceGrid, GMGSolver, PRECISION_MIXED_FP64, workloads as W
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -178,6 +178,46 @@ def test_autotune_whole_solve_refinement_restores_b_and_x(built_cache):
     assert (it1, rel1) == (it0, rel0)
     assert np.array_equal(bits(g.get_channel(0)), bits(x0))
     g.close()
+
+
+@pytest.mark.parametrize("groups", [[["sphere64_small", "ring64_small"], ["ring512"]], [["ring512"], ["ring512", "ring64_small"], ["sphere64_small"]]])
+def test_grids_solved_at_once_give_each_grids_bits(built_cache, groups):
+    """Several grids solved at once (cirrus_gmg_solve_grids: each grid's graph on its own stream)
+    give, grid by grid, the iterations and pressure of that grid's own batched solve bit for bit;
+    the same grid twice is refused; mixed precision (run grid after grid) converges each grid."""
+    grids, rhs = [], []
+    for names in groups:
+        bs = [built_cache(n) for n in names]
+        rhs.append([rhs_of(b) for b in bs])
+        grids.append(DeviceGrid([b.topology for b in bs]))
+
+    def load():
+        for g, rs in zip(grids, rhs):
+            for i, r in enumerate(rs):
+                g.set_channel_instance(i, 1, r)
+                g.set_channel_instance(i, 0, np.zeros_like(r))
+
+    s = GMGSolver()
+    load()
+    alone = []
+    for g in grids:
+        res = s.solve_batch(g)
+        alone.append((res, [g.get_channel_instance(i, 0) for i in range(g.num_instances)]))
+    load()
+    together = s.solve_grids(grids)
+    assert all(r.status == 0 for r in s.last_results)
+    for g, (res, xs), res2 in zip(grids, alone, together):
+        assert res2 == res
+        for i, x in enumerate(xs):
+            assert np.array_equal(bits(g.get_channel_instance(i, 0)), bits(x)), i
+    with pytest.raises(CirrusError):
+        s.solve_grids([grids[0], grids[0]])
+    load()
+    sm = GMGSolver(precision=PRECISION_MIXED_FP64)
+    sm.solve_grids(grids)
+    assert all(r.status == 0 and r.true_rel_residual < 1e-6 for r in sm.last_results)
+    for g in grids:
+        g.close()
 
 
 def test_every_launch_shape_gives_the_same_bits(built_cache):
