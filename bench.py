@@ -88,6 +88,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--pools", type=int, default=2,
+                    help="solve each step's batch as this many grids at once (cirrus_gmg_solve_grids; 1: one grid)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ring512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -427,10 +429,21 @@ def run_ours(args, world, rank, local, pg):
                              KERNEL_RESIDUAL_RESTRICT, TMP_CHANNEL, U_CHANNEL, DeviceGrid, GMGSolver)
 
     K = args.batch
-    b, g = build_batch(args.workload, batch_seeds(rank, K))
+    P = args.pools if args.pools >= 1 and K % args.pools == 0 else 1
+    seeds = batch_seeds(rank, K)
+    b, g = build_batch(args.workload, seeds)
     g.autotune()  # launch shapes per kernel and level for this grid (results unchanged)
     rhs = g.get_channel(B_CHANNEL)
     g.copy_channel(TMP_CHANNEL, B_CHANNEL)  # keep b resident for restoring between steps
+    # the step's batch as P grids of K/P instances solved at once, each grid's solve graph on its
+    # own stream (cirrus_gmg_solve_grids): one grid's latency-bound coarse levels overlap another's
+    # large launches
+    pools = [g]
+    if P > 1:
+        pools = [build_batch(args.workload, seeds[q * K // P:(q + 1) * K // P])[1] for q in range(P)]
+        for gp in pools:
+            gp.autotune()
+            gp.copy_channel(TMP_CHANNEL, B_CHANNEL)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
     solver = GMGSolver()
@@ -443,16 +456,18 @@ def run_ours(args, world, rank, local, pg):
             raise RuntimeError(f"solve did not converge: rel {worst}")
 
     def one():
-        g.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
+        for gp in pools:
+            gp.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        res = solver.solve_batch(g, stream=sh)
+        res = [r for pr in solver.solve_grids(pools, stream=sh) for r in pr]
         e1.record(stream)
         torch.cuda.synchronize()
         iters_seen.extend(r[0] for r in res)
-        launches.append(solver.last_result.kernel_launches)
+        # each result carries its grid's whole launch count: one per pool
+        launches.append(sum(solver.last_results[q * (K // P)].kernel_launches for q in range(P)))
         worst = max(r[1] for r in res)
         if worst >= 1e-6:
             raise RuntimeError(f"solve did not converge: rel {worst}")
@@ -499,26 +514,42 @@ def run_ours(args, world, rank, local, pg):
         e2e_times.append((time.perf_counter() - t0) * 1e3)
     e2e_serial_total = barrier_max(pg, sum(e2e_times))
 
-    g2 = DeviceGrid([b.topology] * K)
-    for kern in (KERNEL_LAPLACIAN, KERNEL_GS_SWEEP, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP, KERNEL_RESIDUAL_RESTRICT):
-        for lv in range(b.topology.num_layers):
-            g2.set_launch_shape(g.get_launch_shape(kern, lv), kern, lv)
-    s2 = torch.cuda.Stream()
-    grids, streams = [g, g2], [sh, s2.cuda_stream]
-    b2_host, x2_host = b_host.clone().pin_memory(), torch.empty_like(b_host).pin_memory()
-    hosts = [(b_np, x_np), (b2_host.numpy(), x2_host.numpy())]
+    # two sets of the step's grids (the pools, and as many grids again with the same topologies and
+    # launch shapes), each grid with its own stream and pinned host buffers
+    tuned = (KERNEL_LAPLACIAN, KERNEL_GS_SWEEP, KERNEL_PRESMOOTH, KERNEL_PROLONG_SWEEP, KERNEL_RESIDUAL_RESTRICT)
+    twins = []
+    for gp in pools:
+        gq = DeviceGrid([b.topology] * gp.num_instances)
+        for kern in tuned:
+            for lv in range(b.topology.num_layers):
+                gq.set_launch_shape(gp.get_launch_shape(kern, lv), kern, lv)
+        twins.append(gq)
+    sets = [pools, twins]
+    side = [[torch.cuda.Stream() for _ in range(P)] for _ in range(2)]
+    streams = [[sh] + [s.cuda_stream for s in side[0][1:]], [s.cuda_stream for s in side[1]]]
+    hosts = []
+    for _ in range(2):
+        hs = []
+        for gp in pools:
+            bh = torch.from_numpy(gp.get_channel(TMP_CHANNEL).reshape(-1)).pin_memory()
+            hs.append((bh.numpy(), torch.empty_like(bh).pin_memory().numpy()))
+        hosts.append(hs)
+    step_bytes = sum(h[0].nbytes for h in hosts[0])
 
     def e2e_pipeline(steps):
         pending = [False, False]
         for k in range(steps):
             j = k % 2
             if pending[j]:
-                check_converged(solver.solve_host_wait(grids[j]))
-            solver.solve_host_submit(grids[j], *hosts[j], stream=streams[j])
+                for gq in sets[j]:
+                    check_converged(solver.solve_host_wait(gq))
+            for q, gq in enumerate(sets[j]):
+                solver.solve_host_submit(gq, *hosts[j][q], stream=streams[j][q])
             pending[j] = True
         for j in (0, 1):
             if pending[j]:
-                check_converged(solver.solve_host_wait(grids[j]))
+                for gq in sets[j]:
+                    check_converged(solver.solve_host_wait(gq))
 
     e2e_pipeline(4)
     torch.cuda.synchronize()
@@ -527,7 +558,8 @@ def run_ours(args, world, rank, local, pg):
     t0 = time.perf_counter()
     e2e_pipeline(args.steps)
     e2e_total = barrier_max(pg, (time.perf_counter() - t0) * 1e3)
-    g2.close()
+    for gq in twins:
+        gq.close()
 
     # roofline of the dominant kernel (fused Laplacian over the batch's LEAF|GHOST tiles), timed
     # with CUDA events on the stream it is launched on
@@ -707,9 +739,12 @@ def run_ours(args, world, rank, local, pg):
                         "pcg_iters_per_solve": int(statistics.median(r.iters for r in ares)),
                         "prepare_ms": round(amg_prepare_ms, 3)},
         "gpu_launches": int(sum(launches)),
+        "schedule": {"pools": P, "instances_per_pool": K // P,
+                     "api": "cirrus_gmg_solve_grids: the step's instances as grids solved at once, each on its own stream"},
         "e2e": {"value": round(n / (e2e_total * 1e-3), 3), "unit": "solves/s",
-                "h2d_bytes_per_step": int(rhs.nbytes), "d2h_bytes_per_step": int(rhs.nbytes),
-                "api": "cirrus_gmg_solve_host_submit/wait, two grids alternating (copies of one batch overlap the other's solve)",
+                "h2d_bytes_per_step": int(step_bytes), "d2h_bytes_per_step": int(step_bytes),
+                "api": f"cirrus_gmg_solve_host_submit/wait, two sets of {P} grid(s) of {K // P} instances alternating (copies of "
+                       "one step's batch overlap the other set's solves; a set's grids solve at once on their own streams)",
                 "serial": {"value": round(n / (e2e_serial_total * 1e-3), 3), "api": "cirrus_gmg_solve_host (copy, solve, copy, return)"}},
         "roofline": {"kernel": f"k_laplacian_fused ({K} instances, {n_leaf} LEAF + {n_ghost} GHOST tiles)", "bound": "hbm",
                      "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
