@@ -88,7 +88,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--pools", type=int, default=2,
+    ap.add_argument("--pools", type=int, default=4,
                     help="solve each step's batch as this many grids at once (cirrus_gmg_solve_grids; 1: one grid)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ring512")
