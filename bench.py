@@ -615,12 +615,13 @@ def run_ours(args, world, rank, local, pg):
     msolver = GMGSolver(precision=PRECISION_MIXED_FP64)
     mtimes, mres = [], []
     for i in range(args.warmup + args.steps):
-        g.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
+        for gp in pools:
+            gp.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        msolver.solve_batch(g, stream=sh)
+        msolver.solve_grids(pools, stream=sh)
         e1.record(stream)
         torch.cuda.synchronize()
         if i >= args.warmup:
@@ -635,12 +636,13 @@ def run_ours(args, world, rank, local, pg):
     tli, tci = msolver.autotune_sweeps(g, stream=sh)
     ttimes, tres = [], []
     for i in range(args.warmup + args.steps):
-        g.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
+        for gp in pools:
+            gp.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        msolver.solve_batch(g, stream=sh, level_iters=tli, coarsest_iters=tci)
+        msolver.solve_grids(pools, stream=sh, level_iters=tli, coarsest_iters=tci)
         e1.record(stream)
         torch.cuda.synchronize()
         if i >= args.warmup:

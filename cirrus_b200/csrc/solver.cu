@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <thread>
 
 namespace cirrus {
 
@@ -281,31 +282,44 @@ int pcg_solve(DevGrid& g, const SolveParams& p0, cudaStream_t s, SolveResult* r,
 int solve_grids(const std::vector<DevGrid*>& grids, const SolveParams& p, cudaStream_t s, std::vector<std::vector<SolveResult>>& r) {
     r.assign(grids.size(), {});
     for (size_t k = 0; k < grids.size(); k++) r[k].resize(grids[k]->num_inst);
-    if (p.precision != 0) {
-        for (size_t k = 0; k < grids.size(); k++) {
-            const int rc = mixed_solve(*grids[k], p, s, r[k].data());
-            if (rc) return rc;
+    for (DevGrid* g : grids) {
+        if (!g->side_stream && cudaStreamCreateWithFlags(&g->side_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            g->side_stream = nullptr;
+            return 2;
         }
-        return 0;
+        if (!g->side_join && cudaEventCreateWithFlags(&g->side_join, cudaEventDisableTiming) != cudaSuccess) {
+            g->side_join = nullptr;
+            return 2;
+        }
     }
     cudaEvent_t fork = nullptr;
     if (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess) return 2;
     cudaEventRecord(fork, s);
+    if (p.precision != 0) {
+        // the mixed-precision outer loop reads residuals on the host: one host thread per grid,
+        // each driving its grid's own stream
+        std::vector<int> rcs(grids.size(), 0);
+        std::vector<std::thread> th;
+        for (size_t k = 0; k < grids.size(); k++) {
+            cudaStreamWaitEvent(grids[k]->side_stream, fork, 0);
+            th.emplace_back([&, k] { rcs[k] = mixed_solve(*grids[k], p, grids[k]->side_stream, r[k].data()); });
+        }
+        for (std::thread& t : th) t.join();
+        for (DevGrid* g : grids) {
+            cudaEventRecord(g->side_join, g->side_stream);
+            cudaStreamWaitEvent(s, g->side_join, 0);
+        }
+        const cudaError_t e = cudaStreamSynchronize(s);
+        cudaEventDestroy(fork);
+        for (int rc : rcs)
+            if (rc) return rc;
+        return e == cudaSuccess ? 0 : 2;
+    }
     std::vector<long long> direct(grids.size(), -1);
     int rc = 0;
     size_t launched = 0;
     for (; launched < grids.size(); launched++) {
         DevGrid& g = *grids[launched];
-        if (!g.side_stream && cudaStreamCreateWithFlags(&g.side_stream, cudaStreamNonBlocking) != cudaSuccess) {
-            g.side_stream = nullptr;
-            rc = 2;
-            break;
-        }
-        if (!g.side_join && cudaEventCreateWithFlags(&g.side_join, cudaEventDisableTiming) != cudaSuccess) {
-            g.side_join = nullptr;
-            rc = 2;
-            break;
-        }
         g.x64_valid = false;
         cudaStreamWaitEvent(g.side_stream, fork, 0);
         rc = pcg_launch(g, p, g.side_stream, nullptr, &direct[launched]);

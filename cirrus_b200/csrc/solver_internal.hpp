@@ -412,7 +412,8 @@ int pcg_launch(DevGrid& g, const SolveParams& p, cudaStream_t s, const InstReque
 void pcg_collect(DevGrid& g, const SolveParams& p, long long direct, SolveResult* r);
 // Plain FP32 solves of several grids at once: each grid's solve is launched on the grid's own
 // stream, forked from s after s's pending work and joined back into s; results per grid, in grid
-// order.  Mixed precision runs the grids one after another on s.
+// order.  Mixed precision drives each grid from a host thread of its own (its outer loop reads
+// residuals on the host).
 int solve_grids(const std::vector<DevGrid*>& grids, const SolveParams& p, cudaStream_t s, std::vector<std::vector<SolveResult>>& r);
 // GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:449-531): b in channel 1, x to channel 0,
 // channels 2 (residual) and 3 (diagonal) as the reference leaves them.  Single-instance grids.

@@ -358,9 +358,9 @@ cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_param
  * it, so the grids' kernels share the GPU (one grid's latency-bound coarse-level launches overlap
  * another's large ones: 32 ring512 instances as two grids of 16 solve about 4 % faster than as
  * one grid of 32).  results: one per instance, grid after grid.  Each result is bit-identical to
- * that grid's cirrus_gmg_solve_batch.  Mixed precision (params->precision) solves the grids one
- * after another on `stream`.  Returns after every result is on the host.  No counterpart in the
- * reference. */
+ * that grid's cirrus_gmg_solve_batch.  Mixed precision (params->precision), whose outer loop
+ * reads residuals on the host, drives each grid from a host thread of its own.  Returns after
+ * every result is on the host.  No counterpart in the reference. */
 cirrus_status cirrus_gmg_solve_grids(cirrus_grid* const* grids, int count, const cirrus_solve_params* params, void* stream,
                                      cirrus_solve_result* results);
 

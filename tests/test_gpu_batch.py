@@ -184,7 +184,8 @@ def test_autotune_whole_solve_refinement_restores_b_and_x(built_cache):
 def test_grids_solved_at_once_give_each_grids_bits(built_cache, groups):
     """Several grids solved at once (cirrus_gmg_solve_grids: each grid's graph on its own stream)
     give, grid by grid, the iterations and pressure of that grid's own batched solve bit for bit;
-    the same grid twice is refused; mixed precision (run grid after grid) converges each grid."""
+    the same grid twice is refused; mixed precision (one host thread per grid) gives each grid's
+    own mixed solve bit for bit."""
     grids, rhs = [], []
     for names in groups:
         bs = [built_cache(n) for n in names]
@@ -212,10 +213,19 @@ def test_grids_solved_at_once_give_each_grids_bits(built_cache, groups):
             assert np.array_equal(bits(g.get_channel_instance(i, 0)), bits(x)), i
     with pytest.raises(CirrusError):
         s.solve_grids([grids[0], grids[0]])
-    load()
     sm = GMGSolver(precision=PRECISION_MIXED_FP64)
-    sm.solve_grids(grids)
+    load()
+    malone = []
+    for g in grids:
+        res = sm.solve_batch(g)
+        malone.append((res, [g.get_channel_instance(i, 0) for i in range(g.num_instances)]))
+    load()
+    mtogether = sm.solve_grids(grids)  # one host thread per grid
     assert all(r.status == 0 and r.true_rel_residual < 1e-6 for r in sm.last_results)
+    for g, (res, xs), res2 in zip(grids, malone, mtogether):
+        assert res2 == res
+        for i, x in enumerate(xs):
+            assert np.array_equal(bits(g.get_channel_instance(i, 0)), bits(x)), i
     for g in grids:
         g.close()
 
