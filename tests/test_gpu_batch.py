@@ -213,6 +213,16 @@ def test_grids_solved_at_once_give_each_grids_bits(built_cache, groups):
             assert np.array_equal(bits(g.get_channel_instance(i, 0)), bits(x)), i
     with pytest.raises(CirrusError):
         s.solve_grids([grids[0], grids[0]])
+    # kernels launched one by one from the host (each grid's loop checked on the host in turn)
+    for g in grids:
+        g.set_launch_mode(True)
+    load()
+    direct = s.solve_grids(grids)
+    for g, (res, xs), res2 in zip(grids, alone, direct):
+        assert res2 == res
+        for i, x in enumerate(xs):
+            assert np.array_equal(bits(g.get_channel_instance(i, 0)), bits(x)), i
+        g.set_launch_mode(False)
     sm = GMGSolver(precision=PRECISION_MIXED_FP64)
     load()
     malone = []
