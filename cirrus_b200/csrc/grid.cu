@@ -543,7 +543,7 @@ int grid_create(const std::vector<const Topology*>& topos, DevGrid** out, std::s
         }
         launch::init_kernel_attributes();
         launch::init_stencil_attributes();
-        g->shapes.assign((size_t)KS_COUNT * num_layers, n <= kSmallGridTiles ? 4 : 1);
+        g->shapes.assign((size_t)KS_COUNT * num_layers, kDefaultShape);
         init_tile_map_cache(*g);
         CK(cudaMalloc(&g->d_err, sizeof(unsigned int)));
         CK(cudaMemset(g->d_err, 0, sizeof(unsigned int)));

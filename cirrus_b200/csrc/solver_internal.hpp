@@ -61,9 +61,11 @@ enum { KS_GS_SWEEP = 0, KS_PRESMOOTH = 1, KS_PROLONG = 2, KS_RESIDUAL = 3, KS_LA
 // them prefetching the tiles of CTAs one resident wave ahead into L2
 constexpr int kNumShapes = 12;
 constexpr int kCommonShapes = 8;
+// The launch shape of an untuned grid: one tile per 128-thread CTA (faster than shape 1 for one
+// ring512 instance up to sixteen: 4.30 against 4.96 ms, 27.4 against 29.0 ms).
+constexpr int kDefaultShape = 4;
 // Grids of at most this many tiles (one instance or a few) are chains of latency-bound launches:
-// they start with one tile per 128-thread CTA (shape 4) rather than shape 1, and the autotuner
-// refines their shapes with whole solves.
+// the autotuner refines their shapes with whole solves.
 constexpr int kSmallGridTiles = 16384;
 // the Laplacian's 8..11 are instead the TMA-staged pipeline (lap_tma.cu) with (consumer groups,
 // stages) = (2, 8), (4, 16), (2, 12), (1, 6); then 12..15 eight cells per thread (lap8.cu), 16..19
@@ -147,7 +149,7 @@ struct DevGrid {
     std::vector<int> mg_offset, mg_count, level_first, level_count;
     std::vector<uint8_t> h_tile_type;
     std::vector<uint8_t> shapes;  // KS_COUNT x num_layers launch-shape choices
-    int shape(int kind, int level) const { return shapes.empty() ? 1 : shapes[(size_t)kind * num_layers + level]; }
+    int shape(int kind, int level) const { return shapes.empty() ? kDefaultShape : shapes[(size_t)kind * num_layers + level]; }
 
     // coarse levels 0..bottom_level of every instance in the shared-memory kernel (-1: none)
     int bottom_level = -1;

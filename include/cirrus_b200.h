@@ -468,7 +468,7 @@ cirrus_status cirrus_bench_launch(cirrus_grid* grid, int kernel, int level, int 
  * halos into a ring of shared-memory stages, 1-4 consumer groups), 12..15, a column of eight cells
  * per thread (64 threads per tile), and 16..19, shapes 2, 3, 5 and 1 prefetching into L2.  Lets a
  * caller reuse tuned shapes for grids of the same structure or pin one.  Before any tuning a grid
- * of at most 16,384 tiles runs shape 4 (one tile per 128-thread CTA) and a larger one shape 1.
+ * runs shape 4 (one tile per 128-thread CTA).
  * Shapes never change results.  No counterpart in the reference. */
 #define CIRRUS_NUM_LAUNCH_SHAPES 20
 cirrus_status cirrus_grid_set_launch_shape(cirrus_grid* grid, int kernel, int level, int shape);

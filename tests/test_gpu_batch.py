@@ -158,7 +158,7 @@ def test_autotune_whole_solve_refinement_restores_b_and_x(built_cache):
     b = built_cache("ring512")
     rhs = rhs_of(b)
     g = DeviceGrid(b.topology)
-    assert g.get_launch_shape(KERNEL_GS_SWEEP, 6) == 4  # the untuned shape of a small grid
+    assert g.get_launch_shape(KERNEL_GS_SWEEP, 6) == 4  # the untuned shape
     s = GMGSolver()
     g.set_channel(1, rhs)
     it0, rel0 = s.solve(g)
