@@ -155,16 +155,13 @@ __device__ __forceinline__ void k_laplacian_fused_body(Topo tp, const int* __res
     }
     TilePre pre[NT];
     tile_pre(tp, tile, t, pre);
-#pragma unroll
-    for (int u = 0; u < NT; u++)
-        if (act[u]) {
-            stage_mask_async(tp.mask_lap, tile[u], t, st[u * TPB + g]);
-            if (WP != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
-        }
     pdl_wait();
 #pragma unroll
     for (int u = 0; u < NT; u++)
-        if (act[u]) stage_async(X, nullptr, nullptr, tile[u], pre[u].nb, t, st[u * TPB + g]);
+        if (act[u]) {
+            stage_async(X, nullptr, tp.mask_lap, tile[u], pre[u].nb, t, st[u * TPB + g]);
+            if (WP != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
+        }
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (ptile[u] >= 0) {
@@ -322,16 +319,13 @@ __device__ __forceinline__ void k_gs_sweep_body(Topo tp, const int* __restrict__
     }
     TilePre pre[NT];
     tile_pre(tp, tile, t, pre);
-#pragma unroll
-    for (int u = 0; u < NT; u++)
-        if (act[u]) {
-            stage_mask_async(tp.mask_mg, tile[u], t, st[u * TPB + g]);
-            if (RD != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
-        }
     pdl_wait();
 #pragma unroll
     for (int u = 0; u < NT; u++)
-        if (act[u]) stage_async(X, R, nullptr, tile[u], pre[u].nb, t, st[u * TPB + g]);
+        if (act[u]) {
+            stage_async(X, R, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
+            if (RD != nullptr && t == 0) cp_async4(st[u * TPB + g].aux, tp.leafslot + tile[u]);
+        }
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (ptile[u] >= 0) {
@@ -533,13 +527,10 @@ __device__ __forceinline__ void k_residual_restrict_body(Topo tp, int first, con
     }
     TilePre pre[NT];
     tile_pre(tp, tile, t, pre);
-#pragma unroll
-    for (int u = 0; u < NT; u++)
-        if (act[u]) stage_mask_async(tp.mask_mg, tile[u], t, st[u * TPB + g]);
     pdl_wait();
 #pragma unroll
     for (int u = 0; u < NT; u++)
-        if (act[u]) stage_async(X, RHS, nullptr, tile[u], pre[u].nb, t, st[u * TPB + g]);
+        if (act[u]) stage_async(X, RHS, tp.mask_mg, tile[u], pre[u].nb, t, st[u * TPB + g]);
 #pragma unroll
     for (int u = 0; u < NT; u++)
         if (ptile[u] >= 0) {

@@ -28,9 +28,10 @@ __device__ __forceinline__ void pdl_entry() {
 }
 // The same two steps apart, for the stencil, coarse-level and vector kernels: between them a
 // kernel reads only the grid's topology (tile lists, metadata, coefficient classes, level
-// constants, stencil masks, chunk and range tables, coarse-level boxes), which is written once
-// when the grid is created and never by a kernel, and writes only its own shared memory -- so
-// that part overlaps the predecessor's tail without changing any result.
+// constants, chunk and range tables, coarse-level boxes), which is written once when the grid is
+// created and never by a kernel, and writes only its own shared memory -- so that part overlaps
+// the predecessor's tail without changing any result.  The staged copies (mask bytes included)
+// follow the wait: issued before it, they cost the batched solve more than they saved.
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
@@ -428,11 +429,6 @@ __device__ __forceinline__ void tile_pre(const Topo& tp, const int (&tile)[NT], 
     for (int u = 0; u < NT; u++) pre[u].lc = tp.lconst[inst[u] * kLevelSlots + meta_level(pre[u].packed)];
 }
 
-// Issue the copy of `tile`'s mask bytes into st (topology: may precede pdl_wait).
-template <class Stage>
-__device__ __forceinline__ void stage_mask_async(const uint8_t* __restrict__ mask, int tile, int t, Stage& st) {
-    if (t < 32) cp_async16(st.mask + t * 16, mask + (size_t)tile * kTileCells + t * 16);
-}
 // Issue the copies of `tile` into st: channel X's values and face halos (0 for absent
 // neighbours), channel B (if given) and the mask bytes (if given).  Completed by
 // cp_async_wait_all + __syncthreads.

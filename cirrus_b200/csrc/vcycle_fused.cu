@@ -122,6 +122,7 @@ __device__ __forceinline__ void k_presmooth_body(Topo tp, const int* __restrict_
         nfc_z[u] = nbz[u] >= 0 ? tp.fcls[nbz[u]] : 0u;
         zmb[u] = nbz[u] >= 0 ? tp.mask_mg[(size_t)nbz[u] * kTileCells + zoff] : 0u;
     }
+    pdl_wait();
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
@@ -129,13 +130,6 @@ __device__ __forceinline__ void k_presmooth_body(Topo tp, const int* __restrict_
         const size_t base = (size_t)tile[u] * kTileCells;
         if (t < 32) cp_async16(ps.mask + t * 16, tp.mask_mg + base + t * 16);
         if (nbf[u] >= 0) cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + (size_t)nbf[u] * kTileCells + foff);
-    }
-    pdl_wait();
-#pragma unroll
-    for (int u = 0; u < NT; u++) {
-        if (!act[u]) continue;
-        PreStage& ps = st[u * TPB + g];
-        const size_t base = (size_t)tile[u] * kTileCells;
         cp_async16(ps.b + t * 4, RHS + base + t * 4);
         if (nbf[u] >= 0) cp_async16(ps.hx + fface * 64 + qq * 4, RHS + (size_t)nbf[u] * kTileCells + foff);
         if (nbz[u] >= 0) cp_async4(ps.hx + zface * 64 + zc, RHS + (size_t)nbz[u] * kTileCells + zoff);
@@ -342,6 +336,7 @@ __device__ __forceinline__ void k_prolong_sweep_body(Topo tp, const int* __restr
             zmb[u] = tp.mask_mg[(size_t)nbz[u] * kTileCells + zoff];
         }
     }
+    pdl_wait();
 #pragma unroll
     for (int u = 0; u < NT; u++) {
         if (!act[u]) continue;
@@ -349,13 +344,6 @@ __device__ __forceinline__ void k_prolong_sweep_body(Topo tp, const int* __restr
         const size_t base = (size_t)tile[u] * kTileCells;
         if (t < 32) cp_async16(ps.mask + t * 16, tp.mask_mg + base + t * 16);
         if (nbf[u] >= 0) cp_async4(ps.hmask + fface * 64 + qq * 4, tp.mask_mg + (size_t)nbf[u] * kTileCells + foff);
-    }
-    pdl_wait();
-#pragma unroll
-    for (int u = 0; u < NT; u++) {
-        if (!act[u]) continue;
-        ProStage& ps = st[u * TPB + g];
-        const size_t base = (size_t)tile[u] * kTileCells;
         if (!ghost[u]) {
             cp_async16(ps.xp + t * 4, XP + base + t * 4);
             cp_async16(ps.b + t * 4, RHS + base + t * 4);
