@@ -27,6 +27,7 @@
  * Calls for one grid are serialised by the registry; the reference's solve is not re-entrant
  * for a grid either.
  *
+ * cirrus_dropin::autotune(grid) tunes the bound pool's launch shapes once (optional).
  * cirrus_dropin::AMGSolver<Grid> (below) replaces the reference's AMGSolver on the same registry.
  */
 #ifndef CIRRUS_GMG_DROPIN_HPP
@@ -205,6 +206,22 @@ struct Access {
 
 };
 }  // namespace detail
+
+/* Tunes the launch shapes of the pool bound to `grid` (binding it first) on the grid's current
+ * right-hand sides (channel 1 of its tiles): cirrus_grid_autotune, about 1-2 s for a
+ * ring512-sized grid, for a caller whose tiles and cell types stay the same over many solves.
+ * The shapes stay with the pool until its tile list or cell types change (a rebuilt pool starts
+ * from the untuned shape again).  Results never change. */
+template <class Grid>
+void autotune(Grid& grid) {
+    using A = detail::Access<Grid>;
+    std::shared_ptr<detail::Binding> b = A::binding(grid);
+    std::lock_guard<std::mutex> lk(b->mu);
+    A::bind(grid, *b);
+    check(cirrus_grid_gather_tiles(b->cg, 1, A::channel_offset(1), nullptr), "gather b");
+    check(cirrus_grid_autotune(b->cg, 0, nullptr), "cirrus_grid_autotune");
+    if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cirrus_dropin: CUDA error");
+}
 
 template <class Grid>
 class GMGSolver {

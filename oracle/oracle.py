@@ -401,6 +401,7 @@ def ref_dropin_lib():
             "refdrop_solve": (C.c_int, [P, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p, f64p]),
             "refdrop_damped_jacobi": (C.c_int, [P, C.c_int, C.c_double, C.c_float, f64p]),
             "refdrop_amg_solve": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, f64p]),
+            "refdrop_autotune": (C.c_int, [P]),
             "refdrop_bound_grids": (C.c_int, []),
             "refdrop_release_all": (None, []),
         }
@@ -602,6 +603,11 @@ class RefHarness:
         if it < 0:
             raise RuntimeError("drop-in solve failed")
         return it, rel.value, ms.value
+
+    def autotune_dropin(self):
+        """cirrus_dropin::autotune on this reference grid (tunes the bound pool's launch shapes)."""
+        if ref_dropin_lib().refdrop_autotune(self.h) != 0:
+            raise RuntimeError("drop-in autotune failed")
 
     def amg_solve_dropin(self, prepare=True, max_iters=1000, tol=1e-6, level_iters=1, coarsest_iters=10, sync_stride=1,
                          pure_neumann=False):

@@ -77,6 +77,18 @@ int refdrop_amg_solve(void* h, int prepare, int max_iters, double tol, int level
     return iters;
 }
 
+// cirrus_dropin::autotune on this grid (the bound pool's launch shapes); 0, or -1 on an exception.
+int refdrop_autotune(void* h) {
+    auto& grid = *static_cast<HADeviceGrid<Tile>*>(ref_grid(h));
+    try {
+        cirrus_dropin::autotune(grid);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "refdrop_autotune: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
 // Bound device pools held by the drop-in's process-wide registry.
 int refdrop_bound_grids() { return cirrus_dropin::bound_grids(); }
 void refdrop_release_all() { cirrus_dropin::release_all(); }

@@ -122,6 +122,23 @@ def test_dropin_in_reference_grid(name, built_cache, ref_ok):
         assert np.array_equal(bits(r_d)[leaf], bits(r_ref)[leaf])
 
 
+def test_dropin_autotune_keeps_the_reference_bits(built_cache, ref_ok):
+    """cirrus_dropin::autotune tunes the launch shapes of the pool bound to the reference's grid
+    (on the grid's right-hand sides in channel 1); the drop-in's solves after it still give the
+    reference's iterations and bits."""
+    b = built_cache("ring512")
+    w = b.workload
+    ref = _ref_grid(b)
+    leaf = (b.tiles[:, 4] & W.LEAF) != 0
+    ref.set_channel(1, ref.rhs(b.velocity))
+    ref.autotune_dropin()
+    (it, rel, x_ref, r_ref), (dit, drel, x_d, r_d, dms) = _ref_then_dropin(ref, b.velocity, w.pure_neumann)
+    print(f"tuned drop-in: {dit} iters ({dms:.2f} ms), reference {it}")
+    assert dit == it and abs(drel - rel) <= 1e-12 * rel
+    assert np.array_equal(bits(x_d)[leaf], bits(x_ref)[leaf])
+    assert np.array_equal(bits(r_d)[leaf], bits(r_ref)[leaf])
+
+
 @pytest.mark.parametrize("name", ["sphere64_small", "ring512"])
 def test_dropin_follows_cell_type_changes(name, built_cache, ref_ok):
     """CalcCellTypesFromLeafs rewrites the cell types every step (src/FluidEuler.h:934) without
