@@ -408,7 +408,7 @@ def dropin_call_site(args, g1, ctypes_host, sh) -> dict:
     assert L.cirrus_grid_set_tile_pointers(g1.handle, ptrs) == 0
     solver = GMGSolver()
     changed = C.c_int()
-    times = []
+    times, iters = [], []
     torch.cuda.synchronize()
     for i in range(args.warmup + args.steps):
         f32[:, TILE_CHANNEL_STRIDE:TILE_CHANNEL_STRIDE + 512] = b  # the reference's next right-hand side
@@ -422,8 +422,10 @@ def dropin_call_site(args, g1, ctypes_host, sh) -> dict:
         torch.cuda.synchronize()
         if i >= args.warmup:
             times.append((time.perf_counter() - t0) * 1e3)
+            iters.append(solver.last_result.iters)
         assert changed.value == 0
     return {"value": round(1e3 / float(np.mean(times)), 3), "unit": "solves/s", "p50_ms": round(float(np.percentile(times, 50)), 4),
+            "iters": int(max(iters)),
             "api": "cirrus_grid_compare_tile_cell_types + cirrus_grid_gather_tiles + cirrus_gmg_solve + cirrus_grid_scatter_tiles x2 "
                    "on tiles held as separate PoissonTile<float> device records (one instance, host clock around the call)",
             "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4}
@@ -707,7 +709,11 @@ def run_ours(args, world, rank, local, pg):
         torch.cuda.synchronize()
         if i >= args.warmup:
             lat.append(e0.elapsed_time(e1))
+    single_iters = solver.last_result.iters
+    g1.copy_channel(B_CHANNEL, TMP_CHANNEL, sh)  # the solves left the residual in channel 1: b again
     dropin = dropin_call_site(args, g1, b1.ctypes, sh)
+    if dropin["iters"] != single_iters:
+        raise RuntimeError(f"drop-in call site solved in {dropin['iters']} iterations, the grid's own solve in {single_iters}")
 
     n = args.steps * world * K
     value = n / (total_ms * 1e-3)
