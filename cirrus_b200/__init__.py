@@ -436,6 +436,8 @@ class GMGSolver:
         self.last_result = res[0]
         return [(r.iters, r.rel_residual) for r in res]
 
+    _grids_fn = "cirrus_gmg_solve_grids"
+
     def solve_grids(self, grids: Sequence[DeviceGrid], stream: int = 0, **kw) -> list[list[tuple[int, float]]]:
         """Solve every instance of several distinct grids at once, each grid's solve on a stream of
         its own (the grids' kernels share the GPU); per grid, per instance (iters, relative
@@ -444,7 +446,7 @@ class GMGSolver:
         counts = [g.num_instances for g in grids]
         res = (SolveResult * sum(counts))()
         hs = (C.c_void_p * len(grids))(*[g.handle.value for g in grids])
-        check(lib().cirrus_gmg_solve_grids(hs, len(grids), C.byref(p), C.c_void_p(stream), res), "cirrus_gmg_solve_grids")
+        check(getattr(lib(), self._grids_fn)(hs, len(grids), C.byref(p), C.c_void_p(stream), res), self._grids_fn)
         self.last_results = list(res)
         self.last_result = res[0]
         out, o = [], 0
@@ -507,6 +509,8 @@ class AMGSolver(GMGSolver):
     PCG around it.  prepare_types_and_coeffs(grid) first (after every change of the cell types);
     solve() then takes b in channel 1 and leaves x in channel 0, using channels 3 and 5 as the
     V-cycle's scratch.  The coefficients live apart from the grid's channels."""
+
+    _grids_fn = "cirrus_amg_solve_grids"
 
     def prepare_types_and_coeffs(self, grid: DeviceGrid, stream: int = 0) -> None:
         """AMGSolver::prepareTypesAndCoeffs (src/AMGSolver.cu:717-720)."""

@@ -209,6 +209,7 @@ _PROTOS = {
     "cirrus_grid_create_from_desc": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
     "cirrus_grid_autotune_sweeps": (C.c_int, [C.c_void_p, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveParams)]),
     "cirrus_gmg_solve_grids": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveResult)]),
+    "cirrus_amg_solve_grids": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(SolveParams), C.c_void_p, C.POINTER(SolveResult)]),
     "cirrus_grid_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "cirrus_grid_get_launch_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "cirrus_bench_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),

@@ -593,8 +593,9 @@ cirrus_status cirrus_gmg_solve_batch(cirrus_grid* grid, const cirrus_solve_param
     return solve_batch_with(0, grid, params, active, tolerances, pure_neumann, stream, results);
 }
 
-cirrus_status cirrus_gmg_solve_grids(cirrus_grid* const* grids, int count, const cirrus_solve_params* params, void* stream,
-                                     cirrus_solve_result* results) {
+namespace {
+cirrus_status solve_grids_with(int preconditioner, cirrus_grid* const* grids, int count, const cirrus_solve_params* params,
+                               void* stream, cirrus_solve_result* results) {
     if (!grids || count <= 0 || !params_ok(params) || !results) return CIRRUS_ERR_INVALID_ARGUMENT;
     std::vector<cirrus::DevGrid*> gs(count);
     for (int k = 0; k < count; k++) {
@@ -603,9 +604,13 @@ cirrus_status cirrus_gmg_solve_grids(cirrus_grid* const* grids, int count, const
         for (int j = 0; j < k; j++)
             if (gs[j] == gs[k]) return CIRRUS_ERR_INVALID_ARGUMENT;  // one solve in flight per grid
     }
+    if (preconditioner == 1)
+        for (cirrus::DevGrid* g : gs)
+            if (!g->amg_ready) return CIRRUS_ERR_STATE;
     return guard([&] {
         cirrus::SolveParams p;
         to_internal(params, &p);
+        p.preconditioner = preconditioner;
         std::vector<std::vector<cirrus::SolveResult>> r;
         const int rc = cirrus::solve_grids(gs, p, S(stream), r);
         if (rc) return map_rc(rc);
@@ -622,6 +627,16 @@ cirrus_status cirrus_gmg_solve_grids(cirrus_grid* const* grids, int count, const
             }
         return CIRRUS_OK;
     });
+}
+}  // namespace
+
+cirrus_status cirrus_gmg_solve_grids(cirrus_grid* const* grids, int count, const cirrus_solve_params* params, void* stream,
+                                     cirrus_solve_result* results) {
+    return solve_grids_with(0, grids, count, params, stream, results);
+}
+cirrus_status cirrus_amg_solve_grids(cirrus_grid* const* grids, int count, const cirrus_solve_params* params, void* stream,
+                                     cirrus_solve_result* results) {
+    return solve_grids_with(1, grids, count, params, stream, results);
 }
 
 cirrus_status cirrus_gmg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream, cirrus_solve_result* result) {

@@ -392,6 +392,10 @@ cirrus_status cirrus_amg_vcycle(cirrus_grid* grid, int x_channel, int f_channel,
 cirrus_status cirrus_amg_solve(cirrus_grid* grid, const cirrus_solve_params* params, void* stream, cirrus_solve_result* result);
 cirrus_status cirrus_amg_solve_batch(cirrus_grid* grid, const cirrus_solve_params* params, const int* active, const double* tolerances,
                                      const int* pure_neumann, void* stream, cirrus_solve_result* results);
+/* cirrus_gmg_solve_grids with the AMG preconditioner: every grid prepared by cirrus_amg_prepare
+ * (CIRRUS_ERR_STATE otherwise). */
+cirrus_status cirrus_amg_solve_grids(cirrus_grid* const* grids, int count, const cirrus_solve_params* params, void* stream,
+                                     cirrus_solve_result* results);
 
 /* End-to-end variant for callers holding host arrays: copies b (num_tiles*512 floats, pinned or
  * pageable) to the device, solves, and copies x back into x_host. */

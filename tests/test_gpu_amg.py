@@ -108,6 +108,44 @@ def test_amg_batch_matches_instances_alone(built_cache):
     g.close()
 
 
+def test_amg_grids_solved_at_once(built_cache):
+    """Several prepared grids solved at once by the AMG variant (cirrus_amg_solve_grids, each
+    grid on its own stream) give each grid's own AMG solve bit for bit; an unprepared grid among
+    them is refused."""
+    names = ["sphere64_small", "ring64_small", "uniform32_small"]
+    bs = [built_cache(n) for n in names]
+    rhs = []
+    for b in bs:
+        g, _ = setup(b)
+        rhs.append(g.get_channel(1))
+        g.close()
+    s = AMGSolver()
+    grids = []
+    for b, r in zip(bs, rhs):
+        g = DeviceGrid(b.topology)
+        g.set_channel(1, r)
+        s.prepare_types_and_coeffs(g)
+        grids.append(g)
+    alone = []
+    for g, r in zip(grids, rhs):
+        g.set_channel(1, r)
+        g.set_channel(0, np.zeros_like(r))
+        alone.append((s.solve(g), g.get_channel(0)))
+    for g, r in zip(grids, rhs):
+        g.set_channel(1, r)
+        g.set_channel(0, np.zeros_like(r))
+    together = s.solve_grids(grids)
+    for g, (it_rel, x), res in zip(grids, alone, together):
+        assert res[0] == it_rel
+        assert np.array_equal(bits(g.get_channel(0)), bits(x))
+    fresh = DeviceGrid(bs[0].topology)
+    with pytest.raises(CirrusError):
+        s.solve_grids([grids[0], fresh])
+    fresh.close()
+    for g in grids:
+        g.close()
+
+
 def test_amg_needs_prepare(built_cache):
     b = built_cache("sphere64_small")
     g, _ = setup(b)
